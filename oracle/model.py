@@ -1,0 +1,612 @@
+"""ORACLE — test infrastructure only (tests/, smoke check, CPU-baseline leg).
+
+Single-rank CPU restatement of goSPL's per-timestep surface-process path with
+the reference's own Python orchestration and the C restatement of its Fortran
+kernels (``oracle/gospl_oracle.c``).  Every method cites the reference lines it
+follows.  MPI reductions and halo exchanges are identities on one rank.  The
+linear systems the reference hands to PETSc KSP (``rtol=1e-8``) are solved
+EXACTLY here (topological sweeps for the flow and SPL systems, a direct or
+1e-14 CG solve for diffusion): the oracle defines the exact solution of the
+assembled systems, which PETSc itself only approaches to ~1e-8.
+
+Grouped sums reproduce ``numpy_indexed.group_by(...).sum`` (stable mergesort of
+the keys, then ``np.add.reduceat``), so per-pit volumes round as in the
+reference.
+"""
+import numpy as np
+import scipy.sparse as sp
+import scipy.sparse.linalg as spla
+
+from . import fortran as F
+from . import mesh as M
+
+MISSING_DATA_SENTINEL = -1.0e8   # gospl/tools/constants.py:34
+GRAPH_OUTLIER_CAP = 1.0e7        # gospl/tools/constants.py:100
+
+
+def group_reduce(keys, values, op=np.add):
+    """numpy_indexed.group_by(keys).reduce(values, op): (unique, reduced)."""
+    keys = np.asarray(keys)
+    if keys.size == 0:
+        return keys[:0], np.zeros(0, dtype=np.asarray(values).dtype)
+    sorter = np.argsort(keys, kind="mergesort")
+    sk = keys[sorter]
+    flag = np.concatenate(([True], sk[1:] != sk[:-1]))
+    start = np.flatnonzero(flag)
+    return sk[start], op.reduceat(np.asarray(values)[sorter], start)
+
+
+class OracleModel:
+    """State and methods of goSPL's ``Model`` restricted to the hot path.
+
+    ``params`` keys: ``dt, tStart, tEnd, flowDir, K, d, m, Cda, Cdm, oFill,
+    sealevel, bc`` plus per-vertex ``rain`` (m/yr) and ``upsub`` (m/yr) arrays.
+    ``K`` may be a scalar (as in the reference) or a per-vertex array.
+    """
+
+    def __init__(self, coords, cells, elev, params, mesh=None, init_flow=True):
+        self.mesh = mesh if mesh is not None else M.build_mesh(coords, cells, params.get("bc", "oooo"))
+        M.load_mesh(self.mesh)
+        m = self.mesh
+        self.lpoints = m["nb"]
+        self.flatModel = m["flat"]
+        self.outletIDs = m["outlet"]
+        self.open_nodes = m["open_nodes"]
+        self.larea = m["larea"].copy()
+        self.maxarea = np.array([m["maxarea"]])
+        self.FVmesh_ngbID = m["ngb"].astype(np.int64)
+        self.gid = np.arange(self.lpoints, dtype=np.int32)
+        self.locIDs = np.arange(self.lpoints, dtype=np.int64)
+        self.inIDs = np.ones(self.lpoints, dtype=int)
+        self.maxnb = F.setmaxnb(self.lpoints)
+        edges = -np.ones((self.lpoints, 2), dtype=int)       # pitfilling.py:80-101
+        edges[self.outletIDs, 0] = self.outletIDs
+        edges[self.outletIDs, 1] = 1
+        self.borders = edges
+        self.outEdges = np.zeros(self.lpoints, dtype=int)
+
+        p = params
+        self.dt = float(p["dt"])
+        self.tStart = float(p.get("tStart", 0.0))
+        self.tEnd = float(p["tEnd"])
+        self.tNow = self.tStart
+        self.flowDir = int(p.get("flowDir", 8))
+        self.flowExp = 1.1                                   # inputparser.py:194
+        self.K = p["K"]
+        self.coeffd = float(p.get("d", 0.0))
+        self.spl_m = float(p.get("m", 0.5))
+        self.Cda = float(p.get("Cda", 0.0))
+        self.Cdm = float(p.get("Cdm", 0.0))
+        self.oFill = float(p.get("oFill", -6000.0))
+        self.sealevel = float(p.get("sealevel", 0.0))
+        self.rainMesh = np.asarray(p["rain"], dtype=np.float64)
+        up = p.get("upsub")
+        self.upsub = None if up is None else np.asarray(up, dtype=np.float64)
+
+        self.h = np.asarray(elev, dtype=np.float64).copy()
+        self.cumED = np.zeros(self.lpoints)
+        self.EbLocal = np.zeros(self.lpoints)
+        self.FAL = np.zeros(self.lpoints)
+        self.fillFAL = np.zeros(self.lpoints)
+        self.stats = []
+        self._hill_seaID = None
+        self._hill_mat = None
+        self.applyForces()
+        if init_flow:
+            self.flowAccumulation()
+
+    # ------------------------------------------------------------------ forcing
+    def applyForces(self):
+        """unstructuredmesh.py:743-794 (constant sea level, uniform-in-time rain)."""
+        self.rainVal = self.rainMesh.copy()
+        self.rainVal[self.rainVal < 0] = 0.0                 # unstructuredmesh.py:960
+        self.bL = self.rainVal * self.larea                  # unstructuredmesh.py:970
+        if self.upsub is not None:                           # unstructuredmesh.py:903-922
+            self.h = self.h + self.upsub * self.dt
+        if self.flatModel:
+            self.h = self._drainOpenEdges(self.h.copy())
+
+    def _drainOpenEdges(self, tmp):
+        """unstructuredmesh.py:796-901"""
+        open_nodes = self.open_nodes
+        if open_nodes.size == 0:
+            return tmp
+        ngb = self.FVmesh_ngbID
+        is_open = np.zeros(tmp.shape[0], dtype=bool)
+        is_open[open_nodes] = True
+        assigned = ~is_open
+        vals = tmp.copy()
+        pending = open_nodes
+        for _ in range(open_nodes.size + 1):
+            nb = ngb[pending]
+            valid = nb >= 0
+            nb_idx = np.where(valid, nb, 0)
+            usable = valid & assigned[nb_idx]
+            cand = np.where(usable, vals[nb_idx], np.inf)
+            mn = cand.min(axis=1)
+            ok = np.isfinite(mn)
+            vals[pending[ok]] = mn[ok]
+            assigned[pending[ok]] = True
+            pending = pending[~ok]
+            if pending.size == 0:
+                break
+        cur = tmp[open_nodes]
+        runmin = np.minimum(cur, vals[open_nodes])
+        marine = cur < self.sealevel
+        tmp[open_nodes] = np.where(marine, cur, runmin)
+        return tmp
+
+    # ------------------------------------------------------------- pit filling
+    def _fillFromEdges(self, mgraph):
+        """pitfilling.py:219-292 (pandas sort/dedup restated with numpy)."""
+        order = np.argsort(mgraph[:, 2], kind="stable")
+        cg = mgraph[order]
+        key = cg[:, 0].astype(np.int64) * (1 << 32) + cg[:, 1].astype(np.int64)
+        _, first = np.unique(key, return_index=True)
+        cgraph = cg[np.sort(first)]
+        nb_global = int(cgraph[:, 1].max()) + 2
+        src = cgraph[:, 0].astype(np.int64)
+        tgt = cgraph[:, 1].astype(np.int64)
+        uniq = np.unique(np.concatenate((src, tgt)))
+        if uniq[0] != 0:
+            uniq = np.concatenate((np.array([0], dtype=uniq.dtype), uniq))
+        nlab = len(uniq)
+        if uniq[-1] >= nb_global:
+            # the reference would raise IndexError writing ggraph[uniq] here
+            raise IndexError("spill graph label %d beyond target range %d" % (uniq[-1], nb_global))
+        cc = cgraph.copy()
+        cc[:, 0] = np.searchsorted(uniq, src)
+        cc[:, 1] = np.searchsorted(uniq, tgt)
+        c12 = cc[:, :2].astype(int).ravel()
+        cmax = np.max(np.bincount(c12)) + 1
+        elev, rank, nodes, spillID = F.fill_edges(nlab + 1, cc, cmax)
+        ggraph = -np.ones((nb_global, 5))
+        ggraph[:, 0] = 1.0e8
+        ggraph[uniq, 0] = elev[:nlab]
+        ggraph[uniq, 1] = nodes[:nlab]
+        ggraph[uniq, 2] = rank[:nlab]
+        gspill = spillID[:nlab].astype(np.int64)
+        valid = (gspill >= 0) & (gspill < nlab)
+        gspill[valid] = uniq[gspill[valid]]
+        ggraph[uniq, 3] = gspill
+        return ggraph
+
+    def _performFilling(self, hl, level, sed):
+        """pitfilling.py:557-702 at one rank."""
+        ledges = F.edge_tile(0.0, self.borders, hl)
+        out = np.where(ledges >= 0)[0]
+        localEdges = np.empty((len(out), 2), dtype=int)
+        localEdges[:, 0] = np.arange(self.lpoints)[out]
+        localEdges[:, 1] = ledges[out]
+        out = np.where(ledges == -2)[0]
+        inIDs = self.inIDs.copy()
+        inIDs[out] = 0
+        outEdges = self.outEdges.copy()
+        outEdges[out] = 0
+        gBounds = np.zeros(self.lpoints, dtype=int)
+        gBounds[np.where((ledges == 0) | (ledges == 2))[0]] = 1
+
+        lFill, label, gnb = F.fill_tile(localEdges, hl, inIDs)
+        lgth = 0
+        if gnb > 0:
+            graph = F.graph_nodes(gnb)
+            lgth = np.amax(graph[:, :2])
+        cgraph, graphnb = F.combine_edges(lFill, label, localEdges[:, 0], outEdges)
+        lgrph = 0
+        if graphnb > 0 and lgth > 0:
+            cgraph = np.concatenate((graph, cgraph[:graphnb]))
+            lgrph = len(cgraph)
+        elif graphnb > 0 and lgth == 0:
+            cgraph = cgraph[:graphnb]
+            lgrph = len(cgraph)
+        elif graphnb == 0 and lgth > 0:
+            cgraph = graph
+            lgrph = len(cgraph)
+        total = lgrph
+        if total == 0:
+            nlab = int(label.max()) + 2 if label.size else 2
+            graph = -np.ones((nlab, 5), dtype=float)
+        else:
+            graph = -np.ones((total, 5), dtype=float)
+            graph[:lgrph, :4] = cgraph
+            graph[:lgrph, 4] = 0
+            graph = self._fillFromEdges(graph)
+        keep = graph[:, 2].astype(int) == 0
+        proc = -np.ones(len(graph))
+        proc[keep] = graph[keep, 1]
+        keep = proc > -1
+        proc[keep] = gBounds[proc[keep].astype(int)]
+        ids = np.where(proc == 1)[0]
+        ids2 = np.where(graph[ids, 0] == graph[graph[ids, 3].astype(int), 0])[0]
+        graph[ids[ids2], 3] = 0.0
+        graph[graph[:, 0] < MISSING_DATA_SENTINEL, 0] = MISSING_DATA_SENTINEL
+        graph[graph[:, 0] > GRAPH_OUTLIER_CAP, 0] = MISSING_DATA_SENTINEL
+        lFill = F.fill_depressions(0.0, hl, lFill, label.astype(int), graph[:, 0])
+        if not sed:
+            idd = lFill < self.sealevel - level
+            lFill[idd] = hl[idd]
+        self.lFill = lFill.copy()
+
+    def _transferIDs(self, pitIDs):
+        """pitfilling.py:294-398 at one rank: consecutive ids 1..P."""
+        self.pitIDs = pitIDs.astype(int)
+        pitnbs = np.max(self.pitIDs) + 1
+        fillIDs = self.pitIDs >= 0
+        valpit = -np.ones(max(pitnbs, 0), dtype=int)
+        valpit[np.unique(self.pitIDs[fillIDs])] = 1
+        pitNb = np.where(valpit > 0)[0]
+        self.pitIDs = F.pits_cons(self.pitIDs, pitNb).astype(int)
+        return pitNb
+
+    def _dirFlats(self):
+        """pitfilling.py:400-519 at one rank."""
+        ids = self.pitIDs > -1
+        if ids.any():
+            pdir = F.fill_dir(self.lspillIDs, self.pitIDs, self.lFill)
+        else:
+            pdir = -np.ones(self.lpoints, dtype=np.int32)
+        stp = 0
+        while True:
+            prev = pdir
+            pdir = F.nghb_dir(self.pitIDs, self.lFill, pdir.astype(int))
+            stp += 1
+            if np.count_nonzero(pdir != prev) == 0 or stp > 10000:
+                break
+        self.pdir = pdir.astype(np.int64)
+        ngb = self.FVmesh_ngbID
+        n = self.lpoints
+        valid = ngb >= 0
+        cidx = np.where(valid, ngb, 0)
+        cpd = self.pdir[cidx]
+        ch = self.lFill[cidx]
+        clid = self.locIDs[cidx].astype(np.int64)
+        cand = (valid & (cpd > -1) & (cpd < self.pdir[:, None]) & (ch <= self.lFill[:, None])
+                & (self.pitIDs[:, None] > -1))
+        BIG = np.iinfo(np.int64).max
+        nid = np.int64(self.locIDs.max()) + 1
+        comp = np.where(cand, cpd.astype(np.int64) * nid + clid, BIG)
+        kbest = comp.argmin(axis=1)
+        rows = np.arange(n)
+        has = comp[rows, kbest] < BIG
+        self.flatDirs = np.full(n, -1, dtype=np.int32)
+        ispit = self.pitIDs > -1
+        self.flatDirs[ispit] = np.where(has[ispit], ngb[rows, kbest][ispit], rows[ispit]).astype(np.int32)
+        self.flatDirs[self.lspillIDs] = -1
+
+    def _getPitParams(self, hl, nbpits):
+        """pitfilling.py:521-555"""
+        ids = self.inIDs == 1
+        uids, vol = group_reduce(self.pitIDs[ids], (self.lFill[ids] - hl[ids]) * self.larea[ids])
+        _, hh = group_reduce(self.pitIDs[ids], self.lFill[ids], np.maximum)
+        _, dh = group_reduce(self.pitIDs[ids], self.lFill[ids] - hl[ids], np.maximum)
+        totv = np.zeros(nbpits)
+        hmax = np.full(nbpits, MISSING_DATA_SENTINEL)
+        diffh = np.zeros(nbpits)
+        ok = uids > -1
+        totv[uids[ok]] = vol[ok]
+        hmax[uids[ok]] = hh[ok]
+        diffh[uids[ok]] = dh[ok]
+        self.pitParams = np.empty((nbpits, 3))
+        self.pitParams[:, 0] = totv
+        self.pitParams[:, 1] = hmax
+        self.pitParams[:, 2] = diffh
+
+    def _pitInformation(self, hl, level, sed=False):
+        """pitfilling.py:704-847 at one rank."""
+        pitIDs = F.label_pits(level if sed else self.sealevel, self.lFill).astype(int)
+        pitIDs[self.outletIDs] = -1
+        pitNb = self._transferIDs(pitIDs)
+        pitnbs = len(pitNb) + 1
+        ngb = self.FVmesh_ngbID
+        valid = ngb >= 0
+        cidx = np.where(valid, ngb, 0)
+        hc = self.lFill[cidx]
+        hi = self.lFill[:, None]
+        lower = valid & (hc < hi)
+        eqlvl = valid & (hc == hi) & ((self.borders[cidx, 1] > 0) | (self.pitIDs[cidx] == -1))
+        ispit = self.pitIDs > -1
+        qual = (lower.any(axis=1) | eqlvl.any(axis=1)) & ispit & (self.inIDs == 1)
+        qidx = np.where(qual)[0]
+        bestlid = np.full(pitnbs, np.iinfo(np.int64).max, dtype=np.int64)
+        if qidx.size:
+            np.minimum.at(bestlid, self.pitIDs[qidx], self.locIDs[qidx])
+        spillIDs = -np.ones(pitnbs, dtype=int)
+        rank = -np.ones(pitnbs, dtype=int)
+        lspill = np.zeros(self.lpoints, dtype=np.int32)
+        if qidx.size:
+            star = qidx[self.locIDs[qidx] == bestlid[self.pitIDs[qidx]]]
+            isA = lower[star].any(axis=1)
+            sA = star[isA]
+            spillIDs[self.pitIDs[sA]] = sA
+            rank[self.pitIDs[sA]] = 0
+            lspill[sA] = 1
+            for i in star[~isA]:
+                knb = ngb[i][eqlvl[i]]
+                s = int(knb[np.argmin(self.locIDs[knb])])
+                spillIDs[self.pitIDs[i]] = s
+                rank[self.pitIDs[i]] = 0
+                lspill[s] = 1
+        self.lspillIDs = np.where(lspill == 1)[0]
+        spillIDs[rank != 0] = -1
+        self.pitInfo = np.zeros((pitnbs, 2), dtype=int)
+        self.pitInfo[:, 0] = spillIDs
+        self.pitInfo[:, 1] = rank
+        self.pitIDs[self.outletIDs] = -1
+        self._dirFlats()
+        idd = self.lFill <= self.sealevel
+        h = hl.copy()
+        self.lFill[idd] = hl[idd]
+        self.flatDirs[idd] = -1
+        if sed:
+            self.lFill[idd] = hl[idd]
+            self.flatDirs[idd] = -1
+        else:
+            h[h < self.sealevel] = self.sealevel
+        self._getPitParams(h, pitnbs)
+
+    def fillElevation(self, sed=False):
+        """pitfilling.py:849-903"""
+        hl = self.h.copy()
+        minh = hl.min()
+        if not self.flatModel:
+            minh += 1.0e-3
+        level = max(minh, self.sealevel + self.oFill)
+        self._performFilling(hl - level, level, sed)
+        self.lFill += level
+        self._pitInformation(hl, level, sed)
+        ids = self.pitParams[:, 0] > 0.0
+        dh = np.zeros((len(self.pitInfo), 6))
+        dh[ids, 0] = self.pitParams[ids, 1] - self.pitParams[ids, 2]
+        dh[ids, 1:] = np.expand_dims(self.pitParams[ids, 2] / 5.0, axis=1)
+        self.filled_lvl = np.cumsum(dh, axis=1)[:, 1:]
+        self.filled_vol = np.zeros((len(self.pitInfo), 5))
+        hl_clip = hl.copy()
+        if not sed:
+            hl_clip[hl_clip < self.sealevel] = self.sealevel
+        self.filled_vol[:, :-1] = F.getpitvol(self.filled_lvl[:, :-1], hl_clip, self.pitIDs, self.inIDs)
+        self.filled_vol[:, -1] = self.pitParams[:, 0]
+        self.level = level
+
+    # ------------------------------------------------------------ flow routing
+    def _buildFlowDirection(self, h, down=True):
+        """flowplex.py:480-544"""
+        self.seaID = np.where(self.lFill <= self.sealevel)[0]
+        rcv, dist, wgt = F.mfdreceivers(self.flowDir, self.flowExp, h, self.sealevel, self.gid)
+        self.rcvID = rcv.astype(int)
+        self.distRcv = dist
+        self.wghtVal = wgt
+        if down:
+            sum_weight = np.sum(self.wghtVal, axis=1)
+            ids = ((h == self.lFill) & (self.pitIDs > -1) & (self.flatDirs > -1) & (sum_weight == 0.0))
+            ids = ids.nonzero()[0]
+            self.rcvID[ids, :] = np.tile(ids, (self.flowDir, 1)).T
+            self.rcvID[ids, 0] = self.flatDirs[ids]
+            self.wghtVal[ids, :] = 0.0
+            self.wghtVal[ids, 0] = 1.0
+        if self.flatModel:
+            self.rcvID[self.outletIDs, :] = np.tile(self.outletIDs, (self.flowDir, 1)).T
+            self.distRcv[self.outletIDs, :] = 0.0
+            self.wghtVal[self.outletIDs, :] = 0.0
+        sum_weight = np.sum(self.wghtVal, axis=1)
+        lsink = sum_weight == 0.0
+        lsink[self.outletIDs] = False
+        lsink[self.seaID] = False
+        self.lsink = (lsink.astype(int) * self.inIDs) == 1
+
+    def _flow_solve(self, b):
+        """Exact (I - W^T) q = b for the current receivers (flowplex.py:429-478)."""
+        q, left = F.flow_solve(self.rcvID, self.wghtVal, b)
+        if left > 0:
+            n = self.lpoints
+            rows, cols, vals = [np.arange(n)], [np.arange(n)], [np.ones(n)]
+            for k in range(self.flowDir):
+                r = self.rcvID[:, k]
+                keep = r != np.arange(n)
+                rows.append(np.arange(n)[keep])
+                cols.append(r[keep])
+                vals.append(-self.wghtVal[keep, k])
+            A = sp.csr_matrix((np.concatenate(vals), (np.concatenate(rows), np.concatenate(cols))),
+                              shape=(n, n)).T.tocsc()
+            q = spla.spsolve(A, b)
+        self.stats.append(("flow_cycles", left))
+        return q
+
+    def _distributeDownstream(self, pitVol, FA, hl, step):
+        """flowplex.py:576-686 (no evaporation)."""
+        excess = False
+        FA = np.multiply(FA, self.inIDs)
+        uID, vol = group_reduce(self.pitIDs[self.lsink], FA[self.lsink])
+        inV = np.zeros(len(self.pitParams))
+        ok = uID > -1
+        inV[uID[ok]] = vol[ok]
+        eV = inV - pitVol
+        nFA = None
+        if (eV > 0.0).any():
+            eIDs = eV > 0.0
+            pitVol[eIDs] = 0.0
+            spillIDs = self.pitInfo[eIDs, 0]
+            localSpill = np.where(self.pitInfo[eIDs, 1] == 0)[0]
+            localPts = spillIDs[localSpill]
+            nFA = np.zeros(self.lpoints)
+            nFA[localPts] = eV[eIDs][localSpill]
+            ids = np.isin(self.pitIDs, np.where(eV > 0.0)[0])
+            self.waterFilled[ids] = self.lFill[ids]
+        if (eV < 0.0).any():
+            eIDs = np.where((eV < 0.0) & (inV > 0.0))[0]
+            pitVol[eIDs] += eV[eIDs]
+            nid = np.absolute(self.filled_vol[eIDs] - pitVol[eIDs][:, None]).argmin(axis=1)
+            fill_lvl = self.filled_lvl[eIDs, nid]
+            in_eIDs = np.isin(self.pitIDs, eIDs)
+            pit_fill_lvl = np.zeros(len(self.pitParams))
+            pit_fill_lvl[eIDs] = fill_lvl
+            node_lvl = pit_fill_lvl[self.pitIDs]
+            mask = in_eIDs & (self.waterFilled <= node_lvl)
+            self.waterFilled[mask] = node_lvl[mask]
+        if (eV > 1.0e-3).any():
+            if step == 100:
+                self._buildFlowDirection(self.lFill)
+            else:
+                self._buildFlowDirection(self.waterFilled)
+            rhs = nFA / self.dt
+            resid = rhs.sum()
+            self._cascade_resid = float(resid)
+            if resid > self.maxarea[0]:
+                excess = True
+                sol = self._flow_solve(rhs)
+                nFA = sol.copy() * self.dt
+                FA = nFA.copy()
+                FA[hl < self.waterFilled] = 0.0
+                self.FAL = self.FAL + FA / self.dt
+            else:
+                nFA = None
+        else:
+            nFA = None
+        return excess, pitVol, nFA
+
+    def flowAccumulation(self):
+        """flowplex.py:752-945 (no evaporation, no ice)."""
+        self.fillElevation(sed=False)
+        pitVol = self.pitParams[:, 0].copy()
+        hl = self.h.copy()
+        self._buildFlowDirection(hl, False)
+        self.wghtVali = self.wghtVal.copy()
+        self.rcvIDi = self.rcvID.copy()
+        self.distRcvi = self.distRcv.copy()
+        self.lsinki = self.lsink.copy()
+        rainA = self.bL.copy()
+        rainA[self.seaID] = 0.0
+        self.FAL = self._flow_solve(rainA)
+        self.waterFilled = hl.copy()
+        npass = 0
+        if (pitVol > 0.0).any():
+            FA = self.FAL.copy() * self.dt
+            excess = True
+            step = 0
+            best_resid = None
+            stall = 0
+            while excess and step <= 100:
+                excess, pitVol, FA = self._distributeDownstream(pitVol, FA, hl, step)
+                step += 1
+                npass += 1
+                if excess:
+                    resid = self._cascade_resid
+                    if best_resid is None or resid < best_resid * (1.0 - 1.0e-3):
+                        best_resid = resid
+                        stall = 0
+                    else:
+                        stall += 1
+                        if stall >= 3:
+                            break
+            FA = self.FAL.copy()
+            ids = (hl <= self.waterFilled) & (self.pitIDs > -1)
+            FA[ids] = 0.0
+            self.FAL = FA.copy()
+            FA[ids] = self.FAL.max() * 0.1
+            self.fillFAL = FA
+        else:
+            self.fillFAL = self.FAL.copy()
+        self.FAL = np.clip(self.FAL, 0.0, None)
+        self.fillFAL = np.clip(self.fillFAL, 0.0, None)
+        self.waterFilled = self.waterFilled - hl
+        self.cascade_passes = npass
+
+    # --------------------------------------------------------------------- SPL
+    def spl_coefficients(self, hOld):
+        """Per-receiver implicit SPL coefficients c_ik (SPL.py:45-114)."""
+        PA = self.FAL
+        K = np.asarray(self.K, dtype=np.float64)
+        Kbr = K * np.ones(self.lpoints) * np.ones(self.lpoints) * (self.rainVal ** self.coeffd)
+        Kbr *= self.dt * (PA ** self.spl_m)
+        Kbr[self.seaID] = 0.0
+        wght = self.wghtVali.copy()
+        wght[self.seaID, :] = 0.0
+        nodes = np.arange(self.lpoints)
+        c = np.zeros((self.lpoints, self.flowDir))
+        for k in range(self.flowDir):
+            dh = hOld - hOld[self.rcvIDi[:, k]]
+            limiter = np.divide(dh, dh + 1.0e-2, out=np.zeros_like(dh), where=dh != 0)
+            data = np.divide(Kbr * limiter, self.distRcvi[:, k], out=np.zeros_like(PA),
+                             where=self.distRcvi[:, k] != 0)
+            data = np.multiply(data, wght[:, k])
+            data[self.rcvIDi[:, k] == nodes] = 0.0
+            c[:, k] = data
+        return c
+
+    def erodepSPL(self):
+        """SPL.py:402-454 with _getEroDepRate SPL.py:260-366 (G = 0)."""
+        hOld = self.h.copy()
+        c = self.spl_coefficients(hOld)
+        stepED, left = F.spl_solve(self.rcvIDi, c, hOld)
+        if left > 0:
+            raise RuntimeError("SPL system is not triangular (%d rows left)" % left)
+        E = (stepED - hOld) / self.dt
+        if self.flatModel:
+            E[self.outletIDs] = 0.0
+        E[self.lsink] = 0.0
+        dz = E * self.dt
+        self.cumED = self.cumED + dz
+        self.h = self.h + dz
+        self.EbLocal = dz / self.dt
+
+    # --------------------------------------------------------------- hillslope
+    def diffusion_matrix(self, Kd):
+        """_buildDiffMat + _assembleDiffMat (hillslope.py:235-293) as CSR."""
+        coeffs = F.sethillslopecoeff(self.lpoints, Kd)
+        if self.flatModel:
+            coeffs[self.outletIDs, 1:] = 0.0
+            coeffs[self.outletIDs, 0] = 1.0
+        n = self.lpoints
+        rows = [np.arange(n)]
+        cols = [np.arange(n)]
+        vals = [coeffs[:, 0]]
+        for k in range(self.maxnb):
+            data = coeffs[:, k + 1]
+            idx = self.FVmesh_ngbID[:, k].copy()
+            nz = data != 0.0
+            rows.append(np.arange(n)[nz])
+            cols.append(idx[nz])
+            vals.append(data[nz])
+        return sp.csr_matrix((np.concatenate(vals), (np.concatenate(rows), np.concatenate(cols))),
+                             shape=(n, n))
+
+    def _diffusion_solve(self, A, b):
+        if self.lpoints <= 300000:
+            return spla.spsolve(A.tocsc(), b)
+        # large meshes: CG on the area-weighted form to 1e-14, then check
+        d = self.larea
+        As = sp.diags(d) @ A
+        x, info = spla.cg(As, d * b, x0=b.copy(), rtol=1e-14, maxiter=5000)
+        return x
+
+    def getHillslope(self):
+        """hillslope.py:614-649 -> _hillSlope(smooth=0) hillslope.py:90-233."""
+        self.seaID = np.where(self.h <= self.sealevel)[0]
+        if self.Cda == 0.0 and self.Cdm == 0.0:
+            return
+        hOld = self.h.copy()
+        if self._hill_mat is None or not np.array_equal(self.seaID, self._hill_seaID):
+            Cd = np.full(self.lpoints, self.Cda)
+            Cd[self.seaID] = self.Cdm
+            self._hill_mat = self.diffusion_matrix(Cd * self.dt)
+            self._hill_seaID = self.seaID.copy()
+        hNew = self._diffusion_solve(self._hill_mat, hOld)
+        tmp = hNew - hOld
+        self.cumED = self.cumED + tmp
+        self.h = hNew
+        self.EbLocal = self.EbLocal + tmp / self.dt
+
+    # ------------------------------------------------------------------- loop
+    def step(self):
+        """One iteration of runProcesses with fast=False, nodep=True (model.py:347-453)."""
+        self.flowAccumulation()
+        self.erodepSPL()
+        self.getHillslope()
+        if self.tNow < self.tEnd:
+            self.applyForces()
+        self.tNow += self.dt
+
+    def runProcesses(self):
+        while self.tNow <= self.tEnd:
+            if self.tNow == self.tEnd:
+                break
+            self.step()
