@@ -1,0 +1,185 @@
+// extern "C" boundary of libgospl_b200.so (declarations in include/gospl_b200.h).
+#include <cstring>
+#include <exception>
+#include <string>
+
+#include "gs_plan.cuh"
+
+namespace gs {
+
+static thread_local std::string g_msg;
+static thread_local int g_code = GS_OK;
+
+void set_error(int code, const std::string& msg) {
+    g_code = code;
+    g_msg = msg;
+}
+int last_code() { return g_code; }
+
+int plan_create(int64_t nb, const int32_t* nnb, const int32_t* ngb, const double* elgt, const double* vdist,
+                const double* farea, const double* larea, const int32_t* outlet_ids, int64_t n_outlet,
+                const int32_t* open_ids, int64_t n_open, int flat, int flow_dir, gs_plan** out);
+int plan_destroy(gs_plan* p);
+
+}  // namespace gs
+
+#define GS_GUARD(body)                                                        \
+    try {                                                                     \
+        body                                                                  \
+    } catch (const std::exception& e) {                                       \
+        gs::set_error(GS_EINVAL, std::string("exception: ") + e.what());     \
+        return GS_EINVAL;                                                     \
+    } catch (...) {                                                           \
+        gs::set_error(GS_EINVAL, "unknown exception");                       \
+        return GS_EINVAL;                                                     \
+    }
+
+#define NEED(p)                                                               \
+    do {                                                                      \
+        if (!(p)) {                                                           \
+            gs::set_error(GS_EINVAL, std::string("null argument: ") + #p);    \
+            return GS_EINVAL;                                                 \
+        }                                                                     \
+    } while (0)
+
+extern "C" {
+
+int gs_version(void) { return 100; }
+
+int gs_last_error(char* buf, int64_t len) {
+    if (buf && len > 0) {
+        std::strncpy(buf, gs::g_msg.c_str(), (size_t)len - 1);
+        buf[len - 1] = 0;
+    }
+    return gs::g_code;
+}
+
+int gs_plan_create(int64_t nb, const int32_t* nnb, const int32_t* ngb, const double* elgt,
+                   const double* vdist, const double* farea, const double* larea,
+                   const int32_t* outlet_ids, int64_t n_outlet, const int32_t* open_ids, int64_t n_open,
+                   int32_t flat_model, int32_t flow_dir, gs_plan** out) {
+    GS_GUARD(return gs::plan_create(nb, nnb, ngb, elgt, vdist, farea, larea, outlet_ids, n_outlet, open_ids,
+                                    n_open, flat_model, flow_dir, out);)
+}
+
+int gs_plan_destroy(gs_plan* plan) { GS_GUARD(return gs::plan_destroy(plan);) }
+
+int gs_plan_set_stream(gs_plan* plan, void* stream) {
+    NEED(plan);
+    plan->stream = (cudaStream_t)stream;
+    return GS_OK;
+}
+
+int64_t gs_plan_launches(const gs_plan* plan) { return plan ? plan->launches : -1; }
+
+int gs_mfdreceivers(gs_plan* plan, int32_t nrcv, double exp, const double* elev, double sl,
+                    const int32_t* gid, int32_t* rcv, double* dist, double* wgt) {
+    NEED(plan);
+    if (plan->n > 0) {
+        NEED(elev);
+        NEED(rcv);
+        NEED(dist);
+        NEED(wgt);
+    }
+    GS_GUARD(return gs::receivers(plan, nrcv, exp, elev, sl, gid, rcv, dist, wgt, nullptr);)
+}
+
+int gs_fill_elevation(gs_plan* plan, const double* h, double sealevel, double ofill, double* lfill,
+                      int32_t* pit_ids, int32_t* flat_dirs, int32_t* npits) {
+    NEED(plan);
+    if (plan->n > 0) {
+        NEED(h);
+        NEED(lfill);
+        NEED(pit_ids);
+        NEED(flat_dirs);
+    }
+    GS_GUARD({
+        gs_stats st{};
+        int s = gs::fill_elevation(plan, h, sealevel, ofill, lfill, pit_ids, flat_dirs, &st);
+        if (npits) *npits = plan->npits;
+        return s;
+    })
+}
+
+int gs_pit_tables(gs_plan* plan, double* pit_params, int32_t* pit_info, double* filled_lvl,
+                  double* filled_vol) {
+    NEED(plan);
+    const size_t np1 = (size_t)plan->npits + 1;
+    if (pit_params)
+        GS_CUDA(cudaMemcpyAsync(pit_params, plan->pit_params, sizeof(double) * 3 * np1, cudaMemcpyDeviceToDevice,
+                                plan->stream));
+    if (pit_info)
+        GS_CUDA(cudaMemcpyAsync(pit_info, plan->pit_info, sizeof(int) * 2 * np1, cudaMemcpyDeviceToDevice,
+                                plan->stream));
+    if (filled_lvl)
+        GS_CUDA(cudaMemcpyAsync(filled_lvl, plan->filled_lvl, sizeof(double) * 5 * np1,
+                                cudaMemcpyDeviceToDevice, plan->stream));
+    if (filled_vol)
+        GS_CUDA(cudaMemcpyAsync(filled_vol, plan->filled_vol, sizeof(double) * 5 * np1,
+                                cudaMemcpyDeviceToDevice, plan->stream));
+    return GS_OK;
+}
+
+int gs_flow_accumulation(gs_plan* plan, const double* h, const double* bl, double sealevel, double ofill,
+                         double dt, double* fal, double* fill_fal, double* water_filled, double* lfill,
+                         int32_t* pit_ids, int32_t* flat_dirs, int32_t* rcv_i, double* dist_i, double* wgt_i,
+                         uint8_t* lsink, uint8_t* sea, gs_stats* stats) {
+    NEED(plan);
+    if (plan->n > 0) {
+        NEED(h); NEED(bl); NEED(fal); NEED(fill_fal); NEED(water_filled); NEED(lfill); NEED(pit_ids);
+        NEED(flat_dirs); NEED(rcv_i); NEED(dist_i); NEED(wgt_i); NEED(lsink); NEED(sea);
+    }
+    if (!(dt > 0)) {
+        gs::set_error(GS_EINVAL, "dt must be positive");
+        return GS_EINVAL;
+    }
+    GS_GUARD({
+        gs_stats st{};
+        int s = gs::flow_accumulation(plan, h, bl, sealevel, ofill, dt, fal, fill_fal, water_filled, lfill,
+                                      pit_ids, flat_dirs, rcv_i, dist_i, wgt_i, lsink, sea, &st);
+        st.status = s;
+        if (stats) *stats = st;
+        return s;
+    })
+}
+
+int gs_erodep_spl(gs_plan* plan, double* h, double* cum_ed, double* eb, const double* fal, const double* rain,
+                  double k_scalar, const double* k_field, double d, double m, double dt, const int32_t* rcv_i,
+                  const double* dist_i, const double* wgt_i, const uint8_t* lsink, const uint8_t* sea,
+                  gs_stats* stats) {
+    NEED(plan);
+    if (plan->n > 0) {
+        NEED(h); NEED(cum_ed); NEED(eb); NEED(fal); NEED(rain); NEED(rcv_i); NEED(dist_i); NEED(wgt_i);
+        NEED(lsink); NEED(sea);
+    }
+    if (!(dt > 0)) {
+        gs::set_error(GS_EINVAL, "dt must be positive");
+        return GS_EINVAL;
+    }
+    GS_GUARD(return gs::erodep_spl(plan, h, cum_ed, eb, fal, rain, k_scalar, k_field, d, m, dt, rcv_i, dist_i,
+                                   wgt_i, lsink, sea, stats);)
+}
+
+int gs_hillslope(gs_plan* plan, double* h, double* cum_ed, double* eb, double sealevel, double cda, double cdm,
+                 double dt, double rtol, int32_t max_iter, gs_stats* stats) {
+    NEED(plan);
+    if (plan->n > 0) {
+        NEED(h); NEED(cum_ed); NEED(eb);
+    }
+    if (!(dt > 0) || !(rtol > 0) || max_iter < 1) {
+        gs::set_error(GS_EINVAL, "dt, rtol must be positive and max_iter >= 1");
+        return GS_EINVAL;
+    }
+    GS_GUARD(return gs::hillslope(plan, h, cum_ed, eb, sealevel, cda, cdm, dt, rtol, max_iter, stats);)
+}
+
+int gs_apply_forces(gs_plan* plan, double* h, const double* rain, const double* upsub, double dt,
+                    double sealevel, double* bl) {
+    NEED(plan);
+    if (plan->n > 0) {
+        NEED(h); NEED(rain); NEED(bl);
+    }
+    GS_GUARD(return gs::apply_forces(plan, h, rain, upsub, dt, sealevel, bl);)
+}
+
+}  // extern "C"

@@ -1,0 +1,285 @@
+// Linear hillslope diffusion: hillSLP.getHillslope -> _hillSlope(smooth=0)
+// (gospl/sed/hillslope.py:90-233, 614-649) with the finite-volume stencil of
+// sethillslopecoeff (fortran/functions.F90:901-938) and the outlet identity
+// rows of _buildDiffMat (hillslope.py:235-257).
+//
+// Row k of (I + L):  diag 1 + sum_p v_kp,  off -v_kp,
+//     v_kp = 0.5 (Kd_k + Kd_p) / A_k * vDist_kp / eLgt_kp.
+// Multiplying row k by A_k gives a symmetric positive-definite operator
+// (vDist and eLgt are per-edge), so the system is solved with
+// Jacobi-preconditioned CG on  A (I + L) h = A hOld,  outlet rows (and rows of
+// zero area, which carry no equation) held at hOld.  The matrix is rebuilt only
+// when the land/sea mask changes, like the reference's cached operator.
+#include "gs_plan.cuh"
+
+namespace gs {
+
+__global__ void k_diff_coef(int n, int W, int flat, const double* __restrict__ h, double sl,
+                            double cda, double cdm, double dt, const int* __restrict__ nbr,
+                            const int8_t* __restrict__ nnb, const double* __restrict__ elen,
+                            const double* __restrict__ vdist, const double* __restrict__ farea,
+                            const uint8_t* __restrict__ outlet, double* coef, uint8_t* dsea) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const double ck = ((h[k] <= sl) ? cdm : cda) * dt;
+    dsea[k] = h[k] <= sl ? 1 : 0;
+    double diag = 0.0;
+    for (int s = 0; s < W; s++) coef[(size_t)(s + 1) * n + k] = 0.0;
+    if (farea[k] > 0) {
+        double s1 = 0.0;
+        const double ak = farea[k];
+        for (int s = 0; s < nnb[k]; s++) {
+            double vd = vdist[(size_t)s * n + k];
+            if (vd > 0.0) {
+                int j = nbr[(size_t)s * n + k];
+                double cn = ((h[j] <= sl) ? cdm : cda) * dt;
+                double c = 0.5 * (ck + cn) / ak;
+                double v = c * vd / elen[(size_t)s * n + k];
+                s1 = s1 + v;
+                coef[(size_t)(s + 1) * n + k] = -v;
+            }
+        }
+        diag = 1.0 + s1;
+    }
+    if (flat && outlet[k]) {
+        diag = 1.0;
+        for (int s = 0; s < W; s++) coef[(size_t)(s + 1) * n + k] = 0.0;
+    }
+    coef[k] = diag;
+}
+
+__device__ __forceinline__ bool diff_fixed(int k, int flat, const uint8_t* outlet, const double* farea) {
+    return (flat && outlet[k]) || !(farea[k] > 0);
+}
+
+// y = A_k * ((I+L) x)_k over free rows; fixed rows and fixed columns excluded
+__device__ __forceinline__ double diff_row(int k, int n, int W, const int* nbr, const int8_t* nnb,
+                                           const double* coef, const double* farea, const uint8_t* outlet,
+                                           int flat, const double* x, bool free_cols_only) {
+    double y = coef[k] * x[k];
+    for (int s = 0; s < nnb[k]; s++) {
+        double o = coef[(size_t)(s + 1) * n + k];
+        if (o == 0.0) continue;
+        int j = nbr[(size_t)s * n + k];
+        if (free_cols_only && diff_fixed(j, flat, outlet, farea)) continue;
+        y = y + o * x[j];
+    }
+    return farea[k] * y;
+}
+
+__global__ void k_cg_init(int n, int W, int flat, const int* __restrict__ nbr, const int8_t* __restrict__ nnb,
+                          const double* __restrict__ coef, const double* __restrict__ farea,
+                          const uint8_t* __restrict__ outlet, const double* __restrict__ hold, double* x,
+                          double* b, double* r, double* z, double* pp) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    x[k] = hold[k];
+    if (diff_fixed(k, flat, outlet, farea)) {
+        b[k] = 0.0; r[k] = 0.0; z[k] = 0.0; pp[k] = 0.0;
+        return;
+    }
+    // right-hand side A_k hOld_k minus known (fixed) columns
+    double bk = hold[k];
+    for (int s = 0; s < nnb[k]; s++) {
+        double o = coef[(size_t)(s + 1) * n + k];
+        if (o == 0.0) continue;
+        int j = nbr[(size_t)s * n + k];
+        if (diff_fixed(j, flat, outlet, farea)) bk = bk - o * hold[j];
+    }
+    bk = farea[k] * bk;
+    b[k] = bk;
+    double ax = diff_row(k, n, W, nbr, nnb, coef, farea, outlet, flat, hold, true);
+    double rk = bk - ax;
+    r[k] = rk;
+    double zk = rk / (farea[k] * coef[k]);
+    z[k] = zk;
+    pp[k] = zk;
+}
+
+__global__ void k_cg_spmv(int n, int W, int flat, const int* __restrict__ nbr, const int8_t* __restrict__ nnb,
+                          const double* __restrict__ coef, const double* __restrict__ farea,
+                          const uint8_t* __restrict__ outlet, const double* __restrict__ pp, double* ap) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    ap[k] = diff_fixed(k, flat, outlet, farea) ? 0.0
+                                               : diff_row(k, n, W, nbr, nnb, coef, farea, outlet, flat, pp, true);
+}
+
+// fixed-shape block partial dot products (deterministic)
+template <int NV>
+__global__ void k_dots(int n, const double* __restrict__ a0, const double* __restrict__ b0,
+                       const double* __restrict__ a1, const double* __restrict__ b1, double* part) {
+    __shared__ double sh[NV][256];
+    double acc[NV];
+    for (int v = 0; v < NV; v++) acc[v] = 0.0;
+    int per = (n + gridDim.x - 1) / gridDim.x;
+    int lo = blockIdx.x * per, hi = lo + per < n ? lo + per : n;
+    for (int i = lo + threadIdx.x; i < hi; i += blockDim.x) {
+        acc[0] += a0[i] * b0[i];
+        if (NV > 1) acc[NV - 1] += a1[i] * b1[i];
+    }
+    for (int v = 0; v < NV; v++) sh[v][threadIdx.x] = acc[v];
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s)
+            for (int v = 0; v < NV; v++) sh[v][threadIdx.x] += sh[v][threadIdx.x + s];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+        for (int v = 0; v < NV; v++) part[v * gridDim.x + blockIdx.x] = sh[v][0];
+}
+
+__global__ void k_dots_final(int parts, int nv, const double* __restrict__ part, double* out) {
+    __shared__ double sh[1024];
+    for (int v = 0; v < nv; v++) {
+        double acc = 0.0;
+        for (int i = threadIdx.x; i < parts; i += blockDim.x) acc += part[v * parts + i];
+        sh[threadIdx.x] = acc;
+        __syncthreads();
+        for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+            if (threadIdx.x < s) sh[threadIdx.x] += sh[threadIdx.x + s];
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) out[v] = sh[0];
+        __syncthreads();
+    }
+}
+
+// x += alpha p ; r -= alpha Ap ; z = r / diag  with alpha = rz / pAp (device scalars)
+__global__ void k_cg_update(int n, int flat, const uint8_t* __restrict__ outlet, const double* __restrict__ farea,
+                            const double* __restrict__ coef, const double* __restrict__ sc, double* x,
+                            double* r, double* z, const double* __restrict__ pp, const double* __restrict__ ap) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    if (diff_fixed(k, flat, outlet, farea)) return;
+    const double alpha = sc[0] / sc[1];
+    x[k] = x[k] + alpha * pp[k];
+    double rk = r[k] - alpha * ap[k];
+    r[k] = rk;
+    z[k] = rk / (farea[k] * coef[k]);
+}
+
+// p = z + beta p, beta = rz_new / rz_old; rotate rz
+__global__ void k_cg_dir(int n, const double* __restrict__ sc_new, double* sc, const double* __restrict__ z,
+                         double* pp) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const double beta = sc_new[0] / sc[0];
+    if (k < n) pp[k] = z[k] + beta * pp[k];
+}
+
+__global__ void k_cg_rotate(const double* __restrict__ sc_new, double* sc) {
+    sc[0] = sc_new[0];
+}
+
+__global__ void k_hill_apply(int n, const double* __restrict__ hold, const double* __restrict__ x, double dt,
+                             double* h, double* cum_ed, double* eb) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    double dz = x[k] - hold[k];
+    cum_ed[k] = cum_ed[k] + dz;
+    h[k] = x[k];
+    eb[k] = eb[k] + dz / dt;
+}
+
+__global__ void k_copy_d2(int n, const double* __restrict__ a, double* b) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) b[i] = a[i];
+}
+
+__global__ void k_mask_changed(int n, const double* __restrict__ h, double sl, const uint8_t* __restrict__ dsea,
+                               int* flag) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < n && (uint8_t)(h[k] <= sl) != dsea[k]) *flag = 1;
+}
+
+int hillslope(gs_plan* p, double* h, double* cum_ed, double* eb, double sealevel, double cda,
+              double cdm, double dt, double rtol, int max_iter, gs_stats* st) {
+    const int n = (int)p->n;
+    if (n == 0 || (cda == 0.0 && cdm == 0.0)) return GS_OK;
+    const int B = 256, G = grid_for(n, B);
+    const int PARTS = 512;
+    int rebuild = 1;
+    if (p->dvalid && p->dvalid_dt == dt && p->dvalid_cda == cda && p->dvalid_cdm == cdm) {
+        GS_CUDA(cudaMemsetAsync(p->i_scalar + 12, 0, sizeof(int), p->stream));
+        launch(p, k_mask_changed, G, B, n, (const double*)h, sealevel, (const uint8_t*)p->dsea, p->i_scalar + 12);
+        GS_LAUNCH();
+        GS_CUDA(cudaMemcpyAsync(&rebuild, p->i_scalar + 12, sizeof(int), cudaMemcpyDeviceToHost, p->stream));
+        GS_CUDA(cudaStreamSynchronize(p->stream));
+    }
+    if (rebuild) {
+        launch(p, k_diff_coef, G, B, n, p->W, p->flat, (const double*)h, sealevel, cda, cdm, dt,
+               (const int*)p->nbr, (const int8_t*)p->nnb, (const double*)p->elen, (const double*)p->vdist,
+               (const double*)p->farea, (const uint8_t*)p->outlet, p->dcoef, p->dsea);
+        GS_LAUNCH();
+        p->dvalid = 1;
+        p->dvalid_dt = dt;
+        p->dvalid_cda = cda;
+        p->dvalid_cdm = cdm;
+    }
+    double* hold = p->hl;
+    launch(p, k_copy_d2, G, B, n, (const double*)h, hold);
+    launch(p, k_cg_init, G, B, n, p->W, p->flat, (const int*)p->nbr, (const int8_t*)p->nnb,
+           (const double*)p->dcoef, (const double*)p->farea, (const uint8_t*)p->outlet, (const double*)hold,
+           p->cg_x, p->cg_b, p->cg_r, p->cg_z, p->cg_p);
+    // sc[0] = rz, sc[1] = pAp ; sc[2] = rz_new, sc[3] = rr ; sc[4] = bb
+    double* sc = p->red + 4096;
+    launch(p, k_dots<2>, PARTS, 256, n, (const double*)p->cg_r, (const double*)p->cg_z,
+           (const double*)p->cg_b, (const double*)p->cg_b, p->red);
+    launch(p, k_dots_final, 1, 1024, PARTS, 2, (const double*)p->red, sc + 5);
+    GS_LAUNCH();
+    double hs[8];
+    GS_CUDA(cudaMemcpyAsync(hs, sc + 5, 2 * sizeof(double), cudaMemcpyDeviceToHost, p->stream));
+    GS_CUDA(cudaStreamSynchronize(p->stream));
+    const double bnorm = sqrt(hs[1]);
+    GS_CUDA(cudaMemcpyAsync(sc, sc + 5, sizeof(double), cudaMemcpyDeviceToDevice, p->stream));   // rz
+    double relres = 0.0;
+    int it = 0;
+    if (bnorm > 0.0) {
+        // residual of the warm start
+        launch(p, k_dots<1>, PARTS, 256, n, (const double*)p->cg_r, (const double*)p->cg_r,
+               (const double*)nullptr, (const double*)nullptr, p->red);
+        launch(p, k_dots_final, 1, 1024, PARTS, 1, (const double*)p->red, sc + 3);
+        GS_LAUNCH();
+        GS_CUDA(cudaMemcpyAsync(hs, sc + 3, sizeof(double), cudaMemcpyDeviceToHost, p->stream));
+        GS_CUDA(cudaStreamSynchronize(p->stream));
+        relres = sqrt(hs[0]) / bnorm;
+        while (relres > rtol && it < max_iter) {
+            launch(p, k_cg_spmv, G, B, n, p->W, p->flat, (const int*)p->nbr, (const int8_t*)p->nnb,
+                   (const double*)p->dcoef, (const double*)p->farea, (const uint8_t*)p->outlet,
+                   (const double*)p->cg_p, p->cg_ap);
+            launch(p, k_dots<1>, PARTS, 256, n, (const double*)p->cg_p, (const double*)p->cg_ap,
+                   (const double*)nullptr, (const double*)nullptr, p->red);
+            launch(p, k_dots_final, 1, 1024, PARTS, 1, (const double*)p->red, sc + 1);
+            launch(p, k_cg_update, G, B, n, p->flat, (const uint8_t*)p->outlet, (const double*)p->farea,
+                   (const double*)p->dcoef, (const double*)sc, p->cg_x, p->cg_r, p->cg_z,
+                   (const double*)p->cg_p, (const double*)p->cg_ap);
+            launch(p, k_dots<2>, PARTS, 256, n, (const double*)p->cg_r, (const double*)p->cg_z,
+                   (const double*)p->cg_r, (const double*)p->cg_r, p->red);
+            launch(p, k_dots_final, 1, 1024, PARTS, 2, (const double*)p->red, sc + 2);
+            launch(p, k_cg_dir, G, B, n, (const double*)(sc + 2), sc, (const double*)p->cg_z, p->cg_p);
+            launch(p, k_cg_rotate, 1, 1, (const double*)(sc + 2), sc);
+            GS_LAUNCH();
+            GS_CUDA(cudaMemcpyAsync(hs, sc + 3, sizeof(double), cudaMemcpyDeviceToHost, p->stream));
+            GS_CUDA(cudaStreamSynchronize(p->stream));
+            relres = sqrt(hs[0]) / bnorm;
+            it++;
+            if (!(relres == relres)) {
+                set_error(GS_ENONFINITE, "hillslope CG produced a non-finite residual");
+                return GS_ENONFINITE;
+            }
+        }
+    }
+    if (st) {
+        st->cg_iters = it;
+        st->cg_relres = relres;
+    }
+    launch(p, k_hill_apply, G, B, n, (const double*)hold, (const double*)p->cg_x, dt, h, cum_ed, eb);
+    GS_LAUNCH();
+    if (relres > rtol) {
+        set_error(GS_EMAXITER, "hillslope CG reached max_iter");
+        return GS_EMAXITER;
+    }
+    return GS_OK;
+}
+
+}  // namespace gs

@@ -1,0 +1,306 @@
+// Flow accumulation with the downstream lake cascade:
+// FAMesh.flowAccumulation (flowplex.py:752-945) and _distributeDownstream
+// (flowplex.py:576-686) without evaporation or ice.
+//
+// Control flow mirrors the reference pass by pass; the per-pit decisions
+// (overflow, partial fill level, thresholds eV > 0, eV > 1e-3) run in small
+// per-pit kernels, and only the handful of flags that steer the pass loop are
+// read back to the host.
+#include "gs_plan.cuh"
+
+namespace gs {
+
+enum { F_POS = 1, F_NEG = 2, F_BIG = 4 };
+
+// deterministic sum / max (fixed two-stage tree, independent of timing)
+__global__ void k_partial_sum(int64_t n, const double* __restrict__ x, double* part) {
+    __shared__ double sh[256];
+    double acc = 0.0;
+    int64_t per = (n + gridDim.x - 1) / gridDim.x;
+    int64_t lo = (int64_t)blockIdx.x * per, hi = lo + per < n ? lo + per : n;
+    for (int64_t i = lo + threadIdx.x; i < hi; i += blockDim.x) acc += x[i];
+    sh[threadIdx.x] = acc;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s) sh[threadIdx.x] += sh[threadIdx.x + s];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) part[blockIdx.x] = sh[0];
+}
+
+__global__ void k_final_sum(int m, const double* __restrict__ part, double* out) {
+    __shared__ double sh[1024];
+    double acc = 0.0;
+    for (int i = threadIdx.x; i < m; i += blockDim.x) acc += part[i];
+    sh[threadIdx.x] = acc;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s) sh[threadIdx.x] += sh[threadIdx.x + s];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *out = sh[0];
+}
+
+__global__ void k_max_key(int64_t n, const double* __restrict__ x, unsigned long long* out) {
+    unsigned long long best = 0ULL;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        unsigned long long k = dkey(x[i]);
+        best = k > best ? k : best;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        unsigned long long v = __shfl_xor_sync(0xffffffffu, best, o);
+        best = v > best ? v : best;
+    }
+    if ((threadIdx.x & 31) == 0) atomicMax(out, best);
+}
+
+static int sum_to_host(gs_plan* p, const double* x, int64_t n, double* out) {
+    const int PARTS = 1024;
+    launch(p, k_partial_sum, PARTS, 256, n, x, p->red);
+    launch(p, k_final_sum, 1, 1024, PARTS, (const double*)p->red, p->red + PARTS);
+    GS_LAUNCH();
+    GS_CUDA(cudaMemcpyAsync(out, p->red + PARTS, sizeof(double), cudaMemcpyDeviceToHost, p->stream));
+    GS_CUDA(cudaStreamSynchronize(p->stream));
+    return GS_OK;
+}
+
+// ---------------------------------------------------------------------------
+__global__ void k_fill_i32(int n, int* a, int v) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) a[i] = v;
+}
+
+__global__ void k_rain_sea(int n, const double* __restrict__ bl, const uint8_t* __restrict__ sea,
+                           double* b) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) b[i] = sea[i] ? 0.0 : bl[i];
+}
+
+__global__ void k_copy(int64_t n, const double* __restrict__ a, double* b) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) b[i] = a[i];
+}
+
+__global__ void k_scale(int64_t n, const double* __restrict__ a, double s, double* b) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) b[i] = a[i] * s;
+}
+
+__global__ void k_div(int64_t n, const double* __restrict__ a, double s, double* b) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) b[i] = a[i] / s;
+}
+
+__global__ void k_any_pos(int np1, const double* __restrict__ params, int* flag) {
+    int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p < np1 && params[3 * p] > 0.0) *flag = 1;
+}
+
+__global__ void k_pitvol_init(int np1, const double* __restrict__ params, double* vol) {
+    int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p < np1) vol[p] = params[3 * p];
+}
+
+// per-pit decisions of one _distributeDownstream pass
+__global__ void k_cascade_pits(int np1, const double* __restrict__ inV, double* vol,
+                               const double* __restrict__ fvol, const double* __restrict__ flvl,
+                               const int* __restrict__ info, double* ev, uint8_t* state,
+                               double* lvl, int* win, int* flags) {
+    int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= np1) return;
+    double in = inV[p];
+    double e = in - vol[p];
+    ev[p] = e;
+    uint8_t s = 0;
+    int f = 0;
+    if (e > 0.0) {
+        f |= F_POS;
+        s = 1;
+        vol[p] = 0.0;
+        if (info[2 * p + 1] == 0) atomicMax(&win[info[2 * p]], p);
+    }
+    if (e < 0.0) {
+        f |= F_NEG;
+        if (in > 0.0) {
+            s = 2;
+            double v = vol[p] + e;
+            vol[p] = v;
+            int best = 0;
+            double bd = fabs(fvol[5 * p] - v);
+            for (int k = 1; k < 5; k++) {
+                double d = fabs(fvol[5 * p + k] - v);
+                if (d < bd) { bd = d; best = k; }
+            }
+            lvl[p] = flvl[5 * p + best];
+        }
+    }
+    if (e > 1.0e-3) f |= F_BIG;
+    state[p] = s;
+    if (f) atomicOr(flags, f);
+}
+
+__global__ void k_cascade_spill(int np1, const double* __restrict__ ev, const uint8_t* __restrict__ state,
+                                const int* __restrict__ info, const int* __restrict__ win, double* nfa) {
+    int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= np1) return;
+    if (state[p] == 1 && info[2 * p + 1] == 0 && win[info[2 * p]] == p) nfa[info[2 * p]] = ev[p];
+}
+
+__global__ void k_cascade_cells(int n, const int* __restrict__ pit, const uint8_t* __restrict__ state,
+                                const double* __restrict__ lvl, const double* __restrict__ lfill,
+                                double* wf) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int p = pit[i];
+    if (p < 0) return;
+    uint8_t s = state[p];
+    if (s == 1) wf[i] = lfill[i];
+    else if (s == 2) {
+        double l = lvl[p];
+        if (wf[i] <= l) wf[i] = l;
+    }
+}
+
+__global__ void k_cascade_accum(int n, const double* __restrict__ sol, double dt,
+                                const double* __restrict__ h, const double* __restrict__ wf,
+                                double* nfa, double* fal) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double v = sol[i] * dt;
+    nfa[i] = v;
+    double fa = (h[i] < wf[i]) ? 0.0 : v;
+    fal[i] = fal[i] + fa / dt;
+}
+
+__global__ void k_lake_zero(int n, const double* __restrict__ h, const double* __restrict__ wf,
+                            const int* __restrict__ pit, double* fal) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    if (h[i] <= wf[i] && pit[i] > -1) fal[i] = 0.0;
+}
+
+__global__ void k_flow_final(int n, int lakes, const double* __restrict__ h, const double* __restrict__ wf,
+                             const int* __restrict__ pit, const unsigned long long* __restrict__ maxkey,
+                             double* fal, double* fill_fal, double* water) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double f = fal[i];
+    double ff = f;
+    if (lakes && h[i] <= wf[i] && pit[i] > -1) ff = dkey_inv(*maxkey) * 0.1;
+    fal[i] = f < 0.0 ? 0.0 : f;
+    fill_fal[i] = ff < 0.0 ? 0.0 : ff;
+    water[i] = wf[i] - h[i];
+}
+
+static int read_flag(gs_plan* p, int* out) {
+    GS_CUDA(cudaMemcpyAsync(out, p->i_scalar + 8, sizeof(int), cudaMemcpyDeviceToHost, p->stream));
+    GS_CUDA(cudaStreamSynchronize(p->stream));
+    return GS_OK;
+}
+
+int flow_accumulation(gs_plan* p, const double* h, const double* bl, double sealevel, double ofill,
+                      double dt, double* fal, double* fill_fal, double* water, double* lfill,
+                      int* pit_ids, int* flat_dirs, int* rcv_i, double* dist_i, double* wgt_i,
+                      uint8_t* lsink, uint8_t* sea, gs_stats* st) {
+    const int n = (int)p->n;
+    if (n == 0) return GS_OK;
+    const int B = 256, G = grid_for(n, B);
+    GS_TRY(fill_elevation(p, h, sealevel, ofill, lfill, pit_ids, flat_dirs, st));
+    const int P = p->npits, np1 = P + 1;
+
+    // receivers on the unfilled surface (down=False) and their snapshots
+    GS_TRY(flow_direction(p, h, false, lfill, pit_ids, flat_dirs, sealevel, rcv_i, dist_i, wgt_i,
+                          p->rslot_i, lsink, sea));
+    launch(p, k_rain_sea, G, B, n, bl, (const uint8_t*)sea, p->nfa);
+    GS_LAUNCH();
+    int cyc = 0;
+    GS_TRY(flow_solve(p, rcv_i, wgt_i, p->rslot_i, p->nfa, fal, &cyc));
+    int total_cycles = cyc;
+    launch(p, k_copy, G, B, (int64_t)n, h, p->wf);
+    // pitVol and "any pit with volume"
+    launch(p, k_pitvol_init, grid_for(np1, B), B, np1, (const double*)p->pit_params, p->pit_vol);
+    GS_CUDA(cudaMemsetAsync(p->i_scalar + 8, 0, sizeof(int), p->stream));
+    launch(p, k_any_pos, grid_for(np1, B), B, np1, (const double*)p->pit_params, p->i_scalar + 8);
+    GS_LAUNCH();
+    int anyvol = 0;
+    GS_TRY(read_flag(p, &anyvol));
+    int passes = 0, solves = 0;
+    if (anyvol) {
+        // FA (m^3 per step) feeding the first pass
+        double* FA = p->q;
+        launch(p, k_scale, G, B, (int64_t)n, (const double*)fal, dt, FA);
+        bool excess = true;
+        int step = 0, stall = 0;
+        bool have_best = false;
+        double best_resid = 0.0;
+        while (excess && step <= 100) {
+            // ---- _distributeDownstream(pitVol, FA, hl, step) ----
+            excess = false;
+            GS_TRY(group_sum_by_pit(p, pit_ids, lsink, FA, p->pit_in, P));
+            GS_CUDA(cudaMemsetAsync(p->i_scalar + 8, 0, sizeof(int), p->stream));
+            launch(p, k_fill_i32, grid_for(n, B), B, n, p->pit_win, -1);
+            launch(p, k_cascade_pits, grid_for(np1, B), B, np1, (const double*)p->pit_in, p->pit_vol,
+                   (const double*)p->filled_vol, (const double*)p->filled_lvl, (const int*)p->pit_info,
+                   p->pit_ev, p->pit_state, p->pit_lvl, p->pit_win, p->i_scalar + 8);
+            GS_LAUNCH();
+            int flags = 0;
+            GS_TRY(read_flag(p, &flags));
+            if (flags & F_POS) {
+                GS_CUDA(cudaMemsetAsync(p->nfa, 0, sizeof(double) * n, p->stream));
+                launch(p, k_cascade_spill, grid_for(np1, B), B, np1, (const double*)p->pit_ev,
+                       (const uint8_t*)p->pit_state, (const int*)p->pit_info, (const int*)p->pit_win,
+                       p->nfa);
+            }
+            if (flags & (F_POS | F_NEG))
+                launch(p, k_cascade_cells, G, B, n, (const int*)pit_ids, (const uint8_t*)p->pit_state,
+                       (const double*)p->pit_lvl, (const double*)lfill, p->wf);
+            GS_LAUNCH();
+            double resid = 0.0;
+            if (flags & F_BIG) {
+                const double* surf = (step == 100) ? lfill : p->wf;
+                GS_TRY(flow_direction(p, surf, true, lfill, pit_ids, flat_dirs, sealevel, p->rcv,
+                                      p->dist, p->wgt, p->rslot, lsink, sea));
+                launch(p, k_div, G, B, (int64_t)n, (const double*)p->nfa, dt, p->q2);
+                GS_LAUNCH();
+                GS_TRY(sum_to_host(p, p->q2, n, &resid));
+                if (resid > p->maxarea) {
+                    excess = true;
+                    // solve into FA's buffer: FA is consumed already
+                    GS_TRY(flow_solve(p, p->rcv, p->wgt, p->rslot, p->q2, p->q, &cyc));
+                    total_cycles += cyc;
+                    launch(p, k_cascade_accum, G, B, n, (const double*)p->q, dt, h, (const double*)p->wf,
+                           p->q, fal);
+                    GS_LAUNCH();
+                    solves++;
+                }
+            }
+            step++;
+            passes++;
+            if (excess) {
+                if (!have_best || resid < best_resid * (1.0 - 1.0e-3)) {
+                    best_resid = resid;
+                    have_best = true;
+                    stall = 0;
+                } else {
+                    stall++;
+                    if (stall >= 3) break;
+                }
+            }
+        }
+        launch(p, k_lake_zero, G, B, n, h, (const double*)p->wf, (const int*)pit_ids, fal);
+        GS_CUDA(cudaMemsetAsync(p->u_scalar, 0, sizeof(unsigned long long), p->stream));
+        launch(p, k_max_key, p->sm_count * 4, 256, (int64_t)n, (const double*)fal, p->u_scalar);
+        GS_LAUNCH();
+    }
+    launch(p, k_flow_final, G, B, n, anyvol ? 1 : 0, h, (const double*)p->wf, (const int*)pit_ids,
+           (const unsigned long long*)p->u_scalar, fal, fill_fal, water);
+    GS_LAUNCH();
+    if (st) {
+        st->cascade_passes = passes;
+        st->cascade_solves = solves;
+        st->cycle_nodes = total_cycles;
+    }
+    return GS_OK;
+}
+
+}  // namespace gs

@@ -1,0 +1,709 @@
+// Depression filling: PITFill.fillElevation(sed=False) (pitfilling.py:849-903).
+//
+// Filled surface.  On one GPU the reference's three Barnes phases (per-tile
+// Priority-Flood fill_tile, label-graph flood fill_edges, fill_depressions)
+// reduce to the plain Priority-Flood fill: the minimax over paths to the seed
+// set of the highest shifted elevation along the path.  (Each watershed label
+// is created by a seed that drains to label 0, so the label-graph level of a
+// watershed never exceeds the fill of its cells and fill_depressions keeps the
+// flood values.)  The GPU computes that minimax without a heap:
+//   1. steepest non-ascending descent (lexicographic (z, id)) links every cell
+//      to a root: a seed or a local minimum (a basin);
+//   2. for each pair of adjacent basins the spill height is max(z_u, z_v);
+//   3. basin levels L(b) = minimax over basin-graph paths to a seed basin,
+//      relaxed with atomicMin until stable;
+//   4. fill = max(z, L(basin)).
+// Only comparisons are involved, so the result is bit-identical to the
+// reference's heap-ordered flood.  Seeds and exclusions follow edge_tile
+// (functions.F90:2036-2080) on z - level; cells at or below the level keep
+// their elevation (fill_depressions, 2290-2329) and open-sea cells are reset
+// (pitfilling.py:689-693).
+//
+// Pit bookkeeping follows _pitInformation (pitfilling.py:704-847):
+// label_pits (equal-fill components holding a cell with no lower neighbour,
+// numbered by their smallest seed id) by union-find; pits_cons renumbering;
+// spill selection by smallest id; fill_dir / nghb_dir hop distances by
+// level-synchronous BFS; the (distance, id) flat receiver pick; pit volumes,
+// depths and depth-volume curves (_getPitParams, getpitvol) by deterministic
+// segmented reductions over pit-sorted cells.
+#include <cub/cub.cuh>
+
+#include <cfloat>
+#include <climits>
+#include <cstring>
+#include <vector>
+
+#include "gs_plan.cuh"
+
+namespace gs {
+
+enum { D_MINH = 0, D_LEVEL = 1 };
+enum { I_CHANGED = 0, I_NEXT = 1, I_NPITS0 = 2, I_NPITS = 3 };
+
+// --------------------------------------------------------------------------
+// reductions
+// --------------------------------------------------------------------------
+__global__ void k_min_key(int n, const double* __restrict__ x, unsigned long long* out) {
+    unsigned long long best = ~0ULL;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        unsigned long long k = dkey(x[i]);
+        best = k < best ? k : best;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        unsigned long long v = __shfl_xor_sync(0xffffffffu, best, o);
+        best = v < best ? v : best;
+    }
+    if ((threadIdx.x & 31) == 0) atomicMin(out, best);
+}
+
+__global__ void k_level(const unsigned long long* minkey, int sphere, double sealevel, double ofill,
+                        double* dsc) {
+    double minh = dkey_inv(*minkey);
+    if (sphere) minh += 1.0e-3;
+    double b = sealevel + ofill;
+    dsc[D_MINH] = minh;
+    dsc[D_LEVEL] = (b > minh) ? b : minh;   // Python max(minh, b)
+}
+
+// --------------------------------------------------------------------------
+// filled surface
+// --------------------------------------------------------------------------
+__global__ void k_classify(int n, const double* __restrict__ h, const double* __restrict__ dsc,
+                           const int* __restrict__ nbr, const int8_t* __restrict__ nnb,
+                           const uint8_t* __restrict__ outlet, int8_t* ledge) {
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= n) return;
+    const double level = dsc[D_LEVEL];
+    const double hs = h[c] - level;
+    int8_t e = -1;
+    if (hs < 0.0) {
+        bool ge = false;
+        for (int s = 0; s < nnb[c]; s++) {
+            int j = nbr[(size_t)s * n + c];
+            if (j >= 0 && h[j] - level >= 0.0) { ge = true; break; }
+        }
+        e = ge ? (outlet[c] ? 2 : 0) : -2;
+    } else if (outlet[c]) {
+        e = 2;
+    }
+    ledge[c] = e;
+}
+
+__global__ void k_descend(int n, const double* __restrict__ h, const double* __restrict__ dsc,
+                          const int* __restrict__ nbr, const int8_t* __restrict__ nnb,
+                          const int8_t* __restrict__ ledge, int* parent) {
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= n) return;
+    int8_t e = ledge[c];
+    if (e != -1) { parent[c] = c; return; }      // seeds, excluded cells: roots
+    const double level = dsc[D_LEVEL];
+    double bz = h[c] - level;
+    int best = c;
+    for (int s = 0; s < nnb[c]; s++) {
+        int j = nbr[(size_t)s * n + c];
+        if (j < 0 || ledge[j] == -2) continue;
+        double z = h[j] - level;
+        if (z < bz || (z == bz && j < best)) { bz = z; best = j; }
+    }
+    parent[c] = best;
+}
+
+__global__ void k_jump(int n, int* parent, int* changed) {
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= n) return;
+    int p = parent[c];
+    int pp = parent[p];
+    if (pp != p) { parent[c] = pp; *changed = 1; }
+}
+
+__global__ void k_basin_init(int n, const int* __restrict__ parent, const int8_t* __restrict__ ledge,
+                             unsigned long long* L) {
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= n) return;
+    if (parent[c] == c) L[c] = (ledge[c] >= 0) ? dkey(-INFINITY) : ~0ULL;
+}
+
+__global__ void k_cross_edges(int n, const double* __restrict__ h, const double* __restrict__ dsc,
+                              const int* __restrict__ nbr, const int8_t* __restrict__ nnb,
+                              const int8_t* __restrict__ ledge, const int* __restrict__ root,
+                              int* xu, int* xv, double* xw, int* count, int64_t cap) {
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= n) return;
+    if (ledge[c] == -2) return;
+    const double level = dsc[D_LEVEL];
+    const int rc = root[c];
+    const double zc = h[c] - level;
+    for (int s = 0; s < nnb[c]; s++) {
+        int j = nbr[(size_t)s * n + c];
+        if (j < 0 || ledge[j] == -2) continue;
+        int rj = root[j];
+        if (rj == rc) continue;
+        double zj = h[j] - level;
+        int pos = atomicAdd(count, 1);
+        if (pos < cap) {
+            xu[pos] = rc;
+            xv[pos] = rj;
+            xw[pos] = zc > zj ? zc : zj;
+        }
+    }
+}
+
+__global__ void k_relax(int m, const int* __restrict__ xu, const int* __restrict__ xv,
+                        const double* __restrict__ xw, unsigned long long* L, int* changed) {
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < m; e += gridDim.x * blockDim.x) {
+        unsigned long long lv = ((volatile unsigned long long*)L)[xv[e]];
+        if (lv == ~0ULL) continue;
+        unsigned long long w = dkey(xw[e]);
+        unsigned long long cand = w > lv ? w : lv;
+        int bu = xu[e];
+        if (cand < ((volatile unsigned long long*)L)[bu]) {
+            unsigned long long old = atomicMin(&L[bu], cand);
+            if (cand < old) *changed = 1;
+        }
+    }
+}
+
+__global__ void k_fill_final(int n, const double* __restrict__ h, const double* __restrict__ dsc,
+                             double sealevel, const int8_t* __restrict__ ledge,
+                             const int* __restrict__ root, const unsigned long long* __restrict__ L,
+                             double* lfill) {
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= n) return;
+    const double level = dsc[D_LEVEL];
+    const double hs = h[c] - level;
+    double f = hs;
+    if (ledge[c] != -2) {
+        unsigned long long k = L[root[c]];
+        if (k != ~0ULL) {
+            double lv = dkey_inv(k);
+            f = lv > hs ? lv : hs;
+        }
+    }
+    double out = (hs > 0.0) ? f : hs;          // fill_depressions: dem > lvl only
+    if (out < sealevel - level) out = hs;      // open sea stays unfilled
+    lfill[c] = out + level;
+}
+
+// --------------------------------------------------------------------------
+// label_pits by union-find
+// --------------------------------------------------------------------------
+__device__ int uf_root(int* comp, int x) {
+    for (int it = 0; it < 1 << 20; it++) {
+        int p = ((volatile int*)comp)[x];
+        if (p == x) return x;
+        int gp = ((volatile int*)comp)[p];
+        if (gp != p) atomicCAS(&comp[x], p, gp);
+        x = p;
+    }
+    return x;
+}
+
+__global__ void k_fill_int(int n, int* a, int v) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) a[i] = v;
+}
+
+__global__ void k_iota(int n, int* a) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) a[i] = i;
+}
+
+__global__ void k_uf_link(int n, const double* __restrict__ f, double sl, const int* __restrict__ nbr,
+                          const int8_t* __restrict__ nnb, int* comp) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double fi = f[i];
+    if (!(fi > sl)) return;
+    for (int s = 0; s < nnb[i]; s++) {
+        int j = nbr[(size_t)s * n + i];
+        if (j < 0 || j > i || f[j] != fi) continue;
+        for (int it = 0; it < 1 << 20; it++) {
+            int a = uf_root(comp, i), b = uf_root(comp, j);
+            if (a == b) break;
+            if (a < b) { int t = a; a = b; b = t; }
+            if (atomicCAS(&comp[a], a, b) == a) break;
+        }
+    }
+}
+
+__global__ void k_uf_flatten(int n, int* comp) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) comp[i] = uf_root(comp, i);
+}
+
+__global__ void k_minseed(int n, const double* __restrict__ f, double sl, const int* __restrict__ nbr,
+                          const int8_t* __restrict__ nnb, const int* __restrict__ comp, int* minseed) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double fi = f[i];
+    if (!(fi > sl)) return;
+    for (int s = 0; s < nnb[i]; s++) {
+        int j = nbr[(size_t)s * n + i];
+        if (j >= 0 && fi > f[j]) return;
+    }
+    atomicMin(&minseed[comp[i]], i);
+}
+
+__global__ void k_seed_flag(int n, const double* __restrict__ f, double sl, const int* __restrict__ comp,
+                            const int* __restrict__ minseed, int* flag) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    flag[i] = (f[i] > sl && minseed[comp[i]] == i) ? 1 : 0;
+}
+
+// label (1..P0) per cell, then outlets removed; present[label] marks survivors
+__global__ void k_label(int n, const double* __restrict__ f, double sl, const int* __restrict__ comp,
+                        const int* __restrict__ minseed, const int* __restrict__ rank,
+                        const uint8_t* __restrict__ outlet, int* lab, int* present) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int l = -1;
+    if (f[i] > sl) {
+        int ms = minseed[comp[i]];
+        if (ms != INT_MAX) l = rank[ms] + 1;
+    }
+    if (outlet[i]) l = -1;
+    lab[i] = l;
+    if (l > 0) present[l] = 1;
+}
+
+__global__ void k_relabel(int n, const int* __restrict__ lab, const int* __restrict__ newid, int* pit) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int l = lab[i];
+    pit[i] = (l > 0) ? newid[l] + 1 : -1;
+}
+
+// --------------------------------------------------------------------------
+// spill points, flat distances, flat receivers
+// --------------------------------------------------------------------------
+__device__ __forceinline__ void rim_tests(int i, int n, const double* f, const int* pit,
+                                          const int* nbr, const int8_t* nnb, const uint8_t* outlet,
+                                          bool* lower, bool* eq) {
+    bool lo = false, e = false;
+    const double fi = f[i];
+    for (int s = 0; s < nnb[i]; s++) {
+        int j = nbr[(size_t)s * n + i];
+        if (j < 0) continue;
+        double fj = f[j];
+        if (fj < fi) lo = true;
+        else if (fj == fi && (outlet[j] || pit[j] == -1)) e = true;
+    }
+    *lower = lo;
+    *eq = e;
+}
+
+__global__ void k_spill_qual(int n, const double* __restrict__ f, const int* __restrict__ pit,
+                             const int* __restrict__ nbr, const int8_t* __restrict__ nnb,
+                             const uint8_t* __restrict__ outlet, int* bestlid) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int p = pit[i];
+    if (p < 0) return;
+    bool lo, eq;
+    rim_tests(i, n, f, pit, nbr, nnb, outlet, &lo, &eq);
+    if (lo || eq) atomicMin(&bestlid[p], i);
+}
+
+__global__ void k_spill_pick(int np1, int n, const double* __restrict__ f, const int* __restrict__ pit,
+                             const int* __restrict__ nbr, const int8_t* __restrict__ nnb,
+                             const uint8_t* __restrict__ outlet, const int* __restrict__ bestlid,
+                             int* pit_info, int* spill_flag) {
+    int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= np1) return;
+    int spill = -1, rank = -1;
+    int i = (p > 0) ? bestlid[p] : INT_MAX;
+    if (i != INT_MAX) {
+        bool lo, eq;
+        rim_tests(i, n, f, pit, nbr, nnb, outlet, &lo, &eq);
+        if (lo) {
+            spill = i;
+        } else {
+            const double fi = f[i];
+            int best = INT_MAX;
+            for (int s = 0; s < nnb[i]; s++) {
+                int j = nbr[(size_t)s * n + i];
+                if (j < 0) continue;
+                if (f[j] == fi && (outlet[j] || pit[j] == -1) && j < best) best = j;
+            }
+            spill = best;
+        }
+        rank = 0;
+        spill_flag[spill] = 1;
+    }
+    pit_info[2 * p] = spill;
+    pit_info[2 * p + 1] = rank;
+}
+
+__global__ void k_bfs_init(int n, const int* __restrict__ spill_flag, int* pdir, int* front, int* cnt) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    if (spill_flag[i]) {
+        pdir[i] = 1;
+        front[atomicAdd(cnt, 1)] = i;
+    } else {
+        pdir[i] = -1;
+    }
+}
+
+__global__ void k_bfs_step(int m, const int* __restrict__ front, int d, int n,
+                           const double* __restrict__ f, const int* __restrict__ pit,
+                           const int* __restrict__ nbr, const int8_t* __restrict__ nnb, int* pdir,
+                           int* next, int* cnt) {
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= m) return;
+    int i = front[t];
+    const double fi = f[i];
+    for (int s = 0; s < nnb[i]; s++) {
+        int c = nbr[(size_t)s * n + i];
+        if (c < 0 || pit[c] < 0 || !(f[c] >= fi)) continue;
+        if (atomicCAS(&pdir[c], -1, d + 1) == -1) next[atomicAdd(cnt, 1)] = c;
+    }
+}
+
+__global__ void k_flat_dirs(int n, const double* __restrict__ f, const int* __restrict__ pit,
+                            const int* __restrict__ pdir, const int* __restrict__ nbr,
+                            const int8_t* __restrict__ nnb, const int* __restrict__ spill_flag,
+                            double sl, const double* __restrict__ h, int* flat, double* lfill) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int out = -1;
+    if (pit[i] > -1) {
+        const int pi = pdir[i];
+        const double fi = f[i];
+        int bd = INT_MAX, bj = INT_MAX;
+        for (int s = 0; s < nnb[i]; s++) {
+            int c = nbr[(size_t)s * n + i];
+            if (c < 0) continue;
+            int pc = pdir[c];
+            if (pc > -1 && pc < pi && f[c] <= fi) {
+                if (pc < bd || (pc == bd && c < bj)) { bd = pc; bj = c; }
+            }
+        }
+        out = (bj != INT_MAX) ? bj : i;
+    }
+    if (spill_flag[i]) out = -1;
+    if (f[i] <= sl) {          // open sea: unfilled, no flat routing (pitfilling.py:822-825)
+        out = -1;
+        lfill[i] = h[i];
+    }
+    flat[i] = out;
+}
+
+// --------------------------------------------------------------------------
+// pit tables
+// --------------------------------------------------------------------------
+__global__ void k_pit_flag(int n, const int* __restrict__ pit, int* flag, int* counts) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int p = pit[i];
+    flag[i] = p >= 0 ? 1 : 0;
+    if (p >= 0) atomicAdd(&counts[p], 1);
+}
+
+__global__ void k_pit_compact(int n, const int* __restrict__ pit, const int* __restrict__ pos,
+                              int* keys, int* vals) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int p = pit[i];
+    if (p < 0) return;
+    keys[pos[i]] = p;
+    vals[pos[i]] = i;
+}
+
+// one warp per pit: vol, max fill, max depth over its cells (sorted by id)
+__global__ void k_pit_params(int np1, const int* __restrict__ start, const int* __restrict__ counts,
+                             const int* __restrict__ cells, const double* __restrict__ f,
+                             const double* __restrict__ h, double sl,
+                             const double* __restrict__ larea, double* params) {
+    int p = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    int lane = threadIdx.x & 31;
+    if (p >= np1) return;
+    int s0 = start[p], c = counts[p];
+    double vol = 0.0, hmax = -INFINITY, dmax = -INFINITY;
+    for (int t = lane; t < c; t += 32) {
+        int i = cells[s0 + t];
+        double hc = h[i] < sl ? sl : h[i];
+        double d = f[i] - hc;
+        vol += d * larea[i];
+        hmax = fmax(hmax, f[i]);
+        dmax = fmax(dmax, d);
+    }
+    vol = warp_sum(vol);
+    for (int o = 16; o > 0; o >>= 1) {
+        hmax = fmax(hmax, __shfl_xor_sync(0xffffffffu, hmax, o));
+        dmax = fmax(dmax, __shfl_xor_sync(0xffffffffu, dmax, o));
+    }
+    if (lane == 0) {
+        if (c > 0) {
+            params[3 * p] = vol;
+            params[3 * p + 1] = hmax;
+            params[3 * p + 2] = dmax;
+        } else {
+            params[3 * p] = 0.0;
+            params[3 * p + 1] = -1.0e8;   // MISSING_DATA_SENTINEL (constants.py:34)
+            params[3 * p + 2] = 0.0;
+        }
+    }
+}
+
+__global__ void k_filled_lvl(int np1, const double* __restrict__ params, double* lvl) {
+    int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= np1) return;
+    double d[6] = {0, 0, 0, 0, 0, 0};
+    if (params[3 * p] > 0.0) {
+        d[0] = params[3 * p + 1] - params[3 * p + 2];
+        double st = params[3 * p + 2] / 5.0;
+        for (int k = 1; k < 6; k++) d[k] = st;
+    }
+    double s = d[0];
+    for (int k = 1; k < 6; k++) {
+        s = s + d[k];
+        lvl[5 * p + k - 1] = s;
+    }
+}
+
+__global__ void k_filled_vol(int np1, const int* __restrict__ start, const int* __restrict__ counts,
+                             const int* __restrict__ cells, const double* __restrict__ h, double sl,
+                             const double* __restrict__ farea, const double* __restrict__ lvl,
+                             const double* __restrict__ params, double* vol) {
+    int p = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    int lane = threadIdx.x & 31;
+    if (p >= np1) return;
+    int s0 = start[p], c = counts[p];
+    double l0 = lvl[5 * p], l1 = lvl[5 * p + 1], l2 = lvl[5 * p + 2], l3 = lvl[5 * p + 3];
+    double v0 = 0, v1 = 0, v2 = 0, v3 = 0;
+    for (int t = lane; t < c; t += 32) {
+        int i = cells[s0 + t];
+        double e = h[i] < sl ? sl : h[i];
+        double a = farea[i];
+        if (l0 > e) v0 += (l0 - e) * a;
+        if (l1 > e) v1 += (l1 - e) * a;
+        if (l2 > e) v2 += (l2 - e) * a;
+        if (l3 > e) v3 += (l3 - e) * a;
+    }
+    v0 = warp_sum(v0);
+    v1 = warp_sum(v1);
+    v2 = warp_sum(v2);
+    v3 = warp_sum(v3);
+    if (lane == 0) {
+        vol[5 * p] = v0;
+        vol[5 * p + 1] = v1;
+        vol[5 * p + 2] = v2;
+        vol[5 * p + 3] = v3;
+        vol[5 * p + 4] = params[3 * p];
+    }
+}
+
+// per-pit masked sum (one warp per pit), deterministic
+__global__ void k_pit_masked_sum(int np1, const int* __restrict__ start, const int* __restrict__ counts,
+                                 const int* __restrict__ cells, const uint8_t* __restrict__ mask,
+                                 const double* __restrict__ vals, double* out) {
+    int p = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    int lane = threadIdx.x & 31;
+    if (p >= np1) return;
+    int s0 = start[p], c = counts[p];
+    double acc = 0.0;
+    for (int t = lane; t < c; t += 32) {
+        int i = cells[s0 + t];
+        if (mask[i]) acc += vals[i];
+    }
+    acc = warp_sum(acc);
+    if (lane == 0) out[p] = acc;
+}
+
+// --------------------------------------------------------------------------
+// host driver
+// --------------------------------------------------------------------------
+static int read_ints(gs_plan* p, int* dst, const int* src, int count) {
+    GS_CUDA(cudaMemcpyAsync(dst, src, sizeof(int) * count, cudaMemcpyDeviceToHost, p->stream));
+    GS_CUDA(cudaStreamSynchronize(p->stream));
+    return GS_OK;
+}
+
+static int exclusive_scan(gs_plan* p, const int* in, int* out, int count) {
+    size_t bytes = p->cub_bytes;
+    GS_CUDA(cub::DeviceScan::ExclusiveSum(p->cub_tmp, bytes, in, out, count, p->stream));
+    p->launches++;
+    return GS_OK;
+}
+
+int group_sum_by_pit(gs_plan* p, const int* /*pit_ids*/, const uint8_t* mask, const double* vals,
+                     double* out, int npits) {
+    const int np1 = npits + 1;
+    launch(p, k_pit_masked_sum, grid_for((int64_t)np1 * 32, 256), 256, np1,
+           (const int*)p->seg_start, (const int*)p->seg_count, (const int*)p->seg_vals2, mask, vals,
+           out);
+    GS_LAUNCH();
+    return GS_OK;
+}
+
+int fill_elevation(gs_plan* p, const double* h, double sealevel, double ofill, double* lfill,
+                   int* pit_ids, int* flat_dirs, gs_stats* st) {
+    const int n = (int)p->n;
+    if (n == 0) { p->npits = 0; return GS_OK; }
+    const int B = 256, G = grid_for(n, B);
+    int hbuf[4];
+
+    // level
+    GS_CUDA(cudaMemsetAsync(p->u_scalar, 0xff, sizeof(unsigned long long), p->stream));
+    launch(p, k_min_key, p->sm_count * 4, 256, n, h, p->u_scalar);
+    launch(p, k_level, 1, 1, (const unsigned long long*)p->u_scalar, p->flat ? 0 : 1, sealevel, ofill,
+           p->d_scalar);
+    GS_LAUNCH();
+
+    // seeds, descent links, roots
+    launch(p, k_classify, G, B, n, h, (const double*)p->d_scalar, (const int*)p->nbr,
+           (const int8_t*)p->nnb, (const uint8_t*)p->outlet, p->ledge);
+    launch(p, k_descend, G, B, n, h, (const double*)p->d_scalar, (const int*)p->nbr,
+           (const int8_t*)p->nnb, (const int8_t*)p->ledge, p->parent);
+    GS_LAUNCH();
+    for (int round = 0; round < 64; round++) {
+        GS_CUDA(cudaMemsetAsync(p->i_scalar + I_CHANGED, 0, sizeof(int), p->stream));
+        for (int r = 0; r < 4; r++) launch(p, k_jump, G, B, n, p->parent, p->i_scalar + I_CHANGED);
+        GS_LAUNCH();
+        GS_TRY(read_ints(p, hbuf, p->i_scalar + I_CHANGED, 1));
+        if (!hbuf[0]) break;
+        if (round == 63) { set_error(GS_EMAXITER, "pit fill: root search did not converge"); return GS_EMAXITER; }
+    }
+    // basin graph and minimax levels
+    launch(p, k_basin_init, G, B, n, (const int*)p->parent, (const int8_t*)p->ledge, p->basinL);
+    GS_CUDA(cudaMemsetAsync(p->i_scalar + I_NEXT, 0, sizeof(int), p->stream));
+    launch(p, k_cross_edges, G, B, n, h, (const double*)p->d_scalar, (const int*)p->nbr,
+           (const int8_t*)p->nnb, (const int8_t*)p->ledge, (const int*)p->parent, p->xe_u, p->xe_v,
+           p->xe_w, p->i_scalar + I_NEXT, p->xe_cap);
+    GS_LAUNCH();
+    GS_TRY(read_ints(p, hbuf, p->i_scalar + I_NEXT, 1));
+    const int64_t m = hbuf[0];
+    if (m > p->xe_cap) { set_error(GS_ENOMEM, "pit fill: cross-edge capacity exceeded"); return GS_ENOMEM; }
+    int rounds = 0;
+    for (;; rounds++) {
+        GS_CUDA(cudaMemsetAsync(p->i_scalar + I_CHANGED, 0, sizeof(int), p->stream));
+        if (m > 0)
+            launch(p, k_relax, p->sm_count * 8, 256, (int)m, (const int*)p->xe_u,
+                   (const int*)p->xe_v, (const double*)p->xe_w, p->basinL, p->i_scalar + I_CHANGED);
+        GS_LAUNCH();
+        GS_TRY(read_ints(p, hbuf, p->i_scalar + I_CHANGED, 1));
+        if (!hbuf[0]) break;
+        if (rounds > 100000) { set_error(GS_EMAXITER, "pit fill: basin relaxation did not converge"); return GS_EMAXITER; }
+    }
+    if (st) st->fill_rounds = rounds + 1;
+    launch(p, k_fill_final, G, B, n, h, (const double*)p->d_scalar, sealevel, (const int8_t*)p->ledge,
+           (const int*)p->parent, (const unsigned long long*)p->basinL, lfill);
+    GS_LAUNCH();
+
+    // label_pits: equal-fill components of cells above sea level
+    launch(p, k_iota, G, B, n, p->comp);
+    launch(p, k_uf_link, G, B, n, (const double*)lfill, sealevel, (const int*)p->nbr,
+           (const int8_t*)p->nnb, p->comp);
+    launch(p, k_uf_flatten, G, B, n, p->comp);
+    launch(p, k_fill_int, G, B, n, p->minseed, (int)INT_MAX);
+    GS_LAUNCH();
+    launch(p, k_minseed, G, B, n, (const double*)lfill, sealevel, (const int*)p->nbr,
+           (const int8_t*)p->nnb, (const int*)p->comp, p->minseed);
+    launch(p, k_seed_flag, G, B, n, (const double*)lfill, sealevel, (const int*)p->comp,
+           (const int*)p->minseed, p->flagbuf);
+    GS_LAUNCH();
+    GS_TRY(exclusive_scan(p, p->flagbuf, p->scanbuf, n));
+    GS_CUDA(cudaMemsetAsync(p->seg_keys, 0, sizeof(int) * (n + 1), p->stream));  // present[]
+    launch(p, k_label, G, B, n, (const double*)lfill, sealevel, (const int*)p->comp,
+           (const int*)p->minseed, (const int*)p->scanbuf, (const uint8_t*)p->outlet, p->lab,
+           p->seg_keys);
+    GS_LAUNCH();
+    // consecutive ids over surviving labels (pits_cons)
+    GS_TRY(exclusive_scan(p, p->seg_keys, p->seg_vals, n + 1));
+    launch(p, k_relabel, G, B, n, (const int*)p->lab, (const int*)p->seg_vals, pit_ids);
+    GS_LAUNCH();
+    {
+        int last[2];
+        GS_CUDA(cudaMemcpyAsync(&last[0], p->seg_vals + n, sizeof(int), cudaMemcpyDeviceToHost, p->stream));
+        GS_CUDA(cudaMemcpyAsync(&last[1], p->seg_keys + n, sizeof(int), cudaMemcpyDeviceToHost, p->stream));
+        GS_CUDA(cudaStreamSynchronize(p->stream));
+        p->npits = last[0] + last[1];
+    }
+    const int P = p->npits, np1 = P + 1;
+    if (st) st->npits = P;
+
+    // spill points
+    launch(p, k_fill_int, grid_for(np1, B), B, np1, p->bestlid, (int)INT_MAX);
+    GS_CUDA(cudaMemsetAsync(p->spill_flag, 0, sizeof(int) * n, p->stream));
+    launch(p, k_spill_qual, G, B, n, (const double*)lfill, (const int*)pit_ids, (const int*)p->nbr,
+           (const int8_t*)p->nnb, (const uint8_t*)p->outlet, p->bestlid);
+    launch(p, k_spill_pick, grid_for(np1, B), B, np1, n, (const double*)lfill, (const int*)pit_ids,
+           (const int*)p->nbr, (const int8_t*)p->nnb, (const uint8_t*)p->outlet,
+           (const int*)p->bestlid, p->pit_info, p->spill_flag);
+    GS_LAUNCH();
+
+    // flat distances (fill_dir + nghb_dir fixed point = BFS hop distance)
+    GS_CUDA(cudaMemsetAsync(p->i_scalar + I_NEXT, 0, sizeof(int), p->stream));
+    launch(p, k_bfs_init, G, B, n, (const int*)p->spill_flag, p->pdir, p->front0, p->i_scalar + I_NEXT);
+    GS_LAUNCH();
+    GS_TRY(read_ints(p, hbuf, p->i_scalar + I_NEXT, 1));
+    int fsize = hbuf[0], d = 1, levels = 0;
+    int* fa = p->front0;
+    int* fb = p->front1;
+    while (fsize > 0) {
+        GS_CUDA(cudaMemsetAsync(p->i_scalar + I_NEXT, 0, sizeof(int), p->stream));
+        launch(p, k_bfs_step, grid_for(fsize, B), B, fsize, (const int*)fa, d, n, (const double*)lfill,
+               (const int*)pit_ids, (const int*)p->nbr, (const int8_t*)p->nnb, p->pdir, fb,
+               p->i_scalar + I_NEXT);
+        GS_LAUNCH();
+        GS_TRY(read_ints(p, hbuf, p->i_scalar + I_NEXT, 1));
+        fsize = hbuf[0];
+        int* t = fa; fa = fb; fb = t;
+        d++;
+        levels++;
+        if (levels > n + 1) { set_error(GS_EMAXITER, "pit fill: flat BFS did not terminate"); return GS_EMAXITER; }
+    }
+    if (st) st->flat_rounds = levels;
+    launch(p, k_flat_dirs, G, B, n, (const double*)lfill, (const int*)pit_ids, (const int*)p->pdir,
+           (const int*)p->nbr, (const int8_t*)p->nnb, (const int*)p->spill_flag, sealevel, h,
+           flat_dirs, lfill);
+    GS_LAUNCH();
+
+    // pit cells sorted by (pit, id): segments for the per-pit reductions.
+    // Ordered compaction (scan) keeps id order; the stable radix sort by pit
+    // then lists every pit's cells in increasing id.
+    GS_CUDA(cudaMemsetAsync(p->seg_count, 0, sizeof(int) * (np1 + 1), p->stream));
+    launch(p, k_pit_flag, G, B, n, (const int*)pit_ids, p->flagbuf, p->seg_count);
+    GS_LAUNCH();
+    GS_TRY(exclusive_scan(p, p->flagbuf, p->scanbuf, n));
+    launch(p, k_pit_compact, G, B, n, (const int*)pit_ids, (const int*)p->scanbuf, p->seg_keys,
+           p->seg_vals);
+    GS_LAUNCH();
+    int ncell = 0;
+    {
+        int last[2];
+        GS_CUDA(cudaMemcpyAsync(&last[0], p->scanbuf + n - 1, sizeof(int), cudaMemcpyDeviceToHost, p->stream));
+        GS_CUDA(cudaMemcpyAsync(&last[1], p->flagbuf + n - 1, sizeof(int), cudaMemcpyDeviceToHost, p->stream));
+        GS_CUDA(cudaStreamSynchronize(p->stream));
+        ncell = last[0] + last[1];
+    }
+    if (ncell > 0) {
+        int bits = 1;
+        while ((1 << bits) <= P && bits < 31) bits++;
+        size_t bytes = p->cub_bytes;
+        GS_CUDA(cub::DeviceRadixSort::SortPairs(p->cub_tmp, bytes, p->seg_keys, p->seg_keys2, p->seg_vals,
+                                                p->seg_vals2, ncell, 0, bits, p->stream));
+        p->launches++;
+    }
+    GS_TRY(exclusive_scan(p, p->seg_count, p->seg_start, np1));
+    // pit tables
+    launch(p, k_pit_params, grid_for((int64_t)np1 * 32, 256), 256, np1, (const int*)p->seg_start,
+           (const int*)p->seg_count, (const int*)p->seg_vals2, (const double*)lfill, h, sealevel,
+           (const double*)p->larea, p->pit_params);
+    launch(p, k_filled_lvl, grid_for(np1, B), B, np1, (const double*)p->pit_params, p->filled_lvl);
+    launch(p, k_filled_vol, grid_for((int64_t)np1 * 32, 256), 256, np1, (const int*)p->seg_start,
+           (const int*)p->seg_count, (const int*)p->seg_vals2, h, sealevel, (const double*)p->farea,
+           (const double*)p->filled_lvl, (const double*)p->pit_params, p->filled_vol);
+    GS_LAUNCH();
+    {
+        double lv;
+        GS_CUDA(cudaMemcpyAsync(&lv, p->d_scalar + D_LEVEL, sizeof(double), cudaMemcpyDeviceToHost, p->stream));
+        GS_CUDA(cudaStreamSynchronize(p->stream));
+        p->level = lv;
+    }
+    return GS_OK;
+}
+
+}  // namespace gs

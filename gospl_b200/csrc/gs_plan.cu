@@ -1,0 +1,241 @@
+// Plan creation: upload of the finite-volume mesh in slot-major layout and
+// allocation of every workspace the hot path needs (nothing is allocated
+// per step).
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <vector>
+
+#include "gs_plan.cuh"
+
+namespace gs {
+
+template <class T>
+static int dalloc(T** ptr, size_t count) {
+    if (count == 0) count = 1;
+    cudaError_t e = cudaMalloc((void**)ptr, sizeof(T) * count);
+    if (e != cudaSuccess) {
+        set_error(GS_ENOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+        return GS_ENOMEM;
+    }
+    return GS_OK;
+}
+
+template <class T>
+static int upload(T** ptr, const std::vector<T>& h) {
+    GS_TRY(dalloc(ptr, h.size()));
+    if (!h.empty()) GS_CUDA(cudaMemcpy(*ptr, h.data(), sizeof(T) * h.size(), cudaMemcpyHostToDevice));
+    return GS_OK;
+}
+
+static void plan_free(gs_plan* p) {
+    void* ptrs[] = {p->nbr, p->elen, p->vdist, p->rev, p->sorder, p->nnb, p->farea, p->larea, p->outlet,
+                    p->outlet_ids, p->open_ids, p->open_mask, p->gid, p->rcv, p->dist, p->wgt, p->rslot,
+                    p->rslot_i, p->lsink, p->sea, p->don_mask, p->don_k, p->cnt, p->queue, p->ctr,
+                    p->done_flag, p->q, p->q2, p->q3, p->c, p->ledge, p->parent, p->basinL, p->xe_u,
+                    p->xe_v, p->xe_w, p->comp, p->minseed, p->lab, p->flagbuf, p->scanbuf, p->pdir,
+                    p->front0, p->front1, p->spill_flag, p->bestlid, p->d_scalar, p->i_scalar,
+                    p->u_scalar, p->pit_params, p->pit_info, p->filled_lvl, p->filled_vol, p->pit_vol,
+                    p->pit_in, p->pit_ev, p->pit_win, p->pit_lvl, p->pit_state, p->seg_keys, p->seg_vals,
+                    p->seg_keys2, p->seg_vals2, p->seg_start, p->seg_count, p->cub_tmp, p->nfa, p->wf,
+                    p->hl, p->dcoef, p->dsea, p->cg_r, p->cg_z, p->cg_p, p->cg_ap, p->cg_x, p->cg_b,
+                    p->red};
+    for (void* q : ptrs)
+        if (q) cudaFree(q);
+}
+
+int plan_create(int64_t nb, const int32_t* nnb, const int32_t* ngb, const double* elgt, const double* vdist,
+                const double* farea, const double* larea, const int32_t* outlet_ids, int64_t n_outlet,
+                const int32_t* open_ids, int64_t n_open, int flat, int flow_dir, gs_plan** out) {
+    if (nb < 0 || nb > (int64_t)0x7fffffff - 64 || flow_dir < 1 || flow_dir > MAXR || !out) {
+        set_error(GS_EINVAL, "gs_plan_create: bad size or flow_dir");
+        return GS_EINVAL;
+    }
+    if (nb > 0 && (!nnb || !ngb || !elgt || !vdist || !farea || !larea)) {
+        set_error(GS_EINVAL, "gs_plan_create: null mesh array");
+        return GS_EINVAL;
+    }
+    const int n = (int)nb;
+    int W = 1;
+    for (int i = 0; i < n; i++) {
+        if (nnb[i] < 0 || nnb[i] > MAXW) {
+            set_error(GS_EINVAL, "gs_plan_create: FVnNb outside 0..12");
+            return GS_EINVAL;
+        }
+        W = std::max(W, (int)nnb[i]);
+    }
+    for (int64_t t = 0; t < n_outlet; t++)
+        if (outlet_ids[t] < 0 || outlet_ids[t] >= n) {
+            set_error(GS_EINVAL, "gs_plan_create: outlet id out of range");
+            return GS_EINVAL;
+        }
+    for (int64_t t = 0; t < n_open; t++)
+        if (open_ids[t] < 0 || open_ids[t] >= n) {
+            set_error(GS_EINVAL, "gs_plan_create: open-edge id out of range");
+            return GS_EINVAL;
+        }
+    gs_plan* p = new gs_plan();
+    p->n = n;
+    p->W = W;
+    p->R = flow_dir;
+    p->flat = flat ? 1 : 0;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&p->sm_count, cudaDevAttrMultiProcessorCount, dev);
+
+    std::vector<int> h_nbr((size_t)W * n, -1);
+    std::vector<double> h_elen((size_t)W * n, 0.0), h_vd((size_t)W * n, 0.0);
+    std::vector<int8_t> h_rev((size_t)W * n, -1), h_nnb(n);
+    std::vector<unsigned long long> h_sorder(n, ~0ULL);
+    for (int i = 0; i < n; i++) {
+        h_nnb[i] = (int8_t)nnb[i];
+        for (int s = 0; s < nnb[i]; s++) {
+            h_nbr[(size_t)s * n + i] = ngb[(size_t)i * 12 + s];
+            h_elen[(size_t)s * n + i] = elgt[(size_t)i * 12 + s];
+            h_vd[(size_t)s * n + i] = vdist[(size_t)i * 12 + s];
+        }
+    }
+    for (int i = 0; i < n; i++) {
+        int slots[12], cnt = 0;
+        for (int s = 0; s < nnb[i]; s++) {
+            int j = ngb[(size_t)i * 12 + s];
+            if (j < 0 || j >= n) continue;
+            slots[cnt++] = s;
+            for (int t = 0; t < nnb[j]; t++)
+                if (ngb[(size_t)j * 12 + t] == i) { h_rev[(size_t)s * n + i] = (int8_t)t; break; }
+        }
+        std::sort(slots, slots + cnt, [&](int a, int b) { return ngb[(size_t)i * 12 + a] < ngb[(size_t)i * 12 + b]; });
+        unsigned long long o = ~0ULL;
+        for (int q = cnt - 1; q >= 0; q--) o = (o << 4) | (unsigned long long)slots[q];
+        h_sorder[i] = o;
+    }
+    std::vector<uint8_t> h_out(n, 0), h_open(n, 0);
+    std::vector<int> h_oid(outlet_ids, outlet_ids + n_outlet), h_open_ids(open_ids, open_ids + n_open);
+    for (int t : h_oid) h_out[t] = 1;
+    for (int t : h_open_ids) h_open[t] = 1;
+    std::vector<int> h_gid(n);
+    for (int i = 0; i < n; i++) h_gid[i] = i;
+    double maxarea = 0.0;
+    for (int i = 0; i < n; i++) maxarea = (i == 0 || larea[i] > maxarea) ? larea[i] : maxarea;
+    p->maxarea = maxarea;
+    p->n_outlet = (int)n_outlet;
+    p->n_open = (int)n_open;
+
+    int st = GS_OK;
+#define TRYP(x)                   \
+    do {                          \
+        st = (x);                 \
+        if (st != GS_OK) goto fail; \
+    } while (0)
+    TRYP(upload(&p->nbr, h_nbr));
+    TRYP(upload(&p->elen, h_elen));
+    TRYP(upload(&p->vdist, h_vd));
+    TRYP(upload(&p->rev, h_rev));
+    TRYP(upload(&p->sorder, h_sorder));
+    TRYP(upload(&p->nnb, h_nnb));
+    TRYP(upload(&p->farea, std::vector<double>(farea, farea + n)));
+    TRYP(upload(&p->larea, std::vector<double>(larea, larea + n)));
+    TRYP(upload(&p->outlet, h_out));
+    TRYP(upload(&p->outlet_ids, h_oid));
+    TRYP(upload(&p->open_ids, h_open_ids));
+    TRYP(upload(&p->open_mask, h_open));
+    TRYP(upload(&p->gid, h_gid));
+    {
+        const size_t N = (size_t)n, R = (size_t)p->R, N1 = N + 1;
+        TRYP(dalloc(&p->rcv, R * N));
+        TRYP(dalloc(&p->dist, R * N));
+        TRYP(dalloc(&p->wgt, R * N));
+        TRYP(dalloc(&p->rslot, R * N));
+        TRYP(dalloc(&p->rslot_i, R * N));
+        TRYP(dalloc(&p->c, R * N));
+        TRYP(dalloc(&p->lsink, N));
+        TRYP(dalloc(&p->sea, N));
+        TRYP(dalloc(&p->don_mask, N));
+        TRYP(dalloc(&p->don_k, N));
+        TRYP(dalloc(&p->cnt, N));
+        TRYP(dalloc(&p->queue, N));
+        TRYP(dalloc(&p->ctr, 16));
+        TRYP(dalloc(&p->done_flag, N));
+        TRYP(dalloc(&p->q, N));
+        TRYP(dalloc(&p->q2, N));
+        TRYP(dalloc(&p->q3, N));
+        TRYP(dalloc(&p->ledge, N));
+        TRYP(dalloc(&p->parent, N));
+        TRYP(dalloc(&p->basinL, N));
+        p->xe_cap = (int64_t)W * N;
+        TRYP(dalloc(&p->xe_u, (size_t)p->xe_cap));
+        TRYP(dalloc(&p->xe_v, (size_t)p->xe_cap));
+        TRYP(dalloc(&p->xe_w, (size_t)p->xe_cap));
+        TRYP(dalloc(&p->comp, N));
+        TRYP(dalloc(&p->minseed, N));
+        TRYP(dalloc(&p->lab, N));
+        TRYP(dalloc(&p->flagbuf, N1));
+        TRYP(dalloc(&p->scanbuf, N1));
+        TRYP(dalloc(&p->pdir, N));
+        TRYP(dalloc(&p->front0, N));
+        TRYP(dalloc(&p->front1, N));
+        TRYP(dalloc(&p->spill_flag, N));
+        TRYP(dalloc(&p->bestlid, N1));
+        TRYP(dalloc(&p->d_scalar, 16));
+        TRYP(dalloc(&p->i_scalar, 16));
+        TRYP(dalloc(&p->u_scalar, 16));
+        TRYP(dalloc(&p->pit_params, 3 * N1));
+        TRYP(dalloc(&p->pit_info, 2 * N1));
+        TRYP(dalloc(&p->filled_lvl, 5 * N1));
+        TRYP(dalloc(&p->filled_vol, 5 * N1));
+        TRYP(dalloc(&p->pit_vol, N1));
+        TRYP(dalloc(&p->pit_in, N1));
+        TRYP(dalloc(&p->pit_ev, N1));
+        TRYP(dalloc(&p->pit_win, N));
+        TRYP(dalloc(&p->pit_lvl, N1));
+        TRYP(dalloc(&p->pit_state, N1));
+        TRYP(dalloc(&p->seg_keys, N1));
+        TRYP(dalloc(&p->seg_vals, N1));
+        TRYP(dalloc(&p->seg_keys2, N1));
+        TRYP(dalloc(&p->seg_vals2, N1));
+        TRYP(dalloc(&p->seg_start, N1 + 1));
+        TRYP(dalloc(&p->seg_count, N1 + 1));
+        TRYP(dalloc(&p->nfa, N));
+        TRYP(dalloc(&p->wf, N));
+        TRYP(dalloc(&p->hl, N));
+        TRYP(dalloc(&p->dcoef, (size_t)(W + 1) * N));
+        TRYP(dalloc(&p->dsea, N));
+        TRYP(dalloc(&p->cg_r, N));
+        TRYP(dalloc(&p->cg_z, N));
+        TRYP(dalloc(&p->cg_p, N));
+        TRYP(dalloc(&p->cg_ap, N));
+        TRYP(dalloc(&p->cg_x, N));
+        TRYP(dalloc(&p->cg_b, N));
+        TRYP(dalloc(&p->red, 8192));
+        size_t b1 = 0, b2 = 0;
+        cub::DeviceRadixSort::SortPairs((void*)nullptr, b1, (const int*)nullptr, (int*)nullptr,
+                                        (const int*)nullptr, (int*)nullptr, (int)N1, 0, 32);
+        cub::DeviceScan::ExclusiveSum((void*)nullptr, b2, (const int*)nullptr, (int*)nullptr, (int)N1 + 1);
+        p->cub_bytes = std::max(b1, b2) + 256;
+        TRYP(dalloc((char**)&p->cub_tmp, p->cub_bytes));
+    }
+#undef TRYP
+    {
+        cudaError_t e = cudaDeviceSynchronize();
+        if (e != cudaSuccess) {
+            set_error(GS_ECUDA, std::string("plan upload: ") + cudaGetErrorString(e));
+            st = GS_ECUDA;
+            goto fail;
+        }
+    }
+    *out = p;
+    return GS_OK;
+fail:
+    plan_free(p);
+    delete p;
+    return st;
+}
+
+int plan_destroy(gs_plan* p) {
+    if (!p) return GS_OK;
+    plan_free(p);
+    delete p;
+    return GS_OK;
+}
+
+}  // namespace gs

@@ -1,0 +1,151 @@
+// Plan (mesh + workspaces) shared by all hot-path stages.
+#pragma once
+#include "gs_common.cuh"
+
+struct gs_plan {
+    int64_t n = 0;      // vertices
+    int W = 0;          // neighbour slots stored (max FVnNb)
+    int R = 0;          // receivers per vertex (flowDir)
+    int flat = 0;       // flatModel
+    int n_outlet = 0;
+    int n_open = 0;
+    double maxarea = 0;
+    cudaStream_t stream = 0;
+    int64_t launches = 0;
+    int sm_count = 148;
+
+    // mesh, slot-major [W][n]
+    int* nbr = nullptr;          // FVnID (-1 pad)
+    double* elen = nullptr;      // FVeLgt
+    double* vdist = nullptr;     // FVvDist
+    int8_t* rev = nullptr;       // position of i in the list of nbr(i,s)
+    unsigned long long* sorder = nullptr;  // slots in ascending neighbour id, 4 bits each
+    int8_t* nnb = nullptr;       // FVnNb
+    double* farea = nullptr;     // FVarea (Fortran kernels)
+    double* larea = nullptr;     // larea (Python side)
+    uint8_t* outlet = nullptr;   // outletIDs mask
+    int* outlet_ids = nullptr;
+    int* open_ids = nullptr;
+    uint8_t* open_mask = nullptr;
+    int* gid = nullptr;          // identity ids (input order)
+
+    // receivers workspace ([R][n]) used for the cascade rebuilds
+    int* rcv = nullptr;
+    double* dist = nullptr;
+    double* wgt = nullptr;
+    int8_t* rslot = nullptr;     // neighbour slot of each receiver (-1 = self)
+    int8_t* rslot_i = nullptr;   // same for the snapshot receivers
+    uint8_t* lsink = nullptr;    // live lsink
+    uint8_t* sea = nullptr;      // lFill <= sea
+
+    // DAG sweep state
+    uint32_t* don_mask = nullptr;        // bit s: nbr(i,s) is a donor of i
+    unsigned long long* don_k = nullptr; // 4 bits per slot: receiver index at the donor
+    int* cnt = nullptr;
+    int* queue = nullptr;
+    unsigned* ctr = nullptr;             // [0]=head [1]=tail [2]=done [3]=status
+    uint8_t* done_flag = nullptr;
+    double* q = nullptr;                 // sweep values
+    double* q2 = nullptr;
+    double* q3 = nullptr;
+    double* c = nullptr;                 // SPL coefficients [R][n]
+
+    // pit filling
+    int8_t* ledge = nullptr;
+    int* parent = nullptr;
+    unsigned long long* basinL = nullptr;
+    int* xe_u = nullptr;                 // cross edges (basin_u, basin_v, w)
+    int* xe_v = nullptr;
+    double* xe_w = nullptr;
+    int64_t xe_cap = 0;
+    int* comp = nullptr;
+    int* minseed = nullptr;
+    int* lab = nullptr;
+    int* flagbuf = nullptr;
+    int* scanbuf = nullptr;
+    int* pdir = nullptr;
+    int* front0 = nullptr;
+    int* front1 = nullptr;
+    int* spill_flag = nullptr;
+    int* bestlid = nullptr;
+    int npits = 0;
+    double level = 0;
+    double* d_scalar = nullptr;          // small device scratch [16]
+    int* i_scalar = nullptr;             // small device scratch [16]
+    unsigned long long* u_scalar = nullptr;
+    // per pit tables (capacity n+1 rows)
+    double* pit_params = nullptr;        // [P+1][3]
+    int* pit_info = nullptr;             // [P+1][2]
+    double* filled_lvl = nullptr;        // [P+1][5]
+    double* filled_vol = nullptr;        // [P+1][5]
+    double* pit_vol = nullptr;           // cascade pitVol [P+1]
+    double* pit_in = nullptr;            // inflow [P+1]
+    double* pit_ev = nullptr;            // eV [P+1]
+    int* pit_win = nullptr;              // winning pit per spill node
+    double* pit_lvl = nullptr;           // partial fill level per pit
+    uint8_t* pit_state = nullptr;        // 1 overflow, 2 partial
+    // segmented reductions
+    int* seg_keys = nullptr;
+    int* seg_vals = nullptr;
+    int* seg_keys2 = nullptr;
+    int* seg_vals2 = nullptr;
+    int* seg_start = nullptr;
+    int* seg_count = nullptr;
+    void* cub_tmp = nullptr;
+    size_t cub_bytes = 0;
+
+    // flow / cascade
+    double* nfa = nullptr;
+    double* wf = nullptr;                // waterFilled (absolute)
+    double* hl = nullptr;                // copy of h
+
+    // diffusion
+    double* dcoef = nullptr;             // [W+1][n]: diag then off-diagonals
+    uint8_t* dsea = nullptr;             // sea mask the matrix was built for
+    int dvalid = 0;
+    double dvalid_dt = 0, dvalid_cda = 0, dvalid_cdm = 0;
+    double* cg_r = nullptr;
+    double* cg_z = nullptr;
+    double* cg_p = nullptr;
+    double* cg_ap = nullptr;
+    double* cg_x = nullptr;
+    double* cg_b = nullptr;
+    double* red = nullptr;               // reduction scratch
+};
+
+namespace gs {
+
+// stage entry points (host side, issue work on plan->stream)
+int receivers(gs_plan* p, int nrcv, double exp, const double* elev, double sl, const int* gid,
+              int* rcv, double* dist, double* wgt, int8_t* rslot);
+int flow_direction(gs_plan* p, const double* h, bool down, const double* lfill,
+                   const int* pit_ids, const int* flat_dirs, double sealevel, int* rcv,
+                   double* dist, double* wgt, int8_t* rslot, uint8_t* lsink, uint8_t* sea);
+int flow_solve(gs_plan* p, const int* rcv, const double* wgt, const int8_t* rslot,
+               const double* b, double* x, int* cycle_nodes);
+int spl_sweep(gs_plan* p, const int* rcv, const double* c, const int8_t* rslot, const double* hold,
+              double* s, int* cycle_nodes);
+int fill_elevation(gs_plan* p, const double* h, double sealevel, double ofill, double* lfill,
+                   int* pit_ids, int* flat_dirs, gs_stats* st);
+int group_sum_by_pit(gs_plan* p, const int* pit_ids, const uint8_t* mask, const double* vals,
+                     double* out, int npits);
+int flow_accumulation(gs_plan* p, const double* h, const double* bl, double sealevel, double ofill,
+                      double dt, double* fal, double* fill_fal, double* water, double* lfill,
+                      int* pit_ids, int* flat_dirs, int* rcv_i, double* dist_i, double* wgt_i,
+                      uint8_t* lsink, uint8_t* sea, gs_stats* st);
+int erodep_spl(gs_plan* p, double* h, double* cum_ed, double* eb, const double* fal,
+               const double* rain, double k_scalar, const double* k_field, double d, double m,
+               double dt, const int* rcv_i, const double* dist_i, const double* wgt_i,
+               const uint8_t* lsink, const uint8_t* sea, gs_stats* st);
+int hillslope(gs_plan* p, double* h, double* cum_ed, double* eb, double sealevel, double cda,
+              double cdm, double dt, double rtol, int max_iter, gs_stats* st);
+int apply_forces(gs_plan* p, double* h, const double* rain, const double* upsub, double dt,
+                 double sealevel, double* bl);
+
+template <class K, class... A>
+inline void launch(gs_plan* p, K kernel, int grid, int block, A... args) {
+    kernel<<<grid, block, 0, p->stream>>>(args...);
+    p->launches++;
+}
+
+}  // namespace gs

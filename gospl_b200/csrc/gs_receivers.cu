@@ -1,0 +1,233 @@
+// Multiple-flow-direction receivers and the flow-direction post-processing.
+//
+// k_mfd_receivers restates fortran/functions.F90:1544-1671 (mfdreceivers):
+// one thread per vertex over the slot-major neighbour arrays, adaptive
+// exponent, gid-keyed 1e-15 tie perturbation, top-R selection.  The top-R
+// order for distinct slopes is the descending order the reference's quicksort
+// produces; when two candidate slopes are exactly equal the reference
+// quicksort/split pair (functions.F90:683-762) is replayed literally so tie
+// order matches.  As in the reference, the distance of output receiver o is
+// the edge length of candidate kk-1-o in candidate order (the sort permutes
+// slopes and ids but not distances).
+//
+// k_flow_direction_post restates flowplex.py:480-540: flat routing on filled
+// pits when down=True, self-sink outlets on flat models, the lsink mask.
+#include "gs_plan.cuh"
+
+namespace gs {
+
+// --- literal replay of the reference quicksort on <=12 candidates ----------
+__device__ void dev_split(double* a, int low, int high, int* mid, int* ix) {
+    int left = low, right = high;
+    double pivot = a[low - 1];
+    int ipivot = ix[low - 1];
+    for (;;) {
+        if (left >= right) break;
+        for (;;) {
+            if (left >= right || a[right - 1] < pivot) break;
+            right = right - 1;
+        }
+        for (;;) {
+            if (left > 12) break;
+            if (a[left - 1] > pivot) break;
+            left = left + 1;
+        }
+        if (left < right) {
+            double sw = a[left - 1]; a[left - 1] = a[right - 1]; a[right - 1] = sw;
+            int is = ix[left - 1]; ix[left - 1] = ix[right - 1]; ix[right - 1] = is;
+        }
+    }
+    a[low - 1] = a[right - 1];
+    a[right - 1] = pivot;
+    *mid = right;
+    ix[low - 1] = ix[right - 1];
+    ix[right - 1] = ipivot;
+}
+
+__device__ void dev_quicksort(double* a, int first, int last, int* ix) {
+    // explicit stack replaying the recursion order (left part first)
+    int stf[32], stl[32];
+    int sp = 0;
+    stf[sp] = first; stl[sp] = last; sp++;
+    while (sp > 0) {
+        sp--;
+        int f = stf[sp], l = stl[sp];
+        if (f < l) {
+            int mid;
+            dev_split(a, f, l, &mid, ix);
+            // recursion: quicksort(first, mid-1) then quicksort(mid+1, last)
+            stf[sp] = mid + 1; stl[sp] = l; sp++;
+            stf[sp] = f; stl[sp] = mid - 1; sp++;
+        }
+    }
+}
+
+__global__ void k_mfd_receivers(int n, int W, int R, double expo, const double* __restrict__ elev,
+                                double sl, const int* __restrict__ gid, const int* __restrict__ nbr,
+                                const double* __restrict__ elen, const int8_t* __restrict__ nnb,
+                                int* __restrict__ rcv, double* __restrict__ dist,
+                                double* __restrict__ wgt, int8_t* __restrict__ rslot) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const double hk = elev[k];
+    for (int o = 0; o < R; o++) {
+        rcv[(size_t)o * n + k] = k;
+        dist[(size_t)o * n + k] = 0.0;
+        wgt[(size_t)o * n + k] = 0.0;
+        if (rslot) rslot[(size_t)o * n + k] = -1;
+    }
+    if (hk <= sl) return;
+    const int deg = nnb[k];
+    double e = 0.0;
+    for (int s = 0; s < deg; s++) {
+        int nb = nbr[(size_t)s * n + k];
+        double L = elen[(size_t)s * n + k];
+        if (nb >= 0 && L > 0.0) {
+            double val = (hk - elev[nb]) / L;
+            e = (val > e) ? val : e;
+        }
+    }
+    double fexp;
+    if (e > 0) {
+        double me = (e < 1.0) ? e : 1.0;
+        fexp = 5.0 * me + expo;
+    } else {
+        fexp = 1.0;
+    }
+    const bool fexp_int = (fexp == floor(fexp));
+    double slp[12], dst[12];
+    int cid[12], cs[12];
+    int kk = 0;
+    for (int s = 0; s < deg; s++) {
+        int nb = nbr[(size_t)s * n + k];
+        double L = elen[(size_t)s * n + k];
+        if (nb >= 0 && L > 0.0) {
+            double d = hk - elev[nb];
+            double val;
+            if (d > 0.0) val = pow(d, fexp) / L;
+            else if (d == 0.0) val = 0.0;
+            else val = fexp_int ? pow(d, fexp) / L : -1.0;   // non-integer power of a
+                                                             // negative base is NaN: no receiver
+            if (val > 0.0) {
+                slp[kk] = val * (1.0 - 1.0e-15 * (double)gid[nb]);
+                cid[kk] = nb;
+                cs[kk] = s;
+                dst[kk] = L;
+                kk++;
+            }
+        }
+    }
+    if (kk == 0) return;
+    if (kk <= R) {
+        double val = 0.0;
+        for (int p = 0; p < kk; p++) {
+            rcv[(size_t)p * n + k] = cid[p];
+            dist[(size_t)p * n + k] = dst[p];
+            if (rslot) rslot[(size_t)p * n + k] = (int8_t)cs[p];
+            val = val + slp[p];
+        }
+        for (int p = 0; p < kk; p++) wgt[(size_t)p * n + k] = slp[p] / val;
+        return;
+    }
+    // kk > R: top-R in descending slope order
+    int top[12];
+    bool tie = false;
+    for (int a = 0; a < kk && !tie; a++)
+        for (int b = a + 1; b < kk; b++)
+            if (slp[a] == slp[b]) { tie = true; break; }
+    if (!tie) {
+        unsigned used = 0;
+        for (int o = 0; o < R; o++) {
+            int best = -1;
+            for (int a = 0; a < kk; a++) {
+                if (used & (1u << a)) continue;
+                if (best < 0 || slp[a] > slp[best]) best = a;
+            }
+            used |= 1u << best;
+            top[o] = best;
+        }
+    } else {
+        double sa[12];
+        int ix[12];
+        for (int a = 0; a < 12; a++) { sa[a] = (a < kk) ? slp[a] : 0.0; ix[a] = a; }
+        dev_quicksort(sa, 1, kk, ix);
+        for (int o = 0; o < R; o++) top[o] = ix[kk - 1 - o];
+    }
+    double val = 0.0;
+    double slope[12];
+    for (int o = 0; o < R; o++) {
+        int a = top[o];
+        slope[o] = slp[a];
+        rcv[(size_t)o * n + k] = cid[a];
+        dist[(size_t)o * n + k] = dst[kk - 1 - o];
+        if (rslot) rslot[(size_t)o * n + k] = (int8_t)cs[a];
+        val = val + slp[a];
+    }
+    for (int o = 0; o < R; o++) wgt[(size_t)o * n + k] = slope[o] / val;
+}
+
+__global__ void k_flow_direction_post(int n, int W, int R, int flat, const double* __restrict__ h,
+                                      int down, const double* __restrict__ lfill,
+                                      const int* __restrict__ pit, const int* __restrict__ fdir,
+                                      double sl, const uint8_t* __restrict__ outlet,
+                                      const int* __restrict__ nbr, int* rcv, double* dist,
+                                      double* wgt, int8_t* rslot, uint8_t* lsink, uint8_t* sea) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const bool is_sea = lfill[i] <= sl;
+    if (down) {
+        double sw = 0.0;
+        for (int k = 0; k < R; k++) sw = sw + wgt[(size_t)k * n + i];
+        if (h[i] == lfill[i] && pit[i] > -1 && fdir[i] > -1 && sw == 0.0) {
+            int f = fdir[i];
+            int slot = -1;
+            if (f != i)
+                for (int s = 0; s < W; s++)
+                    if (nbr[(size_t)s * n + i] == f) { slot = s; break; }
+            for (int k = 0; k < R; k++) {
+                rcv[(size_t)k * n + i] = (k == 0) ? f : i;
+                wgt[(size_t)k * n + i] = (k == 0) ? 1.0 : 0.0;
+                rslot[(size_t)k * n + i] = (k == 0) ? (int8_t)slot : (int8_t)-1;
+            }
+        }
+    }
+    if (flat && outlet[i]) {
+        for (int k = 0; k < R; k++) {
+            rcv[(size_t)k * n + i] = i;
+            dist[(size_t)k * n + i] = 0.0;
+            wgt[(size_t)k * n + i] = 0.0;
+            rslot[(size_t)k * n + i] = -1;
+        }
+    }
+    double sw = 0.0;
+    for (int k = 0; k < R; k++) sw = sw + wgt[(size_t)k * n + i];
+    lsink[i] = (sw == 0.0 && !outlet[i] && !is_sea) ? 1 : 0;
+    sea[i] = is_sea ? 1 : 0;
+}
+
+int receivers(gs_plan* p, int nrcv, double exp, const double* elev, double sl, const int* gid,
+              int* rcv, double* dist, double* wgt, int8_t* rslot) {
+    if (nrcv < 1 || nrcv > 12) {
+        set_error(GS_EINVAL, "mfdreceivers: nrcv must be in 1..12");
+        return GS_EINVAL;
+    }
+    if (p->n == 0) return GS_OK;
+    launch(p, k_mfd_receivers, grid_for(p->n, 128), 128, (int)p->n, p->W, nrcv, exp, elev, sl,
+           gid ? gid : p->gid, p->nbr, p->elen, p->nnb, rcv, dist, wgt, rslot);
+    GS_LAUNCH();
+    return GS_OK;
+}
+
+int flow_direction(gs_plan* p, const double* h, bool down, const double* lfill, const int* pit_ids,
+                   const int* flat_dirs, double sealevel, int* rcv, double* dist, double* wgt,
+                   int8_t* rslot, uint8_t* lsink, uint8_t* sea) {
+    GS_TRY(receivers(p, p->R, 1.1, h, sealevel, p->gid, rcv, dist, wgt, rslot));
+    if (p->n == 0) return GS_OK;
+    launch(p, k_flow_direction_post, grid_for(p->n, 256), 256, (int)p->n, p->W, p->R, p->flat, h,
+           down ? 1 : 0, lfill, pit_ids, flat_dirs, sealevel, p->outlet, p->nbr, rcv, dist, wgt,
+           rslot, lsink, sea);
+    GS_LAUNCH();
+    return GS_OK;
+}
+
+}  // namespace gs

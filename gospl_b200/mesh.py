@@ -1,0 +1,262 @@
+"""Finite-volume mesh of a goSPL landscape (init-time host code).
+
+Vectorised restatement of the mesh set-up the reference performs once at
+start-up on one rank:
+
+* Voronoi helpers of ``gospl/mesher/meshfunc.py`` (edges 295-327 with the
+  void-view ``np.unique`` of ``unique_rows`` 20-28, circumcentres 48-59,
+  400-407, control volumes 175-197);
+* the Fortran ``definetin`` (``fortran/functions.F90:2715-2940``): neighbour
+  lists in edge order, edge lengths (planar ``norm2`` or great-circle),
+  Voronoi face lengths and cell areas (planar Heron or spherical excess),
+  accumulated in the reference's cell/edge order;
+* the single-rank boundary bookkeeping of ``_buildMesh``
+  (``gospl/mesher/unstructuredmesh.py:444-533``) and the area checks of
+  ``_meshStructure`` (``unstructuredmesh.py:120-202``).
+
+Cells are handled as int32 (PETSc ``IntType``); that dtype fixes the
+byte-lexicographic edge order of the void-view unique, hence every vertex's
+neighbour order, on which the reference's receiver distances depend.
+"""
+import numpy as np
+
+_PI = 3.1415926535897932
+_R2D = 180.0 / _PI
+
+
+def _norm2(v):
+    """gfortran NORM2 (scaled sum of squares) over the last axis of size 3."""
+    scale = np.zeros(v.shape[:-1])
+    ssq = np.ones(v.shape[:-1])
+    for c in range(3):
+        x = v[..., c]
+        ax = np.abs(x)
+        nz = x != 0.0
+        up = nz & (scale < ax)
+        dn = nz & ~up
+        with np.errstate(divide="ignore", invalid="ignore"):
+            vu = scale / np.where(up, ax, 1.0)
+            vd = ax / np.where(dn, scale, 1.0)
+        ssq = np.where(up, 1.0 + ssq * vu * vu, np.where(dn, ssq + vd * vd, ssq))
+        scale = np.where(up, ax, scale)
+    return scale * np.sqrt(ssq)
+
+
+def _lonlat(p):
+    r = np.sqrt(p[..., 0] * p[..., 0] + p[..., 1] * p[..., 1] + p[..., 2] * p[..., 2])
+    lat = np.arcsin(p[..., 2] / r) * _R2D
+    lon = np.arctan2(p[..., 1], p[..., 0]) * _R2D
+    return lon * _PI / 180.0, lat * _PI / 180.0
+
+
+def _distance(p1, p2):
+    """functions.F90:368-393: planar norm2 when both z are 0, else great circle."""
+    out = np.empty(p1.shape[:-1])
+    planar = (p2[..., 2] == 0.0) & (p1[..., 2] == 0.0)
+    if planar.any():
+        out[planar] = _norm2(p2[planar] - p1[planar])
+    sph = ~planar
+    if sph.any():
+        a, b = p1[sph], p2[sph]
+        radius = _norm2(a)
+        lon1, lat1 = _lonlat(a)
+        lon2, lat2 = _lonlat(b)
+        c1, s1, c2, s2 = np.cos(lat1), np.sin(lat1), np.cos(lat2), np.sin(lat2)
+        dlon = lon1 - lon2
+        clon, slon = np.cos(dlon), np.sin(dlon)
+        x = c2 * slon
+        y = c1 * s2 - s1 * c2 * clon
+        out[sph] = radius * np.arctan2(np.sqrt(x * x + y * y), (s1 * s2 + c1 * c2 * clon))
+    return out
+
+
+def _slerp_mid(p1, p2):
+    n1 = _norm2(p1)
+    n2 = _norm2(p2)
+    v1 = p1 / n1[:, None]
+    v2 = p2 / n2[:, None]
+    d = v1[:, 0] * v2[:, 0] + v1[:, 1] * v2[:, 1] + v1[:, 2] * v2[:, 2]
+    a = np.arccos(d)
+    sh = np.sin(0.5 * a)[:, None]
+    sa = np.sin(a)[:, None]
+    pt = sh * v1 / sa + sh * v2 / sa
+    return n1[:, None] * pt / _norm2(pt)[:, None]
+
+
+def _striarea(v1, v2, v3):
+    r = np.sqrt(v1[:, 0] * v1[:, 0] + v1[:, 1] * v1[:, 1] + v1[:, 2] * v1[:, 2])
+    lon1, lat1 = _lonlat(v1)
+    lon2, lat2 = _lonlat(v2)
+    lon3, lat3 = _lonlat(v3)
+    a = np.arccos(np.sin(lat2) * np.sin(lat3) + np.cos(lat2) * np.cos(lat3) * np.cos(lon3 - lon2))
+    b = np.arccos(np.sin(lat1) * np.sin(lat3) + np.cos(lat1) * np.cos(lat3) * np.cos(lon3 - lon1))
+    c = np.arccos(np.sin(lat1) * np.sin(lat2) + np.cos(lat1) * np.cos(lat2) * np.cos(lon2 - lon1))
+    al = np.arccos((np.cos(a) - np.cos(b) * np.cos(c)) / (np.sin(b) * np.sin(c)))
+    be = np.arccos((np.cos(b) - np.cos(a) * np.cos(c)) / (np.sin(a) * np.sin(c)))
+    ga = np.arccos((np.cos(c) - np.cos(a) * np.cos(b)) / (np.sin(a) * np.sin(b)))
+    return (al + be + ga - _PI) * (r * r)
+
+
+def _heron(p1, p2, p3):
+    x1, y1, x2, y2, x3, y3 = p1[:, 0], p1[:, 1], p2[:, 0], p2[:, 1], p3[:, 0], p3[:, 1]
+    l1 = np.sqrt((x1 - x2) * (x1 - x2) + (y1 - y2) * (y1 - y2))
+    l2 = np.sqrt((x2 - x3) * (x2 - x3) + (y2 - y3) * (y2 - y3))
+    l3 = np.sqrt((x3 - x1) * (x3 - x1) + (y3 - y1) * (y3 - y1))
+    p = (l1 + l2 + l3) / 2
+    with np.errstate(invalid="ignore"):
+        out = np.sqrt(p * (p - l1) * (p - l2) * (p - l3))
+    degen = ((x1 == x2) & (y1 == y2)) | ((x1 == x3) & (y1 == y3)) | ((x2 == x3) & (y2 == y3))
+    out[degen] = 0.0
+    return out
+
+
+def voronoi(coords, cells):
+    """Edges (reference order), cell->edge map, circumcentres, control volumes."""
+    cells = np.asarray(cells, dtype=np.int32)
+    li = np.array([[1, 2], [2, 0], [0, 1]]).T
+    hier = cells.T[li]                                  # (2, 3, ncell)
+    half = coords[hier[1]] - coords[hier[0]]
+    eij = np.einsum("ijk, ijk->ij", half[[1, 2, 0]], half[[2, 0, 1]])
+    eii = np.einsum("ijk, ijk->ij", half, half)
+    vol = 0.5 * np.sqrt(eij[2] * eij[0] + eij[0] * eij[1] + eij[1] * eij[2])
+    ce = -eij * 0.25 / vol[None]
+    part = 0.25 * eii * ce
+    vals = np.array([sum([part[i] for i in np.where(li.T == k)[0]]) for k in range(3)])
+    cv = np.zeros(len(coords))
+    np.add.at(cv, cells.T, vals)
+    a = np.sort(hier.reshape(2, -1).T)
+    b = np.ascontiguousarray(a).view(np.dtype((np.void, a.dtype.itemsize * 2)))
+    ub, inv, cts = np.unique(b, return_inverse=True, return_counts=True)
+    if np.any(cts > 2):
+        raise ValueError("an edge is shared by more than two cells")
+    edges = ub.view(a.dtype).reshape(-1, 2)
+    X = coords[cells.T]
+    alpha = eii * eij
+    asum = alpha[0] + alpha[1] + alpha[2]
+    beta = alpha / asum[None]
+    aa = X * beta[..., None]
+    cc = aa[0] + aa[1] + aa[2]
+    return edges, inv.reshape(3, -1).T, cc, cv, cts == 1
+
+
+def definetin(coords, cells, edges, cells_edges, cc, curved):
+    """Vectorised definetin: (nnb, ngb[N,12], elgt, vdist, farea, narea)."""
+    n = len(coords)
+    m = len(edges)
+    # neighbours in edge order (first 12 kept)
+    node = np.empty(2 * m, dtype=np.int64)
+    nbr = np.empty(2 * m, dtype=np.int64)
+    node[0::2], nbr[0::2] = edges[:, 0], edges[:, 1]
+    node[1::2], nbr[1::2] = edges[:, 1], edges[:, 0]
+    order = np.argsort(node, kind="stable")
+    node, nbr = node[order], nbr[order]
+    first = np.searchsorted(node, np.arange(n))
+    slot = np.arange(2 * m) - first[node]
+    keep = slot < 12
+    node, nbr, slot = node[keep], nbr[keep], slot[keep]
+    nnb = np.bincount(node, minlength=n).astype(np.int32)
+    ngb = -np.ones((n, 12), dtype=np.int32)
+    ngb[node, slot] = nbr
+    elgt = np.zeros((n, 12))
+    elgt[node, slot] = _distance(coords[node], coords[nbr])
+    # cells around each vertex, ascending, first 12
+    nc = len(cells)
+    cn = np.repeat(np.arange(nc), 3)
+    vn = cells.reshape(-1).astype(np.int64)
+    order = np.argsort(vn, kind="stable")
+    vn, cn = vn[order], cn[order]
+    first = np.searchsorted(vn, np.arange(n))
+    rank = np.arange(len(vn)) - first[vn]
+    keep = rank < 12
+    vn, cn = vn[keep], cn[keep]
+    # contributions (vertex, cell, local edge e) in vertex/cell/e order
+    K = np.repeat(vn, 3)
+    C = np.repeat(cn, 3)
+    E = np.tile(np.arange(3), len(vn))
+    eg = cells_edges[C, E]
+    e1 = edges[eg, 0].astype(np.int64)
+    e2 = edges[eg, 1].astype(np.int64)
+    valid = (e1 == K) | (e2 == K)
+    K, C, e1, e2 = K[valid], C[valid], e1[valid], e2[valid]
+    other = np.where(e1 == K, e2, e1)
+    key_sorted = node * n + nbr                      # (node, nbr) -> slot
+    srt = np.argsort(key_sorted)
+    pos = np.searchsorted(key_sorted[srt], K * n + other)
+    sid = slot[srt][np.clip(pos, 0, len(srt) - 1)]
+    found = key_sorted[srt][np.clip(pos, 0, len(srt) - 1)] == K * n + other
+    if curved:
+        mid = _slerp_mid(coords[e1], coords[e2])
+    else:
+        mid = 0.5 * (coords[e1] + coords[e2])
+    ccc = cc[C]
+    dist = _distance(mid, ccc)
+    vdist = np.zeros(n * 12)
+    np.add.at(vdist, (K * 12 + sid)[found], dist[found])
+    tri = _striarea(coords[K], mid, ccc) if curved else _heron(coords[K], mid, ccc)
+    area = np.zeros(n)
+    np.add.at(area, K, tri)
+    narea = area.copy()
+    farea = area.copy()
+    farea[np.isnan(farea)] = 0.0
+    return nnb, ngb, elgt, vdist.reshape(n, 12), farea, narea
+
+
+class FVMesh:
+    """Finite-volume mesh plus boundary sets, in the reference's node order."""
+
+    def __init__(self, coords, cells, bc="oooo"):
+        coords = np.ascontiguousarray(coords, dtype=np.float64)
+        cells = np.ascontiguousarray(cells, dtype=np.int32)
+        self.coords = coords
+        self.cells = cells
+        self.n = len(coords)
+        edges, cells_edges, cc, cv, bedge = voronoi(coords, cells)
+        self.borders = np.unique(edges[bedge].ravel()).astype(np.int64) if bedge.any() else np.zeros(0, np.int64)
+        self.flat = len(self.borders) > 0
+        larea_mf = np.abs(cv)
+        larea_mf[np.isnan(larea_mf)] = 1.0
+        if not self.flat:
+            radius = np.linalg.norm(coords[0])
+            cc = cc * (radius / np.linalg.norm(cc, axis=1)).reshape((len(cc), 1))
+        (self.nnb, self.ngb, self.elgt, self.vdist, self.farea, narea) = definetin(
+            coords, cells, edges, cells_edges, cc, curved=not self.flat)
+        larea = narea.copy()
+        larea[np.isnan(larea)] = 1.0
+        if self.flat and np.max(np.abs(larea_mf - larea)) > 1.0e2:
+            larea = larea_mf.copy()
+            self.farea = larea_mf.copy()
+        self.larea = larea
+        self.maxarea = float(larea.max())
+        self.outlet = self.borders.copy()
+        self.open_nodes = np.zeros(0, np.int64)
+        if self.flat:
+            flags = dict(zip("NESW", ({"o": 0, "f": 1, "c": 2, "w": 3}[c] for c in bc)))
+            xmin, xmax = coords[:, 0].min(), coords[:, 0].max()
+            ymin, ymax = coords[:, 1].min(), coords[:, 1].max()
+            tol = 1.0e-9
+            pts = {"S": np.where(np.isclose(coords[:, 1], ymin, atol=tol))[0],
+                   "N": np.where(np.isclose(coords[:, 1], ymax, atol=tol))[0],
+                   "E": np.where(np.isclose(coords[:, 0], xmax, atol=tol))[0],
+                   "W": np.where(np.isclose(coords[:, 0], xmin, atol=tol))[0]}
+            wall = [pts[k] for k in "SENW" if flags[k] == 3 and len(pts[k])]
+            if wall:
+                self.outlet = np.setdiff1d(self.borders, np.unique(np.concatenate(wall)))
+            opn = [pts[k] for k in "NESW" if flags[k] == 0 and len(pts[k])]
+            if opn:
+                self.open_nodes = np.unique(np.concatenate(opn)).astype(np.int64)
+
+    @classmethod
+    def from_arrays(cls, d):
+        """Wrap precomputed FV arrays (keys nnb, ngb, elgt, vdist, farea, larea,
+        outlet, open_nodes, flat)."""
+        self = cls.__new__(cls)
+        self.n = len(d["nnb"])
+        for k in ("nnb", "ngb", "elgt", "vdist", "farea", "larea"):
+            setattr(self, k, np.ascontiguousarray(d[k]))
+        self.outlet = np.asarray(d["outlet"], np.int64)
+        self.open_nodes = np.asarray(d.get("open_nodes", np.zeros(0)), np.int64)
+        self.flat = bool(d["flat"])
+        self.maxarea = float(self.larea.max())
+        self.coords = d.get("coords")
+        self.cells = d.get("cells")
+        return self

@@ -1,0 +1,260 @@
+"""PETSc-free goSPL driver for the per-timestep surface-process path on a B200.
+
+``Model`` keeps the reference's entry points and state names
+(``gospl/model.py:179-495``):
+
+* ``flowAccumulation()``  — FAMesh.flowAccumulation (flowplex.py:752-945)
+* ``fillElevation(sed)``  — PITFill.fillElevation (pitfilling.py:849-903)
+* ``_buildFlowDirection(h, down)`` — flowplex.py:480-544
+* ``erodepSPL()``         — SPL.erodepSPL (SPL.py:402-454), n = 1, G = 0
+* ``getHillslope()``      — hillSLP.getHillslope (hillslope.py:614-649)
+* ``applyForces()``       — UnstMesh.applyForces (unstructuredmesh.py:743-794)
+* ``runProcesses()``      — the time loop of model.py:331-466 with
+  ``fast: false, nodep: true``.
+
+All state lives in torch CUDA tensors (float64 / int32 / uint8); every stage is
+one call through the C ABI of ``libgospl_b200.so``.  Per-receiver arrays are
+stored receiver-major ``[R, N]``; the reference's ``[N, R]`` views are exposed
+as transposes (``rcvIDi``, ``wghtVali``, ``distRcvi``).  There is no CPU
+fallback: without a CUDA device or the built library the constructor raises.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+from . import _lib
+from .mesh import FVMesh
+
+_L = None
+
+
+def _lib_handle():
+    global _L
+    if _L is None:
+        _L = _lib.load()
+    return _L
+
+
+class Model:
+    """One landscape on one GPU.
+
+    Build from a goSPL YAML input (``Model("input.yml")``, the subset of keys
+    read by inputparser.py for this path) or from arrays
+    (``Model(coords=..., cells=..., elev=..., params=...)``).  ``params`` keys:
+    dt, tStart, tEnd, flowDir, K (scalar or per-vertex), d, m, Cda, Cdm, oFill,
+    sealevel, bc, rain (per-vertex m/yr), upsub (per-vertex m/yr or None).
+    """
+
+    def __init__(self, filename=None, *, coords=None, cells=None, elev=None, params=None, mesh=None,
+                 device="cuda", init_flow=True, cg_rtol=1.0e-13, cg_maxit=2000):
+        import torch
+
+        if not torch.cuda.is_available():
+            raise RuntimeError("gospl_b200.Model needs a CUDA device")
+        self.torch = torch
+        L = _lib_handle()
+        if filename is not None:
+            from .inputparser import read_input
+            coords, cells, elev, params = read_input(filename)
+        if mesh is None:
+            mesh = FVMesh(coords, cells, params.get("bc", "oooo"))
+        self.mesh = mesh
+        self.dev = torch.device(device)
+        if self.dev.type == "cuda" and self.dev.index is None:
+            self.dev = torch.device("cuda", torch.cuda.current_device())
+        self.lpoints = mesh.n
+        n = mesh.n
+        p = dict(params)
+        self.dt = float(p["dt"])
+        self.tStart = float(p.get("tStart", 0.0))
+        self.tEnd = float(p["tEnd"])
+        self.tNow = self.tStart
+        self.flowDir = int(p.get("flowDir", 8))
+        self.flowExp = 1.1
+        self.coeffd = float(p.get("d", 0.0))
+        self.spl_m = float(p.get("m", 0.5))
+        self.Cda = float(p.get("Cda", 0.0))
+        self.Cdm = float(p.get("Cdm", 0.0))
+        self.oFill = float(p.get("oFill", -6000.0))
+        self.sealevel = float(p.get("sealevel", 0.0))
+        self.flatModel = bool(mesh.flat)
+        self.cg_rtol = cg_rtol
+        self.cg_maxit = cg_maxit
+        self.stats = {}
+
+        f64 = dict(dtype=torch.float64, device=self.dev)
+        i32 = dict(dtype=torch.int32, device=self.dev)
+        u8 = dict(dtype=torch.uint8, device=self.dev)
+        K = p["K"]
+        if np.ndim(K) == 0:
+            self.K = float(K)
+            self.Kfield = None
+        else:
+            self.K = 0.0
+            self.Kfield = torch.as_tensor(np.asarray(K, np.float64), **f64)
+        self.rainMesh = torch.as_tensor(np.asarray(p["rain"], np.float64), **f64)
+        up = p.get("upsub")
+        self.upsub = None if up is None else torch.as_tensor(np.asarray(up, np.float64), **f64)
+
+        R = self.flowDir
+        self.hGlobal = torch.as_tensor(np.asarray(elev, np.float64), **f64).clone()
+        self.cumED = torch.zeros(n, **f64)
+        self.EbLocal = torch.zeros(n, **f64)
+        self.FAL = torch.zeros(n, **f64)
+        self.fillFAL = torch.zeros(n, **f64)
+        self.waterFilled = torch.zeros(n, **f64)
+        self.lFill = torch.zeros(n, **f64)
+        self.bL = torch.zeros(n, **f64)
+        self.pitIDs = torch.zeros(n, **i32)
+        self.flatDirs = torch.zeros(n, **i32)
+        self.rcv_i = torch.zeros((R, n), **i32)
+        self.dist_i = torch.zeros((R, n), **f64)
+        self.wgt_i = torch.zeros((R, n), **f64)
+        self.lsink_mask = torch.zeros(n, **u8)
+        self.sea_mask = torch.zeros(n, **u8)
+
+        handle = ctypes.c_void_p()
+        outlet = np.ascontiguousarray(mesh.outlet, np.int32)
+        opn = np.ascontiguousarray(mesh.open_nodes, np.int32)
+        nnb = np.ascontiguousarray(mesh.nnb, np.int32)
+        ngb = np.ascontiguousarray(mesh.ngb, np.int32)
+        elgt = np.ascontiguousarray(mesh.elgt, np.float64)
+        vd = np.ascontiguousarray(mesh.vdist, np.float64)
+        fa = np.ascontiguousarray(mesh.farea, np.float64)
+        la = np.ascontiguousarray(mesh.larea, np.float64)
+        torch.cuda.set_device(self.dev)
+        _lib.check(L.gs_plan_create(n, _lib.ptr(nnb), _lib.ptr(ngb), _lib.ptr(elgt), _lib.ptr(vd),
+                                    _lib.ptr(fa), _lib.ptr(la), _lib.ptr(outlet), len(outlet),
+                                    _lib.ptr(opn), len(opn), int(self.flatModel), R, ctypes.byref(handle)))
+        self._plan = handle
+        self.stream = torch.cuda.current_stream(self.dev)
+        _lib.check(L.gs_plan_set_stream(self._plan, ctypes.c_void_p(self.stream.cuda_stream)))
+        self.applyForces()
+        if init_flow:
+            self.flowAccumulation()
+
+    # ------------------------------------------------------------- views
+    @property
+    def rcvIDi(self):
+        return self.rcv_i.t()
+
+    @property
+    def wghtVali(self):
+        return self.wgt_i.t()
+
+    @property
+    def distRcvi(self):
+        return self.dist_i.t()
+
+    @property
+    def lsink(self):
+        return self.lsink_mask.bool()
+
+    @property
+    def seaID(self):
+        return self.sea_mask.bool()
+
+    @property
+    def h(self):
+        return self.hGlobal
+
+    def launches(self):
+        return int(_lib_handle().gs_plan_launches(self._plan))
+
+    # ------------------------------------------------------------- stages
+    def applyForces(self):
+        """unstructuredmesh.py:743-794 (constant sea level, uniform-in-time rain)."""
+        L = _lib_handle()
+        _lib.check(L.gs_apply_forces(self._plan, _lib.ptr(self.hGlobal), _lib.ptr(self.rainMesh),
+                                     _lib.ptr(self.upsub), self.dt, self.sealevel, _lib.ptr(self.bL)))
+        self.rainVal = self.rainMesh.clamp(min=0.0)   # unstructuredmesh.py:960
+
+    def fillElevation(self, sed=False):
+        """pitfilling.py:849-903; per-pit tables read with pit_tables()."""
+        if sed:
+            raise NotImplementedError("fillElevation(sed=True) belongs to sediment routing, not this path")
+        L = _lib_handle()
+        npits = ctypes.c_int32()
+        _lib.check(L.gs_fill_elevation(self._plan, _lib.ptr(self.hGlobal), self.sealevel, self.oFill,
+                                       _lib.ptr(self.lFill), _lib.ptr(self.pitIDs), _lib.ptr(self.flatDirs),
+                                       ctypes.byref(npits)))
+        self.npits = int(npits.value)
+
+    def pit_tables(self):
+        """(pitParams [P+1,3], pitInfo [P+1,2], filled_lvl [P+1,5], filled_vol [P+1,5])."""
+        t = self.torch
+        np1 = self.npits + 1
+        pp = t.zeros((np1, 3), dtype=t.float64, device=self.dev)
+        pi = t.zeros((np1, 2), dtype=t.int32, device=self.dev)
+        fl = t.zeros((np1, 5), dtype=t.float64, device=self.dev)
+        fv = t.zeros((np1, 5), dtype=t.float64, device=self.dev)
+        _lib.check(_lib_handle().gs_pit_tables(self._plan, _lib.ptr(pp), _lib.ptr(pi), _lib.ptr(fl),
+                                               _lib.ptr(fv)))
+        return pp, pi, fl, fv
+
+    def _buildFlowDirection(self, h, down=True):
+        """mfdreceivers only (flowplex.py:499-501) into [R, N] tensors."""
+        t = self.torch
+        R, n = self.flowDir, self.lpoints
+        rcv = t.empty((R, n), dtype=t.int32, device=self.dev)
+        dist = t.empty((R, n), dtype=t.float64, device=self.dev)
+        wgt = t.empty((R, n), dtype=t.float64, device=self.dev)
+        _lib.check(_lib_handle().gs_mfdreceivers(self._plan, R, self.flowExp, _lib.ptr(h), self.sealevel, None,
+                                                 _lib.ptr(rcv), _lib.ptr(dist), _lib.ptr(wgt)))
+        return rcv, dist, wgt
+
+    def flowAccumulation(self):
+        L = _lib_handle()
+        st = _lib.GsStats()
+        _lib.check(L.gs_flow_accumulation(
+            self._plan, _lib.ptr(self.hGlobal), _lib.ptr(self.bL), self.sealevel, self.oFill, self.dt,
+            _lib.ptr(self.FAL), _lib.ptr(self.fillFAL), _lib.ptr(self.waterFilled), _lib.ptr(self.lFill),
+            _lib.ptr(self.pitIDs), _lib.ptr(self.flatDirs), _lib.ptr(self.rcv_i), _lib.ptr(self.dist_i),
+            _lib.ptr(self.wgt_i), _lib.ptr(self.lsink_mask), _lib.ptr(self.sea_mask), ctypes.byref(st)))
+        self.npits = st.npits
+        self.stats["flow"] = st.as_dict()
+
+    def erodepSPL(self):
+        L = _lib_handle()
+        st = _lib.GsStats()
+        _lib.check(L.gs_erodep_spl(
+            self._plan, _lib.ptr(self.hGlobal), _lib.ptr(self.cumED), _lib.ptr(self.EbLocal),
+            _lib.ptr(self.FAL), _lib.ptr(self.rainVal), self.K, _lib.ptr(self.Kfield), self.coeffd,
+            self.spl_m, self.dt, _lib.ptr(self.rcv_i), _lib.ptr(self.dist_i), _lib.ptr(self.wgt_i),
+            _lib.ptr(self.lsink_mask), _lib.ptr(self.sea_mask), ctypes.byref(st)))
+
+    def getHillslope(self):
+        L = _lib_handle()
+        st = _lib.GsStats()
+        _lib.check(L.gs_hillslope(self._plan, _lib.ptr(self.hGlobal), _lib.ptr(self.cumED),
+                                  _lib.ptr(self.EbLocal), self.sealevel, self.Cda, self.Cdm, self.dt,
+                                  self.cg_rtol, self.cg_maxit, ctypes.byref(st)))
+        self.stats["hillslope"] = st.as_dict()
+
+    def step(self):
+        """One physics step of runProcesses (model.py:347-453, fast=False, nodep=True)."""
+        self.flowAccumulation()
+        self.erodepSPL()
+        self.getHillslope()
+        if self.tNow < self.tEnd:
+            self.applyForces()
+        self.tNow += self.dt
+
+    def runProcesses(self):
+        while self.tNow <= self.tEnd:
+            if self.tNow == self.tEnd:
+                break
+            self.step()
+
+    def destroy(self):
+        if getattr(self, "_plan", None) is not None:
+            self.torch.cuda.synchronize(self.dev)
+            _lib_handle().gs_plan_destroy(self._plan)
+            self._plan = None
+
+    def __del__(self):
+        try:
+            self.destroy()
+        except Exception:
+            pass

@@ -1,0 +1,150 @@
+/*
+ * gospl_b200 — C ABI of the B200 (sm_100a) implementation of goSPL's
+ * per-timestep surface-process path.
+ *
+ * Conventions
+ *  - Every array argument is a DEVICE pointer (CUDA global memory) owned by the
+ *    caller unless stated otherwise; the library never frees caller memory.
+ *  - Per-vertex arrays have length nb; per-receiver arrays are receiver-major
+ *    ("[nrcv][nb]": element (k, i) at k*nb + i).
+ *  - Node ids are 0-based int32, as the reference's f2py module stores them.
+ *  - Work is issued on the plan's stream (gs_plan_set_stream, default stream
+ *    0).  Functions that must inspect device results (pit counts, cascade
+ *    control flow, CG convergence) synchronise that stream before returning.
+ *  - Every function returns GS_OK (0) or an error code; gs_last_error() gives
+ *    the message of the last failure on the calling host thread.
+ *  - A plan is not thread-safe: use one plan per host thread.
+ */
+#ifndef GOSPL_B200_H
+#define GOSPL_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GS_OK 0
+#define GS_EINVAL 1      /* bad argument (size, range, null pointer)              */
+#define GS_ECUDA 2       /* CUDA runtime error                                    */
+#define GS_EMAXITER 3    /* iteration cap reached without convergence             */
+#define GS_ENONFINITE 4  /* NaN/Inf met in an input or a reduction                */
+#define GS_ECYCLE 5      /* a flow graph that should be acyclic has a cycle       */
+#define GS_ETIMEOUT 6    /* a device-side wait exceeded its time budget           */
+#define GS_ENOMEM 7      /* device allocation failed                              */
+
+typedef struct gs_plan gs_plan;
+
+/* Counters filled by the flow/erosion entry points (host memory). */
+typedef struct gs_stats {
+    int32_t npits;            /* depressions found by the fill (P; ids 1..P)          */
+    int32_t cascade_passes;   /* _distributeDownstream passes executed                */
+    int32_t cascade_solves;   /* cascade flow solves executed                         */
+    int32_t fill_rounds;      /* spill-graph relaxation rounds                        */
+    int32_t flat_rounds;      /* flat-distance BFS levels                             */
+    int32_t cycle_nodes;      /* nodes solved by the cycle fallback (0 when acyclic)  */
+    int32_t cg_iters;         /* hillslope CG iterations                              */
+    int32_t status;           /* last internal status                                 */
+    double cg_relres;         /* final relative residual of the hillslope solve      */
+} gs_stats;
+
+int gs_version(void);
+int gs_last_error(char* buf, int64_t len);
+
+/*
+ * Mesh plan.  The finite-volume arrays are exactly what the reference's
+ * `definetin` (fortran/functions.F90:2715-2940) leaves in module `meshparams`:
+ * nnb = FVnNb, ngb = FVnID (C-order [nb][12], -1 padded), elgt = FVeLgt,
+ * vdist = FVvDist, farea = FVarea; larea is the Python-side cell area
+ * (unstructuredmesh.py:165-188).  HOST pointers (copied).  outlet_ids are the
+ * draining boundary nodes (`outletIDs`, unstructuredmesh.py:463-518) and
+ * open_ids the 'o' edge nodes reset by _drainOpenEdges.
+ */
+int gs_plan_create(int64_t nb, const int32_t* nnb, const int32_t* ngb, const double* elgt,
+                   const double* vdist, const double* farea, const double* larea,
+                   const int32_t* outlet_ids, int64_t n_outlet, const int32_t* open_ids,
+                   int64_t n_open, int32_t flat_model, int32_t flow_dir, gs_plan** out);
+int gs_plan_destroy(gs_plan* plan);
+int gs_plan_set_stream(gs_plan* plan, void* cuda_stream);
+/* Number of device kernels this plan launched since creation. */
+int64_t gs_plan_launches(const gs_plan* plan);
+
+/*
+ * Multiple-flow-direction receivers.  Replaces `mfdreceivers(nRcv, exp, elev,
+ * sl, gid)` (fortran/functions.F90:1544-1671, bound in gospl/_fortran through
+ * fortran/functions.pyf) called from flowplex.py:499-501.  Outputs receiver-
+ * major [nrcv][nb]: rcv (self id = no receiver), dist, wgt.
+ */
+int gs_mfdreceivers(gs_plan* plan, int32_t nrcv, double exp, const double* elev, double sl,
+                    const int32_t* gid, int32_t* rcv, double* dist, double* wgt);
+
+/*
+ * Depression filling.  Replaces PITFill.fillElevation(sed=False)
+ * (gospl/flow/pitfilling.py:849-903) and the Fortran kernels it drives
+ * (edge_tile, fill_tile, fill_edges, fill_depressions, label_pits, pits_cons,
+ * fill_dir, nghb_dir, getpitvol: functions.F90:1845-2499).  Outputs per vertex:
+ * lFill, pitIDs (-1 or 1..P), flatDirs (-1, self or a neighbour).  The per-pit
+ * tables (pitParams, pitInfo, filled_lvl, filled_vol) stay in the plan; read
+ * them with gs_pit_tables.  *npits receives P.
+ */
+int gs_fill_elevation(gs_plan* plan, const double* h, double sealevel, double ofill,
+                      double* lfill, int32_t* pit_ids, int32_t* flat_dirs, int32_t* npits);
+/* Copy the pit tables of the last fill into caller DEVICE buffers sized
+ * (P+1) rows: pit_params [P+1][3], pit_info [P+1][2], filled_lvl [P+1][5],
+ * filled_vol [P+1][5] (rows as in pitfilling.py:521-555, 810-891). */
+int gs_pit_tables(gs_plan* plan, double* pit_params, int32_t* pit_info, double* filled_lvl,
+                  double* filled_vol);
+
+/*
+ * Flow accumulation.  Replaces FAMesh.flowAccumulation (flowplex.py:752-945)
+ * with its fill, _buildFlowDirection(down=False), the (I - W^T) FA solve, the
+ * downstream lake cascade (_distributeDownstream, flowplex.py:576-686) and the
+ * lake zeroing / fillFAL proxy.  bl = rain * larea (m^3/yr).
+ * Outputs: fal, fill_fal, water_filled (= waterFilled - h), lfill, pit_ids,
+ * flat_dirs, the snapshots rcv_i/dist_i/wgt_i ([nrcv][nb], the reference's
+ * rcvIDi/distRcvi/wghtVali), lsink (uint8, the LIVE lsink after the cascade,
+ * as SPL.py:352 reads it) and sea (uint8, lFill <= sealevel).
+ */
+int gs_flow_accumulation(gs_plan* plan, const double* h, const double* bl, double sealevel,
+                         double ofill, double dt, double* fal, double* fill_fal,
+                         double* water_filled, double* lfill, int32_t* pit_ids,
+                         int32_t* flat_dirs, int32_t* rcv_i, double* dist_i, double* wgt_i,
+                         uint8_t* lsink, uint8_t* sea, gs_stats* stats);
+
+/*
+ * Implicit linear stream-power erosion (n = 1, G = 0).  Replaces
+ * SPL.erodepSPL / _getEroDepRate / _eroMats (gospl/eroder/SPL.py:45-114,
+ * 260-366, 402-454).  Kbr = K * rain^d * dt * FAL^m (K a scalar when k_field
+ * is NULL, else a per-vertex field); the implicit system is solved exactly by
+ * a sweep over the receiver graph.  Updates h and cum_ed in place and writes
+ * eb = dz/dt.  Uses the receivers/lsink/sea produced by gs_flow_accumulation.
+ */
+int gs_erodep_spl(gs_plan* plan, double* h, double* cum_ed, double* eb, const double* fal,
+                  const double* rain, double k_scalar, const double* k_field, double d,
+                  double m, double dt, const int32_t* rcv_i, const double* dist_i,
+                  const double* wgt_i, const uint8_t* lsink, const uint8_t* sea,
+                  gs_stats* stats);
+
+/*
+ * Linear hillslope diffusion.  Replaces hillSLP.getHillslope with
+ * _hillSlope(smooth=0) (gospl/sed/hillslope.py:90-233, 614-649) and the
+ * Fortran sethillslopecoeff (functions.F90:901-938): solves (I + L) h = hOld
+ * with Jacobi-preconditioned CG to relative residual `rtol`.  Updates h and
+ * cum_ed in place and adds dz/dt to eb.
+ */
+int gs_hillslope(gs_plan* plan, double* h, double* cum_ed, double* eb, double sealevel,
+                 double cda, double cdm, double dt, double rtol, int32_t max_iter,
+                 gs_stats* stats);
+
+/*
+ * Forcing of one step: UnstMesh.applyForces (unstructuredmesh.py:743-794) with
+ * _updateRain (bl = max(rain,0) * larea), applyTectonics (h += upsub * dt) and
+ * _drainOpenEdges (796-901).  upsub may be NULL.
+ */
+int gs_apply_forces(gs_plan* plan, double* h, const double* rain, const double* upsub, double dt,
+                    double sealevel, double* bl);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,56 @@
+"""C ABI boundary checks that need no GPU: the library loads, exports every
+function include/gospl_b200.h declares, and the stats struct matches."""
+import ctypes
+import os
+import re
+
+import pytest
+
+from conftest import ROOT
+
+
+def _declared():
+    src = open(os.path.join(ROOT, "include", "gospl_b200.h")).read()
+    return sorted(set(re.findall(r"\b(gs_[a-z_0-9]+)\s*\(", src)))
+
+
+def test_library_builds_and_loads():
+    from gospl_b200 import build as B
+    B.build()
+    from gospl_b200 import _lib
+    L = _lib.load()
+    assert L.gs_version() >= 100
+
+
+def test_exports_every_declared_symbol():
+    from gospl_b200 import _lib
+    L = _lib.load()
+    names = _declared()
+    assert len(names) >= 12
+    for name in names:
+        assert hasattr(L, name), name
+    assert set(names) == set(_lib.EXPORTS)
+
+
+def test_stats_struct_layout():
+    from gospl_b200 import _lib
+    assert ctypes.sizeof(_lib.GsStats) == 8 * 4 + 8
+
+
+def test_null_plan_is_rejected():
+    from gospl_b200 import _lib
+    L = _lib.load()
+    assert L.gs_mfdreceivers(None, 3, 1.1, None, 0.0, None, None, None, None) == 1
+    buf = ctypes.create_string_buffer(256)
+    assert L.gs_last_error(buf, 256) == 1
+    assert b"plan" in buf.value
+
+
+def test_bad_plan_arguments_are_rejected():
+    from gospl_b200 import _lib
+    L = _lib.load()
+    h = ctypes.c_void_p()
+    assert L.gs_plan_create(-1, None, None, None, None, None, None, None, 0, None, 0, 0, 3,
+                            ctypes.byref(h)) == 1
+    assert L.gs_plan_create(10, None, None, None, None, None, None, None, 0, None, 0, 0, 13,
+                            ctypes.byref(h)) == 1
