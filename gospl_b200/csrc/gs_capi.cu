@@ -1,4 +1,5 @@
 // extern "C" boundary of libgospl_b200.so (declarations in include/gospl_b200.h).
+#include <algorithm>
 #include <cstring>
 #include <exception>
 #include <string>
@@ -15,6 +16,24 @@ void set_error(int code, const std::string& msg) {
     g_msg = msg;
 }
 int last_code() { return g_code; }
+
+void prof_begin(gs_plan* p, const void* fn, cudaEvent_t* stop) {
+    int idx = -1;
+    for (size_t k = 0; k < p->prof_fn.size(); k++)
+        if (p->prof_fn[k] == fn) { idx = (int)k; break; }
+    if (idx < 0) {
+        idx = (int)p->prof_fn.size();
+        p->prof_fn.push_back(fn);
+    }
+    cudaEvent_t a, b;
+    if (cudaEventCreate(&a) != cudaSuccess) return;
+    if (cudaEventCreate(&b) != cudaSuccess) { cudaEventDestroy(a); return; }
+    cudaEventRecord(a, p->stream);
+    p->prof_ev.push_back(a);
+    p->prof_ev.push_back(b);
+    p->prof_idx.push_back(idx);
+    *stop = b;
+}
 
 int plan_create(int64_t nb, const int32_t* nnb, const int32_t* ngb, const double* elgt, const double* vdist,
                 const double* farea, const double* larea, const int32_t* outlet_ids, int64_t n_outlet,
@@ -71,6 +90,40 @@ int gs_plan_set_stream(gs_plan* plan, void* stream) {
 }
 
 int64_t gs_plan_launches(const gs_plan* plan) { return plan ? plan->launches : -1; }
+
+int gs_plan_profile(gs_plan* plan, int32_t enable) {
+    NEED(plan);
+    for (cudaEvent_t e : plan->prof_ev) cudaEventDestroy(e);
+    plan->prof_ev.clear();
+    plan->prof_idx.clear();
+    plan->profiling = enable ? 1 : 0;
+    return GS_OK;
+}
+
+int gs_plan_profile_report(gs_plan* plan, char* buf, int64_t len) {
+    NEED(plan);
+    GS_CUDA(cudaStreamSynchronize(plan->stream));
+    std::vector<double> tot(plan->prof_fn.size(), 0.0);
+    std::vector<long> cnt(plan->prof_fn.size(), 0);
+    for (size_t q = 0; q + 1 < plan->prof_ev.size(); q += 2) {
+        float ms = 0.f;
+        if (cudaEventElapsedTime(&ms, plan->prof_ev[q], plan->prof_ev[q + 1]) == cudaSuccess) {
+            tot[plan->prof_idx[q / 2]] += ms;
+            cnt[plan->prof_idx[q / 2]] += 1;
+        }
+    }
+    std::string out;
+    for (size_t k = 0; k < plan->prof_fn.size(); k++) {
+        const char* name = "?";
+        cudaFuncGetName(&name, plan->prof_fn[k]);
+        out += std::string(name) + " " + std::to_string(cnt[k]) + " " + std::to_string(tot[k]) + "\n";
+    }
+    if (buf && len > 0) {
+        std::strncpy(buf, out.c_str(), (size_t)len - 1);
+        buf[len - 1] = 0;
+    }
+    return (int)std::min<size_t>(out.size(), (size_t)0x7fffffff);
+}
 
 int gs_mfdreceivers(gs_plan* plan, int32_t nrcv, double exp, const double* elev, double sl,
                     const int32_t* gid, int32_t* rcv, double* dist, double* wgt) {

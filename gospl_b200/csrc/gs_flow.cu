@@ -214,7 +214,7 @@ int flow_accumulation(gs_plan* p, const double* h, const double* bl, double seal
     launch(p, k_rain_sea, G, B, n, bl, (const uint8_t*)sea, p->nfa);
     GS_LAUNCH();
     int cyc = 0;
-    GS_TRY(flow_solve(p, rcv_i, wgt_i, p->rslot_i, p->nfa, fal, &cyc));
+    GS_TRY(flow_solve(p, rcv_i, wgt_i, p->rslot_i, p->nfa, fal, &cyc, h, nullptr, p->order_i));
     int total_cycles = cyc;
     launch(p, k_copy, G, B, (int64_t)n, h, p->wf);
     // pitVol and "any pit with volume"
@@ -266,7 +266,7 @@ int flow_accumulation(gs_plan* p, const double* h, const double* bl, double seal
                 if (resid > p->maxarea) {
                     excess = true;
                     // solve into FA's buffer: FA is consumed already
-                    GS_TRY(flow_solve(p, p->rcv, p->wgt, p->rslot, p->q2, p->q, &cyc));
+                    GS_TRY(flow_solve(p, p->rcv, p->wgt, p->rslot, p->q2, p->q, &cyc, surf, p->pdir, p->order));
                     total_cycles += cyc;
                     launch(p, k_cascade_accum, G, B, n, (const double*)p->q, dt, h, (const double*)p->wf,
                            p->q, fal);

@@ -33,9 +33,20 @@
 #include <cstring>
 #include <vector>
 
+#include <cooperative_groups.h>
+
 #include "gs_plan.cuh"
 
+namespace cg = cooperative_groups;
+
 namespace gs {
+
+__device__ __forceinline__ int agg_append(int* cnt) {
+    cg::coalesced_group g = cg::coalesced_threads();
+    int base = 0;
+    if (g.thread_rank() == 0) base = atomicAdd(cnt, (int)g.size());
+    return g.shfl(base, 0) + (int)g.thread_rank();
+}
 
 enum { D_MINH = 0, D_LEVEL = 1 };
 enum { I_CHANGED = 0, I_NEXT = 1, I_NPITS0 = 2, I_NPITS = 3 };
@@ -357,8 +368,44 @@ __global__ void k_bfs_step(int m, const int* __restrict__ front, int d, int n,
     for (int s = 0; s < nnb[i]; s++) {
         int c = nbr[(size_t)s * n + i];
         if (c < 0 || pit[c] < 0 || !(f[c] >= fi)) continue;
-        if (atomicCAS(&pdir[c], -1, d + 1) == -1) next[atomicAdd(cnt, 1)] = c;
+        if (atomicCAS(&pdir[c], -1, d + 1) == -1) next[agg_append(cnt)] = c;
     }
+}
+
+// All remaining BFS levels in one block: frontier lists in global memory,
+// __syncthreads between levels (the frontiers of lake flats are small, the
+// level count is large).  Bounded by the vertex count.
+__global__ void k_bfs_block(int fsize0, int* fa, int* fb, int* cnt, int d0, int n,
+                            const double* __restrict__ f, const int* __restrict__ pit,
+                            const int* __restrict__ nbr, const int8_t* __restrict__ nnb, int* pdir,
+                            int* levels_out) {
+    __shared__ int s_size;
+    int fsize = fsize0, d = d0, levels = 0;
+    int* cur = fa;
+    int* nxt = fb;
+    while (fsize > 0 && levels <= n) {
+        if (threadIdx.x == 0) *cnt = 0;
+        __syncthreads();
+        for (int t = threadIdx.x; t < fsize; t += blockDim.x) {
+            int i = cur[t];
+            const double fi = f[i];
+            for (int s = 0; s < nnb[i]; s++) {
+                int c = nbr[(size_t)s * n + i];
+                if (c < 0 || pit[c] < 0 || !(f[c] >= fi)) continue;
+                if (atomicCAS(&pdir[c], -1, d + 1) == -1) nxt[agg_append(cnt)] = c;
+            }
+        }
+        __threadfence_block();
+        __syncthreads();
+        if (threadIdx.x == 0) s_size = *(volatile int*)cnt;
+        __syncthreads();
+        fsize = s_size;
+        int* tmp = cur; cur = nxt; nxt = tmp;
+        d++;
+        levels++;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *levels_out = levels;
 }
 
 __global__ void k_flat_dirs(int n, const double* __restrict__ f, const int* __restrict__ pit,
@@ -642,7 +689,8 @@ int fill_elevation(gs_plan* p, const double* h, double sealevel, double ofill, d
     int fsize = hbuf[0], d = 1, levels = 0;
     int* fa = p->front0;
     int* fb = p->front1;
-    while (fsize > 0) {
+    // wide frontiers: one launch per level; narrow ones: the rest in one block
+    while (fsize > 4096) {
         GS_CUDA(cudaMemsetAsync(p->i_scalar + I_NEXT, 0, sizeof(int), p->stream));
         launch(p, k_bfs_step, grid_for(fsize, B), B, fsize, (const int*)fa, d, n, (const double*)lfill,
                (const int*)pit_ids, (const int*)p->nbr, (const int8_t*)p->nnb, p->pdir, fb,
@@ -654,6 +702,13 @@ int fill_elevation(gs_plan* p, const double* h, double sealevel, double ofill, d
         d++;
         levels++;
         if (levels > n + 1) { set_error(GS_EMAXITER, "pit fill: flat BFS did not terminate"); return GS_EMAXITER; }
+    }
+    if (fsize > 0) {
+        launch(p, k_bfs_block, 1, 1024, fsize, fa, fb, p->i_scalar + I_NEXT, d, n, (const double*)lfill,
+               (const int*)pit_ids, (const int*)p->nbr, (const int8_t*)p->nnb, p->pdir, p->i_scalar + 4);
+        GS_LAUNCH();
+        GS_TRY(read_ints(p, hbuf, p->i_scalar + 4, 1));
+        levels += hbuf[0];
     }
     if (st) st->flat_rounds = levels;
     launch(p, k_flat_dirs, G, B, n, (const double*)lfill, (const int*)pit_ids, (const int*)p->pdir,

@@ -32,7 +32,7 @@ static void plan_free(gs_plan* p) {
     void* ptrs[] = {p->nbr, p->elen, p->vdist, p->rev, p->sorder, p->nnb, p->farea, p->larea, p->outlet,
                     p->outlet_ids, p->open_ids, p->open_mask, p->gid, p->rcv, p->dist, p->wgt, p->rslot,
                     p->rslot_i, p->lsink, p->sea, p->don_mask, p->don_k, p->cnt, p->queue, p->ctr,
-                    p->done_flag, p->q, p->q2, p->q3, p->c, p->ledge, p->parent, p->basinL, p->xe_u,
+                    p->done_flag, p->q, p->q2, p->q3, p->order, p->order2, p->pos, p->order_i, p->okey, p->okey2, p->ok32, p->ok32b, p->oval, p->oval2, p->c, p->ledge, p->parent, p->basinL, p->xe_u,
                     p->xe_v, p->xe_w, p->comp, p->minseed, p->lab, p->flagbuf, p->scanbuf, p->pdir,
                     p->front0, p->front1, p->spill_flag, p->bestlid, p->d_scalar, p->i_scalar,
                     p->u_scalar, p->pit_params, p->pit_info, p->filled_lvl, p->filled_vol, p->pit_vol,
@@ -159,6 +159,16 @@ int plan_create(int64_t nb, const int32_t* nnb, const int32_t* ngb, const double
         TRYP(dalloc(&p->q, N));
         TRYP(dalloc(&p->q2, N));
         TRYP(dalloc(&p->q3, N));
+        TRYP(dalloc(&p->order, N));
+        TRYP(dalloc(&p->order_i, N));
+        TRYP(dalloc(&p->okey, N));
+        TRYP(dalloc(&p->okey2, N));
+        TRYP(dalloc(&p->ok32, N));
+        TRYP(dalloc(&p->ok32b, N));
+        TRYP(dalloc(&p->oval, N));
+        TRYP(dalloc(&p->oval2, N));
+        TRYP(dalloc(&p->order2, N));
+        TRYP(dalloc(&p->pos, N));
         TRYP(dalloc(&p->ledge, N));
         TRYP(dalloc(&p->parent, N));
         TRYP(dalloc(&p->basinL, N));
@@ -210,6 +220,11 @@ int plan_create(int64_t nb, const int32_t* nnb, const int32_t* ngb, const double
         size_t b1 = 0, b2 = 0;
         cub::DeviceRadixSort::SortPairs((void*)nullptr, b1, (const int*)nullptr, (int*)nullptr,
                                         (const int*)nullptr, (int*)nullptr, (int)N1, 0, 32);
+        size_t b3 = 0;
+        cub::DeviceRadixSort::SortPairs((void*)nullptr, b3, (const unsigned long long*)nullptr,
+                                        (unsigned long long*)nullptr, (const int*)nullptr, (int*)nullptr, (int)N1,
+                                        0, 64);
+        b1 = std::max(b1, b3);
         cub::DeviceScan::ExclusiveSum((void*)nullptr, b2, (const int*)nullptr, (int*)nullptr, (int)N1 + 1);
         p->cub_bytes = std::max(b1, b2) + 256;
         TRYP(dalloc((char**)&p->cub_tmp, p->cub_bytes));

@@ -1,5 +1,7 @@
 // Plan (mesh + workspaces) shared by all hot-path stages.
 #pragma once
+#include <vector>
+
 #include "gs_common.cuh"
 
 struct gs_plan {
@@ -48,6 +50,17 @@ struct gs_plan {
     double* q = nullptr;                 // sweep values
     double* q2 = nullptr;
     double* q3 = nullptr;
+    int* order = nullptr;                // topological order of the last flow sweep
+    int* order_i = nullptr;              // order of the snapshot (unfilled) flow graph
+    int order_i_valid = 0;
+    unsigned long long* okey = nullptr;
+    unsigned long long* okey2 = nullptr;
+    unsigned* ok32 = nullptr;
+    unsigned* ok32b = nullptr;
+    int* oval = nullptr;
+    int* oval2 = nullptr;
+    int* order2 = nullptr;
+    int* pos = nullptr;
     double* c = nullptr;                 // SPL coefficients [R][n]
 
     // pit filling
@@ -111,6 +124,12 @@ struct gs_plan {
     double* cg_x = nullptr;
     double* cg_b = nullptr;
     double* red = nullptr;               // reduction scratch
+
+    // optional per-kernel timing (CUDA events around launches)
+    int profiling = 0;
+    std::vector<const void*> prof_fn;
+    std::vector<cudaEvent_t> prof_ev;    // start/stop pairs
+    std::vector<int> prof_idx;           // kernel index per pair
 };
 
 namespace gs {
@@ -122,9 +141,10 @@ int flow_direction(gs_plan* p, const double* h, bool down, const double* lfill,
                    const int* pit_ids, const int* flat_dirs, double sealevel, int* rcv,
                    double* dist, double* wgt, int8_t* rslot, uint8_t* lsink, uint8_t* sea);
 int flow_solve(gs_plan* p, const int* rcv, const double* wgt, const int8_t* rslot,
-               const double* b, double* x, int* cycle_nodes);
+               const double* b, double* x, int* cycle_nodes, const double* surface, const int* pdir,
+               int* order);
 int spl_sweep(gs_plan* p, const int* rcv, const double* c, const int8_t* rslot, const double* hold,
-              double* s, int* cycle_nodes);
+              double* s, int* cycle_nodes, bool reuse_order);
 int fill_elevation(gs_plan* p, const double* h, double sealevel, double ofill, double* lfill,
                    int* pit_ids, int* flat_dirs, gs_stats* st);
 int group_sum_by_pit(gs_plan* p, const int* pit_ids, const uint8_t* mask, const double* vals,
@@ -142,9 +162,14 @@ int hillslope(gs_plan* p, double* h, double* cum_ed, double* eb, double sealevel
 int apply_forces(gs_plan* p, double* h, const double* rain, const double* upsub, double dt,
                  double sealevel, double* bl);
 
+void prof_begin(gs_plan* p, const void* fn, cudaEvent_t* stop);
+
 template <class K, class... A>
 inline void launch(gs_plan* p, K kernel, int grid, int block, A... args) {
+    cudaEvent_t stop = nullptr;
+    if (p->profiling) prof_begin(p, (const void*)kernel, &stop);
     kernel<<<grid, block, 0, p->stream>>>(args...);
+    if (stop) cudaEventRecord(stop, p->stream);
     p->launches++;
 }
 

@@ -75,7 +75,7 @@ int erodep_spl(gs_plan* p, double* h, double* cum_ed, double* eb, const double* 
            rcv_i, dist_i, wgt_i, sea, p->c);
     GS_LAUNCH();
     int cyc = 0;
-    GS_TRY(spl_sweep(p, rcv_i, p->c, p->rslot_i, hold, p->q3, &cyc));
+    GS_TRY(spl_sweep(p, rcv_i, p->c, p->rslot_i, hold, p->q3, &cyc, true));
     launch(p, k_spl_update, G, B, n, p->flat, (const uint8_t*)p->outlet, lsink, (const double*)hold,
            (const double*)p->q3, dt, h, cum_ed, eb);
     GS_LAUNCH();

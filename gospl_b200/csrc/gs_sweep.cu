@@ -17,6 +17,7 @@
 // (a cycle) is detected by quiescence (all published vertices processed, queue
 // not full) and reported as GS_ECYCLE, a wall-clock budget backs it up.
 #include <cooperative_groups.h>
+#include <cub/cub.cuh>
 
 #include <cstring>
 
@@ -26,7 +27,7 @@ namespace cg = cooperative_groups;
 
 namespace gs {
 
-enum { C_HEAD = 0, C_TAIL = 1, C_DONE = 2, C_STATUS = 3 };
+enum { C_HEAD = 0, C_TAIL = 1, C_DONE = 2, C_STATUS = 3, C_NSRC = 4 };
 
 __device__ __forceinline__ unsigned agg_add(unsigned* ctr, unsigned v) {
     cg::coalesced_group g = cg::coalesced_threads();
@@ -86,6 +87,32 @@ struct FlowOp {
             if (r != i && wgt[(size_t)k * n + i] != 0.0) sc.dec(r);
         }
     }
+    // block-sweep form: compute, then hand each ready successor to `emit`
+    __device__ __forceinline__ void compute(int i) const {
+        uint32_t m = mask[i];
+        unsigned long long kk = dk[i];
+        unsigned long long ord = sorder[i];
+        double s = b[i];
+        for (int q = 0; q < MAXW && m; q++) {
+            int t = (int)(ord & 15ULL);
+            ord >>= 4;
+            if (!(m & (1u << t))) continue;
+            m &= ~(1u << t);
+            int j = nbr[(size_t)t * n + i];
+            int k = (int)((kk >> (4 * t)) & 15ULL);
+            s = s + wgt[(size_t)k * n + j] * x[j];
+        }
+        x[i] = s;
+        done[i] = 1;
+    }
+    template <class Emit>
+    __device__ __forceinline__ void successors(int i, int* cnt, Emit emit) const {
+        for (int k = 0; k < R; k++) {
+            int r = rcv[(size_t)k * n + i];
+            if (r != i && wgt[(size_t)k * n + i] != 0.0)
+                if (atomicSub(&cnt[r], 1) == 1) emit(r);
+        }
+    }
 };
 
 // ---------------------------------------------------------------------------
@@ -118,38 +145,85 @@ struct SplOp {
             sc.dec(nbr[(size_t)t * n + i]);
         }
     }
+    __device__ __forceinline__ void compute(int i) const {
+        double num = hold[i], den = 1.0;
+        for (int k = 0; k < R; k++) {
+            double ck = c[(size_t)k * n + i];
+            int r = rcv[(size_t)k * n + i];
+            if (r != i && ck != 0.0) num = num + ck * x[r];
+            den = den + ck;
+        }
+        x[i] = num / den;
+        done[i] = 1;
+    }
+    template <class Emit>
+    __device__ __forceinline__ void successors(int i, int* cnt, Emit emit) const {
+        uint32_t m = mask[i];
+        while (m) {
+            int t = __ffs(m) - 1;
+            m &= m - 1;
+            int j = nbr[(size_t)t * n + i];
+            if (atomicSub(&cnt[j], 1) == 1) emit(j);
+        }
+    }
 };
 
+// Warp-cooperative dataflow loop.  Each warp takes 32 consecutive tickets,
+// polls all pending slots with one ballot per round and processes the lanes
+// whose vertices are ready at once; lanes never sleep individually, so a ready
+// vertex is never held behind a sibling lane's wait.  A warp refills only when
+// all its 32 tickets are done.
 template <class Op>
-__global__ void k_dataflow(Op op, Sched sc, int n, unsigned long long budget_ns) {
+__global__ void k_dataflow(Op op, Sched sc, int n_all, unsigned long long budget_ns) {
     const unsigned long long t0 = globaltimer_ns();
+    const int lane = threadIdx.x & 31;
+    const unsigned full = 0xffffffffu;
+    const int n = n_all - (int)sc.ctr[C_NSRC];   // vertices that go through the queue
     for (;;) {
-        unsigned t = agg_add(&sc.ctr[C_HEAD], 1u);
-        if (t >= (unsigned)n) return;
-        int node;
-        unsigned spins = 0, nap = 32;
-        for (;;) {
-            node = ld_acquire(&sc.queue[t]);
-            if (node >= 0) break;
-            if ((++spins & 15u) == 0) {
-                if (ld_relaxed_u32(&sc.ctr[C_STATUS]) != 0) return;
-                unsigned d = ld_relaxed_u32(&sc.ctr[C_DONE]);
-                unsigned tl = ld_relaxed_u32(&sc.ctr[C_TAIL]);
-                if (d == tl && tl <= t) {
-                    atomicCAS(&sc.ctr[C_STATUS], 0u, (unsigned)GS_ECYCLE);
-                    return;
-                }
-                if (globaltimer_ns() - t0 > budget_ns) {
-                    atomicCAS(&sc.ctr[C_STATUS], 0u, (unsigned)GS_ETIMEOUT);
-                    return;
-                }
+        unsigned base = 0;
+        if (lane == 0) base = atomicAdd(&sc.ctr[C_HEAD], 32u);
+        base = __shfl_sync(full, base, 0);
+        if (base >= (unsigned)n) return;
+        const unsigned t = base + lane;
+        unsigned pending = __ballot_sync(full, t < (unsigned)n);
+        unsigned rounds = 0, nap = 0;
+        while (pending) {
+            int node = -1;
+            if (pending & (1u << lane)) node = ld_relaxed_s32(&sc.queue[t]);
+            unsigned ready = __ballot_sync(full, node >= 0) & pending;
+            if (ready) {
+                __threadfence();   // acquire: predecessors' values are visible
+                if (ready & (1u << lane)) op.process(node, sc);
+                __syncwarp();
+                __threadfence();
+                if (lane == 0) atomicAdd(&sc.ctr[C_DONE], (unsigned)__popc(ready));
+                pending &= ~ready;
+                nap = 0;
+                continue;
             }
+            // nothing ready: back off, watch for abort, quiescence and time budget
+            if ((++rounds & 31u) == 0) {
+                int stop = 0;
+                if (lane == 0) {
+                    if (ld_relaxed_u32(&sc.ctr[C_STATUS]) != 0) stop = 1;
+                    unsigned d = 0, tl = 0;
+                    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(d) : "l"(&sc.ctr[C_DONE]) : "memory");
+                    tl = ld_relaxed_u32(&sc.ctr[C_TAIL]);
+                    unsigned first = base + (__ffs(pending) - 1);
+                    if (!stop && d == tl && tl <= first) {
+                        atomicCAS(&sc.ctr[C_STATUS], 0u, (unsigned)GS_ECYCLE);
+                        stop = 1;
+                    }
+                    if (!stop && globaltimer_ns() - t0 > budget_ns) {
+                        atomicCAS(&sc.ctr[C_STATUS], 0u, (unsigned)GS_ETIMEOUT);
+                        stop = 1;
+                    }
+                }
+                if (__shfl_sync(full, stop, 0)) return;
+            }
+            if (nap < 256) nap += 32;
             __nanosleep(nap);
-            if (nap < 1024) nap <<= 1;
         }
-        op.process(node, sc);
-        __threadfence();
-        agg_add(&sc.ctr[C_DONE], 1u);
     }
 }
 
@@ -192,21 +266,30 @@ __global__ void k_spl_donors(int n, int R, const int* __restrict__ rcv, const do
     cnt[j] = own;
 }
 
+// vertices without predecessors are marked (done = 2) and counted; they are
+// computed by k_sources in one parallel pass, the rest by k_dataflow
 __global__ void k_flow_setup(int n, const uint32_t* __restrict__ mask, int* cnt, Sched sc,
                              uint8_t* done) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     int c = __popc(mask[i]);
     cnt[i] = c;
-    done[i] = 0;
-    if (c == 0) sc.publish(i);
+    done[i] = c == 0 ? 2 : 0;
+    if (c == 0) agg_add(&sc.ctr[C_NSRC], 1u);
 }
 
 __global__ void k_spl_setup(int n, const int* __restrict__ cnt, Sched sc, uint8_t* done) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    done[i] = 0;
-    if (cnt[i] == 0) sc.publish(i);
+    done[i] = cnt[i] == 0 ? 2 : 0;
+    if (cnt[i] == 0) agg_add(&sc.ctr[C_NSRC], 1u);
+}
+
+template <class Op>
+__global__ void k_sources(Op op, Sched sc, int n, const uint8_t* __restrict__ mark) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    if (mark[i] == 2) op.process(i, sc);
 }
 
 // Jacobi iteration for the vertices a flow sweep could not order (cycle
@@ -238,25 +321,25 @@ __global__ void k_flow_jacobi(int n, const int* __restrict__ nbr, const uint32_t
 }
 
 static int sweep_status(gs_plan* p, int* status_out) {
-    unsigned h[4];
+    unsigned h[8];
     GS_CUDA(cudaMemcpyAsync(h, p->ctr, sizeof(h), cudaMemcpyDeviceToHost, p->stream));
     GS_CUDA(cudaStreamSynchronize(p->stream));
     *status_out = (int)h[C_STATUS];
-    if (*status_out == 0 && h[C_DONE] != (unsigned)p->n) *status_out = GS_ECYCLE;
+    if (*status_out == 0 && h[C_DONE] + h[C_NSRC] != (unsigned)p->n) *status_out = GS_ECYCLE;
     return GS_OK;
 }
 
 static const unsigned long long SWEEP_BUDGET_NS = 4000000000ULL;   // 4 s
 
-int flow_solve(gs_plan* p, const int* rcv, const double* wgt, const int8_t* rslot,
-               const double* b, double* x, int* cycle_nodes) {
+int flow_solve_counted(gs_plan* p, const int* rcv, const double* wgt, const int8_t* rslot,
+                       const double* b, double* x, int* cycle_nodes) {
     const int n = (int)p->n;
     *cycle_nodes = 0;
     if (n == 0) return GS_OK;
     GS_CUDA(cudaMemsetAsync(p->don_mask, 0, sizeof(uint32_t) * n, p->stream));
     GS_CUDA(cudaMemsetAsync(p->don_k, 0, sizeof(unsigned long long) * n, p->stream));
     GS_CUDA(cudaMemsetAsync(p->queue, 0xff, sizeof(int) * n, p->stream));
-    GS_CUDA(cudaMemsetAsync(p->ctr, 0, sizeof(unsigned) * 4, p->stream));
+    GS_CUDA(cudaMemsetAsync(p->ctr, 0, sizeof(unsigned) * 8, p->stream));
     launch(p, k_flow_donors, grid_for(n, 256), 256, n, p->R, rcv, wgt, rslot,
            (const int8_t*)p->rev, p->don_mask, p->don_k);
     GS_LAUNCH();
@@ -265,7 +348,8 @@ int flow_solve(gs_plan* p, const int* rcv, const double* wgt, const int8_t* rslo
            p->done_flag);
     GS_LAUNCH();
     FlowOp op{n, p->R, p->nbr, p->don_mask, p->don_k, p->sorder, wgt, rcv, b, x, p->done_flag};
-    launch(p, k_dataflow<FlowOp>, p->sm_count * 8, 256, op, sc, n, SWEEP_BUDGET_NS);
+    launch(p, k_sources<FlowOp>, grid_for(n, 256), 256, op, sc, n, (const uint8_t*)p->done_flag);
+    launch(p, k_dataflow<FlowOp>, p->sm_count * 4, 128, op, sc, n, SWEEP_BUDGET_NS);
     GS_LAUNCH();
     int st = 0;
     GS_TRY(sweep_status(p, &st));
@@ -300,10 +384,10 @@ int flow_solve(gs_plan* p, const int* rcv, const double* wgt, const int8_t* rslo
         if (hmd == 0 || d < 1e-15) converged = 1;
     }
     if (xa != x) GS_CUDA(cudaMemcpyAsync(x, xa, sizeof(double) * n, cudaMemcpyDeviceToDevice, p->stream));
-    unsigned h[4];
+    unsigned h[8];
     GS_CUDA(cudaMemcpyAsync(h, p->ctr, sizeof(h), cudaMemcpyDeviceToHost, p->stream));
     GS_CUDA(cudaStreamSynchronize(p->stream));
-    *cycle_nodes = n - (int)h[C_DONE];
+    *cycle_nodes = n - (int)h[C_DONE] - (int)h[C_NSRC];
     if (!converged) {
         set_error(GS_EMAXITER, "flow cycle fallback did not converge");
         return GS_EMAXITER;
@@ -311,14 +395,14 @@ int flow_solve(gs_plan* p, const int* rcv, const double* wgt, const int8_t* rslo
     return GS_OK;
 }
 
-int spl_sweep(gs_plan* p, const int* rcv, const double* c, const int8_t* rslot,
-              const double* hold, double* s, int* cycle_nodes) {
+int spl_sweep_counted(gs_plan* p, const int* rcv, const double* c, const int8_t* rslot,
+                      const double* hold, double* s, int* cycle_nodes) {
     const int n = (int)p->n;
     *cycle_nodes = 0;
     if (n == 0) return GS_OK;
     GS_CUDA(cudaMemsetAsync(p->don_mask, 0, sizeof(uint32_t) * n, p->stream));
     GS_CUDA(cudaMemsetAsync(p->queue, 0xff, sizeof(int) * n, p->stream));
-    GS_CUDA(cudaMemsetAsync(p->ctr, 0, sizeof(unsigned) * 4, p->stream));
+    GS_CUDA(cudaMemsetAsync(p->ctr, 0, sizeof(unsigned) * 8, p->stream));
     launch(p, k_spl_donors, grid_for(n, 256), 256, n, p->R, rcv, c, rslot, (const int8_t*)p->rev,
            p->don_mask, p->cnt);
     GS_LAUNCH();
@@ -326,16 +410,314 @@ int spl_sweep(gs_plan* p, const int* rcv, const double* c, const int8_t* rslot,
     launch(p, k_spl_setup, grid_for(n, 256), 256, n, (const int*)p->cnt, sc, p->done_flag);
     GS_LAUNCH();
     SplOp op{n, p->R, p->nbr, p->don_mask, rcv, c, hold, s, p->done_flag};
-    launch(p, k_dataflow<SplOp>, p->sm_count * 8, 256, op, sc, n, SWEEP_BUDGET_NS);
+    launch(p, k_sources<SplOp>, grid_for(n, 256), 256, op, sc, n, (const uint8_t*)p->done_flag);
+    launch(p, k_dataflow<SplOp>, p->sm_count * 4, 128, op, sc, n, SWEEP_BUDGET_NS);
     GS_LAUNCH();
     int st = 0;
     GS_TRY(sweep_status(p, &st));
     if (st != 0) {
-        unsigned h[4];
+        unsigned h[8];
         GS_CUDA(cudaMemcpyAsync(h, p->ctr, sizeof(h), cudaMemcpyDeviceToHost, p->stream));
         GS_CUDA(cudaStreamSynchronize(p->stream));
-        *cycle_nodes = n - (int)h[C_DONE];
+        *cycle_nodes = n - (int)h[C_DONE] - (int)h[C_NSRC];
         set_error(st, "SPL sweep: receiver graph is not acyclic");
+        return st;
+    }
+    return GS_OK;
+}
+
+
+// ===========================================================================
+// Ordered sweeps.  A static topological order (elevation order) is given;
+// tickets are handed out in that order and each vertex polls the values of
+// its predecessors directly: unsolved values hold a sentinel NaN pattern and
+// an aligned 64-bit store is single-copy atomic, so a value that is not the
+// sentinel is final.  Per dependency hop the critical path is one store and
+// one load through L2, with no atomics or fences.  Lanes of a warp wait
+// together (one ballot per polling round) and each ready lane proceeds at
+// once.  Predecessors always precede in the order (checked before the sweep),
+// so the smallest unfinished ticket is always computable: no deadlock.
+// ===========================================================================
+constexpr unsigned long long SENT = 0x7ff4dead0badf00dULL;
+
+__device__ __forceinline__ double ld_val(const double* p) {
+    unsigned long long v;
+    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return __longlong_as_double((long long)v);
+}
+__device__ __forceinline__ bool is_sent(double v) {
+    return (unsigned long long)__double_as_longlong(v) == SENT;
+}
+__device__ __forceinline__ void st_val(double* p, double v) {
+    asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"((unsigned long long)__double_as_longlong(v)) : "memory");
+}
+
+__global__ void k_gather_u64(int n, const unsigned long long* __restrict__ a, const int* __restrict__ idx,
+                             unsigned long long* out) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = a[idx[i]];
+}
+
+__global__ void k_reverse(int n, const int* __restrict__ a, int* out) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = a[n - 1 - i];
+}
+
+__global__ void k_fill_sent(int n, double* x) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) x[i] = __longlong_as_double((long long)SENT);
+}
+
+// order keys: descending surface (flow direction), ties by descending flat distance
+__global__ void k_order_keys(int n, const double* __restrict__ z, const int* __restrict__ pdir,
+                             unsigned long long* key, unsigned* key2, int* val) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    key[i] = ~dkey(z[i]);
+    key2[i] = pdir ? ~(unsigned)(pdir[i] + 1) : 0u;
+    val[i] = i;
+}
+
+__global__ void k_positions(int n, const int* __restrict__ order, int* pos) {
+    int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p < n) pos[order[p]] = p;
+}
+
+// every flow edge j -> r (w != 0, r != j) must have pos[j] < pos[r]
+__global__ void k_check_order(int n, int R, const int* __restrict__ rcv, const double* __restrict__ w,
+                              const int* __restrict__ pos, int* bad) {
+    int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    for (int k = 0; k < R; k++) {
+        int r = rcv[(size_t)k * n + j];
+        if (r != j && w[(size_t)k * n + j] != 0.0 && pos[j] >= pos[r]) { *bad = 1; return; }
+    }
+}
+
+struct FlowOrd {
+    int n;
+    const int* nbr;
+    const uint32_t* mask;
+    const unsigned long long* dk;
+    const unsigned long long* sorder;
+    const double* wgt;
+    const double* b;
+    double* x;
+    static constexpr int MAXP = MAXW;
+    // gather the predecessors (donors, ascending id) and their weights
+    __device__ __forceinline__ int prep(int i, int* pj, double* pw) const {
+        uint32_t m = mask[i];
+        unsigned long long kk = dk[i], ord = sorder[i];
+        int np = 0;
+        for (int q = 0; q < MAXW && m; q++) {
+            int t = (int)(ord & 15ULL);
+            ord >>= 4;
+            if (!(m & (1u << t))) continue;
+            m &= ~(1u << t);
+            int j = nbr[(size_t)t * n + i];
+            int k = (int)((kk >> (4 * t)) & 15ULL);
+            pj[np] = j;
+            pw[np] = wgt[(size_t)k * n + j];
+            np++;
+        }
+        return np;
+    }
+    __device__ __forceinline__ double init(int i) const { return b[i]; }
+    __device__ __forceinline__ double combine(double s, double w, double xj) const { return s + w * xj; }
+    __device__ __forceinline__ double finish(int, double s, double) const { return s; }
+};
+
+struct SplOrd {
+    int n, R;
+    const int* rcv;
+    const double* c;
+    const double* hold;
+    double* x;
+    static constexpr int MAXP = MAXR;
+    __device__ __forceinline__ int prep(int i, int* pj, double* pw) const {
+        int np = 0;
+        for (int k = 0; k < R; k++) {
+            double ck = c[(size_t)k * n + i];
+            int r = rcv[(size_t)k * n + i];
+            if (r != i && ck != 0.0) { pj[np] = r; pw[np] = ck; np++; }
+        }
+        return np;
+    }
+    __device__ __forceinline__ double init(int i) const { return hold[i]; }
+    __device__ __forceinline__ double combine(double s, double w, double xj) const { return s + w * xj; }
+    __device__ __forceinline__ double finish(int i, double num, double) const {
+        double den = 1.0;
+        for (int k = 0; k < R; k++) den = den + c[(size_t)k * n + i];
+        return num / den;
+    }
+};
+
+template <class Op>
+__global__ void __launch_bounds__(128) k_ordered(Op op, int n, const int* __restrict__ order, unsigned* ctr,
+                                                 unsigned long long budget_ns) {
+    const unsigned long long t0 = globaltimer_ns();
+    const int lane = threadIdx.x & 31;
+    const unsigned full = 0xffffffffu;
+    int pj[Op::MAXP];
+    double pw[Op::MAXP];
+    for (;;) {
+        unsigned base = 0;
+        if (lane == 0) base = atomicAdd(&ctr[C_HEAD], 32u);
+        base = __shfl_sync(full, base, 0);
+        if (base >= (unsigned)n) return;
+        const unsigned t = base + lane;
+        int node = -1, np = 0;
+        if (t < (unsigned)n) {
+            node = order[t];
+            np = op.prep(node, pj, pw);
+        }
+        unsigned pending = __ballot_sync(full, node >= 0);
+        unsigned rounds = 0, nap = 0;
+        while (pending) {
+            bool rdy = false;
+            double acc = 0.0;
+            if (pending & (1u << lane)) {
+                rdy = true;
+                acc = op.init(node);
+                for (int q = 0; q < np; q++) {
+                    double v = ld_val(&op.x[pj[q]]);
+                    if (is_sent(v)) { rdy = false; break; }
+                    acc = op.combine(acc, pw[q], v);
+                }
+                if (rdy) st_val(&op.x[node], op.finish(node, acc, 0.0));
+            }
+            unsigned done = __ballot_sync(full, rdy);
+            pending &= ~done;
+            if (done) { nap = 0; continue; }
+            if ((++rounds & 63u) == 0) {
+                int stop = 0;
+                if (lane == 0) {
+                    if (ld_relaxed_u32(&ctr[C_STATUS]) != 0) stop = 1;
+                    else if (globaltimer_ns() - t0 > budget_ns) {
+                        atomicCAS(&ctr[C_STATUS], 0u, (unsigned)GS_ETIMEOUT);
+                        stop = 1;
+                    }
+                }
+                if (__shfl_sync(full, stop, 0)) return;
+            }
+            if (nap < 128) nap += 16;
+            __nanosleep(nap);
+        }
+    }
+}
+
+// sort vertices by (surface desc, flat distance desc); returns 1 when the
+// order is topological for the given flow edges
+static int build_order(gs_plan* p, const double* z, const int* pdir, const int* rcv, const double* w,
+                       int* order, int* ok) {
+    const int n = (int)p->n;
+    const int B = 256, G = grid_for(n, B);
+    unsigned long long* key = p->okey;
+    unsigned long long* key_out = p->okey2;
+    unsigned* key2 = p->ok32;
+    unsigned* key2_out = p->ok32b;
+    int* val = p->oval;
+    int* val2 = p->oval2;
+    launch(p, k_order_keys, G, B, n, z, pdir, key, key2, val);
+    GS_LAUNCH();
+    size_t bytes = p->cub_bytes;
+    if (pdir) {
+        GS_CUDA(cub::DeviceRadixSort::SortPairs(p->cub_tmp, bytes, key2, key2_out, val, val2, n, 0, 32, p->stream));
+        p->launches++;
+        // gather primary keys in the new order
+        launch(p, k_gather_u64, G, B, n, (const unsigned long long*)key, (const int*)val2, key_out);
+        GS_CUDA(cub::DeviceRadixSort::SortPairs(p->cub_tmp, bytes, key_out, key, val2, order, n, 0, 64,
+                                                p->stream));
+    } else {
+        GS_CUDA(cub::DeviceRadixSort::SortPairs(p->cub_tmp, bytes, key, key_out, val, order, n, 0, 64,
+                                                p->stream));
+    }
+    p->launches++;
+    launch(p, k_positions, G, B, n, (const int*)order, p->pos);
+    GS_CUDA(cudaMemsetAsync(p->i_scalar + 14, 0, sizeof(int), p->stream));
+    launch(p, k_check_order, G, B, n, p->R, rcv, w, (const int*)p->pos, p->i_scalar + 14);
+    GS_LAUNCH();
+    int bad = 0;
+    GS_CUDA(cudaMemcpyAsync(&bad, p->i_scalar + 14, sizeof(int), cudaMemcpyDeviceToHost, p->stream));
+    GS_CUDA(cudaStreamSynchronize(p->stream));
+    *ok = bad ? 0 : 1;
+    return GS_OK;
+}
+
+static int ordered_status(gs_plan* p, int* st) {
+    unsigned h[8];
+    GS_CUDA(cudaMemcpyAsync(h, p->ctr, sizeof(h), cudaMemcpyDeviceToHost, p->stream));
+    GS_CUDA(cudaStreamSynchronize(p->stream));
+    *st = (int)h[C_STATUS];
+    return GS_OK;
+}
+
+int flow_solve(gs_plan* p, const int* rcv, const double* wgt, const int8_t* rslot, const double* b, double* x,
+               int* cycle_nodes, const double* surface, const int* pdir, int* order) {
+    const int n = (int)p->n;
+    *cycle_nodes = 0;
+    if (n == 0) return GS_OK;
+    int ok = 0;
+    if (surface) GS_TRY(build_order(p, surface, pdir, rcv, wgt, order, &ok));
+    if (order == p->order_i) p->order_i_valid = ok;
+    if (!ok) return flow_solve_counted(p, rcv, wgt, rslot, b, x, cycle_nodes);
+    GS_CUDA(cudaMemsetAsync(p->don_mask, 0, sizeof(uint32_t) * n, p->stream));
+    GS_CUDA(cudaMemsetAsync(p->don_k, 0, sizeof(unsigned long long) * n, p->stream));
+    GS_CUDA(cudaMemsetAsync(p->ctr, 0, sizeof(unsigned) * 8, p->stream));
+    launch(p, k_flow_donors, grid_for(n, 256), 256, n, p->R, rcv, wgt, rslot, (const int8_t*)p->rev, p->don_mask,
+           p->don_k);
+    launch(p, k_fill_sent, grid_for(n, 256), 256, n, x);
+    FlowOrd op{n, p->nbr, p->don_mask, p->don_k, p->sorder, wgt, b, x};
+    launch(p, k_ordered<FlowOrd>, p->sm_count * 8, 128, op, n, (const int*)order, p->ctr, SWEEP_BUDGET_NS);
+    GS_LAUNCH();
+    int st = 0;
+    GS_TRY(ordered_status(p, &st));
+    if (st != 0) {
+        set_error(st, "ordered flow sweep did not complete");
+        return st;
+    }
+    return GS_OK;
+}
+
+// SPL edges i -> rcv (c != 0) run against the flow order: need pos[rcv] > pos[i]
+__global__ void k_check_spl_order(int n, int R, const int* __restrict__ rcv, const double* __restrict__ c,
+                                  const int* __restrict__ pos, int* bad) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    for (int k = 0; k < R; k++) {
+        int r = rcv[(size_t)k * n + i];
+        if (r != i && c[(size_t)k * n + i] != 0.0 && pos[r] <= pos[i]) { *bad = 1; return; }
+    }
+}
+
+int spl_sweep(gs_plan* p, const int* rcv, const double* c, const int8_t* rslot, const double* hold, double* s,
+              int* cycle_nodes, bool reuse_order) {
+    const int n = (int)p->n;
+    *cycle_nodes = 0;
+    if (n == 0) return GS_OK;
+    int ok = reuse_order && p->order_i_valid;
+    if (ok) {
+        launch(p, k_positions, grid_for(n, 256), 256, n, (const int*)p->order_i, p->pos);
+        GS_CUDA(cudaMemsetAsync(p->i_scalar + 14, 0, sizeof(int), p->stream));
+        launch(p, k_check_spl_order, grid_for(n, 256), 256, n, p->R, rcv, c, (const int*)p->pos, p->i_scalar + 14);
+        GS_LAUNCH();
+        int bad = 0;
+        GS_CUDA(cudaMemcpyAsync(&bad, p->i_scalar + 14, sizeof(int), cudaMemcpyDeviceToHost, p->stream));
+        GS_CUDA(cudaStreamSynchronize(p->stream));
+        ok = !bad;
+    }
+    if (!ok) return spl_sweep_counted(p, rcv, c, rslot, hold, s, cycle_nodes);
+    // the SPL system is solved receivers first: the flow order reversed
+    launch(p, k_reverse, grid_for(n, 256), 256, n, (const int*)p->order_i, p->order2);
+    GS_CUDA(cudaMemsetAsync(p->ctr, 0, sizeof(unsigned) * 8, p->stream));
+    launch(p, k_fill_sent, grid_for(n, 256), 256, n, s);
+    SplOrd op{n, p->R, rcv, c, hold, s};
+    launch(p, k_ordered<SplOrd>, p->sm_count * 8, 128, op, n, (const int*)p->order2, p->ctr, SWEEP_BUDGET_NS);
+    GS_LAUNCH();
+    int st = 0;
+    GS_TRY(ordered_status(p, &st));
+    if (st != 0) {
+        set_error(st, "ordered SPL sweep did not complete");
         return st;
     }
     return GS_OK;

@@ -110,6 +110,10 @@ def _heron(p1, p2, p3):
     return out
 
 
+def _bswap32(x):
+    return np.asarray(x).astype(np.uint32).byteswap().astype(np.uint64)
+
+
 def voronoi(coords, cells):
     """Edges (reference order), cell->edge map, circumcentres, control volumes."""
     cells = np.asarray(cells, dtype=np.int32)
@@ -125,11 +129,15 @@ def voronoi(coords, cells):
     cv = np.zeros(len(coords))
     np.add.at(cv, cells.T, vals)
     a = np.sort(hier.reshape(2, -1).T)
-    b = np.ascontiguousarray(a).view(np.dtype((np.void, a.dtype.itemsize * 2)))
-    ub, inv, cts = np.unique(b, return_inverse=True, return_counts=True)
+    # The reference orders edges with np.unique on a void view of the int32
+    # pairs, i.e. byte-lexicographically (memcmp of the little-endian bytes).
+    # The same order comes from unsigned 64-bit keys of the byte-swapped ids.
+    key = (_bswap32(a[:, 0]) << np.uint64(32)) | _bswap32(a[:, 1])
+    uk, inv, cts = np.unique(key, return_inverse=True, return_counts=True)
     if np.any(cts > 2):
         raise ValueError("an edge is shared by more than two cells")
-    edges = ub.view(a.dtype).reshape(-1, 2)
+    edges = np.stack([_bswap32((uk >> np.uint64(32)).astype(np.uint32)),
+                      _bswap32((uk & np.uint64(0xffffffff)).astype(np.uint32))], axis=1).astype(np.int32)
     X = coords[cells.T]
     alpha = eii * eij
     asum = alpha[0] + alpha[1] + alpha[2]
@@ -201,10 +209,54 @@ def definetin(coords, cells, edges, cells_edges, cc, curved):
     return nnb, ngb, elgt, vdist.reshape(n, 12), farea, narea
 
 
-class FVMesh:
-    """Finite-volume mesh plus boundary sets, in the reference's node order."""
+def definetin_device(coords, cells, edges, cells_edges, cc, curved, device="cuda"):
+    """definetin on the GPU through gs_mesh_geometry (same outputs as definetin)."""
+    import ctypes
+    import torch
+    from . import _lib
 
-    def __init__(self, coords, cells, bc="oooo"):
+    L = _lib.load()
+    n, m, nc = len(coords), len(edges), len(cells)
+    node = np.empty(2 * m, dtype=np.int64)
+    node[0::2], node[1::2] = edges[:, 0], edges[:, 1]
+    eid = np.repeat(np.arange(m, dtype=np.int32), 2)
+    o = np.argsort(node, kind="stable")
+    vedge = eid[o]
+    vptr = np.zeros(n + 1, np.int32)
+    np.cumsum(np.bincount(node, minlength=n), out=vptr[1:])
+    vn = cells.reshape(-1).astype(np.int64)
+    o = np.argsort(vn, kind="stable")
+    vcell = np.repeat(np.arange(nc, dtype=np.int32), 3)[o]
+    cptr = np.zeros(n + 1, np.int32)
+    np.cumsum(np.bincount(vn, minlength=n), out=cptr[1:])
+    dev = torch.device(device)
+    T = lambda a, dt: torch.as_tensor(np.ascontiguousarray(a, dtype=dt), device=dev)
+    xyz, ed, vp, ve, ce, ccd, cp, vc = (T(coords, np.float64), T(edges, np.int32), T(vptr, np.int32),
+                                        T(vedge, np.int32), T(cells_edges, np.int32), T(cc, np.float64),
+                                        T(cptr, np.int32), T(vcell, np.int32))
+    nnb = torch.empty(n, dtype=torch.int32, device=dev)
+    ngb = torch.empty((n, 12), dtype=torch.int32, device=dev)
+    elgt = torch.empty((n, 12), dtype=torch.float64, device=dev)
+    vdist = torch.empty((n, 12), dtype=torch.float64, device=dev)
+    farea = torch.empty(n, dtype=torch.float64, device=dev)
+    narea = torch.empty(n, dtype=torch.float64, device=dev)
+    stream = ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
+    _lib.check(L.gs_mesh_geometry(n, _lib.ptr(xyz), m, _lib.ptr(ed), _lib.ptr(vp), _lib.ptr(ve), nc,
+                                  _lib.ptr(ce), _lib.ptr(ccd), _lib.ptr(cp), _lib.ptr(vc), int(curved),
+                                  _lib.ptr(nnb), _lib.ptr(ngb), _lib.ptr(elgt), _lib.ptr(vdist),
+                                  _lib.ptr(farea), _lib.ptr(narea), stream))
+    torch.cuda.synchronize(dev)
+    return (nnb.cpu().numpy(), ngb.cpu().numpy(), elgt.cpu().numpy(), vdist.cpu().numpy(),
+            farea.cpu().numpy(), narea.cpu().numpy())
+
+
+class FVMesh:
+    """Finite-volume mesh plus boundary sets, in the reference's node order.
+
+    ``device`` selects where the definetin geometry is computed: None (host,
+    numpy) or a CUDA device (gs_mesh_geometry)."""
+
+    def __init__(self, coords, cells, bc="oooo", device=None):
         coords = np.ascontiguousarray(coords, dtype=np.float64)
         cells = np.ascontiguousarray(cells, dtype=np.int32)
         self.coords = coords
@@ -218,7 +270,9 @@ class FVMesh:
         if not self.flat:
             radius = np.linalg.norm(coords[0])
             cc = cc * (radius / np.linalg.norm(cc, axis=1)).reshape((len(cc), 1))
-        (self.nnb, self.ngb, self.elgt, self.vdist, self.farea, narea) = definetin(
+        build = definetin if device is None else (
+            lambda *a, **k: definetin_device(*a, device=device, **k))
+        (self.nnb, self.ngb, self.elgt, self.vdist, self.farea, narea) = build(
             coords, cells, edges, cells_edges, cc, curved=not self.flat)
         larea = narea.copy()
         larea[np.isnan(larea)] = 1.0

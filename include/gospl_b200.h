@@ -68,6 +68,29 @@ int gs_plan_destroy(gs_plan* plan);
 int gs_plan_set_stream(gs_plan* plan, void* cuda_stream);
 /* Number of device kernels this plan launched since creation. */
 int64_t gs_plan_launches(const gs_plan* plan);
+/* Per-kernel timing: when enabled, every launch of the plan is bracketed by
+ * CUDA events on the plan's stream (clears previous records). */
+int gs_plan_profile(gs_plan* plan, int32_t enable);
+/* Writes "kernel_name launches total_ms" lines for the recorded launches into
+ * buf (synchronises the plan's stream); returns the report length. */
+int gs_plan_profile_report(gs_plan* plan, char* buf, int64_t len);
+
+/*
+ * Finite-volume geometry of a triangulated mesh (init-time), replacing the
+ * Fortran `definetin` (fortran/functions.F90:2715-2940) called from
+ * unstructuredmesh.py:164-170.  Inputs (DEVICE): xyz [n][3]; edges [m][2] in
+ * the reference's edge order (meshfunc.py:295-327); vptr/vedge: CSR of each
+ * vertex's edges in edge order; cells_edges [ncell][3]; cc [ncell][3]
+ * circumcentres (projected on the sphere when curved); cptr/vcell: CSR of
+ * each vertex's cells in cell order.  Outputs (DEVICE): nnb [n], ngb
+ * [n][12] (-1 padded), elgt/vdist [n][12], farea [n] (NaN -> 0) and narea
+ * [n] (raw).  `stream` is a cudaStream_t (NULL = default stream).
+ */
+int gs_mesh_geometry(int64_t n, const double* xyz, int64_t m, const int32_t* edges,
+                     const int32_t* vptr, const int32_t* vedge, int64_t ncell,
+                     const int32_t* cells_edges, const double* cc, const int32_t* cptr,
+                     const int32_t* vcell, int32_t curved, int32_t* nnb, int32_t* ngb,
+                     double* elgt, double* vdist, double* farea, double* narea, void* stream);
 
 /*
  * Multiple-flow-direction receivers.  Replaces `mfdreceivers(nRcv, exp, elev,
