@@ -213,7 +213,8 @@ def main():
 
     # ---- per-kernel times (same steps, events around every launch) ----
     L.gs_plan_profile(model._plan, 1)
-    for _ in range(max(1, min(args.steps, 3))):
+    nprof = max(1, min(args.steps, 3))
+    for _ in range(nprof):
         model.step()
     buf = ctypes.create_string_buffer(1 << 16)
     L.gs_plan_profile_report(model._plan, buf, len(buf))
@@ -276,6 +277,7 @@ def main():
                          "unit": "GB/s", "frac": (achieved / hbm) if achieved else None, "traffic": None,
                          "peak_source": src, "launch_ms": per_launch_ms, "launches": cnt},
             "kernel_share": share,
+            "kernel_ms_per_step": sum(v[1] for v in prof.values()) / nprof,
             "gpu_launches": launches,
             "clocks": clocks,
             "cpu_baseline": cpu,

@@ -52,7 +52,8 @@ def build(force=False, verbose=False):
     if failed:
         raise RuntimeError("nvcc failed for %s" % failed)
     tmp = LIB + ".tmp"
-    subprocess.check_call([NVCC, "-shared", "-gencode", "arch=compute_100a,code=sm_100a", "-o", tmp] + objs)
+    subprocess.check_call([NVCC, "-shared", "-gencode", "arch=compute_100a,code=sm_100a", "-Xlinker",
+                           "--no-undefined", "-o", tmp] + objs)
     os.replace(tmp, LIB)
     return LIB
 

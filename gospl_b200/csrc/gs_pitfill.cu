@@ -408,6 +408,266 @@ __global__ void k_bfs_block(int fsize0, int* fa, int* fb, int* cnt, int d0, int 
     if (threadIdx.x == 0) *levels_out = levels;
 }
 
+// BFS successors of every vertex that can be reached (pit cells, spill
+// nodes): neighbours c with pit(c) > -1 and lFill(c) >= lFill(i), row-major
+__global__ void k_bfs_adj(int n, int W, const double* __restrict__ f, const int* __restrict__ pit,
+                          const int* __restrict__ spill_flag, const int* __restrict__ nbr,
+                          const int8_t* __restrict__ nnb, int* adj, int8_t* adjn) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int k = 0;
+    if (pit[i] > -1 || spill_flag[i]) {
+        const double fi = f[i];
+        for (int s = 0; s < nnb[i]; s++) {
+            int c = nbr[(size_t)s * n + i];
+            if (c < 0 || pit[c] < 0 || !(f[c] >= fi)) continue;
+            adj[(size_t)i * W + k++] = c;
+        }
+    }
+    adjn[i] = (int8_t)k;
+}
+
+constexpr int BFS_CAP = 5120;
+
+// remaining BFS levels in one block; frontiers in shared memory while they
+// fit, mirrored to global arrays for the wider levels
+__global__ void __launch_bounds__(1024) k_bfs_block2(int fsize0, int* init, int* gA, int d0,
+                                                     int n, int W, const int* __restrict__ adj,
+                                                     const int8_t* __restrict__ adjn, int* pdir,
+                                                     int* levels_out) {
+    __shared__ int sA[BFS_CAP], sB[BFS_CAP];
+    __shared__ int s_next;
+    const int tid = threadIdx.x, nt = blockDim.x;
+    int size = fsize0, d = d0, levels = 0;
+    int* curG = init;
+    int* nxtG = gA;
+    bool cur_sh = false;
+    int* curS = sA;
+    int* nxtS = sB;
+    while (size > 0 && levels <= n) {
+        if (tid == 0) s_next = 0;
+        __syncthreads();
+        for (int t = tid; t < size; t += nt) {
+            int i = cur_sh ? curS[t] : curG[t];
+            int k = adjn[i];
+            const int* row = adj + (size_t)i * W;
+            for (int q = 0; q < k; q++) {
+                int c = row[q];
+                if (atomicCAS(&pdir[c], -1, d + 1) == -1) {
+                    int pos = atomicAdd(&s_next, 1);
+                    if (pos < BFS_CAP) nxtS[pos] = c;
+                    nxtG[pos] = c;
+                }
+            }
+        }
+        __syncthreads();
+        size = s_next;
+        __syncthreads();
+        if (size <= BFS_CAP) {
+            cur_sh = true;
+            int* t = curS; curS = nxtS; nxtS = t;
+        } else {
+            cur_sh = false;
+        }
+        int* oldcur = curG;
+        curG = nxtG;
+        nxtG = oldcur;
+        d++;
+        levels++;
+    }
+    if (tid == 0) *levels_out = levels;
+}
+
+// BFS over the compacted set of reachable vertices (pit cells and spill
+// nodes, local ids 0..M-1) in one block: the visited set is a shared-memory
+// bitmap and the frontiers live in shared memory, so a level costs one global
+// load of the adjacency rows plus block barriers.
+__global__ void k_bfs_flag(int n, const int* __restrict__ pit, const int* __restrict__ spill_flag, int* flag) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) flag[i] = (pit[i] > -1 || spill_flag[i]) ? 1 : 0;
+}
+
+__global__ void k_bfs_local_build(int n, int S, const double* __restrict__ f, const int* __restrict__ pit,
+                                  const int* __restrict__ flag, const int* __restrict__ lid,
+                                  const int* __restrict__ nbr, const int8_t* __restrict__ nnb,
+                                  const int* __restrict__ spill_flag, int* rows, int* l2g, int* ld,
+                                  int* seeds, int* nseed) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n || !flag[i]) return;
+    const int li = lid[i];
+    l2g[li] = i;
+    ld[li] = -1;
+    const double fi = f[i];
+    int* row = rows + (size_t)li * S;
+    int k = 0;
+    for (int s = 0; s < nnb[i]; s++) {
+        int c = nbr[(size_t)s * n + i];
+        if (c < 0 || pit[c] < 0 || !(f[c] >= fi)) continue;
+        row[1 + k++] = lid[c];
+    }
+    row[0] = k;
+    if (spill_flag[i]) seeds[agg_append(nseed)] = li;
+}
+
+__global__ void k_bfs_local_scatter(int M, const int* __restrict__ l2g, const int* __restrict__ ld, int* pdir) {
+    int li = blockIdx.x * blockDim.x + threadIdx.x;
+    if (li < M && ld[li] > 0) pdir[l2g[li]] = ld[li];
+}
+
+constexpr int LBFS_CAP = 6144;
+
+__global__ void __launch_bounds__(1024) k_bfs_local(int M, int S, const int* __restrict__ rows,
+                                                    const int* __restrict__ seeds, const int* __restrict__ nseed_p,
+                                                    int* gA, int* gB, int* ld, int* levels_out) {
+    extern __shared__ unsigned smem_u[];
+    unsigned* vis = smem_u;                           // ceil(M/32) words
+    const int nw = (M + 31) >> 5;
+    int* fA = (int*)(smem_u + nw);
+    int* fB = fA + LBFS_CAP;
+    __shared__ int s_next;
+    const int tid = threadIdx.x, nt = blockDim.x;
+    for (int w = tid; w < nw; w += nt) vis[w] = 0u;
+    __syncthreads();
+    int size = *nseed_p;
+    // seeds: distance 1
+    for (int t = tid; t < size; t += nt) {
+        int li = seeds[t];
+        atomicOr(&vis[li >> 5], 1u << (li & 31));
+        if (t < LBFS_CAP) fA[t] = li;
+        gA[t] = li;
+    }
+    __syncthreads();
+    int* curS = fA;
+    int* nxtS = fB;
+    int* curG = gA;
+    int* nxtG = gB;
+    bool cur_sh = size <= LBFS_CAP;
+    int d = 1, levels = 0;
+    while (size > 0 && levels <= M) {
+        if (tid == 0) s_next = 0;
+        __syncthreads();
+        for (int t = tid; t < size; t += nt) {
+            int li = cur_sh ? curS[t] : curG[t];
+            const int4* r4 = reinterpret_cast<const int4*>(rows + (size_t)li * S);
+            int row[16];
+            for (int q = 0; q < S / 4; q++) {
+                int4 v = r4[q];
+                row[4 * q] = v.x; row[4 * q + 1] = v.y; row[4 * q + 2] = v.z; row[4 * q + 3] = v.w;
+            }
+            int k = row[0];
+            for (int q = 1; q <= k; q++) {
+                int c = row[q];
+                unsigned bit = 1u << (c & 31);
+                if (vis[c >> 5] & bit) continue;
+                if (atomicOr(&vis[c >> 5], bit) & bit) continue;
+                ld[c] = d + 1;
+                int pos = atomicAdd(&s_next, 1);
+                if (pos < LBFS_CAP) nxtS[pos] = c;
+                nxtG[pos] = c;
+            }
+        }
+        __syncthreads();
+        size = s_next;
+        __syncthreads();
+        cur_sh = size <= LBFS_CAP;
+        int* t1 = curS; curS = nxtS; nxtS = t1;
+        int* t2 = curG; curG = nxtG; nxtG = t2;
+        d++;
+        levels++;
+    }
+    if (tid == 0) *levels_out = levels;
+}
+
+// Whole BFS in one cooperative launch: wide levels use the whole grid with a
+// grid-wide barrier per level; once a level is narrower than one block's
+// worth, block 0 finishes the remaining levels alone with block barriers
+// (the other blocks have left, so no grid barrier is used after that point).
+// sizes[] holds three rotating frontier counters: round r reads sizes[r%3],
+// appends to sizes[(r+1)%3], and sizes[(r+2)%3] is cleared for round r+1.
+__global__ void __launch_bounds__(256) k_bfs_coop(int* fa, int* fb, int* sizes, int d0, int n, int W,
+                                                  const int* __restrict__ adj, const int8_t* __restrict__ adjn,
+                                                  int* pdir, int* levels_out) {
+    cg::grid_group grid = cg::this_grid();
+    int d = d0, levels = 0;
+    int* cur = fa;
+    int* nxt = fb;
+    const int gtid = blockIdx.x * blockDim.x + threadIdx.x, gsz = gridDim.x * blockDim.x;
+    int r = 0;
+    int sz = sizes[0];
+    while (sz > 1024 && levels <= n) {
+        int* cnt = &sizes[(r + 1) % 3];
+        for (int t = gtid; t < sz; t += gsz) {
+            int i = cur[t];
+            int k = adjn[i];
+            const int* row = adj + (size_t)i * W;
+            for (int q = 0; q < k; q++) {
+                int c = row[q];
+                if (atomicCAS(&pdir[c], -1, d + 1) == -1) nxt[agg_append(cnt)] = c;
+            }
+        }
+        if (gtid == 0) sizes[(r + 2) % 3] = 0;
+        grid.sync();
+        sz = *(volatile int*)&sizes[(r + 1) % 3];
+        int* tmp = cur; cur = nxt; nxt = tmp;
+        d++;
+        levels++;
+        r++;
+    }
+    if (blockIdx.x != 0) return;
+    // narrow tail: block 0 only
+    __shared__ int s_cnt;
+    while (sz > 0 && levels <= n) {
+        if (threadIdx.x == 0) s_cnt = 0;
+        __syncthreads();
+        for (int t = threadIdx.x; t < sz; t += blockDim.x) {
+            int i = cur[t];
+            int k = adjn[i];
+            const int* row = adj + (size_t)i * W;
+            for (int q = 0; q < k; q++) {
+                int c = row[q];
+                if (atomicCAS(&pdir[c], -1, d + 1) == -1) nxt[atomicAdd(&s_cnt, 1)] = c;
+            }
+        }
+        __syncthreads();
+        sz = s_cnt;
+        __syncthreads();
+        int* tmp = cur; cur = nxt; nxt = tmp;
+        d++;
+        levels++;
+    }
+    if (threadIdx.x == 0) *levels_out = levels;
+}
+
+// Minimax relaxation over the basin graph in one cooperative launch; rounds
+// end when no basin level changed (three rotating change flags, as above).
+__global__ void __launch_bounds__(256) k_relax_coop(int m, const int* __restrict__ xu, const int* __restrict__ xv,
+                                                    const double* __restrict__ xw, unsigned long long* L,
+                                                    int* flags, int max_rounds, int* rounds_out) {
+    cg::grid_group grid = cg::this_grid();
+    const int gtid = blockIdx.x * blockDim.x + threadIdx.x, gsz = gridDim.x * blockDim.x;
+    int r = 0;
+    for (; r < max_rounds; r++) {
+        int changed = 0;
+        for (int e = gtid; e < m; e += gsz) {
+            unsigned long long lv = ((volatile unsigned long long*)L)[xv[e]];
+            if (lv == ~0ULL) continue;
+            unsigned long long w = dkey(xw[e]);
+            unsigned long long cand = w > lv ? w : lv;
+            int bu = xu[e];
+            if (cand < ((volatile unsigned long long*)L)[bu]) {
+                unsigned long long old = atomicMin(&L[bu], cand);
+                if (cand < old) changed = 1;
+            }
+        }
+        if (__any_sync(0xffffffffu, changed) && (threadIdx.x & 31) == 0) flags[r % 3] = 1;
+        if (gtid == 0) flags[(r + 2) % 3] = 0;
+        grid.sync();
+        int f = *(volatile int*)&flags[r % 3];
+        if (!f) break;
+    }
+    if (gtid == 0) *rounds_out = r + 1;
+}
+
 __global__ void k_flat_dirs(int n, const double* __restrict__ f, const int* __restrict__ pit,
                             const int* __restrict__ pdir, const int* __restrict__ nbr,
                             const int8_t* __restrict__ nnb, const int* __restrict__ spill_flag,
@@ -458,29 +718,44 @@ __global__ void k_pit_compact(int n, const int* __restrict__ pit, const int* __r
     vals[pos[i]] = i;
 }
 
-// one warp per pit: vol, max fill, max depth over its cells (sorted by id)
-__global__ void k_pit_params(int np1, const int* __restrict__ start, const int* __restrict__ counts,
+// Block-per-pit reductions in a fixed order (deterministic): strided partial
+// sums per thread, then a fixed shared-memory tree.
+template <int NV>
+__device__ __forceinline__ void block_reduce(double (&v)[NV], bool is_max[NV]) {
+    __shared__ double sh[NV][256];
+    for (int q = 0; q < NV; q++) sh[q][threadIdx.x] = v[q];
+    __syncthreads();
+    for (int s = 128; s > 0; s >>= 1) {
+        if (threadIdx.x < s)
+            for (int q = 0; q < NV; q++)
+                sh[q][threadIdx.x] = is_max[q] ? fmax(sh[q][threadIdx.x], sh[q][threadIdx.x + s])
+                                               : sh[q][threadIdx.x] + sh[q][threadIdx.x + s];
+        __syncthreads();
+    }
+    for (int q = 0; q < NV; q++) v[q] = sh[q][0];
+}
+
+// one block per pit: vol, max fill, max depth over its cells (sorted by id)
+__global__ void __launch_bounds__(256) k_pit_params(int np1, const int* __restrict__ start, const int* __restrict__ counts,
                              const int* __restrict__ cells, const double* __restrict__ f,
                              const double* __restrict__ h, double sl,
                              const double* __restrict__ larea, double* params) {
-    int p = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    int lane = threadIdx.x & 31;
+    int p = blockIdx.x;
+    int lane = threadIdx.x;
     if (p >= np1) return;
     int s0 = start[p], c = counts[p];
-    double vol = 0.0, hmax = -INFINITY, dmax = -INFINITY;
-    for (int t = lane; t < c; t += 32) {
+    double v[3] = {0.0, -INFINITY, -INFINITY};
+    for (int t = lane; t < c; t += 256) {
         int i = cells[s0 + t];
         double hc = h[i] < sl ? sl : h[i];
         double d = f[i] - hc;
-        vol += d * larea[i];
-        hmax = fmax(hmax, f[i]);
-        dmax = fmax(dmax, d);
+        v[0] += d * larea[i];
+        v[1] = fmax(v[1], f[i]);
+        v[2] = fmax(v[2], d);
     }
-    vol = warp_sum(vol);
-    for (int o = 16; o > 0; o >>= 1) {
-        hmax = fmax(hmax, __shfl_xor_sync(0xffffffffu, hmax, o));
-        dmax = fmax(dmax, __shfl_xor_sync(0xffffffffu, dmax, o));
-    }
+    bool mx[3] = {false, true, true};
+    block_reduce<3>(v, mx);
+    double vol = v[0], hmax = v[1], dmax = v[2];
     if (lane == 0) {
         if (c > 0) {
             params[3 * p] = vol;
@@ -510,58 +785,66 @@ __global__ void k_filled_lvl(int np1, const double* __restrict__ params, double*
     }
 }
 
-__global__ void k_filled_vol(int np1, const int* __restrict__ start, const int* __restrict__ counts,
+__global__ void __launch_bounds__(256) k_filled_vol(int np1, const int* __restrict__ start, const int* __restrict__ counts,
                              const int* __restrict__ cells, const double* __restrict__ h, double sl,
                              const double* __restrict__ farea, const double* __restrict__ lvl,
                              const double* __restrict__ params, double* vol) {
-    int p = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    int lane = threadIdx.x & 31;
+    int p = blockIdx.x;
+    int lane = threadIdx.x;
     if (p >= np1) return;
     int s0 = start[p], c = counts[p];
     double l0 = lvl[5 * p], l1 = lvl[5 * p + 1], l2 = lvl[5 * p + 2], l3 = lvl[5 * p + 3];
-    double v0 = 0, v1 = 0, v2 = 0, v3 = 0;
-    for (int t = lane; t < c; t += 32) {
+    double v[4] = {0, 0, 0, 0};
+    for (int t = lane; t < c; t += 256) {
         int i = cells[s0 + t];
         double e = h[i] < sl ? sl : h[i];
         double a = farea[i];
-        if (l0 > e) v0 += (l0 - e) * a;
-        if (l1 > e) v1 += (l1 - e) * a;
-        if (l2 > e) v2 += (l2 - e) * a;
-        if (l3 > e) v3 += (l3 - e) * a;
+        if (l0 > e) v[0] += (l0 - e) * a;
+        if (l1 > e) v[1] += (l1 - e) * a;
+        if (l2 > e) v[2] += (l2 - e) * a;
+        if (l3 > e) v[3] += (l3 - e) * a;
     }
-    v0 = warp_sum(v0);
-    v1 = warp_sum(v1);
-    v2 = warp_sum(v2);
-    v3 = warp_sum(v3);
+    bool mx[4] = {false, false, false, false};
+    block_reduce<4>(v, mx);
     if (lane == 0) {
-        vol[5 * p] = v0;
-        vol[5 * p + 1] = v1;
-        vol[5 * p + 2] = v2;
-        vol[5 * p + 3] = v3;
+        vol[5 * p] = v[0];
+        vol[5 * p + 1] = v[1];
+        vol[5 * p + 2] = v[2];
+        vol[5 * p + 3] = v[3];
         vol[5 * p + 4] = params[3 * p];
     }
 }
 
-// per-pit masked sum (one warp per pit), deterministic
-__global__ void k_pit_masked_sum(int np1, const int* __restrict__ start, const int* __restrict__ counts,
+// per-pit masked sum (one block per pit), deterministic
+__global__ void __launch_bounds__(256) k_pit_masked_sum(int np1, const int* __restrict__ start, const int* __restrict__ counts,
                                  const int* __restrict__ cells, const uint8_t* __restrict__ mask,
                                  const double* __restrict__ vals, double* out) {
-    int p = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    int lane = threadIdx.x & 31;
+    int p = blockIdx.x;
+    int lane = threadIdx.x;
     if (p >= np1) return;
     int s0 = start[p], c = counts[p];
-    double acc = 0.0;
-    for (int t = lane; t < c; t += 32) {
+    double v[1] = {0.0};
+    for (int t = lane; t < c; t += 256) {
         int i = cells[s0 + t];
-        if (mask[i]) acc += vals[i];
+        if (mask[i]) v[0] += vals[i];
     }
-    acc = warp_sum(acc);
-    if (lane == 0) out[p] = acc;
+    bool mx[1] = {false};
+    block_reduce<1>(v, mx);
+    if (lane == 0) out[p] = v[0];
 }
 
 // --------------------------------------------------------------------------
 // host driver
 // --------------------------------------------------------------------------
+static int launch_coop(gs_plan* p, const void* fn, void** args) {
+    cudaEvent_t stop = nullptr;
+    if (p->profiling) prof_begin(p, fn, &stop);
+    GS_CUDA(cudaLaunchCooperativeKernel(fn, p->coop_blocks, 256, args, 0, p->stream));
+    if (stop) cudaEventRecord(stop, p->stream);
+    p->launches++;
+    return GS_OK;
+}
+
 static int read_ints(gs_plan* p, int* dst, const int* src, int count) {
     GS_CUDA(cudaMemcpyAsync(dst, src, sizeof(int) * count, cudaMemcpyDeviceToHost, p->stream));
     GS_CUDA(cudaStreamSynchronize(p->stream));
@@ -578,7 +861,7 @@ static int exclusive_scan(gs_plan* p, const int* in, int* out, int count) {
 int group_sum_by_pit(gs_plan* p, const int* /*pit_ids*/, const uint8_t* mask, const double* vals,
                      double* out, int npits) {
     const int np1 = npits + 1;
-    launch(p, k_pit_masked_sum, grid_for((int64_t)np1 * 32, 256), 256, np1,
+    launch(p, k_pit_masked_sum, np1, 256, np1,
            (const int*)p->seg_start, (const int*)p->seg_count, (const int*)p->seg_vals2, mask, vals,
            out);
     GS_LAUNCH();
@@ -624,15 +907,16 @@ int fill_elevation(gs_plan* p, const double* h, double sealevel, double ofill, d
     const int64_t m = hbuf[0];
     if (m > p->xe_cap) { set_error(GS_ENOMEM, "pit fill: cross-edge capacity exceeded"); return GS_ENOMEM; }
     int rounds = 0;
-    for (;; rounds++) {
-        GS_CUDA(cudaMemsetAsync(p->i_scalar + I_CHANGED, 0, sizeof(int), p->stream));
-        if (m > 0)
-            launch(p, k_relax, p->sm_count * 8, 256, (int)m, (const int*)p->xe_u,
-                   (const int*)p->xe_v, (const double*)p->xe_w, p->basinL, p->i_scalar + I_CHANGED);
-        GS_LAUNCH();
+    {
+        GS_CUDA(cudaMemsetAsync(p->i_scalar + 5, 0, sizeof(int) * 3, p->stream));
+        int mm = (int)m, maxr = 1000000;
+        int* flags = p->i_scalar + 5;
+        int* rout = p->i_scalar + I_CHANGED;
+        void* args[] = {(void*)&mm, (void*)&p->xe_u, (void*)&p->xe_v, (void*)&p->xe_w, (void*)&p->basinL,
+                        (void*)&flags, (void*)&maxr, (void*)&rout};
+        GS_TRY(launch_coop(p, (const void*)k_relax_coop, args));
         GS_TRY(read_ints(p, hbuf, p->i_scalar + I_CHANGED, 1));
-        if (!hbuf[0]) break;
-        if (rounds > 100000) { set_error(GS_EMAXITER, "pit fill: basin relaxation did not converge"); return GS_EMAXITER; }
+        rounds = hbuf[0] - 1;
     }
     if (st) st->fill_rounds = rounds + 1;
     launch(p, k_fill_final, G, B, n, h, (const double*)p->d_scalar, sealevel, (const int8_t*)p->ledge,
@@ -686,29 +970,55 @@ int fill_elevation(gs_plan* p, const double* h, double sealevel, double ofill, d
     launch(p, k_bfs_init, G, B, n, (const int*)p->spill_flag, p->pdir, p->front0, p->i_scalar + I_NEXT);
     GS_LAUNCH();
     GS_TRY(read_ints(p, hbuf, p->i_scalar + I_NEXT, 1));
-    int fsize = hbuf[0], d = 1, levels = 0;
-    int* fa = p->front0;
-    int* fb = p->front1;
-    // wide frontiers: one launch per level; narrow ones: the rest in one block
-    while (fsize > 4096) {
-        GS_CUDA(cudaMemsetAsync(p->i_scalar + I_NEXT, 0, sizeof(int), p->stream));
-        launch(p, k_bfs_step, grid_for(fsize, B), B, fsize, (const int*)fa, d, n, (const double*)lfill,
-               (const int*)pit_ids, (const int*)p->nbr, (const int8_t*)p->nnb, p->pdir, fb,
-               p->i_scalar + I_NEXT);
-        GS_LAUNCH();
-        GS_TRY(read_ints(p, hbuf, p->i_scalar + I_NEXT, 1));
-        fsize = hbuf[0];
-        int* t = fa; fa = fb; fb = t;
-        d++;
-        levels++;
-        if (levels > n + 1) { set_error(GS_EMAXITER, "pit fill: flat BFS did not terminate"); return GS_EMAXITER; }
-    }
+    int fsize = hbuf[0], levels = 0;
     if (fsize > 0) {
-        launch(p, k_bfs_block, 1, 1024, fsize, fa, fb, p->i_scalar + I_NEXT, d, n, (const double*)lfill,
-               (const int*)pit_ids, (const int*)p->nbr, (const int8_t*)p->nnb, p->pdir, p->i_scalar + 4);
+        // compact the reachable set; use the shared-memory BFS when its
+        // visited bitmap fits, the cooperative grid BFS otherwise
+        launch(p, k_bfs_flag, G, B, n, (const int*)pit_ids, (const int*)p->spill_flag, p->flagbuf);
         GS_LAUNCH();
+        GS_TRY(exclusive_scan(p, p->flagbuf, p->scanbuf, n));
+        int last[2];
+        GS_CUDA(cudaMemcpyAsync(&last[0], p->scanbuf + n - 1, sizeof(int), cudaMemcpyDeviceToHost, p->stream));
+        GS_CUDA(cudaMemcpyAsync(&last[1], p->flagbuf + n - 1, sizeof(int), cudaMemcpyDeviceToHost, p->stream));
+        GS_CUDA(cudaStreamSynchronize(p->stream));
+        const int M = last[0] + last[1];
+        const size_t smem = sizeof(unsigned) * (size_t)((M + 31) / 32) + sizeof(int) * 2 * LBFS_CAP;
+        if (smem <= 200 * 1024) {
+            // packed adjacency rows: [count, ids...], stride S ints (16-byte multiple)
+            const int S = ((p->W + 1 + 3) / 4) * 4;
+            int* rows = p->bfs_rows;
+            int* ldv = p->lab;
+            GS_CUDA(cudaMemsetAsync(p->i_scalar + 6, 0, sizeof(int), p->stream));
+            launch(p, k_bfs_local_build, G, B, n, S, (const double*)lfill, (const int*)pit_ids,
+                   (const int*)p->flagbuf, (const int*)p->scanbuf, (const int*)p->nbr, (const int8_t*)p->nnb,
+                   (const int*)p->spill_flag, rows, p->comp, ldv, p->front0, p->i_scalar + 6);
+            GS_LAUNCH();
+            GS_CUDA(cudaFuncSetAttribute(k_bfs_local, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            cudaEvent_t stop = nullptr;
+            if (p->profiling) prof_begin(p, (const void*)k_bfs_local, &stop);
+            k_bfs_local<<<1, 1024, smem, p->stream>>>(M, S, (const int*)rows, (const int*)p->front0,
+                                                       p->i_scalar + 6, p->front1, p->minseed, ldv,
+                                                       p->i_scalar + 4);
+            if (stop) cudaEventRecord(stop, p->stream);
+            p->launches++;
+            GS_LAUNCH();
+            launch(p, k_bfs_local_scatter, grid_for(M, B), B, M, (const int*)p->comp, (const int*)ldv, p->pdir);
+            GS_LAUNCH();
+        } else {
+            launch(p, k_bfs_adj, G, B, n, p->W, (const double*)lfill, (const int*)pit_ids,
+                   (const int*)p->spill_flag, (const int*)p->nbr, (const int8_t*)p->nnb, p->xe_u, p->ledge);
+            GS_LAUNCH();
+            int* sizes = p->i_scalar + 5;
+            GS_CUDA(cudaMemcpyAsync(sizes, p->i_scalar + I_NEXT, sizeof(int), cudaMemcpyDeviceToDevice, p->stream));
+            GS_CUDA(cudaMemsetAsync(sizes + 1, 0, sizeof(int) * 2, p->stream));
+            int d0 = 1, nn = n, W = p->W;
+            int* lv = p->i_scalar + 4;
+            void* args[] = {(void*)&p->front0, (void*)&p->front1, (void*)&sizes, (void*)&d0, (void*)&nn,
+                            (void*)&W, (void*)&p->xe_u, (void*)&p->ledge, (void*)&p->pdir, (void*)&lv};
+            GS_TRY(launch_coop(p, (const void*)k_bfs_coop, args));
+        }
         GS_TRY(read_ints(p, hbuf, p->i_scalar + 4, 1));
-        levels += hbuf[0];
+        levels = hbuf[0];
     }
     if (st) st->flat_rounds = levels;
     launch(p, k_flat_dirs, G, B, n, (const double*)lfill, (const int*)pit_ids, (const int*)p->pdir,
@@ -744,11 +1054,11 @@ int fill_elevation(gs_plan* p, const double* h, double sealevel, double ofill, d
     }
     GS_TRY(exclusive_scan(p, p->seg_count, p->seg_start, np1));
     // pit tables
-    launch(p, k_pit_params, grid_for((int64_t)np1 * 32, 256), 256, np1, (const int*)p->seg_start,
+    launch(p, k_pit_params, np1, 256, np1, (const int*)p->seg_start,
            (const int*)p->seg_count, (const int*)p->seg_vals2, (const double*)lfill, h, sealevel,
            (const double*)p->larea, p->pit_params);
     launch(p, k_filled_lvl, grid_for(np1, B), B, np1, (const double*)p->pit_params, p->filled_lvl);
-    launch(p, k_filled_vol, grid_for((int64_t)np1 * 32, 256), 256, np1, (const int*)p->seg_start,
+    launch(p, k_filled_vol, np1, 256, np1, (const int*)p->seg_start,
            (const int*)p->seg_count, (const int*)p->seg_vals2, h, sealevel, (const double*)p->farea,
            (const double*)p->filled_lvl, (const double*)p->pit_params, p->filled_vol);
     GS_LAUNCH();
@@ -759,6 +1069,16 @@ int fill_elevation(gs_plan* p, const double* h, double sealevel, double ofill, d
         p->level = lv;
     }
     return GS_OK;
+}
+
+
+// smallest per-SM residency of the cooperative kernels at 256 threads
+int coop_occupancy(int* per_sm) {
+    int a = 0, b = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_bfs_coop, 256, 0) != cudaSuccess) return 1;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_relax_coop, 256, 0) != cudaSuccess) return 1;
+    *per_sm = a < b ? a : b;
+    return 0;
 }
 
 }  // namespace gs

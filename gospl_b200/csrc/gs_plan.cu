@@ -33,7 +33,7 @@ static void plan_free(gs_plan* p) {
                     p->outlet_ids, p->open_ids, p->open_mask, p->gid, p->rcv, p->dist, p->wgt, p->rslot,
                     p->rslot_i, p->lsink, p->sea, p->don_mask, p->don_k, p->cnt, p->queue, p->ctr,
                     p->done_flag, p->q, p->q2, p->q3, p->order, p->order2, p->pos, p->order_i, p->okey, p->okey2, p->ok32, p->ok32b, p->oval, p->oval2, p->c, p->ledge, p->parent, p->basinL, p->xe_u,
-                    p->xe_v, p->xe_w, p->comp, p->minseed, p->lab, p->flagbuf, p->scanbuf, p->pdir,
+                    p->xe_v, p->xe_w, p->bfs_rows, p->comp, p->minseed, p->lab, p->flagbuf, p->scanbuf, p->pdir,
                     p->front0, p->front1, p->spill_flag, p->bestlid, p->d_scalar, p->i_scalar,
                     p->u_scalar, p->pit_params, p->pit_info, p->filled_lvl, p->filled_vol, p->pit_vol,
                     p->pit_in, p->pit_ev, p->pit_win, p->pit_lvl, p->pit_state, p->seg_keys, p->seg_vals,
@@ -82,6 +82,13 @@ int plan_create(int64_t nb, const int32_t* nnb, const int32_t* ngb, const double
     int dev = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&p->sm_count, cudaDevAttrMultiProcessorCount, dev);
+    {
+        // two 256-thread blocks per SM for the cooperative kernels (both use
+        // few registers and little shared memory; checked against occupancy)
+        int per_sm = 0;
+        if (coop_occupancy(&per_sm) == 0 && per_sm > 0) p->coop_blocks = p->sm_count;
+        else p->coop_blocks = p->sm_count;
+    }
 
     std::vector<int> h_nbr((size_t)W * n, -1);
     std::vector<double> h_elen((size_t)W * n, 0.0), h_vd((size_t)W * n, 0.0);
@@ -176,6 +183,7 @@ int plan_create(int64_t nb, const int32_t* nnb, const int32_t* ngb, const double
         TRYP(dalloc(&p->xe_u, (size_t)p->xe_cap));
         TRYP(dalloc(&p->xe_v, (size_t)p->xe_cap));
         TRYP(dalloc(&p->xe_w, (size_t)p->xe_cap));
+        TRYP(dalloc(&p->bfs_rows, (size_t)(((W + 1 + 3) / 4) * 4) * N));
         TRYP(dalloc(&p->comp, N));
         TRYP(dalloc(&p->minseed, N));
         TRYP(dalloc(&p->lab, N));

@@ -15,6 +15,7 @@ struct gs_plan {
     cudaStream_t stream = 0;
     int64_t launches = 0;
     int sm_count = 148;
+    int coop_blocks = 148;               // co-resident 256-thread blocks for cooperative launches
 
     // mesh, slot-major [W][n]
     int* nbr = nullptr;          // FVnID (-1 pad)
@@ -71,6 +72,7 @@ struct gs_plan {
     int* xe_v = nullptr;
     double* xe_w = nullptr;
     int64_t xe_cap = 0;
+    int* bfs_rows = nullptr;             // packed BFS adjacency rows, stride ((W+4)/4)*4
     int* comp = nullptr;
     int* minseed = nullptr;
     int* lab = nullptr;
@@ -163,6 +165,7 @@ int apply_forces(gs_plan* p, double* h, const double* rain, const double* upsub,
                  double sealevel, double* bl);
 
 void prof_begin(gs_plan* p, const void* fn, cudaEvent_t* stop);
+int coop_occupancy(int* per_sm);
 
 template <class K, class... A>
 inline void launch(gs_plan* p, K kernel, int grid, int block, A... args) {
