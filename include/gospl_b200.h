@@ -167,6 +167,25 @@ int gs_hillslope(gs_plan* plan, double* h, double* cum_ed, double* eb, double se
 int gs_apply_forces(gs_plan* plan, double* h, const double* rain, const double* upsub, double dt,
                     double sealevel, double* bl);
 
+/*
+ * Allocation-free flow solve.  No counterpart in the reference: goSPL always
+ * allocates its PETSc matrices and vectors.  For callers that cannot call
+ * cudaMalloc (an embedding application that owns every allocation, a fixed
+ * memory budget, a stream under capture), this solves (I - W^T) q = b for the
+ * receiver graph rcv/wgt ([nrcv][nb], as gs_mfdreceivers writes them) with
+ * all scratch in a fixed file-scope device array, so it allocates nothing.
+ * The caller passes inputs and the output q.  Limits: nb <= GS_NOALLOC_MAX_NB,
+ * nrcv <= GS_NOALLOC_MAX_RCV, else GS_EINVAL.  Every GPU that loads the
+ * library holds the array (about 40 MB) until the process exits.  All calls
+ * share it: calls that overlap on the GPU race and must be serialised by the
+ * caller.  The first call on each device resolves the array's address (make
+ * it before any stream capture).  Synchronises `stream` before returning.
+ */
+#define GS_NOALLOC_MAX_NB 1048576
+#define GS_NOALLOC_MAX_RCV 4
+int gs_flow_solve_noalloc(int64_t nb, int32_t nrcv, const int32_t* rcv, const double* wgt,
+                          const double* b, double* q, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
