@@ -50,7 +50,7 @@ class Clocks:
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
         try:
             self.p = subprocess.Popen(["nvidia-smi", "-i", str(index), "--query-gpu=" + q,
-                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                       "--format=csv,noheader,nounits", "-lms", "50"],
                                       stdout=self.f, stderr=subprocess.DEVNULL)
         except Exception:
             self.p = None
@@ -81,13 +81,16 @@ def sphere_inputs(level, seed=20261205):
     return S.sphere_config(level=level, seed=seed)
 
 
-def cpu_sample(level=6, steps=1):
+def cpu_sample(level=7, steps=2, warm=0):
     """Oracle (single-threaded C + numpy restatement of the reference) on a
-    smaller sphere of the same recipe: vertex-steps/s of the timed steps."""
+    smaller sphere of the same recipe: vertex-steps/s of the timed steps
+    (model set-up and `warm` untimed steps excluded)."""
     from oracle.model import OracleModel
     c, f, z, rain, up, p = sphere_inputs(level)
     p = dict(p, rain=rain, upsub=up)
     om = OracleModel(c, f, z, p)
+    for _ in range(warm):
+        om.step()
     t0 = time.perf_counter()
     for _ in range(steps):
         om.step()
@@ -96,41 +99,54 @@ def cpu_sample(level=6, steps=1):
 
 
 def _cpu_worker(args):
-    level, steps = args
-    return cpu_sample(level, steps)
+    level, steps, warm = args
+    return cpu_sample(level, steps, warm)
+
+
+def host_cores():
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
 
 
 def run_reference(args, rank, world):
     """CPU reference arm: the oracle restatement of the reference path on all
-    host cores (independent samples in parallel processes)."""
+    host cores.  One process per core advances its own copy of the sample
+    landscape (the reference's own mpirun path cannot be built: it needs
+    gfortran, PETSc and MPI); the aggregate throughput is the sum of the
+    concurrent per-process rates."""
     if rank != 0:
         return
     import multiprocessing as mp
-    cores = os.cpu_count() or 1
+    cores = min(host_cores(), 96)
     level = args.cpu_level
+    steps = max(1, min(args.steps, 2))
+    warm = 1 if args.warmup > 0 else 0
     t0 = time.perf_counter()
     with mp.get_context("spawn").Pool(cores) as pool:
-        for _ in range(args.warmup and 1):
-            pool.map(_cpu_worker, [(level, 1)] * cores)
-        t1 = time.perf_counter()
-        res = pool.map(_cpu_worker, [(level, 1)] * (cores * max(1, args.steps // 5)))
-        t2 = time.perf_counter()
-    vs = sum(r[1] * r[2] for r in res)
-    value = vs / (t2 - t1)
+        res = pool.map(_cpu_worker, [(level, steps, warm)] * cores)
+    wall = time.perf_counter() - t0
+    value = sum(r[0] for r in res)
     n = res[0][1]
-    sample = "oracle on icosphere level %d (%d vertices), %d one-step samples in %d processes" % (
-        level, n, len(res), cores)
+    sample = ("oracle on icosphere level %d (%d vertices), %d concurrent processes x %d timed step(s) "
+              "after %d untimed" % (level, n, cores, steps, warm))
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "vertex-steps/s", "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * 2621442 / value,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * sphere_vertices(args.level) / value,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic (seeded)",
-            "config": {"workload": "sphere level 9 (2,621,442 vertices), one physics step; CPU samples at level %d"
-                       % level, "global_batch": 1, "seq_len": 0, "parallelism": "replicas"},
+            "data": "synthetic (seeded sphere, SH relief)",
+            "config": {"workload": "sphere level %d (%d vertices), full physics step; CPU samples at level %d"
+                       % (args.level, sphere_vertices(args.level), level),
+                       "global_batch": 1, "seq_len": 0, "parallelism": "processes"},
             "cpu_baseline": {"value": value, "unit": "vertex-steps/s", "cores": cores, "kind": "port",
                              "sample": sample},
             "e2e": {"value": value, "unit": "vertex-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-            "wall_s": t2 - t0}
+            "wall_s": wall}
     print(json.dumps(line), flush=True)
+
+
+def sphere_vertices(level):
+    return 10 * 4 ** level + 2
 
 
 def parse_profile(report):
@@ -145,11 +161,11 @@ def parse_profile(report):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--level", type=int, default=9)
-    ap.add_argument("--cpu-level", type=int, default=6)
+    ap.add_argument("--cpu-level", type=int, default=7)
     ap.add_argument("--no-cpu", action="store_true")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
@@ -247,35 +263,43 @@ def main():
     hbm, src = peaks()
     top = max(prof.items(), key=lambda kv: kv[1][1]) if prof else ("none", (1, 1.0))
     name, (cnt, tot_ms) = top
+    kname = _short(name)
     per_launch_ms = tot_ms / max(cnt, 1)
-    bytes_per_vertex = ALGO_BYTES.get(_short(name), None)
-    if bytes_per_vertex is not None:
-        units = n * bytes_per_vertex[1](model)
-        achieved = units * bytes_per_vertex[0] / (per_launch_ms / 1000.0) / 1e9
-    else:
-        achieved = None
-    share = {(_short(k)): round(v[1] / sum(x[1] for x in prof.values()), 4) for k, v in prof.items()}
+    layout = launch_layout(model, stats)
+    algo = algo_bytes_per_launch(kname, layout)
+    achieved = algo / (per_launch_ms / 1000.0) / 1e9 if algo else None
+    traffic = NCU_TRAFFIC_PER_VERTEX.get(kname)
+    share = {}
+    for k, v in prof.items():
+        sk = _short(k)
+        share[sk] = round(share.get(sk, 0.0) + v[1] / sum(x[1] for x in prof.values()), 4)
+    step_bytes = step_algo_bytes(layout)
+    step_gbs = step_bytes / (ms / args.steps / 1000.0) / 1e9
 
     cpu = None
     if rank == 0 and not args.no_cpu:
-        v, nn, st, dt = cpu_sample(args.cpu_level, 1)
+        v, nn, st, dt = cpu_sample(args.cpu_level, 2)
         cpu = {"value": v, "unit": "vertex-steps/s", "cores": 1, "kind": "port",
                "sample": "oracle (C + numpy restatement of the reference path) on icosphere level %d "
-                         "(%d vertices), 1 physics step, %.1f s" % (args.cpu_level, nn, dt)}
+                         "(%d vertices), %d physics steps, %.1f s" % (args.cpu_level, nn, st, dt)}
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "vertex-steps/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded sphere, SH relief)",
-            "config": {"workload": "sphere level 9 (2,621,442 vertices), full physics step: receivers, pit fill, "
-                                   "flow accumulation + lake cascade, SPL, hillslope, forcing",
+            "config": {"workload": "sphere level %d (%d vertices), full physics step: receivers, pit fill, "
+                                   "flow accumulation + lake cascade, SPL, hillslope, forcing" % (args.level, n),
                        "vertices": n, "global_batch": world, "seq_len": 0,
                        "parallelism": "replicas" if world > 1 else "single",
                        "l2": "working set > 126 MB L2 (mesh arrays alone ~1 GB)"},
             "e2e": {"value": e2e, "unit": "vertex-steps/s", "h2d_bytes_per_step": 8 * n, "d2h_bytes_per_step": 8 * n},
-            "roofline": {"bound": "hbm", "kernel": _short(name), "achieved": achieved, "peak": hbm,
-                         "unit": "GB/s", "frac": (achieved / hbm) if achieved else None, "traffic": None,
-                         "peak_source": src, "launch_ms": per_launch_ms, "launches": cnt},
+            "roofline": {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": hbm,
+                         "unit": "GB/s", "frac": (achieved / hbm) if achieved else None,
+                         "traffic": (traffic * n) if traffic else None,
+                         "algorithmic_bytes": algo, "peak_source": src + " (MEASURED_PEAKS.json hbm_gbs)"
+                         if src == "measured" else src, "launch_ms": per_launch_ms, "launches": cnt},
+            "step_roofline": {"algorithmic_bytes": step_bytes, "achieved": step_gbs, "peak": hbm, "unit": "GB/s",
+                              "frac": step_gbs / hbm, "counts": layout},
             "kernel_share": share,
             "kernel_ms_per_step": sum(v[1] for v in prof.values()) / nprof,
             "gpu_launches": launches,
@@ -291,14 +315,15 @@ def main():
 
 
 def _short(name):
+    """gs::k_name from a (possibly mangled) kernel name; the two ordered
+    sweeps are told apart by their operator type."""
     s = name
-    for key in ("k_dataflow<gs::FlowOp>", "k_dataflow<gs::SplOp>"):
-        pass
+    if "k_ordered" in s:
+        return "k_ordered_flow" if "FlowOrd" in s else ("k_ordered_spl" if "SplOrd" in s else "k_ordered")
     if "k_dataflow" in s:
         return "k_dataflow_flow" if "FlowOp" in s else ("k_dataflow_spl" if "SplOp" in s else "k_dataflow")
     for tok in s.replace("(", " ").replace("<", " ").split():
         if tok.startswith("_ZN2gs"):
-            # mangled gs::k_name
             rest = tok[6:]
             ln = ""
             while rest and rest[0].isdigit():
@@ -310,12 +335,69 @@ def _short(name):
     return s
 
 
-# algorithmic bytes per vertex (compulsory traffic, d = 6 neighbour slots, R = 3)
-# and the multiplier of vertices per launch
-ALGO_BYTES = {
-    "k_mfd_receivers": (4 + 6 * 4 + 6 * 8 + 8 + 6 * 4 + 3 * 4 + 3 * 8 + 3 * 8 + 3 * 1, lambda m: 1),
-    "k_dataflow_flow": (4 + 4 + 8 + 3 * 4 + 3 * 8 + 8 + 8 + 8 + 4 + 1, lambda m: 1),
-    "k_dataflow_spl": (3 * 4 + 3 * 8 + 8 + 8 + 4 + 4 + 1, lambda m: 1),
+def launch_layout(model, stats):
+    """Counts the byte models need: vertices, receiver links with a nonzero
+    weight (donor edges of the flow sweep), flat-BFS cells and the executed
+    per-step iteration counts of the last step."""
+    import torch
+    n = model.lpoints
+    R = model.flowDir
+    w = model.wgt_i
+    selfr = model.rcv_i == torch.arange(n, device=w.device, dtype=model.rcv_i.dtype).unsqueeze(0)
+    links = int(((w != 0) & ~selfr).sum().item())
+    fl = stats.get("flow", {})
+    hs = stats.get("hillslope", {})
+    pit_cells = int((model.pitIDs > -1).sum().item())
+    return {"n": n, "R": R, "W": int(np.max(model.mesh.nnb)),
+            "links": links, "pit_cells": pit_cells,
+            "cascade_solves": int(fl.get("cascade_solves", 0)), "flat_rounds": int(fl.get("flat_rounds", 0)),
+            "fill_rounds": int(fl.get("fill_rounds", 0)), "cg_iters": int(hs.get("cg_iters", 0))}
+
+
+def algo_bytes_per_launch(kname, L):
+    """Compulsory bytes of one launch, from the device layout (int32 ids,
+    float64 values, slot-major [W][n] neighbour tables).  Gathers of values
+    another thread wrote in the same sweep count as cache hits."""
+    n, R, W, E = L["n"], L["R"], L["W"], L["links"]
+    if kname == "k_ordered_flow":
+        # order 4, link mask 4, receiver-slot codes 8, sorted slot order 8,
+        # b 8, q write 8; per donor link: neighbour id 4 + weight 8
+        return n * (4 + 4 + 8 + 8 + 8 + 8) + E * (4 + 8)
+    if kname == "k_ordered_spl":
+        # order 4, rcv 4R, coefficient 8R, hOld 8, h write 8
+        return n * (4 + 12 * R + 16)
+    if kname == "k_bfs_local":
+        # packed rows of the pit cells (count + up to W local ids, padded to
+        # a multiple of 4 ints) and one distance write per cell
+        S = ((W + 1 + 3) // 4) * 4
+        return L["pit_cells"] * (4 * S + 4)
+    if kname == "k_mfd_receivers":
+        # h 8, gid 4, neighbour count 1, W ids 4 + W lengths 8 (slot-major),
+        # writes rcv 4R + dist 8R + wgt 8R
+        return n * (8 + 4 + 1 + 12 * W + 20 * R)
+    if kname in ("k_dataflow_flow",):
+        return n * (4 + 4 + 8 + 12 * R + 8 + 8 + 8 + 4 + 1)
+    if kname in ("k_dataflow_spl",):
+        return n * (12 * R + 8 + 8 + 4 + 4 + 1)
+    return None
+
+
+def step_algo_bytes(L):
+    """Compulsory bytes of one physics step, per vertex by stage with the
+    executed counts: receivers 144, pit fill 52 per full-vertex propagation
+    pass (steepest descent, cross-basin edges, final fill: 3) plus 40 per
+    labelling/flat pass (pit labels, flat directions: 2), flow sweep 60, SPL
+    108, 164 per CG iteration, 204 per cascade solve (receivers rebuild +
+    flow sweep) and forcing 40."""
+    per_vertex = (144 + (52 * 3 + 40 * 2) + 60 + 108 + 164 * L["cg_iters"] + 204 * L["cascade_solves"] + 40)
+    return L["n"] * per_vertex
+
+
+# DRAM bytes per vertex (dram__bytes_read.sum + dram__bytes_write.sum of one
+# launch divided by the vertices it processed) from the ncu captures summarised
+# under profiles/; scaled by the vertex count of the run.
+NCU_TRAFFIC_PER_VERTEX = {
+    "k_mfd_receivers": (45.681152e6 + 20.494080e6) / 655362,
 }
 
 

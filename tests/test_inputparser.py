@@ -1,0 +1,73 @@
+"""goSPL YAML input subset (gospl/tools/inputparser.py) read by Model(filename)."""
+import numpy as np
+import pytest
+
+from gospl_b200.inputparser import parse_bc, read_input
+
+YML = """name: incising-like
+domain:
+    npdata: ['{mesh}','v','c','z']
+    flowdir: 3
+    bc: '0f01'
+    nodep: False
+time:
+    start: 0.
+    end: 300.
+    tout: 300
+    dt: 100.
+spl:
+    K: 4.0e-6
+    d: 0.
+    m: 0.5
+    G: 0.
+diffusion:
+    hillslopeKa: 0.01
+    hillslopeKm: 0.2
+sea:
+    position: -100.
+climate:
+  - start: 0.
+    uniform: 1
+tectonics:
+  - start: 0.
+    end: 300.
+    upsub: ['{mesh}', 'u']
+"""
+
+
+def _write(tmp_path, text):
+    rng = np.random.default_rng(3)
+    v = rng.random((10, 3))
+    c = np.array([[0, 1, 2], [2, 3, 4]], np.int32)
+    np.savez(tmp_path / "m.npz", v=v, c=c, z=rng.random(10), u=np.full(10, 1e-3))
+    y = tmp_path / "in.yml"
+    y.write_text(text.format(mesh=str(tmp_path / "m")))
+    return y, v
+
+
+def test_reads_the_path_keys(tmp_path):
+    y, v = _write(tmp_path, YML)
+    coords, cells, elev, p = read_input(str(y))
+    assert np.array_equal(coords, v) and cells.shape == (2, 3) and elev.shape == (10,)
+    assert p["flowDir"] == 3 and p["bc"] == "ofof"
+    assert (p["tStart"], p["tEnd"], p["dt"], p["tout"]) == (0.0, 300.0, 100.0, 300.0)
+    assert (p["K"], p["d"], p["m"]) == (4.0e-6, 0.0, 0.5)
+    assert (p["Cda"], p["Cdm"], p["oFill"], p["sealevel"]) == (0.01, 0.2, -6000.0, -100.0)
+    assert np.all(p["rain"] == 1.0) and np.allclose(p["upsub"], 1e-3)
+
+
+def test_defaults_and_errors(tmp_path):
+    y, _ = _write(tmp_path, YML.replace("    G: 0.\n", "    G: 1.\n"))
+    with pytest.raises(ValueError):
+        read_input(str(y))
+    y, _ = _write(tmp_path, YML.replace("    end: 300.\n    tout", "    end: -1.\n    tout"))
+    with pytest.raises(ValueError):
+        read_input(str(y))
+    with pytest.raises(ValueError):
+        parse_bc("oox")
+    with pytest.raises(ValueError):
+        parse_bc("cooo")
+    assert parse_bc("0101") == "ofof"
+    y, _ = _write(tmp_path, YML.replace("spl:\n    K: 4.0e-6\n    d: 0.\n    m: 0.5\n    G: 0.\n", ""))
+    _, _, _, p = read_input(str(y))
+    assert (p["K"], p["d"], p["m"]) == (1.0e-12, 0.0, 0.5)
