@@ -32,6 +32,7 @@ void prof_begin(gs_plan* p, const void* fn, cudaEvent_t* stop) {
     p->prof_ev.push_back(a);
     p->prof_ev.push_back(b);
     p->prof_idx.push_back(idx);
+    p->prof_stream.push_back(p->stream == p->side_a ? 1 : (p->stream == p->side_b ? 2 : 0));
     *stop = b;
 }
 
@@ -96,6 +97,7 @@ int gs_plan_profile(gs_plan* plan, int32_t enable) {
     for (cudaEvent_t e : plan->prof_ev) cudaEventDestroy(e);
     plan->prof_ev.clear();
     plan->prof_idx.clear();
+    plan->prof_stream.clear();
     plan->profiling = enable ? 1 : 0;
     return GS_OK;
 }
@@ -117,6 +119,29 @@ int gs_plan_profile_report(gs_plan* plan, char* buf, int64_t len) {
         const char* name = "?";
         cudaFuncGetName(&name, plan->prof_fn[k]);
         out += std::string(name) + " " + std::to_string(cnt[k]) + " " + std::to_string(tot[k]) + "\n";
+    }
+    if (buf && len > 0) {
+        std::strncpy(buf, out.c_str(), (size_t)len - 1);
+        buf[len - 1] = 0;
+    }
+    return (int)std::min<size_t>(out.size(), (size_t)0x7fffffff);
+}
+
+int gs_plan_profile_trace(gs_plan* plan, char* buf, int64_t len) {
+    NEED(plan);
+    GS_CUDA(cudaDeviceSynchronize());
+    std::string out;
+    if (plan->prof_ev.size() >= 2) {
+        cudaEvent_t t0 = plan->prof_ev[0];
+        for (size_t q = 0; q + 1 < plan->prof_ev.size(); q += 2) {
+            float a = 0.f, b = 0.f;
+            if (cudaEventElapsedTime(&a, t0, plan->prof_ev[q]) != cudaSuccess) continue;
+            if (cudaEventElapsedTime(&b, t0, plan->prof_ev[q + 1]) != cudaSuccess) continue;
+            const char* name = "?";
+            cudaFuncGetName(&name, plan->prof_fn[plan->prof_idx[q / 2]]);
+            out += std::string(name) + " " + std::to_string(plan->prof_stream[q / 2]) + " " +
+                   std::to_string(a) + " " + std::to_string(b) + "\n";
+        }
     }
     if (buf && len > 0) {
         std::strncpy(buf, out.c_str(), (size_t)len - 1);

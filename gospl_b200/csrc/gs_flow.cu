@@ -205,16 +205,34 @@ int flow_accumulation(gs_plan* p, const double* h, const double* bl, double seal
     const int n = (int)p->n;
     if (n == 0) return GS_OK;
     const int B = 256, G = grid_for(n, B);
-    GS_TRY(fill_elevation(p, h, sealevel, ofill, lfill, pit_ids, flat_dirs, st));
+    // Receivers on the unfilled surface (down=False: they read h, not the
+    // fill) and the topological order of their graph, on side_a while the
+    // main stream fills depressions.
+    int* bad_a = p->h_pinned + 1;
+    GS_CUDA(cudaEventRecord(p->ev_fork_a, p->stream));
+    GS_CUDA(cudaStreamWaitEvent(p->side_a, p->ev_fork_a, 0));
+    {
+        StreamSwap sw(p, p->side_a, p->cub_tmp2);
+        GS_TRY(flow_direction(p, h, false, nullptr, nullptr, nullptr, sealevel, rcv_i, dist_i, wgt_i,
+                              p->rslot_i, nullptr, nullptr));
+        GS_TRY(flow_order(p, h, p->order_i));
+        GS_TRY(flow_prepare(p, rcv_i, wgt_i, p->rslot_i, fal, p->order_i, bad_a));
+    }
+    GS_CUDA(cudaEventRecord(p->ev_a, p->side_a));
+    GS_TRY(fill_elevation(p, h, sealevel, ofill, lfill, pit_ids, flat_dirs, st, true, sea));
     const int P = p->npits, np1 = P + 1;
 
-    // receivers on the unfilled surface (down=False) and their snapshots
-    GS_TRY(flow_direction(p, h, false, lfill, pit_ids, flat_dirs, sealevel, rcv_i, dist_i, wgt_i,
-                          p->rslot_i, lsink, sea));
+    // join: lsink of the snapshot graph, rain on land, the first flow sweep
+    // (its flat directions are still being computed on side_b)
+    GS_CUDA(cudaStreamWaitEvent(p->stream, p->ev_a, 0));
+    GS_TRY(sink_mask(p, wgt_i, sea, lsink));
     launch(p, k_rain_sea, G, B, n, bl, (const uint8_t*)sea, p->nfa);
     GS_LAUNCH();
+    GS_CUDA(cudaEventSynchronize(p->ev_a));
+    const int ok_i = *bad_a ? 0 : 1;
+    p->order_i_valid = ok_i;
     int cyc = 0;
-    GS_TRY(flow_solve(p, rcv_i, wgt_i, p->rslot_i, p->nfa, fal, &cyc, h, nullptr, p->order_i));
+    GS_TRY(flow_run(p, rcv_i, wgt_i, p->rslot_i, p->nfa, fal, &cyc, p->order_i, ok_i));
     int total_cycles = cyc;
     launch(p, k_copy, G, B, (int64_t)n, h, p->wf);
     // pitVol and "any pit with volume"
@@ -258,15 +276,24 @@ int flow_accumulation(gs_plan* p, const double* h, const double* bl, double seal
             double resid = 0.0;
             if (flags & F_BIG) {
                 const double* surf = (step == 100) ? lfill : p->wf;
-                GS_TRY(flow_direction(p, surf, true, lfill, pit_ids, flat_dirs, sealevel, p->rcv,
-                                      p->dist, p->wgt, p->rslot, lsink, sea));
+                // receivers and the surface order do not need the flat BFS;
+                // the flat routing and the order's ties do: join it between
+                GS_TRY(receivers(p, p->R, 1.1, surf, sealevel, p->gid, p->rcv, p->dist, p->wgt, p->rslot));
+                GS_TRY(flow_order(p, surf, p->order));
+                GS_TRY(fill_join(p, st));
+                GS_TRY(flow_direction_post(p, surf, true, lfill, pit_ids, flat_dirs, sealevel, p->rcv, p->dist,
+                                           p->wgt, p->rslot, lsink, sea));
+                GS_TRY(flow_order_ties(p, p->pdir, p->order));
                 launch(p, k_div, G, B, (int64_t)n, (const double*)p->nfa, dt, p->q2);
                 GS_LAUNCH();
                 GS_TRY(sum_to_host(p, p->q2, n, &resid));
                 if (resid > p->maxarea) {
                     excess = true;
                     // solve into FA's buffer: FA is consumed already
-                    GS_TRY(flow_solve(p, p->rcv, p->wgt, p->rslot, p->q2, p->q, &cyc, surf, p->pdir, p->order));
+                    GS_TRY(flow_prepare(p, p->rcv, p->wgt, p->rslot, p->q, p->order, p->h_pinned));
+                    GS_CUDA(cudaStreamSynchronize(p->stream));
+                    GS_TRY(flow_run(p, p->rcv, p->wgt, p->rslot, p->q2, p->q, &cyc, p->order,
+                                    p->h_pinned[0] ? 0 : 1));
                     total_cycles += cyc;
                     launch(p, k_cascade_accum, G, B, n, (const double*)p->q, dt, h, (const double*)p->wf,
                            p->q, fal);
@@ -292,6 +319,7 @@ int flow_accumulation(gs_plan* p, const double* h, const double* bl, double seal
         launch(p, k_max_key, p->sm_count * 4, 256, (int64_t)n, (const double*)fal, p->u_scalar);
         GS_LAUNCH();
     }
+    GS_TRY(fill_join(p, st));
     launch(p, k_flow_final, G, B, n, anyvol ? 1 : 0, h, (const double*)p->wf, (const int*)pit_ids,
            (const unsigned long long*)p->u_scalar, fal, fill_fal, water);
     GS_LAUNCH();

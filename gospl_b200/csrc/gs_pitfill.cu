@@ -119,12 +119,25 @@ __global__ void k_descend(int n, const double* __restrict__ h, const double* __r
     parent[c] = best;
 }
 
+// Pointer jumping towards the basin roots, up to JUMP_HOPS hops per vertex
+// and launch.  Other threads shorten the same chains concurrently; every
+// parent value ever stored is an ancestor on the vertex's descent path, so
+// reading a stale or a fresh value are both valid steps.  *changed is set
+// while some vertex has not reached its root.
+constexpr int JUMP_HOPS = 16;
 __global__ void k_jump(int n, int* parent, int* changed) {
     int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= n) return;
-    int p = parent[c];
-    int pp = parent[p];
-    if (pp != p) { parent[c] = pp; *changed = 1; }
+    const int p0 = parent[c];
+    int p = p0;
+    int hop = 0;
+    for (; hop < JUMP_HOPS; hop++) {
+        int pp = ld_relaxed_s32(parent + p);
+        if (pp == p) break;
+        p = pp;
+    }
+    if (p != p0) parent[c] = p;
+    if (hop == JUMP_HOPS) *changed = 1;
 }
 
 __global__ void k_basin_init(int n, const int* __restrict__ parent, const int8_t* __restrict__ ledge,
@@ -141,8 +154,10 @@ __global__ void k_cross_edges(int n, const double* __restrict__ h, const double*
     int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= n) return;
     if (ledge[c] == -2) return;
-    const double level = dsc[D_LEVEL];
     const int rc = root[c];
+    // a seed basin keeps level -inf: no edge can lower it
+    if (ledge[rc] >= 0) return;
+    const double level = dsc[D_LEVEL];
     const double zc = h[c] - level;
     for (int s = 0; s < nnb[c]; s++) {
         int j = nbr[(size_t)s * n + c];
@@ -150,7 +165,7 @@ __global__ void k_cross_edges(int n, const double* __restrict__ h, const double*
         int rj = root[j];
         if (rj == rc) continue;
         double zj = h[j] - level;
-        int pos = atomicAdd(count, 1);
+        int pos = agg_append(count);
         if (pos < cap) {
             xu[pos] = rc;
             xv[pos] = rj;
@@ -481,7 +496,7 @@ __global__ void __launch_bounds__(1024) k_bfs_block2(int fsize0, int* init, int*
 // BFS over the compacted set of reachable vertices (pit cells and spill
 // nodes, local ids 0..M-1) in one block: the visited set is a shared-memory
 // bitmap and the frontiers live in shared memory, so a level costs one global
-// load of the adjacency rows plus block barriers.
+// load of the adjacency rows, warp-aggregated appends and one block barrier.
 __global__ void k_bfs_flag(int n, const int* __restrict__ pit, const int* __restrict__ spill_flag, int* flag) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) flag[i] = (pit[i] > -1 || spill_flag[i]) ? 1 : 0;
@@ -524,56 +539,93 @@ __global__ void __launch_bounds__(1024) k_bfs_local(int M, int S, const int* __r
     const int nw = (M + 31) >> 5;
     int* fA = (int*)(smem_u + nw);
     int* fB = fA + LBFS_CAP;
-    __shared__ int s_next;
-    const int tid = threadIdx.x, nt = blockDim.x;
+    // three rotating frontier counters: level r reads s_cnt[r%3], appends to
+    // s_cnt[(r+1)%3] and clears s_cnt[(r+2)%3], so one barrier per level
+    // separates every write of a counter from its reads
+    __shared__ int s_cnt[3];
+    const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31;
     for (int w = tid; w < nw; w += nt) vis[w] = 0u;
+    if (tid < 3) s_cnt[tid] = 0;
     __syncthreads();
     int size = *nseed_p;
-    // seeds: distance 1
+    // seeds: distance 1; frontier entries beyond LBFS_CAP live in global memory
     for (int t = tid; t < size; t += nt) {
         int li = seeds[t];
         atomicOr(&vis[li >> 5], 1u << (li & 31));
         if (t < LBFS_CAP) fA[t] = li;
-        gA[t] = li;
+        else gA[t] = li;
     }
     __syncthreads();
     int* curS = fA;
     int* nxtS = fB;
     int* curG = gA;
     int* nxtG = gB;
-    bool cur_sh = size <= LBFS_CAP;
-    int d = 1, levels = 0;
+    const int S4 = S >> 2;
+    int d = 1, levels = 0, r = 0;
     while (size > 0 && levels <= M) {
-        if (tid == 0) s_next = 0;
-        __syncthreads();
-        for (int t = tid; t < size; t += nt) {
-            int li = cur_sh ? curS[t] : curG[t];
-            const int4* r4 = reinterpret_cast<const int4*>(rows + (size_t)li * S);
+        int* cnt = &s_cnt[(r + 1) % 3];
+        if (tid == 0) s_cnt[(r + 2) % 3] = 0;
+        // every warp runs the same number of batches so that ballots see all lanes
+        for (int base = 0; base < size; base += nt) {
+            const int t = base + tid;
             int row[16];
-            for (int q = 0; q < S / 4; q++) {
-                int4 v = r4[q];
-                row[4 * q] = v.x; row[4 * q + 1] = v.y; row[4 * q + 2] = v.z; row[4 * q + 3] = v.w;
+            int k = 0;
+            if (t < size) {
+                const int li = t < LBFS_CAP ? curS[t] : curG[t];
+                const int4* r4 = reinterpret_cast<const int4*>(rows + (size_t)li * S);
+#pragma unroll
+                for (int q = 0; q < 4; q++) {
+                    if (q < S4) {
+                        int4 v = r4[q];
+                        row[4 * q] = v.x; row[4 * q + 1] = v.y; row[4 * q + 2] = v.z; row[4 * q + 3] = v.w;
+                    }
+                }
+                k = row[0];
             }
-            int k = row[0];
-            for (int q = 1; q <= k; q++) {
-                int c = row[q];
-                unsigned bit = 1u << (c & 31);
-                if (vis[c >> 5] & bit) continue;
-                if (atomicOr(&vis[c >> 5], bit) & bit) continue;
-                ld[c] = d + 1;
-                int pos = atomicAdd(&s_next, 1);
-                if (pos < LBFS_CAP) nxtS[pos] = c;
-                nxtG[pos] = c;
+            // claim the unvisited out-neighbours: plain checks, then the
+            // atomics, all independent so their latencies overlap
+            unsigned cand = 0u;
+#pragma unroll
+            for (int q = 1; q < 16; q++)
+                if (q <= k && !(vis[row[q] >> 5] & (1u << (row[q] & 31)))) cand |= 1u << q;
+            unsigned olds[16];
+#pragma unroll
+            for (int q = 1; q < 16; q++)
+                olds[q] = (cand & (1u << q)) ? atomicOr(&vis[row[q] >> 5], 1u << (row[q] & 31)) : 0xffffffffu;
+#pragma unroll
+            for (int q = 1; q < 16; q++)
+                if ((cand & (1u << q)) && (olds[q] & (1u << (row[q] & 31)))) cand &= ~(1u << q);
+            // warp-aggregated append of the claimed cells
+            const int mine = __popc(cand);
+            int incl = mine;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                int v = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += v;
+            }
+            const int total = __shfl_sync(0xffffffffu, incl, 31);
+            int pos0 = 0;
+            if (lane == 31 && total > 0) pos0 = atomicAdd(cnt, total);
+            pos0 = __shfl_sync(0xffffffffu, pos0, 31);
+            int pos = pos0 + incl - mine;
+#pragma unroll
+            for (int q = 1; q < 16; q++) {
+                if (cand & (1u << q)) {
+                    const int c = row[q];
+                    ld[c] = d + 1;
+                    if (pos < LBFS_CAP) nxtS[pos] = c;
+                    else nxtG[pos] = c;
+                    pos++;
+                }
             }
         }
         __syncthreads();
-        size = s_next;
-        __syncthreads();
-        cur_sh = size <= LBFS_CAP;
+        size = *cnt;
         int* t1 = curS; curS = nxtS; nxtS = t1;
         int* t2 = curG; curG = nxtG; nxtG = t2;
         d++;
         levels++;
+        r++;
     }
     if (tid == 0) *levels_out = levels;
 }
@@ -868,9 +920,19 @@ int group_sum_by_pit(gs_plan* p, const int* /*pit_ids*/, const uint8_t* mask, co
     return GS_OK;
 }
 
+int fill_join(gs_plan* p, gs_stats* st) {
+    if (!p->bfs_pending) return GS_OK;
+    p->bfs_pending = 0;
+    GS_CUDA(cudaStreamWaitEvent(p->stream, p->ev_b, 0));
+    GS_CUDA(cudaEventSynchronize(p->ev_b));
+    if (st) st->flat_rounds = p->h_pinned[2];
+    return GS_OK;
+}
+
 int fill_elevation(gs_plan* p, const double* h, double sealevel, double ofill, double* lfill,
-                   int* pit_ids, int* flat_dirs, gs_stats* st) {
+                   int* pit_ids, int* flat_dirs, gs_stats* st, bool defer_flats, uint8_t* sea_out) {
     const int n = (int)p->n;
+    GS_TRY(fill_join(p, nullptr));
     if (n == 0) { p->npits = 0; return GS_OK; }
     const int B = 256, G = grid_for(n, B);
     int hbuf[4];
@@ -890,7 +952,7 @@ int fill_elevation(gs_plan* p, const double* h, double sealevel, double ofill, d
     GS_LAUNCH();
     for (int round = 0; round < 64; round++) {
         GS_CUDA(cudaMemsetAsync(p->i_scalar + I_CHANGED, 0, sizeof(int), p->stream));
-        for (int r = 0; r < 4; r++) launch(p, k_jump, G, B, n, p->parent, p->i_scalar + I_CHANGED);
+        for (int r = 0; r < 2; r++) launch(p, k_jump, G, B, n, p->parent, p->i_scalar + I_CHANGED);
         GS_LAUNCH();
         GS_TRY(read_ints(p, hbuf, p->i_scalar + I_CHANGED, 1));
         if (!hbuf[0]) break;
@@ -965,12 +1027,21 @@ int fill_elevation(gs_plan* p, const double* h, double sealevel, double ofill, d
            (const int*)p->bestlid, p->pit_info, p->spill_flag);
     GS_LAUNCH();
 
-    // flat distances (fill_dir + nghb_dir fixed point = BFS hop distance)
+    // seaID before the flat pass resets open-sea cells to h (the reset keeps
+    // lFill <= sea level, so the mask is the same before and after it)
+    if (sea_out) GS_TRY(sea_mask(p, lfill, sealevel, sea_out));
+
+    // flat distances (fill_dir + nghb_dir fixed point = BFS hop distance).
+    // The shared-memory BFS and the flat directions run on side_b, beside the
+    // pit tables on the main stream: they share only read-only inputs, and
+    // the sea reset of lFill in k_flat_dirs touches open-sea cells, which
+    // hold no pit.
     GS_CUDA(cudaMemsetAsync(p->i_scalar + I_NEXT, 0, sizeof(int), p->stream));
     launch(p, k_bfs_init, G, B, n, (const int*)p->spill_flag, p->pdir, p->front0, p->i_scalar + I_NEXT);
     GS_LAUNCH();
     GS_TRY(read_ints(p, hbuf, p->i_scalar + I_NEXT, 1));
     int fsize = hbuf[0], levels = 0;
+    bool forked = false;
     if (fsize > 0) {
         // compact the reachable set; use the shared-memory BFS when its
         // visited bitmap fits, the cooperative grid BFS otherwise
@@ -984,26 +1055,40 @@ int fill_elevation(gs_plan* p, const double* h, double sealevel, double ofill, d
         const int M = last[0] + last[1];
         const size_t smem = sizeof(unsigned) * (size_t)((M + 31) / 32) + sizeof(int) * 2 * LBFS_CAP;
         if (smem <= 200 * 1024) {
-            // packed adjacency rows: [count, ids...], stride S ints (16-byte multiple)
-            const int S = ((p->W + 1 + 3) / 4) * 4;
-            int* rows = p->bfs_rows;
-            int* ldv = p->lab;
-            GS_CUDA(cudaMemsetAsync(p->i_scalar + 6, 0, sizeof(int), p->stream));
-            launch(p, k_bfs_local_build, G, B, n, S, (const double*)lfill, (const int*)pit_ids,
-                   (const int*)p->flagbuf, (const int*)p->scanbuf, (const int*)p->nbr, (const int8_t*)p->nnb,
-                   (const int*)p->spill_flag, rows, p->comp, ldv, p->front0, p->i_scalar + 6);
-            GS_LAUNCH();
-            GS_CUDA(cudaFuncSetAttribute(k_bfs_local, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-            cudaEvent_t stop = nullptr;
-            if (p->profiling) prof_begin(p, (const void*)k_bfs_local, &stop);
-            k_bfs_local<<<1, 1024, smem, p->stream>>>(M, S, (const int*)rows, (const int*)p->front0,
-                                                       p->i_scalar + 6, p->front1, p->minseed, ldv,
-                                                       p->i_scalar + 4);
-            if (stop) cudaEventRecord(stop, p->stream);
-            p->launches++;
-            GS_LAUNCH();
-            launch(p, k_bfs_local_scatter, grid_for(M, B), B, M, (const int*)p->comp, (const int*)ldv, p->pdir);
-            GS_LAUNCH();
+            GS_CUDA(cudaEventRecord(p->ev_fork_b, p->stream));
+            GS_CUDA(cudaStreamWaitEvent(p->side_b, p->ev_fork_b, 0));
+            {
+                StreamSwap sw(p, p->side_b, nullptr);
+                // packed adjacency rows: [count, ids...], stride S ints (16-byte multiple)
+                const int S = ((p->W + 1 + 3) / 4) * 4;
+                int* rows = p->bfs_rows;
+                int* ldv = p->lab;
+                GS_CUDA(cudaMemsetAsync(p->i_scalar + 6, 0, sizeof(int), p->stream));
+                launch(p, k_bfs_local_build, G, B, n, S, (const double*)lfill, (const int*)pit_ids,
+                       (const int*)p->flagbuf, (const int*)p->scanbuf, (const int*)p->nbr, (const int8_t*)p->nnb,
+                       (const int*)p->spill_flag, rows, p->comp, ldv, p->front0, p->i_scalar + 6);
+                GS_LAUNCH();
+                GS_CUDA(cudaFuncSetAttribute(k_bfs_local, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+                cudaEvent_t stop = nullptr;
+                if (p->profiling) prof_begin(p, (const void*)k_bfs_local, &stop);
+                k_bfs_local<<<1, 1024, smem, p->stream>>>(M, S, (const int*)rows, (const int*)p->front0,
+                                                           p->i_scalar + 6, p->front1, p->minseed, ldv,
+                                                           p->i_scalar + 4);
+                if (stop) cudaEventRecord(stop, p->stream);
+                p->launches++;
+                GS_LAUNCH();
+                launch(p, k_bfs_local_scatter, grid_for(M, B), B, M, (const int*)p->comp, (const int*)ldv,
+                       p->pdir);
+                launch(p, k_flat_dirs, G, B, n, (const double*)lfill, (const int*)pit_ids, (const int*)p->pdir,
+                       (const int*)p->nbr, (const int8_t*)p->nnb, (const int*)p->spill_flag, sealevel, h,
+                       flat_dirs, lfill);
+                GS_LAUNCH();
+                GS_CUDA(cudaMemcpyAsync(p->h_pinned + 2, p->i_scalar + 4, sizeof(int), cudaMemcpyDeviceToHost,
+                                        p->stream));
+            }
+            GS_CUDA(cudaEventRecord(p->ev_b, p->side_b));
+            p->bfs_pending = 1;
+            forked = true;
         } else {
             launch(p, k_bfs_adj, G, B, n, p->W, (const double*)lfill, (const int*)pit_ids,
                    (const int*)p->spill_flag, (const int*)p->nbr, (const int8_t*)p->nnb, p->xe_u, p->ledge);
@@ -1016,31 +1101,33 @@ int fill_elevation(gs_plan* p, const double* h, double sealevel, double ofill, d
             void* args[] = {(void*)&p->front0, (void*)&p->front1, (void*)&sizes, (void*)&d0, (void*)&nn,
                             (void*)&W, (void*)&p->xe_u, (void*)&p->ledge, (void*)&p->pdir, (void*)&lv};
             GS_TRY(launch_coop(p, (const void*)k_bfs_coop, args));
+            GS_TRY(read_ints(p, hbuf, p->i_scalar + 4, 1));
+            levels = hbuf[0];
         }
-        GS_TRY(read_ints(p, hbuf, p->i_scalar + 4, 1));
-        levels = hbuf[0];
     }
-    if (st) st->flat_rounds = levels;
-    launch(p, k_flat_dirs, G, B, n, (const double*)lfill, (const int*)pit_ids, (const int*)p->pdir,
-           (const int*)p->nbr, (const int8_t*)p->nnb, (const int*)p->spill_flag, sealevel, h,
-           flat_dirs, lfill);
-    GS_LAUNCH();
+    if (!forked) {
+        if (st) st->flat_rounds = levels;
+        launch(p, k_flat_dirs, G, B, n, (const double*)lfill, (const int*)pit_ids, (const int*)p->pdir,
+               (const int*)p->nbr, (const int8_t*)p->nnb, (const int*)p->spill_flag, sealevel, h,
+               flat_dirs, lfill);
+        GS_LAUNCH();
+    }
 
     // pit cells sorted by (pit, id): segments for the per-pit reductions.
     // Ordered compaction (scan) keeps id order; the stable radix sort by pit
     // then lists every pit's cells in increasing id.
     GS_CUDA(cudaMemsetAsync(p->seg_count, 0, sizeof(int) * (np1 + 1), p->stream));
-    launch(p, k_pit_flag, G, B, n, (const int*)pit_ids, p->flagbuf, p->seg_count);
+    launch(p, k_pit_flag, G, B, n, (const int*)pit_ids, p->pflag, p->seg_count);
     GS_LAUNCH();
-    GS_TRY(exclusive_scan(p, p->flagbuf, p->scanbuf, n));
-    launch(p, k_pit_compact, G, B, n, (const int*)pit_ids, (const int*)p->scanbuf, p->seg_keys,
+    GS_TRY(exclusive_scan(p, p->pflag, p->pscan, n));
+    launch(p, k_pit_compact, G, B, n, (const int*)pit_ids, (const int*)p->pscan, p->seg_keys,
            p->seg_vals);
     GS_LAUNCH();
     int ncell = 0;
     {
         int last[2];
-        GS_CUDA(cudaMemcpyAsync(&last[0], p->scanbuf + n - 1, sizeof(int), cudaMemcpyDeviceToHost, p->stream));
-        GS_CUDA(cudaMemcpyAsync(&last[1], p->flagbuf + n - 1, sizeof(int), cudaMemcpyDeviceToHost, p->stream));
+        GS_CUDA(cudaMemcpyAsync(&last[0], p->pscan + n - 1, sizeof(int), cudaMemcpyDeviceToHost, p->stream));
+        GS_CUDA(cudaMemcpyAsync(&last[1], p->pflag + n - 1, sizeof(int), cudaMemcpyDeviceToHost, p->stream));
         GS_CUDA(cudaStreamSynchronize(p->stream));
         ncell = last[0] + last[1];
     }
@@ -1068,6 +1155,7 @@ int fill_elevation(gs_plan* p, const double* h, double sealevel, double ofill, d
         GS_CUDA(cudaStreamSynchronize(p->stream));
         p->level = lv;
     }
+    if (!defer_flats) GS_TRY(fill_join(p, st));
     return GS_OK;
 }
 

@@ -21,6 +21,10 @@ static int dalloc(T** ptr, size_t count) {
     return GS_OK;
 }
 
+struct ScanMax {
+    __device__ __forceinline__ int operator()(int a, int b) const { return a > b ? a : b; }
+};
+
 template <class T>
 static int upload(T** ptr, const std::vector<T>& h) {
     GS_TRY(dalloc(ptr, h.size()));
@@ -39,9 +43,18 @@ static void plan_free(gs_plan* p) {
                     p->pit_in, p->pit_ev, p->pit_win, p->pit_lvl, p->pit_state, p->seg_keys, p->seg_vals,
                     p->seg_keys2, p->seg_vals2, p->seg_start, p->seg_count, p->cub_tmp, p->nfa, p->wf,
                     p->hl, p->dcoef, p->dsea, p->cg_r, p->cg_z, p->cg_p, p->cg_ap, p->cg_x, p->cg_b,
-                    p->red};
+                    p->red, p->cub_tmp2, p->pflag, p->pscan};
     for (void* q : ptrs)
         if (q) cudaFree(q);
+    cudaEvent_t evs[] = {p->ev_fork_a, p->ev_a, p->ev_fork_b, p->ev_b};
+    for (cudaEvent_t e : evs)
+        if (e) cudaEventDestroy(e);
+    for (cudaEvent_t e : p->prof_ev)
+        if (e) cudaEventDestroy(e);
+    p->prof_ev.clear();
+    if (p->side_a) cudaStreamDestroy(p->side_a);
+    if (p->side_b) cudaStreamDestroy(p->side_b);
+    if (p->h_pinned) cudaFreeHost(p->h_pinned);
 }
 
 int plan_create(int64_t nb, const int32_t* nnb, const int32_t* ngb, const double* elgt, const double* vdist,
@@ -234,8 +247,26 @@ int plan_create(int64_t nb, const int32_t* nnb, const int32_t* ngb, const double
                                         0, 64);
         b1 = std::max(b1, b3);
         cub::DeviceScan::ExclusiveSum((void*)nullptr, b2, (const int*)nullptr, (int*)nullptr, (int)N1 + 1);
-        p->cub_bytes = std::max(b1, b2) + 256;
+        size_t b4 = 0;
+        cub::DeviceScan::InclusiveScan((void*)nullptr, b4, (const int*)nullptr, (int*)nullptr, ScanMax(), (int)N1);
+        p->cub_bytes = std::max(std::max(b1, b2), b4) + 256;
         TRYP(dalloc((char**)&p->cub_tmp, p->cub_bytes));
+        TRYP(dalloc((char**)&p->cub_tmp2, p->cub_bytes));
+        TRYP(dalloc(&p->pflag, N1));
+        TRYP(dalloc(&p->pscan, N1));
+    }
+    {
+        cudaError_t e = cudaStreamCreateWithFlags(&p->side_a, cudaStreamNonBlocking);
+        if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&p->side_b, cudaStreamNonBlocking);
+        cudaEvent_t* evs[] = {&p->ev_fork_a, &p->ev_a, &p->ev_fork_b, &p->ev_b};
+        for (cudaEvent_t* ev : evs)
+            if (e == cudaSuccess) e = cudaEventCreateWithFlags(ev, cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaMallocHost((void**)&p->h_pinned, sizeof(int) * 16);
+        if (e != cudaSuccess) {
+            set_error(GS_ECUDA, std::string("plan streams: ") + cudaGetErrorString(e));
+            st = GS_ECUDA;
+            goto fail;
+        }
     }
 #undef TRYP
     {

@@ -108,6 +108,18 @@ struct gs_plan {
     int* seg_count = nullptr;
     void* cub_tmp = nullptr;
     size_t cub_bytes = 0;
+    void* cub_tmp2 = nullptr;            // cub scratch of work issued on side stream A
+    int* pflag = nullptr;                // pit-table compaction flags / scan (main stream)
+    int* pscan = nullptr;
+
+    // side streams: A builds the unfilled-surface receivers and their order
+    // while the main stream fills depressions; B runs the flat-distance BFS
+    // while the main stream builds the pit tables and the first flow sweep.
+    cudaStream_t side_a = nullptr;
+    cudaStream_t side_b = nullptr;
+    cudaEvent_t ev_fork_a = nullptr, ev_a = nullptr, ev_fork_b = nullptr, ev_b = nullptr;
+    int* h_pinned = nullptr;             // pinned host words [16]
+    int bfs_pending = 0;                 // flat BFS issued on side_b, not yet joined
 
     // flow / cascade
     double* nfa = nullptr;
@@ -132,6 +144,7 @@ struct gs_plan {
     std::vector<const void*> prof_fn;
     std::vector<cudaEvent_t> prof_ev;    // start/stop pairs
     std::vector<int> prof_idx;           // kernel index per pair
+    std::vector<int> prof_stream;        // 0 main, 1 side_a, 2 side_b per pair
 };
 
 namespace gs {
@@ -142,13 +155,32 @@ int receivers(gs_plan* p, int nrcv, double exp, const double* elev, double sl, c
 int flow_direction(gs_plan* p, const double* h, bool down, const double* lfill,
                    const int* pit_ids, const int* flat_dirs, double sealevel, int* rcv,
                    double* dist, double* wgt, int8_t* rslot, uint8_t* lsink, uint8_t* sea);
+// the part of flow_direction after the receivers (flat routing, outlets, masks)
+int flow_direction_post(gs_plan* p, const double* h, bool down, const double* lfill, const int* pit_ids,
+                        const int* flat_dirs, double sealevel, int* rcv, double* dist, double* wgt,
+                        int8_t* rslot, uint8_t* lsink, uint8_t* sea);
+// lsink / sea masks for flow_direction(..., lsink = nullptr) graphs
+int sea_mask(gs_plan* p, const double* lfill, double sl, uint8_t* sea);
+int sink_mask(gs_plan* p, const double* wgt, const uint8_t* sea, uint8_t* lsink);
 int flow_solve(gs_plan* p, const int* rcv, const double* wgt, const int8_t* rslot,
                const double* b, double* x, int* cycle_nodes, const double* surface, const int* pdir,
                int* order);
 int spl_sweep(gs_plan* p, const int* rcv, const double* c, const int8_t* rslot, const double* hold,
               double* s, int* cycle_nodes, bool reuse_order);
 int fill_elevation(gs_plan* p, const double* h, double sealevel, double ofill, double* lfill,
-                   int* pit_ids, int* flat_dirs, gs_stats* st);
+                   int* pit_ids, int* flat_dirs, gs_stats* st, bool defer_flats = false,
+                   uint8_t* sea_out = nullptr);
+// joins the flat-distance BFS of the last fill (if it ran on side_b) into the
+// main stream and records its level count
+int fill_join(gs_plan* p, gs_stats* st);
+// topological order of a flow graph: vertices by surface descending
+// (flow_order), then surface ties by flat distance descending (flow_order_ties)
+int flow_order(gs_plan* p, const double* surface, int* order);
+int flow_order_ties(gs_plan* p, const int* pdir, int* order);
+int flow_prepare(gs_plan* p, const int* rcv, const double* wgt, const int8_t* rslot, double* x, const int* order,
+                 int* bad_host);
+int flow_run(gs_plan* p, const int* rcv, const double* wgt, const int8_t* rslot, const double* b,
+             double* x, int* cycle_nodes, int* order, int ok);
 int group_sum_by_pit(gs_plan* p, const int* pit_ids, const uint8_t* mask, const double* vals,
                      double* out, int npits);
 int flow_accumulation(gs_plan* p, const double* h, const double* bl, double sealevel, double ofill,
@@ -166,6 +198,21 @@ int apply_forces(gs_plan* p, double* h, const double* rain, const double* upsub,
 
 void prof_begin(gs_plan* p, const void* fn, cudaEvent_t* stop);
 int coop_occupancy(int* per_sm);
+
+// issues the plan's work on another stream (and cub scratch) for its scope
+struct StreamSwap {
+    gs_plan* p;
+    cudaStream_t s0;
+    void* c0;
+    StreamSwap(gs_plan* p_, cudaStream_t s, void* cub) : p(p_), s0(p_->stream), c0(p_->cub_tmp) {
+        p->stream = s;
+        if (cub) p->cub_tmp = cub;
+    }
+    ~StreamSwap() {
+        p->stream = s0;
+        p->cub_tmp = c0;
+    }
+};
 
 template <class K, class... A>
 inline void launch(gs_plan* p, K kernel, int grid, int block, A... args) {

@@ -174,7 +174,6 @@ __global__ void k_flow_direction_post(int n, int W, int R, int flat, const doubl
                                       double* wgt, int8_t* rslot, uint8_t* lsink, uint8_t* sea) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    const bool is_sea = lfill[i] <= sl;
     if (down) {
         double sw = 0.0;
         for (int k = 0; k < R; k++) sw = sw + wgt[(size_t)k * n + i];
@@ -199,10 +198,43 @@ __global__ void k_flow_direction_post(int n, int W, int R, int flat, const doubl
             rslot[(size_t)k * n + i] = -1;
         }
     }
+    if (!lsink) return;  // graph only: the masks are set by k_sink_mask once lFill exists
+    const bool is_sea = lfill[i] <= sl;
     double sw = 0.0;
     for (int k = 0; k < R; k++) sw = sw + wgt[(size_t)k * n + i];
     lsink[i] = (sw == 0.0 && !outlet[i] && !is_sea) ? 1 : 0;
     sea[i] = is_sea ? 1 : 0;
+}
+
+// seaID (lFill <= sea level, flowplex.py:493) as a mask
+__global__ void k_sea_mask(int n, const double* __restrict__ lfill, double sl, uint8_t* sea) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) sea[i] = lfill[i] <= sl ? 1 : 0;
+}
+
+// lsink (flowplex.py:531-540) from the weights and a precomputed sea mask
+__global__ void k_sink_mask(int n, int R, const double* __restrict__ wgt, const uint8_t* __restrict__ outlet,
+                            const uint8_t* __restrict__ sea, uint8_t* lsink) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double sw = 0.0;
+    for (int k = 0; k < R; k++) sw = sw + wgt[(size_t)k * n + i];
+    lsink[i] = (sw == 0.0 && !outlet[i] && !sea[i]) ? 1 : 0;
+}
+
+int sea_mask(gs_plan* p, const double* lfill, double sl, uint8_t* sea) {
+    if (p->n == 0) return GS_OK;
+    launch(p, k_sea_mask, grid_for(p->n, 256), 256, (int)p->n, lfill, sl, sea);
+    GS_LAUNCH();
+    return GS_OK;
+}
+
+int sink_mask(gs_plan* p, const double* wgt, const uint8_t* sea, uint8_t* lsink) {
+    if (p->n == 0) return GS_OK;
+    launch(p, k_sink_mask, grid_for(p->n, 256), 256, (int)p->n, p->R, wgt, (const uint8_t*)p->outlet, sea,
+           lsink);
+    GS_LAUNCH();
+    return GS_OK;
 }
 
 int receivers(gs_plan* p, int nrcv, double exp, const double* elev, double sl, const int* gid,
@@ -222,6 +254,12 @@ int flow_direction(gs_plan* p, const double* h, bool down, const double* lfill, 
                    const int* flat_dirs, double sealevel, int* rcv, double* dist, double* wgt,
                    int8_t* rslot, uint8_t* lsink, uint8_t* sea) {
     GS_TRY(receivers(p, p->R, 1.1, h, sealevel, p->gid, rcv, dist, wgt, rslot));
+    return flow_direction_post(p, h, down, lfill, pit_ids, flat_dirs, sealevel, rcv, dist, wgt, rslot, lsink, sea);
+}
+
+int flow_direction_post(gs_plan* p, const double* h, bool down, const double* lfill, const int* pit_ids,
+                        const int* flat_dirs, double sealevel, int* rcv, double* dist, double* wgt,
+                        int8_t* rslot, uint8_t* lsink, uint8_t* sea) {
     if (p->n == 0) return GS_OK;
     launch(p, k_flow_direction_post, grid_for(p->n, 256), 256, (int)p->n, p->W, p->R, p->flat, h,
            down ? 1 : 0, lfill, pit_ids, flat_dirs, sealevel, p->outlet, p->nbr, rcv, dist, wgt,

@@ -608,41 +608,113 @@ __global__ void __launch_bounds__(128) k_ordered(Op op, int n, const int* __rest
 
 // sort vertices by (surface desc, flat distance desc); returns 1 when the
 // order is topological for the given flow edges
-static int build_order(gs_plan* p, const double* z, const int* pdir, const int* rcv, const double* w,
-                       int* order, int* ok) {
+// Tie groups of the surface-sorted order: run start of every position (max-
+// scanned afterwards) and the membership flag of runs longer than one.
+__global__ void k_tie_runs(int n, const unsigned long long* __restrict__ skey, int* run, int* flag) {
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const unsigned long long k = skey[t];
+    const bool first = t == 0 || skey[t - 1] != k;
+    const bool last = t == n - 1 || skey[t + 1] != k;
+    run[t] = first ? t : 0;
+    flag[t] = (first && last) ? 0 : 1;
+}
+
+// tie members as (run start, descending flat distance) keys, in position order
+__global__ void k_tie_compact(int n, const int* __restrict__ run, const int* __restrict__ flag,
+                              const int* __restrict__ scan, const int* __restrict__ order,
+                              const int* __restrict__ pdir, unsigned long long* ckey, int* cval, int* cpos) {
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n || !flag[t]) return;
+    const int j = scan[t];
+    const int v = order[t];
+    ckey[j] = ((unsigned long long)(unsigned)run[t] << 32) | (unsigned long long)(~(unsigned)(pdir[v] + 1));
+    cval[j] = v;
+    cpos[j] = t;
+}
+
+__global__ void k_tie_scatter(int m, const int* __restrict__ cpos, const int* __restrict__ cval, int* order) {
+    int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j < m) order[cpos[j]] = cval[j];
+}
+
+struct MaxOp {
+    __device__ __forceinline__ int operator()(int a, int b) const { return a > b ? a : b; }
+};
+
+// Vertices by surface descending (ties by vertex id): keys and one stable
+// 64-bit radix sort.  The sorted keys stay in okey2 for order_ties.
+static int order_by_surface(gs_plan* p, const double* z, int* order) {
     const int n = (int)p->n;
     const int B = 256, G = grid_for(n, B);
-    unsigned long long* key = p->okey;
-    unsigned long long* key_out = p->okey2;
-    unsigned* key2 = p->ok32;
-    unsigned* key2_out = p->ok32b;
-    int* val = p->oval;
-    int* val2 = p->oval2;
-    launch(p, k_order_keys, G, B, n, z, pdir, key, key2, val);
+    launch(p, k_order_keys, G, B, n, z, (const int*)nullptr, p->okey, p->ok32, p->oval);
     GS_LAUNCH();
     size_t bytes = p->cub_bytes;
-    if (pdir) {
-        GS_CUDA(cub::DeviceRadixSort::SortPairs(p->cub_tmp, bytes, key2, key2_out, val, val2, n, 0, 32, p->stream));
-        p->launches++;
-        // gather primary keys in the new order
-        launch(p, k_gather_u64, G, B, n, (const unsigned long long*)key, (const int*)val2, key_out);
-        GS_CUDA(cub::DeviceRadixSort::SortPairs(p->cub_tmp, bytes, key_out, key, val2, order, n, 0, 64,
-                                                p->stream));
-    } else {
-        GS_CUDA(cub::DeviceRadixSort::SortPairs(p->cub_tmp, bytes, key, key_out, val, order, n, 0, 64,
-                                                p->stream));
-    }
+    GS_CUDA(cub::DeviceRadixSort::SortPairs(p->cub_tmp, bytes, p->okey, p->okey2, p->oval, order, n, 0, 64,
+                                            p->stream));
     p->launches++;
-    launch(p, k_positions, G, B, n, (const int*)order, p->pos);
+    return GS_OK;
+}
+
+// Breaks the surface ties of order_by_surface by flat distance descending
+// (ties of both by vertex id): only the members of tie groups are re-sorted,
+// by (group start, ~(pdir + 1)), and written back to their positions.  Gives
+// the order of a stable sort by (surface desc, pdir desc).
+static int order_ties(gs_plan* p, const int* pdir, int* order) {
+    const int n = (int)p->n;
+    const int B = 256, G = grid_for(n, B);
+    int* run0 = p->oval;
+    int* run = (int*)p->ok32b;
+    int* flag = p->oval2;
+    int* scan = (int*)p->ok32;
+    launch(p, k_tie_runs, G, B, n, (const unsigned long long*)p->okey2, run0, flag);
+    GS_LAUNCH();
+    size_t bytes = p->cub_bytes;
+    GS_CUDA(cub::DeviceScan::InclusiveScan(p->cub_tmp, bytes, run0, run, MaxOp(), n, p->stream));
+    p->launches++;
+    bytes = p->cub_bytes;
+    GS_CUDA(cub::DeviceScan::ExclusiveSum(p->cub_tmp, bytes, flag, scan, n, p->stream));
+    p->launches++;
+    int last[2];
+    GS_CUDA(cudaMemcpyAsync(&last[0], scan + n - 1, sizeof(int), cudaMemcpyDeviceToHost, p->stream));
+    GS_CUDA(cudaMemcpyAsync(&last[1], flag + n - 1, sizeof(int), cudaMemcpyDeviceToHost, p->stream));
+    GS_CUDA(cudaStreamSynchronize(p->stream));
+    const int m = last[0] + last[1];
+    if (m == 0) return GS_OK;
+    int* cval = p->oval;
+    int* cval2 = (int*)p->ok32b;
+    int* cpos = p->pos;  // rewritten by the positions pass that follows
+    launch(p, k_tie_compact, G, B, n, (const int*)run, (const int*)flag, (const int*)scan, (const int*)order, pdir,
+           p->okey, cval, cpos);
+    GS_LAUNCH();
+    int hb = 1;
+    while ((1LL << hb) <= (long long)n && hb < 31) hb++;
+    bytes = p->cub_bytes;
+    GS_CUDA(cub::DeviceRadixSort::SortPairs(p->cub_tmp, bytes, p->okey, p->okey2, cval, cval2, m, 0, 32 + hb,
+                                            p->stream));
+    p->launches++;
+    launch(p, k_tie_scatter, grid_for(m, B), B, m, (const int*)cpos, (const int*)cval2, order);
+    GS_LAUNCH();
+    return GS_OK;
+}
+
+// Checks that every weighted edge goes forward in `order`; the result
+// (nonzero = not a topological order) is copied to the pinned host word
+// bad_host without synchronising.
+static int order_check_async(gs_plan* p, const int* rcv, const double* w, const int* order, int* bad_host) {
+    const int n = (int)p->n;
+    const int B = 256, G = grid_for(n, B);
+    launch(p, k_positions, G, B, n, order, p->pos);
     GS_CUDA(cudaMemsetAsync(p->i_scalar + 14, 0, sizeof(int), p->stream));
     launch(p, k_check_order, G, B, n, p->R, rcv, w, (const int*)p->pos, p->i_scalar + 14);
     GS_LAUNCH();
-    int bad = 0;
-    GS_CUDA(cudaMemcpyAsync(&bad, p->i_scalar + 14, sizeof(int), cudaMemcpyDeviceToHost, p->stream));
-    GS_CUDA(cudaStreamSynchronize(p->stream));
-    *ok = bad ? 0 : 1;
+    GS_CUDA(cudaMemcpyAsync(bad_host, p->i_scalar + 14, sizeof(int), cudaMemcpyDeviceToHost, p->stream));
     return GS_OK;
 }
+
+int flow_order(gs_plan* p, const double* surface, int* order) { return order_by_surface(p, surface, order); }
+
+int flow_order_ties(gs_plan* p, const int* pdir, int* order) { return order_ties(p, pdir, order); }
 
 static int ordered_status(gs_plan* p, int* st) {
     unsigned h[8];
@@ -652,21 +724,32 @@ static int ordered_status(gs_plan* p, int* st) {
     return GS_OK;
 }
 
-int flow_solve(gs_plan* p, const int* rcv, const double* wgt, const int8_t* rslot, const double* b, double* x,
-               int* cycle_nodes, const double* surface, const int* pdir, int* order) {
+// Everything of an ordered flow sweep that does not need b, for an order
+// built by flow_order (+ flow_order_ties): its check (result in *bad_host once
+// the stream reaches it), the donor masks and the sentinel-filled output.
+int flow_prepare(gs_plan* p, const int* rcv, const double* wgt, const int8_t* rslot, double* x, const int* order,
+                 int* bad_host) {
     const int n = (int)p->n;
-    *cycle_nodes = 0;
     if (n == 0) return GS_OK;
-    int ok = 0;
-    if (surface) GS_TRY(build_order(p, surface, pdir, rcv, wgt, order, &ok));
-    if (order == p->order_i) p->order_i_valid = ok;
-    if (!ok) return flow_solve_counted(p, rcv, wgt, rslot, b, x, cycle_nodes);
+    GS_TRY(order_check_async(p, rcv, wgt, order, bad_host));
     GS_CUDA(cudaMemsetAsync(p->don_mask, 0, sizeof(uint32_t) * n, p->stream));
     GS_CUDA(cudaMemsetAsync(p->don_k, 0, sizeof(unsigned long long) * n, p->stream));
-    GS_CUDA(cudaMemsetAsync(p->ctr, 0, sizeof(unsigned) * 8, p->stream));
     launch(p, k_flow_donors, grid_for(n, 256), 256, n, p->R, rcv, wgt, rslot, (const int8_t*)p->rev, p->don_mask,
            p->don_k);
     launch(p, k_fill_sent, grid_for(n, 256), 256, n, x);
+    GS_LAUNCH();
+    return GS_OK;
+}
+
+// The sweep proper, after flow_prepare: the ordered kernel when the order is
+// valid (ok), else the counter-based dataflow solve.
+int flow_run(gs_plan* p, const int* rcv, const double* wgt, const int8_t* rslot, const double* b, double* x,
+             int* cycle_nodes, int* order, int ok) {
+    const int n = (int)p->n;
+    *cycle_nodes = 0;
+    if (n == 0) return GS_OK;
+    if (!ok) return flow_solve_counted(p, rcv, wgt, rslot, b, x, cycle_nodes);
+    GS_CUDA(cudaMemsetAsync(p->ctr, 0, sizeof(unsigned) * 8, p->stream));
     FlowOrd op{n, p->nbr, p->don_mask, p->don_k, p->sorder, wgt, b, x};
     launch(p, k_ordered<FlowOrd>, p->sm_count * 8, 128, op, n, (const int*)order, p->ctr, SWEEP_BUDGET_NS);
     GS_LAUNCH();
@@ -677,6 +760,23 @@ int flow_solve(gs_plan* p, const int* rcv, const double* wgt, const int8_t* rslo
         return st;
     }
     return GS_OK;
+}
+
+int flow_solve(gs_plan* p, const int* rcv, const double* wgt, const int8_t* rslot, const double* b, double* x,
+               int* cycle_nodes, const double* surface, const int* pdir, int* order) {
+    const int n = (int)p->n;
+    *cycle_nodes = 0;
+    if (n == 0) return GS_OK;
+    int ok = 0;
+    if (surface) {
+        GS_TRY(order_by_surface(p, surface, order));
+        if (pdir) GS_TRY(order_ties(p, pdir, order));
+        GS_TRY(flow_prepare(p, rcv, wgt, rslot, x, order, p->h_pinned));
+        GS_CUDA(cudaStreamSynchronize(p->stream));
+        ok = p->h_pinned[0] ? 0 : 1;
+    }
+    if (order == p->order_i) p->order_i_valid = ok;
+    return flow_run(p, rcv, wgt, rslot, b, x, cycle_nodes, order, ok);
 }
 
 // SPL edges i -> rcv (c != 0) run against the flow order: need pos[rcv] > pos[i]

@@ -221,10 +221,46 @@ def planar_config(n=20000, side=100.0e3, seed=20261204, zmax=50.0):
     return coords, cells, z, np.ones(len(z)), up, params
 
 
+def morton_order(coords):
+    """Vertex permutation along a 3-D Morton (Z-order) curve of the positions,
+    21 bits per axis over the bounding box: consecutive ids become spatial
+    neighbours, so the neighbour gathers of every kernel hit the same cache
+    lines."""
+    lo = coords.min(axis=0)
+    span = np.maximum(coords.max(axis=0) - lo, 1e-300)
+    q = np.clip(((coords - lo) / span * ((1 << 21) - 1)).astype(np.uint64), 0, (1 << 21) - 1)
+
+    def spread(x):
+        x = x & np.uint64(0x1fffff)
+        x = (x | (x << np.uint64(32))) & np.uint64(0x1f00000000ffff)
+        x = (x | (x << np.uint64(16))) & np.uint64(0x1f0000ff0000ff)
+        x = (x | (x << np.uint64(8))) & np.uint64(0x100f00f00f00f00f)
+        x = (x | (x << np.uint64(4))) & np.uint64(0x10c30c30c30c30c3)
+        x = (x | (x << np.uint64(2))) & np.uint64(0x1249249249249249)
+        return x
+
+    key = spread(q[:, 0]) | (spread(q[:, 1]) << np.uint64(1)) | (spread(q[:, 2]) << np.uint64(2))
+    return np.argsort(key, kind="stable")
+
+
+def renumber(coords, cells, order):
+    """Mesh with vertex i of the result = vertex order[i] of the input; cells
+    sorted by their smallest new vertex id."""
+    inv = np.empty(len(order), np.int64)
+    inv[order] = np.arange(len(order))
+    c2 = inv[cells]
+    c2 = c2[np.argsort(c2.min(axis=1), kind="stable")]
+    return coords[order], c2.astype(cells.dtype)
+
+
 def sphere_config(level=9, seed=20261205, lmax=256, zlo=-4000.0, zhi=3000.0, steps=50, dt=1.0e4,
-                  K=5.0e-7, kd=0.05):
-    """Icosahedral sphere: SH(l<=lmax, l^-2) relief, lognormal rain, three uplift belts."""
+                  K=5.0e-7, kd=0.05, ordered=True):
+    """Icosahedral sphere: SH(l<=lmax, l^-2) relief, lognormal rain, three uplift
+    belts.  With `ordered` the vertices are numbered along a Morton curve
+    (the same landscape; only the numbering differs)."""
     coords, cells = icosphere(level)
+    if ordered:
+        coords, cells = renumber(coords, cells, morton_order(coords))
     z = rescale(sh_field(coords, lmax, seed + 1), zlo, zhi)
     g = sh_field(coords, 32, seed + 2)
     g = (g - g.mean()) / g.std()

@@ -74,6 +74,10 @@ int gs_plan_profile(gs_plan* plan, int32_t enable);
 /* Writes "kernel_name launches total_ms" lines for the recorded launches into
  * buf (synchronises the plan's stream); returns the report length. */
 int gs_plan_profile_report(gs_plan* plan, char* buf, int64_t len);
+/* Writes one "kernel_name stream start_ms end_ms" line per recorded launch
+ * (stream 0 = the plan's stream, 1 and 2 = its two internal side streams;
+ * times from the first recorded launch; synchronises the device). */
+int gs_plan_profile_trace(gs_plan* plan, char* buf, int64_t len);
 
 /*
  * Finite-volume geometry of a triangulated mesh (init-time), replacing the
