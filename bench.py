@@ -167,6 +167,9 @@ def main():
     ap.add_argument("--level", type=int, default=9)
     ap.add_argument("--cpu-level", type=int, default=7)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--workload", default="sphere", choices=["sphere", "ensemble"])
+    ap.add_argument("--members", type=int, default=256)
+    ap.add_argument("--loop", action="store_true", help="ensemble: also time the per-member loop")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -190,11 +193,27 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
         pg = dist
     t_setup = time.perf_counter()
-    c, f, z, rain, up, p = sphere_inputs(args.level)
-    p = dict(p, rain=rain, upsub=up, tEnd=1.0e30)
-    mesh = FVMesh(c, f, p["bc"], device=dev)
-    model = Model(coords=c, cells=f, elev=z, params=p, mesh=mesh, device=dev)
+    ens_members = None
+    if args.workload == "sphere":
+        c, f, z, rain, up, p = sphere_inputs(args.level)
+        p = dict(p, rain=rain, upsub=up, tEnd=1.0e30)
+        mesh = FVMesh(c, f, p["bc"], device=dev)
+        model = Model(coords=c, cells=f, elev=z, params=p, mesh=mesh, device=dev)
+    else:
+        from gospl_b200 import synthetic as S
+        from gospl_b200.ensemble import Ensemble, partition
+        sizes = S.ensemble_sizes(256)[:args.members]
+        mine = partition(sizes, world)[rank]
+        ens_members = [S.ensemble_member(int(sizes[i]), 20261300 + i) for i in mine]
+        ens_members = [(c, f, z, r, u, dict(p, tEnd=1.0e30)) for c, f, z, r, u, p in ens_members]
+        ens = Ensemble(ens_members, device=dev)
+        model = ens.model
     n = model.lpoints
+    n_all = n
+    if pg is not None:
+        t = torch.tensor([n], dtype=torch.int64, device=dev)
+        pg.all_reduce(t)
+        n_all = int(t.item())
     setup_s = time.perf_counter() - t_setup
     stream = torch.cuda.current_stream(dev)
     L = _lib.load()
@@ -225,7 +244,7 @@ def main():
         t = torch.tensor([ms], dtype=torch.float64, device=dev)
         pg.all_reduce(t, op=pg.ReduceOp.MAX)
         ms = float(t.item())
-    value = world * n * args.steps / (ms / 1000.0)
+    value = n_all * args.steps / (ms / 1000.0)
 
     # ---- per-kernel times (same steps, events around every launch) ----
     L.gs_plan_profile(model._plan, 1)
@@ -257,7 +276,7 @@ def main():
         t = torch.tensor([ms_e2e], dtype=torch.float64, device=dev)
         pg.all_reduce(t, op=pg.ReduceOp.MAX)
         ms_e2e = float(t.item())
-    e2e = world * n * args.steps / (ms_e2e / 1000.0)
+    e2e = n_all * args.steps / (ms_e2e / 1000.0)
 
     # ---- roofline of the dominant kernel ----
     hbm, src = peaks()
@@ -276,22 +295,47 @@ def main():
     step_bytes = step_algo_bytes(layout)
     step_gbs = step_bytes / (ms / args.steps / 1000.0) / 1e9
 
+    loop = None
+    if ens_members is not None and args.loop:
+        # the same members as separate models, stepped one after the other
+        models = [Model(coords=c, cells=f, elev=z, params=dict(p, rain=r, upsub=u), device=dev,
+                        mesh=FVMesh(c, f, p["bc"], device=dev)) for c, f, z, r, u, p in ens_members]
+        for _ in range(args.warmup):
+            for m in models:
+                m.step()
+        barrier()
+        e4 = torch.cuda.Event(enable_timing=True)
+        e5 = torch.cuda.Event(enable_timing=True)
+        e4.record(stream)
+        for _ in range(args.steps):
+            for m in models:
+                m.step()
+        e5.record(stream)
+        torch.cuda.synchronize(dev)
+        ms_loop = e4.elapsed_time(e5)
+        if pg is not None:
+            t = torch.tensor([ms_loop], dtype=torch.float64, device=dev)
+            pg.all_reduce(t, op=pg.ReduceOp.MAX)
+            ms_loop = float(t.item())
+        loop = {"value": n_all * args.steps / (ms_loop / 1000.0), "ms_per_step": ms_loop / args.steps,
+                "what": "the same members as separate models stepped one after another on the same GPU(s)"}
+        for m in models:
+            m.destroy()
+
     cpu = None
-    if rank == 0 and not args.no_cpu:
+    if rank == 0 and not args.no_cpu and ens_members is None:
         v, nn, st, dt = cpu_sample(args.cpu_level, 2)
         cpu = {"value": v, "unit": "vertex-steps/s", "cores": 1, "kind": "port",
                "sample": "oracle (C + numpy restatement of the reference path) on icosphere level %d "
                          "(%d vertices), %d physics steps, %.1f s" % (args.cpu_level, nn, st, dt)}
     if rank == 0:
         line = {
-            "metric": METRIC, "value": value, "unit": "vertex-steps/s", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "metric": METRIC if args.workload == "sphere" else "landscape vertex-steps/s, planar ensemble",
+            "value": value, "unit": "vertex-steps/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "weak" if args.workload == "sphere" else "strong",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded sphere, SH relief)",
-            "config": {"workload": "sphere level %d (%d vertices), full physics step: receivers, pit fill, "
-                                   "flow accumulation + lake cascade, SPL, hillslope, forcing" % (args.level, n),
-                       "vertices": n, "global_batch": world, "seq_len": 0,
-                       "parallelism": "replicas" if world > 1 else "single",
-                       "l2": "working set > 126 MB L2 (mesh arrays alone ~1 GB)"},
+            "config": config_of(args, n, n_all, world),
             "e2e": {"value": e2e, "unit": "vertex-steps/s", "h2d_bytes_per_step": 8 * n, "d2h_bytes_per_step": 8 * n},
             "roofline": {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": hbm,
                          "unit": "GB/s", "frac": (achieved / hbm) if achieved else None,
@@ -306,12 +350,28 @@ def main():
             "clocks": clocks,
             "cpu_baseline": cpu,
             "stats": stats.get("flow"),
+            "loop_baseline": loop,
             "setup_s": setup_s,
         }
         print(json.dumps(line), flush=True)
     if pg is not None:
         pg.barrier()
         pg.destroy_process_group()
+
+
+def config_of(args, n, n_all, world):
+    if args.workload == "sphere":
+        return {"workload": "sphere level %d (%d vertices), full physics step: receivers, pit fill, "
+                            "flow accumulation + lake cascade, SPL, hillslope, forcing" % (args.level, n),
+                "vertices": n, "global_batch": world, "seq_len": 0,
+                "parallelism": "replicas" if world > 1 else "single",
+                "l2": "working set > 126 MB L2 (mesh arrays alone ~1 GB)"}
+    return {"workload": "ensemble of %d planar landscapes (%d vertices in all; sizes log-uniform 1e4-5e5, "
+                        "250 m spacing, own K and rain), full physics step, all members per launch"
+                        % (args.members, n_all),
+            "vertices": n_all, "global_batch": args.members, "seq_len": 0,
+            "parallelism": "members sharded over %d GPU(s)" % world,
+            "l2": "working set > 126 MB L2"}
 
 
 def _short(name):

@@ -84,6 +84,13 @@ int gs_plan_create(int64_t nb, const int32_t* nnb, const int32_t* ngb, const dou
 
 int gs_plan_destroy(gs_plan* plan) { GS_GUARD(return gs::plan_destroy(plan);) }
 
+int gs_plan_set_members(gs_plan* plan, int32_t nmem, const int64_t* start, const double* maxarea) {
+    NEED(plan);
+    NEED(start);
+    NEED(maxarea);
+    GS_GUARD(return gs::set_members(plan, nmem, start, maxarea);)
+}
+
 int gs_plan_set_stream(gs_plan* plan, void* stream) {
     NEED(plan);
     plan->stream = (cudaStream_t)stream;

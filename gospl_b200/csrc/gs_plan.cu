@@ -52,6 +52,7 @@ static void plan_free(gs_plan* p) {
     for (cudaEvent_t e : p->prof_ev)
         if (e) cudaEventDestroy(e);
     p->prof_ev.clear();
+    free_members(p);
     if (p->side_a) cudaStreamDestroy(p->side_a);
     if (p->side_b) cudaStreamDestroy(p->side_b);
     if (p->h_pinned) cudaFreeHost(p->h_pinned);
@@ -277,12 +278,96 @@ int plan_create(int64_t nb, const int32_t* nnb, const int32_t* ngb, const double
             goto fail;
         }
     }
+    {
+        const int64_t st0[2] = {0, (int64_t)n};
+        const double ma0[1] = {maxarea};
+        int r = set_members(p, 1, st0, ma0);
+        if (r != GS_OK) {
+            st = r;
+            goto fail;
+        }
+    }
     *out = p;
     return GS_OK;
 fail:
     plan_free(p);
     delete p;
     return st;
+}
+
+void free_members(gs_plan* p) {
+    void* ptrs[] = {p->vmember, p->pmember, p->chunk_lo, p->mchunk0, p->chunk_part, p->mact, p->mbig,
+                    p->msolve, p->mlakes, p->mflags, p->mresid, p->mmax, p->lsink_prev};
+    for (void* q : ptrs)
+        if (q) cudaFree(q);
+    if (p->h_mflags) cudaFreeHost(p->h_mflags);
+    if (p->h_mresid) cudaFreeHost(p->h_mresid);
+    p->vmember = p->pmember = p->chunk_lo = p->mchunk0 = nullptr;
+    p->chunk_part = nullptr;
+    p->mact = p->mbig = p->msolve = p->mlakes = nullptr;
+    p->mflags = nullptr;
+    p->mresid = nullptr;
+    p->mmax = nullptr;
+    p->lsink_prev = nullptr;
+    p->h_mflags = nullptr;
+    p->h_mresid = nullptr;
+}
+
+__global__ void k_fill_member(int lo, int hi, int m, int* vmember) {
+    int i = lo + blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < hi) vmember[i] = m;
+}
+
+// Members are contiguous vertex ranges [start[m], start[m+1]); every
+// reduction over a member runs over chunks of at most 65536 of its vertices
+// in a fixed order.
+int set_members(gs_plan* p, int nmem, const int64_t* start, const double* maxarea) {
+    const int64_t n = p->n;
+    if (nmem < 1 || !start || !maxarea || start[0] != 0 || start[nmem] != n) {
+        set_error(GS_EINVAL, "members: need start[0] = 0, start[nmem] = nb and nmem >= 1");
+        return GS_EINVAL;
+    }
+    for (int m = 0; m < nmem && n > 0; m++)
+        if (start[m + 1] <= start[m]) {
+            set_error(GS_EINVAL, "members: every member needs at least one vertex");
+            return GS_EINVAL;
+        }
+    free_members(p);
+    p->nmem = nmem;
+    p->mstart.assign(start, start + nmem + 1);
+    p->mmaxarea.assign(maxarea, maxarea + nmem);
+    const int64_t CH = 65536;
+    std::vector<int> lo, m0;
+    for (int m = 0; m < nmem; m++) {
+        m0.push_back((int)lo.size());
+        for (int64_t a = start[m]; a < start[m + 1]; a += CH) lo.push_back((int)a);
+    }
+    m0.push_back((int)lo.size());
+    p->nchunk = (int)lo.size();
+    lo.push_back((int)n);
+    const size_t N = (size_t)std::max<int64_t>(n, 1);
+    GS_TRY(dalloc(&p->vmember, N));
+    GS_TRY(dalloc(&p->pmember, N + 1));
+    GS_TRY(upload(&p->chunk_lo, lo));
+    GS_TRY(upload(&p->mchunk0, m0));
+    GS_TRY(dalloc(&p->chunk_part, (size_t)p->nchunk + 1));
+    GS_TRY(dalloc(&p->mact, (size_t)nmem));
+    GS_TRY(dalloc(&p->mbig, (size_t)nmem));
+    GS_TRY(dalloc(&p->msolve, (size_t)nmem));
+    GS_TRY(dalloc(&p->mlakes, (size_t)nmem));
+    GS_TRY(dalloc(&p->mflags, (size_t)nmem));
+    GS_TRY(dalloc(&p->mresid, (size_t)nmem));
+    GS_TRY(dalloc(&p->mmax, (size_t)nmem));
+    GS_TRY(dalloc(&p->lsink_prev, N));
+    GS_CUDA(cudaMallocHost((void**)&p->h_mflags, sizeof(int) * nmem));
+    GS_CUDA(cudaMallocHost((void**)&p->h_mresid, sizeof(double) * nmem));
+    for (int m = 0; m < nmem; m++) {
+        const int a = (int)start[m], b = (int)start[m + 1];
+        if (b > a) k_fill_member<<<(b - a + 255) / 256, 256, 0, p->stream>>>(a, b, m, p->vmember);
+    }
+    GS_CUDA(cudaGetLastError());
+    GS_CUDA(cudaStreamSynchronize(p->stream));
+    return GS_OK;
 }
 
 int plan_destroy(gs_plan* p) {

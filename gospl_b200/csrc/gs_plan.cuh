@@ -126,6 +126,29 @@ struct gs_plan {
     double* wf = nullptr;                // waterFilled (absolute)
     double* hl = nullptr;                // copy of h
 
+    // landscape members (independent meshes packed into one plan; contiguous
+    // vertex ranges).  One member covering every vertex unless
+    // gs_plan_set_members says otherwise.
+    int nmem = 1;
+    std::vector<int64_t> mstart;         // host [nmem+1]
+    std::vector<double> mmaxarea;        // host [nmem]: largest cell area per member
+    int* vmember = nullptr;              // [n] member of each vertex
+    int* pmember = nullptr;              // [n+1] member of each pit
+    int nchunk = 0;                      // reduction chunks (never straddle members)
+    int* chunk_lo = nullptr;             // [nchunk+1]
+    int* mchunk0 = nullptr;              // [nmem+1] first chunk of each member
+    double* chunk_part = nullptr;        // [nchunk]
+    uint8_t* mact = nullptr;             // [nmem] member still in the cascade loop
+    uint8_t* mbig = nullptr;             // [nmem] member rebuilt its receivers this pass
+    uint8_t* msolve = nullptr;           // [nmem] member solves this pass
+    uint8_t* mlakes = nullptr;           // [nmem] member has pit volume
+    int* mflags = nullptr;               // [nmem] per-pass flags
+    double* mresid = nullptr;            // [nmem]
+    unsigned long long* mmax = nullptr;  // [nmem] max FAL key
+    int* h_mflags = nullptr;             // pinned host [nmem]
+    double* h_mresid = nullptr;          // pinned host [nmem]
+    uint8_t* lsink_prev = nullptr;       // [n]
+
     // diffusion
     double* dcoef = nullptr;             // [W+1][n]: diag then off-diagonals
     uint8_t* dsea = nullptr;             // sea mask the matrix was built for
@@ -198,6 +221,8 @@ int apply_forces(gs_plan* p, double* h, const double* rain, const double* upsub,
 
 void prof_begin(gs_plan* p, const void* fn, cudaEvent_t* stop);
 int coop_occupancy(int* per_sm);
+int set_members(gs_plan* p, int nmem, const int64_t* start, const double* maxarea);
+void free_members(gs_plan* p);
 
 // issues the plan's work on another stream (and cub scratch) for its scope
 struct StreamSwap {

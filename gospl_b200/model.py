@@ -44,10 +44,12 @@ class Model:
     (``Model(coords=..., cells=..., elev=..., params=...)``).  ``params`` keys:
     dt, tStart, tEnd, flowDir, K (scalar or per-vertex), d, m, Cda, Cdm, oFill,
     sealevel, bc, rain (per-vertex m/yr), upsub (per-vertex m/yr or None).
+    ``members`` = (start, maxarea) declares the mesh a disjoint union of
+    landscapes (``gospl_b200.ensemble``).
     """
 
     def __init__(self, filename=None, *, coords=None, cells=None, elev=None, params=None, mesh=None,
-                 device="cuda", init_flow=True, cg_rtol=1.0e-13, cg_maxit=2000):
+                 device="cuda", init_flow=True, cg_rtol=1.0e-13, cg_maxit=2000, members=None):
         import torch
 
         if not torch.cuda.is_available():
@@ -130,6 +132,11 @@ class Model:
         self._plan = handle
         self.stream = torch.cuda.current_stream(self.dev)
         _lib.check(L.gs_plan_set_stream(self._plan, ctypes.c_void_p(self.stream.cuda_stream)))
+        if members is not None:
+            # (start [nmem+1], maxarea [nmem]): landscapes packed in this mesh
+            start = np.ascontiguousarray(members[0], np.int64)
+            marea = np.ascontiguousarray(members[1], np.float64)
+            _lib.check(L.gs_plan_set_members(self._plan, len(marea), _lib.ptr(start), _lib.ptr(marea)))
         self.applyForces()
         if init_flow:
             self.flowAccumulation()

@@ -65,6 +65,18 @@ int gs_plan_create(int64_t nb, const int32_t* nnb, const int32_t* ngb, const dou
                    const int32_t* outlet_ids, int64_t n_outlet, const int32_t* open_ids,
                    int64_t n_open, int32_t flat_model, int32_t flow_dir, gs_plan** out);
 int gs_plan_destroy(gs_plan* plan);
+/*
+ * Landscape members.  No counterpart in the reference (goSPL runs one
+ * landscape per model).  A plan built over the disjoint union of several
+ * meshes (member m = vertices [start[m], start[m+1]), no edge between
+ * members) advances them all with one launch per stage while each member
+ * keeps its own control flow: the lake-cascade loop of
+ * FAMesh.flowAccumulation (flowplex.py:850-904: excess, pass limit,
+ * stagnation, `resid > maxarea` with the member's own largest cell area
+ * maxarea[m]), its own lake zeroing and fillFAL maximum.  HOST arrays,
+ * start[0] = 0, start[nmem] = nb.  A new plan has one member.
+ */
+int gs_plan_set_members(gs_plan* plan, int32_t nmem, const int64_t* start, const double* maxarea);
 int gs_plan_set_stream(gs_plan* plan, void* cuda_stream);
 /* Number of device kernels this plan launched since creation. */
 int64_t gs_plan_launches(const gs_plan* plan);
