@@ -170,6 +170,7 @@ def main():
     ap.add_argument("--workload", default="sphere", choices=["sphere", "ensemble"])
     ap.add_argument("--members", type=int, default=256)
     ap.add_argument("--loop", action="store_true", help="ensemble: also time the per-member loop")
+    ap.add_argument("--adjoint-steps", type=int, default=4, help="sphere: steps of the adjoint timing (0: skip)")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -295,6 +296,10 @@ def main():
     step_bytes = step_algo_bytes(layout)
     step_gbs = step_bytes / (ms / args.steps / 1000.0) / 1e9
 
+    adj = None
+    if ens_members is None and args.adjoint_steps > 0:
+        adj = adjoint_ratio(model, args.adjoint_steps, stream, dev, pg)
+
     loop = None
     if ens_members is not None and args.loop:
         # the same members as separate models, stepped one after the other
@@ -351,12 +356,46 @@ def main():
             "cpu_baseline": cpu,
             "stats": stats.get("flow"),
             "loop_baseline": loop,
+            "adjoint": adj,
             "setup_s": setup_s,
         }
         print(json.dumps(line), flush=True)
     if pg is not None:
         pg.barrier()
         pg.destroy_process_group()
+
+
+def adjoint_ratio(model, k, stream, dev, pg):
+    """Adjoint:forward cost ratio on the same landscape: k forward steps with
+    one checkpoint, then the backward pass (replay of the k steps with
+    recording + k adjoint steps), both timed with CUDA events, max over ranks."""
+    import torch
+    from gospl_b200 import adjoint as A
+    n = model.lpoints
+    f64 = dict(dtype=torch.float64, device=dev)
+    K = torch.full((n,), model.K if model.Kfield is None else 0.0, **f64) if model.Kfield is None else model.Kfield
+    U = model.upsub if model.upsub is not None else torch.zeros(n, **f64)
+    rain = model.rainMesh
+    h0 = model.hGlobal.clone()
+    hT, ck = A.run(model, K, U, rain, h0, k, k)   # warm-up of the forward path
+    A.backward(model, K, U, rain, ck, k, k, torch.ones_like(hT))
+    torch.cuda.synchronize(dev)
+    e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    e[0].record(stream)
+    hT, ck = A.run(model, K, U, rain, h0, k, k)
+    e[1].record(stream)
+    gK, gU, grain, gh = A.backward(model, K, U, rain, ck, k, k, 2.0 * (hT - h0))
+    e[2].record(stream)
+    torch.cuda.synchronize(dev)
+    tf, tb = e[0].elapsed_time(e[1]), e[1].elapsed_time(e[2])
+    if pg is not None:
+        t = torch.tensor([tf, tb], dtype=torch.float64, device=dev)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        tf, tb = float(t[0]), float(t[1])
+    return {"ratio": tb / tf, "forward_ms_per_step": tf / k, "adjoint_ms_per_step": tb / k, "steps": k,
+            "checkpoint_every": k, "what": "adjoint step = replay of the step with recording + its reverse "
+                                          "(gradients wrt K, U, rain and h0)",
+            "finite": bool(torch.isfinite(gK).all() and torch.isfinite(gh).all())}
 
 
 def config_of(args, n, n_all, world):

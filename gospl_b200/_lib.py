@@ -18,7 +18,8 @@ EXPORTS = ("gs_version", "gs_last_error", "gs_plan_create", "gs_plan_destroy", "
            "gs_plan_set_stream",
            "gs_plan_launches", "gs_mfdreceivers", "gs_fill_elevation", "gs_pit_tables",
            "gs_flow_accumulation", "gs_erodep_spl", "gs_hillslope", "gs_apply_forces", "gs_mesh_geometry", "gs_plan_profile",
-           "gs_plan_profile_report", "gs_plan_profile_trace", "gs_flow_solve_noalloc")
+           "gs_plan_profile_report", "gs_plan_profile_trace", "gs_plan_record", "gs_plan_record_slot",
+           "gs_adjoint_step", "gs_flow_solve_noalloc")
 
 
 class GsError(RuntimeError):
@@ -73,6 +74,9 @@ def load(path=None):
     L.gs_flow_solve_noalloc.argtypes = [i64, i32, P, P, P, P, P]
     L.gs_plan_profile_report.argtypes = [P, ctypes.c_char_p, i64]
     L.gs_plan_profile_trace.argtypes = [P, ctypes.c_char_p, i64]
+    L.gs_plan_record.argtypes = [P, i32]
+    L.gs_plan_record_slot.argtypes = [P, i32]
+    L.gs_adjoint_step.argtypes = [P, i32, P, P, d, P, d, d, d, d, d, d, d, i32, P, P, P, P]
     L.gs_mesh_geometry.argtypes = [i64, P, i64, P, P, P, i64, P, P, P, P, i32, P, P, P, P, P, P, P]
     for name in EXPORTS:
         if name not in ("gs_version", "gs_plan_launches"):

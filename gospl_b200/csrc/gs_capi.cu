@@ -84,6 +84,33 @@ int gs_plan_create(int64_t nb, const int32_t* nnb, const int32_t* ngb, const dou
 
 int gs_plan_destroy(gs_plan* plan) { GS_GUARD(return gs::plan_destroy(plan);) }
 
+int gs_plan_record(gs_plan* plan, int32_t nslots) {
+    NEED(plan);
+    GS_GUARD(return gs::record_setup(plan, nslots);)
+}
+
+int gs_plan_record_slot(gs_plan* plan, int32_t slot) {
+    NEED(plan);
+    GS_GUARD(return gs::record_select(plan, slot);)
+}
+
+int gs_adjoint_step(gs_plan* plan, int32_t slot, double* lam, const double* rain, double k_scalar,
+                    const double* k_field, double d, double m, double dt, double sealevel, double cda, double cdm,
+                    double rtol, int32_t max_iter, double* grad_k, double* grad_u, double* grad_rain,
+                    double* grad_bl) {
+    NEED(plan);
+    if (plan->n > 0) {
+        NEED(lam);
+        NEED(rain);
+    }
+    if (!(dt > 0)) {
+        gs::set_error(GS_EINVAL, "dt must be positive");
+        return GS_EINVAL;
+    }
+    GS_GUARD(return gs::adjoint_step(plan, slot, lam, rain, k_scalar, k_field, d, m, dt, sealevel, cda, cdm, rtol,
+                                     max_iter, grad_k, grad_u, grad_rain, grad_bl);)
+}
+
 int gs_plan_set_members(gs_plan* plan, int32_t nmem, const int64_t* start, const double* maxarea) {
     NEED(plan);
     NEED(start);

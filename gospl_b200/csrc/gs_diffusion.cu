@@ -195,6 +195,7 @@ __global__ void k_mask_changed(int n, const double* __restrict__ h, double sl, c
 int hillslope(gs_plan* p, double* h, double* cum_ed, double* eb, double sealevel, double cda,
               double cdm, double dt, double rtol, int max_iter, gs_stats* st) {
     const int n = (int)p->n;
+    GS_TRY(rec_hill(p, h));
     if (n == 0 || (cda == 0.0 && cdm == 0.0)) return GS_OK;
     const int B = 256, G = grid_for(n, B);
     const int PARTS = 512;
@@ -277,6 +278,133 @@ int hillslope(gs_plan* p, double* h, double* cum_ed, double* eb, double sealevel
     GS_LAUNCH();
     if (relres > rtol) {
         set_error(GS_EMAXITER, "hillslope CG reached max_iter");
+        return GS_EMAXITER;
+    }
+    return GS_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Adjoint of hillslope().  Forward: fixed rows F^c (flat outlets, zero area)
+// keep x = h; free rows solve S_FF x_F = A_F h_F - S_FX h_X with S = A (I+L)
+// symmetric.  Given lam = dJ/dx: nu = S_FF^-1 lam_F (same operator and CG),
+// dJ/dh_F = A_F nu, dJ/dh_X = lam_X - sum_{free j next to X} A_j o_jX nu_j.
+
+// warm start x0 = rhs / A (exact when L = 0: the diffusion of one step is a
+// small perturbation of the identity), 0 on fixed rows
+__global__ void k_cg_x0(int n, int flat, const uint8_t* __restrict__ outlet, const double* __restrict__ farea,
+                        const double* __restrict__ rhs, double* x, double* b) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const bool fx = diff_fixed(k, flat, outlet, farea);
+    x[k] = fx ? 0.0 : rhs[k] / farea[k];
+    b[k] = fx ? 0.0 : rhs[k];
+}
+
+__global__ void k_cg_init_rhs(int n, int W, int flat, const int* __restrict__ nbr, const int8_t* __restrict__ nnb,
+                              const double* __restrict__ coef, const double* __restrict__ farea,
+                              const uint8_t* __restrict__ outlet, const double* __restrict__ x,
+                              const double* __restrict__ b, double* r, double* z, double* pp) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    if (diff_fixed(k, flat, outlet, farea)) {
+        r[k] = 0.0; z[k] = 0.0; pp[k] = 0.0;
+        return;
+    }
+    const double rk = b[k] - diff_row(k, n, W, nbr, nnb, coef, farea, outlet, flat, x, true);
+    r[k] = rk;
+    const double zk = rk / (farea[k] * coef[k]);
+    z[k] = zk;
+    pp[k] = zk;
+}
+
+__global__ void k_hill_adj_out(int n, int flat, const int* __restrict__ nbr, const int8_t* __restrict__ nnb,
+                               const int8_t* __restrict__ rev, const double* __restrict__ coef,
+                               const double* __restrict__ farea, const uint8_t* __restrict__ outlet,
+                               const double* __restrict__ nu, double* lam) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    if (!diff_fixed(k, flat, outlet, farea)) {
+        lam[k] = farea[k] * nu[k];
+        return;
+    }
+    double acc = lam[k];
+    for (int t = 0; t < nnb[k]; t++) {
+        int j = nbr[(size_t)t * n + k];
+        if (j < 0 || diff_fixed(j, flat, outlet, farea)) continue;
+        int s = rev[(size_t)t * n + k];
+        if (s < 0) continue;
+        double o = coef[(size_t)(s + 1) * n + j];
+        acc = acc - farea[j] * o * nu[j];
+    }
+    lam[k] = acc;
+}
+
+// lam: dJ/dx (h after diffusion) on entry, dJ/dh (before) on return.  h_in
+// is the elevation the forward diffused (its sea mask sets the operator).
+int hillslope_adjoint(gs_plan* p, const double* h_in, double* lam, double sealevel, double cda, double cdm,
+                      double dt, double rtol, int max_iter, int* iters) {
+    const int n = (int)p->n;
+    if (iters) *iters = 0;
+    if (n == 0 || (cda == 0.0 && cdm == 0.0)) return GS_OK;
+    const int B = 256, G = grid_for(n, B);
+    const int PARTS = 512;
+    launch(p, k_diff_coef, G, B, n, p->W, p->flat, h_in, sealevel, cda, cdm, dt, (const int*)p->nbr,
+           (const int8_t*)p->nnb, (const double*)p->elen, (const double*)p->vdist, (const double*)p->farea,
+           (const uint8_t*)p->outlet, p->dcoef, p->dsea);
+    GS_LAUNCH();
+    p->dvalid = 0;   // the forward's cached operator was overwritten
+    launch(p, k_cg_x0, G, B, n, p->flat, (const uint8_t*)p->outlet, (const double*)p->farea, (const double*)lam,
+           p->cg_x, p->cg_b);
+    launch(p, k_cg_init_rhs, G, B, n, p->W, p->flat, (const int*)p->nbr, (const int8_t*)p->nnb,
+           (const double*)p->dcoef, (const double*)p->farea, (const uint8_t*)p->outlet, (const double*)p->cg_x,
+           (const double*)p->cg_b, p->cg_r, p->cg_z, p->cg_p);
+    double* sc = p->red + 4096;
+    launch(p, k_dots<2>, PARTS, 256, n, (const double*)p->cg_r, (const double*)p->cg_z,
+           (const double*)p->cg_b, (const double*)p->cg_b, p->red);
+    launch(p, k_dots_final, 1, 1024, PARTS, 2, (const double*)p->red, sc + 5);
+    launch(p, k_dots<1>, PARTS, 256, n, (const double*)p->cg_r, (const double*)p->cg_r,
+           (const double*)nullptr, (const double*)nullptr, p->red);
+    launch(p, k_dots_final, 1, 1024, PARTS, 1, (const double*)p->red, sc + 3);
+    GS_LAUNCH();
+    double hs[8];
+    // sc[3] = rr, sc[5] = rz, sc[6] = bb
+    GS_CUDA(cudaMemcpyAsync(hs, sc + 3, 4 * sizeof(double), cudaMemcpyDeviceToHost, p->stream));
+    GS_CUDA(cudaStreamSynchronize(p->stream));
+    const double bnorm = sqrt(hs[3]);
+    GS_CUDA(cudaMemcpyAsync(sc, sc + 5, sizeof(double), cudaMemcpyDeviceToDevice, p->stream));
+    int it = 0;
+    double relres = bnorm > 0.0 ? sqrt(hs[0]) / bnorm : 0.0;
+    while (bnorm > 0.0 && relres > rtol && it < max_iter) {
+        launch(p, k_cg_spmv, G, B, n, p->W, p->flat, (const int*)p->nbr, (const int8_t*)p->nnb,
+               (const double*)p->dcoef, (const double*)p->farea, (const uint8_t*)p->outlet,
+               (const double*)p->cg_p, p->cg_ap);
+        launch(p, k_dots<1>, PARTS, 256, n, (const double*)p->cg_p, (const double*)p->cg_ap,
+               (const double*)nullptr, (const double*)nullptr, p->red);
+        launch(p, k_dots_final, 1, 1024, PARTS, 1, (const double*)p->red, sc + 1);
+        launch(p, k_cg_update, G, B, n, p->flat, (const uint8_t*)p->outlet, (const double*)p->farea,
+               (const double*)p->dcoef, (const double*)sc, p->cg_x, p->cg_r, p->cg_z,
+               (const double*)p->cg_p, (const double*)p->cg_ap);
+        launch(p, k_dots<2>, PARTS, 256, n, (const double*)p->cg_r, (const double*)p->cg_z,
+               (const double*)p->cg_r, (const double*)p->cg_r, p->red);
+        launch(p, k_dots_final, 1, 1024, PARTS, 2, (const double*)p->red, sc + 2);
+        launch(p, k_cg_dir, G, B, n, (const double*)(sc + 2), sc, (const double*)p->cg_z, p->cg_p);
+        launch(p, k_cg_rotate, 1, 1, (const double*)(sc + 2), sc);
+        GS_LAUNCH();
+        GS_CUDA(cudaMemcpyAsync(hs, sc + 3, sizeof(double), cudaMemcpyDeviceToHost, p->stream));
+        GS_CUDA(cudaStreamSynchronize(p->stream));
+        relres = sqrt(hs[0]) / bnorm;
+        it++;
+        if (!(relres == relres)) {
+            set_error(GS_ENONFINITE, "hillslope adjoint CG produced a non-finite residual");
+            return GS_ENONFINITE;
+        }
+    }
+    if (iters) *iters = it;
+    launch(p, k_hill_adj_out, G, B, n, p->flat, (const int*)p->nbr, (const int8_t*)p->nnb, (const int8_t*)p->rev,
+           (const double*)p->dcoef, (const double*)p->farea, (const uint8_t*)p->outlet, (const double*)p->cg_x, lam);
+    GS_LAUNCH();
+    if (relres > rtol) {
+        set_error(GS_EMAXITER, "hillslope adjoint CG reached max_iter");
         return GS_EMAXITER;
     }
     return GS_OK;

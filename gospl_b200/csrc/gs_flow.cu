@@ -309,6 +309,7 @@ int flow_accumulation(gs_plan* p, const double* h, const double* bl, double seal
     p->order_i_valid = ok_i;
     int cyc = 0;
     GS_TRY(flow_run(p, rcv_i, wgt_i, p->rslot_i, p->nfa, fal, &cyc, p->order_i, ok_i));
+    GS_TRY(rec_initial(p, h, rcv_i, wgt_i, dist_i, p->rslot_i, p->order_i, ok_i, fal, sea));
     int total_cycles = cyc;
     launch(p, k_copy, G, B, (int64_t)n, h, p->wf);
     // pitVol and, per member, "any pit with volume"
@@ -355,6 +356,7 @@ int flow_accumulation(gs_plan* p, const double* h, const double* bl, double seal
                    p->pit_win, p->mflags);
             GS_LAUNCH();
             GS_CUDA(cudaMemcpyAsync(p->h_mflags, p->mflags, sizeof(int) * nm, cudaMemcpyDeviceToHost, p->stream));
+            GS_TRY(rec_pass_pits(p, step, lsink, np1));
             GS_CUDA(cudaStreamSynchronize(p->stream));
             int flags = 0;
             bool anybig = false, allbig = true;
@@ -392,6 +394,7 @@ int flow_accumulation(gs_plan* p, const double* h, const double* bl, double seal
                 if (!allbig)
                     launch(p, k_lsink_keep, G, B, n, (const int*)p->vmember, (const uint8_t*)p->mbig,
                            (const uint8_t*)p->lsink_prev, lsink);
+                GS_TRY(rec_pass_rebuild(p, step, surf));
                 GS_TRY(flow_order_ties(p, p->pdir, p->order));
                 launch(p, k_div, G, B, (int64_t)n, (const double*)p->nfa, dt, p->q2);
                 launch(p, k_chunk_sum, p->nchunk, 256, (const int*)p->chunk_lo, (const double*)p->q2,
@@ -417,8 +420,9 @@ int flow_accumulation(gs_plan* p, const double* h, const double* bl, double seal
                     // solve into FA's buffer: FA is consumed already
                     GS_TRY(flow_prepare(p, p->rcv, p->wgt, p->rslot, p->q, p->order, p->h_pinned));
                     GS_CUDA(cudaStreamSynchronize(p->stream));
-                    GS_TRY(flow_run(p, p->rcv, p->wgt, p->rslot, p->q2, p->q, &cyc, p->order,
-                                    p->h_pinned[0] ? 0 : 1));
+                    const int ok_c = p->h_pinned[0] ? 0 : 1;
+                    GS_TRY(flow_run(p, p->rcv, p->wgt, p->rslot, p->q2, p->q, &cyc, p->order, ok_c));
+                    GS_TRY(rec_pass_solve(p, step, p->order, ok_c, p->q));
                     total_cycles += cyc;
                     launch(p, k_cascade_accum, G, B, n, (const double*)p->q, dt, h, (const double*)p->wf,
                            p->q, fal);
@@ -454,6 +458,7 @@ int flow_accumulation(gs_plan* p, const double* h, const double* bl, double seal
     launch(p, k_flow_final, G, B, n, (const uint8_t*)p->mlakes, (const int*)p->vmember, h, (const double*)p->wf,
            (const int*)pit_ids, (const unsigned long long*)p->mmax, fal, fill_fal, water);
     GS_LAUNCH();
+    GS_TRY(rec_final(p, passes, fal, pit_ids, lfill, anyvol ? 1 : 0));
     if (st) {
         st->cascade_passes = passes;
         st->cascade_solves = solves;

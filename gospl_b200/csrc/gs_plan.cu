@@ -53,6 +53,7 @@ static void plan_free(gs_plan* p) {
         if (e) cudaEventDestroy(e);
     p->prof_ev.clear();
     free_members(p);
+    record_free(p);
     if (p->side_a) cudaStreamDestroy(p->side_a);
     if (p->side_b) cudaStreamDestroy(p->side_b);
     if (p->h_pinned) cudaFreeHost(p->h_pinned);

@@ -149,6 +149,17 @@ struct gs_plan {
     double* h_mresid = nullptr;          // pinned host [nmem]
     uint8_t* lsink_prev = nullptr;       // [n]
 
+    // adjoint scratch: [R][n] edge terms, [W][n] neighbour terms, vectors
+    double* adj_er = nullptr;
+    double* adj_gw = nullptr;
+    double* adj_nb = nullptr;
+    double* adj_v0 = nullptr;
+    double* adj_v1 = nullptr;
+    double* adj_v2 = nullptr;
+    double* adj_v3 = nullptr;
+    struct gs_record* rec = nullptr;     // per-step records of the forward (adjoint replay)
+    int rec_slot = -1;                   // slot the forward writes, -1 = not recording
+
     // diffusion
     double* dcoef = nullptr;             // [W+1][n]: diag then off-diagonals
     uint8_t* dsea = nullptr;             // sea mask the matrix was built for
@@ -188,6 +199,32 @@ int sink_mask(gs_plan* p, const double* wgt, const uint8_t* sea, uint8_t* lsink)
 int flow_solve(gs_plan* p, const int* rcv, const double* wgt, const int8_t* rslot,
                const double* b, double* x, int* cycle_nodes, const double* surface, const int* pdir,
                int* order);
+int receivers_adjoint(gs_plan* p, const double* z, double sl, const int8_t* rslot, const double* gw, double* gself,
+                      double* gnb, double* gz);
+int spl_adjoint(gs_plan* p, const double* hold, const double* s, const double* fal, const double* rain,
+                double k_scalar, const double* k_field, double d, double m, double dt, const int* rcv,
+                const double* dist, const double* wgt, const int8_t* rslot, const int* order, const uint8_t* lsink,
+                const uint8_t* sea, double* lam, double* gK, double* grain, double* gfal, double* gw_out);
+// per-step records of the forward for the adjoint replay (gs_adjoint.cu)
+int record_setup(gs_plan* p, int nslots);
+int record_select(gs_plan* p, int slot);
+void record_free(gs_plan* p);
+int rec_initial(gs_plan* p, const double* h, const int* rcv, const double* wgt, const double* dist,
+                const int8_t* rslot, const int* order, int order_ok, const double* q0, const uint8_t* sea);
+int rec_pass_pits(gs_plan* p, int t, const uint8_t* lsink, int np1);
+int rec_pass_rebuild(gs_plan* p, int t, const double* surf);
+int rec_pass_solve(gs_plan* p, int t, const int* order, int order_ok, const double* x);
+int rec_final(gs_plan* p, int npass, const double* fal, const int* pit, const double* lfill, int lakes);
+int rec_spl(gs_plan* p, const double* s, const uint8_t* lsink);
+int rec_hill(gs_plan* p, const double* h_in);
+int adjoint_step(gs_plan* p, int slot, double* lam, const double* rain, double k_scalar, const double* k_field,
+                 double d, double m, double dt, double sealevel, double cda, double cdm, double rtol, int max_iter,
+                 double* gK, double* gU, double* grain, double* gbl);
+int hillslope_adjoint(gs_plan* p, const double* h_in, double* lam, double sealevel, double cda, double cdm,
+                      double dt, double rtol, int max_iter, int* iters);
+int sweep_flow_adjoint(gs_plan* p, const int* rcv, const double* wgt, const int* order, const double* g, double* y);
+int sweep_spl_adjoint(gs_plan* p, const int* rcv, const double* wgt, const int8_t* rslot, const double* c,
+                      const int* order, const double* g, double* y);
 int spl_sweep(gs_plan* p, const int* rcv, const double* c, const int8_t* rslot, const double* hold,
               double* s, int* cycle_nodes, bool reuse_order);
 int fill_elevation(gs_plan* p, const double* h, double sealevel, double ofill, double* lfill,

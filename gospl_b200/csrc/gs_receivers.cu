@@ -269,3 +269,123 @@ int flow_direction_post(gs_plan* p, const double* h, bool down, const double* lf
 }
 
 }  // namespace gs
+
+namespace gs {
+
+// Reverse of the slope-weight computation of k_mfd_receivers with the
+// receiver choice held fixed (the slots in rslot): given gw[o][k] = dJ/dw_ok,
+// writes dJ/dz_k to gself[k] and dJ/dz of the neighbour in slot s to
+// gnb[s][k].  The weights are w_o = slp_o / sum(slp), slp_o = (z_k - z_o)^f /
+// L_o (1 - 1e-15 gid_o), and the adaptive exponent f = 5 min(e, 1) + expo
+// with e the steepest descent (z_k - z_a) / L_a.  Cells without MFD receivers
+// (sea, outlets, flat-routed cells) carry no derivative.
+__global__ void k_mfd_weights_adj(int n, int W, int R, double expo, const double* __restrict__ z, double sl,
+                                  const int* __restrict__ gid, const int* __restrict__ nbr,
+                                  const double* __restrict__ elen, const int8_t* __restrict__ nnb,
+                                  const int8_t* __restrict__ rslot, const double* __restrict__ gw,
+                                  double* gself, double* gnb) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    for (int s = 0; s < W; s++) gnb[(size_t)s * n + k] = 0.0;
+    gself[k] = 0.0;
+    const double hk = z[k];
+    if (hk <= sl) return;
+    int so[MAXR];
+    int nsel = 0;
+    for (int o = 0; o < R; o++) {
+        int s = rslot[(size_t)o * n + k];
+        so[o] = s;
+        if (s >= 0) nsel++;
+    }
+    if (nsel == 0) return;
+    const int deg = nnb[k];
+    double e = 0.0;
+    int a = -1;
+    for (int s = 0; s < deg; s++) {
+        int nb = nbr[(size_t)s * n + k];
+        double L = elen[(size_t)s * n + k];
+        if (nb >= 0 && L > 0.0) {
+            double val = (hk - z[nb]) / L;
+            if (val > e) { e = val; a = s; }
+        }
+    }
+    double fexp, dfe = 0.0;
+    if (e > 0) {
+        double me = (e < 1.0) ? e : 1.0;
+        fexp = 5.0 * me + expo;
+        if (e < 1.0) dfe = 5.0;
+    } else {
+        fexp = 1.0;
+    }
+    double slp[MAXR], dval[MAXR], fval[MAXR], gfac[MAXR];
+    double V = 0.0;
+    for (int o = 0; o < R; o++) {
+        slp[o] = 0.0;
+        int s = so[o];
+        if (s < 0) continue;
+        int nb = nbr[(size_t)s * n + k];
+        double L = elen[(size_t)s * n + k];
+        double d = hk - z[nb];
+        if (!(d > 0.0) || !(L > 0.0)) return;   // not an MFD receiver (flat routing): no derivative
+        double val = pow(d, fexp) / L;
+        gfac[o] = 1.0 - 1.0e-15 * (double)gid[nb];
+        slp[o] = val * gfac[o];
+        dval[o] = fexp * pow(d, fexp - 1.0) / L;
+        fval[o] = val * log(d);
+        V = V + slp[o];
+    }
+    if (!(V > 0.0)) return;
+    double sw = 0.0;
+    for (int o = 0; o < R; o++)
+        if (so[o] >= 0) sw += gw[(size_t)o * n + k] * (slp[o] / V);
+    double gs_ = 0.0, gf = 0.0;
+    for (int o = 0; o < R; o++) {
+        int s = so[o];
+        if (s < 0) continue;
+        double gslp = (gw[(size_t)o * n + k] - sw) / V;
+        double gval = gslp * gfac[o];
+        double gd = gval * dval[o];
+        gf += gval * fval[o];
+        gs_ += gd;
+        gnb[(size_t)s * n + k] -= gd;
+    }
+    if (dfe != 0.0 && a >= 0) {
+        double La = elen[(size_t)a * n + k];
+        double ge = gf * dfe / La;
+        gs_ += ge;
+        gnb[(size_t)a * n + k] -= ge;
+    }
+    gself[k] = gs_;
+}
+
+// gz[v] += gself[v] + sum over the cells k that have v as neighbour of gnb[slot of v at k][k]
+__global__ void k_nb_gather(int n, const int* __restrict__ nbr, const int8_t* __restrict__ nnb,
+                            const int8_t* __restrict__ rev, const double* __restrict__ gself,
+                            const double* __restrict__ gnb, double* gz) {
+    int v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= n) return;
+    double acc = gself[v];
+    for (int t = 0; t < nnb[v]; t++) {
+        int k = nbr[(size_t)t * n + v];
+        if (k < 0) continue;
+        int s = rev[(size_t)t * n + v];
+        if (s >= 0) acc += gnb[(size_t)s * n + k];
+    }
+    gz[v] += acc;
+}
+
+// dJ/dz of the surface the receivers were built on, accumulated into gz,
+// from dJ/dw (gw, receiver-major [R][n]); gself/gnb are [n] / [W][n] scratch.
+int receivers_adjoint(gs_plan* p, const double* z, double sl, const int8_t* rslot, const double* gw, double* gself,
+                      double* gnb, double* gz) {
+    const int n = (int)p->n;
+    if (n == 0) return GS_OK;
+    launch(p, k_mfd_weights_adj, grid_for(n, 128), 128, n, p->W, p->R, 1.1, z, sl, (const int*)p->gid,
+           (const int*)p->nbr, (const double*)p->elen, (const int8_t*)p->nnb, rslot, gw, gself, gnb);
+    launch(p, k_nb_gather, grid_for(n, 256), 256, n, (const int*)p->nbr, (const int8_t*)p->nnb,
+           (const int8_t*)p->rev, (const double*)gself, (const double*)gnb, gz);
+    GS_LAUNCH();
+    return GS_OK;
+}
+
+}  // namespace gs

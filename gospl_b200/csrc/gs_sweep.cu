@@ -552,6 +552,69 @@ struct SplOrd {
     }
 };
 
+// Transposed flow system (I - W) y = g: y_i = g_i + sum_k w_ik y_{rcv_ik},
+// receivers first (the flow order reversed).
+struct FlowAdjOrd {
+    int n, R;
+    const int* rcv;
+    const double* wgt;
+    const double* g;
+    double* x;
+    static constexpr int MAXP = MAXR;
+    __device__ __forceinline__ int prep(int i, int* pj, double* pw) const {
+        int np = 0;
+        for (int k = 0; k < R; k++) {
+            double w = wgt[(size_t)k * n + i];
+            int r = rcv[(size_t)k * n + i];
+            if (r != i && w != 0.0) { pj[np] = r; pw[np] = w; np++; }
+        }
+        return np;
+    }
+    __device__ __forceinline__ double init(int i) const { return g[i]; }
+    __device__ __forceinline__ double combine(double s, double w, double xj) const { return s + w * xj; }
+    __device__ __forceinline__ double finish(int, double s, double) const { return s; }
+};
+
+// Transposed SPL system M^T y = g: y_j = (g_j + sum_{donors i} c_ik y_i) / den_j,
+// den_j = 1 + sum_k c_jk, donors first (the flow order).
+struct SplAdjOrd {
+    int n, R;
+    const int* nbr;
+    const uint32_t* mask;
+    const unsigned long long* dk;
+    const unsigned long long* sorder;
+    const double* c;
+    const double* g;
+    double* x;
+    static constexpr int MAXP = MAXW;
+    __device__ __forceinline__ int prep(int i, int* pj, double* pw) const {
+        uint32_t m = mask[i];
+        unsigned long long kk = dk[i], ord = sorder[i];
+        int np = 0;
+        for (int q = 0; q < MAXW && m; q++) {
+            int t = (int)(ord & 15ULL);
+            ord >>= 4;
+            if (!(m & (1u << t))) continue;
+            m &= ~(1u << t);
+            int j = nbr[(size_t)t * n + i];
+            int k = (int)((kk >> (4 * t)) & 15ULL);
+            double cj = c[(size_t)k * n + j];
+            if (cj == 0.0) continue;
+            pj[np] = j;
+            pw[np] = cj;
+            np++;
+        }
+        return np;
+    }
+    __device__ __forceinline__ double init(int i) const { return g[i]; }
+    __device__ __forceinline__ double combine(double s, double w, double xj) const { return s + w * xj; }
+    __device__ __forceinline__ double finish(int i, double s, double) const {
+        double den = 1.0;
+        for (int k = 0; k < R; k++) den = den + c[(size_t)k * n + i];
+        return s / den;
+    }
+};
+
 template <class Op>
 __global__ void __launch_bounds__(128) k_ordered(Op op, int n, const int* __restrict__ order, unsigned* ctr,
                                                  unsigned long long budget_ns) {
@@ -818,6 +881,49 @@ int spl_sweep(gs_plan* p, const int* rcv, const double* c, const int8_t* rslot, 
     GS_TRY(ordered_status(p, &st));
     if (st != 0) {
         set_error(st, "ordered SPL sweep did not complete");
+        return st;
+    }
+    return GS_OK;
+}
+
+// y = (I - W)^-1 g over the graph rcv/wgt whose valid flow order is `order`
+int sweep_flow_adjoint(gs_plan* p, const int* rcv, const double* wgt, const int* order, const double* g, double* y) {
+    const int n = (int)p->n;
+    if (n == 0) return GS_OK;
+    launch(p, k_reverse, grid_for(n, 256), 256, n, order, p->order2);
+    GS_CUDA(cudaMemsetAsync(p->ctr, 0, sizeof(unsigned) * 8, p->stream));
+    launch(p, k_fill_sent, grid_for(n, 256), 256, n, y);
+    FlowAdjOrd op{n, p->R, rcv, wgt, g, y};
+    launch(p, k_ordered<FlowAdjOrd>, p->sm_count * 8, 128, op, n, (const int*)p->order2, p->ctr, SWEEP_BUDGET_NS);
+    GS_LAUNCH();
+    int st = 0;
+    GS_TRY(ordered_status(p, &st));
+    if (st != 0) {
+        set_error(st, "adjoint flow sweep did not complete");
+        return st;
+    }
+    return GS_OK;
+}
+
+// y = M^-T g for the SPL matrix of coefficients c on the graph rcv/wgt/rslot
+// (flow order `order`)
+int sweep_spl_adjoint(gs_plan* p, const int* rcv, const double* wgt, const int8_t* rslot, const double* c,
+                      const int* order, const double* g, double* y) {
+    const int n = (int)p->n;
+    if (n == 0) return GS_OK;
+    GS_CUDA(cudaMemsetAsync(p->don_mask, 0, sizeof(uint32_t) * n, p->stream));
+    GS_CUDA(cudaMemsetAsync(p->don_k, 0, sizeof(unsigned long long) * n, p->stream));
+    launch(p, k_flow_donors, grid_for(n, 256), 256, n, p->R, rcv, wgt, rslot, (const int8_t*)p->rev, p->don_mask,
+           p->don_k);
+    GS_CUDA(cudaMemsetAsync(p->ctr, 0, sizeof(unsigned) * 8, p->stream));
+    launch(p, k_fill_sent, grid_for(n, 256), 256, n, y);
+    SplAdjOrd op{n, p->R, p->nbr, p->don_mask, p->don_k, p->sorder, c, g, y};
+    launch(p, k_ordered<SplAdjOrd>, p->sm_count * 8, 128, op, n, order, p->ctr, SWEEP_BUDGET_NS);
+    GS_LAUNCH();
+    int st = 0;
+    GS_TRY(ordered_status(p, &st));
+    if (st != 0) {
+        set_error(st, "adjoint SPL sweep did not complete");
         return st;
     }
     return GS_OK;

@@ -254,6 +254,24 @@ class Model:
                 break
             self.step()
 
+    # ------------------------------------------------------------- adjoint
+    def record(self, nslots):
+        """Allocate `nslots` per-step records for the adjoint (0 frees them)."""
+        _lib.check(_lib_handle().gs_plan_record(self._plan, int(nslots)))
+
+    def record_slot(self, slot):
+        """Record the next step into `slot` (-1: stop recording)."""
+        _lib.check(_lib_handle().gs_plan_record_slot(self._plan, int(slot)))
+
+    def adjoint_step(self, slot, lam, grad_k=None, grad_u=None, grad_rain=None, grad_bl=None, rtol=1.0e-13,
+                     maxit=2000):
+        """Reverse the step recorded in `slot`: lam (dJ/dh after it) becomes
+        dJ/dh before it; parameter gradients are accumulated (grad_bl written)."""
+        _lib.check(_lib_handle().gs_adjoint_step(
+            self._plan, int(slot), _lib.ptr(lam), _lib.ptr(self.rainVal), self.K, _lib.ptr(self.Kfield),
+            self.coeffd, self.spl_m, self.dt, self.sealevel, self.Cda, self.Cdm, rtol, maxit, _lib.ptr(grad_k),
+            _lib.ptr(grad_u), _lib.ptr(grad_rain), _lib.ptr(grad_bl)))
+
     def destroy(self):
         if getattr(self, "_plan", None) is not None:
             self.torch.cuda.synchronize(self.dev)

@@ -184,6 +184,27 @@ int gs_apply_forces(gs_plan* plan, double* h, const double* rain, const double* 
                     double sealevel, double* bl);
 
 /*
+ * Adjoint.  No counterpart in the reference (goSPL has no derivatives).
+ * gs_plan_record allocates nslots per-step records (0 frees them; single-
+ * landscape plans only); after gs_plan_record_slot(plan, s) the forward calls
+ * of one step (gs_flow_accumulation, gs_erodep_spl, gs_hillslope) store what
+ * the adjoint needs in slot s (-1 stops recording).  gs_adjoint_step reverses
+ * the recorded step with its discrete decisions held fixed (receiver choice,
+ * pits, flat routing, cascade states, masks): on entry lam = dJ/dh after the
+ * step's uplift (h_{t+1}), on return lam = dJ/dh_t; it accumulates dJ/dK
+ * (grad_k, per vertex), dJ/dU (grad_u, the uplift rate) and the direct SPL
+ * part of dJ/drain (grad_rain, rain^d), and writes dJ/dbL_t (grad_bl: the
+ * step's rain volume rain * larea); any output may be NULL.  The level of a
+ * partially filled lake is held constant.  Synchronises the plan's stream.
+ */
+int gs_plan_record(gs_plan* plan, int32_t nslots);
+int gs_plan_record_slot(gs_plan* plan, int32_t slot);
+int gs_adjoint_step(gs_plan* plan, int32_t slot, double* lam, const double* rain, double k_scalar,
+                    const double* k_field, double d, double m, double dt, double sealevel, double cda, double cdm,
+                    double rtol, int32_t max_iter, double* grad_k, double* grad_u, double* grad_rain,
+                    double* grad_bl);
+
+/*
  * Allocation-free flow solve.  No counterpart in the reference: goSPL always
  * allocates its PETSc matrices and vectors.  For callers that cannot call
  * cudaMalloc (an embedding application that owns every allocation, a fixed
