@@ -174,21 +174,6 @@ __global__ void k_cross_edges(int n, const double* __restrict__ h, const double*
     }
 }
 
-__global__ void k_relax(int m, const int* __restrict__ xu, const int* __restrict__ xv,
-                        const double* __restrict__ xw, unsigned long long* L, int* changed) {
-    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < m; e += gridDim.x * blockDim.x) {
-        unsigned long long lv = ((volatile unsigned long long*)L)[xv[e]];
-        if (lv == ~0ULL) continue;
-        unsigned long long w = dkey(xw[e]);
-        unsigned long long cand = w > lv ? w : lv;
-        int bu = xu[e];
-        if (cand < ((volatile unsigned long long*)L)[bu]) {
-            unsigned long long old = atomicMin(&L[bu], cand);
-            if (cand < old) *changed = 1;
-        }
-    }
-}
-
 __global__ void k_fill_final(int n, const double* __restrict__ h, const double* __restrict__ dsc,
                              double sealevel, const int8_t* __restrict__ ledge,
                              const int* __restrict__ root, const unsigned long long* __restrict__ L,
@@ -690,34 +675,48 @@ __global__ void __launch_bounds__(256) k_bfs_coop(int* fa, int* fb, int* sizes, 
     if (threadIdx.x == 0) *levels_out = levels;
 }
 
-// Minimax relaxation over the basin graph in one cooperative launch; rounds
-// end when no basin level changed (three rotating change flags, as above).
-__global__ void __launch_bounds__(256) k_relax_coop(int m, const int* __restrict__ xu, const int* __restrict__ xv,
-                                                    const double* __restrict__ xw, unsigned long long* L,
-                                                    int* flags, int max_rounds, int* rounds_out) {
+// Minimax relaxation over the basin graph in one cooperative launch, edge-
+// parallel: round r relaxes the edges whose source basin was lowered in round
+// r-1 or later (stamp[v] >= r - 1; seed basins carry stamp 0), so every round
+// reads every edge's source once but does the level work only for the active
+// ones.  Lowered basins get stamp r.  Rounds end when none changed (three
+// rotating change flags); the fixed point is that of the all-edges
+// relaxation, whatever the order of the updates.
+__global__ void k_basin_stamp(int n, const unsigned long long* __restrict__ L, int* stamp) {
+    int v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v < n) stamp[v] = (L[v] != ~0ULL) ? 0 : -1;
+}
+
+__global__ void __launch_bounds__(256) k_relax_active(int m, const int* __restrict__ xu, const int* __restrict__ xv,
+                                                      const double* __restrict__ xw, unsigned long long* L,
+                                                      int* stamp, int* flags, int max_rounds, int* rounds_out) {
     cg::grid_group grid = cg::this_grid();
     const int gtid = blockIdx.x * blockDim.x + threadIdx.x, gsz = gridDim.x * blockDim.x;
-    int r = 0;
-    for (; r < max_rounds; r++) {
+    int r = 1;
+    for (; r <= max_rounds; r++) {
         int changed = 0;
         for (int e = gtid; e < m; e += gsz) {
-            unsigned long long lv = ((volatile unsigned long long*)L)[xv[e]];
+            const int v = xv[e];
+            if (((volatile int*)stamp)[v] < r - 1) continue;
+            const unsigned long long lv = ((volatile unsigned long long*)L)[v];
             if (lv == ~0ULL) continue;
-            unsigned long long w = dkey(xw[e]);
-            unsigned long long cand = w > lv ? w : lv;
-            int bu = xu[e];
-            if (cand < ((volatile unsigned long long*)L)[bu]) {
-                unsigned long long old = atomicMin(&L[bu], cand);
-                if (cand < old) changed = 1;
+            const unsigned long long w = dkey(xw[e]);
+            const unsigned long long cand = w > lv ? w : lv;
+            const int u = xu[e];
+            if (cand < ((volatile unsigned long long*)L)[u]) {
+                const unsigned long long old = atomicMin(&L[u], cand);
+                if (cand < old) {
+                    ((volatile int*)stamp)[u] = r;
+                    changed = 1;
+                }
             }
         }
         if (__any_sync(0xffffffffu, changed) && (threadIdx.x & 31) == 0) flags[r % 3] = 1;
         if (gtid == 0) flags[(r + 2) % 3] = 0;
         grid.sync();
-        int f = *(volatile int*)&flags[r % 3];
-        if (!f) break;
+        if (!*(volatile int*)&flags[r % 3]) break;
     }
-    if (gtid == 0) *rounds_out = r + 1;
+    if (gtid == 0) *rounds_out = r;
 }
 
 __global__ void k_flat_dirs(int n, const double* __restrict__ f, const int* __restrict__ pit,
@@ -970,13 +969,15 @@ int fill_elevation(gs_plan* p, const double* h, double sealevel, double ofill, d
     if (m > p->xe_cap) { set_error(GS_ENOMEM, "pit fill: cross-edge capacity exceeded"); return GS_ENOMEM; }
     int rounds = 0;
     {
+        launch(p, k_basin_stamp, G, B, n, (const unsigned long long*)p->basinL, p->comp);
         GS_CUDA(cudaMemsetAsync(p->i_scalar + 5, 0, sizeof(int) * 3, p->stream));
+        GS_LAUNCH();
         int mm = (int)m, maxr = 1000000;
         int* flags = p->i_scalar + 5;
         int* rout = p->i_scalar + I_CHANGED;
         void* args[] = {(void*)&mm, (void*)&p->xe_u, (void*)&p->xe_v, (void*)&p->xe_w, (void*)&p->basinL,
-                        (void*)&flags, (void*)&maxr, (void*)&rout};
-        GS_TRY(launch_coop(p, (const void*)k_relax_coop, args));
+                        (void*)&p->comp, (void*)&flags, (void*)&maxr, (void*)&rout};
+        GS_TRY(launch_coop(p, (const void*)k_relax_active, args));
         GS_TRY(read_ints(p, hbuf, p->i_scalar + I_CHANGED, 1));
         rounds = hbuf[0] - 1;
     }
@@ -1164,7 +1165,7 @@ int fill_elevation(gs_plan* p, const double* h, double sealevel, double ofill, d
 int coop_occupancy(int* per_sm) {
     int a = 0, b = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_bfs_coop, 256, 0) != cudaSuccess) return 1;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_relax_coop, 256, 0) != cudaSuccess) return 1;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_relax_active, 256, 0) != cudaSuccess) return 1;
     *per_sm = a < b ? a : b;
     return 0;
 }
