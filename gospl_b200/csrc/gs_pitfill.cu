@@ -553,6 +553,8 @@ __global__ void __launch_bounds__(1024) k_bfs_local(int M, int S, const int* __r
         // every warp runs the same number of batches so that ballots see all lanes
         for (int base = 0; base < size; base += nt) {
             const int t = base + tid;
+            // warps past the end of the frontier go straight to the barrier
+            if (!__any_sync(0xffffffffu, t < size)) break;
             int row[16];
             int k = 0;
             if (t < size) {
@@ -569,17 +571,24 @@ __global__ void __launch_bounds__(1024) k_bfs_local(int M, int S, const int* __r
             }
             // claim the unvisited out-neighbours: plain checks, then the
             // atomics, all independent so their latencies overlap
+            const int kmax = __reduce_max_sync(0xffffffffu, k);
             unsigned cand = 0u;
 #pragma unroll
-            for (int q = 1; q < 16; q++)
+            for (int q = 1; q < 16; q++) {
+                if (q > kmax) break;
                 if (q <= k && !(vis[row[q] >> 5] & (1u << (row[q] & 31)))) cand |= 1u << q;
+            }
             unsigned olds[16];
 #pragma unroll
-            for (int q = 1; q < 16; q++)
+            for (int q = 1; q < 16; q++) {
+                if (q > kmax) break;
                 olds[q] = (cand & (1u << q)) ? atomicOr(&vis[row[q] >> 5], 1u << (row[q] & 31)) : 0xffffffffu;
+            }
 #pragma unroll
-            for (int q = 1; q < 16; q++)
+            for (int q = 1; q < 16; q++) {
+                if (q > kmax) break;
                 if ((cand & (1u << q)) && (olds[q] & (1u << (row[q] & 31)))) cand &= ~(1u << q);
+            }
             // warp-aggregated append of the claimed cells
             const int mine = __popc(cand);
             int incl = mine;
@@ -595,6 +604,7 @@ __global__ void __launch_bounds__(1024) k_bfs_local(int M, int S, const int* __r
             int pos = pos0 + incl - mine;
 #pragma unroll
             for (int q = 1; q < 16; q++) {
+                if (q > kmax) break;
                 if (cand & (1u << q)) {
                     const int c = row[q];
                     ld[c] = d + 1;
@@ -680,7 +690,8 @@ __global__ void __launch_bounds__(256) k_bfs_coop(int* fa, int* fb, int* sizes, 
 // r-1 or later (stamp[v] >= r - 1; seed basins carry stamp 0), so every round
 // reads every edge's source once but does the level work only for the active
 // ones.  Lowered basins get stamp r.  Rounds end when none changed (three
-// rotating change flags); the fixed point is that of the all-edges
+// rotating change flags: round r sets flags[r % 3], reads it after the
+// barrier and clears flags[(r + 1) % 3]); the fixed point is that of the all-edges
 // relaxation, whatever the order of the updates.
 __global__ void k_basin_stamp(int n, const unsigned long long* __restrict__ L, int* stamp) {
     int v = blockIdx.x * blockDim.x + threadIdx.x;
@@ -712,7 +723,10 @@ __global__ void __launch_bounds__(256) k_relax_active(int m, const int* __restri
             }
         }
         if (__any_sync(0xffffffffu, changed) && (threadIdx.x & 31) == 0) flags[r % 3] = 1;
-        if (gtid == 0) flags[(r + 2) % 3] = 0;
+        // clear the flag of the next round: its last readers (end of round
+        // r - 2) have all passed the barrier of round r - 1.  The flag of
+        // round r - 1 may still be unread by slow threads.
+        if (gtid == 0) flags[(r + 1) % 3] = 0;
         grid.sync();
         if (!*(volatile int*)&flags[r % 3]) break;
     }

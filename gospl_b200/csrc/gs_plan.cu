@@ -98,10 +98,11 @@ int plan_create(int64_t nb, const int32_t* nnb, const int32_t* ngb, const double
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&p->sm_count, cudaDevAttrMultiProcessorCount, dev);
     {
-        // two 256-thread blocks per SM for the cooperative kernels (both use
-        // few registers and little shared memory; checked against occupancy)
+        // cooperative kernels: up to four co-resident 256-thread blocks per SM
+        // (checked against occupancy), enough warps to hide the gather latency
+        // of the edge-parallel rounds
         int per_sm = 0;
-        if (coop_occupancy(&per_sm) == 0 && per_sm > 0) p->coop_blocks = p->sm_count;
+        if (coop_occupancy(&per_sm) == 0 && per_sm > 0) p->coop_blocks = p->sm_count * std::min(per_sm, 4);
         else p->coop_blocks = p->sm_count;
     }
 
