@@ -496,7 +496,10 @@ def step_algo_bytes(L):
 # launch divided by the vertices it processed) from the ncu captures summarised
 # under profiles/; scaled by the vertex count of the run.
 NCU_TRAFFIC_PER_VERTEX = {
-    "k_mfd_receivers": (45.681152e6 + 20.494080e6) / 655362,
+    "k_mfd_receivers": (37.528064e6 + 19.233024e6) / 655362,
+    "k_ordered_flow": (34.788608e6 + 1.394944e6) / 655362,
+    "k_bfs_local": 1.788672e6 / 655362,
+    "k_relax_active": (9.614592e6 + 0.072192e6) / 655362,
 }
 
 

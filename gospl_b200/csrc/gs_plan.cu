@@ -321,7 +321,7 @@ __global__ void k_fill_member(int lo, int hi, int m, int* vmember) {
 }
 
 // Members are contiguous vertex ranges [start[m], start[m+1]); every
-// reduction over a member runs over chunks of at most 65536 of its vertices
+// reduction over a member runs over chunks of at most 8192 of its vertices
 // in a fixed order.
 int set_members(gs_plan* p, int nmem, const int64_t* start, const double* maxarea) {
     const int64_t n = p->n;
@@ -338,7 +338,7 @@ int set_members(gs_plan* p, int nmem, const int64_t* start, const double* maxare
     p->nmem = nmem;
     p->mstart.assign(start, start + nmem + 1);
     p->mmaxarea.assign(maxarea, maxarea + nmem);
-    const int64_t CH = 65536;
+    const int64_t CH = 8192;
     std::vector<int> lo, m0;
     for (int m = 0; m < nmem; m++) {
         m0.push_back((int)lo.size());
