@@ -10,9 +10,77 @@
 // Jacobi-preconditioned CG on  A (I + L) h = A hOld,  outlet rows (and rows of
 // zero area, which carry no equation) held at hOld.  The matrix is rebuilt only
 // when the land/sea mask changes, like the reference's cached operator.
+#include <cooperative_groups.h>
+
+#include <algorithm>
+
 #include "gs_plan.cuh"
 
+namespace cg = cooperative_groups;
+
 namespace gs {
+
+// row k of (I + L) for the land/sea mask `sea` (sea: Cd = cdm, land: cda)
+__device__ __forceinline__ void diff_row_build(int k, int n, int W, int flat, const uint8_t* sea, double cda,
+                                               double cdm, double dt, const int* nbr, const int8_t* nnb,
+                                               const double* elen, const double* vdist, const double* farea,
+                                               const uint8_t* outlet, double* coef) {
+    const double ck = (sea[k] ? cdm : cda) * dt;
+    double diag = 0.0;
+    for (int s = 0; s < W; s++) coef[(size_t)(s + 1) * n + k] = 0.0;
+    if (farea[k] > 0) {
+        double s1 = 0.0;
+        const double ak = farea[k];
+        for (int s = 0; s < nnb[k]; s++) {
+            double vd = vdist[(size_t)s * n + k];
+            if (vd > 0.0) {
+                int j = nbr[(size_t)s * n + k];
+                double cn = (sea[j] ? cdm : cda) * dt;
+                double c = 0.5 * (ck + cn) / ak;
+                double v = c * vd / elen[(size_t)s * n + k];
+                s1 = s1 + v;
+                coef[(size_t)(s + 1) * n + k] = -v;
+            }
+        }
+        diag = 1.0 + s1;
+    }
+    if (flat && outlet[k]) {
+        diag = 1.0;
+        for (int s = 0; s < W; s++) coef[(size_t)(s + 1) * n + k] = 0.0;
+    }
+    coef[k] = diag;
+}
+
+__global__ void k_sea_of(int n, const double* __restrict__ h, double sl, uint8_t* sea) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < n) sea[k] = h[k] <= sl ? 1 : 0;
+}
+
+// all rows for the mask `sea`
+__global__ void k_diff_rows(int n, int W, int flat, const uint8_t* __restrict__ sea, double cda, double cdm,
+                            double dt, const int* __restrict__ nbr, const int8_t* __restrict__ nnb,
+                            const double* __restrict__ elen, const double* __restrict__ vdist,
+                            const double* __restrict__ farea, const uint8_t* __restrict__ outlet, double* coef) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < n) diff_row_build(k, n, W, flat, sea, cda, cdm, dt, nbr, nnb, elen, vdist, farea, outlet, coef);
+}
+
+// only the rows whose own or a neighbour's mask changed from `old` to `sea`
+__global__ void k_diff_rows_dirty(int n, int W, int flat, const uint8_t* __restrict__ sea,
+                                  const uint8_t* __restrict__ old, double cda, double cdm, double dt,
+                                  const int* __restrict__ nbr, const int8_t* __restrict__ nnb,
+                                  const double* __restrict__ elen, const double* __restrict__ vdist,
+                                  const double* __restrict__ farea, const uint8_t* __restrict__ outlet,
+                                  double* coef) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    bool dirty = sea[k] != old[k];
+    for (int s = 0; s < nnb[k] && !dirty; s++) {
+        int j = nbr[(size_t)s * n + k];
+        if (j >= 0 && sea[j] != old[j]) dirty = true;
+    }
+    if (dirty) diff_row_build(k, n, W, flat, sea, cda, cdm, dt, nbr, nnb, elen, vdist, farea, outlet, coef);
+}
 
 __global__ void k_diff_coef(int n, int W, int flat, const double* __restrict__ h, double sl,
                             double cda, double cdm, double dt, const int* __restrict__ nbr,
@@ -192,90 +260,184 @@ __global__ void k_mask_changed(int n, const double* __restrict__ h, double sl, c
     if (k < n && (uint8_t)(h[k] <= sl) != dsea[k]) *flag = 1;
 }
 
+// ---------------------------------------------------------------------------
+// The whole CG loop in one cooperative launch: three grid barriers per
+// iteration (after A p and its dot, after the update and its dots, after the
+// new direction), convergence decided on the device.  Dot products are block
+// partials in a fixed order; every block sums the partials of all blocks in
+// the same order (one warp, lane-strided, then a shuffle-down tree), so all
+// threads hold bitwise the same scalars and leave the loop together.
+__device__ __forceinline__ void block_sum2(double a, double b, double* out_a, double* out_b) {
+    __shared__ double sa[256], sb[256];
+    sa[threadIdx.x] = a;
+    sb[threadIdx.x] = b;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s) {
+            sa[threadIdx.x] += sa[threadIdx.x + s];
+            sb[threadIdx.x] += sb[threadIdx.x + s];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        *out_a = sa[0];
+        *out_b = sb[0];
+    }
+    __syncthreads();
+}
+
+// sum over blocks of part[i * stride + off], identical in every block
+__device__ __forceinline__ double grid_total(const double* part, int stride, int off, int nb) {
+    __shared__ double tot;
+    if (threadIdx.x < 32) {
+        double acc = 0.0;
+        for (int i = threadIdx.x; i < nb; i += 32) acc += ((volatile const double*)part)[(size_t)i * stride + off];
+        for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+        if (threadIdx.x == 0) tot = acc;
+    }
+    __syncthreads();
+    double t = tot;
+    __syncthreads();
+    return t;
+}
+
+__global__ void __launch_bounds__(256) k_cg_coop(int n, const int* __restrict__ nbr, const int8_t* __restrict__ nnb,
+                                                 const double* __restrict__ coef, const double* __restrict__ farea,
+                                                 const uint8_t* __restrict__ fix, const double* __restrict__ b,
+                                                 double* x, double* r, double* z, double* pp, double* ap,
+                                                 double* part, double rtol, int max_iter, int* it_out,
+                                                 double* res_out) {
+    cg::grid_group grid = cg::this_grid();
+    const int nb = gridDim.x, blk = blockIdx.x;
+    const int gtid = blk * blockDim.x + threadIdx.x, gsz = nb * blockDim.x;
+    double* pc = part;             // initial dots [3 nb]
+    double* pa = part + 3 * nb;    // p.Ap [2 nb]
+    double* pb = part + 5 * nb;    // r.z, r.r [2 nb]
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+    for (int k = gtid; k < n; k += gsz) {
+        a0 += r[k] * z[k];
+        a1 += r[k] * r[k];
+        a2 += b[k] * b[k];
+    }
+    block_sum2(a0, a1, &pc[3 * blk], &pc[3 * blk + 1]);
+    block_sum2(a2, 0.0, &pc[3 * blk + 2], &pa[2 * blk + 1]);
+    grid.sync();
+    double rz = grid_total(pc, 3, 0, nb);
+    const double rr0 = grid_total(pc, 3, 1, nb);
+    const double bnorm = sqrt(grid_total(pc, 3, 2, nb));
+    double relres = bnorm > 0.0 ? sqrt(rr0) / bnorm : 0.0;
+    int it = 0;
+    while (bnorm > 0.0 && relres > rtol && it < max_iter) {
+        double acc = 0.0;
+        for (int k = gtid; k < n; k += gsz) {
+            double y = 0.0;
+            if (!fix[k]) {
+                y = coef[k] * pp[k];
+                for (int s = 0; s < nnb[k]; s++) {
+                    double o = coef[(size_t)(s + 1) * n + k];
+                    if (o == 0.0) continue;
+                    int j = nbr[(size_t)s * n + k];
+                    if (fix[j]) continue;
+                    y = y + o * pp[j];
+                }
+                y = farea[k] * y;
+            }
+            ap[k] = y;
+            acc += pp[k] * y;
+        }
+        block_sum2(acc, 0.0, &pa[2 * blk], &pa[2 * blk + 1]);
+        grid.sync();
+        const double pap = grid_total(pa, 2, 0, nb);
+        const double alpha = (pap != 0.0) ? rz / pap : 0.0;
+        double c0 = 0.0, c1 = 0.0;
+        for (int k = gtid; k < n; k += gsz) {
+            if (fix[k]) continue;
+            x[k] = x[k] + alpha * pp[k];
+            const double rk = r[k] - alpha * ap[k];
+            r[k] = rk;
+            const double zk = rk / (farea[k] * coef[k]);
+            z[k] = zk;
+            c0 += rk * zk;
+            c1 += rk * rk;
+        }
+        block_sum2(c0, c1, &pb[2 * blk], &pb[2 * blk + 1]);
+        grid.sync();
+        const double rzn = grid_total(pb, 2, 0, nb);
+        const double rr = grid_total(pb, 2, 1, nb);
+        const double beta = (rz != 0.0) ? rzn / rz : 0.0;
+        rz = rzn;
+        relres = sqrt(rr) / bnorm;
+        it++;
+        if (!(relres == relres) || relres <= rtol || it >= max_iter) break;
+        for (int k = gtid; k < n; k += gsz) pp[k] = z[k] + beta * pp[k];
+        grid.sync();
+    }
+    if (gtid == 0) {
+        *it_out = it;
+        *res_out = relres;
+    }
+}
+
 int hillslope(gs_plan* p, double* h, double* cum_ed, double* eb, double sealevel, double cda,
               double cdm, double dt, double rtol, int max_iter, gs_stats* st) {
     const int n = (int)p->n;
     GS_TRY(rec_hill(p, h));
     if (n == 0 || (cda == 0.0 && cdm == 0.0)) return GS_OK;
     const int B = 256, G = grid_for(n, B);
-    const int PARTS = 512;
-    int rebuild = 1;
-    if (p->dvalid && p->dvalid_dt == dt && p->dvalid_cda == cda && p->dvalid_cdm == cdm) {
-        GS_CUDA(cudaMemsetAsync(p->i_scalar + 12, 0, sizeof(int), p->stream));
-        launch(p, k_mask_changed, G, B, n, (const double*)h, sealevel, (const uint8_t*)p->dsea, p->i_scalar + 12);
-        GS_LAUNCH();
-        GS_CUDA(cudaMemcpyAsync(&rebuild, p->i_scalar + 12, sizeof(int), cudaMemcpyDeviceToHost, p->stream));
-        GS_CUDA(cudaStreamSynchronize(p->stream));
-    }
-    if (rebuild) {
-        launch(p, k_diff_coef, G, B, n, p->W, p->flat, (const double*)h, sealevel, cda, cdm, dt,
-               (const int*)p->nbr, (const int8_t*)p->nnb, (const double*)p->elen, (const double*)p->vdist,
-               (const double*)p->farea, (const uint8_t*)p->outlet, p->dcoef, p->dsea);
-        GS_LAUNCH();
-        p->dvalid = 1;
-        p->dvalid_dt = dt;
-        p->dvalid_cda = cda;
-        p->dvalid_cdm = cdm;
-    }
+    // operator for the current land/sea mask: every row when the parameters
+    // changed, else only the rows next to a coastline that moved
+    const bool fresh = !(p->dvalid && p->dvalid_dt == dt && p->dvalid_cda == cda && p->dvalid_cdm == cdm);
+    launch(p, k_sea_of, G, B, n, (const double*)h, sealevel, p->dsea2);
+    if (fresh)
+        launch(p, k_diff_rows, G, B, n, p->W, p->flat, (const uint8_t*)p->dsea2, cda, cdm, dt, (const int*)p->nbr,
+               (const int8_t*)p->nnb, (const double*)p->elen, (const double*)p->vdist, (const double*)p->farea,
+               (const uint8_t*)p->outlet, p->dcoef);
+    else
+        launch(p, k_diff_rows_dirty, G, B, n, p->W, p->flat, (const uint8_t*)p->dsea2, (const uint8_t*)p->dsea, cda,
+               cdm, dt, (const int*)p->nbr, (const int8_t*)p->nnb, (const double*)p->elen,
+               (const double*)p->vdist, (const double*)p->farea, (const uint8_t*)p->outlet, p->dcoef);
+    GS_LAUNCH();
+    std::swap(p->dsea, p->dsea2);
+    p->dvalid = 1;
+    p->dvalid_dt = dt;
+    p->dvalid_cda = cda;
+    p->dvalid_cdm = cdm;
     double* hold = p->hl;
     launch(p, k_copy_d2, G, B, n, (const double*)h, hold);
     launch(p, k_cg_init, G, B, n, p->W, p->flat, (const int*)p->nbr, (const int8_t*)p->nnb,
            (const double*)p->dcoef, (const double*)p->farea, (const uint8_t*)p->outlet, (const double*)hold,
            p->cg_x, p->cg_b, p->cg_r, p->cg_z, p->cg_p);
-    // sc[0] = rz, sc[1] = pAp ; sc[2] = rz_new, sc[3] = rr ; sc[4] = bb
-    double* sc = p->red + 4096;
-    launch(p, k_dots<2>, PARTS, 256, n, (const double*)p->cg_r, (const double*)p->cg_z,
-           (const double*)p->cg_b, (const double*)p->cg_b, p->red);
-    launch(p, k_dots_final, 1, 1024, PARTS, 2, (const double*)p->red, sc + 5);
     GS_LAUNCH();
-    double hs[8];
-    GS_CUDA(cudaMemcpyAsync(hs, sc + 5, 2 * sizeof(double), cudaMemcpyDeviceToHost, p->stream));
-    GS_CUDA(cudaStreamSynchronize(p->stream));
-    const double bnorm = sqrt(hs[1]);
-    GS_CUDA(cudaMemcpyAsync(sc, sc + 5, sizeof(double), cudaMemcpyDeviceToDevice, p->stream));   // rz
-    double relres = 0.0;
-    int it = 0;
-    if (bnorm > 0.0) {
-        // residual of the warm start
-        launch(p, k_dots<1>, PARTS, 256, n, (const double*)p->cg_r, (const double*)p->cg_r,
-               (const double*)nullptr, (const double*)nullptr, p->red);
-        launch(p, k_dots_final, 1, 1024, PARTS, 1, (const double*)p->red, sc + 3);
-        GS_LAUNCH();
-        GS_CUDA(cudaMemcpyAsync(hs, sc + 3, sizeof(double), cudaMemcpyDeviceToHost, p->stream));
-        GS_CUDA(cudaStreamSynchronize(p->stream));
-        relres = sqrt(hs[0]) / bnorm;
-        while (relres > rtol && it < max_iter) {
-            launch(p, k_cg_spmv, G, B, n, p->W, p->flat, (const int*)p->nbr, (const int8_t*)p->nnb,
-                   (const double*)p->dcoef, (const double*)p->farea, (const uint8_t*)p->outlet,
-                   (const double*)p->cg_p, p->cg_ap);
-            launch(p, k_dots<1>, PARTS, 256, n, (const double*)p->cg_p, (const double*)p->cg_ap,
-                   (const double*)nullptr, (const double*)nullptr, p->red);
-            launch(p, k_dots_final, 1, 1024, PARTS, 1, (const double*)p->red, sc + 1);
-            launch(p, k_cg_update, G, B, n, p->flat, (const uint8_t*)p->outlet, (const double*)p->farea,
-                   (const double*)p->dcoef, (const double*)sc, p->cg_x, p->cg_r, p->cg_z,
-                   (const double*)p->cg_p, (const double*)p->cg_ap);
-            launch(p, k_dots<2>, PARTS, 256, n, (const double*)p->cg_r, (const double*)p->cg_z,
-                   (const double*)p->cg_r, (const double*)p->cg_r, p->red);
-            launch(p, k_dots_final, 1, 1024, PARTS, 2, (const double*)p->red, sc + 2);
-            launch(p, k_cg_dir, G, B, n, (const double*)(sc + 2), sc, (const double*)p->cg_z, p->cg_p);
-            launch(p, k_cg_rotate, 1, 1, (const double*)(sc + 2), sc);
-            GS_LAUNCH();
-            GS_CUDA(cudaMemcpyAsync(hs, sc + 3, sizeof(double), cudaMemcpyDeviceToHost, p->stream));
-            GS_CUDA(cudaStreamSynchronize(p->stream));
-            relres = sqrt(hs[0]) / bnorm;
-            it++;
-            if (!(relres == relres)) {
-                set_error(GS_ENONFINITE, "hillslope CG produced a non-finite residual");
-                return GS_ENONFINITE;
-            }
-        }
+    int* it_d = p->i_scalar + 12;
+    double* res_d = p->red + 4100;
+    {
+        int nn = n, mi = max_iter;
+        double rt = rtol;
+        void* args[] = {(void*)&nn, (void*)&p->nbr, (void*)&p->nnb, (void*)&p->dcoef, (void*)&p->farea,
+                        (void*)&p->dfix, (void*)&p->cg_b, (void*)&p->cg_x, (void*)&p->cg_r, (void*)&p->cg_z,
+                        (void*)&p->cg_p, (void*)&p->cg_ap, (void*)&p->red, (void*)&rt, (void*)&mi, (void*)&it_d,
+                        (void*)&res_d};
+        cudaEvent_t stop = nullptr;
+        if (p->profiling) prof_begin(p, (const void*)k_cg_coop, &stop);
+        GS_CUDA(cudaLaunchCooperativeKernel((const void*)k_cg_coop, p->coop_blocks, 256, args, 0, p->stream));
+        if (stop) cudaEventRecord(stop, p->stream);
+        p->launches++;
     }
+    launch(p, k_hill_apply, G, B, n, (const double*)hold, (const double*)p->cg_x, dt, h, cum_ed, eb);
+    GS_LAUNCH();
+    int it = 0;
+    double relres = 0.0;
+    GS_CUDA(cudaMemcpyAsync(&it, it_d, sizeof(int), cudaMemcpyDeviceToHost, p->stream));
+    GS_CUDA(cudaMemcpyAsync(&relres, res_d, sizeof(double), cudaMemcpyDeviceToHost, p->stream));
+    GS_CUDA(cudaStreamSynchronize(p->stream));
     if (st) {
         st->cg_iters = it;
         st->cg_relres = relres;
     }
-    launch(p, k_hill_apply, G, B, n, (const double*)hold, (const double*)p->cg_x, dt, h, cum_ed, eb);
-    GS_LAUNCH();
+    if (!(relres == relres)) {
+        set_error(GS_ENONFINITE, "hillslope CG produced a non-finite residual");
+        return GS_ENONFINITE;
+    }
     if (relres > rtol) {
         set_error(GS_EMAXITER, "hillslope CG reached max_iter");
         return GS_EMAXITER;

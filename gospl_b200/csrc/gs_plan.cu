@@ -42,7 +42,7 @@ static void plan_free(gs_plan* p) {
                     p->u_scalar, p->pit_params, p->pit_info, p->filled_lvl, p->filled_vol, p->pit_vol,
                     p->pit_in, p->pit_ev, p->pit_win, p->pit_lvl, p->pit_state, p->seg_keys, p->seg_vals,
                     p->seg_keys2, p->seg_vals2, p->seg_start, p->seg_count, p->cub_tmp, p->nfa, p->wf,
-                    p->hl, p->dcoef, p->dsea, p->cg_r, p->cg_z, p->cg_p, p->cg_ap, p->cg_x, p->cg_b,
+                    p->hl, p->dcoef, p->dsea, p->dsea2, p->dfix, p->cg_r, p->cg_z, p->cg_p, p->cg_ap, p->cg_x, p->cg_b,
                     p->red, p->cub_tmp2, p->pflag, p->pscan};
     for (void* q : ptrs)
         if (q) cudaFree(q);
@@ -159,6 +159,11 @@ int plan_create(int64_t nb, const int32_t* nnb, const int32_t* ngb, const double
     TRYP(upload(&p->farea, std::vector<double>(farea, farea + n)));
     TRYP(upload(&p->larea, std::vector<double>(larea, larea + n)));
     TRYP(upload(&p->outlet, h_out));
+    {
+        std::vector<uint8_t> h_fix(n);
+        for (int i = 0; i < n; i++) h_fix[i] = ((flat && h_out[i]) || !(farea[i] > 0)) ? 1 : 0;
+        TRYP(upload(&p->dfix, h_fix));
+    }
     TRYP(upload(&p->outlet_ids, h_oid));
     TRYP(upload(&p->open_ids, h_open_ids));
     TRYP(upload(&p->open_mask, h_open));
@@ -234,6 +239,7 @@ int plan_create(int64_t nb, const int32_t* nnb, const int32_t* ngb, const double
         TRYP(dalloc(&p->hl, N));
         TRYP(dalloc(&p->dcoef, (size_t)(W + 1) * N));
         TRYP(dalloc(&p->dsea, N));
+        TRYP(dalloc(&p->dsea2, N));
         TRYP(dalloc(&p->cg_r, N));
         TRYP(dalloc(&p->cg_z, N));
         TRYP(dalloc(&p->cg_p, N));

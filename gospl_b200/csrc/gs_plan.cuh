@@ -163,6 +163,8 @@ struct gs_plan {
     // diffusion
     double* dcoef = nullptr;             // [W+1][n]: diag then off-diagonals
     uint8_t* dsea = nullptr;             // sea mask the matrix was built for
+    uint8_t* dsea2 = nullptr;            // sea mask of the current solve (swapped with dsea)
+    uint8_t* dfix = nullptr;             // rows held fixed (flat-model outlets, zero area)
     int dvalid = 0;
     double dvalid_dt = 0, dvalid_cda = 0, dvalid_cdm = 0;
     double* cg_r = nullptr;
@@ -258,6 +260,11 @@ int apply_forces(gs_plan* p, double* h, const double* rain, const double* upsub,
 
 void prof_begin(gs_plan* p, const void* fn, cudaEvent_t* stop);
 int coop_occupancy(int* per_sm);
+__global__ void k_cg_coop(int n, const int* __restrict__ nbr, const int8_t* __restrict__ nnb,
+                          const double* __restrict__ coef, const double* __restrict__ farea,
+                          const uint8_t* __restrict__ fix, const double* __restrict__ b, double* x, double* r,
+                          double* z, double* pp, double* ap, double* part, double rtol, int max_iter, int* it_out,
+                          double* res_out);
 int set_members(gs_plan* p, int nmem, const int64_t* start, const double* maxarea);
 void free_members(gs_plan* p);
 
