@@ -638,14 +638,25 @@ __global__ void __launch_bounds__(128) k_ordered(Op op, int n, const int* __rest
         unsigned rounds = 0, nap = 0;
         while (pending) {
             bool rdy = false;
-            double acc = 0.0;
             if (pending & (1u << lane)) {
+                // predecessor loads go out four at a time before any is looked
+                // at, so a polling round costs one memory latency per four
+                // predecessors; the sum keeps the predecessors' order
                 rdy = true;
-                acc = op.init(node);
-                for (int q = 0; q < np; q++) {
-                    double v = ld_val(&op.x[pj[q]]);
-                    if (is_sent(v)) { rdy = false; break; }
-                    acc = op.combine(acc, pw[q], v);
+                double acc = op.init(node);
+                for (int q0 = 0; q0 < np && rdy; q0 += 4) {
+                    double v[4];
+#pragma unroll
+                    for (int u = 0; u < 4; u++)
+                        if (q0 + u < np) v[u] = ld_val(&op.x[pj[q0 + u]]);
+#pragma unroll
+                    for (int u = 0; u < 4; u++)
+                        if (q0 + u < np && is_sent(v[u])) rdy = false;
+                    if (rdy) {
+#pragma unroll
+                        for (int u = 0; u < 4; u++)
+                            if (q0 + u < np) acc = op.combine(acc, pw[q0 + u], v[u]);
+                    }
                 }
                 if (rdy) st_val(&op.x[node], op.finish(node, acc, 0.0));
             }
