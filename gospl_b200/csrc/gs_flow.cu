@@ -387,15 +387,9 @@ int flow_accumulation(gs_plan* p, const double* h, const double* bl, double seal
                 // receivers and the surface order do not need the flat BFS;
                 // the flat routing and the order's ties do: join it between
                 GS_TRY(receivers(p, p->R, 1.1, surf, sealevel, p->gid, p->rcv, p->dist, p->wgt, p->rslot));
-                GS_TRY(flow_order(p, surf, p->order));
-                GS_TRY(fill_join(p, st));
-                GS_TRY(flow_direction_post(p, surf, true, lfill, pit_ids, flat_dirs, sealevel, p->rcv, p->dist,
-                                           p->wgt, p->rslot, lsink, sea));
-                if (!allbig)
-                    launch(p, k_lsink_keep, G, B, n, (const int*)p->vmember, (const uint8_t*)p->mbig,
-                           (const uint8_t*)p->lsink_prev, lsink);
-                GS_TRY(rec_pass_rebuild(p, step, surf));
-                GS_TRY(flow_order_ties(p, p->pdir, p->order));
+                // the water surface differs from h only on lakes: reuse h's order
+                GS_TRY(flow_order_from(p, surf, h, p->order_i, p->order));
+                GS_TRY(flow_order_ties_prepare(p));
                 launch(p, k_div, G, B, (int64_t)n, (const double*)p->nfa, dt, p->q2);
                 launch(p, k_chunk_sum, p->nchunk, 256, (const int*)p->chunk_lo, (const double*)p->q2,
                        p->chunk_part);
@@ -404,6 +398,14 @@ int flow_accumulation(gs_plan* p, const double* h, const double* bl, double seal
                 GS_LAUNCH();
                 GS_CUDA(cudaMemcpyAsync(p->h_mresid, p->mresid, sizeof(double) * nm, cudaMemcpyDeviceToHost,
                                         p->stream));
+                GS_TRY(fill_join(p, st));
+                GS_TRY(flow_direction_post(p, surf, true, lfill, pit_ids, flat_dirs, sealevel, p->rcv, p->dist,
+                                           p->wgt, p->rslot, lsink, sea));
+                if (!allbig)
+                    launch(p, k_lsink_keep, G, B, n, (const int*)p->vmember, (const uint8_t*)p->mbig,
+                           (const uint8_t*)p->lsink_prev, lsink);
+                GS_TRY(rec_pass_rebuild(p, step, surf));
+                GS_TRY(flow_order_ties(p, p->pdir, p->order));
                 GS_CUDA(cudaStreamSynchronize(p->stream));
                 bool anysolve = false, allsolve = true;
                 for (int m = 0; m < nm; m++) {

@@ -54,6 +54,7 @@ struct gs_plan {
     int* order = nullptr;                // topological order of the last flow sweep
     int* order_i = nullptr;              // order of the snapshot (unfilled) flow graph
     int order_i_valid = 0;
+    int tie_m = 0;                       // vertices in surface tie groups of the last flow_order
     unsigned long long* okey = nullptr;
     unsigned long long* okey2 = nullptr;
     unsigned* ok32 = nullptr;
@@ -238,7 +239,12 @@ int fill_join(gs_plan* p, gs_stats* st);
 // topological order of a flow graph: vertices by surface descending
 // (flow_order), then surface ties by flat distance descending (flow_order_ties)
 int flow_order(gs_plan* p, const double* surface, int* order);
-int flow_order_ties(gs_plan* p, const int* pdir, int* order);
+// same order as flow_order(surface), built from the order of a surface that
+// differs from it at few vertices (base_order = flow_order(base_surface))
+int flow_order_from(gs_plan* p, const double* surface, const double* base_surface, const int* base_order,
+                    int* order);
+int flow_order_ties_prepare(gs_plan* p);   // after flow_order: tie groups of the surface
+int flow_order_ties(gs_plan* p, const int* pdir, int* order);   // after prepare: ties by pdir
 int flow_prepare(gs_plan* p, const int* rcv, const double* wgt, const int8_t* rslot, double* x, const int* order,
                  int* bad_host);
 int flow_run(gs_plan* p, const int* rcv, const double* wgt, const int8_t* rslot, const double* b,

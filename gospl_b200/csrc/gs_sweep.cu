@@ -730,11 +730,7 @@ static int order_by_surface(gs_plan* p, const double* z, int* order) {
     return GS_OK;
 }
 
-// Breaks the surface ties of order_by_surface by flat distance descending
-// (ties of both by vertex id): only the members of tie groups are re-sorted,
-// by (group start, ~(pdir + 1)), and written back to their positions.  Gives
-// the order of a stable sort by (surface desc, pdir desc).
-static int order_ties(gs_plan* p, const int* pdir, int* order) {
+static int order_ties_prepare(gs_plan* p) {
     const int n = (int)p->n;
     const int B = 256, G = grid_for(n, B);
     int* run0 = p->oval;
@@ -753,23 +749,43 @@ static int order_ties(gs_plan* p, const int* pdir, int* order) {
     GS_CUDA(cudaMemcpyAsync(&last[0], scan + n - 1, sizeof(int), cudaMemcpyDeviceToHost, p->stream));
     GS_CUDA(cudaMemcpyAsync(&last[1], flag + n - 1, sizeof(int), cudaMemcpyDeviceToHost, p->stream));
     GS_CUDA(cudaStreamSynchronize(p->stream));
-    const int m = last[0] + last[1];
+    p->tie_m = last[0] + last[1];
+    return GS_OK;
+}
+
+static int order_ties_finish(gs_plan* p, const int* pdir, int* order) {
+    const int n = (int)p->n;
+    const int B = 256, G = grid_for(n, B);
+    const int m = p->tie_m;
     if (m == 0) return GS_OK;
+    const int* run = (const int*)p->ok32b;
+    const int* flag = p->oval2;
+    const int* scan = (const int*)p->ok32;
     int* cval = p->oval;
-    int* cval2 = (int*)p->ok32b;
-    int* cpos = p->pos;  // rewritten by the positions pass that follows
-    launch(p, k_tie_compact, G, B, n, (const int*)run, (const int*)flag, (const int*)scan, (const int*)order, pdir,
-           p->okey, cval, cpos);
+    int* cval2 = (int*)p->ok32b;   // run is consumed by the compaction before the sort writes here
+    int* cpos = p->pos;            // rewritten by the positions pass that follows
+    launch(p, k_tie_compact, G, B, n, run, flag, scan, (const int*)order, pdir, p->okey, cval, cpos);
     GS_LAUNCH();
     int hb = 1;
     while ((1LL << hb) <= (long long)n && hb < 31) hb++;
-    bytes = p->cub_bytes;
+    size_t bytes = p->cub_bytes;
     GS_CUDA(cub::DeviceRadixSort::SortPairs(p->cub_tmp, bytes, p->okey, p->okey2, cval, cval2, m, 0, 32 + hb,
                                             p->stream));
     p->launches++;
     launch(p, k_tie_scatter, grid_for(m, B), B, m, (const int*)cpos, (const int*)cval2, order);
     GS_LAUNCH();
     return GS_OK;
+}
+
+// Breaks the surface ties of order_by_surface by flat distance descending
+// (ties of both by vertex id): only the members of tie groups are re-sorted,
+// by (group start, ~(pdir + 1)), and written back to their positions.  Gives
+// the order of a stable sort by (surface desc, pdir desc).  The tie groups
+// depend on the surface only (order_ties_prepare, which reads their count back
+// to the host); the flat distances are needed only by order_ties_finish.
+static int order_ties(gs_plan* p, const int* pdir, int* order) {
+    GS_TRY(order_ties_prepare(p));
+    return order_ties_finish(p, pdir, order);
 }
 
 // Checks that every weighted edge goes forward in `order`; the result
@@ -786,9 +802,118 @@ static int order_check_async(gs_plan* p, const int* rcv, const double* w, const 
     return GS_OK;
 }
 
+// ---- order of a surface that differs from an already ordered one in few
+// places (the cascade's water surface against h): the unchanged vertices keep
+// their relative order from the base order, the changed ones are sorted
+// alone, and the two sorted runs are merged by (key, vertex id) ranks.
+__global__ void k_changed(int n, const double* __restrict__ z, const double* __restrict__ zb, int* flag) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) flag[i] = dkey(z[i]) != dkey(zb[i]) ? 1 : 0;
+}
+
+__global__ void k_changed_compact(int n, const int* __restrict__ flag, const int* __restrict__ scan,
+                                  const double* __restrict__ z, unsigned long long* ckey, int* cid) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n || !flag[i]) return;
+    ckey[scan[i]] = ~dkey(z[i]);
+    cid[scan[i]] = i;
+}
+
+__global__ void k_kept_flag(int n, const int* __restrict__ base, const int* __restrict__ flag, int* kf) {
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < n) kf[t] = flag[base[t]] ? 0 : 1;
+}
+
+__global__ void k_kept_compact(int n, const int* __restrict__ base, const int* __restrict__ kf,
+                               const int* __restrict__ scan, const double* __restrict__ z, unsigned long long* akey,
+                               int* aid) {
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n || !kf[t]) return;
+    const int v = base[t];
+    akey[scan[t]] = ~dkey(z[v]);
+    aid[scan[t]] = v;
+}
+
+// number of entries of the sorted run (k, id) that come before (key, vid)
+__device__ __forceinline__ int rank_in(const unsigned long long* __restrict__ k, const int* __restrict__ id, int len,
+                                       unsigned long long key, int vid) {
+    int lo = 0, hi = len;
+    while (lo < hi) {
+        int mid = (lo + hi) >> 1;
+        if (k[mid] < key || (k[mid] == key && id[mid] < vid)) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo;
+}
+
+__global__ void k_merge_runs(int na, const unsigned long long* __restrict__ akey, const int* __restrict__ aid,
+                             int nc, const unsigned long long* __restrict__ ckey, const int* __restrict__ cid,
+                             int* order, unsigned long long* okey) {
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < na) {
+        const int o = t + rank_in(ckey, cid, nc, akey[t], aid[t]);
+        order[o] = aid[t];
+        okey[o] = akey[t];
+    } else if (t < na + nc) {
+        const int c = t - na;
+        const int o = c + rank_in(akey, aid, na, ckey[c], cid[c]);
+        order[o] = cid[c];
+        okey[o] = ckey[c];
+    }
+}
+
+// The order of `surface` (descending, ties by vertex id), given the order
+// `base` of `zb` built by order_by_surface; sorted keys left in okey2 as
+// order_by_surface leaves them.
+static int order_by_surface_from(gs_plan* p, const double* z, const double* zb, const int* base, int* order) {
+    const int n = (int)p->n;
+    const int B = 256, G = grid_for(n, B);
+    int* flag = p->pos;
+    int* cscan = (int*)p->ok32;
+    launch(p, k_changed, G, B, n, z, zb, flag);
+    GS_LAUNCH();
+    size_t bytes = p->cub_bytes;
+    GS_CUDA(cub::DeviceScan::ExclusiveSum(p->cub_tmp, bytes, (const int*)flag, cscan, n, p->stream));
+    p->launches++;
+    int last[2];
+    GS_CUDA(cudaMemcpyAsync(&last[0], cscan + n - 1, sizeof(int), cudaMemcpyDeviceToHost, p->stream));
+    GS_CUDA(cudaMemcpyAsync(&last[1], flag + n - 1, sizeof(int), cudaMemcpyDeviceToHost, p->stream));
+    // kept vertices, in the base order
+    int* kf = (int*)p->ok32b;
+    int* kscan = p->cnt;
+    launch(p, k_kept_flag, G, B, n, base, (const int*)flag, kf);
+    GS_LAUNCH();
+    bytes = p->cub_bytes;
+    GS_CUDA(cub::DeviceScan::ExclusiveSum(p->cub_tmp, bytes, (const int*)kf, kscan, n, p->stream));
+    p->launches++;
+    launch(p, k_kept_compact, G, B, n, base, (const int*)kf, (const int*)kscan, zb, p->don_k, p->queue);
+    launch(p, k_changed_compact, G, B, n, (const int*)flag, (const int*)cscan, z, p->okey, p->oval);
+    GS_LAUNCH();
+    GS_CUDA(cudaStreamSynchronize(p->stream));
+    const int nc = last[0] + last[1], na = n - nc;
+    if (nc > 0) {
+        int hb = 64;
+        bytes = p->cub_bytes;
+        GS_CUDA(cub::DeviceRadixSort::SortPairs(p->cub_tmp, bytes, p->okey, p->basinL, p->oval, p->oval2, nc, 0, hb,
+                                                p->stream));
+        p->launches++;
+    }
+    launch(p, k_merge_runs, grid_for(n, B), B, na, (const unsigned long long*)p->don_k, (const int*)p->queue, nc,
+           (const unsigned long long*)p->basinL, (const int*)p->oval2, order, p->okey2);
+    GS_LAUNCH();
+    return GS_OK;
+}
+
 int flow_order(gs_plan* p, const double* surface, int* order) { return order_by_surface(p, surface, order); }
 
-int flow_order_ties(gs_plan* p, const int* pdir, int* order) { return order_ties(p, pdir, order); }
+int flow_order_from(gs_plan* p, const double* surface, const double* base_surface, const int* base_order,
+                    int* order) {
+    return order_by_surface_from(p, surface, base_surface, base_order, order);
+}
+
+int flow_order_ties_prepare(gs_plan* p) { return order_ties_prepare(p); }
+
+int flow_order_ties(gs_plan* p, const int* pdir, int* order) { return order_ties_finish(p, pdir, order); }
 
 static int ordered_status(gs_plan* p, int* st) {
     unsigned h[8];
