@@ -159,17 +159,34 @@ __global__ void k_cross_edges(int n, const double* __restrict__ h, const double*
     if (ledge[rc] >= 0) return;
     const double level = dsc[D_LEVEL];
     const double zc = h[c] - level;
+    // one edge per distinct neighbouring basin, with the smallest pass height
+    // (parallel edges of larger weight can never lower a level further)
+    int rb[MAXW];
+    double wb[MAXW];
+    int nb_ = 0;
     for (int s = 0; s < nnb[c]; s++) {
         int j = nbr[(size_t)s * n + c];
         if (j < 0 || ledge[j] == -2) continue;
         int rj = root[j];
         if (rj == rc) continue;
         double zj = h[j] - level;
+        double w = zc > zj ? zc : zj;
+        int q = 0;
+        while (q < nb_ && rb[q] != rj) q++;
+        if (q == nb_) {
+            rb[nb_] = rj;
+            wb[nb_] = w;
+            nb_++;
+        } else if (w < wb[q]) {
+            wb[q] = w;
+        }
+    }
+    for (int q = 0; q < nb_; q++) {
         int pos = agg_append(count);
         if (pos < cap) {
             xu[pos] = rc;
-            xv[pos] = rj;
-            xw[pos] = zc > zj ? zc : zj;
+            xv[pos] = rb[q];
+            xw[pos] = wb[q];
         }
     }
 }
