@@ -723,19 +723,32 @@ __global__ void __launch_bounds__(256) k_relax_active(int m, const int* __restri
     int r = 1;
     for (; r <= max_rounds; r++) {
         int changed = 0;
-        for (int e = gtid; e < m; e += gsz) {
-            const int v = xv[e];
-            if (((volatile int*)stamp)[v] < r - 1) continue;
-            const unsigned long long lv = ((volatile unsigned long long*)L)[v];
-            if (lv == ~0ULL) continue;
-            const unsigned long long w = dkey(xw[e]);
-            const unsigned long long cand = w > lv ? w : lv;
-            const int u = xu[e];
-            if (cand < ((volatile unsigned long long*)L)[u]) {
-                const unsigned long long old = atomicMin(&L[u], cand);
-                if (cand < old) {
-                    ((volatile int*)stamp)[u] = r;
-                    changed = 1;
+        // four edges per thread and pass: their source ids and stamps are
+        // loaded before any is used, so the gathers overlap
+        for (int e0 = gtid; e0 < m; e0 += 4 * gsz) {
+            int v[4], sv[4];
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                const int e = e0 + q * gsz;
+                v[q] = e < m ? xv[e] : -1;
+            }
+#pragma unroll
+            for (int q = 0; q < 4; q++) sv[q] = v[q] >= 0 ? ((volatile int*)stamp)[v[q]] : -2;
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                if (sv[q] < r - 1) continue;
+                const int e = e0 + q * gsz;
+                const unsigned long long lv = ((volatile unsigned long long*)L)[v[q]];
+                if (lv == ~0ULL) continue;
+                const unsigned long long w = dkey(xw[e]);
+                const unsigned long long cand = w > lv ? w : lv;
+                const int u = xu[e];
+                if (cand < ((volatile unsigned long long*)L)[u]) {
+                    const unsigned long long old = atomicMin(&L[u], cand);
+                    if (cand < old) {
+                        ((volatile int*)stamp)[u] = r;
+                        changed = 1;
+                    }
                 }
             }
         }
