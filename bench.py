@@ -224,13 +224,12 @@ def main():
             pg.barrier()
         torch.cuda.synchronize(dev)
 
-    for _ in range(args.warmup):
-        model.step()
-    # clock sampling starts here; one more untimed step runs while nvidia-smi
-    # comes up, so the samples cover the timed region
+    # clock sampling starts before the warm-up and nvidia-smi gets a second to
+    # come up (no steps run meanwhile: the timed steps are those of the
+    # configured run), so its samples cover the timed region
     clk = Clocks(local)
-    t_wait = time.perf_counter()
-    while time.perf_counter() - t_wait < 1.0:
+    time.sleep(1.0)
+    for _ in range(args.warmup):
         model.step()
     barrier()
     # ---- timed region: device-resident state ----
