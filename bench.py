@@ -167,7 +167,7 @@ def main():
     ap.add_argument("--level", type=int, default=9)
     ap.add_argument("--cpu-level", type=int, default=7)
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--workload", default="sphere", choices=["sphere", "ensemble"])
+    ap.add_argument("--workload", default="sphere", choices=["sphere", "planar", "ensemble"])
     ap.add_argument("--members", type=int, default=256)
     ap.add_argument("--loop", action="store_true", help="ensemble: also time the per-member loop")
     ap.add_argument("--adjoint-steps", type=int, default=4, help="sphere: steps of the adjoint timing (0: skip)")
@@ -197,6 +197,12 @@ def main():
     ens_members = None
     if args.workload == "sphere":
         c, f, z, rain, up, p = sphere_inputs(args.level)
+        p = dict(p, rain=rain, upsub=up, tEnd=1.0e30)
+        mesh = FVMesh(c, f, p["bc"], device=dev)
+        model = Model(coords=c, cells=f, elev=z, params=p, mesh=mesh, device=dev)
+    elif args.workload == "planar":
+        from gospl_b200 import synthetic as S
+        c, f, z, rain, up, p = S.planar_config()
         p = dict(p, rain=rain, upsub=up, tEnd=1.0e30)
         mesh = FVMesh(c, f, p["bc"], device=dev)
         model = Model(coords=c, cells=f, elev=z, params=p, mesh=mesh, device=dev)
@@ -332,18 +338,22 @@ def main():
             m.destroy()
 
     cpu = None
-    if rank == 0 and not args.no_cpu and ens_members is None:
+    if rank == 0 and not args.no_cpu and args.workload == "sphere":
         v, nn, st, dt = cpu_sample(args.cpu_level, 2)
         cpu = {"value": v, "unit": "vertex-steps/s", "cores": 1, "kind": "port",
                "sample": "oracle (C + numpy restatement of the reference path) on icosphere level %d "
                          "(%d vertices), %d physics steps, %.1f s" % (args.cpu_level, nn, st, dt)}
     if rank == 0:
         line = {
-            "metric": METRIC if args.workload == "sphere" else "landscape vertex-steps/s, planar ensemble",
+            "metric": {"sphere": METRIC, "planar": "landscape vertex-steps/s, 20k planar",
+                       "ensemble": "landscape vertex-steps/s, planar ensemble"}[args.workload],
             "value": value, "unit": "vertex-steps/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
-            "scaling": "weak" if args.workload == "sphere" else "strong",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded sphere, SH relief)",
+            "scaling": "strong" if args.workload == "ensemble" else "weak",
+            "vs_baseline": None, "dtype": "f64",
+            "data": {"sphere": "synthetic (seeded sphere, SH relief)",
+                     "planar": "synthetic (seeded jittered hex mesh, fractal relief)",
+                     "ensemble": "synthetic (seeded planar members, fractal relief)"}[args.workload],
             "config": config_of(args, n, n_all, world),
             "e2e": {"value": e2e, "unit": "vertex-steps/s", "h2d_bytes_per_step": 8 * n, "d2h_bytes_per_step": 8 * n},
             "roofline": {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": hbm,
@@ -409,6 +419,12 @@ def config_of(args, n, n_all, world):
                 "vertices": n, "global_batch": world, "seq_len": 0,
                 "parallelism": "replicas" if world > 1 else "single",
                 "l2": "working set > 126 MB L2 (mesh arrays alone ~1 GB)"}
+    if args.workload == "planar":
+        return {"workload": "planar landscape, 20,000-vertex jittered hex lattice over 100 x 100 km, fractal "
+                            "relief 0-50 m, fixed boundaries, U = 1 mm/yr, rain 1 m/yr, K = 2e-6, dt = 1000 yr",
+                "vertices": n, "global_batch": world, "seq_len": 0,
+                "parallelism": "replicas" if world > 1 else "single",
+                "l2": "working set fits in L2 (launch-latency bound)"}
     return {"workload": "ensemble of %d planar landscapes (%d vertices in all; sizes log-uniform 1e4-5e5, "
                         "250 m spacing, own K and rain), full physics step, all members per launch"
                         % (args.members, n_all),
