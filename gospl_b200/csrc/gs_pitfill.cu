@@ -231,9 +231,22 @@ __global__ void k_fill_int(int n, int* a, int v) {
     if (i < n) a[i] = v;
 }
 
-__global__ void k_iota(int n, int* a) {
+// union-find start: every cell above sea level points to its smallest-id
+// equal-fill neighbour (or itself), so the linking pass starts from short
+// chains instead of singletons
+__global__ void k_uf_init(int n, const double* __restrict__ f, double sl, const int* __restrict__ nbr,
+                          const int8_t* __restrict__ nnb, int* comp) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) a[i] = i;
+    if (i >= n) return;
+    int best = i;
+    const double fi = f[i];
+    if (fi > sl) {
+        for (int s = 0; s < nnb[i]; s++) {
+            int j = nbr[(size_t)s * n + i];
+            if (j >= 0 && j < best && f[j] == fi) best = j;
+        }
+    }
+    comp[i] = best;
 }
 
 __global__ void k_uf_link(int n, const double* __restrict__ f, double sl, const int* __restrict__ nbr,
@@ -1031,7 +1044,8 @@ int fill_elevation(gs_plan* p, const double* h, double sealevel, double ofill, d
     GS_LAUNCH();
 
     // label_pits: equal-fill components of cells above sea level
-    launch(p, k_iota, G, B, n, p->comp);
+    launch(p, k_uf_init, G, B, n, (const double*)lfill, sealevel, (const int*)p->nbr, (const int8_t*)p->nnb,
+           p->comp);
     launch(p, k_uf_link, G, B, n, (const double*)lfill, sealevel, (const int*)p->nbr,
            (const int8_t*)p->nnb, p->comp);
     launch(p, k_uf_flatten, G, B, n, p->comp);
