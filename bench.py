@@ -171,6 +171,7 @@ def main():
     ap.add_argument("--members", type=int, default=256)
     ap.add_argument("--loop", action="store_true", help="ensemble: also time the per-member loop")
     ap.add_argument("--adjoint-steps", type=int, default=4, help="sphere: steps of the adjoint timing (0: skip)")
+    ap.add_argument("--no-tune", action="store_true", help="keep the default launch shapes")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -230,6 +231,13 @@ def main():
             pg.barrier()
         torch.cuda.synchronize(dev)
 
+    tuned = None
+    if not args.no_tune:
+        from gospl_b200 import autotune
+        best, table = autotune.tune(model, steps=2)
+        tuned = {"sweep_blocks_per_sm": best[0], "coop_blocks_per_sm": best[1],
+                 "ms_per_step": {"%d,%d" % k: round(v, 4) for k, v in table.items()},
+                 "what": "launch shapes timed on this landscape before the warm-up (state restored after each)"}
     # clock sampling starts before the warm-up and nvidia-smi gets a second to
     # come up (no steps run meanwhile: the timed steps are those of the
     # configured run), so its samples cover the timed region
@@ -370,6 +378,7 @@ def main():
             "cpu_baseline": cpu,
             "stats": stats.get("flow"),
             "loop_baseline": loop,
+            "tuned": tuned,
             "adjoint": adj,
             "setup_s": setup_s,
         }

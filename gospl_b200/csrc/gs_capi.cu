@@ -84,6 +84,13 @@ int gs_plan_create(int64_t nb, const int32_t* nnb, const int32_t* ngb, const dou
 
 int gs_plan_destroy(gs_plan* plan) { GS_GUARD(return gs::plan_destroy(plan);) }
 
+int gs_plan_tune(gs_plan* plan, int32_t knob, int32_t value) {
+    NEED(plan);
+    GS_GUARD(return gs::plan_tune(plan, knob, value);)
+}
+
+int gs_plan_tuning(const gs_plan* plan, int32_t knob) { return plan ? gs::plan_tuning(plan, knob) : -1; }
+
 int gs_plan_record(gs_plan* plan, int32_t nslots) {
     NEED(plan);
     GS_GUARD(return gs::record_setup(plan, nslots);)

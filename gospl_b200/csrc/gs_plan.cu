@@ -102,8 +102,13 @@ int plan_create(int64_t nb, const int32_t* nnb, const int32_t* ngb, const double
         // (checked against occupancy), enough warps to hide the gather latency
         // of the edge-parallel rounds
         int per_sm = 0;
-        if (coop_occupancy(&per_sm) == 0 && per_sm > 0) p->coop_blocks = p->sm_count * std::min(per_sm, 4);
-        else p->coop_blocks = p->sm_count;
+        if (coop_occupancy(&per_sm) == 0 && per_sm > 0) {
+            p->coop_max_per_sm = per_sm;
+            p->coop_blocks = p->sm_count * std::min(per_sm, 4);
+        } else {
+            p->coop_max_per_sm = 1;
+            p->coop_blocks = p->sm_count;
+        }
     }
 
     std::vector<int> h_nbr((size_t)W * n, -1);
@@ -376,6 +381,37 @@ int set_members(gs_plan* p, int nmem, const int64_t* start, const double* maxare
     GS_CUDA(cudaGetLastError());
     GS_CUDA(cudaStreamSynchronize(p->stream));
     return GS_OK;
+}
+
+// launch-shape knobs (GS_TUNE_*): blocks per SM of the ordered sweeps
+// (1..32) and of the cooperative kernels (1..their occupancy limit)
+int plan_tune(gs_plan* p, int knob, int value) {
+    if (knob == GS_TUNE_SWEEP_BLOCKS) {
+        if (value < 1 || value > 32) {
+            set_error(GS_EINVAL, "tune: sweep blocks per SM must be in 1..32");
+            return GS_EINVAL;
+        }
+        p->sweep_per_sm = value;
+        return GS_OK;
+    }
+    if (knob == GS_TUNE_COOP_BLOCKS) {
+        if (value < 1 || value > p->coop_max_per_sm) {
+            set_error(GS_EINVAL, "tune: cooperative blocks per SM must be in 1.." +
+                                     std::to_string(p->coop_max_per_sm) + " (co-residency limit)");
+            return GS_EINVAL;
+        }
+        p->coop_blocks = p->sm_count * value;
+        return GS_OK;
+    }
+    set_error(GS_EINVAL, "tune: unknown knob");
+    return GS_EINVAL;
+}
+
+int plan_tuning(const gs_plan* p, int knob) {
+    if (knob == GS_TUNE_SWEEP_BLOCKS) return p->sweep_per_sm;
+    if (knob == GS_TUNE_COOP_BLOCKS) return p->coop_blocks / std::max(p->sm_count, 1);
+    if (knob == GS_TUNE_COOP_BLOCKS + 1) return p->coop_max_per_sm;
+    return -1;
 }
 
 int plan_destroy(gs_plan* p) {

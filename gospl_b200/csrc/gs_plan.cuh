@@ -16,6 +16,8 @@ struct gs_plan {
     int64_t launches = 0;
     int sm_count = 148;
     int coop_blocks = 148;               // co-resident 256-thread blocks for cooperative launches
+    int coop_max_per_sm = 1;             // occupancy limit of the cooperative kernels
+    int sweep_per_sm = 8;                // 128-thread blocks per SM of the ordered sweeps
 
     // mesh, slot-major [W][n]
     int* nbr = nullptr;          // FVnID (-1 pad)
@@ -272,6 +274,8 @@ __global__ void k_cg_coop(int n, const int* __restrict__ nbr, const int8_t* __re
                           double* z, double* pp, double* ap, double* part, double rtol, int max_iter, int* it_out,
                           double* res_out);
 int set_members(gs_plan* p, int nmem, const int64_t* start, const double* maxarea);
+int plan_tune(gs_plan* p, int knob, int value);
+int plan_tuning(const gs_plan* p, int knob);
 void free_members(gs_plan* p);
 
 // issues the plan's work on another stream (and cub scratch) for its scope

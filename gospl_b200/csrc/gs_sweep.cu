@@ -950,7 +950,7 @@ int flow_run(gs_plan* p, const int* rcv, const double* wgt, const int8_t* rslot,
     if (!ok) return flow_solve_counted(p, rcv, wgt, rslot, b, x, cycle_nodes);
     GS_CUDA(cudaMemsetAsync(p->ctr, 0, sizeof(unsigned) * 8, p->stream));
     FlowOrd op{n, p->nbr, p->don_mask, p->don_k, p->sorder, wgt, b, x};
-    launch(p, k_ordered<FlowOrd>, p->sm_count * 8, 128, op, n, (const int*)order, p->ctr, SWEEP_BUDGET_NS);
+    launch(p, k_ordered<FlowOrd>, p->sm_count * p->sweep_per_sm, 128, op, n, (const int*)order, p->ctr, SWEEP_BUDGET_NS);
     GS_LAUNCH();
     int st = 0;
     GS_TRY(ordered_status(p, &st));
@@ -1011,7 +1011,7 @@ int spl_sweep(gs_plan* p, const int* rcv, const double* c, const int8_t* rslot, 
     GS_CUDA(cudaMemsetAsync(p->ctr, 0, sizeof(unsigned) * 8, p->stream));
     launch(p, k_fill_sent, grid_for(n, 256), 256, n, s);
     SplOrd op{n, p->R, rcv, c, hold, s};
-    launch(p, k_ordered<SplOrd>, p->sm_count * 8, 128, op, n, (const int*)p->order2, p->ctr, SWEEP_BUDGET_NS);
+    launch(p, k_ordered<SplOrd>, p->sm_count * p->sweep_per_sm, 128, op, n, (const int*)p->order2, p->ctr, SWEEP_BUDGET_NS);
     GS_LAUNCH();
     int st = 0;
     GS_TRY(ordered_status(p, &st));
@@ -1030,7 +1030,7 @@ int sweep_flow_adjoint(gs_plan* p, const int* rcv, const double* wgt, const int*
     GS_CUDA(cudaMemsetAsync(p->ctr, 0, sizeof(unsigned) * 8, p->stream));
     launch(p, k_fill_sent, grid_for(n, 256), 256, n, y);
     FlowAdjOrd op{n, p->R, rcv, wgt, g, y};
-    launch(p, k_ordered<FlowAdjOrd>, p->sm_count * 8, 128, op, n, (const int*)p->order2, p->ctr, SWEEP_BUDGET_NS);
+    launch(p, k_ordered<FlowAdjOrd>, p->sm_count * p->sweep_per_sm, 128, op, n, (const int*)p->order2, p->ctr, SWEEP_BUDGET_NS);
     GS_LAUNCH();
     int st = 0;
     GS_TRY(ordered_status(p, &st));
@@ -1054,7 +1054,7 @@ int sweep_spl_adjoint(gs_plan* p, const int* rcv, const double* wgt, const int8_
     GS_CUDA(cudaMemsetAsync(p->ctr, 0, sizeof(unsigned) * 8, p->stream));
     launch(p, k_fill_sent, grid_for(n, 256), 256, n, y);
     SplAdjOrd op{n, p->R, p->nbr, p->don_mask, p->don_k, p->sorder, c, g, y};
-    launch(p, k_ordered<SplAdjOrd>, p->sm_count * 8, 128, op, n, order, p->ctr, SWEEP_BUDGET_NS);
+    launch(p, k_ordered<SplAdjOrd>, p->sm_count * p->sweep_per_sm, 128, op, n, order, p->ctr, SWEEP_BUDGET_NS);
     GS_LAUNCH();
     int st = 0;
     GS_TRY(ordered_status(p, &st));

@@ -78,6 +78,20 @@ int gs_plan_destroy(gs_plan* plan);
  */
 int gs_plan_set_members(gs_plan* plan, int32_t nmem, const int64_t* start, const double* maxarea);
 int gs_plan_set_stream(gs_plan* plan, void* cuda_stream);
+/*
+ * Launch-shape knobs (no counterpart in the reference).  GS_TUNE_SWEEP_BLOCKS:
+ * 128-thread blocks per SM of the ordered dependency sweeps (1..32, default
+ * 8).  GS_TUNE_COOP_BLOCKS: 256-thread blocks per SM of the cooperative
+ * kernels (basin relaxation, grid BFS, hillslope CG; 1..their co-residency
+ * limit, default min(limit, 4)); gs_plan_tuning(plan, GS_TUNE_COOP_BLOCKS + 1)
+ * returns that limit.  Results do not depend on the knobs beyond the
+ * rounding of the hillslope CG's inner products (block partial sums); speed
+ * does (gospl_b200.autotune picks them by timing steps).
+ */
+#define GS_TUNE_SWEEP_BLOCKS 1
+#define GS_TUNE_COOP_BLOCKS 2
+int gs_plan_tune(gs_plan* plan, int32_t knob, int32_t value);
+int gs_plan_tuning(const gs_plan* plan, int32_t knob);
 /* Number of device kernels this plan launched since creation. */
 int64_t gs_plan_launches(const gs_plan* plan);
 /* Per-kernel timing: when enabled, every launch of the plan is bracketed by
