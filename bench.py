@@ -167,7 +167,7 @@ def main():
     ap.add_argument("--level", type=int, default=9)
     ap.add_argument("--cpu-level", type=int, default=7)
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--workload", default="sphere", choices=["sphere", "planar", "ensemble"])
+    ap.add_argument("--workload", default="sphere", choices=["sphere", "planar", "ensemble", "precision"])
     ap.add_argument("--members", type=int, default=256)
     ap.add_argument("--loop", action="store_true", help="ensemble: also time the per-member loop")
     ap.add_argument("--adjoint-steps", type=int, default=4, help="sphere: steps of the adjoint timing (0: skip)")
@@ -188,6 +188,9 @@ def main():
 
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
+    if args.workload == "precision":
+        run_precision(args, dev)
+        return
     pg = None
     if world > 1:
         import datetime
@@ -419,6 +422,67 @@ def adjoint_ratio(model, k, stream, dev, pg):
             "checkpoint_every": k, "what": "adjoint step = replay of the step with recording + its reverse "
                                           "(gradients wrt K, U, rain and h0)",
             "finite": bool(torch.isfinite(gK).all() and torch.isfinite(gh).all())}
+
+
+def run_precision(args, dev):
+    """FP32-bulk form against the plain FP64 path on the 10.5M-vertex sphere
+    (icosphere level 10, SH relief to degree 512 scaled to -5000..+4000 m,
+    rain and uplift as for the 2.6M sphere, dt = 5000 yr): the same steps from
+    the same state in both, wall time per step of each and the relative error
+    of drainage area, erosion rate and elevation of the FP32 form."""
+    import torch
+    from gospl_b200 import _lib
+    from gospl_b200 import synthetic as S
+    from gospl_b200.mesh import FVMesh
+    from gospl_b200.model import Model
+    level = args.level if args.level != 9 else 10
+    c, f, z, rain, up, p = S.sphere_config(level=level, lmax=512, zlo=-5000.0, zhi=4000.0, dt=5000.0)
+    p = dict(p, rain=rain, upsub=up, tEnd=1.0e30)
+    mesh = FVMesh(c, f, p["bc"], device=dev)
+    stream = torch.cuda.current_stream(dev)
+    out = {}
+    for bits in (32, 64):
+        m = Model(coords=c, cells=f, elev=z, params=p, mesh=mesh, device=dev, precision=bits, refine_tol=1e-10)
+        m.step()
+        first = dict(FAL=m.FAL.cpu().numpy(), Eb=m.EbLocal.cpu().numpy(), h=m.hGlobal.cpu().numpy())
+        for _ in range(max(args.warmup - 1, 0)):
+            m.step()
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            m.step()
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        out[bits] = dict(ms=e0.elapsed_time(e1) / args.steps, FAL=m.FAL.cpu().numpy(), Eb=m.EbLocal.cpu().numpy(),
+                         h=m.hGlobal.cpu().numpy(), passes=int(_lib.load().gs_plan_tuning(m._plan, 4)),
+                         first=first)
+        m.destroy()
+    n = len(z)
+
+    def err(key, first=False):
+        a, b = (out[32]["first"][key], out[64]["first"][key]) if first else (out[32][key], out[64][key])
+        d = np.abs(a - b) / max(np.abs(b).max(), 1e-300)
+        return {"max": float(d.max()), "median": float(np.median(d)), "p99": float(np.quantile(d, 0.99))}
+
+    line = {"metric": "landscape vertex-steps/s, FP32-refined form @10.5M-vertex sphere",
+            "value": n * 1000.0 / out[32]["ms"], "unit": "vertex-steps/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": out[32]["ms"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 sweeps/CG with f64 refinement",
+            "data": "synthetic (seeded sphere, SH relief to degree 512)",
+            "config": {"workload": "sphere level %d (%d vertices), -5000..+4000 m, dt 5000 yr" % (level, n),
+                       "vertices": n, "global_batch": 1, "seq_len": 0, "parallelism": "single"},
+            "precision": {"fp64_ms_per_step": out[64]["ms"], "fp32_ms_per_step": out[32]["ms"],
+                          "speedup": out[64]["ms"] / out[32]["ms"], "refine_tol": 1e-10,
+                          "refinement_passes": out[32]["passes"],
+                          "rel_error_vs_fp64_after_first_step": {"drainage_area": err("FAL", True),
+                                                                 "erosion_rate": err("Eb", True),
+                                                                 "elevation": err("h", True)},
+                          "rel_error_vs_fp64_after_all_steps": {"drainage_area": err("FAL"),
+                                                                "erosion_rate": err("Eb"), "elevation": err("h")},
+                          "note": "errors relative to the largest |value| of the FP64 field; over many steps the "
+                                  "two trajectories part where a discrete decision (tie, threshold) flips"}}
+    print(json.dumps(line), flush=True)
 
 
 def config_of(args, n, n_all, world):

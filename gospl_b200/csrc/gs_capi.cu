@@ -91,6 +91,17 @@ int gs_plan_tune(gs_plan* plan, int32_t knob, int32_t value) {
 
 int gs_plan_tuning(const gs_plan* plan, int32_t knob) { return plan ? gs::plan_tuning(plan, knob) : -1; }
 
+int gs_plan_set_precision(gs_plan* plan, int32_t bits, double tol) {
+    NEED(plan);
+    if ((bits != 32 && bits != 64) || !(tol > 0.0) || !(tol < 1.0)) {
+        gs::set_error(GS_EINVAL, "precision: bits must be 32 or 64 and 0 < tol < 1");
+        return GS_EINVAL;
+    }
+    plan->fp32 = bits == 32 ? 1 : 0;
+    plan->refine_tol = tol;
+    return GS_OK;
+}
+
 int gs_plan_record(gs_plan* plan, int32_t nslots) {
     NEED(plan);
     GS_GUARD(return gs::record_setup(plan, nslots);)

@@ -378,6 +378,167 @@ __global__ void __launch_bounds__(256) k_cg_coop(int n, const int* __restrict__ 
     }
 }
 
+// FP32 CG (precision form): S d = rhs from d = 0 with FP32 vectors and FP32
+// arithmetic (coefficients rounded on load), dot products accumulated in FP64;
+// the same barrier structure as k_cg_coop.
+__global__ void __launch_bounds__(256) k_cg_coop32(int n, const int* __restrict__ nbr, const int8_t* __restrict__ nnb,
+                                                   const double* __restrict__ coef, const double* __restrict__ farea,
+                                                   const uint8_t* __restrict__ fix, const double* __restrict__ rhs,
+                                                   float* x, float* r, float* z, float* pp, float* ap, double* part,
+                                                   double rtol, int max_iter, int* it_out, double* res_out) {
+    cg::grid_group grid = cg::this_grid();
+    const int nb = gridDim.x, blk = blockIdx.x;
+    const int gtid = blk * blockDim.x + threadIdx.x, gsz = nb * blockDim.x;
+    double* pc = part;
+    double* pa = part + 3 * nb;
+    double* pb = part + 5 * nb;
+    double a0 = 0.0, a1 = 0.0;
+    for (int k = gtid; k < n; k += gsz) {
+        x[k] = 0.0f;
+        if (fix[k]) {
+            r[k] = z[k] = pp[k] = 0.0f;
+            continue;
+        }
+        const float rk = (float)rhs[k];
+        const float zk = rk / (float)(farea[k] * coef[k]);
+        r[k] = rk;
+        z[k] = zk;
+        pp[k] = zk;
+        a0 += (double)rk * (double)zk;
+        a1 += (double)rk * (double)rk;
+    }
+    block_sum2(a0, a1, &pc[3 * blk], &pc[3 * blk + 1]);
+    grid.sync();
+    double rz = grid_total(pc, 3, 0, nb);
+    const double bnorm = sqrt(grid_total(pc, 3, 1, nb));
+    double relres = bnorm > 0.0 ? 1.0 : 0.0;
+    int it = 0;
+    while (bnorm > 0.0 && relres > rtol && it < max_iter) {
+        double acc = 0.0;
+        for (int k = gtid; k < n; k += gsz) {
+            float y = 0.0f;
+            if (!fix[k]) {
+                y = (float)coef[k] * pp[k];
+                for (int s = 0; s < nnb[k]; s++) {
+                    double o = coef[(size_t)(s + 1) * n + k];
+                    if (o == 0.0) continue;
+                    int j = nbr[(size_t)s * n + k];
+                    if (fix[j]) continue;
+                    y = y + (float)o * pp[j];
+                }
+                y = (float)farea[k] * y;
+            }
+            ap[k] = y;
+            acc += (double)pp[k] * (double)y;
+        }
+        block_sum2(acc, 0.0, &pa[2 * blk], &pa[2 * blk + 1]);
+        grid.sync();
+        const double pap = grid_total(pa, 2, 0, nb);
+        const float alpha = (float)((pap != 0.0) ? rz / pap : 0.0);
+        double c0 = 0.0, c1 = 0.0;
+        for (int k = gtid; k < n; k += gsz) {
+            if (fix[k]) continue;
+            x[k] = x[k] + alpha * pp[k];
+            const float rk = r[k] - alpha * ap[k];
+            r[k] = rk;
+            const float zk = rk / (float)(farea[k] * coef[k]);
+            z[k] = zk;
+            c0 += (double)rk * (double)zk;
+            c1 += (double)rk * (double)rk;
+        }
+        block_sum2(c0, c1, &pb[2 * blk], &pb[2 * blk + 1]);
+        grid.sync();
+        const double rzn = grid_total(pb, 2, 0, nb);
+        const double rr = grid_total(pb, 2, 1, nb);
+        const float beta = (float)((rz != 0.0) ? rzn / rz : 0.0);
+        rz = rzn;
+        relres = sqrt(rr) / bnorm;
+        it++;
+        if (!(relres == relres) || relres <= rtol || it >= max_iter) break;
+        for (int k = gtid; k < n; k += gsz) pp[k] = z[k] + beta * pp[k];
+        grid.sync();
+    }
+    if (gtid == 0) {
+        *it_out = it;
+        *res_out = relres;
+    }
+}
+
+__global__ void k_add_f32_d(int n, const float* __restrict__ d, double* x) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) x[i] = x[i] + (double)d[i];
+}
+
+// r = b - S x on free rows (FP64), 0 on fixed rows
+__global__ void k_cg_resid(int n, int W, int flat, const int* __restrict__ nbr, const int8_t* __restrict__ nnb,
+                           const double* __restrict__ coef, const double* __restrict__ farea,
+                           const uint8_t* __restrict__ outlet, const double* __restrict__ b,
+                           const double* __restrict__ x, double* r) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    r[k] = diff_fixed(k, flat, outlet, farea) ? 0.0
+                                              : b[k] - diff_row(k, n, W, nbr, nnb, coef, farea, outlet, flat, x, true);
+}
+
+static int cg_launch(gs_plan* p, const void* fn, void** args) {
+    cudaEvent_t stop = nullptr;
+    if (p->profiling) prof_begin(p, fn, &stop);
+    GS_CUDA(cudaLaunchCooperativeKernel(fn, p->coop_blocks, 256, args, 0, p->stream));
+    if (stop) cudaEventRecord(stop, p->stream);
+    p->launches++;
+    return GS_OK;
+}
+
+// precision form of the solve: FP32 CG corrections of an FP64 iterate, FP64
+// residuals, until |r| <= tol |b| (2-norms)
+static int hillslope_refine32(gs_plan* p, double tol, int max_iter, int* outer, double* relres_out) {
+    const int n = (int)p->n;
+    const int B = 256, G = grid_for(n, B), PARTS = 512;
+    GS_TRY(precision_buffers(p));
+    const size_t N = (size_t)std::max(n, 1);
+    float** bufs[] = {&p->f32b, &p->f32c, &p->f32d, &p->f32e};
+    for (float** q : bufs)
+        if (!*q) GS_CUDA(cudaMalloc((void**)q, sizeof(float) * N));
+    double* sc = p->red + 4096;
+    launch(p, k_dots<2>, PARTS, 256, n, (const double*)p->cg_b, (const double*)p->cg_b,
+           (const double*)p->cg_r, (const double*)p->cg_r, p->red);
+    launch(p, k_dots_final, 1, 1024, PARTS, 2, (const double*)p->red, sc + 5);
+    GS_LAUNCH();
+    double hs[2];
+    GS_CUDA(cudaMemcpyAsync(hs, sc + 5, 2 * sizeof(double), cudaMemcpyDeviceToHost, p->stream));
+    GS_CUDA(cudaStreamSynchronize(p->stream));
+    const double bnorm = sqrt(hs[0]);
+    double relres = bnorm > 0.0 ? sqrt(hs[1]) / bnorm : 0.0;
+    int it = 0;
+    int* it_d = p->i_scalar + 12;
+    double* res_d = p->red + 4100;
+    for (; it < 10 && relres > tol; it++) {
+        int nn = n, mi = max_iter;
+        double rt = 1.0e-5;
+        void* args[] = {(void*)&nn, (void*)&p->nbr, (void*)&p->nnb, (void*)&p->dcoef, (void*)&p->farea,
+                        (void*)&p->dfix, (void*)&p->cg_r, (void*)&p->f32a, (void*)&p->f32b, (void*)&p->f32c,
+                        (void*)&p->f32d, (void*)&p->f32e, (void*)&p->red, (void*)&rt, (void*)&mi, (void*)&it_d,
+                        (void*)&res_d};
+        GS_TRY(cg_launch(p, (const void*)k_cg_coop32, args));
+        launch(p, k_add_f32_d, G, B, n, (const float*)p->f32a, p->cg_x);
+        launch(p, k_cg_resid, G, B, n, p->W, p->flat, (const int*)p->nbr, (const int8_t*)p->nnb,
+               (const double*)p->dcoef, (const double*)p->farea, (const uint8_t*)p->outlet, (const double*)p->cg_b,
+               (const double*)p->cg_x, p->cg_r);
+        launch(p, k_dots<1>, PARTS, 256, n, (const double*)p->cg_r, (const double*)p->cg_r, (const double*)nullptr,
+               (const double*)nullptr, p->red);
+        launch(p, k_dots_final, 1, 1024, PARTS, 1, (const double*)p->red, sc + 3);
+        GS_LAUNCH();
+        GS_CUDA(cudaMemcpyAsync(hs, sc + 3, sizeof(double), cudaMemcpyDeviceToHost, p->stream));
+        GS_CUDA(cudaStreamSynchronize(p->stream));
+        relres = bnorm > 0.0 ? sqrt(hs[0]) / bnorm : 0.0;
+        if (!(relres == relres)) break;
+    }
+    p->refine_iters += it;
+    *outer = it;
+    *relres_out = relres;
+    return GS_OK;
+}
+
 int hillslope(gs_plan* p, double* h, double* cum_ed, double* eb, double sealevel, double cda,
               double cdm, double dt, double rtol, int max_iter, gs_stats* st) {
     const int n = (int)p->n;
@@ -408,6 +569,27 @@ int hillslope(gs_plan* p, double* h, double* cum_ed, double* eb, double sealevel
            (const double*)p->dcoef, (const double*)p->farea, (const uint8_t*)p->outlet, (const double*)hold,
            p->cg_x, p->cg_b, p->cg_r, p->cg_z, p->cg_p);
     GS_LAUNCH();
+    if (p->fp32) {
+        int outer = 0;
+        double relres = 0.0;
+        const double tol = std::max(rtol, p->refine_tol);
+        GS_TRY(hillslope_refine32(p, tol, max_iter, &outer, &relres));
+        launch(p, k_hill_apply, G, B, n, (const double*)hold, (const double*)p->cg_x, dt, h, cum_ed, eb);
+        GS_LAUNCH();
+        if (st) {
+            st->cg_iters = outer;
+            st->cg_relres = relres;
+        }
+        if (!(relres == relres)) {
+            set_error(GS_ENONFINITE, "hillslope FP32 CG produced a non-finite residual");
+            return GS_ENONFINITE;
+        }
+        if (relres > tol) {
+            set_error(GS_EMAXITER, "hillslope FP32 refinement did not reach its tolerance");
+            return GS_EMAXITER;
+        }
+        return GS_OK;
+    }
     int* it_d = p->i_scalar + 12;
     double* res_d = p->red + 4100;
     {

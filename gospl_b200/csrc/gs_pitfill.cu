@@ -1224,10 +1224,12 @@ int coop_occupancy(int* per_sm) {
     int a = 0, b = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_bfs_coop, 256, 0) != cudaSuccess) return 1;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_relax_active, 256, 0) != cudaSuccess) return 1;
-    int c = 0;
+    int c = 0, d = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c, k_cg_coop, 256, 0) != cudaSuccess) return 1;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&d, k_cg_coop32, 256, 0) != cudaSuccess) return 1;
     *per_sm = a < b ? a : b;
     *per_sm = *per_sm < c ? *per_sm : c;
+    *per_sm = *per_sm < d ? *per_sm : d;
     return 0;
 }
 

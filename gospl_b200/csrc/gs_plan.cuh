@@ -18,6 +18,16 @@ struct gs_plan {
     int coop_blocks = 148;               // co-resident 256-thread blocks for cooperative launches
     int coop_max_per_sm = 1;             // occupancy limit of the cooperative kernels
     int sweep_per_sm = 8;                // 128-thread blocks per SM of the ordered sweeps
+    // precision form: FP32 sweeps and CG inside FP64 refinement loops
+    int fp32 = 0;
+    double refine_tol = 1.0e-10;         // max|r| / max|b| of every refined solve
+    int64_t refine_iters = 0;            // refinement passes since the last reset
+    float* f32a = nullptr;               // FP32 correction / CG vectors
+    float* f32b = nullptr;
+    float* f32c = nullptr;
+    float* f32d = nullptr;
+    float* f32e = nullptr;
+    double* r64 = nullptr;               // FP64 residual
 
     // mesh, slot-major [W][n]
     int* nbr = nullptr;          // FVnID (-1 pad)
@@ -268,6 +278,11 @@ int apply_forces(gs_plan* p, double* h, const double* rain, const double* upsub,
 
 void prof_begin(gs_plan* p, const void* fn, cudaEvent_t* stop);
 int coop_occupancy(int* per_sm);
+__global__ void k_cg_coop32(int n, const int* __restrict__ nbr, const int8_t* __restrict__ nnb,
+                            const double* __restrict__ coef, const double* __restrict__ farea,
+                            const uint8_t* __restrict__ fix, const double* __restrict__ rhs, float* x, float* r,
+                            float* z, float* pp, float* ap, double* part, double rtol, int max_iter, int* it_out,
+                            double* res_out);
 __global__ void k_cg_coop(int n, const int* __restrict__ nbr, const int8_t* __restrict__ nnb,
                           const double* __restrict__ coef, const double* __restrict__ farea,
                           const uint8_t* __restrict__ fix, const double* __restrict__ b, double* x, double* r,
@@ -275,6 +290,9 @@ __global__ void k_cg_coop(int n, const int* __restrict__ nbr, const int8_t* __re
                           double* res_out);
 int set_members(gs_plan* p, int nmem, const int64_t* start, const double* maxarea);
 int plan_tune(gs_plan* p, int knob, int value);
+int precision_buffers(gs_plan* p);
+int flow_refine32(gs_plan* p, const double* wgt, const double* b, double* x, const int* order);
+int spl_refine32(gs_plan* p, const int* rcv, const double* c, const double* hold, double* x, const int* order2);
 int plan_tuning(const gs_plan* p, int knob);
 void free_members(gs_plan* p);
 

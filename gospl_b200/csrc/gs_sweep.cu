@@ -19,6 +19,7 @@
 #include <cooperative_groups.h>
 #include <cub/cub.cuh>
 
+#include <algorithm>
 #include <cstring>
 
 #include "gs_plan.cuh"
@@ -452,6 +453,23 @@ __device__ __forceinline__ void st_val(double* p, double v) {
     asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"((unsigned long long)__double_as_longlong(v)) : "memory");
 }
 
+// 32-bit counterparts for the FP32 sweeps of the precision form
+constexpr unsigned SENT32 = 0x7fa0dead;
+__device__ __forceinline__ float ld_val(const float* p) {
+    unsigned v;
+    asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return __uint_as_float(v);
+}
+__device__ __forceinline__ bool is_sent(float v) { return __float_as_uint(v) == SENT32; }
+__device__ __forceinline__ void st_val(float* p, float v) {
+    asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(__float_as_uint(v)) : "memory");
+}
+
+__global__ void k_fill_sent32(int n, float* x) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) x[i] = __uint_as_float(SENT32);
+}
+
 __global__ void k_gather_u64(int n, const unsigned long long* __restrict__ a, const int* __restrict__ idx,
                              unsigned long long* out) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -495,6 +513,7 @@ __global__ void k_check_order(int n, int R, const int* __restrict__ rcv, const d
 }
 
 struct FlowOrd {
+    using T = double;
     int n;
     const int* nbr;
     const uint32_t* mask;
@@ -528,6 +547,7 @@ struct FlowOrd {
 };
 
 struct SplOrd {
+    using T = double;
     int n, R;
     const int* rcv;
     const double* c;
@@ -555,6 +575,7 @@ struct SplOrd {
 // Transposed flow system (I - W) y = g: y_i = g_i + sum_k w_ik y_{rcv_ik},
 // receivers first (the flow order reversed).
 struct FlowAdjOrd {
+    using T = double;
     int n, R;
     const int* rcv;
     const double* wgt;
@@ -578,6 +599,7 @@ struct FlowAdjOrd {
 // Transposed SPL system M^T y = g: y_j = (g_j + sum_{donors i} c_ik y_i) / den_j,
 // den_j = 1 + sum_k c_jk, donors first (the flow order).
 struct SplAdjOrd {
+    using T = double;
     int n, R;
     const int* nbr;
     const uint32_t* mask;
@@ -615,14 +637,77 @@ struct SplAdjOrd {
     }
 };
 
+// ---- FP32 operators of the precision form: values and arithmetic in FP32,
+// weights, coefficients and right-hand sides read from their FP64 arrays and
+// rounded on load.  They solve for corrections of an FP64 refinement loop.
+struct FlowOrd32 {
+    using T = float;
+    int n;
+    const int* nbr;
+    const uint32_t* mask;
+    const unsigned long long* dk;
+    const unsigned long long* sorder;
+    const double* wgt;
+    const double* b;
+    float* x;
+    static constexpr int MAXP = MAXW;
+    __device__ __forceinline__ int prep(int i, int* pj, float* pw) const {
+        uint32_t m = mask[i];
+        unsigned long long kk = dk[i], ord = sorder[i];
+        int np = 0;
+        for (int q = 0; q < MAXW && m; q++) {
+            int t = (int)(ord & 15ULL);
+            ord >>= 4;
+            if (!(m & (1u << t))) continue;
+            m &= ~(1u << t);
+            int j = nbr[(size_t)t * n + i];
+            int k = (int)((kk >> (4 * t)) & 15ULL);
+            pj[np] = j;
+            pw[np] = (float)wgt[(size_t)k * n + j];
+            np++;
+        }
+        return np;
+    }
+    __device__ __forceinline__ float init(int i) const { return (float)b[i]; }
+    __device__ __forceinline__ float combine(float s, float w, float xj) const { return s + w * xj; }
+    __device__ __forceinline__ float finish(int, float s, double) const { return s; }
+};
+
+struct SplOrd32 {
+    using T = float;
+    int n, R;
+    const int* rcv;
+    const double* c;
+    const double* hold;
+    float* x;
+    static constexpr int MAXP = MAXR;
+    __device__ __forceinline__ int prep(int i, int* pj, float* pw) const {
+        int np = 0;
+        for (int k = 0; k < R; k++) {
+            double ck = c[(size_t)k * n + i];
+            int r = rcv[(size_t)k * n + i];
+            if (r != i && ck != 0.0) { pj[np] = r; pw[np] = (float)ck; np++; }
+        }
+        return np;
+    }
+    __device__ __forceinline__ float init(int i) const { return (float)hold[i]; }
+    __device__ __forceinline__ float combine(float s, float w, float xj) const { return s + w * xj; }
+    __device__ __forceinline__ float finish(int i, float num, double) const {
+        float den = 1.0f;
+        for (int k = 0; k < R; k++) den = den + (float)c[(size_t)k * n + i];
+        return num / den;
+    }
+};
+
 template <class Op>
 __global__ void __launch_bounds__(128) k_ordered(Op op, int n, const int* __restrict__ order, unsigned* ctr,
                                                  unsigned long long budget_ns) {
     const unsigned long long t0 = globaltimer_ns();
     const int lane = threadIdx.x & 31;
     const unsigned full = 0xffffffffu;
+    using T = typename Op::T;
     int pj[Op::MAXP];
-    double pw[Op::MAXP];
+    T pw[Op::MAXP];
     for (;;) {
         unsigned base = 0;
         if (lane == 0) base = atomicAdd(&ctr[C_HEAD], 32u);
@@ -643,9 +728,9 @@ __global__ void __launch_bounds__(128) k_ordered(Op op, int n, const int* __rest
                 // at, so a polling round costs one memory latency per four
                 // predecessors; the sum keeps the predecessors' order
                 rdy = true;
-                double acc = op.init(node);
+                T acc = op.init(node);
                 for (int q0 = 0; q0 < np && rdy; q0 += 4) {
-                    double v[4];
+                    T v[4];
 #pragma unroll
                     for (int u = 0; u < 4; u++)
                         if (q0 + u < np) v[u] = ld_val(&op.x[pj[q0 + u]]);
@@ -948,6 +1033,7 @@ int flow_run(gs_plan* p, const int* rcv, const double* wgt, const int8_t* rslot,
     *cycle_nodes = 0;
     if (n == 0) return GS_OK;
     if (!ok) return flow_solve_counted(p, rcv, wgt, rslot, b, x, cycle_nodes);
+    if (p->fp32) return flow_refine32(p, wgt, b, x, order);
     GS_CUDA(cudaMemsetAsync(p->ctr, 0, sizeof(unsigned) * 8, p->stream));
     FlowOrd op{n, p->nbr, p->don_mask, p->don_k, p->sorder, wgt, b, x};
     launch(p, k_ordered<FlowOrd>, p->sm_count * p->sweep_per_sm, 128, op, n, (const int*)order, p->ctr, SWEEP_BUDGET_NS);
@@ -1008,6 +1094,7 @@ int spl_sweep(gs_plan* p, const int* rcv, const double* c, const int8_t* rslot, 
     if (!ok) return spl_sweep_counted(p, rcv, c, rslot, hold, s, cycle_nodes);
     // the SPL system is solved receivers first: the flow order reversed
     launch(p, k_reverse, grid_for(n, 256), 256, n, (const int*)p->order_i, p->order2);
+    if (p->fp32) return spl_refine32(p, rcv, c, hold, s, p->order2);
     GS_CUDA(cudaMemsetAsync(p->ctr, 0, sizeof(unsigned) * 8, p->stream));
     launch(p, k_fill_sent, grid_for(n, 256), 256, n, s);
     SplOrd op{n, p->R, rcv, c, hold, s};
@@ -1061,6 +1148,174 @@ int sweep_spl_adjoint(gs_plan* p, const int* rcv, const double* wgt, const int8_
     if (st != 0) {
         set_error(st, "adjoint SPL sweep did not complete");
         return st;
+    }
+    return GS_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Precision form: FP32 sweeps inside an FP64 refinement loop.  x_0 = 0, then
+// repeat: d = T^-1 r in FP32 (one ordered sweep), x += d in FP64, r = b - T x
+// in FP64, until max|r| <= tol max|b|.
+__global__ void k_zero_d(int n, double* x) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) x[i] = 0.0;
+}
+
+__global__ void k_add_f32(int n, const float* __restrict__ d, double* x) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) x[i] = x[i] + (double)d[i];
+}
+
+__global__ void k_copy_dd(int n, const double* __restrict__ a, double* b) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) b[i] = a[i];
+}
+
+// r = b - (I - W^T) x, donors summed in ascending id as in the FP64 sweep
+__global__ void k_flow_resid(int n, const int* __restrict__ nbr, const uint32_t* __restrict__ mask,
+                             const unsigned long long* __restrict__ dk, const unsigned long long* __restrict__ sorder,
+                             const double* __restrict__ wgt, const double* __restrict__ b,
+                             const double* __restrict__ x, double* r) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    uint32_t m = mask[i];
+    unsigned long long kk = dk[i], ord = sorder[i];
+    double s = b[i];
+    for (int q = 0; q < MAXW && m; q++) {
+        int t = (int)(ord & 15ULL);
+        ord >>= 4;
+        if (!(m & (1u << t))) continue;
+        m &= ~(1u << t);
+        int j = nbr[(size_t)t * n + i];
+        int k = (int)((kk >> (4 * t)) & 15ULL);
+        s = s + wgt[(size_t)k * n + j] * x[j];
+    }
+    r[i] = s - x[i];
+}
+
+// r = hOld - M x for the SPL matrix (den_i x_i - sum_k c_ik x_rcv)
+__global__ void k_spl_resid(int n, int R, const int* __restrict__ rcv, const double* __restrict__ c,
+                            const double* __restrict__ hold, const double* __restrict__ x, double* r) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double num = hold[i], den = 1.0;
+    for (int k = 0; k < R; k++) {
+        double ck = c[(size_t)k * n + i];
+        int q = rcv[(size_t)k * n + i];
+        if (q != i && ck != 0.0) num = num + ck * x[q];
+        den = den + ck;
+    }
+    r[i] = num - den * x[i];
+}
+
+__global__ void k_absmax_key(int n, const double* __restrict__ x, unsigned long long* out) {
+    unsigned long long best = 0ULL;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        unsigned long long k = dkey(fabs(x[i]));
+        best = k > best ? k : best;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        unsigned long long v = __shfl_xor_sync(0xffffffffu, best, o);
+        best = v > best ? v : best;
+    }
+    if ((threadIdx.x & 31) == 0) atomicMax(out, best);
+}
+
+int precision_buffers(gs_plan* p) {
+    const size_t n = (size_t)std::max<int64_t>(p->n, 1);
+    if (!p->f32a) GS_CUDA(cudaMalloc((void**)&p->f32a, sizeof(float) * n));
+    if (!p->r64) GS_CUDA(cudaMalloc((void**)&p->r64, sizeof(double) * n));
+    return GS_OK;
+}
+
+static int absmax_ratio(gs_plan* p, const double* r, const double* b, double* ratio) {
+    const int n = (int)p->n;
+    GS_CUDA(cudaMemsetAsync(p->u_scalar + 2, 0, 2 * sizeof(unsigned long long), p->stream));
+    launch(p, k_absmax_key, p->sm_count * 4, 256, n, r, p->u_scalar + 2);
+    launch(p, k_absmax_key, p->sm_count * 4, 256, n, b, p->u_scalar + 3);
+    GS_LAUNCH();
+    unsigned long long k[2];
+    GS_CUDA(cudaMemcpyAsync(k, p->u_scalar + 2, sizeof(k), cudaMemcpyDeviceToHost, p->stream));
+    GS_CUDA(cudaStreamSynchronize(p->stream));
+    auto inv = [](unsigned long long u) {
+        unsigned long long v = (u & 0x8000000000000000ULL) ? (u & 0x7fffffffffffffffULL) : ~u;
+        double d;
+        memcpy(&d, &v, sizeof(d));
+        return d;
+    };
+    const double rr = k[0] ? inv(k[0]) : 0.0, bb = k[1] ? inv(k[1]) : 0.0;
+    *ratio = bb > 0.0 ? rr / bb : rr;
+    return GS_OK;
+}
+
+// (I - W^T) x = b with the donor masks of flow_prepare and a valid flow order
+int flow_refine32(gs_plan* p, const double* wgt, const double* b, double* x, const int* order) {
+    const int n = (int)p->n;
+    const int B = 256, G = grid_for(n, B);
+    GS_TRY(precision_buffers(p));
+    launch(p, k_copy_dd, G, B, n, b, p->r64);
+    launch(p, k_zero_d, G, B, n, x);
+    int it = 0;
+    double ratio = 1.0;
+    for (; it < 8; it++) {
+        GS_CUDA(cudaMemsetAsync(p->ctr, 0, sizeof(unsigned) * 8, p->stream));
+        launch(p, k_fill_sent32, G, B, n, p->f32a);
+        FlowOrd32 op{n, p->nbr, p->don_mask, p->don_k, p->sorder, wgt, (const double*)p->r64, p->f32a};
+        launch(p, k_ordered<FlowOrd32>, p->sm_count * p->sweep_per_sm, 128, op, n, order, p->ctr, SWEEP_BUDGET_NS);
+        GS_LAUNCH();
+        int st = 0;
+        GS_TRY(ordered_status(p, &st));
+        if (st != 0) {
+            set_error(st, "FP32 flow sweep did not complete");
+            return st;
+        }
+        launch(p, k_add_f32, G, B, n, (const float*)p->f32a, x);
+        launch(p, k_flow_resid, G, B, n, (const int*)p->nbr, (const uint32_t*)p->don_mask,
+               (const unsigned long long*)p->don_k, (const unsigned long long*)p->sorder, wgt, b, (const double*)x,
+               p->r64);
+        GS_LAUNCH();
+        GS_TRY(absmax_ratio(p, p->r64, b, &ratio));
+        if (!(ratio > p->refine_tol)) break;
+    }
+    p->refine_iters += it + 1;
+    if (ratio > p->refine_tol) {
+        set_error(GS_EMAXITER, "FP32 flow refinement did not reach its tolerance");
+        return GS_EMAXITER;
+    }
+    return GS_OK;
+}
+
+// M s = hOld for the SPL coefficients c, receivers first (order2)
+int spl_refine32(gs_plan* p, const int* rcv, const double* c, const double* hold, double* x, const int* order2) {
+    const int n = (int)p->n;
+    const int B = 256, G = grid_for(n, B);
+    GS_TRY(precision_buffers(p));
+    launch(p, k_copy_dd, G, B, n, hold, p->r64);
+    launch(p, k_zero_d, G, B, n, x);
+    int it = 0;
+    double ratio = 1.0;
+    for (; it < 8; it++) {
+        GS_CUDA(cudaMemsetAsync(p->ctr, 0, sizeof(unsigned) * 8, p->stream));
+        launch(p, k_fill_sent32, G, B, n, p->f32a);
+        SplOrd32 op{n, p->R, rcv, c, (const double*)p->r64, p->f32a};
+        launch(p, k_ordered<SplOrd32>, p->sm_count * p->sweep_per_sm, 128, op, n, order2, p->ctr, SWEEP_BUDGET_NS);
+        GS_LAUNCH();
+        int st = 0;
+        GS_TRY(ordered_status(p, &st));
+        if (st != 0) {
+            set_error(st, "FP32 SPL sweep did not complete");
+            return st;
+        }
+        launch(p, k_add_f32, G, B, n, (const float*)p->f32a, x);
+        launch(p, k_spl_resid, G, B, n, p->R, rcv, c, hold, (const double*)x, p->r64);
+        GS_LAUNCH();
+        GS_TRY(absmax_ratio(p, p->r64, hold, &ratio));
+        if (!(ratio > p->refine_tol)) break;
+    }
+    p->refine_iters += it + 1;
+    if (ratio > p->refine_tol) {
+        set_error(GS_EMAXITER, "FP32 SPL refinement did not reach its tolerance");
+        return GS_EMAXITER;
     }
     return GS_OK;
 }

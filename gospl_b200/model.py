@@ -45,11 +45,13 @@ class Model:
     dt, tStart, tEnd, flowDir, K (scalar or per-vertex), d, m, Cda, Cdm, oFill,
     sealevel, bc, rain (per-vertex m/yr), upsub (per-vertex m/yr or None).
     ``members`` = (start, maxarea) declares the mesh a disjoint union of
-    landscapes (``gospl_b200.ensemble``).
+    landscapes (``gospl_b200.ensemble``).  ``precision=32`` selects the FP32
+    sweeps and CG with FP64 refinement to ``refine_tol``.
     """
 
     def __init__(self, filename=None, *, coords=None, cells=None, elev=None, params=None, mesh=None,
-                 device="cuda", init_flow=True, cg_rtol=1.0e-13, cg_maxit=2000, members=None):
+                 device="cuda", init_flow=True, cg_rtol=1.0e-13, cg_maxit=2000, members=None, precision=64,
+                 refine_tol=1.0e-10):
         import torch
 
         if not torch.cuda.is_available():
@@ -132,6 +134,9 @@ class Model:
         self._plan = handle
         self.stream = torch.cuda.current_stream(self.dev)
         _lib.check(L.gs_plan_set_stream(self._plan, ctypes.c_void_p(self.stream.cuda_stream)))
+        if precision != 64:
+            # FP32 sweeps and CG inside FP64 refinement to refine_tol
+            _lib.check(L.gs_plan_set_precision(self._plan, int(precision), float(refine_tol)))
         if members is not None:
             # (start [nmem+1], maxarea [nmem]): landscapes packed in this mesh
             start = np.ascontiguousarray(members[0], np.int64)

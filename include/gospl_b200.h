@@ -90,7 +90,17 @@ int gs_plan_set_stream(gs_plan* plan, void* cuda_stream);
  */
 #define GS_TUNE_SWEEP_BLOCKS 1
 #define GS_TUNE_COOP_BLOCKS 2
+#define GS_TUNE_REFINE_PASSES 4   /* gs_plan_tuning only: refinement passes so far */
 int gs_plan_tune(gs_plan* plan, int32_t knob, int32_t value);
+/*
+ * Precision form (no counterpart in the reference, which is FP64 only).
+ * bits = 32: the flow-accumulation and SPL sweeps and the hillslope CG run in
+ * FP32 inside FP64 iterative refinement (FP64 residuals, corrections solved in
+ * FP32) until max|r| <= tol max|b| (sweeps) or |r|_2 <= max(rtol, tol) |b|_2
+ * (CG); receivers, pit filling, the cascade and every mass sum stay FP64.
+ * bits = 64 (default): the plain FP64 path.
+ */
+int gs_plan_set_precision(gs_plan* plan, int32_t bits, double tol);
 int gs_plan_tuning(const gs_plan* plan, int32_t knob);
 /* Number of device kernels this plan launched since creation. */
 int64_t gs_plan_launches(const gs_plan* plan);
