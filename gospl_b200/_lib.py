@@ -15,7 +15,7 @@ ERRORS = {1: "GS_EINVAL", 2: "GS_ECUDA", 3: "GS_EMAXITER", 4: "GS_ENONFINITE", 5
           6: "GS_ETIMEOUT", 7: "GS_ENOMEM"}
 
 EXPORTS = ("gs_version", "gs_last_error", "gs_plan_create", "gs_plan_destroy", "gs_plan_set_members",
-           "gs_plan_tune", "gs_plan_tuning", "gs_plan_set_precision",
+           "gs_plan_tune", "gs_plan_tuning", "gs_plan_set_precision", "gs_plan_set_deposition",
            "gs_plan_set_stream",
            "gs_plan_launches", "gs_mfdreceivers", "gs_fill_elevation", "gs_pit_tables",
            "gs_flow_accumulation", "gs_erodep_spl", "gs_hillslope", "gs_apply_forces", "gs_mesh_geometry", "gs_plan_profile",
@@ -63,6 +63,7 @@ def load(path=None):
     L.gs_plan_tune.argtypes = [P, i32, i32]
     L.gs_plan_tuning.argtypes = [P, i32]
     L.gs_plan_set_precision.argtypes = [P, i32, d]
+    L.gs_plan_set_deposition.argtypes = [P, d]
     L.gs_plan_set_stream.argtypes = [P, P]
     L.gs_plan_launches.argtypes = [P]
     L.gs_plan_launches.restype = i64

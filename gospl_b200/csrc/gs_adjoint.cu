@@ -448,6 +448,10 @@ int adjoint_step(gs_plan* p, int slot, double* lam, const double* rain, double k
         return GS_EINVAL;
     }
     StepRec& r = p->rec->steps[slot];
+    if (p->fdepa > 0.0) {
+        set_error(GS_EINVAL, "adjoint: transport-limited SPL (G > 0) has no adjoint here");
+        return GS_EINVAL;
+    }
     if (!r.order_ok) {
         set_error(GS_EINVAL, "adjoint: the recorded step used the unordered flow solve");
         return GS_EINVAL;

@@ -91,6 +91,16 @@ int gs_plan_tune(gs_plan* plan, int32_t knob, int32_t value) {
 
 int gs_plan_tuning(const gs_plan* plan, int32_t knob) { return plan ? gs::plan_tuning(plan, knob) : -1; }
 
+int gs_plan_set_deposition(gs_plan* plan, double g) {
+    NEED(plan);
+    if (!(g >= 0.0)) {
+        gs::set_error(GS_EINVAL, "deposition coefficient G must be >= 0");
+        return GS_EINVAL;
+    }
+    plan->fdepa = g;
+    return GS_OK;
+}
+
 int gs_plan_set_precision(gs_plan* plan, int32_t bits, double tol) {
     NEED(plan);
     if ((bits != 32 && bits != 64) || !(tol > 0.0) || !(tol < 1.0)) {

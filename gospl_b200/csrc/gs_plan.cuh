@@ -20,6 +20,9 @@ struct gs_plan {
     int sweep_per_sm = 8;                // 128-thread blocks per SM of the ordered sweeps
     // precision form: FP32 sweeps and CG inside FP64 refinement loops
     int fp32 = 0;
+    double fdepa = 0.0;                  // SPL deposition coefficient G (0: detachment-limited)
+    int ed_iters = 0;                    // BiCGSTAB iterations of the last coupled solve
+    double* ed_buf = nullptr;            // [6][n] coupled-solve scratch
     double refine_tol = 1.0e-10;         // max|r| / max|b| of every refined solve
     int64_t refine_iters = 0;            // refinement passes since the last reset
     float* f32a = nullptr;               // FP32 correction / CG vectors
@@ -291,6 +294,10 @@ __global__ void k_cg_coop(int n, const int* __restrict__ nbr, const int8_t* __re
 int set_members(gs_plan* p, int nmem, const int64_t* start, const double* maxarea);
 int plan_tune(gs_plan* p, int knob, int value);
 int precision_buffers(gs_plan* p);
+int build_donors(gs_plan* p, const int* rcv, const double* wgt, const int8_t* rslot);
+int spl_order(gs_plan* p);
+int sweep_flow_rhs(gs_plan* p, const double* wgt, const int* order, const double* b, double* x);
+int sweep_spl_rhs(gs_plan* p, const int* rcv, const double* c, const int* order2, const double* rhs, double* x);
 int flow_refine32(gs_plan* p, const double* wgt, const double* b, double* x, const int* order);
 int spl_refine32(gs_plan* p, const int* rcv, const double* c, const double* hold, double* x, const int* order2);
 int plan_tuning(const gs_plan* p, int knob);

@@ -1320,4 +1320,59 @@ int spl_refine32(gs_plan* p, const int* rcv, const double* c, const double* hold
     return GS_OK;
 }
 
+// Plain FP64 sweeps with caller-given right-hand sides, for solvers that
+// apply the flow or SPL inverse repeatedly (the coupled erosion-deposition
+// system).  sweep_flow_rhs needs the donor masks of the graph (flow_prepare or
+// build_donors) and a valid flow order; sweep_spl_rhs the receivers-first
+// order (the flow order reversed).
+int build_donors(gs_plan* p, const int* rcv, const double* wgt, const int8_t* rslot) {
+    const int n = (int)p->n;
+    GS_CUDA(cudaMemsetAsync(p->don_mask, 0, sizeof(uint32_t) * n, p->stream));
+    GS_CUDA(cudaMemsetAsync(p->don_k, 0, sizeof(unsigned long long) * n, p->stream));
+    launch(p, k_flow_donors, grid_for(n, 256), 256, n, p->R, rcv, wgt, rslot, (const int8_t*)p->rev, p->don_mask,
+           p->don_k);
+    GS_LAUNCH();
+    return GS_OK;
+}
+
+int sweep_flow_rhs(gs_plan* p, const double* wgt, const int* order, const double* b, double* x) {
+    const int n = (int)p->n;
+    GS_CUDA(cudaMemsetAsync(p->ctr, 0, sizeof(unsigned) * 8, p->stream));
+    launch(p, k_fill_sent, grid_for(n, 256), 256, n, x);
+    FlowOrd op{n, p->nbr, p->don_mask, p->don_k, p->sorder, wgt, b, x};
+    launch(p, k_ordered<FlowOrd>, p->sm_count * p->sweep_per_sm, 128, op, n, order, p->ctr, SWEEP_BUDGET_NS);
+    GS_LAUNCH();
+    int st = 0;
+    GS_TRY(ordered_status(p, &st));
+    if (st != 0) {
+        set_error(st, "flow sweep did not complete");
+        return st;
+    }
+    return GS_OK;
+}
+
+int sweep_spl_rhs(gs_plan* p, const int* rcv, const double* c, const int* order2, const double* rhs, double* x) {
+    const int n = (int)p->n;
+    GS_CUDA(cudaMemsetAsync(p->ctr, 0, sizeof(unsigned) * 8, p->stream));
+    launch(p, k_fill_sent, grid_for(n, 256), 256, n, x);
+    SplOrd op{n, p->R, rcv, c, rhs, x};
+    launch(p, k_ordered<SplOrd>, p->sm_count * p->sweep_per_sm, 128, op, n, order2, p->ctr, SWEEP_BUDGET_NS);
+    GS_LAUNCH();
+    int st = 0;
+    GS_TRY(ordered_status(p, &st));
+    if (st != 0) {
+        set_error(st, "SPL sweep did not complete");
+        return st;
+    }
+    return GS_OK;
+}
+
+// order2 = the snapshot flow order reversed (receivers first)
+int spl_order(gs_plan* p) {
+    const int n = (int)p->n;
+    launch(p, k_reverse, grid_for(n, 256), 256, n, (const int*)p->order_i, p->order2);
+    GS_LAUNCH();
+    return GS_OK;
+}
+
 }  // namespace gs

@@ -7,7 +7,7 @@ uses, with goSPL's names, defaults and errors (gospl/tools/inputparser.py):
   ``.npz`` mesh, :263-266), ``flowdir`` (default 8, :189), ``bc`` (four of
   ``o f w c``, legacy ``0``/``1`` -> ``o``/``f``, :208-246), ``fast``, ``nodep``;
 * ``time``: ``start``, ``end``, ``dt`` required, ``tout`` (:343-404);
-* ``spl``: ``K``, ``d`` (0), ``m`` (0.5) (:454-496); ``G`` must be 0;
+* ``spl``: ``K``, ``d`` (0), ``m`` (0.5), ``G`` (0) (:454-496);
 * ``diffusion``: ``hillslopeKa``, ``hillslopeKm``, ``oFill`` (-6000) (:498-545);
 * ``sea``: ``position`` (default 0, :710-787);
 * ``climate``: events with ``start`` and ``uniform`` or ``map: [file, key]``
@@ -19,8 +19,8 @@ Paths are taken as given (relative to the working directory, as goSPL does),
 then relative to the YAML file.  Keys of other goSPL subsystems (sediment,
 stratigraphy, flexure, ice, orography, output) are ignored; options that would
 change this path's arithmetic and that the library does not implement
-(transport-limited SPL ``G > 0``, sea-level curves, time-varying climate or
-tectonic events, horizontal tectonics) raise ``ValueError``.
+(sea-level curves, time-varying climate or tectonic events, horizontal
+tectonics) raise ``ValueError``.
 """
 import os
 
@@ -97,10 +97,9 @@ def read_input(filename):
         if "K" not in spl:
             raise KeyError("Key 'K' is required in the 'spl' declaration")
         p["K"], p["d"], p["m"] = float(spl["K"]), float(spl.get("d", 0.0)), float(spl.get("m", 0.5))
-        if float(spl.get("G", 0.0)) != 0.0:
-            raise ValueError("transport-limited SPL (spl.G > 0) is not implemented by gospl_b200")
+        p["G"] = float(spl.get("G", 0.0))
     else:
-        p["K"], p["d"], p["m"] = 1.0e-12, 0.0, 0.5
+        p["K"], p["d"], p["m"], p["G"] = 1.0e-12, 0.0, 0.5, 0.0
 
     hill = inp.get("diffusion")
     if hill is not None:

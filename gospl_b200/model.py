@@ -6,7 +6,7 @@
 * ``flowAccumulation()``  — FAMesh.flowAccumulation (flowplex.py:752-945)
 * ``fillElevation(sed)``  — PITFill.fillElevation (pitfilling.py:849-903)
 * ``_buildFlowDirection(h, down)`` — flowplex.py:480-544
-* ``erodepSPL()``         — SPL.erodepSPL (SPL.py:402-454), n = 1, G = 0
+* ``erodepSPL()``         — SPL.erodepSPL (SPL.py:402-454), n = 1, G >= 0
 * ``getHillslope()``      — hillSLP.getHillslope (hillslope.py:614-649)
 * ``applyForces()``       — UnstMesh.applyForces (unstructuredmesh.py:743-794)
 * ``runProcesses()``      — the time loop of model.py:331-466 with
@@ -42,7 +42,7 @@ class Model:
     Build from a goSPL YAML input (``Model("input.yml")``, the subset of keys
     read by inputparser.py for this path) or from arrays
     (``Model(coords=..., cells=..., elev=..., params=...)``).  ``params`` keys:
-    dt, tStart, tEnd, flowDir, K (scalar or per-vertex), d, m, Cda, Cdm, oFill,
+    dt, tStart, tEnd, flowDir, K (scalar or per-vertex), d, m, G, Cda, Cdm, oFill,
     sealevel, bc, rain (per-vertex m/yr), upsub (per-vertex m/yr or None).
     ``members`` = (start, maxarea) declares the mesh a disjoint union of
     landscapes (``gospl_b200.ensemble``).  ``precision=32`` selects the FP32
@@ -134,6 +134,10 @@ class Model:
         self._plan = handle
         self.stream = torch.cuda.current_stream(self.dev)
         _lib.check(L.gs_plan_set_stream(self._plan, ctypes.c_void_p(self.stream.cuda_stream)))
+        self.fDepa = float(p.get("G", 0.0))
+        if self.fDepa > 0.0:
+            # transport-limited SPL (SPL.py:116-258, 305-336)
+            _lib.check(L.gs_plan_set_deposition(self._plan, self.fDepa))
         if precision != 64:
             # FP32 sweeps and CG inside FP64 refinement to refine_tol
             _lib.check(L.gs_plan_set_precision(self._plan, int(precision), float(refine_tol)))

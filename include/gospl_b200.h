@@ -182,6 +182,13 @@ int gs_flow_accumulation(gs_plan* plan, const double* h, const double* bl, doubl
  * a sweep over the receiver graph.  Updates h and cum_ed in place and writes
  * eb = dz/dt.  Uses the receivers/lsink/sea produced by gs_flow_accumulation.
  */
+/*
+ * Transport-limited SPL: the deposition coefficient G of goSPL's `spl: G`
+ * (inputparser.py:472; default 0).  With G > 0 gs_erodep_spl solves the
+ * coupled erosion-deposition system of _getEroDepRate / _coupledEDSystem
+ * (SPL.py:116-258, 305-336) instead of the detachment-limited one.
+ */
+int gs_plan_set_deposition(gs_plan* plan, double g);
 int gs_erodep_spl(gs_plan* plan, double* h, double* cum_ed, double* eb, const double* fal,
                   const double* rain, double k_scalar, const double* k_field, double d,
                   double m, double dt, const int32_t* rcv_i, const double* dist_i,

@@ -75,6 +75,7 @@ class OracleModel:
         self.K = p["K"]
         self.coeffd = float(p.get("d", 0.0))
         self.spl_m = float(p.get("m", 0.5))
+        self.fDepa = float(p.get("G", 0.0))
         self.Cda = float(p.get("Cda", 0.0))
         self.Cdm = float(p.get("Cdm", 0.0))
         self.oFill = float(p.get("oFill", -6000.0))
@@ -532,13 +533,55 @@ class OracleModel:
             c[:, k] = data
         return c
 
+    def coupled_ed(self, hOld, c):
+        """Transport-limited SPL, _getEroDepRate's G > 0 branch (SPL.py:305-336)
+        and _coupledEDSystem (SPL.py:116-258): the nested system
+            [eMat - diag(f)      -diag(f dt / A)] [h]   [(1 - f) hOld ]
+            [diag(A / dt)         (I - W)^T     ] [q] = [hOld A / dt  ]
+        with f = G A / max(FAL, G A / 0.99) (0 where FAL = 0, at sea and at
+        flat-model outlets, capped at 0.99) and (I - W)^T the snapshot flow
+        matrix fMati (flowplex.py:787-791, matrixFlow 429-478), solved exactly
+        (sparse direct) where goSPL uses TFQMR with a Schur fieldsplit."""
+        n = self.lpoints
+        PA = self.FAL
+        num = self.fDepa * self.larea
+        floor_ = num / 0.99
+        f = np.divide(num, np.maximum(PA, floor_), out=np.zeros_like(PA), where=PA != 0)
+        f[self.seaID] = 0.0
+        f[f > 0.99] = 0.99
+        if self.flatModel:
+            f[self.outletIDs] = 0.0
+        nodes = np.arange(n)
+        R = self.flowDir
+        rows, cols, vals = [nodes], [nodes], [1.0 + c.sum(axis=1) - f]
+        wr, wc, wv = [nodes], [nodes], [np.ones(n)]
+        for k in range(R):
+            r = self.rcvIDi[:, k]
+            keep = r != nodes
+            rows.append(nodes[keep]); cols.append(r[keep]); vals.append(-c[keep, k])
+            w = self.wghtVali[:, k]
+            keepw = keep & (w != 0.0)
+            # (I - W)^T: row r gets -w at column i
+            wr.append(r[keepw]); wc.append(nodes[keepw]); wv.append(-w[keepw])
+        A00 = sp.csr_matrix((np.concatenate(vals), (np.concatenate(rows), np.concatenate(cols))), shape=(n, n))
+        A11 = sp.csr_matrix((np.concatenate(wv), (np.concatenate(wr), np.concatenate(wc))), shape=(n, n))
+        A01 = sp.diags(-f * self.dt / self.larea)
+        A10 = sp.diags(self.larea / self.dt)
+        M = sp.bmat([[A00, A01], [A10, A11]], format="csc")
+        rhs = np.concatenate([(1.0 - f) * hOld, hOld * self.larea / self.dt])
+        return spla.spsolve(M, rhs)[:n]
+
     def erodepSPL(self):
-        """SPL.py:402-454 with _getEroDepRate SPL.py:260-366 (G = 0)."""
+        """SPL.py:402-454 with _getEroDepRate SPL.py:260-366 (G = 0, or the
+        coupled erosion-deposition system when G > 0)."""
         hOld = self.h.copy()
         c = self.spl_coefficients(hOld)
-        stepED, left = F.spl_solve(self.rcvIDi, c, hOld)
-        if left > 0:
-            raise RuntimeError("SPL system is not triangular (%d rows left)" % left)
+        if self.fDepa > 0.0:
+            stepED = self.coupled_ed(hOld, c)
+        else:
+            stepED, left = F.spl_solve(self.rcvIDi, c, hOld)
+            if left > 0:
+                raise RuntimeError("SPL system is not triangular (%d rows left)" % left)
         E = (stepED - hOld) / self.dt
         if self.flatModel:
             E[self.outletIDs] = 0.0

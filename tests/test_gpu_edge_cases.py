@@ -77,3 +77,12 @@ def test_empty_plan():
     _lib.check(L.gs_flow_accumulation(plan, None, None, 0.0, -6000.0, 1.0, None, None, None, None, None, None,
                                       None, None, None, None, None, ctypes.byref(st)))
     _lib.check(L.gs_plan_destroy(plan))
+
+
+@pytest.mark.parametrize("G", [0.5, 1.0])
+def test_transport_limited_spl(G):
+    """spl: G > 0 (SPL.py:116-258, 305-336): the coupled erosion-deposition
+    system against the oracle's sparse direct solve."""
+    coords, cells, z, params = _planar(3000, 29, "ffff")
+    params = dict(params, G=G)
+    _step_vs_oracle(coords, cells, z, params)

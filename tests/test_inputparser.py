@@ -58,8 +58,7 @@ def test_reads_the_path_keys(tmp_path):
 
 def test_defaults_and_errors(tmp_path):
     y, _ = _write(tmp_path, YML.replace("    G: 0.\n", "    G: 1.\n"))
-    with pytest.raises(ValueError):
-        read_input(str(y))
+    assert read_input(str(y))[3]["G"] == 1.0
     y, _ = _write(tmp_path, YML.replace("    end: 300.\n    tout", "    end: -1.\n    tout"))
     with pytest.raises(ValueError):
         read_input(str(y))
