@@ -9,6 +9,8 @@ if ROOT not in sys.path:
 
 GOLDEN = os.path.join(ROOT, "tests", "golden")
 GOLDEN_CASES = ["incising", "sphere3766", "planar2k", "ico2562"]
+# transport-limited SPL (G > 0), compared step by step from the reference's state
+GOLDEN_G_CASES = ["ico2562_G05", "planar2k_G1"]
 
 
 def pytest_configure(config):

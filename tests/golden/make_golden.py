@@ -3,7 +3,7 @@
 Run in a container where a goSPL checkout is available (default
 /root/reference, override with GOSPL_REF):
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py [case ...]
 
 For each case it (1) checks the oracle's restatement of the numpy Voronoi
 helpers against the reference's own ``gospl/mesher/meshfunc.py``, (2) runs the
@@ -65,6 +65,11 @@ def cases():
     p = dict(dt=1.0e4, tEnd=1.0e5, flowDir=3, K=5.0e-7, d=0.0, m=0.5, Cda=0.05, Cdm=0.05,
              sealevel=0.0, bc="oooo", rain=rain, upsub=up)
     out.append(("ico2562", c, f, z, p, 3))
+    # transport-limited SPL (G > 0): the coupled erosion-deposition system
+    out.append(("ico2562_G05", c, f, z, dict(p, G=0.5), 3))
+    c, f, z, rain, up, p = S.planar_config(n=2000, side=30.0e3, seed=7)
+    p = dict(p, rain=rain, upsub=up, tEnd=10 * p["dt"], G=1.0)
+    out.append(("planar2k_G1", c, f, z, p, 3))
     return out
 
 
@@ -75,7 +80,10 @@ def main():
 
     mf = RH.load_meshfunc(REF)
     RefModel = RH.make_model_class(REF)
+    only = set(sys.argv[1:])
     for name, coords, cells, z, params, nsteps in cases():
+        if only and name not in only:
+            continue
         cells = np.asarray(cells, dtype=np.int32)
         # (1) meshfunc restatement vs the reference's meshfunc
         vb = mf.VoroBuild()
@@ -120,6 +128,8 @@ def main():
         for k in ("dt", "tEnd", "flowDir", "K", "d", "m", "Cda", "Cdm", "sealevel"):
             arrs["p_" + k] = np.array(params[k])
         arrs["p_bc"] = np.array(params["bc"])
+        if "G" in params:
+            arrs["p_G"] = np.array(params["G"])
         for i, s in enumerate(snaps):
             for k, v in s.items():
                 arrs["s%d_%s" % (i, k)] = np.asarray(v)

@@ -34,7 +34,7 @@ import scipy.sparse.linalg as spla
 # petsc4py stand-in
 # ---------------------------------------------------------------------------
 class Vec:
-    def __init__(self, n_or_arr):
+    def __init__(self, n_or_arr=0):
         if np.isscalar(n_or_arr):
             self.a = np.zeros(int(n_or_arr))
         else:
@@ -93,6 +93,28 @@ class Vec:
 
     def getSizes(self):
         return (len(self.a), len(self.a))
+
+    def scale(self, alpha):
+        self.a[:] = alpha * self.a
+
+    # nested vectors (SPL.py _coupledEDSystem): one flat array, blocks by IS
+    def createNest(self, vecs, comm=None):
+        self.a = np.concatenate([v.a for v in vecs])
+        return self
+
+    def setUp(self):
+        pass
+
+    def getSubVector(self, iset):
+        return Vec(self.a[iset.idx])
+
+    def destroy(self):
+        pass
+
+
+class IS:
+    def __init__(self, idx):
+        self.idx = idx
 
     def destroy(self):
         pass
@@ -155,6 +177,18 @@ class Mat:
     def mult(self, x, y):
         y.a[:] = self.A @ x.a
 
+    # nested matrices (SPL.py _coupledEDSystem): assembled as one sparse block matrix
+    def createNest(self, mats, comm=None):
+        self.A = sp.bmat([[m.A for m in row] for row in mats], format="csr")
+        self.blocks = [row[0].A.shape[0] for row in mats]
+        self.n = self.A.shape[0]
+        return self
+
+    def getNestISs(self):
+        off = np.concatenate([[0], np.cumsum(self.blocks)])
+        iss = [IS(np.arange(off[k], off[k + 1])) for k in range(len(self.blocks))]
+        return iss, iss
+
     def norm(self, *a):
         return float(spla.norm(self.A))
 
@@ -206,6 +240,9 @@ class KSP:
     class ConvergedReason:
         CONVERGED_RTOL = 2
 
+    Type = types.SimpleNamespace(TFQMR="tfqmr", RICHARDSON="richardson", CG="cg", GMRES="gmres",
+                                 FGMRES="fgmres", PREONLY="preonly", BCGS="bcgs")
+
     def create(self, comm=None):
         return KSP()
 
@@ -232,7 +269,7 @@ class KSP:
 
     def solve(self, b, x):
         A = self.Aop.A
-        if getattr(self, "prefix", "") == "hilllin_":
+        if getattr(self, "prefix", "") in ("hilllin_", "spl_ed_"):
             x.a[:] = spla.spsolve(A.tocsc(), b.a)
         else:
             sol, _ = exact_solve(A, b.a)
@@ -244,9 +281,21 @@ class KSP:
     def getIterationNumber(self):
         return 1
 
+    def destroy(self):
+        pass
+
 
 class PC:
     def setType(self, t):
+        pass
+
+    def setFieldSplitIS(self, *fields):
+        pass
+
+    def getFieldSplitSubKSP(self):
+        return [KSP(), KSP()]
+
+    def destroy(self):
         pass
 
     def setReusePreconditioner(self, f):
@@ -256,6 +305,9 @@ class PC:
 class _Options(dict):
     def setValue(self, k, v):
         self[k] = v
+
+    def hasName(self, k):
+        return k in self
 
 
 class _Comm:
@@ -282,6 +334,7 @@ def _petsc_module():
     PETSc.COMM_WORLD = _Comm()
     PETSc.IntType = np.int32
     PETSc.Mat = Mat
+    PETSc.Vec = Vec
     PETSc.KSP = KSP
     PETSc.Options = lambda _o=_Options(): _o
     PETSc.NormType = types.SimpleNamespace(FROBENIUS=3)
@@ -468,7 +521,7 @@ def make_model_class(refroot):
             self.flowExp = 1.1
             self.K = p["K"]
             self.coeffd = float(p.get("d", 0.0))
-            self.fDepa = 0.0
+            self.fDepa = float(p.get("G", 0.0))
             self.spl_m = float(p.get("m", 0.5))
             self.spl_n = 1.0
             self.Cda = float(p["Cda"])
