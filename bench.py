@@ -167,7 +167,8 @@ def main():
     ap.add_argument("--level", type=int, default=9)
     ap.add_argument("--cpu-level", type=int, default=7)
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--workload", default="sphere", choices=["sphere", "planar", "ensemble", "precision"])
+    ap.add_argument("--workload", default="sphere", choices=["sphere", "planar", "ensemble", "precision",
+                                                                   "transport"])
     ap.add_argument("--members", type=int, default=256)
     ap.add_argument("--loop", action="store_true", help="ensemble: also time the per-member loop")
     ap.add_argument("--adjoint-steps", type=int, default=4, help="sphere: steps of the adjoint timing (0: skip)")
@@ -190,6 +191,9 @@ def main():
     torch.cuda.set_device(dev)
     if args.workload == "precision":
         run_precision(args, dev)
+        return
+    if args.workload == "transport":
+        run_transport(args, dev)
         return
     pg = None
     if world > 1:
@@ -482,6 +486,57 @@ def run_precision(args, dev):
                                                                 "erosion_rate": err("Eb"), "elevation": err("h")},
                           "note": "errors relative to the largest |value| of the FP64 field; over many steps the "
                                   "two trajectories part where a discrete decision (tie, threshold) flips"}}
+    print(json.dumps(line), flush=True)
+
+
+def run_transport(args, dev, G=1.0):
+    """Transport-limited SPL (G = 1) against detachment-limited SPL (G = 0) on
+    the 2.6M-vertex sphere: the same steps from the same state, time per
+    step, time of the erosion stage alone and the coupled solver's iterations."""
+    import torch
+    from gospl_b200.mesh import FVMesh
+    from gospl_b200.model import Model
+    c, f, z, rain, up, p = sphere_inputs(args.level)
+    p = dict(p, rain=rain, upsub=up, tEnd=1.0e30)
+    mesh = FVMesh(c, f, p["bc"], device=dev)
+    stream = torch.cuda.current_stream(dev)
+    out = {}
+    for g in (G, 0.0):
+        m = Model(coords=c, cells=f, elev=z, params=dict(p, G=g), mesh=mesh, device=dev)
+        for _ in range(args.warmup):
+            m.step()
+        torch.cuda.synchronize(dev)
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2 * args.steps + 2)]
+        iters = []
+        ev[0].record(stream)
+        for k in range(args.steps):
+            m.flowAccumulation()
+            ev[2 + 2 * k].record(stream)
+            m.erodepSPL()
+            ev[3 + 2 * k].record(stream)
+            iters.append(m.stats["spl"]["cg_iters"])
+            m.getHillslope()
+            if m.tNow < m.tEnd:
+                m.applyForces()
+            m.tNow += m.dt
+        ev[1].record(stream)
+        torch.cuda.synchronize(dev)
+        spl = sum(ev[2 + 2 * k].elapsed_time(ev[3 + 2 * k]) for k in range(args.steps)) / args.steps
+        out[g] = dict(ms=ev[0].elapsed_time(ev[1]) / args.steps, spl_ms=spl, iters=iters,
+                      relres=m.stats["spl"]["cg_relres"])
+        m.destroy()
+    n = len(z)
+    line = {"metric": "landscape vertex-steps/s, transport-limited SPL (G = %g) @2.6M-vertex sphere" % G,
+            "value": n * 1000.0 / out[G]["ms"], "unit": "vertex-steps/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": out[G]["ms"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded sphere, SH relief)",
+            "config": {"workload": "sphere level %d (%d vertices), full physics step with the coupled "
+                                   "erosion-deposition solve" % (args.level, n),
+                       "vertices": n, "G": G, "global_batch": 1, "seq_len": 0, "parallelism": "single"},
+            "transport": {"ms_per_step": out[G]["ms"], "erosion_ms_per_step": out[G]["spl_ms"],
+                          "bicgstab_iterations": out[G]["iters"], "final_relres": out[G]["relres"],
+                          "detachment_limited_ms_per_step": out[0.0]["ms"],
+                          "detachment_limited_erosion_ms_per_step": out[0.0]["spl_ms"]}}
     print(json.dumps(line), flush=True)
 
 

@@ -22,6 +22,7 @@ struct gs_plan {
     int fp32 = 0;
     double fdepa = 0.0;                  // SPL deposition coefficient G (0: detachment-limited)
     int ed_iters = 0;                    // BiCGSTAB iterations of the last coupled solve
+    double ed_relres = 0.0;              // its final relative residual
     double* ed_buf = nullptr;            // [6][n] coupled-solve scratch
     double refine_tol = 1.0e-10;         // max|r| / max|b| of every refined solve
     int64_t refine_iters = 0;            // refinement passes since the last reset

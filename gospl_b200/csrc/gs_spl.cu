@@ -252,6 +252,7 @@ static int coupled_ed(gs_plan* p, const double* hold, const double* fal, const u
         if (!(rn == rn)) break;
     }
     p->ed_iters = it;
+    p->ed_relres = anorm > 0.0 ? sqrt(rn) / anorm : 0.0;
     if (!(rn == rn) || sqrt(rn) > tol * anorm * 1.0e3) {
         set_error(GS_EMAXITER, "transport-limited SPL: BiCGSTAB did not converge");
         return GS_EMAXITER;
@@ -278,7 +279,10 @@ int erodep_spl(gs_plan* p, double* h, double* cum_ed, double* eb, const double* 
     launch(p, k_spl_update, G, B, n, p->flat, (const uint8_t*)p->outlet, lsink, (const double*)hold,
            (const double*)p->q3, dt, h, cum_ed, eb);
     GS_LAUNCH();
-    (void)st;
+    if (st) {
+        st->cg_iters = p->fdepa > 0.0 ? p->ed_iters : 0;
+        st->cg_relres = p->fdepa > 0.0 ? p->ed_relres : 0.0;
+    }
     return GS_OK;
 }
 

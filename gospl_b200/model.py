@@ -239,6 +239,7 @@ class Model:
             _lib.ptr(self.FAL), _lib.ptr(self.rainVal), self.K, _lib.ptr(self.Kfield), self.coeffd,
             self.spl_m, self.dt, _lib.ptr(self.rcv_i), _lib.ptr(self.dist_i), _lib.ptr(self.wgt_i),
             _lib.ptr(self.lsink_mask), _lib.ptr(self.sea_mask), ctypes.byref(st)))
+        self.stats["spl"] = st.as_dict()
 
     def getHillslope(self):
         L = _lib_handle()
