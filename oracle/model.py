@@ -80,6 +80,14 @@ class OracleModel:
         self.Cdm = float(p.get("Cdm", 0.0))
         self.oFill = float(p.get("oFill", -6000.0))
         self.sealevel = float(p.get("sealevel", 0.0))
+        self.nodep = bool(p.get("nodep", True))
+        self.seaDepo = bool(p.get("seadepo", False))
+        if not self.nodep and self.seaDepo:
+            raise NotImplementedError("marine deposition (seaChange) is not restated")
+        self.nl_pit_volume = float(p.get("nlPitVolume", 1.0e9))   # inputparser.py:562,584
+        self.nl_pit_depth = float(p.get("nlPitDepth", 100.0))     # inputparser.py:563,585
+        self._domainHasOutlet = len(self.outletIDs) > 0           # sedplex.py:45-47
+        self.lcoords = np.asarray(coords, dtype=np.float64).reshape(-1, 3)
         self.rainMesh = np.asarray(p["rain"], dtype=np.float64)
         up = p.get("upsub")
         self.upsub = None if up is None else np.asarray(up, dtype=np.float64)
@@ -638,11 +646,180 @@ class OracleModel:
         self.h = hNew
         self.EbLocal = self.EbLocal + tmp / self.dt
 
+    # ------------------------------------------------- continental deposition
+    def _getSedFlux(self):
+        """sedplex.py:103-188 (no stratigraphy, no provenance): the volumetric
+        sediment flux vSed (m3/yr) = (I - W^T)^-1 (-Eb * area) over the
+        snapshot receivers of the last flowAccumulation (fMati)."""
+        rhs = -self.EbLocal * self.larea
+        q, left = F.flow_solve(self.rcvIDi, self.wghtVali, rhs)
+        if left > 0:
+            raise RuntimeError("snapshot flow graph is not acyclic (%d rows left)" % left)
+        self.vSed = q
+
+    def _moveDownstream(self, vSed, step):
+        """sedplex.py:190-374 (single lithology, no provenance, one rank).
+        Returns (excess, routed flux or None)."""
+        excess = False
+        changed = False
+        csink = self.lsink & (self.pitIDs < 0)
+        if csink.any():
+            if not self._domainHasOutlet:
+                self._closedDepo[csink] += vSed[csink]
+            vSed = vSed.copy()
+            vSed[csink] = 0.0
+        uID, vol = group_reduce(self.pitIDs[self.lsink], vSed[self.lsink])
+        inV = np.zeros(len(self.pitParams))
+        ok = uID > -1
+        inV[uID[ok]] = vol[ok]
+        nvSed = np.zeros(self.lpoints)
+        eV = inV - self.pitVol
+        if (eV > 0.0).any():
+            eIDs = eV > 0.0
+            spillIDs = self.pitInfo[eIDs, 0]
+            localSpill = np.where(self.pitInfo[eIDs, 1] == 0)[0]
+            localPts = spillIDs[localSpill]
+            nvSed[localPts] = eV[eIDs][localSpill]
+            self.pitVol[eIDs] = 0.0
+            ids = np.isin(self.pitIDs, np.where(eV > 0.0)[0])
+            self.sedFilled[ids] = self.lFill[ids]
+            changed = True
+        eIDs = eV < 0
+        self.pitVol[eIDs] -= inV[eIDs]
+        self.pitVol[self.pitVol < 0] = 0.0
+        routed = None
+        if (eV > 1.0e-3).any():
+            if changed or step == 0 or step == 100:
+                if step == 100:
+                    self._buildFlowDirection(self.lFill)
+                else:
+                    self._buildFlowDirection(self.sedFilled)
+            if nvSed.sum() > 0.5 * self.maxarea[0]:
+                excess = True
+                routed = self._flow_solve(nvSed)
+        return excess, routed
+
+    def _distributeSediment(self, hl):
+        """sedplex.py:376-522 (single lithology, no provenance)."""
+        vSed = self.vSed.copy() * self.dt
+        self._closedDepo = np.zeros(self.lpoints)
+        step = 0
+        excess = True
+        while excess:
+            if step >= 5000:
+                break
+            excess, routed = self._moveDownstream(vSed, step)
+            if excess:
+                vSed = routed.copy()
+                nvSed = vSed.copy()
+                nvSed[hl < self.sedFilled] = 0.0
+                self.vSed = self.vSed + nvSed / self.dt
+                vSed[self.outletIDs] = 0.0
+            step += 1
+        self.sed_passes = step
+        if self._closedDepo.any():
+            delta = np.zeros(self.lpoints)
+            nz = self._closedDepo > 0.0
+            delta[nz] = self._closedDepo[nz] / self.larea[nz]
+            self.cumED = self.cumED + delta
+            self.h = self.h + delta
+
+    def _bottomUpDelta(self, hl, depo, pit_select):
+        """sedplex.py:524-559: lake surface at the level whose filled volume
+        matches the deposit (np.interp over the pit's depth-volume table)."""
+        num_pits = len(self.pitParams)
+        target_lvl = np.full(num_pits, -np.inf)
+        active = np.where(pit_select & (depo > 0))[0]
+        for p in active:
+            pit_min = self.pitParams[p, 1] - self.pitParams[p, 2]
+            vols = np.concatenate(([0.0], self.filled_vol[p]))
+            lvls = np.concatenate(([pit_min], self.filled_lvl[p]))
+            target_lvl[p] = np.interp(depo[p], vols, lvls)
+        node_target_lvl = np.full(self.lpoints, -np.inf)
+        in_pit = self.pitIDs >= 0
+        node_target_lvl[in_pit] = target_lvl[self.pitIDs[in_pit]]
+        surface = np.minimum(node_target_lvl, self.lFill)
+        delta = np.maximum(0.0, surface - hl)
+        sel_node = np.isin(self.pitIDs, active) if active.size > 0 else np.zeros(self.lpoints, bool)
+        delta[~sel_node] = 0.0
+        return delta
+
+    def _addPitMicroTilt(self, delta, pit_select):
+        """sedplex.py:561-644: tilt each partly filled lake surface by 1e-6
+        m/m towards its spill point, per-pit mean distance removed."""
+        num_pits = len(self.pitParams)
+        if not pit_select.any():
+            return delta
+        active_pit = np.where(pit_select)[0]
+        sel_node = np.isin(self.pitIDs, active_pit) & (delta > 0)
+        spill_xyz = np.zeros((num_pits, 3))
+        spill_idx = self.pitInfo[:, 0].astype(int)
+        mp = np.where((self.pitInfo[:, 1] == 0) & (spill_idx >= 0))[0]
+        spill_xyz[mp] = self.lcoords[spill_idx[mp]]
+        in_pit = self.pitIDs >= 0
+        pit_safe = np.where(in_pit, self.pitIDs, 0)
+        dist = np.linalg.norm(self.lcoords - spill_xyz[pit_safe], axis=1)
+        local_sum = np.zeros(num_pits)
+        local_cnt = np.zeros(num_pits)
+        if sel_node.any():
+            ids = self.pitIDs[sel_node]
+            up, sums = group_reduce(ids, dist[sel_node])
+            _, cnts = group_reduce(ids, np.ones_like(dist[sel_node]))
+            local_sum[up] = sums
+            local_cnt[up] = cnts
+        with np.errstate(divide="ignore", invalid="ignore"):
+            mean_dist = np.where(local_cnt > 0, local_sum / np.maximum(local_cnt, 1.0), 0.0)
+        tilt = 1.0e-6 * (dist - mean_dist[pit_safe])
+        tilt[~sel_node] = 0.0
+        tilted = delta + tilt
+        tilted[tilted < 0] = 0.0
+        return tilted
+
+    def _updateSinks(self, hl):
+        """sedplex.py:982-1059 (paths 1 and 2; path 3, non-linear diffusion in
+        large deep partly filled pits, is not restated)."""
+        depo = self.pitParams[:, 0] - self.pitVol
+        depo[depo < 0] = 0.0
+        pit_volume = self.pitParams[:, 0]
+        pit_depth = self.pitParams[:, 2]
+        active = depo > 0
+        full_fill = active & (depo >= pit_volume - 1.0e-6)
+        partial = active & ~full_fill
+        is_large = (pit_volume >= self.nl_pit_volume) & (pit_depth >= self.nl_pit_depth)
+        diffuse_path = partial & is_large
+        bottomup_path = full_fill | (partial & ~is_large)
+        if diffuse_path.any():
+            raise NotImplementedError("lake deposition by non-linear diffusion (%d large deep pits)"
+                                      % int(diffuse_path.sum()))
+        delta = self._bottomUpDelta(hl, depo, bottomup_path)
+        if bottomup_path.any():
+            delta = self._addPitMicroTilt(delta, bottomup_path)
+        self.sed_delta = delta
+        self.cumED = self.cumED + delta
+        self.h = self.h + delta
+        self.pitParams[:, 0] = self.pitVol.copy()
+
+    def sedChange(self):
+        """sedplex.py:1061-1086."""
+        self._getSedFlux()
+        self.fillElevation(sed=True)
+        hl = self.h.copy()
+        self.lsink = self.lsinki.copy()
+        self.pitVol = self.pitParams[:, 0].copy()
+        self.sedFilled = hl.copy()
+        self._distributeSediment(hl)
+        self._updateSinks(hl)
+
     # ------------------------------------------------------------------- loop
     def step(self):
-        """One iteration of runProcesses with fast=False, nodep=True (model.py:347-453)."""
+        """One iteration of runProcesses with fast=False (model.py:347-453):
+        flow, erosion, continental deposition unless nodep (flow again, then
+        sedChange), hillslope, forcing."""
         self.flowAccumulation()
         self.erodepSPL()
+        if not self.nodep:
+            self.flowAccumulation()
+            self.sedChange()
         self.getHillslope()
         if self.tNow < self.tEnd:
             self.applyForces()

@@ -32,6 +32,10 @@ SNAP = ("h", "cumED", "EbLocal", "FAL", "fillFAL", "lFill", "pitIDs", "flatDirs"
 
 def snapshot(m, ref):
     out = {}
+    if not m.nodep:
+        # continental deposition: routed sediment flux (m3/yr)
+        out["vSed"] = (m.vSedLocal.getArray().copy() if ref else m.vSed.copy()) if hasattr(m, "vSed") \
+            else np.zeros(len(m.larea))
     get = (lambda v: v.getArray().copy()) if ref else (lambda v: np.array(v, copy=True))
     for k in SNAP:
         if k in ("h",):
@@ -70,6 +74,23 @@ def cases():
     c, f, z, rain, up, p = S.planar_config(n=2000, side=30.0e3, seed=7)
     p = dict(p, rain=rain, upsub=up, tEnd=10 * p["dt"], G=1.0)
     out.append(("planar2k_G1", c, f, z, p, 3))
+    # continental sediment routing and deposition in depressions (nodep off,
+    # no marine deposition)
+    d = np.load(os.path.join(REF, "tests", "fixtures", "incising.npz"))
+    out.append(("incising_sed", d["v"], d["c"], d["z"],
+                dict(dt=100.0, tEnd=300.0, flowDir=3, K=4.0e-6, d=0.0, m=0.5, Cda=0.01, Cdm=0.2,
+                     sealevel=-100.0, bc="oooo", rain=np.ones(len(d["z"])), upsub=None, nodep=False), 3))
+    c, f, z, rain, up, p = S.planar_config(n=2000, side=30.0e3, seed=7)
+    p = dict(p, rain=rain, upsub=up, tEnd=10 * p["dt"], nodep=False)
+    out.append(("planar2k_sed", c, f, z, p, 3))
+    c, f = S.icosphere(4)
+    z = S.rescale(S.sh_field(c, 48, 11), -4000.0, 3000.0)
+    g = S.sh_field(c, 16, 12)
+    rain = np.exp(0.5 * (g - g.mean()) / g.std())
+    up = S.belt_uplift(c, 13)
+    p = dict(dt=1.0e4, tEnd=1.0e5, flowDir=3, K=5.0e-7, d=0.0, m=0.5, Cda=0.05, Cdm=0.05,
+             sealevel=0.0, bc="oooo", rain=rain, upsub=up, nodep=False, nlPitVolume=1.0e30)
+    out.append(("ico2562_sed", c, f, z, p, 3))
     return out
 
 
@@ -110,7 +131,7 @@ def main():
             osn.append(snapshot(om, False))
         worst = {}
         for s_ref, s_or in zip(snaps, osn):
-            for k in SNAP:
+            for k in s_ref:
                 a, b = np.asarray(s_ref[k], float), np.asarray(s_or[k], float)
                 if a.shape != b.shape:
                     worst[k] = "shape %s vs %s" % (a.shape, b.shape)
@@ -128,8 +149,9 @@ def main():
         for k in ("dt", "tEnd", "flowDir", "K", "d", "m", "Cda", "Cdm", "sealevel"):
             arrs["p_" + k] = np.array(params[k])
         arrs["p_bc"] = np.array(params["bc"])
-        if "G" in params:
-            arrs["p_G"] = np.array(params["G"])
+        for k in ("G", "nodep", "nlPitVolume", "nlPitDepth"):
+            if k in params:
+                arrs["p_" + k] = np.array(params[k])
         for i, s in enumerate(snaps):
             for k, v in s.items():
                 arrs["s%d_%s" % (i, k)] = np.asarray(v)

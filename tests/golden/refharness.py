@@ -458,7 +458,8 @@ def load_reference(refroot):
     pitfilling = importlib.import_module("gospl.flow.pitfilling")
     SPLm = importlib.import_module("gospl.eroder.SPL")
     hill = importlib.import_module("gospl.sed.hillslope")
-    return flowplex.FAMesh, pitfilling.PITFill, SPLm.SPL, hill.hillSLP
+    sedplex = importlib.import_module("gospl.sed.sedplex")
+    return flowplex.FAMesh, pitfilling.PITFill, SPLm.SPL, hill.hillSLP, sedplex.SEDMesh
 
 
 def load_meshfunc(refroot):
@@ -479,9 +480,9 @@ class _NullProfiler:
 
 
 def make_model_class(refroot):
-    FAMesh, PITFill, SPL, hillSLP = load_reference(refroot)
+    FAMesh, PITFill, SPL, hillSLP, SEDMesh = load_reference(refroot)
 
-    class RefModel(FAMesh, PITFill, SPL, hillSLP):
+    class RefModel(FAMesh, PITFill, SPL, hillSLP, SEDMesh):
         """One-rank goSPL model restricted to flowAccumulation / erodepSPL /
         getHillslope; forcing follows unstructuredmesh.py:743-972."""
 
@@ -544,10 +545,17 @@ def make_model_class(refroot):
             self.evapStream = False
             self.sedfacVal = None
             self.evapLoss = 0.0
+            self.nodep = bool(p.get("nodep", True))
+            self.provOn = False
+            self.provNb = 0
+            self.lcoords = np.asarray(mesh["coords"], dtype=np.float64).reshape(-1, 3)
+            self.nl_pit_volume = float(p.get("nlPitVolume", 1.0e9))
+            self.nl_pit_depth = float(p.get("nlPitDepth", 100.0))
             FAMesh.__init__(self)
             PITFill.__init__(self)
             SPL.__init__(self)
             hillSLP.__init__(self)
+            SEDMesh.__init__(self)
             self.applyForces()
             self.flowAccumulation()
 
@@ -578,6 +586,9 @@ def make_model_class(refroot):
         def step(self):
             self.flowAccumulation()
             self.erodepSPL()
+            if not self.nodep:
+                self.flowAccumulation()
+                self.sedChange()
             self.getHillslope()
             if self.tNow < self.tEnd:
                 self.applyForces()
