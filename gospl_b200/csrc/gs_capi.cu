@@ -300,6 +300,23 @@ int gs_erodep_spl(gs_plan* plan, double* h, double* cum_ed, double* eb, const do
                                    wgt_i, lsink, sea, stats);)
 }
 
+int gs_sed_change(gs_plan* plan, double* h, double* cum_ed, const double* eb, const double* xyz, double sealevel,
+                  double ofill, double dt, double nl_pit_volume, double nl_pit_depth, double* lfill,
+                  int32_t* pit_ids, int32_t* flat_dirs, const int32_t* rcv_i, const double* wgt_i, uint8_t* lsink,
+                  const uint8_t* sea, double* vsed, gs_stats* stats) {
+    NEED(plan);
+    if (plan->n > 0) {
+        NEED(h); NEED(cum_ed); NEED(eb); NEED(xyz); NEED(lfill); NEED(pit_ids); NEED(flat_dirs); NEED(rcv_i);
+        NEED(wgt_i); NEED(lsink); NEED(sea); NEED(vsed);
+    }
+    if (!(dt > 0)) {
+        gs::set_error(GS_EINVAL, "dt must be positive");
+        return GS_EINVAL;
+    }
+    GS_GUARD(return gs::sed_change(plan, h, cum_ed, eb, xyz, sealevel, ofill, dt, nl_pit_volume, nl_pit_depth,
+                                   lfill, pit_ids, flat_dirs, rcv_i, wgt_i, lsink, sea, vsed, stats);)
+}
+
 int gs_hillslope(gs_plan* plan, double* h, double* cum_ed, double* eb, double sealevel, double cda, double cdm,
                  double dt, double rtol, int32_t max_iter, gs_stats* stats) {
     NEED(plan);

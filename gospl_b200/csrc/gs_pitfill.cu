@@ -986,7 +986,7 @@ int fill_join(gs_plan* p, gs_stats* st) {
 }
 
 int fill_elevation(gs_plan* p, const double* h, double sealevel, double ofill, double* lfill,
-                   int* pit_ids, int* flat_dirs, gs_stats* st, bool defer_flats, uint8_t* sea_out) {
+                   int* pit_ids, int* flat_dirs, gs_stats* st, bool defer_flats, uint8_t* sea_out, bool sed) {
     const int n = (int)p->n;
     GS_TRY(fill_join(p, nullptr));
     if (n == 0) { p->npits = 0; return GS_OK; }
@@ -999,6 +999,17 @@ int fill_elevation(gs_plan* p, const double* h, double sealevel, double ofill, d
     launch(p, k_level, 1, 1, (const unsigned long long*)p->u_scalar, p->flat ? 0 : 1, sealevel, ofill,
            p->d_scalar);
     GS_LAUNCH();
+    // Filling with sediment (pitfilling.py:557-702, 704-847 with sed=True):
+    // open-sea depressions are filled too, pits are labelled above the fill
+    // level instead of sea level, and pit volumes use the unclipped surface.
+    double label_sl = sealevel, clip_sl = sealevel, marine_sl = sealevel;
+    if (sed) {
+        GS_CUDA(cudaMemcpyAsync(&label_sl, p->d_scalar + D_LEVEL, sizeof(double), cudaMemcpyDeviceToHost,
+                                p->stream));
+        GS_CUDA(cudaStreamSynchronize(p->stream));
+        clip_sl = -INFINITY;
+        marine_sl = -INFINITY;
+    }
 
     // seeds, descent links, roots
     launch(p, k_classify, G, B, n, h, (const double*)p->d_scalar, (const int*)p->nbr,
@@ -1039,26 +1050,26 @@ int fill_elevation(gs_plan* p, const double* h, double sealevel, double ofill, d
         rounds = hbuf[0] - 1;
     }
     if (st) st->fill_rounds = rounds + 1;
-    launch(p, k_fill_final, G, B, n, h, (const double*)p->d_scalar, sealevel, (const int8_t*)p->ledge,
+    launch(p, k_fill_final, G, B, n, h, (const double*)p->d_scalar, marine_sl, (const int8_t*)p->ledge,
            (const int*)p->parent, (const unsigned long long*)p->basinL, lfill);
     GS_LAUNCH();
 
     // label_pits: equal-fill components of cells above sea level
-    launch(p, k_uf_init, G, B, n, (const double*)lfill, sealevel, (const int*)p->nbr, (const int8_t*)p->nnb,
+    launch(p, k_uf_init, G, B, n, (const double*)lfill, label_sl, (const int*)p->nbr, (const int8_t*)p->nnb,
            p->comp);
-    launch(p, k_uf_link, G, B, n, (const double*)lfill, sealevel, (const int*)p->nbr,
+    launch(p, k_uf_link, G, B, n, (const double*)lfill, label_sl, (const int*)p->nbr,
            (const int8_t*)p->nnb, p->comp);
     launch(p, k_uf_flatten, G, B, n, p->comp);
     launch(p, k_fill_int, G, B, n, p->minseed, (int)INT_MAX);
     GS_LAUNCH();
-    launch(p, k_minseed, G, B, n, (const double*)lfill, sealevel, (const int*)p->nbr,
+    launch(p, k_minseed, G, B, n, (const double*)lfill, label_sl, (const int*)p->nbr,
            (const int8_t*)p->nnb, (const int*)p->comp, p->minseed);
-    launch(p, k_seed_flag, G, B, n, (const double*)lfill, sealevel, (const int*)p->comp,
+    launch(p, k_seed_flag, G, B, n, (const double*)lfill, label_sl, (const int*)p->comp,
            (const int*)p->minseed, p->flagbuf);
     GS_LAUNCH();
     GS_TRY(exclusive_scan(p, p->flagbuf, p->scanbuf, n));
     GS_CUDA(cudaMemsetAsync(p->seg_keys, 0, sizeof(int) * (n + 1), p->stream));  // present[]
-    launch(p, k_label, G, B, n, (const double*)lfill, sealevel, (const int*)p->comp,
+    launch(p, k_label, G, B, n, (const double*)lfill, label_sl, (const int*)p->comp,
            (const int*)p->minseed, (const int*)p->scanbuf, (const uint8_t*)p->outlet, p->lab,
            p->seg_keys);
     GS_LAUNCH();
@@ -1201,11 +1212,11 @@ int fill_elevation(gs_plan* p, const double* h, double sealevel, double ofill, d
     GS_TRY(exclusive_scan(p, p->seg_count, p->seg_start, np1));
     // pit tables
     launch(p, k_pit_params, np1, 256, np1, (const int*)p->seg_start,
-           (const int*)p->seg_count, (const int*)p->seg_vals2, (const double*)lfill, h, sealevel,
+           (const int*)p->seg_count, (const int*)p->seg_vals2, (const double*)lfill, h, clip_sl,
            (const double*)p->larea, p->pit_params);
     launch(p, k_filled_lvl, grid_for(np1, B), B, np1, (const double*)p->pit_params, p->filled_lvl);
     launch(p, k_filled_vol, np1, 256, np1, (const int*)p->seg_start,
-           (const int*)p->seg_count, (const int*)p->seg_vals2, h, sealevel, (const double*)p->farea,
+           (const int*)p->seg_count, (const int*)p->seg_vals2, h, clip_sl, (const double*)p->farea,
            (const double*)p->filled_lvl, (const double*)p->pit_params, p->filled_vol);
     GS_LAUNCH();
     {

@@ -24,6 +24,8 @@ struct gs_plan {
     int ed_iters = 0;                    // BiCGSTAB iterations of the last coupled solve
     double ed_relres = 0.0;              // its final relative residual
     double* ed_buf = nullptr;            // [6][n] coupled-solve scratch
+    double* sed_buf = nullptr;           // [8][n] sediment-routing scratch
+    uint8_t* sed_mask = nullptr;         // [2][n] sediment-routing masks
     double refine_tol = 1.0e-10;         // max|r| / max|b| of every refined solve
     int64_t refine_iters = 0;            // refinement passes since the last reset
     float* f32a = nullptr;               // FP32 correction / CG vectors
@@ -248,7 +250,7 @@ int spl_sweep(gs_plan* p, const int* rcv, const double* c, const int8_t* rslot, 
               double* s, int* cycle_nodes, bool reuse_order);
 int fill_elevation(gs_plan* p, const double* h, double sealevel, double ofill, double* lfill,
                    int* pit_ids, int* flat_dirs, gs_stats* st, bool defer_flats = false,
-                   uint8_t* sea_out = nullptr);
+                   uint8_t* sea_out = nullptr, bool sed = false);
 // joins the flat-distance BFS of the last fill (if it ran on side_b) into the
 // main stream and records its level count
 int fill_join(gs_plan* p, gs_stats* st);
@@ -275,6 +277,10 @@ int erodep_spl(gs_plan* p, double* h, double* cum_ed, double* eb, const double* 
                const double* rain, double k_scalar, const double* k_field, double d, double m,
                double dt, const int* rcv_i, const double* dist_i, const double* wgt_i,
                const uint8_t* lsink, const uint8_t* sea, gs_stats* st);
+int sed_change(gs_plan* p, double* h, double* cum_ed, const double* eb, const double* xyz, double sealevel,
+               double ofill, double dt, double nl_pit_volume, double nl_pit_depth, double* lfill, int* pit_ids,
+               int* flat_dirs, const int* rcv_i, const double* wgt_i, uint8_t* lsink, const uint8_t* sea,
+               double* vsed, gs_stats* st);
 int hillslope(gs_plan* p, double* h, double* cum_ed, double* eb, double sealevel, double cda,
               double cdm, double dt, double rtol, int max_iter, gs_stats* st);
 int apply_forces(gs_plan* p, double* h, const double* rain, const double* upsub, double dt,

@@ -1,0 +1,432 @@
+// Continental sediment routing and deposition in depressions: goSPL's
+// SEDMesh.sedChange (gospl/sed/sedplex.py:1061-1086) for one landscape with a
+// single lithology and no provenance tracers.
+//
+//   1. _getSedFlux (sedplex.py:103-188): vSed = (I - W^T)^-1 (-Eb * area) over
+//      the snapshot receivers of the preceding flow accumulation (fMati), one
+//      ordered flow sweep.
+//   2. fillElevation(sed=True): depressions of the eroded surface filled with
+//      sediment (marine depressions included, pits labelled above the fill
+//      level, volumes of the unclipped surface).
+//   3. _distributeSediment / _moveDownstream (sedplex.py:190-522): per pass,
+//      the sediment volume reaching each depression through its sink cells;
+//      depressions that overflow are filled to their spill level (sedFilled),
+//      their excess leaves through the spill node, the flow graph is rebuilt
+//      on sedFilled (pit-flat routing, down=True) when a depression filled,
+//      and the excess is routed downstream by an ordered flow sweep; flux on
+//      cells not under a filled lake adds to vSed.  Terminal cells that are
+//      not a depression keep their sediment on closed domains.
+//   4. _updateSinks (sedplex.py:982-1059) paths 1 and 2: each depression that
+//      received sediment gets a horizontal deposit surface at the level whose
+//      filled volume matches the deposit (np.interp over its five-level
+//      depth-volume table, restated below), tilted by 1e-6 m/m towards its
+//      spill point (_addPitMicroTilt, sedplex.py:561-644).  Path 3 (partly
+//      filled depressions of at least nlPitVolume and nlPitDepth, smoothed by
+//      non-linear diffusion) is reported as an error.
+#include <string>
+
+#include "gs_plan.cuh"
+
+namespace gs {
+
+namespace {
+
+enum { S_POS = 1, S_BIG = 4 };
+
+__global__ void k_sed_rhs(int n, const double* __restrict__ eb, const double* __restrict__ larea, double* b) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) b[i] = (-eb[i]) * larea[i];
+}
+
+__global__ void k_sed_init(int n, const double* __restrict__ vsed, const double* __restrict__ h, double dt,
+                           double* vol, double* hl, double* sfill, double* closed) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    vol[i] = vsed[i] * dt;
+    hl[i] = h[i];
+    sfill[i] = h[i];
+    closed[i] = 0.0;
+}
+
+__global__ void k_sed_pitvol(int np1, const double* __restrict__ params, double* vol) {
+    int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p < np1) vol[p] = params[3 * p];
+}
+
+// flow-terminal cells that are no depression: their sediment leaves the
+// routed flux (kept in place on a closed domain)
+__global__ void k_sed_csink(int n, const uint8_t* __restrict__ lsink, const int* __restrict__ pit, int keep,
+                            double* vol, double* closed) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n || !lsink[i] || pit[i] >= 0) return;
+    if (keep) closed[i] = closed[i] + vol[i];
+    vol[i] = 0.0;
+}
+
+__global__ void k_fill_int_s(int n, int* a, int v) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) a[i] = v;
+}
+
+// per-pit decisions of one _moveDownstream pass (sedplex.py:290-330)
+__global__ void k_sed_pits(int np1, const double* __restrict__ inV, double* vol, const int* __restrict__ info,
+                           double* ev, uint8_t* state, int* win, int* flags) {
+    int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= np1) return;
+    const double in = inV[p];
+    const double e = in - vol[p];
+    ev[p] = e;
+    uint8_t s = 0;
+    int f = 0;
+    if (e > 0.0) {
+        f |= S_POS;
+        s = 1;
+        vol[p] = 0.0;
+        // nvSed[spill] = eV: with a spill node shared by several pits the
+        // highest pit id is written last
+        if (info[2 * p + 1] == 0) atomicMax(&win[info[2 * p]], p);
+    }
+    if (e < 0.0) {
+        double v = vol[p] - in;
+        vol[p] = v < 0.0 ? 0.0 : v;
+    }
+    if (e > 1.0e-3) f |= S_BIG;
+    state[p] = s;
+    if (f) atomicOr(flags, f);
+}
+
+__global__ void k_sed_spill(int np1, const double* __restrict__ ev, const uint8_t* __restrict__ state,
+                            const int* __restrict__ info, const int* __restrict__ win, double* nv) {
+    int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= np1) return;
+    if (state[p] == 1 && info[2 * p + 1] == 0 && win[info[2 * p]] == p) nv[info[2 * p]] = ev[p];
+}
+
+__global__ void k_sed_cells(int n, const int* __restrict__ pit, const uint8_t* __restrict__ state,
+                            const double* __restrict__ lfill, double* sfill) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int p = pit[i];
+    if (p >= 0 && state[p] == 1) sfill[i] = lfill[i];
+}
+
+// routed excess: next pass's volumes, and the flux outside filled lakes added
+// to vSed (sedplex.py:443-451)
+__global__ void k_sed_accum(int n, const double* __restrict__ routed, const double* __restrict__ hl,
+                            const double* __restrict__ sfill, const uint8_t* __restrict__ outlet, double dt,
+                            double* vol, double* vsed) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double v = routed[i];
+    const double keep = (hl[i] < sfill[i]) ? 0.0 : v;
+    vsed[i] = vsed[i] + keep / dt;
+    vol[i] = outlet[i] ? 0.0 : v;
+}
+
+// np.interp(x, xp, fp) for one scalar x and six increasing abscissae, as
+// numpy's arr_interp evaluates it: outside the range the end values, at an
+// abscissa its value, else slope * (x - xp[j]) + fp[j] with j the last
+// abscissa <= x.
+__device__ double interp6(double x, const double* xp, const double* fp) {
+    if (x > xp[5]) return fp[5];
+    if (x < xp[0]) return fp[0];
+    int j = 0;
+    for (int k = 1; k < 6; k++)
+        if (xp[k] <= x) j = k;
+    if (j == 5) return fp[5];
+    if (xp[j] == x) return fp[j];
+    const double slope = __ddiv_rn(__dsub_rn(fp[j + 1], fp[j]), __dsub_rn(xp[j + 1], xp[j]));
+    double r = __dadd_rn(__dmul_rn(slope, __dsub_rn(x, xp[j])), fp[j]);
+    if (r != r) {
+        r = __dadd_rn(__dmul_rn(slope, __dsub_rn(x, xp[j + 1])), fp[j + 1]);
+        if (r != r && fp[j] == fp[j + 1]) r = fp[j];
+    }
+    return r;
+}
+
+// _updateSinks path selection and _bottomUpDelta's lake level per pit
+// (sedplex.py:524-559, 1000-1014)
+__global__ void k_sed_depo(int np1, const double* __restrict__ params, const double* __restrict__ vol,
+                           const double* __restrict__ fvol, const double* __restrict__ flvl, double nlv,
+                           double nld, uint8_t* sel, double* target, int* ndiffuse) {
+    int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= np1) return;
+    const double pv = params[3 * p], pd = params[3 * p + 2];
+    double depo = pv - vol[p];
+    if (depo < 0.0) depo = 0.0;
+    const bool active = depo > 0.0;
+    const bool full = active && depo >= pv - 1.0e-6;
+    const bool partial = active && !full;
+    const bool large = pv >= nlv && pd >= nld;
+    if (partial && large) atomicAdd(ndiffuse, 1);
+    const bool bottomup = full || (partial && !large);
+    sel[p] = bottomup ? 1 : 0;
+    double t = -INFINITY;
+    if (bottomup && depo > 0.0) {
+        double xp[6], fp[6];
+        xp[0] = 0.0;
+        fp[0] = params[3 * p + 1] - params[3 * p + 2];
+        for (int k = 0; k < 5; k++) {
+            xp[k + 1] = fvol[5 * p + k];
+            fp[k + 1] = flvl[5 * p + k];
+        }
+        t = interp6(depo, xp, fp);
+    }
+    target[p] = t;
+}
+
+__global__ void k_sed_closed(int n, const double* __restrict__ closed, const double* __restrict__ larea, double* h,
+                             double* cum) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double c = closed[i];
+    if (c > 0.0) {
+        const double d = c / larea[i];
+        cum[i] = cum[i] + d;
+        h[i] = h[i] + d;
+    }
+}
+
+// bottom-up deposit, and for the micro-tilt the distance of every deposit
+// cell to its pit's spill point (sedplex.py:550-556, 601-608)
+__global__ void k_sed_delta(int n, const int* __restrict__ pit, const uint8_t* __restrict__ sel,
+                            const double* __restrict__ target, const double* __restrict__ lfill,
+                            const double* __restrict__ hl, const double* __restrict__ xyz,
+                            const int* __restrict__ info, double* delta, double* dist, uint8_t* tmask) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int p = pit[i];
+    double d = 0.0;
+    if (p >= 0 && sel[p]) {
+        const double t = target[p], f = lfill[i];
+        const double surf = t < f ? t : f;
+        const double v = __dsub_rn(surf, hl[i]);
+        d = v > 0.0 ? v : 0.0;
+    }
+    delta[i] = d;
+    const bool m = p >= 0 && sel[p] && d > 0.0;
+    tmask[i] = m ? 1 : 0;
+    double ds = 0.0;
+    if (m) {
+        double sx = 0.0, sy = 0.0, sz = 0.0;
+        const int sp = info[2 * p];
+        if (info[2 * p + 1] == 0 && sp >= 0) {
+            sx = xyz[3 * (size_t)sp];
+            sy = xyz[3 * (size_t)sp + 1];
+            sz = xyz[3 * (size_t)sp + 2];
+        }
+        const double dx = __dsub_rn(xyz[3 * (size_t)i], sx);
+        const double dy = __dsub_rn(xyz[3 * (size_t)i + 1], sy);
+        const double dz = __dsub_rn(xyz[3 * (size_t)i + 2], sz);
+        ds = sqrt(__dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz)));
+    }
+    dist[i] = ds;
+}
+
+__global__ void k_sed_ones(int n, double* a) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) a[i] = 1.0;
+}
+
+// tilt towards the spill with the per-pit mean distance removed, then the
+// deposit joins h and cumED (sedplex.py:620-644, 1038-1043)
+__global__ void k_sed_apply(int n, const int* __restrict__ pit, const uint8_t* __restrict__ tmask,
+                            const double* __restrict__ dist, const double* __restrict__ dsum,
+                            const double* __restrict__ dcnt, int tilt, const double* __restrict__ delta, double* h,
+                            double* cum) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double d = delta[i];
+    if (tilt && tmask[i]) {
+        const int p = pit[i];
+        const double c = dcnt[p];
+        const double mean = c > 0.0 ? dsum[p] / (c > 1.0 ? c : 1.0) : 0.0;
+        const double t = __dmul_rn(1.0e-6, __dsub_rn(dist[i], mean));
+        d = __dadd_rn(d, t);
+        if (d < 0.0) d = 0.0;
+    }
+    cum[i] = cum[i] + d;
+    h[i] = h[i] + d;
+}
+
+__global__ void k_sed_pitfinal(int np1, const double* __restrict__ vol, double* params) {
+    int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p < np1) params[3 * p] = vol[p];
+}
+
+__global__ void k_sed_sum_part(int n, const double* __restrict__ x, double* part) {
+    __shared__ double sh[256];
+    double acc = 0.0;
+    const int per = (n + gridDim.x - 1) / gridDim.x;
+    const int lo = blockIdx.x * per, hi = lo + per < n ? lo + per : n;
+    for (int i = lo + threadIdx.x; i < hi; i += blockDim.x) acc += x[i];
+    sh[threadIdx.x] = acc;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s) sh[threadIdx.x] += sh[threadIdx.x + s];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) part[blockIdx.x] = sh[0];
+}
+
+__global__ void k_sed_sum_final(int parts, const double* __restrict__ part, double* out) {
+    __shared__ double sh[512];
+    double acc = 0.0;
+    for (int i = threadIdx.x; i < parts; i += blockDim.x) acc += part[i];
+    sh[threadIdx.x] = acc;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s) sh[threadIdx.x] += sh[threadIdx.x + s];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *out = sh[0];
+}
+
+}  // namespace
+
+int sed_change(gs_plan* p, double* h, double* cum_ed, const double* eb, const double* xyz, double sealevel,
+               double ofill, double dt, double nl_pit_volume, double nl_pit_depth, double* lfill, int* pit_ids,
+               int* flat_dirs, const int* rcv_i, const double* wgt_i, uint8_t* lsink, const uint8_t* sea,
+               double* vsed, gs_stats* st) {
+    const int n = (int)p->n;
+    if (n == 0) return GS_OK;
+    if (p->nmem > 1) {
+        set_error(GS_EINVAL, "sedChange: sediment routing of ensemble members is not built");
+        return GS_EINVAL;
+    }
+    const int B = 256, G = grid_for(n, B);
+    if (!p->sed_buf) GS_CUDA(cudaMalloc((void**)&p->sed_buf, sizeof(double) * (size_t)n * 8));
+    if (!p->sed_mask) GS_CUDA(cudaMalloc((void**)&p->sed_mask, (size_t)n * 2));
+    double* vol = p->sed_buf;
+    double* nv = vol + n;
+    double* routed = nv + n;
+    double* closed = routed + n;
+    double* hl = closed + n;
+    double* sfill = hl + n;
+    double* delta = sfill + n;
+    double* dist = delta + n;
+    uint8_t* sea_s = p->sed_mask;
+    uint8_t* tmask = sea_s + n;
+    const int keep_closed = p->n_outlet > 0 ? 0 : 1;   // sedplex.py:45-47
+
+    // 1. sediment flux over the snapshot graph of the last flow accumulation
+    int cyc = 0, total_cycles = 0;
+    launch(p, k_sed_rhs, G, B, n, eb, (const double*)p->larea, p->q2);
+    GS_LAUNCH();
+    GS_TRY(flow_prepare(p, rcv_i, wgt_i, p->rslot_i, vsed, p->order_i, p->h_pinned + 3));
+    GS_TRY(flow_run(p, rcv_i, wgt_i, p->rslot_i, p->q2, vsed, &cyc, p->order_i, p->order_i_valid));
+    total_cycles += cyc;
+    // lsinki: sinks of the snapshot graph (flowplex.py:785-791)
+    GS_TRY(sink_mask(p, wgt_i, sea, lsink));
+    launch(p, k_sed_init, G, B, n, (const double*)vsed, (const double*)h, dt, vol, hl, sfill, closed);
+    GS_LAUNCH();
+
+    // 2. depressions of the eroded surface, filled with sediment
+    GS_TRY(fill_elevation(p, h, sealevel, ofill, lfill, pit_ids, flat_dirs, st, true, nullptr, true));
+    const int P = p->npits, np1 = P + 1;
+    launch(p, k_sed_pitvol, grid_for(np1, B), B, np1, (const double*)p->pit_params, p->pit_vol);
+    GS_LAUNCH();
+
+    // 3. cascade over the depressions
+    int* flags = p->i_scalar + 10;
+    int step = 0, solves = 0;
+    bool excess = true;
+    while (excess) {
+        if (step >= 5000) break;
+        excess = false;
+        launch(p, k_sed_csink, G, B, n, (const uint8_t*)lsink, (const int*)pit_ids, keep_closed, vol, closed);
+        GS_LAUNCH();
+        GS_TRY(group_sum_by_pit(p, pit_ids, lsink, vol, p->pit_in, P));
+        GS_CUDA(cudaMemsetAsync(flags, 0, sizeof(int), p->stream));
+        launch(p, k_fill_int_s, G, B, n, p->pit_win, -1);
+        launch(p, k_sed_pits, grid_for(np1, B), B, np1, (const double*)p->pit_in, p->pit_vol,
+               (const int*)p->pit_info, p->pit_ev, p->pit_state, p->pit_win, flags);
+        GS_LAUNCH();
+        int f = 0;
+        GS_CUDA(cudaMemcpyAsync(&f, flags, sizeof(int), cudaMemcpyDeviceToHost, p->stream));
+        GS_CUDA(cudaStreamSynchronize(p->stream));
+        GS_CUDA(cudaMemsetAsync(nv, 0, sizeof(double) * n, p->stream));
+        const bool changed = (f & S_POS) != 0;
+        if (changed) {
+            launch(p, k_sed_spill, grid_for(np1, B), B, np1, (const double*)p->pit_ev, (const uint8_t*)p->pit_state,
+                   (const int*)p->pit_info, (const int*)p->pit_win, nv);
+            launch(p, k_sed_cells, G, B, n, (const int*)pit_ids, (const uint8_t*)p->pit_state, (const double*)lfill,
+                   sfill);
+            GS_LAUNCH();
+        }
+        if (f & S_BIG) {
+            if (changed || step == 0 || step == 100) {
+                // flow graph of the sediment-filled surface (down=True)
+                const double* surf = (step == 100) ? lfill : sfill;
+                GS_TRY(receivers(p, p->R, 1.1, surf, sealevel, p->gid, p->rcv, p->dist, p->wgt, p->rslot));
+                GS_TRY(flow_order_from(p, surf, hl, p->order_i, p->order));
+                GS_TRY(flow_order_ties_prepare(p));
+                GS_TRY(fill_join(p, st));
+                GS_TRY(flow_direction_post(p, surf, true, lfill, pit_ids, flat_dirs, sealevel, p->rcv, p->dist,
+                                           p->wgt, p->rslot, lsink, sea_s));
+                GS_TRY(flow_order_ties(p, p->pdir, p->order));
+            }
+            const int PARTS = 256;
+            launch(p, k_sed_sum_part, PARTS, 256, n, (const double*)nv, p->red);
+            launch(p, k_sed_sum_final, 1, 512, PARTS, (const double*)p->red, p->red + 4200);
+            GS_LAUNCH();
+            double total = 0.0;
+            GS_CUDA(cudaMemcpyAsync(&total, p->red + 4200, sizeof(double), cudaMemcpyDeviceToHost, p->stream));
+            GS_CUDA(cudaStreamSynchronize(p->stream));
+            if (total > 0.5 * p->maxarea) {
+                excess = true;
+                GS_TRY(flow_prepare(p, p->rcv, p->wgt, p->rslot, routed, p->order, p->h_pinned));
+                GS_CUDA(cudaStreamSynchronize(p->stream));
+                const int ok = p->h_pinned[0] ? 0 : 1;
+                GS_TRY(flow_run(p, p->rcv, p->wgt, p->rslot, nv, routed, &cyc, p->order, ok));
+                total_cycles += cyc;
+                launch(p, k_sed_accum, G, B, n, (const double*)routed, (const double*)hl, (const double*)sfill,
+                       (const uint8_t*)p->outlet, dt, vol, vsed);
+                GS_LAUNCH();
+                solves++;
+            }
+        }
+        step++;
+    }
+    GS_TRY(fill_join(p, st));
+
+    // 4. deposits in the depressions
+    GS_CUDA(cudaMemsetAsync(p->i_scalar + 11, 0, sizeof(int), p->stream));
+    launch(p, k_sed_depo, grid_for(np1, B), B, np1, (const double*)p->pit_params, (const double*)p->pit_vol,
+           (const double*)p->filled_vol, (const double*)p->filled_lvl, nl_pit_volume, nl_pit_depth, p->pit_state,
+           p->pit_lvl, p->i_scalar + 11);
+    GS_LAUNCH();
+    int ndiff = 0;
+    GS_CUDA(cudaMemcpyAsync(&ndiff, p->i_scalar + 11, sizeof(int), cudaMemcpyDeviceToHost, p->stream));
+    GS_CUDA(cudaStreamSynchronize(p->stream));
+    if (st) {
+        st->npits = P;
+        st->cascade_passes = step;
+        st->cascade_solves = solves;
+        st->cycle_nodes = total_cycles;
+        st->status = ndiff;
+    }
+    if (ndiff > 0) {
+        set_error(GS_EINVAL, "sedChange: " + std::to_string(ndiff) +
+                                 " partly filled depressions reach nlPitVolume and nlPitDepth (deposit smoothed "
+                                 "by non-linear diffusion), which is not built");
+        return GS_EINVAL;
+    }
+    if (keep_closed) {
+        launch(p, k_sed_closed, G, B, n, (const double*)closed, (const double*)p->larea, h, cum_ed);
+        GS_LAUNCH();
+    }
+    launch(p, k_sed_delta, G, B, n, (const int*)pit_ids, (const uint8_t*)p->pit_state, (const double*)p->pit_lvl,
+           (const double*)lfill, (const double*)hl, xyz, (const int*)p->pit_info, delta, dist, tmask);
+    launch(p, k_sed_ones, G, B, n, routed);
+    GS_LAUNCH();
+    GS_TRY(group_sum_by_pit(p, pit_ids, tmask, dist, p->pit_in, P));
+    GS_TRY(group_sum_by_pit(p, pit_ids, tmask, routed, p->pit_ev, P));
+    launch(p, k_sed_apply, G, B, n, (const int*)pit_ids, (const uint8_t*)tmask, (const double*)dist,
+           (const double*)p->pit_in, (const double*)p->pit_ev, 1, (const double*)delta, h, cum_ed);
+    launch(p, k_sed_pitfinal, grid_for(np1, B), B, np1, (const double*)p->pit_vol, p->pit_params);
+    GS_LAUNCH();
+    return GS_OK;
+}
+
+}  // namespace gs

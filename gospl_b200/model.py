@@ -7,10 +7,13 @@
 * ``fillElevation(sed)``  — PITFill.fillElevation (pitfilling.py:849-903)
 * ``_buildFlowDirection(h, down)`` — flowplex.py:480-544
 * ``erodepSPL()``         — SPL.erodepSPL (SPL.py:402-454), n = 1, G >= 0
+* ``sedChange()``         — SEDMesh.sedChange (sedplex.py:1061-1086):
+  continental sediment routing and deposition in depressions
 * ``getHillslope()``      — hillSLP.getHillslope (hillslope.py:614-649)
 * ``applyForces()``       — UnstMesh.applyForces (unstructuredmesh.py:743-794)
 * ``runProcesses()``      — the time loop of model.py:331-466 with
-  ``fast: false, nodep: true``.
+  ``fast: false`` and continental deposition unless ``nodep`` (marine
+  deposition, ``seadepo``, is not built).
 
 All state lives in torch CUDA tensors (float64 / int32 / uint8); every stage is
 one call through the C ABI of ``libgospl_b200.so``.  Per-receiver arrays are
@@ -43,7 +46,9 @@ class Model:
     read by inputparser.py for this path) or from arrays
     (``Model(coords=..., cells=..., elev=..., params=...)``).  ``params`` keys:
     dt, tStart, tEnd, flowDir, K (scalar or per-vertex), d, m, G, Cda, Cdm, oFill,
-    sealevel, bc, rain (per-vertex m/yr), upsub (per-vertex m/yr or None).
+    sealevel, bc, rain (per-vertex m/yr), upsub (per-vertex m/yr or None),
+    nodep (default True: no continental deposition), nlPitVolume (1e9 m3) and
+    nlPitDepth (100 m).
     ``members`` = (start, maxarea) declares the mesh a disjoint union of
     landscapes (``gospl_b200.ensemble``).  ``precision=32`` selects the FP32
     sweeps and CG with FP64 refinement to ``refine_tol``.
@@ -83,6 +88,11 @@ class Model:
         self.oFill = float(p.get("oFill", -6000.0))
         self.sealevel = float(p.get("sealevel", 0.0))
         self.flatModel = bool(mesh.flat)
+        self.nodep = bool(p.get("nodep", True))
+        if not self.nodep and bool(p.get("seadepo", False)):
+            raise NotImplementedError("marine deposition (seaChange, seadepo) is not built")
+        self.nl_pit_volume = float(p.get("nlPitVolume", 1.0e9))    # inputparser.py:562,584
+        self.nl_pit_depth = float(p.get("nlPitDepth", 100.0))      # inputparser.py:563,585
         self.cg_rtol = cg_rtol
         self.cg_maxit = cg_maxit
         self.stats = {}
@@ -117,6 +127,15 @@ class Model:
         self.wgt_i = torch.zeros((R, n), **f64)
         self.lsink_mask = torch.zeros(n, **u8)
         self.sea_mask = torch.zeros(n, **u8)
+        self.vSed = torch.zeros(n, **f64)
+        self.xyz = None
+        if not self.nodep:
+            if coords is None:
+                raise ValueError("continental deposition needs the vertex coordinates")
+            xyz = np.zeros((n, 3))
+            c = np.asarray(coords, np.float64)
+            xyz[:, :c.shape[1]] = c
+            self.xyz = torch.as_tensor(xyz, **f64)
 
         handle = ctypes.c_void_p()
         outlet = np.ascontiguousarray(mesh.outlet, np.int32)
@@ -187,9 +206,10 @@ class Model:
         self.rainVal = self.rainMesh.clamp(min=0.0)   # unstructuredmesh.py:960
 
     def fillElevation(self, sed=False):
-        """pitfilling.py:849-903; per-pit tables read with pit_tables()."""
+        """pitfilling.py:849-903; per-pit tables read with pit_tables().  The
+        sediment fill (sed=True) runs inside sedChange."""
         if sed:
-            raise NotImplementedError("fillElevation(sed=True) belongs to sediment routing, not this path")
+            raise NotImplementedError("fillElevation(sed=True) runs inside sedChange()")
         L = _lib_handle()
         npits = ctypes.c_int32()
         _lib.check(L.gs_fill_elevation(self._plan, _lib.ptr(self.hGlobal), self.sealevel, self.oFill,
@@ -241,6 +261,23 @@ class Model:
             _lib.ptr(self.lsink_mask), _lib.ptr(self.sea_mask), ctypes.byref(st)))
         self.stats["spl"] = st.as_dict()
 
+    def sedChange(self):
+        """SEDMesh.sedChange (sedplex.py:1061-1086): sediment flux over the
+        snapshot receivers of the last flowAccumulation, depressions filled
+        with sediment, the cascade of overflowing depressions and the lake
+        deposits.  vSed holds the routed sediment flux (m3/yr)."""
+        if self.xyz is None:
+            raise RuntimeError("sedChange needs a Model built with nodep=False")
+        L = _lib_handle()
+        st = _lib.GsStats()
+        _lib.check(L.gs_sed_change(
+            self._plan, _lib.ptr(self.hGlobal), _lib.ptr(self.cumED), _lib.ptr(self.EbLocal), _lib.ptr(self.xyz),
+            self.sealevel, self.oFill, self.dt, self.nl_pit_volume, self.nl_pit_depth, _lib.ptr(self.lFill),
+            _lib.ptr(self.pitIDs), _lib.ptr(self.flatDirs), _lib.ptr(self.rcv_i), _lib.ptr(self.wgt_i),
+            _lib.ptr(self.lsink_mask), _lib.ptr(self.sea_mask), _lib.ptr(self.vSed), ctypes.byref(st)))
+        self.npits = st.npits
+        self.stats["sed"] = st.as_dict()
+
     def getHillslope(self):
         L = _lib_handle()
         st = _lib.GsStats()
@@ -250,9 +287,14 @@ class Model:
         self.stats["hillslope"] = st.as_dict()
 
     def step(self):
-        """One physics step of runProcesses (model.py:347-453, fast=False, nodep=True)."""
+        """One physics step of runProcesses (model.py:347-453, fast=False):
+        flow, erosion, continental deposition unless nodep (flow again, then
+        sedChange), hillslope, forcing."""
         self.flowAccumulation()
         self.erodepSPL()
+        if not self.nodep:
+            self.flowAccumulation()
+            self.sedChange()
         self.getHillslope()
         if self.tNow < self.tEnd:
             self.applyForces()
@@ -267,6 +309,8 @@ class Model:
     # ------------------------------------------------------------- adjoint
     def record(self, nslots):
         """Allocate `nslots` per-step records for the adjoint (0 frees them)."""
+        if nslots and not self.nodep:
+            raise NotImplementedError("the adjoint covers steps without continental deposition (nodep)")
         _lib.check(_lib_handle().gs_plan_record(self._plan, int(nslots)))
 
     def record_slot(self, slot):

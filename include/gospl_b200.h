@@ -204,6 +204,30 @@ int gs_erodep_spl(gs_plan* plan, double* h, double* cum_ed, double* eb, const do
  * with Jacobi-preconditioned CG to relative residual `rtol`.  Updates h and
  * cum_ed in place and adds dz/dt to eb.
  */
+/*
+ * Continental sediment routing and deposition in depressions:
+ * SEDMesh.sedChange (gospl/sed/sedplex.py:1061-1086) with _getSedFlux
+ * (103-188), fillElevation(sed=True) (flow/pitfilling.py:849-903),
+ * _distributeSediment / _moveDownstream (190-522) and _updateSinks (982-1059)
+ * for one landscape, one lithology, no provenance.  Call it right after
+ * gs_flow_accumulation on the same h (goSPL's runProcesses with nodep=False
+ * runs flowAccumulation, then sedChange): rcv_i / wgt_i are that call's
+ * snapshot receivers and sea its sea mask.  xyz holds the vertex coordinates
+ * [nb][3] (the micro-tilt of lake deposits).  Updates h and cum_ed, writes
+ * vsed (routed sediment flux, m3/yr), the sediment fill (lfill, pit_ids,
+ * flat_dirs and the plan's pit tables, with pitParams volumes left to the
+ * unfilled remainder) and lsink.  Partly filled depressions of at least
+ * nl_pit_volume (m3) and nl_pit_depth (m), whose deposit goSPL smooths by
+ * non-linear diffusion, return GS_EINVAL (stats.status = their count);
+ * ensembles (gs_plan_set_members) return GS_EINVAL.  stats: npits, cascade
+ * passes and solves.
+ */
+int gs_sed_change(gs_plan* plan, double* h, double* cum_ed, const double* eb, const double* xyz,
+                  double sealevel, double ofill, double dt, double nl_pit_volume, double nl_pit_depth,
+                  double* lfill, int32_t* pit_ids, int32_t* flat_dirs, const int32_t* rcv_i,
+                  const double* wgt_i, uint8_t* lsink, const uint8_t* sea, double* vsed,
+                  gs_stats* stats);
+
 int gs_hillslope(gs_plan* plan, double* h, double* cum_ed, double* eb, double sealevel,
                  double cda, double cdm, double dt, double rtol, int32_t max_iter,
                  gs_stats* stats);

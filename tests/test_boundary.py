@@ -32,6 +32,25 @@ def test_exports_every_declared_symbol():
     assert set(names) == set(_lib.EXPORTS)
 
 
+def test_every_export_has_argument_types():
+    """ctypes cannot pass Python floats without declared argument types: every
+    entry point with arguments declares them."""
+    from gospl_b200 import _lib
+    L = _lib.load()
+    for name in _lib.EXPORTS:
+        if name in ("gs_version",):
+            continue
+        assert getattr(L, name).argtypes is not None, name
+
+
+def test_sed_change_rejects_null_plan():
+    from gospl_b200 import _lib
+    L = _lib.load()
+    st = _lib.GsStats()
+    assert L.gs_sed_change(None, None, None, None, None, 0.0, -6000.0, 1.0, 1e9, 100.0, None, None, None, None,
+                           None, None, None, None, ctypes.byref(st)) == 1
+
+
 def test_stats_struct_layout():
     from gospl_b200 import _lib
     assert ctypes.sizeof(_lib.GsStats) == 8 * 4 + 8

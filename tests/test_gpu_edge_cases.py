@@ -30,6 +30,11 @@ def _step_vs_oracle(coords, cells, z, params):
     assert np.abs(fal - om.FAL).max() <= 1e-10 * max(np.abs(om.FAL).max(), 1.0), "drainage area"
     h = gm.hGlobal.cpu().numpy()
     assert np.abs(h - om.h).max() <= 1e-10 * max(np.abs(om.h).max(), 1.0), "elevation"
+    if not params.get("nodep", True):
+        vs = gm.vSed.cpu().numpy()
+        assert np.abs(vs - om.vSed).max() <= 1e-10 * max(np.abs(om.vSed).max(), 1.0), "sediment flux"
+        cum = gm.cumED.cpu().numpy()
+        assert np.abs(cum - om.cumED).max() <= 1e-10 * max(np.abs(om.h).max(), 1.0), "cumED"
     gm.destroy()
 
 
@@ -86,3 +91,31 @@ def test_transport_limited_spl(G):
     coords, cells, z, params = _planar(3000, 29, "ffff")
     params = dict(params, G=G)
     _step_vs_oracle(coords, cells, z, params)
+
+
+@pytest.mark.parametrize("bc", ["ffff", "wwww", "wfwf"])
+def test_continental_deposition(bc):
+    """sedChange (sedplex.py:1061-1086) over open, closed (no outlet: stray
+    sinks keep their sediment) and mixed boundaries, one step against the
+    oracle."""
+    coords, cells, z, params = _planar(3000, 31, bc)
+    params = dict(params, nodep=False)
+    _step_vs_oracle(coords, cells, z, params)
+
+
+def test_lake_diffusion_path_rejected():
+    """Partly filled depressions of at least nlPitVolume and nlPitDepth are
+    smoothed by non-linear diffusion in goSPL (sedplex.py:679-858); that path
+    is not built and must fail loudly, not deposit something else."""
+    import torch
+    from gospl_b200 import _lib
+    from gospl_b200.mesh import FVMesh
+    from gospl_b200.model import Model
+    coords, cells, z, params = _planar(3000, 31, "ffff")
+    params = dict(params, nodep=False, nlPitVolume=0.0, nlPitDepth=0.0)
+    fv = FVMesh(coords, cells, params["bc"])
+    gm = Model(coords=coords, cells=cells, elev=z, params=params, mesh=fv, device="cuda:0")
+    with pytest.raises(_lib.GsError, match="not built"):
+        gm.step()
+    torch.cuda.synchronize()
+    gm.destroy()

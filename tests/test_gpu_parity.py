@@ -18,7 +18,7 @@ must agree to 1e-10 relative.
 import numpy as np
 import pytest
 
-from conftest import GOLDEN_CASES, GOLDEN_G_CASES, golden_mesh, golden_params, load_golden
+from conftest import GOLDEN_CASES, GOLDEN_G_CASES, GOLDEN_SED_CASES, golden_mesh, golden_params, load_golden
 
 pytestmark = pytest.mark.gpu
 
@@ -196,4 +196,87 @@ def test_transport_limited_matches_reference_golden(case):
         assert _rel(gm.hGlobal, g[t + "h"]) <= 1e-11, s
         assert np.abs(_np(gm.cumED) - g[t + "cumED"]).max() <= 1e-11 * hs, s
         assert np.abs(_np(gm.EbLocal) - g[t + "EbLocal"]).max() <= 1e-11 * hs / float(params["dt"]), s
+    gm.destroy()
+
+
+def _compare_sed(gm, om, tag):
+    """sedChange outputs: the sediment fill (exact), the routed flux, the
+    deposit (h and cumED to 1e-12 of the elevation scale)."""
+    import torch
+    torch.cuda.synchronize()
+    for k in ("pitIDs", "flatDirs", "lsink"):
+        assert np.array_equal(_np(getattr(gm, k)).astype(np.int64),
+                              np.asarray(getattr(om, k)).astype(np.int64)), "%s %s" % (tag, k)
+    assert np.array_equal(_np(gm.lFill), om.lFill), "%s lFill" % tag
+    pp, pi, fl, fv = gm.pit_tables()
+    assert np.array_equal(_np(pi), om.pitInfo), "%s pitInfo" % tag
+    assert _rel(pp, om.pitParams) <= 1e-12, "%s pitParams %g" % (tag, _rel(pp, om.pitParams))
+    assert _rel(fl, om.filled_lvl) <= 1e-12, "%s filled_lvl" % tag
+    assert _rel(fv, om.filled_vol) <= 1e-12, "%s filled_vol" % tag
+    assert _rel(gm.vSed, om.vSed) <= 1e-12, "%s vSed %g" % (tag, _rel(gm.vSed, om.vSed))
+    hs = float(np.abs(om.h).max())
+    assert np.abs(_np(gm.hGlobal) - om.h).max() <= 1e-12 * hs, "%s h" % tag
+    assert np.abs(_np(gm.cumED) - om.cumED).max() <= 1e-12 * hs, "%s cumED" % tag
+
+
+@pytest.mark.parametrize("case", GOLDEN_SED_CASES)
+def test_sed_stage_parity_from_identical_state(case):
+    """Continental deposition (sedplex.py:1061-1086) from the oracle's exact
+    state: every stage of the step, including the second flow accumulation
+    and sedChange, starts from the oracle's fields."""
+    import torch
+    from oracle.model import OracleModel
+    g = load_golden(case)
+    params = golden_params(g)
+    gm = _gpu_model(g, params)
+    om = OracleModel(g["v"], g["c"], g["z"], params, mesh=golden_mesh(g))
+    for s in range(int(g["nsteps"])):
+        tag = "step%d" % (s + 1)
+        _resync(gm, om)
+        gm.flowAccumulation()
+        om.flowAccumulation()
+        _compare_flow(gm, om, tag + " flow", 1e-12)
+        _resync_flow(gm, om)
+        gm.erodepSPL()
+        om.erodepSPL()
+        torch.cuda.synchronize()
+        _compare_dz(gm, om, tag + " spl")
+        _resync(gm, om)
+        gm.flowAccumulation()
+        om.flowAccumulation()
+        _compare_flow(gm, om, tag + " flow2", 1e-12)
+        _resync_flow(gm, om)
+        gm.sedChange()
+        om.sedChange()
+        _compare_sed(gm, om, tag + " sed")
+        _resync(gm, om)
+        gm.getHillslope()
+        om.getHillslope()
+        torch.cuda.synchronize()
+        _compare_dz(gm, om, tag + " hillslope")
+        _resync(gm, om)
+        gm.applyForces()
+        om.applyForces()
+        torch.cuda.synchronize()
+        assert np.array_equal(_np(gm.hGlobal), om.h), "%s forcing h" % tag
+    gm.destroy()
+
+
+@pytest.mark.parametrize("case", GOLDEN_SED_CASES)
+def test_sed_matches_reference_golden_first_step(case):
+    """One free-running step with continental deposition against the
+    reference's own sedplex.py run (the fixtures)."""
+    import torch
+    g = load_golden(case)
+    params = golden_params(g)
+    gm = _gpu_model(g, params)
+    gm.step()
+    torch.cuda.synchronize()
+    assert np.array_equal(_np(gm.rcvIDi), g["s1_rcvIDi"].astype(np.int32))
+    assert np.array_equal(_np(gm.pitIDs), g["s1_pitIDs"])
+    assert np.array_equal(_np(gm.flatDirs), g["s1_flatDirs"])
+    for k in ("FAL", "fillFAL", "cumED", "waterFilled"):
+        assert _rel(getattr(gm, k), g["s1_" + k]) <= 1e-10, k
+    assert _rel(gm.vSed, g["s1_vSed"]) <= 1e-10
+    assert _rel(gm.hGlobal, g["s1_h"]) <= 1e-10
     gm.destroy()
