@@ -168,7 +168,7 @@ def main():
     ap.add_argument("--cpu-level", type=int, default=7)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--workload", default="sphere", choices=["sphere", "planar", "ensemble", "precision",
-                                                                   "transport"])
+                                                                   "transport", "sediment"])
     ap.add_argument("--members", type=int, default=256)
     ap.add_argument("--loop", action="store_true", help="ensemble: also time the per-member loop")
     ap.add_argument("--adjoint-steps", type=int, default=4, help="sphere: steps of the adjoint timing (0: skip)")
@@ -194,6 +194,9 @@ def main():
         return
     if args.workload == "transport":
         run_transport(args, dev)
+        return
+    if args.workload == "sediment":
+        run_sediment(args, dev)
         return
     pg = None
     if world > 1:
@@ -537,6 +540,66 @@ def run_transport(args, dev, G=1.0):
                           "bicgstab_iterations": out[G]["iters"], "final_relres": out[G]["relres"],
                           "detachment_limited_ms_per_step": out[0.0]["ms"],
                           "detachment_limited_erosion_ms_per_step": out[0.0]["spl_ms"]}}
+    print(json.dumps(line), flush=True)
+
+
+def run_sediment(args, dev):
+    """Continental deposition (nodep off: a second flow accumulation and
+    sedChange per step) against the plain step on the 2.6M-vertex sphere; the
+    same steps from the same state, time per step, time of the deposition
+    stage (second flow accumulation + sedChange) and the sediment cascade's
+    passes.  Lake deposits are all bottom-up (nlPitVolume = inf): the
+    non-linear diffusion of large deep lakes is not built."""
+    import torch
+    from gospl_b200.mesh import FVMesh
+    from gospl_b200.model import Model
+    c, f, z, rain, up, p = sphere_inputs(args.level)
+    p = dict(p, rain=rain, upsub=up, tEnd=1.0e30, nlPitVolume=float("inf"))
+    mesh = FVMesh(c, f, p["bc"], device=dev)
+    stream = torch.cuda.current_stream(dev)
+    out = {}
+    for nodep in (False, True):
+        m = Model(coords=c, cells=f, elev=z, params=dict(p, nodep=nodep), mesh=mesh, device=dev)
+        for _ in range(args.warmup):
+            m.step()
+        torch.cuda.synchronize(dev)
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2 * args.steps + 2)]
+        passes = []
+        ev[0].record(stream)
+        for k in range(args.steps):
+            m.flowAccumulation()
+            m.erodepSPL()
+            ev[2 + 2 * k].record(stream)
+            if not nodep:
+                m.flowAccumulation()
+                m.sedChange()
+                passes.append(m.stats["sed"]["cascade_passes"])
+            ev[3 + 2 * k].record(stream)
+            m.getHillslope()
+            if m.tNow < m.tEnd:
+                m.applyForces()
+            m.tNow += m.dt
+        ev[1].record(stream)
+        torch.cuda.synchronize(dev)
+        sed = sum(ev[2 + 2 * k].elapsed_time(ev[3 + 2 * k]) for k in range(args.steps)) / args.steps
+        out[nodep] = dict(ms=ev[0].elapsed_time(ev[1]) / args.steps, sed_ms=sed, passes=passes,
+                          npits=m.stats.get("sed", {}).get("npits"),
+                          vsed_max=float(m.vSed.max().item()))
+        m.destroy()
+    n = len(z)
+    line = {"metric": "landscape vertex-steps/s with continental deposition @2.6M-vertex sphere",
+            "value": n * 1000.0 / out[False]["ms"], "unit": "vertex-steps/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": out[False]["ms"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded sphere, SH relief)",
+            "config": {"workload": "sphere level %d (%d vertices), full physics step with nodep off: flow, SPL, "
+                                   "flow, sedChange (lake deposits bottom-up), hillslope, forcing"
+                                   % (args.level, n),
+                       "vertices": n, "global_batch": 1, "seq_len": 0, "parallelism": "single"},
+            "sediment": {"ms_per_step": out[False]["ms"],
+                         "deposition_ms_per_step": out[False]["sed_ms"],
+                         "cascade_passes": out[False]["passes"], "sed_pits": out[False]["npits"],
+                         "vsed_max_m3_per_yr": out[False]["vsed_max"],
+                         "nodep_ms_per_step": out[True]["ms"]}}
     print(json.dumps(line), flush=True)
 
 

@@ -5,10 +5,13 @@ uses, with goSPL's names, defaults and errors (gospl/tools/inputparser.py):
 
 * ``domain``: ``npdata: [file, coords_key, cells_key, elev_key]`` (the
   ``.npz`` mesh, :263-266), ``flowdir`` (default 8, :189), ``bc`` (four of
-  ``o f w c``, legacy ``0``/``1`` -> ``o``/``f``, :208-246), ``fast``, ``nodep``;
+  ``o f w c``, legacy ``0``/``1`` -> ``o``/``f``, :208-246), ``fast``, ``nodep``
+  and ``seadepo`` (:289-300; continental deposition runs unless ``nodep``,
+  marine deposition is not implemented and must be switched off);
 * ``time``: ``start``, ``end``, ``dt`` required, ``tout`` (:343-404);
 * ``spl``: ``K``, ``d`` (0), ``m`` (0.5), ``G`` (0) (:454-496);
-* ``diffusion``: ``hillslopeKa``, ``hillslopeKm``, ``oFill`` (-6000) (:498-545);
+* ``diffusion``: ``hillslopeKa``, ``hillslopeKm``, ``oFill`` (-6000) (:498-545),
+  ``nlPitVolume`` (1e9), ``nlPitDepth`` (100) (:546-590);
 * ``sea``: ``position`` (default 0, :710-787);
 * ``climate``: events with ``start`` and ``uniform`` or ``map: [file, key]``
   (:1352-1520);
@@ -20,7 +23,7 @@ then relative to the YAML file.  Keys of other goSPL subsystems (sediment,
 stratigraphy, flexure, ice, orography, output) are ignored; options that would
 change this path's arithmetic and that the library does not implement
 (sea-level curves, time-varying climate or tectonic events, horizontal
-tectonics) raise ``ValueError``.
+tectonics, marine deposition) raise ``ValueError``.
 """
 import os
 
@@ -79,7 +82,11 @@ def read_input(filename):
     elev = np.asarray(mesh[info[3]], np.float64).ravel()
     n = len(coords)
     p = {"flowDir": int(dom.get("flowdir", 8)), "bc": parse_bc(dom.get("bc", "oooo")),
-         "fast": bool(dom.get("fast", False)), "nodep": bool(dom.get("nodep", False))}
+         "fast": bool(dom.get("fast", False)), "nodep": bool(dom.get("nodep", False)),
+         "seadepo": bool(dom.get("seadepo", True))}
+    if not p["nodep"] and p["seadepo"]:
+        raise ValueError("marine deposition (domain.seadepo, seaplex.py) is not implemented by gospl_b200; "
+                         "set domain.seadepo: False (continental deposition only) or domain.nodep: True")
 
     if "time" not in inp:
         raise KeyError("Key time is required in the input file!")
@@ -106,8 +113,11 @@ def read_input(filename):
         p["Cda"] = float(hill["hillslopeKa"])
         p["Cdm"] = float(hill["hillslopeKm"])
         p["oFill"] = float(hill.get("oFill", -6000.0))
+        p["nlPitVolume"] = float(hill.get("nlPitVolume", 1.0e9))
+        p["nlPitDepth"] = float(hill.get("nlPitDepth", 100.0))
     else:
         p["Cda"], p["Cdm"], p["oFill"] = 0.0, 0.0, -6000.0
+        p["nlPitVolume"], p["nlPitDepth"] = 1.0e9, 100.0
 
     sea = inp.get("sea") or {}
     if "curve" in sea:

@@ -10,6 +10,7 @@ domain:
     flowdir: 3
     bc: '0f01'
     nodep: False
+    seadepo: False
 time:
     start: 0.
     end: 300.
@@ -54,6 +55,17 @@ def test_reads_the_path_keys(tmp_path):
     assert (p["K"], p["d"], p["m"]) == (4.0e-6, 0.0, 0.5)
     assert (p["Cda"], p["Cdm"], p["oFill"], p["sealevel"]) == (0.01, 0.2, -6000.0, -100.0)
     assert np.all(p["rain"] == 1.0) and np.allclose(p["upsub"], 1e-3)
+    assert (p["nodep"], p["seadepo"], p["nlPitVolume"], p["nlPitDepth"]) == (False, False, 1.0e9, 100.0)
+
+
+def test_marine_deposition_is_refused(tmp_path):
+    """goSPL's default (nodep False, seadepo True) also runs marine deposition,
+    which this library does not implement: the input must switch it off."""
+    y, _ = _write(tmp_path, YML.replace("    seadepo: False\n", ""))
+    with pytest.raises(ValueError, match="seadepo"):
+        read_input(str(y))
+    y, _ = _write(tmp_path, YML.replace("    nodep: False\n    seadepo: False\n", "    nodep: True\n"))
+    assert read_input(str(y))[3]["nodep"] is True
 
 
 def test_defaults_and_errors(tmp_path):
