@@ -404,6 +404,14 @@ int plan_tune(gs_plan* p, int knob, int value) {
         p->coop_blocks = p->sm_count * value;
         return GS_OK;
     }
+    if (knob == GS_TUNE_SWEEP_NAP) {
+        if (value < 0 || value > 1024) {
+            set_error(GS_EINVAL, "tune: sweep back-off must be in 0..1024 ns");
+            return GS_EINVAL;
+        }
+        p->sweep_nap = (unsigned)value;
+        return GS_OK;
+    }
     set_error(GS_EINVAL, "tune: unknown knob");
     return GS_EINVAL;
 }
@@ -412,6 +420,7 @@ int plan_tuning(const gs_plan* p, int knob) {
     if (knob == GS_TUNE_SWEEP_BLOCKS) return p->sweep_per_sm;
     if (knob == GS_TUNE_COOP_BLOCKS) return p->coop_blocks / std::max(p->sm_count, 1);
     if (knob == GS_TUNE_COOP_BLOCKS + 1) return p->coop_max_per_sm;
+    if (knob == GS_TUNE_SWEEP_NAP) return (int)p->sweep_nap;
     if (knob == GS_TUNE_REFINE_PASSES) return (int)std::min<int64_t>(p->refine_iters, 0x7fffffff);
     return -1;
 }

@@ -18,6 +18,7 @@ struct gs_plan {
     int coop_blocks = 148;               // co-resident 256-thread blocks for cooperative launches
     int coop_max_per_sm = 1;             // occupancy limit of the cooperative kernels
     int sweep_per_sm = 8;                // 128-thread blocks per SM of the ordered sweeps
+    unsigned sweep_nap = 128;            // longest back-off (ns) between polls of the ordered sweeps
     // precision form: FP32 sweeps and CG inside FP64 refinement loops
     int fp32 = 0;
     double fdepa = 0.0;                  // SPL deposition coefficient G (0: detachment-limited)

@@ -701,7 +701,7 @@ struct SplOrd32 {
 
 template <class Op>
 __global__ void __launch_bounds__(128) k_ordered(Op op, int n, const int* __restrict__ order, unsigned* ctr,
-                                                 unsigned long long budget_ns) {
+                                                 unsigned long long budget_ns, unsigned nap_max) {
     const unsigned long long t0 = globaltimer_ns();
     const int lane = threadIdx.x & 31;
     const unsigned full = 0xffffffffu;
@@ -759,8 +759,8 @@ __global__ void __launch_bounds__(128) k_ordered(Op op, int n, const int* __rest
                 }
                 if (__shfl_sync(full, stop, 0)) return;
             }
-            if (nap < 128) nap += 16;
-            __nanosleep(nap);
+            if (nap < nap_max) nap += 16;
+            if (nap) __nanosleep(nap);
         }
     }
 }
@@ -1036,7 +1036,7 @@ int flow_run(gs_plan* p, const int* rcv, const double* wgt, const int8_t* rslot,
     if (p->fp32) return flow_refine32(p, wgt, b, x, order);
     GS_CUDA(cudaMemsetAsync(p->ctr, 0, sizeof(unsigned) * 8, p->stream));
     FlowOrd op{n, p->nbr, p->don_mask, p->don_k, p->sorder, wgt, b, x};
-    launch(p, k_ordered<FlowOrd>, p->sm_count * p->sweep_per_sm, 128, op, n, (const int*)order, p->ctr, SWEEP_BUDGET_NS);
+    launch(p, k_ordered<FlowOrd>, p->sm_count * p->sweep_per_sm, 128, op, n, (const int*)order, p->ctr, SWEEP_BUDGET_NS, p->sweep_nap);
     GS_LAUNCH();
     int st = 0;
     GS_TRY(ordered_status(p, &st));
@@ -1098,7 +1098,7 @@ int spl_sweep(gs_plan* p, const int* rcv, const double* c, const int8_t* rslot, 
     GS_CUDA(cudaMemsetAsync(p->ctr, 0, sizeof(unsigned) * 8, p->stream));
     launch(p, k_fill_sent, grid_for(n, 256), 256, n, s);
     SplOrd op{n, p->R, rcv, c, hold, s};
-    launch(p, k_ordered<SplOrd>, p->sm_count * p->sweep_per_sm, 128, op, n, (const int*)p->order2, p->ctr, SWEEP_BUDGET_NS);
+    launch(p, k_ordered<SplOrd>, p->sm_count * p->sweep_per_sm, 128, op, n, (const int*)p->order2, p->ctr, SWEEP_BUDGET_NS, p->sweep_nap);
     GS_LAUNCH();
     int st = 0;
     GS_TRY(ordered_status(p, &st));
@@ -1117,7 +1117,7 @@ int sweep_flow_adjoint(gs_plan* p, const int* rcv, const double* wgt, const int*
     GS_CUDA(cudaMemsetAsync(p->ctr, 0, sizeof(unsigned) * 8, p->stream));
     launch(p, k_fill_sent, grid_for(n, 256), 256, n, y);
     FlowAdjOrd op{n, p->R, rcv, wgt, g, y};
-    launch(p, k_ordered<FlowAdjOrd>, p->sm_count * p->sweep_per_sm, 128, op, n, (const int*)p->order2, p->ctr, SWEEP_BUDGET_NS);
+    launch(p, k_ordered<FlowAdjOrd>, p->sm_count * p->sweep_per_sm, 128, op, n, (const int*)p->order2, p->ctr, SWEEP_BUDGET_NS, p->sweep_nap);
     GS_LAUNCH();
     int st = 0;
     GS_TRY(ordered_status(p, &st));
@@ -1141,7 +1141,7 @@ int sweep_spl_adjoint(gs_plan* p, const int* rcv, const double* wgt, const int8_
     GS_CUDA(cudaMemsetAsync(p->ctr, 0, sizeof(unsigned) * 8, p->stream));
     launch(p, k_fill_sent, grid_for(n, 256), 256, n, y);
     SplAdjOrd op{n, p->R, p->nbr, p->don_mask, p->don_k, p->sorder, c, g, y};
-    launch(p, k_ordered<SplAdjOrd>, p->sm_count * p->sweep_per_sm, 128, op, n, order, p->ctr, SWEEP_BUDGET_NS);
+    launch(p, k_ordered<SplAdjOrd>, p->sm_count * p->sweep_per_sm, 128, op, n, order, p->ctr, SWEEP_BUDGET_NS, p->sweep_nap);
     GS_LAUNCH();
     int st = 0;
     GS_TRY(ordered_status(p, &st));
@@ -1261,7 +1261,7 @@ int flow_refine32(gs_plan* p, const double* wgt, const double* b, double* x, con
         GS_CUDA(cudaMemsetAsync(p->ctr, 0, sizeof(unsigned) * 8, p->stream));
         launch(p, k_fill_sent32, G, B, n, p->f32a);
         FlowOrd32 op{n, p->nbr, p->don_mask, p->don_k, p->sorder, wgt, (const double*)p->r64, p->f32a};
-        launch(p, k_ordered<FlowOrd32>, p->sm_count * p->sweep_per_sm, 128, op, n, order, p->ctr, SWEEP_BUDGET_NS);
+        launch(p, k_ordered<FlowOrd32>, p->sm_count * p->sweep_per_sm, 128, op, n, order, p->ctr, SWEEP_BUDGET_NS, p->sweep_nap);
         GS_LAUNCH();
         int st = 0;
         GS_TRY(ordered_status(p, &st));
@@ -1298,7 +1298,7 @@ int spl_refine32(gs_plan* p, const int* rcv, const double* c, const double* hold
         GS_CUDA(cudaMemsetAsync(p->ctr, 0, sizeof(unsigned) * 8, p->stream));
         launch(p, k_fill_sent32, G, B, n, p->f32a);
         SplOrd32 op{n, p->R, rcv, c, (const double*)p->r64, p->f32a};
-        launch(p, k_ordered<SplOrd32>, p->sm_count * p->sweep_per_sm, 128, op, n, order2, p->ctr, SWEEP_BUDGET_NS);
+        launch(p, k_ordered<SplOrd32>, p->sm_count * p->sweep_per_sm, 128, op, n, order2, p->ctr, SWEEP_BUDGET_NS, p->sweep_nap);
         GS_LAUNCH();
         int st = 0;
         GS_TRY(ordered_status(p, &st));
@@ -1340,7 +1340,7 @@ int sweep_flow_rhs(gs_plan* p, const double* wgt, const int* order, const double
     GS_CUDA(cudaMemsetAsync(p->ctr, 0, sizeof(unsigned) * 8, p->stream));
     launch(p, k_fill_sent, grid_for(n, 256), 256, n, x);
     FlowOrd op{n, p->nbr, p->don_mask, p->don_k, p->sorder, wgt, b, x};
-    launch(p, k_ordered<FlowOrd>, p->sm_count * p->sweep_per_sm, 128, op, n, order, p->ctr, SWEEP_BUDGET_NS);
+    launch(p, k_ordered<FlowOrd>, p->sm_count * p->sweep_per_sm, 128, op, n, order, p->ctr, SWEEP_BUDGET_NS, p->sweep_nap);
     GS_LAUNCH();
     int st = 0;
     GS_TRY(ordered_status(p, &st));
@@ -1356,7 +1356,7 @@ int sweep_spl_rhs(gs_plan* p, const int* rcv, const double* c, const int* order2
     GS_CUDA(cudaMemsetAsync(p->ctr, 0, sizeof(unsigned) * 8, p->stream));
     launch(p, k_fill_sent, grid_for(n, 256), 256, n, x);
     SplOrd op{n, p->R, rcv, c, rhs, x};
-    launch(p, k_ordered<SplOrd>, p->sm_count * p->sweep_per_sm, 128, op, n, order2, p->ctr, SWEEP_BUDGET_NS);
+    launch(p, k_ordered<SplOrd>, p->sm_count * p->sweep_per_sm, 128, op, n, order2, p->ctr, SWEEP_BUDGET_NS, p->sweep_nap);
     GS_LAUNCH();
     int st = 0;
     GS_TRY(ordered_status(p, &st));
