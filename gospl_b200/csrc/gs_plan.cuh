@@ -22,9 +22,10 @@ struct gs_plan {
     // precision form: FP32 sweeps and CG inside FP64 refinement loops
     int fp32 = 0;
     double fdepa = 0.0;                  // SPL deposition coefficient G (0: detachment-limited)
-    int ed_iters = 0;                    // BiCGSTAB iterations of the last coupled solve
+    int ed_iters = 0;                    // operator applications of the last coupled solve
     double ed_relres = 0.0;              // its final relative residual
     double* ed_buf = nullptr;            // [6][n] coupled-solve scratch
+    double* ed_basis = nullptr;          // GMRES basis [31][n] and reduction scratch
     double* sed_buf = nullptr;           // [8][n] sediment-routing scratch
     uint8_t* sed_mask = nullptr;         // [2][n] sediment-routing masks
     double refine_tol = 1.0e-10;         // max|r| / max|b| of every refined solve

@@ -74,7 +74,7 @@ __global__ void k_copy_d(int n, const double* __restrict__ a, double* b) {
 // gives (I + B) h = a with B = M^-1 diag(f dt / A) W^T (I - W^T)^-1 diag(A / dt)
 // (M = eMat, W^T (I - W^T)^-1 = (I - W^T)^-1 - I) and a = M^-1 hOld + B hOld.
 // B is applied with one flow sweep (donors first) and one SPL sweep
-// (receivers first); the system is solved by BiCGSTAB in FP64 from the
+// (receivers first); the system is solved by restarted GMRES in FP64 from the
 // detachment-limited solution.  f = G A / max(FAL, G A / 0.99), 0 where
 // FAL = 0, at sea and at flat-model outlets, capped at 0.99.
 __global__ void k_fdep(int n, double G, const double* __restrict__ larea, const double* __restrict__ fal,
@@ -138,6 +138,8 @@ __global__ void k_ed_dot_final(int parts, const double* __restrict__ part, doubl
     if (threadIdx.x == 0) *out = sh[0];
 }
 
+constexpr int GMRES_M1 = 31;   // GMRES restart length + 1
+
 struct EdSolve {
     gs_plan* p;
     int n;
@@ -174,6 +176,60 @@ struct EdSolve {
     }
 };
 
+// GMRES kernels: block partial dot products of w with the first k basis
+// vectors, their fixed-order totals, and w -= sum_j h_j V_j
+__global__ void k_mdot_part(int n, int k, const double* __restrict__ V, const double* __restrict__ w,
+                            double* part) {
+    __shared__ double sh[4][256];
+    const int per = (n + gridDim.x - 1) / gridDim.x;
+    const int lo = blockIdx.x * per, hi = lo + per < n ? lo + per : n;
+    for (int jb = 0; jb < k; jb += 4) {
+        double acc[4] = {0.0, 0.0, 0.0, 0.0};
+        for (int i = lo + threadIdx.x; i < hi; i += blockDim.x) {
+            const double wi = w[i];
+#pragma unroll
+            for (int u = 0; u < 4; u++)
+                if (jb + u < k) acc[u] += V[(size_t)(jb + u) * n + i] * wi;
+        }
+#pragma unroll
+        for (int u = 0; u < 4; u++) sh[u][threadIdx.x] = acc[u];
+        __syncthreads();
+        for (int s2 = blockDim.x / 2; s2 > 0; s2 >>= 1) {
+            if (threadIdx.x < s2)
+#pragma unroll
+                for (int u = 0; u < 4; u++) sh[u][threadIdx.x] += sh[u][threadIdx.x + s2];
+            __syncthreads();
+        }
+        if (threadIdx.x < 4 && jb + threadIdx.x < k)
+            part[(size_t)blockIdx.x * GMRES_M1 + jb + threadIdx.x] = sh[threadIdx.x][0];
+        __syncthreads();
+    }
+}
+
+// one block per basis vector: the block partials summed in a fixed order
+__global__ void k_mdot_final(int parts, int k, const double* __restrict__ part, double* out) {
+    __shared__ double sh[256];
+    const int j = blockIdx.x;
+    if (j >= k) return;
+    double acc = 0.0;
+    for (int b = threadIdx.x; b < parts; b += blockDim.x) acc += part[(size_t)b * GMRES_M1 + j];
+    sh[threadIdx.x] = acc;
+    __syncthreads();
+    for (int s2 = blockDim.x / 2; s2 > 0; s2 >>= 1) {
+        if (threadIdx.x < s2) sh[threadIdx.x] += sh[threadIdx.x + s2];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) out[j] = sh[0];
+}
+
+__global__ void k_mupdate(int n, int k, const double* __restrict__ V, const double* __restrict__ h, double* w) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double s = w[i];
+    for (int j = 0; j < k; j++) s -= h[j] * V[(size_t)j * n + i];
+    w[i] = s;
+}
+
 static int coupled_ed(gs_plan* p, const double* hold, const double* fal, const uint8_t* sea, double dt,
                       const int* rcv_i, const double* wgt_i, double* x) {
     const int n = (int)p->n;
@@ -182,14 +238,23 @@ static int coupled_ed(gs_plan* p, const double* hold, const double* fal, const u
         set_error(GS_EINVAL, "transport-limited SPL needs a topological order of the receiver graph");
         return GS_EINVAL;
     }
+    constexpr int M = GMRES_M1 - 1;   // restart length
+    const int PARTS = p->sm_count * 8;
     if (!p->ed_buf) GS_CUDA(cudaMalloc((void**)&p->ed_buf, sizeof(double) * (size_t)std::max(n, 1) * 6));
+    if (!p->ed_basis)
+        GS_CUDA(cudaMalloc((void**)&p->ed_basis,
+                           sizeof(double) * ((size_t)std::max(n, 1) * GMRES_M1 + (size_t)PARTS * GMRES_M1 + 4 * GMRES_M1)));
+    // (PARTS depends only on the SM count, fixed for the plan's device)
     double* f = p->ed_buf;
     double* t1 = f + n;
     double* u = t1 + n;
     double* w = u + n;
     double* y2 = w + n;
     double* a = y2 + n;
-    double *r = p->cg_r, *r0 = p->cg_b, *pp = p->cg_p, *v = p->cg_ap, *sv = p->cg_z, *tv = p->cg_x;
+    double* V = p->ed_basis;
+    double* part = V + (size_t)n * GMRES_M1;
+    double* hd = part + (size_t)PARTS * GMRES_M1;    // [0, M1): pass 1, [M1, 2 M1): pass 2, 2 M1: norm^2
+    double* r = p->cg_r;
     launch(p, k_fdep, G, B, n, p->fdepa, (const double*)p->larea, fal, sea, (const uint8_t*)p->outlet, p->flat, f);
     GS_LAUNCH();
     GS_TRY(build_donors(p, rcv_i, wgt_i, p->rslot_i));
@@ -201,60 +266,89 @@ static int coupled_ed(gs_plan* p, const double* hold, const double* fal, const u
     launch(p, k_ed_axpby, G, B, n, 1.0, (const double*)a, -1.0, hold, a);
     launch(p, k_ed_axpby, G, B, n, 1.0, (const double*)a, 1.0, (const double*)x, a);
     GS_LAUNCH();
-    // BiCGSTAB on (I + B) x = a
-    GS_TRY(op.apply(x, v));
-    launch(p, k_ed_axpby, G, B, n, 1.0, (const double*)a, -1.0, (const double*)v, r);
-    launch(p, k_ed_axpby, G, B, n, 1.0, (const double*)r, 0.0, (const double*)r, r0);
-    GS_CUDA(cudaMemsetAsync(pp, 0, sizeof(double) * n, p->stream));
-    GS_CUDA(cudaMemsetAsync(v, 0, sizeof(double) * n, p->stream));
-    GS_LAUNCH();
-    double an = 0.0, rn = 0.0;
+    double an = 0.0;
     GS_TRY(op.dot(a, a, &an));
-    GS_TRY(op.dot(r, r, &rn));
     const double anorm = sqrt(an);
     const double tol = 1.0e-13;
-    double rho = 1.0, alpha = 1.0, omega = 1.0;
-    int it = 0;
-    for (; it < 200 && anorm > 0.0 && sqrt(rn) > tol * anorm; it++) {
-        double rho1 = 0.0;
-        GS_TRY(op.dot(r0, r, &rho1));
-        const double beta = (rho1 / rho) * (alpha / omega);
-        // p = r + beta (p - omega v)
-        launch(p, k_ed_axpby, G, B, n, 1.0, (const double*)pp, -omega, (const double*)v, pp);
-        launch(p, k_ed_axpby, G, B, n, 1.0, (const double*)r, beta, (const double*)pp, pp);
+    // GMRES(M) on (I + B) x = a: Arnoldi with classical Gram-Schmidt applied
+    // twice, Givens rotations of the Hessenberg matrix on the host, one
+    // synchronisation per step
+    std::vector<double> H((size_t)(M + 1) * M), cs(M), sn(M), g(M + 1), y(M), hh(2 * GMRES_M1 + 1);
+    int applies = 0;
+    double res = 0.0;
+    bool conv = anorm == 0.0;
+    while (!conv && applies < 200) {
+        // r = a - (I + B) x, V_0 = r / |r|
+        GS_TRY(op.apply(x, r));
+        applies++;
+        launch(p, k_ed_axpby, G, B, n, 1.0, (const double*)a, -1.0, (const double*)r, r);
         GS_LAUNCH();
-        GS_TRY(op.apply(pp, v));
-        double r0v = 0.0;
-        GS_TRY(op.dot(r0, v, &r0v));
-        alpha = rho1 / r0v;
-        launch(p, k_ed_axpby, G, B, n, 1.0, (const double*)r, -alpha, (const double*)v, sv);
+        double rn2 = 0.0;
+        GS_TRY(op.dot(r, r, &rn2));
+        const double beta = sqrt(rn2);
+        res = beta;
+        if (!(beta == beta)) break;
+        if (beta <= tol * anorm) { conv = true; break; }
+        launch(p, k_ed_axpby, G, B, n, 1.0 / beta, (const double*)r, 0.0, (const double*)r, V);
         GS_LAUNCH();
-        double sn = 0.0;
-        GS_TRY(op.dot(sv, sv, &sn));
-        if (sqrt(sn) <= tol * anorm) {
-            launch(p, k_ed_axpby, G, B, n, 1.0, (const double*)x, alpha, (const double*)pp, x);
+        std::fill(g.begin(), g.end(), 0.0);
+        g[0] = beta;
+        int k = 0;
+        for (; k < M && applies < 200; k++) {
+            double* vk1 = V + (size_t)(k + 1) * n;
+            GS_TRY(op.apply(V + (size_t)k * n, vk1));
+            applies++;
+            for (int pass = 0; pass < 2; pass++) {
+                launch(p, k_mdot_part, PARTS, 256, n, k + 1, (const double*)V, (const double*)vk1, part);
+                launch(p, k_mdot_final, k + 1, 256, PARTS, k + 1, (const double*)part, hd + pass * GMRES_M1);
+                launch(p, k_mupdate, G, B, n, k + 1, (const double*)V, (const double*)(hd + pass * GMRES_M1), vk1);
+                GS_LAUNCH();
+            }
+            launch(p, k_ed_dot_part, 512, 256, n, (const double*)vk1, (const double*)vk1, p->red);
+            launch(p, k_ed_dot_final, 1, 1024, 512, (const double*)p->red, hd + 2 * GMRES_M1);
             GS_LAUNCH();
-            rn = sn;
-            it++;
-            break;
+            GS_CUDA(cudaMemcpyAsync(hh.data(), hd, sizeof(double) * (2 * GMRES_M1 + 1), cudaMemcpyDeviceToHost,
+                                    p->stream));
+            GS_CUDA(cudaStreamSynchronize(p->stream));
+            double* col = &H[(size_t)k * (M + 1)];
+            for (int j = 0; j <= k; j++) col[j] = hh[j] + hh[GMRES_M1 + j];
+            const double hn = sqrt(hh[2 * GMRES_M1]);
+            col[k + 1] = hn;
+            for (int j = 0; j < k; j++) {
+                const double t = cs[j] * col[j] + sn[j] * col[j + 1];
+                col[j + 1] = -sn[j] * col[j] + cs[j] * col[j + 1];
+                col[j] = t;
+            }
+            const double den = std::hypot(col[k], col[k + 1]);
+            cs[k] = den > 0.0 ? col[k] / den : 1.0;
+            sn[k] = den > 0.0 ? col[k + 1] / den : 0.0;
+            col[k] = den;
+            col[k + 1] = 0.0;
+            g[k + 1] = -sn[k] * g[k];
+            g[k] = cs[k] * g[k];
+            res = std::fabs(g[k + 1]);
+            if (!(res == res)) break;
+            if (res <= tol * anorm || hn == 0.0) { k++; conv = true; break; }
+            launch(p, k_ed_axpby, G, B, n, 1.0 / hn, (const double*)vk1, 0.0, (const double*)vk1, vk1);
+            GS_LAUNCH();
         }
-        GS_TRY(op.apply(sv, tv));
-        double ts = 0.0, tt = 0.0;
-        GS_TRY(op.dot(tv, sv, &ts));
-        GS_TRY(op.dot(tv, tv, &tt));
-        omega = ts / tt;
-        launch(p, k_ed_axpby, G, B, n, 1.0, (const double*)x, alpha, (const double*)pp, x);
-        launch(p, k_ed_axpby, G, B, n, 1.0, (const double*)x, omega, (const double*)sv, x);
-        launch(p, k_ed_axpby, G, B, n, 1.0, (const double*)sv, -omega, (const double*)tv, r);
+        // x += V y, H y = g (upper triangular, k columns)
+        for (int i = k - 1; i >= 0; i--) {
+            double s2 = g[i];
+            for (int j = i + 1; j < k; j++) s2 -= H[(size_t)j * (M + 1) + i] * y[j];
+            y[i] = s2 / H[(size_t)i * (M + 1) + i];
+        }
+        for (int i = 0; i < k; i++) y[i] = -y[i];
+        GS_CUDA(cudaMemcpyAsync(hd, y.data(), sizeof(double) * k, cudaMemcpyHostToDevice, p->stream));
+        launch(p, k_mupdate, G, B, n, k, (const double*)V, (const double*)hd, x);
         GS_LAUNCH();
-        GS_TRY(op.dot(r, r, &rn));
-        rho = rho1;
-        if (!(rn == rn)) break;
+        GS_CUDA(cudaStreamSynchronize(p->stream));
+        if (!(res == res)) break;
     }
-    p->ed_iters = it;
-    p->ed_relres = anorm > 0.0 ? sqrt(rn) / anorm : 0.0;
-    if (!(rn == rn) || sqrt(rn) > tol * anorm * 1.0e3) {
-        set_error(GS_EMAXITER, "transport-limited SPL: BiCGSTAB did not converge");
+    p->ed_iters = applies;
+    p->ed_relres = anorm > 0.0 ? res / anorm : 0.0;
+    if (!conv) {
+        set_error(GS_EMAXITER, "transport-limited SPL: GMRES did not converge");
         return GS_EMAXITER;
     }
     return GS_OK;

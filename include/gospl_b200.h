@@ -188,8 +188,8 @@ int gs_flow_accumulation(gs_plan* plan, const double* h, const double* bl, doubl
  * (inputparser.py:472; default 0).  With G > 0 gs_erodep_spl solves the
  * coupled erosion-deposition system of _getEroDepRate / _coupledEDSystem
  * (SPL.py:116-258, 305-336) instead of the detachment-limited one; its
- * stats then report the solver's iterations (cg_iters) and final relative
- * residual (cg_relres).
+ * stats then report the solver's operator applications (cg_iters; each is
+ * one flow sweep and one SPL sweep) and final relative residual (cg_relres).
  */
 int gs_plan_set_deposition(gs_plan* plan, double g);
 int gs_erodep_spl(gs_plan* plan, double* h, double* cum_ed, double* eb, const double* fal,
