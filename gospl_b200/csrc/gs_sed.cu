@@ -1,6 +1,6 @@
 // Continental sediment routing and deposition in depressions: goSPL's
-// SEDMesh.sedChange (gospl/sed/sedplex.py:1061-1086) for one landscape with a
-// single lithology and no provenance tracers.
+// SEDMesh.sedChange (gospl/sed/sedplex.py:1061-1086) for a landscape (or an
+// ensemble of landscapes) with a single lithology and no provenance tracers.
 //
 //   1. _getSedFlux (sedplex.py:103-188): vSed = (I - W^T)^-1 (-Eb * area) over
 //      the snapshot receivers of the preceding flow accumulation (fMati), one
@@ -15,7 +15,8 @@
 //      on sedFilled (pit-flat routing, down=True) when a depression filled,
 //      and the excess is routed downstream by an ordered flow sweep; flux on
 //      cells not under a filled lake adds to vSed.  Terminal cells that are
-//      not a depression keep their sediment on closed domains.
+//      not a depression keep their sediment on closed domains.  Ensemble
+//      members (gs_plan_set_members) each run their own loop.
 //   4. _updateSinks (sedplex.py:982-1059) paths 1 and 2: each depression that
 //      received sediment gets a horizontal deposit surface at the level whose
 //      filled volume matches the deposit (np.interp over its five-level
@@ -24,10 +25,21 @@
 //      filled depressions of at least nlPitVolume and nlPitDepth, smoothed by
 //      non-linear diffusion) is reported as an error.
 #include <string>
+#include <vector>
 
 #include "gs_plan.cuh"
 
 namespace gs {
+
+// member helpers of the flow cascade (gs_flow.cu)
+__global__ void k_pit_member(int np1, const int* __restrict__ seg_start, const int* __restrict__ seg_count,
+                             const int* __restrict__ cells, const int* __restrict__ vmember, int* pmember);
+__global__ void k_chunk_sum(const int* __restrict__ lo, const double* __restrict__ x, double* part);
+__global__ void k_member_sum(int nmem, const int* __restrict__ m0, const double* __restrict__ part, double* out);
+__global__ void k_lsink_keep(int n, const int* __restrict__ vmember, const uint8_t* __restrict__ mbig,
+                             const uint8_t* __restrict__ prev, uint8_t* lsink);
+__global__ void k_rhs_members(int n, const int* __restrict__ vmember, const uint8_t* __restrict__ msolve,
+                              double* b);
 
 namespace {
 
@@ -55,11 +67,14 @@ __global__ void k_sed_pitvol(int np1, const double* __restrict__ params, double*
 
 // flow-terminal cells that are no depression: their sediment leaves the
 // routed flux (kept in place on a closed domain)
-__global__ void k_sed_csink(int n, const uint8_t* __restrict__ lsink, const int* __restrict__ pit, int keep,
-                            double* vol, double* closed) {
+__global__ void k_sed_csink(int n, const uint8_t* __restrict__ lsink, const int* __restrict__ pit,
+                            const uint8_t* __restrict__ mout, const int* __restrict__ vmember,
+                            const uint8_t* __restrict__ mact, double* vol, double* closed) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n || !lsink[i] || pit[i] >= 0) return;
-    if (keep) closed[i] = closed[i] + vol[i];
+    const int m = vmember[i];
+    if (!mact[m]) return;
+    if (!mout[m]) closed[i] = closed[i] + vol[i];
     vol[i] = 0.0;
 }
 
@@ -68,11 +83,18 @@ __global__ void k_fill_int_s(int n, int* a, int v) {
     if (i < n) a[i] = v;
 }
 
-// per-pit decisions of one _moveDownstream pass (sedplex.py:290-330)
+// per-pit decisions of one _moveDownstream pass (sedplex.py:290-330); the
+// pits of members whose loop has ended are not touched
 __global__ void k_sed_pits(int np1, const double* __restrict__ inV, double* vol, const int* __restrict__ info,
-                           double* ev, uint8_t* state, int* win, int* flags) {
+                           const int* __restrict__ pmember, const uint8_t* __restrict__ mact, double* ev,
+                           uint8_t* state, int* win, int* mflags) {
     int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= np1) return;
+    const int mem = pmember[p];
+    if (!mact[mem]) {
+        state[p] = 0;
+        return;
+    }
     const double in = inV[p];
     const double e = in - vol[p];
     ev[p] = e;
@@ -92,7 +114,7 @@ __global__ void k_sed_pits(int np1, const double* __restrict__ inV, double* vol,
     }
     if (e > 1.0e-3) f |= S_BIG;
     state[p] = s;
-    if (f) atomicOr(flags, f);
+    if (f) atomicOr(&mflags[mem], f);
 }
 
 __global__ void k_sed_spill(int np1, const double* __restrict__ ev, const uint8_t* __restrict__ state,
@@ -114,9 +136,10 @@ __global__ void k_sed_cells(int n, const int* __restrict__ pit, const uint8_t* _
 // to vSed (sedplex.py:443-451)
 __global__ void k_sed_accum(int n, const double* __restrict__ routed, const double* __restrict__ hl,
                             const double* __restrict__ sfill, const uint8_t* __restrict__ outlet, double dt,
-                            double* vol, double* vsed) {
+                            const int* __restrict__ vmember, const uint8_t* __restrict__ msolve, double* vol,
+                            double* vsed) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
+    if (i >= n || !msolve[vmember[i]]) return;
     const double v = routed[i];
     const double keep = (hl[i] < sfill[i]) ? 0.0 : v;
     vsed[i] = vsed[i] + keep / dt;
@@ -223,6 +246,13 @@ __global__ void k_sed_delta(int n, const int* __restrict__ pit, const uint8_t* _
     dist[i] = ds;
 }
 
+// members with a draining outlet (sedplex.py:45-47, _domainHasOutlet per landscape)
+__global__ void k_sed_moutlet(int nout, const int* __restrict__ outlet_ids, const int* __restrict__ vmember,
+                              uint8_t* mout) {
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < nout) mout[vmember[outlet_ids[t]]] = 1;
+}
+
 __global__ void k_sed_ones(int n, double* a) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) a[i] = 1.0;
@@ -254,34 +284,6 @@ __global__ void k_sed_pitfinal(int np1, const double* __restrict__ vol, double* 
     if (p < np1) params[3 * p] = vol[p];
 }
 
-__global__ void k_sed_sum_part(int n, const double* __restrict__ x, double* part) {
-    __shared__ double sh[256];
-    double acc = 0.0;
-    const int per = (n + gridDim.x - 1) / gridDim.x;
-    const int lo = blockIdx.x * per, hi = lo + per < n ? lo + per : n;
-    for (int i = lo + threadIdx.x; i < hi; i += blockDim.x) acc += x[i];
-    sh[threadIdx.x] = acc;
-    __syncthreads();
-    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
-        if (threadIdx.x < s) sh[threadIdx.x] += sh[threadIdx.x + s];
-        __syncthreads();
-    }
-    if (threadIdx.x == 0) part[blockIdx.x] = sh[0];
-}
-
-__global__ void k_sed_sum_final(int parts, const double* __restrict__ part, double* out) {
-    __shared__ double sh[512];
-    double acc = 0.0;
-    for (int i = threadIdx.x; i < parts; i += blockDim.x) acc += part[i];
-    sh[threadIdx.x] = acc;
-    __syncthreads();
-    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
-        if (threadIdx.x < s) sh[threadIdx.x] += sh[threadIdx.x + s];
-        __syncthreads();
-    }
-    if (threadIdx.x == 0) *out = sh[0];
-}
-
 }  // namespace
 
 int sed_change(gs_plan* p, double* h, double* cum_ed, const double* eb, const double* xyz, double sealevel,
@@ -290,13 +292,9 @@ int sed_change(gs_plan* p, double* h, double* cum_ed, const double* eb, const do
                double* vsed, gs_stats* st) {
     const int n = (int)p->n;
     if (n == 0) return GS_OK;
-    if (p->nmem > 1) {
-        set_error(GS_EINVAL, "sedChange: sediment routing of ensemble members is not built");
-        return GS_EINVAL;
-    }
     const int B = 256, G = grid_for(n, B);
     if (!p->sed_buf) GS_CUDA(cudaMalloc((void**)&p->sed_buf, sizeof(double) * (size_t)n * 8));
-    if (!p->sed_mask) GS_CUDA(cudaMalloc((void**)&p->sed_mask, (size_t)n * 2));
+    if (!p->sed_mask) GS_CUDA(cudaMalloc((void**)&p->sed_mask, (size_t)n * 3));
     double* vol = p->sed_buf;
     double* nv = vol + n;
     double* routed = nv + n;
@@ -307,7 +305,11 @@ int sed_change(gs_plan* p, double* h, double* cum_ed, const double* eb, const do
     double* dist = delta + n;
     uint8_t* sea_s = p->sed_mask;
     uint8_t* tmask = sea_s + n;
-    const int keep_closed = p->n_outlet > 0 ? 0 : 1;   // sedplex.py:45-47
+    uint8_t* mout = tmask + n;   // [nmem] (nmem <= n)
+    GS_CUDA(cudaMemsetAsync(mout, 0, (size_t)p->nmem, p->stream));
+    if (p->n_outlet > 0)
+        launch(p, k_sed_moutlet, grid_for(p->n_outlet, B), B, p->n_outlet, (const int*)p->outlet_ids,
+               (const int*)p->vmember, mout);
 
     // 1. sediment flux over the snapshot graph of the last flow accumulation
     int cyc = 0, total_cycles = 0;
@@ -327,36 +329,65 @@ int sed_change(gs_plan* p, double* h, double* cum_ed, const double* eb, const do
     launch(p, k_sed_pitvol, grid_for(np1, B), B, np1, (const double*)p->pit_params, p->pit_vol);
     GS_LAUNCH();
 
-    // 3. cascade over the depressions
-    int* flags = p->i_scalar + 10;
+    // 3. cascade over the depressions.  Every member runs its own
+    // _distributeSediment loop (sedplex.py:430-453): it leaves when it has no
+    // excess left, and the pits, cells and sinks of members that left are not
+    // touched by later passes of the others.
+    const int nm = p->nmem;
+    launch(p, k_pit_member, grid_for(np1, B), B, np1, (const int*)p->seg_start, (const int*)p->seg_count,
+           (const int*)p->seg_vals2, (const int*)p->vmember, p->pmember);
+    GS_LAUNCH();
+    std::vector<uint8_t> act(nm, 1), big(nm), rebuild(nm), solve(nm);
+    auto any = [](const std::vector<uint8_t>& v) {
+        for (uint8_t x : v)
+            if (x) return true;
+        return false;
+    };
+    auto all = [](const std::vector<uint8_t>& v) {
+        for (uint8_t x : v)
+            if (!x) return false;
+        return true;
+    };
     int step = 0, solves = 0;
-    bool excess = true;
-    while (excess) {
-        if (step >= 5000) break;
-        excess = false;
-        launch(p, k_sed_csink, G, B, n, (const uint8_t*)lsink, (const int*)pit_ids, keep_closed, vol, closed);
+    while (any(act) && step < 5000) {
+        GS_CUDA(cudaMemcpyAsync(p->mact, act.data(), nm, cudaMemcpyHostToDevice, p->stream));
+        launch(p, k_sed_csink, G, B, n, (const uint8_t*)lsink, (const int*)pit_ids, (const uint8_t*)mout,
+               (const int*)p->vmember, (const uint8_t*)p->mact, vol, closed);
         GS_LAUNCH();
         GS_TRY(group_sum_by_pit(p, pit_ids, lsink, vol, p->pit_in, P));
-        GS_CUDA(cudaMemsetAsync(flags, 0, sizeof(int), p->stream));
+        GS_CUDA(cudaMemsetAsync(p->mflags, 0, sizeof(int) * nm, p->stream));
         launch(p, k_fill_int_s, G, B, n, p->pit_win, -1);
         launch(p, k_sed_pits, grid_for(np1, B), B, np1, (const double*)p->pit_in, p->pit_vol,
-               (const int*)p->pit_info, p->pit_ev, p->pit_state, p->pit_win, flags);
+               (const int*)p->pit_info, (const int*)p->pmember, (const uint8_t*)p->mact, p->pit_ev, p->pit_state,
+               p->pit_win, p->mflags);
         GS_LAUNCH();
-        int f = 0;
-        GS_CUDA(cudaMemcpyAsync(&f, flags, sizeof(int), cudaMemcpyDeviceToHost, p->stream));
+        GS_CUDA(cudaMemcpyAsync(p->h_mflags, p->mflags, sizeof(int) * nm, cudaMemcpyDeviceToHost, p->stream));
         GS_CUDA(cudaStreamSynchronize(p->stream));
+        int anyf = 0;
+        for (int m = 0; m < nm; m++) {
+            const int f = act[m] ? p->h_mflags[m] : 0;
+            anyf |= f;
+            big[m] = (f & S_BIG) ? 1 : 0;
+            rebuild[m] = (big[m] && ((f & S_POS) || step == 0 || step == 100)) ? 1 : 0;
+            solve[m] = 0;
+        }
         GS_CUDA(cudaMemsetAsync(nv, 0, sizeof(double) * n, p->stream));
-        const bool changed = (f & S_POS) != 0;
-        if (changed) {
+        if (anyf & S_POS) {
             launch(p, k_sed_spill, grid_for(np1, B), B, np1, (const double*)p->pit_ev, (const uint8_t*)p->pit_state,
                    (const int*)p->pit_info, (const int*)p->pit_win, nv);
             launch(p, k_sed_cells, G, B, n, (const int*)pit_ids, (const uint8_t*)p->pit_state, (const double*)lfill,
                    sfill);
             GS_LAUNCH();
         }
-        if (f & S_BIG) {
-            if (changed || step == 0 || step == 100) {
-                // flow graph of the sediment-filled surface (down=True)
+        if (any(big)) {
+            if (any(rebuild)) {
+                // flow graph of the sediment-filled surface (down=True); the
+                // sinks of members that do not rebuild are kept
+                const bool every = all(rebuild);
+                if (!every) {
+                    GS_CUDA(cudaMemcpyAsync(p->lsink_prev, lsink, n, cudaMemcpyDeviceToDevice, p->stream));
+                    GS_CUDA(cudaMemcpyAsync(p->mbig, rebuild.data(), nm, cudaMemcpyHostToDevice, p->stream));
+                }
                 const double* surf = (step == 100) ? lfill : sfill;
                 GS_TRY(receivers(p, p->R, 1.1, surf, sealevel, p->gid, p->rcv, p->dist, p->wgt, p->rslot));
                 GS_TRY(flow_order_from(p, surf, hl, p->order_i, p->order));
@@ -364,28 +395,35 @@ int sed_change(gs_plan* p, double* h, double* cum_ed, const double* eb, const do
                 GS_TRY(fill_join(p, st));
                 GS_TRY(flow_direction_post(p, surf, true, lfill, pit_ids, flat_dirs, sealevel, p->rcv, p->dist,
                                            p->wgt, p->rslot, lsink, sea_s));
+                if (!every)
+                    launch(p, k_lsink_keep, G, B, n, (const int*)p->vmember, (const uint8_t*)p->mbig,
+                           (const uint8_t*)p->lsink_prev, lsink);
                 GS_TRY(flow_order_ties(p, p->pdir, p->order));
             }
-            const int PARTS = 256;
-            launch(p, k_sed_sum_part, PARTS, 256, n, (const double*)nv, p->red);
-            launch(p, k_sed_sum_final, 1, 512, PARTS, (const double*)p->red, p->red + 4200);
+            // excess of each member (tmp.sum() > 0.5 maxarea, sedplex.py:349)
+            launch(p, k_chunk_sum, p->nchunk, 256, (const int*)p->chunk_lo, (const double*)nv, p->chunk_part);
+            launch(p, k_member_sum, grid_for(nm, 128), 128, nm, (const int*)p->mchunk0, (const double*)p->chunk_part,
+                   p->mresid);
             GS_LAUNCH();
-            double total = 0.0;
-            GS_CUDA(cudaMemcpyAsync(&total, p->red + 4200, sizeof(double), cudaMemcpyDeviceToHost, p->stream));
+            GS_CUDA(cudaMemcpyAsync(p->h_mresid, p->mresid, sizeof(double) * nm, cudaMemcpyDeviceToHost, p->stream));
             GS_CUDA(cudaStreamSynchronize(p->stream));
-            if (total > 0.5 * p->maxarea) {
-                excess = true;
+            for (int m = 0; m < nm; m++) solve[m] = (big[m] && p->h_mresid[m] > 0.5 * p->mmaxarea[m]) ? 1 : 0;
+            if (any(solve)) {
+                GS_CUDA(cudaMemcpyAsync(p->msolve, solve.data(), nm, cudaMemcpyHostToDevice, p->stream));
+                if (!all(solve))
+                    launch(p, k_rhs_members, G, B, n, (const int*)p->vmember, (const uint8_t*)p->msolve, nv);
                 GS_TRY(flow_prepare(p, p->rcv, p->wgt, p->rslot, routed, p->order, p->h_pinned));
                 GS_CUDA(cudaStreamSynchronize(p->stream));
                 const int ok = p->h_pinned[0] ? 0 : 1;
                 GS_TRY(flow_run(p, p->rcv, p->wgt, p->rslot, nv, routed, &cyc, p->order, ok));
                 total_cycles += cyc;
                 launch(p, k_sed_accum, G, B, n, (const double*)routed, (const double*)hl, (const double*)sfill,
-                       (const uint8_t*)p->outlet, dt, vol, vsed);
+                       (const uint8_t*)p->outlet, dt, (const int*)p->vmember, (const uint8_t*)p->msolve, vol, vsed);
                 GS_LAUNCH();
                 solves++;
             }
         }
+        for (int m = 0; m < nm; m++) act[m] = solve[m];
         step++;
     }
     GS_TRY(fill_join(p, st));
@@ -412,10 +450,8 @@ int sed_change(gs_plan* p, double* h, double* cum_ed, const double* eb, const do
                                  "by non-linear diffusion), which is not built");
         return GS_EINVAL;
     }
-    if (keep_closed) {
-        launch(p, k_sed_closed, G, B, n, (const double*)closed, (const double*)p->larea, h, cum_ed);
-        GS_LAUNCH();
-    }
+    launch(p, k_sed_closed, G, B, n, (const double*)closed, (const double*)p->larea, h, cum_ed);
+    GS_LAUNCH();
     launch(p, k_sed_delta, G, B, n, (const int*)pit_ids, (const uint8_t*)p->pit_state, (const double*)p->pit_lvl,
            (const double*)lfill, (const double*)hl, xyz, (const int*)p->pit_info, delta, dist, tmask);
     launch(p, k_sed_ones, G, B, n, routed);

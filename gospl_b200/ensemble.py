@@ -13,8 +13,11 @@ its step lengths from inner products over all members (each member's system
 is still solved to the relative tolerance), and per-member residual sums run
 in a different (fixed) order.
 
-Members must share the time step, sea level, flow directions, exponents and
-diffusivities (per-member erodibility, rainfall and uplift are fields), and
+Members must share the time step, sea level, flow directions, exponents,
+diffusivities and the deposition switches (nodep, nlPitVolume, nlPitDepth;
+per-member erodibility, rainfall and uplift are fields); with deposition on,
+each member runs its own sediment cascade (continental sediment routing of
+the member alone); and
 the fill level max(min h, sea + oFill) of every member must be the same (the
 planar ensembles here pin their boundary at 0 m).
 
@@ -27,7 +30,8 @@ import numpy as np
 from .mesh import FVMesh
 from .model import Model
 
-COMMON = ("dt", "tStart", "tEnd", "flowDir", "d", "m", "Cda", "Cdm", "sealevel", "oFill")
+COMMON = ("dt", "tStart", "tEnd", "flowDir", "d", "m", "Cda", "Cdm", "sealevel", "oFill", "nodep", "nlPitVolume",
+          "nlPitDepth")
 
 
 def partition(sizes, world):
@@ -111,11 +115,12 @@ class Ensemble:
             upsub = np.concatenate([np.zeros(k) if u is None else np.asarray(u, np.float64) for k, u in zip(n, ups)])
         params = dict(p0, K=K, rain=rain, upsub=upsub)
         elev = np.concatenate([np.asarray(z, np.float64) for c, f, z, r, up, p in members])
+        coords = np.concatenate([np.asarray(c, np.float64) for c, f, z, r, up, p in members])
         marea = np.array([float(me.larea.max()) for me in meshes])
         self.start = start
         self.sizes = np.asarray(n)
         self.mesh = mesh
-        self.model = Model(elev=elev, params=params, mesh=mesh, device=dev, members=(start, marea),
+        self.model = Model(coords=coords, elev=elev, params=params, mesh=mesh, device=dev, members=(start, marea),
                            cg_rtol=cg_rtol)
 
     @property

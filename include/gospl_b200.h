@@ -219,9 +219,10 @@ int gs_erodep_spl(gs_plan* plan, double* h, double* cum_ed, double* eb, const do
  * flat_dirs and the plan's pit tables, with pitParams volumes left to the
  * unfilled remainder) and lsink.  Partly filled depressions of at least
  * nl_pit_volume (m3) and nl_pit_depth (m), whose deposit goSPL smooths by
- * non-linear diffusion, return GS_EINVAL (stats.status = their count);
- * ensembles (gs_plan_set_members) return GS_EINVAL.  stats: npits, cascade
- * passes and solves.
+ * non-linear diffusion, return GS_EINVAL (stats.status = their count).
+ * Ensemble members (gs_plan_set_members) each run their own cascade, with
+ * closed-domain deposits for members without an outlet.  stats: npits,
+ * cascade passes and solves.
  */
 int gs_sed_change(gs_plan* plan, double* h, double* cum_ed, const double* eb, const double* xyz,
                   double sealevel, double ofill, double dt, double nl_pit_volume, double nl_pit_depth,

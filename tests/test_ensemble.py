@@ -73,12 +73,16 @@ def test_two_rank_partition_gloo():
 
 
 @pytest.mark.gpu
-def test_members_evolve_as_alone():
+@pytest.mark.parametrize("nodep", [True, False])
+def test_members_evolve_as_alone(nodep):
+    """Each member of an ensemble evolves as it would alone, with and without
+    continental deposition (each member its own flow and sediment cascade)."""
     import torch
     from gospl_b200.ensemble import Ensemble
     from gospl_b200.model import Model
 
     members = [S.ensemble_member(n, seed) for n, seed in ((2500, 11), (4000, 12), (6000, 13))]
+    members = [(c, f, z, r, u, dict(p, nodep=nodep)) for c, f, z, r, u, p in members]
     ens = Ensemble(members)
     dev = torch.device("cuda", torch.cuda.current_device())
     alone = []
@@ -103,10 +107,10 @@ def test_members_evolve_as_alone():
                     a = np.where(a >= 0, a - off, a)
                 assert np.array_equal(a, b), (step, k, name)
             hscale = max(np.abs(m.hGlobal.cpu().numpy()).max(), 1.0)
-            for name in ("FAL", "hGlobal", "cumED", "lFill"):
+            for name in ("FAL", "hGlobal", "cumED", "lFill") + (() if nodep else ("vSed",)):
                 a = ens.view(getattr(ens.model, name), k).cpu().numpy()
                 b = getattr(m, name).cpu().numpy()
-                scale = max(np.abs(b).max(), 1.0) if name == "FAL" else hscale
+                scale = max(np.abs(b).max(), 1.0) if name in ("FAL", "vSed") else hscale
                 assert np.abs(a - b).max() <= 1e-12 * scale, (step, k, name, np.abs(a - b).max())
     for m in alone:
         m.destroy()
