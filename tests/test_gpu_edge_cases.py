@@ -119,3 +119,12 @@ def test_lake_diffusion_path_rejected():
         gm.step()
     torch.cuda.synchronize()
     gm.destroy()
+
+
+def test_transport_limited_with_deposition():
+    """Both deposition paths of goSPL in one step: transport-limited erosion
+    (G > 0, SPL.py:305-336) followed by continental sediment routing
+    (sedplex.py:1061-1086)."""
+    coords, cells, z, params = _planar(3000, 33, "ffff")
+    params = dict(params, G=1.0, nodep=False)
+    _step_vs_oracle(coords, cells, z, params)
