@@ -142,6 +142,36 @@ def sethillslopecoeff(nb, kd):
     return out
 
 
+def jacobiancoeff(h, kd, kp):
+    """f2py: dcoeff = jacobiancoeff(h, Kd, Kp) (functions.F90:1423-1467): per
+    row the non-linear diffusion Jacobian, column 0 the diagonal and column
+    p+1 the neighbour in slot p, faces gated by Kd > 0 on both sides.  numpy
+    restatement over the mesh installed by setmesh; the diagonal accumulates
+    in slot order as the Fortran loop does."""
+    h = _f64(h)
+    kd = _f64(kd)
+    kp = _f64(kp)
+    nnb, ngb, el, vd, ar = getmesh()
+    nb = h.shape[0]
+    out = np.zeros((nb, 13))
+    has = ar > 0
+    for p in range(12):
+        ok = has & (p < nnb) & (vd[:, p] > 0.0)
+        j = np.where(ok, ngb[:, p], 0)
+        ck, cn, cpk, cpn = kd, kd[j], kp, kp[j]
+        g = ok & (ck > 0.0) & (cn > 0.0)
+        if not g.any():
+            continue
+        a = ar[g]
+        c1 = 0.5 * (ck[g] + cn[g] + cpk[g] * (h[g] - h[j][g])) / a
+        v1 = c1 * vd[g, p] / el[g, p]
+        out[g, 0] = out[g, 0] + v1
+        c2 = 0.5 * (ck[g] + cn[g] + cpn[g] * (h[j][g] - h[g])) / a
+        v2 = c2 * vd[g, p] / el[g, p]
+        out[g, p + 1] = -v2
+    return out
+
+
 # --- receivers ------------------------------------------------------------------
 def mfdreceivers(nrcv, exp, elev, sl, gid, powfn=None):
     """f2py: rcv, dist, wgt = mfdreceivers(nrcv, exp, elev, sl, gid)."""

@@ -86,6 +86,13 @@ class OracleModel:
             raise NotImplementedError("marine deposition (seaChange) is not restated")
         self.nl_pit_volume = float(p.get("nlPitVolume", 1.0e9))   # inputparser.py:562,584
         self.nl_pit_depth = float(p.get("nlPitDepth", 100.0))     # inputparser.py:563,585
+        self.nl_pit_K = float(p.get("nlPitK", p.get("nonlinKm", 10.0)))             # inputparser.py:564
+        self.nl_pit_inlet_bias = min(1.0, max(0.0, float(p.get("pitInletBias", 0.5))))  # :569,587,593
+        self.marineSolver = str(p.get("marineSolver", "ts")).lower()                 # inputparser.py:576
+        self.picardSub = int(p.get("picardSub", 10))
+        self.picardIts = int(p.get("picardIts", 2))
+        self.dexp = 0.05                                                             # hillslope.py:34
+        self.minDiff = 1.0e-4                                                        # hillslope.py:35
         self._domainHasOutlet = len(self.outletIDs) > 0           # sedplex.py:45-47
         self.lcoords = np.asarray(coords, dtype=np.float64).reshape(-1, 3)
         self.rainMesh = np.asarray(p["rain"], dtype=np.float64)
@@ -775,9 +782,123 @@ class OracleModel:
         tilted[tilted < 0] = 0.0
         return tilted
 
+    def _identifyPitInlets(self):
+        """sedplex.py:646-677: cells receiving flow (snapshot receivers) from a
+        donor outside their own depression."""
+        R = self.rcvIDi.shape[1]
+        src = np.repeat(np.arange(self.lpoints), R)
+        dst = self.rcvIDi.flatten().astype(int)
+        good = src != dst
+        src, dst = src[good], dst[good]
+        sp, dp = self.pitIDs[src], self.pitIDs[dst]
+        e = (dp >= 0) & (sp != dp)
+        mask = np.zeros(self.lpoints, dtype=bool)
+        if e.any():
+            mask[dst[e]] = True
+        return mask
+
+    def _diffuseImplicitPicard(self, dh, mask, Cd_val):
+        """hillslope.py:988-1076 (marineSolver picard): picardSub backward-Euler
+        sub-steps, each with picardIts solves of (I + dt_sub L(C_d(h))) h =
+        h_start, L from jacobiancoeff with Kp = 0; solved exactly here where
+        goSPL runs Richardson + block Jacobi to rtol."""
+        nsub, npic = self.picardSub, self.picardIts
+        dt_sub = self.dt / nsub
+        n = self.lpoints
+        Cd0 = np.zeros(n)
+        Cd0[mask] = Cd_val
+        minDiff_vec = np.zeros(n)
+        minDiff_vec[mask] = self.minDiff
+        zb = self.h.copy()
+        zeroKp = np.zeros(n)
+        h = dh + zb
+        nodes = np.arange(n)
+        ngb = self.FVmesh_ngbID[:, :self.maxnb]
+        for _ in range(nsub):
+            hstart = h.copy()
+            for _ in range(npic):
+                dhdep = h - zb
+                dhdep[dhdep < 0.1] = 0.0
+                Cd = minDiff_vec + np.multiply(Cd0, 1.0 - np.exp(-self.dexp * dhdep))
+                nlC = F.jacobiancoeff(h, Cd, zeroKp)
+                coeffs = dt_sub * nlC
+                coeffs[:, 0] += 1.0
+                off = coeffs[:, 1:1 + self.maxnb]
+                keep = off != 0.0
+                rows = np.concatenate([nodes, np.repeat(nodes, self.maxnb)[keep.ravel()]])
+                cols = np.concatenate([nodes, ngb.ravel()[keep.ravel()]])
+                vals = np.concatenate([coeffs[:, 0], off.ravel()[keep.ravel()]])
+                M = sp.csr_matrix((vals, (rows, cols)), shape=(n, n))
+                h = spla.spsolve(M.tocsc(), hstart)
+        ndepo = h - zb
+        ndepo[ndepo < 0.0] = 0.0
+        return ndepo
+
+    def _diffuseLargePit(self, hl, depo, pit_select):
+        """sedplex.py:679-858 (one rank): bathymetric bottom-up baseline plus an
+        inlet pile, smoothed by non-linear diffusion over the pit cells, each
+        pit's deposit rescaled to its volume."""
+        num_pits = len(self.pitParams)
+        active = np.where(pit_select & (depo > 0))[0]
+        if active.size == 0:
+            return np.zeros(self.lpoints)
+        sel_node = np.isin(self.pitIDs, active)
+        inlet_mask = self._identifyPitInlets() & sel_node
+        inlet_count = np.zeros(num_pits)
+        if inlet_mask.any():
+            ids = self.pitIDs[inlet_mask]
+            up, cnts = group_reduce(ids, np.ones_like(ids, dtype=np.float64))
+            inlet_count[up] = cnts
+        no_inlet = active[inlet_count[active] == 0]
+        for p in no_inlet:
+            pit_local = np.where(self.pitIDs == p)[0]
+            if pit_local.size > 0:
+                k = np.argmax(hl[pit_local])
+                inlet_mask[int(pit_local[k])] = True
+                inlet_count[p] = 1.0
+        bias_frac = self.nl_pit_inlet_bias
+        target_lvl = np.full(num_pits, -np.inf)
+        for p in active:
+            pit_min = self.pitParams[p, 1] - self.pitParams[p, 2]
+            vols = np.concatenate(([0.0], self.filled_vol[p]))
+            lvls = np.concatenate(([pit_min], self.filled_lvl[p]))
+            target_lvl[p] = np.interp(depo[p], vols, lvls)
+        in_pit = self.pitIDs >= 0
+        pit_safe = np.where(in_pit, self.pitIDs, 0)
+        node_lvl = np.where(in_pit, target_lvl[pit_safe], -np.inf)
+        water_depth = np.maximum(0.0, node_lvl - hl)
+        water_depth[~sel_node] = 0.0
+        denom = np.zeros(num_pits)
+        if sel_node.any():
+            ids = self.pitIDs[sel_node]
+            up, sums = group_reduce(ids, (water_depth * self.larea)[sel_node])
+            denom[up] = sums
+        delta_init = np.zeros(self.lpoints)
+        denom_node = denom[pit_safe]
+        ok = (denom_node > 0) & sel_node
+        delta_init[ok] = ((1.0 - bias_frac) * depo[pit_safe[ok]] * water_depth[ok]
+                          / np.maximum(denom_node[ok], 1e-30))
+        bias_at_inlet = np.where(denom > 0, bias_frac, 1.0)
+        for c in np.where(inlet_mask)[0]:
+            p = self.pitIDs[c]
+            if inlet_count[p] > 0:
+                delta_init[c] += bias_at_inlet[p] * depo[p] / (inlet_count[p] * self.larea[c])
+        delta_smooth = self._diffuseImplicitPicard(delta_init, sel_node, self.nl_pit_K)
+        actual_vol = np.zeros(num_pits)
+        if sel_node.any():
+            ids = self.pitIDs[sel_node]
+            up, sums = group_reduce(ids, (delta_smooth * self.larea)[sel_node])
+            actual_vol[up] = sums
+        with np.errstate(divide="ignore", invalid="ignore"):
+            scale = np.where(actual_vol > 0, depo / np.maximum(actual_vol, 1e-30), 1.0)
+        node_scale = scale[pit_safe]
+        node_scale[~sel_node] = 0.0
+        return delta_smooth * node_scale
+
     def _updateSinks(self, hl):
-        """sedplex.py:982-1059 (paths 1 and 2; path 3, non-linear diffusion in
-        large deep partly filled pits, is not restated)."""
+        """sedplex.py:982-1059.  Path 3 (partly filled depressions of at least
+        nlPitVolume and nlPitDepth) is restated for marineSolver picard; goSPL's
+        default adaptive TS solve is not."""
         depo = self.pitParams[:, 0] - self.pitVol
         depo[depo < 0] = 0.0
         pit_volume = self.pitParams[:, 0]
@@ -788,12 +909,14 @@ class OracleModel:
         is_large = (pit_volume >= self.nl_pit_volume) & (pit_depth >= self.nl_pit_depth)
         diffuse_path = partial & is_large
         bottomup_path = full_fill | (partial & ~is_large)
-        if diffuse_path.any():
-            raise NotImplementedError("lake deposition by non-linear diffusion (%d large deep pits)"
-                                      % int(diffuse_path.sum()))
+        if diffuse_path.any() and self.marineSolver != "picard":
+            raise NotImplementedError("lake deposition by non-linear diffusion (%d large deep pits) with the "
+                                      "adaptive TS solver" % int(diffuse_path.sum()))
         delta = self._bottomUpDelta(hl, depo, bottomup_path)
         if bottomup_path.any():
             delta = self._addPitMicroTilt(delta, bottomup_path)
+        if diffuse_path.any():
+            delta = delta + self._diffuseLargePit(hl, depo, diffuse_path)
         self.sed_delta = delta
         self.cumED = self.cumED + delta
         self.h = self.h + delta

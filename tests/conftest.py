@@ -12,7 +12,7 @@ GOLDEN_CASES = ["incising", "sphere3766", "planar2k", "ico2562"]
 # transport-limited SPL (G > 0), compared step by step from the reference's state
 GOLDEN_G_CASES = ["ico2562_G05", "planar2k_G1"]
 # continental sediment routing and deposition (nodep off)
-GOLDEN_SED_CASES = ["incising_sed", "planar2k_sed", "ico2562_sed"]
+GOLDEN_SED_CASES = ["incising_sed", "planar2k_sed", "ico2562_sed", "planar2k_lake"]
 
 
 def pytest_configure(config):

@@ -91,6 +91,12 @@ def cases():
     p = dict(dt=1.0e4, tEnd=1.0e5, flowDir=3, K=5.0e-7, d=0.0, m=0.5, Cda=0.05, Cdm=0.05,
              sealevel=0.0, bc="oooo", rain=rain, upsub=up, nodep=False, nlPitVolume=1.0e30)
     out.append(("ico2562_sed", c, f, z, p, 3))
+    # lake deposits smoothed by non-linear diffusion (every partly filled
+    # depression takes that path; Picard solver)
+    c, f, z, rain, up, p = S.planar_config(n=2000, side=30.0e3, seed=7)
+    p = dict(p, rain=rain, upsub=up, tEnd=10 * p["dt"], nodep=False, nlPitVolume=0.0, nlPitDepth=0.0,
+             marineSolver="picard", picardSub=2, picardIts=2)
+    out.append(("planar2k_lake", c, f, z, p, 3))
     return out
 
 
@@ -149,7 +155,7 @@ def main():
         for k in ("dt", "tEnd", "flowDir", "K", "d", "m", "Cda", "Cdm", "sealevel"):
             arrs["p_" + k] = np.array(params[k])
         arrs["p_bc"] = np.array(params["bc"])
-        for k in ("G", "nodep", "nlPitVolume", "nlPitDepth"):
+        for k in ("G", "nodep", "nlPitVolume", "nlPitDepth", "marineSolver", "picardSub", "picardIts"):
             if k in params:
                 arrs["p_" + k] = np.array(params[k])
         for i, s in enumerate(snaps):

@@ -269,7 +269,7 @@ class KSP:
 
     def solve(self, b, x):
         A = self.Aop.A
-        if getattr(self, "prefix", "") in ("hilllin_", "spl_ed_"):
+        if getattr(self, "prefix", "") in ("hilllin_", "spl_ed_", "marpicard_"):
             x.a[:] = spla.spsolve(A.tocsc(), b.a)
         else:
             sol, _ = exact_solve(A, b.a)
@@ -338,6 +338,7 @@ def _petsc_module():
     PETSc.KSP = KSP
     PETSc.Options = lambda _o=_Options(): _o
     PETSc.NormType = types.SimpleNamespace(FROBENIUS=3)
+    PETSc.InsertMode = types.SimpleNamespace(ADD_VALUES=1, INSERT_VALUES=0)
     petsc4py = types.ModuleType("petsc4py")
     petsc4py.PETSc = PETSc
     petsc4py.init = lambda *a, **k: None
@@ -440,9 +441,9 @@ def load_reference(refroot):
     fort = types.ModuleType("gospl._fortran")
     for name in ("mfdreceivers", "sethillslopecoeff", "edge_tile", "fill_tile", "fill_edges",
                  "fill_dir", "nghb_dir", "getpitvol", "pits_cons", "fill_depressions",
-                 "graph_nodes", "combine_edges", "label_pits", "setmaxnb"):
+                 "graph_nodes", "combine_edges", "label_pits", "setmaxnb", "jacobiancoeff"):
         setattr(fort, name, getattr(F, name))
-    for name in ("sort_ids", "hillslp_nl", "jacobiancoeff", "fctcoeff"):
+    for name in ("sort_ids", "hillslp_nl", "fctcoeff"):
         setattr(fort, name, lambda *a, **k: (_ for _ in ()).throw(NotImplementedError(name)))
     gospl_dir = os.path.join(refroot, "gospl")
     for pkg in ("gospl", "gospl.flow", "gospl.eroder", "gospl.sed", "gospl.tools"):
@@ -551,6 +552,11 @@ def make_model_class(refroot):
             self.lcoords = np.asarray(mesh["coords"], dtype=np.float64).reshape(-1, 3)
             self.nl_pit_volume = float(p.get("nlPitVolume", 1.0e9))
             self.nl_pit_depth = float(p.get("nlPitDepth", 100.0))
+            self.nl_pit_K = float(p.get("nlPitK", 10.0))
+            self.nl_pit_inlet_bias = float(p.get("pitInletBias", 0.5))
+            self.marineSolver = str(p.get("marineSolver", "ts"))
+            self.picardSub = int(p.get("picardSub", 10))
+            self.picardIts = int(p.get("picardIts", 2))
             FAMesh.__init__(self)
             PITFill.__init__(self)
             SPL.__init__(self)
