@@ -300,6 +300,20 @@ int gs_erodep_spl(gs_plan* plan, double* h, double* cum_ed, double* eb, const do
                                    wgt_i, lsink, sea, stats);)
 }
 
+int gs_plan_set_lake_diffusion(gs_plan* plan, double k, double inlet_bias, int32_t nsub, int32_t npic) {
+    NEED(plan);
+    if (!(k >= 0.0) || !(inlet_bias >= 0.0 && inlet_bias <= 1.0) || nsub < 0 || npic < 1) {
+        gs::set_error(GS_EINVAL, "lake diffusion: need K >= 0, 0 <= inlet_bias <= 1, nsub >= 0, npic >= 1");
+        return GS_EINVAL;
+    }
+    plan->lake_on = nsub > 0 ? 1 : 0;
+    plan->lake_K = k;
+    plan->lake_bias = inlet_bias;
+    plan->lake_nsub = nsub;
+    plan->lake_npic = npic;
+    return GS_OK;
+}
+
 int gs_sed_change(gs_plan* plan, double* h, double* cum_ed, const double* eb, const double* xyz, double sealevel,
                   double ofill, double dt, double nl_pit_volume, double nl_pit_depth, double* lfill,
                   int32_t* pit_ids, int32_t* flat_dirs, const int32_t* rcv_i, const double* wgt_i, uint8_t* lsink,

@@ -627,6 +627,53 @@ int hillslope(gs_plan* p, double* h, double* cum_ed, double* eb, double sealevel
     return GS_OK;
 }
 
+// Solve (I + L) x = rhs for an operator given as rows (diag, then one
+// coefficient per neighbour slot, [W+1][n], the hillslope layout), rows held
+// fixed as in the hillslope solve; the cooperative CG on the area-weighted
+// symmetric form.  Used by the non-linear lake diffusion of the sediment step.
+int diffusion_solve(gs_plan* p, const double* coef, const double* rhs, double* x, double rtol, int max_iter,
+                    int* iters) {
+    const int n = (int)p->n;
+    if (n == 0) return GS_OK;
+    const int B = 256, G = grid_for(n, B);
+    launch(p, k_cg_init, G, B, n, p->W, p->flat, (const int*)p->nbr, (const int8_t*)p->nnb, coef,
+           (const double*)p->farea, (const uint8_t*)p->outlet, rhs, p->cg_x, p->cg_b, p->cg_r, p->cg_z, p->cg_p);
+    GS_LAUNCH();
+    int* it_d = p->i_scalar + 12;
+    double* res_d = p->red + 4100;
+    {
+        int nn = n, mi = max_iter;
+        double rt = rtol;
+        const double* cf = coef;
+        void* args[] = {(void*)&nn, (void*)&p->nbr, (void*)&p->nnb, (void*)&cf, (void*)&p->farea,
+                        (void*)&p->dfix, (void*)&p->cg_b, (void*)&p->cg_x, (void*)&p->cg_r, (void*)&p->cg_z,
+                        (void*)&p->cg_p, (void*)&p->cg_ap, (void*)&p->red, (void*)&rt, (void*)&mi, (void*)&it_d,
+                        (void*)&res_d};
+        cudaEvent_t stop = nullptr;
+        if (p->profiling) prof_begin(p, (const void*)k_cg_coop, &stop);
+        GS_CUDA(cudaLaunchCooperativeKernel((const void*)k_cg_coop, p->coop_blocks, 256, args, 0, p->stream));
+        if (stop) cudaEventRecord(stop, p->stream);
+        p->launches++;
+    }
+    launch(p, k_copy_d2, G, B, n, (const double*)p->cg_x, x);
+    GS_LAUNCH();
+    int it = 0;
+    double relres = 0.0;
+    GS_CUDA(cudaMemcpyAsync(&it, it_d, sizeof(int), cudaMemcpyDeviceToHost, p->stream));
+    GS_CUDA(cudaMemcpyAsync(&relres, res_d, sizeof(double), cudaMemcpyDeviceToHost, p->stream));
+    GS_CUDA(cudaStreamSynchronize(p->stream));
+    if (iters) *iters = it;
+    if (!(relres == relres)) {
+        set_error(GS_ENONFINITE, "diffusion CG produced a non-finite residual");
+        return GS_ENONFINITE;
+    }
+    if (relres > rtol) {
+        set_error(GS_EMAXITER, "diffusion CG reached max_iter");
+        return GS_EMAXITER;
+    }
+    return GS_OK;
+}
+
 // ---------------------------------------------------------------------------
 // Adjoint of hillslope().  Forward: fixed rows F^c (flat outlets, zero area)
 // keep x = h; free rows solve S_FF x_F = A_F h_F - S_FX h_X with S = A (I+L)

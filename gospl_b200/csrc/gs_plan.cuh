@@ -26,8 +26,15 @@ struct gs_plan {
     double ed_relres = 0.0;              // its final relative residual
     double* ed_buf = nullptr;            // [6][n] coupled-solve scratch
     double* ed_basis = nullptr;          // GMRES basis [31][n] and reduction scratch
-    double* sed_buf = nullptr;           // [8][n] sediment-routing scratch
-    uint8_t* sed_mask = nullptr;         // [2][n] sediment-routing masks
+    double* sed_buf = nullptr;           // [10][n] sediment-routing scratch
+    uint8_t* sed_mask = nullptr;         // [5][n] sediment-routing masks
+    double* sed_pit = nullptr;           // [2][n+1] per-depression scratch
+    double* sed_coef = nullptr;          // [W+1][n] lake diffusion operator
+    int lake_on = 0;                     // lake deposits of large deep pits by non-linear diffusion (Picard)
+    double lake_K = 10.0;                // its diffusivity (nlPitK)
+    double lake_bias = 0.5;              // share of the deposit piled at the inlets (pitInletBias)
+    int lake_nsub = 10;                  // backward-Euler sub-steps (picardSub)
+    int lake_npic = 2;                   // Picard updates per sub-step (picardIts)
     double refine_tol = 1.0e-10;         // max|r| / max|b| of every refined solve
     int64_t refine_iters = 0;            // refinement passes since the last reset
     float* f32a = nullptr;               // FP32 correction / CG vectors
@@ -283,6 +290,8 @@ int sed_change(gs_plan* p, double* h, double* cum_ed, const double* eb, const do
                double ofill, double dt, double nl_pit_volume, double nl_pit_depth, double* lfill, int* pit_ids,
                int* flat_dirs, const int* rcv_i, const double* wgt_i, uint8_t* lsink, const uint8_t* sea,
                double* vsed, gs_stats* st);
+int diffusion_solve(gs_plan* p, const double* coef, const double* rhs, double* x, double rtol, int max_iter,
+                    int* iters);
 int hillslope(gs_plan* p, double* h, double* cum_ed, double* eb, double sealevel, double cda,
               double cdm, double dt, double rtol, int max_iter, gs_stats* st);
 int apply_forces(gs_plan* p, double* h, const double* rain, const double* upsub, double dt,

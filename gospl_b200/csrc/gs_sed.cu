@@ -171,21 +171,24 @@ __device__ double interp6(double x, const double* xp, const double* fp) {
 // (sedplex.py:524-559, 1000-1014)
 __global__ void k_sed_depo(int np1, const double* __restrict__ params, const double* __restrict__ vol,
                            const double* __restrict__ fvol, const double* __restrict__ flvl, double nlv,
-                           double nld, uint8_t* sel, double* target, int* ndiffuse) {
+                           double nld, uint8_t* sel, double* target, double* pdepo, int* ndiffuse) {
     int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= np1) return;
     const double pv = params[3 * p], pd = params[3 * p + 2];
     double depo = pv - vol[p];
     if (depo < 0.0) depo = 0.0;
+    pdepo[p] = depo;
     const bool active = depo > 0.0;
     const bool full = active && depo >= pv - 1.0e-6;
     const bool partial = active && !full;
     const bool large = pv >= nlv && pd >= nld;
-    if (partial && large) atomicAdd(ndiffuse, 1);
+    const bool diffuse = partial && large;
+    if (diffuse) atomicAdd(ndiffuse, 1);
     const bool bottomup = full || (partial && !large);
-    sel[p] = bottomup ? 1 : 0;
+    // 1: bottom-up (paths 1, 2); 2: non-linear diffusion (path 3)
+    sel[p] = bottomup ? 1 : (diffuse ? 2 : 0);
     double t = -INFINITY;
-    if (bottomup && depo > 0.0) {
+    if ((bottomup || diffuse) && depo > 0.0) {
         double xp[6], fp[6];
         xp[0] = 0.0;
         fp[0] = params[3 * p + 1] - params[3 * p + 2];
@@ -220,14 +223,14 @@ __global__ void k_sed_delta(int n, const int* __restrict__ pit, const uint8_t* _
     if (i >= n) return;
     const int p = pit[i];
     double d = 0.0;
-    if (p >= 0 && sel[p]) {
+    if (p >= 0 && sel[p] == 1) {
         const double t = target[p], f = lfill[i];
         const double surf = t < f ? t : f;
         const double v = __dsub_rn(surf, hl[i]);
         d = v > 0.0 ? v : 0.0;
     }
     delta[i] = d;
-    const bool m = p >= 0 && sel[p] && d > 0.0;
+    const bool m = p >= 0 && sel[p] == 1 && d > 0.0;
     tmask[i] = m ? 1 : 0;
     double ds = 0.0;
     if (m) {
@@ -262,8 +265,8 @@ __global__ void k_sed_ones(int n, double* a) {
 // deposit joins h and cumED (sedplex.py:620-644, 1038-1043)
 __global__ void k_sed_apply(int n, const int* __restrict__ pit, const uint8_t* __restrict__ tmask,
                             const double* __restrict__ dist, const double* __restrict__ dsum,
-                            const double* __restrict__ dcnt, int tilt, const double* __restrict__ delta, double* h,
-                            double* cum) {
+                            const double* __restrict__ dcnt, int tilt, const double* __restrict__ delta,
+                            const double* __restrict__ ddiff, double* h, double* cum) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     double d = delta[i];
@@ -275,8 +278,180 @@ __global__ void k_sed_apply(int n, const int* __restrict__ pit, const uint8_t* _
         d = __dadd_rn(d, t);
         if (d < 0.0) d = 0.0;
     }
+    if (ddiff) d = __dadd_rn(d, ddiff[i]);
     cum[i] = cum[i] + d;
     h[i] = h[i] + d;
+}
+
+// ---- path 3: lake deposits smoothed by non-linear diffusion
+// (_diffuseLargePit sedplex.py:679-858 with _diffuseImplicitPicard
+// hillslope.py:988-1076)
+
+// cells of path-3 pits, and the inlets among them: cells receiving flow
+// (snapshot receivers) from a donor outside their pit (sedplex.py:646-677)
+__global__ void k_lake_cells(int n, const int* __restrict__ pit, const uint8_t* __restrict__ sel, uint8_t* lmask,
+                             uint8_t* inlet) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int p = pit[i];
+    lmask[i] = (p >= 0 && sel[p] == 2) ? 1 : 0;
+    inlet[i] = 0;
+}
+
+__global__ void k_lake_inlets(int n, int R, const int* __restrict__ pit, const uint8_t* __restrict__ sel,
+                              const int* __restrict__ rcv, uint8_t* inlet) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int pi = pit[i];
+    for (int k = 0; k < R; k++) {
+        const int r = rcv[(size_t)k * n + i];
+        if (r == i) continue;
+        const int pr = pit[r];
+        if (pr >= 0 && pr != pi && sel[pr] == 2) inlet[r] = 1;
+    }
+}
+
+// pits without an inlet pile their inlet share on their highest cell (the
+// first in id order among equals, as np.argmax)
+__global__ void __launch_bounds__(256) k_lake_top(int np1, const int* __restrict__ start,
+                                                  const int* __restrict__ counts, const int* __restrict__ cells,
+                                                  const uint8_t* __restrict__ sel, const double* __restrict__ hl,
+                                                  double* pcnt, uint8_t* inlet) {
+    __shared__ double sv[256];
+    __shared__ int si[256];
+    const int p = blockIdx.x;
+    if (p >= np1 || sel[p] != 2 || pcnt[p] > 0.0) return;
+    const int s0 = start[p], c = counts[p];
+    double bv = -INFINITY;
+    int bi = INT_MAX;
+    for (int t = threadIdx.x; t < c; t += 256) {
+        const double v = hl[cells[s0 + t]];
+        if (v > bv || (v == bv && t < bi)) { bv = v; bi = t; }
+    }
+    sv[threadIdx.x] = bv;
+    si[threadIdx.x] = bi;
+    __syncthreads();
+    for (int s2 = 128; s2 > 0; s2 >>= 1) {
+        if (threadIdx.x < s2) {
+            const double v = sv[threadIdx.x + s2];
+            const int i2 = si[threadIdx.x + s2];
+            if (v > sv[threadIdx.x] || (v == sv[threadIdx.x] && i2 < si[threadIdx.x])) {
+                sv[threadIdx.x] = v;
+                si[threadIdx.x] = i2;
+            }
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0 && si[0] != INT_MAX) {
+        inlet[cells[s0 + si[0]]] = 1;
+        pcnt[p] = 1.0;
+    }
+}
+
+// water depth under the deposit level and its area-weighted volume terms
+__global__ void k_lake_depth(int n, const int* __restrict__ pit, const uint8_t* __restrict__ lmask,
+                             const double* __restrict__ target, const double* __restrict__ hl,
+                             const double* __restrict__ larea, double* wd, double* wda) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double w = 0.0;
+    if (lmask[i]) {
+        const double v = __dsub_rn(target[pit[i]], hl[i]);
+        w = v > 0.0 ? v : 0.0;
+    }
+    wd[i] = w;
+    wda[i] = __dmul_rn(w, larea[i]);
+}
+
+// initial deposit: bathymetric share plus the inlet pile (sedplex.py:812-838)
+__global__ void k_lake_init(int n, const int* __restrict__ pit, const uint8_t* __restrict__ lmask,
+                            const uint8_t* __restrict__ inlet, const double* __restrict__ wd,
+                            const double* __restrict__ denom, const double* __restrict__ pcnt,
+                            const double* __restrict__ depo, const double* __restrict__ larea, double bias,
+                            const double* __restrict__ zb, double* hcur) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double d = 0.0;
+    const int p = pit[i];
+    if (lmask[i]) {
+        const double dn = denom[p];
+        if (dn > 0.0) d = __ddiv_rn(__dmul_rn(__dmul_rn(1.0 - bias, depo[p]), wd[i]), dn > 1e-30 ? dn : 1e-30);
+        if (inlet[i] && pcnt[p] > 0.0) {
+            const double b = dn > 0.0 ? bias : 1.0;
+            d = __dadd_rn(d, __ddiv_rn(__dmul_rn(b, depo[p]), __dmul_rn(pcnt[p], larea[i])));
+        }
+    }
+    hcur[i] = __dadd_rn(d, zb[i]);
+}
+
+// diffusivity of the deposit: C_d = minDiff + K (1 - exp(-dexp dh)), dh below
+// 0.1 m counted as 0, on the lake cells only (hillslope.py:1046-1051)
+__global__ void k_lake_cd(int n, const uint8_t* __restrict__ lmask, const double* __restrict__ hcur,
+                          const double* __restrict__ zb, double K, double dexp, double mind, double* cd) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double c = 0.0;
+    if (lmask[i]) {
+        double dd = __dsub_rn(hcur[i], zb[i]);
+        if (dd < 0.1) dd = 0.0;
+        c = __dadd_rn(mind, __dmul_rn(K, __dsub_rn(1.0, exp(__dmul_rn(-dexp, dd)))));
+    }
+    cd[i] = c;
+}
+
+// rows of I + dt_sub L(C_d): jacobiancoeff with Kp = 0 (functions.F90:1423-1467),
+// faces closed where either side has no diffusivity
+__global__ void k_lake_rows(int n, int W, const int* __restrict__ nbr, const int8_t* __restrict__ nnb,
+                            const double* __restrict__ elen, const double* __restrict__ vdist,
+                            const double* __restrict__ farea, const double* __restrict__ cd, double dts, double* coef) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    for (int s = 0; s < W; s++) coef[(size_t)(s + 1) * n + k] = 0.0;
+    double dg = 0.0;
+    const double ak = farea[k];
+    if (ak > 0.0) {
+        const double ck = cd[k];
+        for (int s = 0; s < nnb[k]; s++) {
+            const double vd = vdist[(size_t)s * n + k];
+            if (!(vd > 0.0)) continue;
+            const int j = nbr[(size_t)s * n + k];
+            const double cn = cd[j];
+            if (ck > 0.0 && cn > 0.0) {
+                const double c = __ddiv_rn(__dmul_rn(0.5, __dadd_rn(ck, cn)), ak);
+                const double v = __ddiv_rn(__dmul_rn(c, vd), elen[(size_t)s * n + k]);
+                dg = __dadd_rn(dg, v);
+                coef[(size_t)(s + 1) * n + k] = __dmul_rn(dts, -v);
+            }
+        }
+    }
+    coef[k] = __dadd_rn(__dmul_rn(dts, dg), 1.0);
+}
+
+// smoothed deposit (clipped at 0) and its area-weighted volume terms
+__global__ void k_lake_depo(int n, const uint8_t* __restrict__ lmask, const double* __restrict__ hcur,
+                            const double* __restrict__ zb, const double* __restrict__ larea, double* nd, double* nda) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double v = __dsub_rn(hcur[i], zb[i]);
+    if (v < 0.0) v = 0.0;
+    nd[i] = v;
+    nda[i] = lmask[i] ? __dmul_rn(v, larea[i]) : 0.0;
+}
+
+// per-pit rescale to the deposited volume (sedplex.py:842-857)
+__global__ void k_lake_scale(int n, const int* __restrict__ pit, const uint8_t* __restrict__ lmask,
+                             const double* __restrict__ nd, const double* __restrict__ actual,
+                             const double* __restrict__ depo, double* ddiff) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double d = 0.0;
+    if (lmask[i]) {
+        const int p = pit[i];
+        const double a = actual[p];
+        const double sc = a > 0.0 ? __ddiv_rn(depo[p], a > 1e-30 ? a : 1e-30) : 1.0;
+        d = __dmul_rn(nd[i], sc);
+    }
+    ddiff[i] = d;
 }
 
 __global__ void k_sed_pitfinal(int np1, const double* __restrict__ vol, double* params) {
@@ -293,8 +468,8 @@ int sed_change(gs_plan* p, double* h, double* cum_ed, const double* eb, const do
     const int n = (int)p->n;
     if (n == 0) return GS_OK;
     const int B = 256, G = grid_for(n, B);
-    if (!p->sed_buf) GS_CUDA(cudaMalloc((void**)&p->sed_buf, sizeof(double) * (size_t)n * 8));
-    if (!p->sed_mask) GS_CUDA(cudaMalloc((void**)&p->sed_mask, (size_t)n * 3));
+    if (!p->sed_buf) GS_CUDA(cudaMalloc((void**)&p->sed_buf, sizeof(double) * (size_t)n * 10));
+    if (!p->sed_mask) GS_CUDA(cudaMalloc((void**)&p->sed_mask, (size_t)n * 5));
     double* vol = p->sed_buf;
     double* nv = vol + n;
     double* routed = nv + n;
@@ -303,6 +478,7 @@ int sed_change(gs_plan* p, double* h, double* cum_ed, const double* eb, const do
     double* sfill = hl + n;
     double* delta = sfill + n;
     double* dist = delta + n;
+    double* sed_extra = dist + n;   // [2][n]
     uint8_t* sea_s = p->sed_mask;
     uint8_t* tmask = sea_s + n;
     uint8_t* mout = tmask + n;   // [nmem] (nmem <= n)
@@ -429,10 +605,13 @@ int sed_change(gs_plan* p, double* h, double* cum_ed, const double* eb, const do
     GS_TRY(fill_join(p, st));
 
     // 4. deposits in the depressions
+    if (!p->sed_pit) GS_CUDA(cudaMalloc((void**)&p->sed_pit, sizeof(double) * ((size_t)n + 1) * 2));
+    double* pdepo = p->sed_pit;
+    double* pcnt = pdepo + (n + 1);
     GS_CUDA(cudaMemsetAsync(p->i_scalar + 11, 0, sizeof(int), p->stream));
     launch(p, k_sed_depo, grid_for(np1, B), B, np1, (const double*)p->pit_params, (const double*)p->pit_vol,
            (const double*)p->filled_vol, (const double*)p->filled_lvl, nl_pit_volume, nl_pit_depth, p->pit_state,
-           p->pit_lvl, p->i_scalar + 11);
+           p->pit_lvl, pdepo, p->i_scalar + 11);
     GS_LAUNCH();
     int ndiff = 0;
     GS_CUDA(cudaMemcpyAsync(&ndiff, p->i_scalar + 11, sizeof(int), cudaMemcpyDeviceToHost, p->stream));
@@ -444,22 +623,73 @@ int sed_change(gs_plan* p, double* h, double* cum_ed, const double* eb, const do
         st->cycle_nodes = total_cycles;
         st->status = ndiff;
     }
-    if (ndiff > 0) {
+    if (ndiff > 0 && !p->lake_on) {
         set_error(GS_EINVAL, "sedChange: " + std::to_string(ndiff) +
                                  " partly filled depressions reach nlPitVolume and nlPitDepth (deposit smoothed "
-                                 "by non-linear diffusion), which is not built");
+                                 "by non-linear diffusion): built for marineSolver picard only");
         return GS_EINVAL;
     }
+    // sediment kept at closed terminal sinks (sedplex.py:486-500)
     launch(p, k_sed_closed, G, B, n, (const double*)closed, (const double*)p->larea, h, cum_ed);
+    launch(p, k_sed_ones, G, B, n, routed);
     GS_LAUNCH();
+    double* ddiff = nullptr;
+    if (ndiff > 0) {
+        // path 3 on the surface after the closed-sink deposits (zb = h)
+        uint8_t* lmask = mout + n;
+        uint8_t* inlet = lmask + n;
+        double* hcur = vol;
+        double* hstart = nv;
+        double* cd = closed;
+        double* wd = sfill;
+        double* wda = sed_extra;
+        ddiff = sed_extra + n;
+        const double* zb = h;
+        if (!p->sed_coef)
+            GS_CUDA(cudaMalloc((void**)&p->sed_coef, sizeof(double) * (size_t)n * (size_t)(p->W + 1)));
+        launch(p, k_lake_cells, G, B, n, (const int*)pit_ids, (const uint8_t*)p->pit_state, lmask, inlet);
+        launch(p, k_lake_inlets, G, B, n, p->R, (const int*)pit_ids, (const uint8_t*)p->pit_state, rcv_i, inlet);
+        GS_LAUNCH();
+        GS_TRY(group_sum_by_pit(p, pit_ids, inlet, routed, pcnt, P));
+        launch(p, k_lake_top, np1, 256, np1, (const int*)p->seg_start, (const int*)p->seg_count,
+               (const int*)p->seg_vals2, (const uint8_t*)p->pit_state, (const double*)hl, pcnt, inlet);
+        launch(p, k_lake_depth, G, B, n, (const int*)pit_ids, (const uint8_t*)lmask, (const double*)p->pit_lvl,
+               (const double*)hl, (const double*)p->larea, wd, wda);
+        GS_LAUNCH();
+        GS_TRY(group_sum_by_pit(p, pit_ids, lmask, wda, p->pit_in, P));
+        launch(p, k_lake_init, G, B, n, (const int*)pit_ids, (const uint8_t*)lmask, (const uint8_t*)inlet,
+               (const double*)wd, (const double*)p->pit_in, (const double*)pcnt, (const double*)pdepo,
+               (const double*)p->larea, p->lake_bias, zb, hcur);
+        GS_LAUNCH();
+        const double dts = dt / p->lake_nsub;
+        for (int sub = 0; sub < p->lake_nsub; sub++) {
+            GS_CUDA(cudaMemcpyAsync(hstart, hcur, sizeof(double) * n, cudaMemcpyDeviceToDevice, p->stream));
+            for (int it = 0; it < p->lake_npic; it++) {
+                launch(p, k_lake_cd, G, B, n, (const uint8_t*)lmask, (const double*)hcur, zb, p->lake_K, 0.05, 1.0e-4,
+                       cd);
+                launch(p, k_lake_rows, G, B, n, p->W, (const int*)p->nbr, (const int8_t*)p->nnb,
+                       (const double*)p->elen, (const double*)p->vdist, (const double*)p->farea, (const double*)cd,
+                       dts, p->sed_coef);
+                GS_LAUNCH();
+                GS_TRY(diffusion_solve(p, p->sed_coef, hstart, hcur, 1.0e-13, 5000, nullptr));
+            }
+        }
+        launch(p, k_lake_depo, G, B, n, (const uint8_t*)lmask, (const double*)hcur, zb, (const double*)p->larea, wd,
+               wda);
+        GS_LAUNCH();
+        GS_TRY(group_sum_by_pit(p, pit_ids, lmask, wda, p->pit_ev, P));
+        launch(p, k_lake_scale, G, B, n, (const int*)pit_ids, (const uint8_t*)lmask, (const double*)wd,
+               (const double*)p->pit_ev, (const double*)pdepo, ddiff);
+        GS_LAUNCH();
+    }
     launch(p, k_sed_delta, G, B, n, (const int*)pit_ids, (const uint8_t*)p->pit_state, (const double*)p->pit_lvl,
            (const double*)lfill, (const double*)hl, xyz, (const int*)p->pit_info, delta, dist, tmask);
-    launch(p, k_sed_ones, G, B, n, routed);
     GS_LAUNCH();
     GS_TRY(group_sum_by_pit(p, pit_ids, tmask, dist, p->pit_in, P));
     GS_TRY(group_sum_by_pit(p, pit_ids, tmask, routed, p->pit_ev, P));
     launch(p, k_sed_apply, G, B, n, (const int*)pit_ids, (const uint8_t*)tmask, (const double*)dist,
-           (const double*)p->pit_in, (const double*)p->pit_ev, 1, (const double*)delta, h, cum_ed);
+           (const double*)p->pit_in, (const double*)p->pit_ev, 1, (const double*)delta, (const double*)ddiff, h,
+           cum_ed);
     launch(p, k_sed_pitfinal, grid_for(np1, B), B, np1, (const double*)p->pit_vol, p->pit_params);
     GS_LAUNCH();
     return GS_OK;

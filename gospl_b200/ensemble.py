@@ -31,7 +31,7 @@ from .mesh import FVMesh
 from .model import Model
 
 COMMON = ("dt", "tStart", "tEnd", "flowDir", "d", "m", "Cda", "Cdm", "sealevel", "oFill", "nodep", "nlPitVolume",
-          "nlPitDepth")
+          "nlPitDepth", "nlPitK", "pitInletBias", "picardSub", "picardIts")
 
 
 def partition(sizes, world):

@@ -11,7 +11,9 @@ uses, with goSPL's names, defaults and errors (gospl/tools/inputparser.py):
 * ``time``: ``start``, ``end``, ``dt`` required, ``tout`` (:343-404);
 * ``spl``: ``K``, ``d`` (0), ``m`` (0.5), ``G`` (0) (:454-496);
 * ``diffusion``: ``hillslopeKa``, ``hillslopeKm``, ``oFill`` (-6000) (:498-545),
-  ``nlPitVolume`` (1e9), ``nlPitDepth`` (100) (:546-590);
+  ``nlPitVolume`` (1e9), ``nlPitDepth`` (100), ``nonlinKm``/``nlPitK`` (10),
+  ``pitInletBias`` (0.10; 0.50 without the section), ``marineSolver`` (ts),
+  ``picardSub`` (10), ``picardIts`` (2) (:546-593);
 * ``sea``: ``position`` (default 0, :710-787);
 * ``climate``: events with ``start`` and ``uniform`` or ``map: [file, key]``
   (:1352-1520);
@@ -115,9 +117,16 @@ def read_input(filename):
         p["oFill"] = float(hill.get("oFill", -6000.0))
         p["nlPitVolume"] = float(hill.get("nlPitVolume", 1.0e9))
         p["nlPitDepth"] = float(hill.get("nlPitDepth", 100.0))
+        p["nlPitK"] = float(hill.get("nlPitK", hill.get("nonlinKm", 10.0)))
+        p["pitInletBias"] = float(hill.get("pitInletBias", 0.10))
+        p["marineSolver"] = str(hill.get("marineSolver", "ts")).lower()
+        p["picardSub"] = int(hill.get("picardSub", 10))
+        p["picardIts"] = int(hill.get("picardIts", 2))
     else:
         p["Cda"], p["Cdm"], p["oFill"] = 0.0, 0.0, -6000.0
         p["nlPitVolume"], p["nlPitDepth"] = 1.0e9, 100.0
+        p["nlPitK"], p["pitInletBias"], p["marineSolver"] = 10.0, 0.50, "ts"
+        p["picardSub"], p["picardIts"] = 10, 2
 
     sea = inp.get("sea") or {}
     if "curve" in sea:

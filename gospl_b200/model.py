@@ -47,8 +47,10 @@ class Model:
     (``Model(coords=..., cells=..., elev=..., params=...)``).  ``params`` keys:
     dt, tStart, tEnd, flowDir, K (scalar or per-vertex), d, m, G, Cda, Cdm, oFill,
     sealevel, bc, rain (per-vertex m/yr), upsub (per-vertex m/yr or None),
-    nodep (default True: no continental deposition), nlPitVolume (1e9 m3) and
-    nlPitDepth (100 m).
+    nodep (default True: no continental deposition), nlPitVolume (1e9 m3),
+    nlPitDepth (100 m), and for the lake deposits of large deep depressions
+    marineSolver ("picard" builds them; goSPL's default "ts" is refused when
+    they occur), nlPitK (10), pitInletBias (0.5), picardSub (10), picardIts (2).
     ``members`` = (start, maxarea) declares the mesh a disjoint union of
     landscapes (``gospl_b200.ensemble``).  ``precision=32`` selects the FP32
     sweeps and CG with FP64 refinement to ``refine_tol``.
@@ -93,6 +95,13 @@ class Model:
             raise NotImplementedError("marine deposition (seaChange, seadepo) is not built")
         self.nl_pit_volume = float(p.get("nlPitVolume", 1.0e9))    # inputparser.py:562,584
         self.nl_pit_depth = float(p.get("nlPitDepth", 100.0))      # inputparser.py:563,585
+        # lake deposits of large deep depressions: marineSolver picard
+        # (inputparser.py:564-580); goSPL's default adaptive TS is not built
+        self.marineSolver = str(p.get("marineSolver", "ts")).lower()
+        self.nl_pit_K = float(p.get("nlPitK", p.get("nonlinKm", 10.0)))
+        self.nl_pit_inlet_bias = min(1.0, max(0.0, float(p.get("pitInletBias", 0.5))))
+        self.picardSub = int(p.get("picardSub", 10))
+        self.picardIts = int(p.get("picardIts", 2))
         self.cg_rtol = cg_rtol
         self.cg_maxit = cg_maxit
         self.stats = {}
@@ -153,6 +162,9 @@ class Model:
         self._plan = handle
         self.stream = torch.cuda.current_stream(self.dev)
         _lib.check(L.gs_plan_set_stream(self._plan, ctypes.c_void_p(self.stream.cuda_stream)))
+        if not self.nodep and self.marineSolver == "picard":
+            _lib.check(L.gs_plan_set_lake_diffusion(self._plan, self.nl_pit_K, self.nl_pit_inlet_bias,
+                                                     self.picardSub, self.picardIts))
         self.fDepa = float(p.get("G", 0.0))
         if self.fDepa > 0.0:
             # transport-limited SPL (SPL.py:116-258, 305-336)

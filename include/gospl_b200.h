@@ -219,11 +219,24 @@ int gs_erodep_spl(gs_plan* plan, double* h, double* cum_ed, double* eb, const do
  * flat_dirs and the plan's pit tables, with pitParams volumes left to the
  * unfilled remainder) and lsink.  Partly filled depressions of at least
  * nl_pit_volume (m3) and nl_pit_depth (m), whose deposit goSPL smooths by
- * non-linear diffusion, return GS_EINVAL (stats.status = their count).
+ * non-linear diffusion, take gs_plan_set_lake_diffusion's path, or return
+ * GS_EINVAL when it is off (stats.status = their count).
  * Ensemble members (gs_plan_set_members) each run their own cascade, with
  * closed-domain deposits for members without an outlet.  stats: npits,
  * cascade passes and solves.
  */
+/*
+ * Lake deposits of large deep depressions (gs_sed_change path 3): goSPL's
+ * _diffuseLargePit (sedplex.py:679-858) with the lagged-diffusivity solver of
+ * marineSolver picard (_diffuseImplicitPicard, hillslope.py:988-1076): an
+ * inlet pile (share inlet_bias, pitInletBias) over a bathymetric baseline,
+ * nsub backward-Euler sub-steps (picardSub) of npic Picard updates each
+ * (picardIts) with diffusivity 1e-4 + k (1 - exp(-0.05 dh)) (nlPitK), then a
+ * per-pit rescale to the deposited volume.  nsub = 0 switches it off (the
+ * default: goSPL's default adaptive TS solver is not built, and those
+ * depressions make gs_sed_change return GS_EINVAL).
+ */
+int gs_plan_set_lake_diffusion(gs_plan* plan, double k, double inlet_bias, int32_t nsub, int32_t npic);
 int gs_sed_change(gs_plan* plan, double* h, double* cum_ed, const double* eb, const double* xyz,
                   double sealevel, double ofill, double dt, double nl_pit_volume, double nl_pit_depth,
                   double* lfill, int32_t* pit_ids, int32_t* flat_dirs, const int32_t* rcv_i,

@@ -105,8 +105,9 @@ def test_continental_deposition(bc):
 
 def test_lake_diffusion_path_rejected():
     """Partly filled depressions of at least nlPitVolume and nlPitDepth are
-    smoothed by non-linear diffusion in goSPL (sedplex.py:679-858); that path
-    is not built and must fail loudly, not deposit something else."""
+    smoothed by non-linear diffusion in goSPL (sedplex.py:679-858); with the
+    default adaptive TS solver that path is not built and must fail loudly,
+    not deposit something else (marineSolver picard builds it)."""
     import torch
     from gospl_b200 import _lib
     from gospl_b200.mesh import FVMesh
@@ -115,7 +116,7 @@ def test_lake_diffusion_path_rejected():
     params = dict(params, nodep=False, nlPitVolume=0.0, nlPitDepth=0.0)
     fv = FVMesh(coords, cells, params["bc"])
     gm = Model(coords=coords, cells=cells, elev=z, params=params, mesh=fv, device="cuda:0")
-    with pytest.raises(_lib.GsError, match="not built"):
+    with pytest.raises(_lib.GsError, match="marineSolver picard"):
         gm.step()
     torch.cuda.synchronize()
     gm.destroy()
@@ -127,4 +128,15 @@ def test_transport_limited_with_deposition():
     (sedplex.py:1061-1086)."""
     coords, cells, z, params = _planar(3000, 33, "ffff")
     params = dict(params, G=1.0, nodep=False)
+    _step_vs_oracle(coords, cells, z, params)
+
+
+@pytest.mark.parametrize("bc", ["ffff", "wwww"])
+def test_lake_diffusion_picard(bc):
+    """Path 3 of the lake deposits with marineSolver picard: every partly
+    filled depression (nlPitVolume = nlPitDepth = 0) gets the inlet pile, the
+    lagged-diffusivity sub-steps and the per-pit rescale, against the oracle."""
+    coords, cells, z, params = _planar(3000, 31, bc)
+    params = dict(params, nodep=False, nlPitVolume=0.0, nlPitDepth=0.0, marineSolver="picard", picardSub=3,
+                  picardIts=2)
     _step_vs_oracle(coords, cells, z, params)
