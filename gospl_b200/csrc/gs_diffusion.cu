@@ -633,11 +633,20 @@ int hillslope(gs_plan* p, double* h, double* cum_ed, double* eb, double sealevel
 // symmetric form.  Used by the non-linear lake diffusion of the sediment step.
 int diffusion_solve(gs_plan* p, const double* coef, const double* rhs, double* x, double rtol, int max_iter,
                     int* iters) {
-    const int n = (int)p->n;
+    return diffusion_solve_on(p, (int)p->n, p->nbr, p->nnb, p->farea, p->dfix, p->flat, p->outlet, coef, rhs, x, rtol,
+                              max_iter, iters);
+}
+
+// the same on a sub-mesh of m rows (slot-major [W][m] neighbours, -1 or a zero
+// coefficient where a neighbour lies outside)
+int diffusion_solve_on(gs_plan* p, int m, const int* nbr, const int8_t* nnb, const double* farea, const uint8_t* fix,
+                       int flat, const uint8_t* outlet, const double* coef, const double* rhs, double* x, double rtol,
+                       int max_iter, int* iters) {
+    const int n = m;
     if (n == 0) return GS_OK;
     const int B = 256, G = grid_for(n, B);
-    launch(p, k_cg_init, G, B, n, p->W, p->flat, (const int*)p->nbr, (const int8_t*)p->nnb, coef,
-           (const double*)p->farea, (const uint8_t*)p->outlet, rhs, p->cg_x, p->cg_b, p->cg_r, p->cg_z, p->cg_p);
+    launch(p, k_cg_init, G, B, n, p->W, flat, nbr, nnb, coef, farea, outlet, rhs, p->cg_x, p->cg_b, p->cg_r, p->cg_z,
+           p->cg_p);
     GS_LAUNCH();
     int* it_d = p->i_scalar + 12;
     double* res_d = p->red + 4100;
@@ -645,8 +654,8 @@ int diffusion_solve(gs_plan* p, const double* coef, const double* rhs, double* x
         int nn = n, mi = max_iter;
         double rt = rtol;
         const double* cf = coef;
-        void* args[] = {(void*)&nn, (void*)&p->nbr, (void*)&p->nnb, (void*)&cf, (void*)&p->farea,
-                        (void*)&p->dfix, (void*)&p->cg_b, (void*)&p->cg_x, (void*)&p->cg_r, (void*)&p->cg_z,
+        void* args[] = {(void*)&nn, (void*)&nbr, (void*)&nnb, (void*)&cf, (void*)&farea,
+                        (void*)&fix, (void*)&p->cg_b, (void*)&p->cg_x, (void*)&p->cg_r, (void*)&p->cg_z,
                         (void*)&p->cg_p, (void*)&p->cg_ap, (void*)&p->red, (void*)&rt, (void*)&mi, (void*)&it_d,
                         (void*)&res_d};
         cudaEvent_t stop = nullptr;

@@ -29,7 +29,10 @@ struct gs_plan {
     double* sed_buf = nullptr;           // [10][n] sediment-routing scratch
     uint8_t* sed_mask = nullptr;         // [5][n] sediment-routing masks
     double* sed_pit = nullptr;           // [2][n+1] per-depression scratch
-    double* sed_coef = nullptr;          // [W+1][n] lake diffusion operator
+    double* sed_coef = nullptr;          // [W+1][n] lake diffusion operator (compacted to the lake cells)
+    int* lake_i = nullptr;               // [W+1][n]: lake cell list, then the compact neighbour slots
+    double* lake_d = nullptr;            // [3][n]: compact cell areas, right-hand side, solution
+    uint8_t* lake_u8 = nullptr;          // [2][n]: compact neighbour counts, fixed rows
     int lake_on = 0;                     // lake deposits of large deep pits by non-linear diffusion (Picard)
     double lake_K = 10.0;                // its diffusivity (nlPitK)
     double lake_bias = 0.5;              // share of the deposit piled at the inlets (pitInletBias)
@@ -292,6 +295,9 @@ int sed_change(gs_plan* p, double* h, double* cum_ed, const double* eb, const do
                double* vsed, gs_stats* st);
 int diffusion_solve(gs_plan* p, const double* coef, const double* rhs, double* x, double rtol, int max_iter,
                     int* iters);
+int diffusion_solve_on(gs_plan* p, int m, const int* nbr, const int8_t* nnb, const double* farea, const uint8_t* fix,
+                       int flat, const uint8_t* outlet, const double* coef, const double* rhs, double* x, double rtol,
+                       int max_iter, int* iters);
 int hillslope(gs_plan* p, double* h, double* cum_ed, double* eb, double sealevel, double cda,
               double cdm, double dt, double rtol, int max_iter, gs_stats* st);
 int apply_forces(gs_plan* p, double* h, const double* rain, const double* upsub, double dt,

@@ -24,6 +24,8 @@
 //      spill point (_addPitMicroTilt, sedplex.py:561-644).  Path 3 (partly
 //      filled depressions of at least nlPitVolume and nlPitDepth, smoothed by
 //      non-linear diffusion) is reported as an error.
+#include <cub/cub.cuh>
+
 #include <string>
 #include <vector>
 
@@ -427,6 +429,70 @@ __global__ void k_lake_rows(int n, int W, const int* __restrict__ nbr, const int
     coef[k] = __dadd_rn(__dmul_rn(dts, dg), 1.0);
 }
 
+// the lake cells as a sub-mesh: faces to other cells carry no diffusivity,
+// so the rows outside are the identity and the solve decouples
+__global__ void k_lake_flag(int n, const uint8_t* __restrict__ lmask, int* flag) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) flag[i] = lmask[i] ? 1 : 0;
+}
+
+__global__ void k_lake_list(int n, const uint8_t* __restrict__ lmask, const int* __restrict__ lid, int* cell) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n && lmask[i]) cell[lid[i]] = i;
+}
+
+__global__ void k_lake_submesh(int m, int n, int W, const int* __restrict__ cell, const int* __restrict__ lid,
+                               const uint8_t* __restrict__ lmask, const int* __restrict__ nbr,
+                               const int8_t* __restrict__ nnb, const double* __restrict__ farea, int* nbr_c,
+                               int8_t* nnb_c, double* farea_c, uint8_t* fix_c) {
+    int li = blockIdx.x * blockDim.x + threadIdx.x;
+    if (li >= m) return;
+    const int i = cell[li];
+    nnb_c[li] = nnb[i];
+    farea_c[li] = farea[i];
+    fix_c[li] = farea[i] > 0.0 ? 0 : 1;
+    for (int s = 0; s < W; s++) {
+        const int j = nbr[(size_t)s * n + i];
+        nbr_c[(size_t)s * m + li] = (j >= 0 && lmask[j]) ? lid[j] : -1;
+    }
+}
+
+// rows of I + dt_sub L(C_d) for the lake cells (k_lake_rows restricted)
+__global__ void k_lake_rows_c(int m, int n, int W, const int* __restrict__ cell, const int* __restrict__ nbr,
+                              const int8_t* __restrict__ nnb, const double* __restrict__ elen,
+                              const double* __restrict__ vdist, const double* __restrict__ farea,
+                              const double* __restrict__ cd, double dts, const double* __restrict__ hstart,
+                              double* coef_c, double* rhs_c) {
+    int li = blockIdx.x * blockDim.x + threadIdx.x;
+    if (li >= m) return;
+    const int k = cell[li];
+    for (int s = 0; s < W; s++) coef_c[(size_t)(s + 1) * m + li] = 0.0;
+    double dg = 0.0;
+    const double ak = farea[k];
+    if (ak > 0.0) {
+        const double ck = cd[k];
+        for (int s = 0; s < nnb[k]; s++) {
+            const double vd = vdist[(size_t)s * n + k];
+            if (!(vd > 0.0)) continue;
+            const int j = nbr[(size_t)s * n + k];
+            const double cn = cd[j];
+            if (ck > 0.0 && cn > 0.0) {
+                const double c = __ddiv_rn(__dmul_rn(0.5, __dadd_rn(ck, cn)), ak);
+                const double v = __ddiv_rn(__dmul_rn(c, vd), elen[(size_t)s * n + k]);
+                dg = __dadd_rn(dg, v);
+                coef_c[(size_t)(s + 1) * m + li] = __dmul_rn(dts, -v);
+            }
+        }
+    }
+    coef_c[li] = __dadd_rn(__dmul_rn(dts, dg), 1.0);
+    rhs_c[li] = hstart[k];
+}
+
+__global__ void k_lake_scatter(int m, const int* __restrict__ cell, const double* __restrict__ x_c, double* hcur) {
+    int li = blockIdx.x * blockDim.x + threadIdx.x;
+    if (li < m) hcur[cell[li]] = x_c[li];
+}
+
 // smoothed deposit (clipped at 0) and its area-weighted volume terms
 __global__ void k_lake_depo(int n, const uint8_t* __restrict__ lmask, const double* __restrict__ hcur,
                             const double* __restrict__ zb, const double* __restrict__ larea, double* nd, double* nda) {
@@ -661,17 +727,56 @@ int sed_change(gs_plan* p, double* h, double* cum_ed, const double* eb, const do
                (const double*)wd, (const double*)p->pit_in, (const double*)pcnt, (const double*)pdepo,
                (const double*)p->larea, p->lake_bias, zb, hcur);
         GS_LAUNCH();
+        // the lake cells as a sub-mesh of m rows
+        const int W = p->W;
+        if (!p->lake_i) {
+            GS_CUDA(cudaMalloc((void**)&p->lake_i, sizeof(int) * (size_t)n * (size_t)(W + 1)));
+            GS_CUDA(cudaMalloc((void**)&p->lake_d, sizeof(double) * (size_t)n * 3));
+            GS_CUDA(cudaMalloc((void**)&p->lake_u8, (size_t)n * 2));
+        }
+        int* cell = p->lake_i;
+        int* nbr_c = cell + n;
+        double* farea_c = p->lake_d;
+        double* rhs_c = farea_c + n;
+        double* x_c = rhs_c + n;
+        int8_t* nnb_c = (int8_t*)p->lake_u8;
+        uint8_t* fix_c = p->lake_u8 + n;
+        launch(p, k_lake_flag, G, B, n, (const uint8_t*)lmask, p->flagbuf);
+        GS_LAUNCH();
+        {
+            size_t bytes = p->cub_bytes;
+            GS_CUDA(cub::DeviceScan::ExclusiveSum(p->cub_tmp, bytes, (const int*)p->flagbuf, p->scanbuf, n, p->stream));
+            p->launches++;
+        }
+        int last[2];
+        GS_CUDA(cudaMemcpyAsync(&last[0], p->scanbuf + n - 1, sizeof(int), cudaMemcpyDeviceToHost, p->stream));
+        GS_CUDA(cudaMemcpyAsync(&last[1], p->flagbuf + n - 1, sizeof(int), cudaMemcpyDeviceToHost, p->stream));
+        GS_CUDA(cudaStreamSynchronize(p->stream));
+        const int m = last[0] + last[1];
+        if (m == 0) {
+            set_error(GS_EINVAL, "sedChange: lake diffusion without lake cells");
+            return GS_EINVAL;
+        }
+        launch(p, k_lake_list, G, B, n, (const uint8_t*)lmask, (const int*)p->scanbuf, cell);
+        GS_LAUNCH();
+        launch(p, k_lake_submesh, grid_for(m, B), B, m, n, W, (const int*)cell, (const int*)p->scanbuf,
+               (const uint8_t*)lmask, (const int*)p->nbr, (const int8_t*)p->nnb, (const double*)p->farea, nbr_c, nnb_c,
+               farea_c, fix_c);
+        GS_LAUNCH();
         const double dts = dt / p->lake_nsub;
         for (int sub = 0; sub < p->lake_nsub; sub++) {
             GS_CUDA(cudaMemcpyAsync(hstart, hcur, sizeof(double) * n, cudaMemcpyDeviceToDevice, p->stream));
             for (int it = 0; it < p->lake_npic; it++) {
                 launch(p, k_lake_cd, G, B, n, (const uint8_t*)lmask, (const double*)hcur, zb, p->lake_K, 0.05, 1.0e-4,
                        cd);
-                launch(p, k_lake_rows, G, B, n, p->W, (const int*)p->nbr, (const int8_t*)p->nnb,
-                       (const double*)p->elen, (const double*)p->vdist, (const double*)p->farea, (const double*)cd,
-                       dts, p->sed_coef);
+                launch(p, k_lake_rows_c, grid_for(m, B), B, m, n, W, (const int*)cell, (const int*)p->nbr,
+                       (const int8_t*)p->nnb, (const double*)p->elen, (const double*)p->vdist, (const double*)p->farea,
+                       (const double*)cd, dts, (const double*)hstart, p->sed_coef, rhs_c);
                 GS_LAUNCH();
-                GS_TRY(diffusion_solve(p, p->sed_coef, hstart, hcur, 1.0e-13, 5000, nullptr));
+                GS_TRY(diffusion_solve_on(p, m, nbr_c, nnb_c, farea_c, fix_c, 0, nullptr, p->sed_coef, rhs_c, x_c,
+                                          1.0e-13, 5000, nullptr));
+                launch(p, k_lake_scatter, grid_for(m, B), B, m, (const int*)cell, (const double*)x_c, hcur);
+                GS_LAUNCH();
             }
         }
         launch(p, k_lake_depo, G, B, n, (const uint8_t*)lmask, (const double*)hcur, zb, (const double*)p->larea, wd,
