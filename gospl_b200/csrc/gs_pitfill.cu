@@ -1183,6 +1183,11 @@ int fill_elevation(gs_plan* p, const double* h, double sealevel, double ofill, d
         GS_LAUNCH();
     }
 
+    // With sediment the open-sea reset of lFill in k_flat_dirs touches pit
+    // cells (marine depressions are labelled), and the pit tables read the
+    // reset lFill (pitfilling.py:820-846): join the BFS first.
+    if (sed) GS_TRY(fill_join(p, st));
+
     // pit cells sorted by (pit, id): segments for the per-pit reductions.
     // Ordered compaction (scan) keeps id order; the stable radix sort by pit
     // then lists every pit's cells in increasing id.

@@ -553,6 +553,11 @@ int sed_change(gs_plan* p, double* h, double* cum_ed, const double* eb, const do
         launch(p, k_sed_moutlet, grid_for(p->n_outlet, B), B, p->n_outlet, (const int*)p->outlet_ids,
                (const int*)p->vmember, mout);
 
+    // 2. depressions of the eroded surface, filled with sediment (the flat
+    // directions and the open-sea reset of lFill are joined inside)
+    GS_TRY(fill_elevation(p, h, sealevel, ofill, lfill, pit_ids, flat_dirs, st, true, nullptr, true));
+    const int P = p->npits, np1 = P + 1;
+
     // 1. sediment flux over the snapshot graph of the last flow accumulation
     int cyc = 0, total_cycles = 0;
     launch(p, k_sed_rhs, G, B, n, eb, (const double*)p->larea, p->q2);
@@ -565,9 +570,6 @@ int sed_change(gs_plan* p, double* h, double* cum_ed, const double* eb, const do
     launch(p, k_sed_init, G, B, n, (const double*)vsed, (const double*)h, dt, vol, hl, sfill, closed);
     GS_LAUNCH();
 
-    // 2. depressions of the eroded surface, filled with sediment
-    GS_TRY(fill_elevation(p, h, sealevel, ofill, lfill, pit_ids, flat_dirs, st, true, nullptr, true));
-    const int P = p->npits, np1 = P + 1;
     launch(p, k_sed_pitvol, grid_for(np1, B), B, np1, (const double*)p->pit_params, p->pit_vol);
     GS_LAUNCH();
 
