@@ -380,6 +380,8 @@ int flow_accumulation(gs_plan* p, const double* h, const double* bl, double seal
             GS_LAUNCH();
             if (anybig) {
                 const double* surf = (step == 100) ? lfill : p->wf;
+                // lFill is final only after the flat pass (open-sea reset)
+                if (step == 100) GS_TRY(fill_join(p, st));
                 if (!allbig) {
                     GS_CUDA(cudaMemcpyAsync(p->lsink_prev, lsink, n, cudaMemcpyDeviceToDevice, p->stream));
                     GS_CUDA(cudaMemcpyAsync(p->mbig, big.data(), nm, cudaMemcpyHostToDevice, p->stream));
