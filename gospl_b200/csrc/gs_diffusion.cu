@@ -627,18 +627,12 @@ int hillslope(gs_plan* p, double* h, double* cum_ed, double* eb, double sealevel
     return GS_OK;
 }
 
-// Solve (I + L) x = rhs for an operator given as rows (diag, then one
-// coefficient per neighbour slot, [W+1][n], the hillslope layout), rows held
-// fixed as in the hillslope solve; the cooperative CG on the area-weighted
-// symmetric form.  Used by the non-linear lake diffusion of the sediment step.
-int diffusion_solve(gs_plan* p, const double* coef, const double* rhs, double* x, double rtol, int max_iter,
-                    int* iters) {
-    return diffusion_solve_on(p, (int)p->n, p->nbr, p->nnb, p->farea, p->dfix, p->flat, p->outlet, coef, rhs, x, rtol,
-                              max_iter, iters);
-}
-
-// the same on a sub-mesh of m rows (slot-major [W][m] neighbours, -1 or a zero
-// coefficient where a neighbour lies outside)
+// Solve (I + L) x = rhs on a sub-mesh of m rows given as rows (diag, then
+// one coefficient per neighbour slot, [W+1][m], the hillslope layout; slot-major
+// [W][m] neighbours, -1 or a zero coefficient where a neighbour lies outside),
+// rows without area held fixed as in the hillslope solve; the cooperative CG on
+// the area-weighted symmetric form.  Used by the non-linear lake diffusion of
+// the sediment step.
 int diffusion_solve_on(gs_plan* p, int m, const int* nbr, const int8_t* nnb, const double* farea, const uint8_t* fix,
                        int flat, const uint8_t* outlet, const double* coef, const double* rhs, double* x, double rtol,
                        int max_iter, int* iters) {

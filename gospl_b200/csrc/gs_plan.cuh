@@ -293,8 +293,6 @@ int sed_change(gs_plan* p, double* h, double* cum_ed, const double* eb, const do
                double ofill, double dt, double nl_pit_volume, double nl_pit_depth, double* lfill, int* pit_ids,
                int* flat_dirs, const int* rcv_i, const double* wgt_i, uint8_t* lsink, const uint8_t* sea,
                double* vsed, gs_stats* st);
-int diffusion_solve(gs_plan* p, const double* coef, const double* rhs, double* x, double rtol, int max_iter,
-                    int* iters);
 int diffusion_solve_on(gs_plan* p, int m, const int* nbr, const int8_t* nnb, const double* farea, const uint8_t* fix,
                        int flat, const uint8_t* outlet, const double* coef, const double* rhs, double* x, double rtol,
                        int max_iter, int* iters);

@@ -401,34 +401,6 @@ __global__ void k_lake_cd(int n, const uint8_t* __restrict__ lmask, const double
     cd[i] = c;
 }
 
-// rows of I + dt_sub L(C_d): jacobiancoeff with Kp = 0 (functions.F90:1423-1467),
-// faces closed where either side has no diffusivity
-__global__ void k_lake_rows(int n, int W, const int* __restrict__ nbr, const int8_t* __restrict__ nnb,
-                            const double* __restrict__ elen, const double* __restrict__ vdist,
-                            const double* __restrict__ farea, const double* __restrict__ cd, double dts, double* coef) {
-    int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= n) return;
-    for (int s = 0; s < W; s++) coef[(size_t)(s + 1) * n + k] = 0.0;
-    double dg = 0.0;
-    const double ak = farea[k];
-    if (ak > 0.0) {
-        const double ck = cd[k];
-        for (int s = 0; s < nnb[k]; s++) {
-            const double vd = vdist[(size_t)s * n + k];
-            if (!(vd > 0.0)) continue;
-            const int j = nbr[(size_t)s * n + k];
-            const double cn = cd[j];
-            if (ck > 0.0 && cn > 0.0) {
-                const double c = __ddiv_rn(__dmul_rn(0.5, __dadd_rn(ck, cn)), ak);
-                const double v = __ddiv_rn(__dmul_rn(c, vd), elen[(size_t)s * n + k]);
-                dg = __dadd_rn(dg, v);
-                coef[(size_t)(s + 1) * n + k] = __dmul_rn(dts, -v);
-            }
-        }
-    }
-    coef[k] = __dadd_rn(__dmul_rn(dts, dg), 1.0);
-}
-
 // the lake cells as a sub-mesh: faces to other cells carry no diffusivity,
 // so the rows outside are the identity and the solve decouples
 __global__ void k_lake_flag(int n, const uint8_t* __restrict__ lmask, int* flag) {
@@ -457,7 +429,9 @@ __global__ void k_lake_submesh(int m, int n, int W, const int* __restrict__ cell
     }
 }
 
-// rows of I + dt_sub L(C_d) for the lake cells (k_lake_rows restricted)
+// rows of I + dt_sub L(C_d) for the lake cells: jacobiancoeff with Kp = 0
+// (functions.F90:1423-1467), faces closed where either side has no
+// diffusivity
 __global__ void k_lake_rows_c(int m, int n, int W, const int* __restrict__ cell, const int* __restrict__ nbr,
                               const int8_t* __restrict__ nnb, const double* __restrict__ elen,
                               const double* __restrict__ vdist, const double* __restrict__ farea,
