@@ -56,6 +56,13 @@ def test_reads_the_path_keys(tmp_path):
     assert (p["Cda"], p["Cdm"], p["oFill"], p["sealevel"]) == (0.01, 0.2, -6000.0, -100.0)
     assert np.all(p["rain"] == 1.0) and np.allclose(p["upsub"], 1e-3)
     assert (p["nodep"], p["seadepo"], p["nlPitVolume"], p["nlPitDepth"]) == (False, False, 1.0e9, 100.0)
+    # lake diffusion keys of the diffusion section (inputparser.py:546-593)
+    assert (p["nlPitK"], p["pitInletBias"], p["marineSolver"], p["picardSub"], p["picardIts"]) == \
+        (10.0, 0.10, "ts", 10, 2)
+    y, _ = _write(tmp_path, YML.replace("    hillslopeKm: 0.2\n", "    hillslopeKm: 0.2\n    nonlinKm: 4.0\n"
+                                        "    marineSolver: Picard\n    picardSub: 3\n"))
+    q = read_input(str(y))[3]
+    assert (q["nlPitK"], q["marineSolver"], q["picardSub"]) == (4.0, "picard", 3)
 
 
 def test_marine_deposition_is_refused(tmp_path):
