@@ -30,7 +30,7 @@ import numpy as np
 from .mesh import FVMesh
 from .model import Model
 
-COMMON = ("dt", "tStart", "tEnd", "flowDir", "d", "m", "Cda", "Cdm", "sealevel", "oFill", "nodep", "nlPitVolume",
+COMMON = ("dt", "tStart", "tEnd", "flowDir", "d", "m", "G", "Cda", "Cdm", "sealevel", "oFill", "nodep", "nlPitVolume",
           "nlPitDepth", "nlPitK", "pitInletBias", "picardSub", "picardIts")
 
 

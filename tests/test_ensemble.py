@@ -73,16 +73,18 @@ def test_two_rank_partition_gloo():
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("nodep", [True, False])
-def test_members_evolve_as_alone(nodep):
+@pytest.mark.parametrize("nodep,G", [(True, 0.0), (False, 0.0), (True, 1.0)])
+def test_members_evolve_as_alone(nodep, G):
     """Each member of an ensemble evolves as it would alone, with and without
-    continental deposition (each member its own flow and sediment cascade)."""
+    continental deposition (each member its own flow and sediment cascade) and
+    with transport-limited erosion (one coupled solve for all members, to the
+    solver's tolerance)."""
     import torch
     from gospl_b200.ensemble import Ensemble
     from gospl_b200.model import Model
 
     members = [S.ensemble_member(n, seed) for n, seed in ((2500, 11), (4000, 12), (6000, 13))]
-    members = [(c, f, z, r, u, dict(p, nodep=nodep)) for c, f, z, r, u, p in members]
+    members = [(c, f, z, r, u, dict(p, nodep=nodep, G=G)) for c, f, z, r, u, p in members]
     ens = Ensemble(members)
     dev = torch.device("cuda", torch.cuda.current_device())
     alone = []
@@ -90,7 +92,9 @@ def test_members_evolve_as_alone(nodep):
         m = Model(coords=c, cells=f, elev=z, params=dict(p, rain=rain, upsub=up),
                   mesh=FVMesh(c, f, p["bc"], device=dev))
         alone.append(m)
-    for step in range(3):
+    # with G > 0 one step: the members' solutions differ from the solo runs at
+    # the solver's tolerance, which later discrete decisions may amplify
+    for step in range(3 if G == 0.0 else 1):
         ens.step()
         for m in alone:
             m.step()
@@ -111,7 +115,8 @@ def test_members_evolve_as_alone(nodep):
                 a = ens.view(getattr(ens.model, name), k).cpu().numpy()
                 b = getattr(m, name).cpu().numpy()
                 scale = max(np.abs(b).max(), 1.0) if name in ("FAL", "vSed") else hscale
-                assert np.abs(a - b).max() <= 1e-12 * scale, (step, k, name, np.abs(a - b).max())
+                tol = 1e-12 if G == 0.0 else 1e-10
+                assert np.abs(a - b).max() <= tol * scale, (step, k, name, np.abs(a - b).max())
     for m in alone:
         m.destroy()
     ens.destroy()
