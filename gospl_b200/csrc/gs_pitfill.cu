@@ -728,10 +728,13 @@ __global__ void k_basin_stamp(int n, const unsigned long long* __restrict__ L, i
     if (v < n) stamp[v] = (L[v] != ~0ULL) ? 0 : -1;
 }
 
-__global__ void __launch_bounds__(256) k_relax_active(int m, const int* __restrict__ xu, const int* __restrict__ xv,
+__global__ void __launch_bounds__(256) k_relax_active(const int* __restrict__ m_count, int cap,
+                                                      const int* __restrict__ xu, const int* __restrict__ xv,
                                                       const double* __restrict__ xw, unsigned long long* L,
                                                       int* stamp, int* flags, int max_rounds, int* rounds_out) {
     cg::grid_group grid = cg::this_grid();
+    // edge count as k_cross_edges left it (its appends stop at the capacity)
+    const int m = *m_count < cap ? *m_count : cap;
     const int gtid = blockIdx.x * blockDim.x + threadIdx.x, gsz = gridDim.x * blockDim.x;
     int r = 1;
     for (; r <= max_rounds; r++) {
@@ -1032,24 +1035,24 @@ int fill_elevation(gs_plan* p, const double* h, double sealevel, double ofill, d
            (const int8_t*)p->nnb, (const int8_t*)p->ledge, (const int*)p->parent, p->xe_u, p->xe_v,
            p->xe_w, p->i_scalar + I_NEXT, p->xe_cap);
     GS_LAUNCH();
-    GS_TRY(read_ints(p, hbuf, p->i_scalar + I_NEXT, 1));
-    const int64_t m = hbuf[0];
-    if (m > p->xe_cap) { set_error(GS_ENOMEM, "pit fill: cross-edge capacity exceeded"); return GS_ENOMEM; }
-    int rounds = 0;
     {
+        // the edge count stays on the device: the relaxation reads it, and the
+        // host checks it against the capacity at the next synchronisation
         launch(p, k_basin_stamp, G, B, n, (const unsigned long long*)p->basinL, p->comp);
         GS_CUDA(cudaMemsetAsync(p->i_scalar + 5, 0, sizeof(int) * 3, p->stream));
         GS_LAUNCH();
-        int mm = (int)m, maxr = 1000000;
+        const int* mc = p->i_scalar + I_NEXT;
+        int cap = (int)std::min<int64_t>(p->xe_cap, INT_MAX), maxr = 1000000;
         int* flags = p->i_scalar + 5;
         int* rout = p->i_scalar + I_CHANGED;
-        void* args[] = {(void*)&mm, (void*)&p->xe_u, (void*)&p->xe_v, (void*)&p->xe_w, (void*)&p->basinL,
-                        (void*)&p->comp, (void*)&flags, (void*)&maxr, (void*)&rout};
+        void* args[] = {(void*)&mc, (void*)&cap, (void*)&p->xe_u, (void*)&p->xe_v, (void*)&p->xe_w,
+                        (void*)&p->basinL, (void*)&p->comp, (void*)&flags, (void*)&maxr, (void*)&rout};
         GS_TRY(launch_coop(p, (const void*)k_relax_active, args));
-        GS_TRY(read_ints(p, hbuf, p->i_scalar + I_CHANGED, 1));
-        rounds = hbuf[0] - 1;
+        GS_CUDA(cudaMemcpyAsync(p->h_pinned + 6, p->i_scalar + I_CHANGED, sizeof(int), cudaMemcpyDeviceToHost,
+                                p->stream));
+        GS_CUDA(cudaMemcpyAsync(p->h_pinned + 7, p->i_scalar + I_NEXT, sizeof(int), cudaMemcpyDeviceToHost,
+                                p->stream));
     }
-    if (st) st->fill_rounds = rounds + 1;
     launch(p, k_fill_final, G, B, n, h, (const double*)p->d_scalar, marine_sl, (const int8_t*)p->ledge,
            (const int*)p->parent, (const unsigned long long*)p->basinL, lfill);
     GS_LAUNCH();
@@ -1084,6 +1087,11 @@ int fill_elevation(gs_plan* p, const double* h, double sealevel, double ofill, d
         GS_CUDA(cudaStreamSynchronize(p->stream));
         p->npits = last[0] + last[1];
     }
+    if ((int64_t)p->h_pinned[7] > p->xe_cap) {
+        set_error(GS_ENOMEM, "pit fill: cross-edge capacity exceeded");
+        return GS_ENOMEM;
+    }
+    if (st) st->fill_rounds = p->h_pinned[6];
     const int P = p->npits, np1 = P + 1;
     if (st) st->npits = P;
 
@@ -1224,12 +1232,6 @@ int fill_elevation(gs_plan* p, const double* h, double sealevel, double ofill, d
            (const int*)p->seg_count, (const int*)p->seg_vals2, h, clip_sl, (const double*)p->farea,
            (const double*)p->filled_lvl, (const double*)p->pit_params, p->filled_vol);
     GS_LAUNCH();
-    {
-        double lv;
-        GS_CUDA(cudaMemcpyAsync(&lv, p->d_scalar + D_LEVEL, sizeof(double), cudaMemcpyDeviceToHost, p->stream));
-        GS_CUDA(cudaStreamSynchronize(p->stream));
-        p->level = lv;
-    }
     if (!defer_flats) GS_TRY(fill_join(p, st));
     return GS_OK;
 }

@@ -115,7 +115,6 @@ struct gs_plan {
     int* spill_flag = nullptr;
     int* bestlid = nullptr;
     int npits = 0;
-    double level = 0;
     double* d_scalar = nullptr;          // small device scratch [16]
     int* i_scalar = nullptr;             // small device scratch [16]
     unsigned long long* u_scalar = nullptr;
