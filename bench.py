@@ -401,7 +401,9 @@ def main():
 def adjoint_ratio(model, k, stream, dev, pg):
     """Adjoint:forward cost ratio on the same landscape: k forward steps with
     one checkpoint, then the backward pass (replay of the k steps with
-    recording + k adjoint steps), both timed with CUDA events, max over ranks."""
+    recording + k adjoint steps), both timed with CUDA events, max over ranks;
+    and the same with every step recorded during the forward, so that the
+    backward only reverses (records_kept)."""
     import torch
     from gospl_b200 import adjoint as A
     n = model.lpoints
@@ -421,14 +423,30 @@ def adjoint_ratio(model, k, stream, dev, pg):
     e[2].record(stream)
     torch.cuda.synchronize(dev)
     tf, tb = e[0].elapsed_time(e[1]), e[1].elapsed_time(e[2])
+    # the same with every step recorded during the forward (no recomputation)
+    A.run(model, K, U, rain, h0, k, None)
+    A.backward(model, K, U, rain, None, k, None, torch.ones_like(hT))
+    torch.cuda.synchronize(dev)
+    e[0].record(stream)
+    hT2, _ = A.run(model, K, U, rain, h0, k, None)
+    e[1].record(stream)
+    gK2, _, _, gh2 = A.backward(model, K, U, rain, None, k, None, 2.0 * (hT2 - h0))
+    e[2].record(stream)
+    torch.cuda.synchronize(dev)
+    tfr, tbr = e[0].elapsed_time(e[1]), e[1].elapsed_time(e[2])
     if pg is not None:
-        t = torch.tensor([tf, tb], dtype=torch.float64, device=dev)
+        t = torch.tensor([tf, tb, tfr, tbr], dtype=torch.float64, device=dev)
         pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        tf, tb = float(t[0]), float(t[1])
+        tf, tb, tfr, tbr = (float(v) for v in t)
+    finite = all(bool(torch.isfinite(v).all()) for v in (gK, gh, gK2, gh2))
     return {"ratio": tb / tf, "forward_ms_per_step": tf / k, "adjoint_ms_per_step": tb / k, "steps": k,
             "checkpoint_every": k, "what": "adjoint step = replay of the step with recording + its reverse "
                                           "(gradients wrt K, U, rain and h0)",
-            "finite": bool(torch.isfinite(gK).all() and torch.isfinite(gh).all())}
+            "records_kept": {"ratio": tbr / tf, "recording_forward_ms_per_step": tfr / k,
+                             "adjoint_ms_per_step": tbr / k,
+                             "what": "every step recorded during the forward (no recomputation); ratio = "
+                                     "reverse step / plain forward step"},
+            "finite": finite}
 
 
 def run_precision(args, dev):

@@ -8,7 +8,9 @@ final elevation; its backward pass is the hand-written adjoint of the library
 (``gs_adjoint_step``): transposed sweeps in reverse topological order, the
 reversed lake cascade and the adjoint CG of the diffusion.  Memory is bounded
 by checkpointing: the forward keeps the elevation every ``every`` steps; the
-backward re-runs each segment with recording on and reverses it.
+backward re-runs each segment with recording on and reverses it.  With
+``every=None`` the forward records every step instead (memory for all of
+them, no recomputation) and the backward only reverses.
 
 Discrete decisions of every step (receivers, pits, flat routing, cascade
 states, land/sea and lake masks) are held fixed, so the gradient is that of
@@ -38,9 +40,20 @@ def _restart(model, h):
 
 
 def run(model, K, U, rain, h0, nsteps, every=10):
-    """Forward with checkpoints: (h_T, [h at steps 0, every, 2 every, ...])."""
+    """Forward with checkpoints: (h_T, [h at steps 0, every, 2 every, ...]);
+    with every=None every step is recorded for the backward instead
+    (h_T, None)."""
     _set_params(model, K, U, rain)
     _restart(model, h0)
+    if every is None:
+        model.record(nsteps)
+        try:
+            for s in range(nsteps):
+                model.record_slot(s)
+                model.step()
+        finally:
+            model.record_slot(-1)
+        return model.hGlobal.clone(), None
     ckpt = []
     for s in range(nsteps):
         if s % every == 0:
@@ -50,7 +63,8 @@ def run(model, K, U, rain, h0, nsteps, every=10):
 
 
 def backward(model, K, U, rain, ckpt, nsteps, every, lam_T):
-    """dJ/d(K, U, rain, h0) from lam_T = dJ/dh_T by checkpointed replay."""
+    """dJ/d(K, U, rain, h0) from lam_T = dJ/dh_T by checkpointed replay, or
+    from the records of a forward run with every=None."""
     t = model.torch
     n = model.lpoints
     f64 = dict(dtype=t.float64, device=model.dev)
@@ -61,6 +75,11 @@ def backward(model, K, U, rain, ckpt, nsteps, every, lam_T):
     gbl = t.zeros(n, **f64)
     lam = lam_T.detach().to(**f64).contiguous().clone()
     larea = t.as_tensor(np.asarray(model.mesh.larea, np.float64), **f64)
+    if every is None:
+        for j in range(nsteps - 1, -1, -1):
+            model.adjoint_step(j, lam, gK, gU, grain, gbl)
+            grain += t.where(model.rainMesh > 0, gbl * larea, t.zeros_like(gbl))
+        return gK, gU, grain, lam
     # the records stay allocated for the next backward (model.record(0) frees them)
     model.record(every)
     try:
@@ -87,6 +106,8 @@ class SurfaceEvolution:
 
     @staticmethod
     def apply(K, U, rain, h0, model, nsteps, every=10):
+        """every: checkpoint interval of the replay, or None to record every
+        step during the forward (no recomputation)."""
         import torch
 
         class _Fn(torch.autograd.Function):

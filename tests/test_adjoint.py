@@ -81,6 +81,15 @@ def test_autograd_function_and_records():
     loss.backward()
     assert Kp.grad is not None and torch.isfinite(Kp.grad).all() and Kp.grad.abs().max() > 0
     assert torch.isfinite(Up.grad).all()
+    # records kept from the forward (every=None) give the same gradients as
+    # the checkpointed replay: the replayed steps record the same states
+    Kq = K.clone().requires_grad_(True)
+    Uq = U.clone().requires_grad_(True)
+    hT2 = SurfaceEvolution.apply(Kq, Uq, rain, h0, model, 4, None)
+    assert torch.equal(hT2, hT.detach())
+    (hT2 ** 2).sum().backward()
+    assert torch.allclose(Kq.grad, Kp.grad, rtol=1e-12, atol=0.0)
+    assert torch.allclose(Uq.grad, Up.grad, rtol=1e-12, atol=0.0)
     # the adjoint refuses a slot that holds no recorded step
     from gospl_b200 import _lib
     model.record(2)
