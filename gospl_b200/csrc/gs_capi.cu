@@ -353,4 +353,14 @@ int gs_apply_forces(gs_plan* plan, double* h, const double* rain, const double* 
     GS_GUARD(return gs::apply_forces(plan, h, rain, upsub, dt, sealevel, bl);)
 }
 
+int gs_output_fields(gs_plan* plan, const double* h, const double* cum_ed, const double* eb,
+                     const double* water_filled, const double* fill_fa, const double* fa, const double* vsed,
+                     const double* upsub, const double* rain, const uint8_t* sea, float* out) {
+    NEED(plan);
+    if (plan->n > 0) {
+        NEED(h); NEED(cum_ed); NEED(eb); NEED(water_filled); NEED(fill_fa); NEED(fa); NEED(vsed); NEED(out);
+    }
+    GS_GUARD(return gs::output_fields(plan, h, cum_ed, eb, water_filled, fill_fa, fa, vsed, upsub, rain, sea, out);)
+}
+
 }  // extern "C"

@@ -543,8 +543,16 @@ int hillslope(gs_plan* p, double* h, double* cum_ed, double* eb, double sealevel
               double cdm, double dt, double rtol, int max_iter, gs_stats* st) {
     const int n = (int)p->n;
     GS_TRY(rec_hill(p, h));
-    if (n == 0 || (cda == 0.0 && cdm == 0.0)) return GS_OK;
+    if (n == 0) return GS_OK;
     const int B = 256, G = grid_for(n, B);
+    if (cda == 0.0 && cdm == 0.0) {
+        // no diffusion; the step's land/sea mask (hillslope.py:620) is still kept
+        launch(p, k_sea_of, G, B, n, (const double*)h, sealevel, p->dsea);
+        GS_LAUNCH();
+        p->dvalid = 0;
+        p->hill_sea = 1;
+        return GS_OK;
+    }
     // operator for the current land/sea mask: every row when the parameters
     // changed, else only the rows next to a coastline that moved
     const bool fresh = !(p->dvalid && p->dvalid_dt == dt && p->dvalid_cda == cda && p->dvalid_cdm == cdm);
@@ -560,6 +568,7 @@ int hillslope(gs_plan* p, double* h, double* cum_ed, double* eb, double sealevel
     GS_LAUNCH();
     std::swap(p->dsea, p->dsea2);
     p->dvalid = 1;
+    p->hill_sea = 1;
     p->dvalid_dt = dt;
     p->dvalid_cda = cda;
     p->dvalid_cdm = cdm;
@@ -747,6 +756,7 @@ int hillslope_adjoint(gs_plan* p, const double* h_in, double* lam, double sealev
            (const uint8_t*)p->outlet, p->dcoef, p->dsea);
     GS_LAUNCH();
     p->dvalid = 0;   // the forward's cached operator was overwritten
+    p->hill_sea = 0;
     launch(p, k_cg_x0, G, B, n, p->flat, (const uint8_t*)p->outlet, (const double*)p->farea, (const double*)lam,
            p->cg_x, p->cg_b);
     launch(p, k_cg_init_rhs, G, B, n, p->W, p->flat, (const int*)p->nbr, (const int8_t*)p->nnb,

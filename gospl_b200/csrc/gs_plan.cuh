@@ -197,6 +197,7 @@ struct gs_plan {
     uint8_t* dfix = nullptr;             // rows held fixed (flat-model outlets, zero area)
     int dvalid = 0;
     double dvalid_dt = 0, dvalid_cda = 0, dvalid_cdm = 0;
+    int hill_sea = 0;                    // dsea = land/sea mask of the last hillslope input
     double* cg_r = nullptr;
     double* cg_z = nullptr;
     double* cg_p = nullptr;
@@ -299,6 +300,9 @@ int hillslope(gs_plan* p, double* h, double* cum_ed, double* eb, double sealevel
               double cdm, double dt, double rtol, int max_iter, gs_stats* st);
 int apply_forces(gs_plan* p, double* h, const double* rain, const double* upsub, double dt,
                  double sealevel, double* bl);
+int output_fields(gs_plan* p, const double* h, const double* cum_ed, const double* eb, const double* water_filled,
+                  const double* fill_fa, const double* fa, const double* vsed, const double* upsub,
+                  const double* rain, const uint8_t* sea, float* out);
 
 void prof_begin(gs_plan* p, const void* fn, cudaEvent_t* stop);
 int coop_occupancy(int* per_sm);

@@ -8,7 +8,10 @@ uses, with goSPL's names, defaults and errors (gospl/tools/inputparser.py):
   ``o f w c``, legacy ``0``/``1`` -> ``o``/``f``, :208-246), ``fast``, ``nodep``
   and ``seadepo`` (:289-300; continental deposition runs unless ``nodep``,
   marine deposition is not implemented and must be switched off);
-* ``time``: ``start``, ``end``, ``dt`` required, ``tout`` (:343-404);
+* ``time``: ``start``, ``end``, ``dt`` required, ``tout`` (:343-404, clamped
+  to [dt, end - start] as :413-429 does), ``rstep`` (restart, :411);
+* ``output``: ``dir`` (output), ``makedir`` (False), ``compression`` (gzip)
+  (:2096-2117);
 * ``spl``: ``K``, ``d`` (0), ``m`` (0.5), ``G`` (0) (:454-496);
 * ``diffusion``: ``hillslopeKa``, ``hillslopeKm``, ``oFill`` (-6000) (:498-545),
   ``nlPitVolume`` (1e9), ``nlPitDepth`` (100), ``nonlinKm``/``nlPitK`` (10),
@@ -22,7 +25,7 @@ uses, with goSPL's names, defaults and errors (gospl/tools/inputparser.py):
 
 Paths are taken as given (relative to the working directory, as goSPL does),
 then relative to the YAML file.  Keys of other goSPL subsystems (sediment,
-stratigraphy, flexure, ice, orography, output) are ignored; options that would
+stratigraphy, flexure, ice, orography) are ignored; options that would
 change this path's arithmetic and that the library does not implement
 (sea-level curves, time-varying climate or tectonic events, horizontal
 tectonics, marine deposition) raise ``ValueError``.
@@ -100,6 +103,11 @@ def read_input(filename):
     if p["tEnd"] <= p["tStart"]:
         raise ValueError("Simulation end/start times do not make any sense!")
     p["tout"] = float(t.get("tout", p["tEnd"] - p["tStart"]))
+    p["rStep"] = int(t.get("rstep", 0))                       # :411
+    if p["tStart"] + p["tout"] > p["tEnd"]:                   # :413-420
+        p["tout"] = p["tEnd"] - p["tStart"]
+    if p["tout"] < p["dt"]:                                   # :422-429
+        p["tout"] = p["dt"]
 
     spl = inp.get("spl")
     if spl is not None:
@@ -159,4 +167,12 @@ def read_input(filename):
             raise ValueError("horizontal tectonics (hdisp/zfit) are not implemented by gospl_b200")
         if e.get("upsub") is not None:
             p["upsub"] = _npz(e["upsub"], base, "tectonics upsub").ravel()
+
+    # output (:2096-2117): directory, numbered copies, HDF5 compression; a
+    # restart reuses the directory
+    out = inp.get("output") or {}
+    p["outputDir"] = str(out.get("dir", "output"))
+    p["makedir"] = bool(out.get("makedir", False)) and p["rStep"] == 0
+    p["compression"] = out.get("compression", "gzip")
+    p["finput"] = filename
     return coords, cells, elev, p

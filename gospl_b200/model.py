@@ -11,6 +11,8 @@
   continental sediment routing and deposition in depressions
 * ``getHillslope()``      — hillSLP.getHillslope (hillslope.py:614-649)
 * ``applyForces()``       — UnstMesh.applyForces (unstructuredmesh.py:743-794)
+* ``visModel()`` / ``readData()`` — WriteMesh (tools/outmesh.py): HDF5 and
+  XDMF outputs every ``tout`` years and the restart from output ``rStep``
 * ``runProcesses()``      — the time loop of model.py:331-466 with
   ``fast: false`` and continental deposition unless ``nodep`` (marine
   deposition, ``seadepo``, is not built).
@@ -54,6 +56,11 @@ class Model:
     ``members`` = (start, maxarea) declares the mesh a disjoint union of
     landscapes (``gospl_b200.ensemble``).  ``precision=32`` selects the FP32
     sweeps and CG with FP64 refinement to ``refine_tol``.
+
+    Outputs (goSPL's ``output`` and ``time`` keys): ``outputDir`` (None: no
+    files; a YAML input defaults to "output"), ``makedir`` (False),
+    ``compression`` ("gzip", a level 0-9 or "none"), ``tout`` (tEnd - tStart)
+    and ``rStep`` (restart from that output step, 0: a new run).
     """
 
     def __init__(self, filename=None, *, coords=None, cells=None, elev=None, params=None, mesh=None,
@@ -71,6 +78,8 @@ class Model:
         if mesh is None:
             mesh = FVMesh(coords, cells, params.get("bc", "oooo"))
         self.mesh = mesh
+        self.mesh_coords = coords
+        self.mesh_cells = cells
         self.dev = torch.device(device)
         if self.dev.type == "cuda" and self.dev.index is None:
             self.dev = torch.device("cuda", torch.cuda.current_device())
@@ -105,6 +114,8 @@ class Model:
         self.cg_rtol = cg_rtol
         self.cg_maxit = cg_maxit
         self.stats = {}
+        self._hill_ran = False
+        self.output = None
 
         f64 = dict(dtype=torch.float64, device=self.dev)
         i32 = dict(dtype=torch.int32, device=self.dev)
@@ -177,7 +188,20 @@ class Model:
             start = np.ascontiguousarray(members[0], np.int64)
             marea = np.ascontiguousarray(members[1], np.float64)
             _lib.check(L.gs_plan_set_members(self._plan, len(marea), _lib.ptr(start), _lib.ptr(marea)))
+        out_dir = p.get("outputDir")
+        self.rStep = int(p.get("rStep", 0))
+        if out_dir is not None:
+            if cells is None or coords is None:
+                raise ValueError("outputs need the mesh coordinates and cells")
+            from .outmesh import WriteMesh
+            # WriteMesh.__init__ (outmesh.py:31-87) runs before the forcing
+            self.output = WriteMesh(self, out_dir, bool(p.get("makedir", False)), p.get("compression", "gzip"),
+                                    p.get("tout"), self.rStep, p.get("finput"))
+        elif self.rStep > 0:
+            raise ValueError("a restart (rStep > 0) needs the output directory it reads")
         self.applyForces()
+        if self.rStep > 0:
+            self.readData()   # model.py:289-291
         if init_flow:
             self.flowAccumulation()
 
@@ -297,6 +321,7 @@ class Model:
                                   _lib.ptr(self.EbLocal), self.sealevel, self.Cda, self.Cdm, self.dt,
                                   self.cg_rtol, self.cg_maxit, ctypes.byref(st)))
         self.stats["hillslope"] = st.as_dict()
+        self._hill_ran = True
 
     def step(self):
         """One physics step of runProcesses (model.py:347-453, fast=False):
@@ -313,10 +338,30 @@ class Model:
         self.tNow += self.dt
 
     def runProcesses(self):
-        while self.tNow <= self.tEnd:
-            if self.tNow == self.tEnd:
-                break
-            self.step()
+        """model.py:331-466: output, then a step, until tEnd; the run ends
+        with every output on disk."""
+        try:
+            while self.tNow <= self.tEnd:
+                self.visModel()
+                if self.tNow == self.tEnd:
+                    break
+                self.step()
+        finally:
+            if self.output is not None:
+                self.output.flush()
+
+    # ------------------------------------------------------------- outputs
+    def visModel(self):
+        """WriteMesh.visModel (outmesh.py:89-103); a no-op without outputDir."""
+        if self.output is not None:
+            self.output.visModel()
+
+    def readData(self):
+        """WriteMesh.readData (outmesh.py:505-620): restart state from the
+        output files."""
+        if self.output is None:
+            raise ValueError("readData needs the output directory")
+        self.output.readData()
 
     # ------------------------------------------------------------- adjoint
     def record(self, nslots):
@@ -339,6 +384,9 @@ class Model:
             _lib.ptr(grad_u), _lib.ptr(grad_rain), _lib.ptr(grad_bl)))
 
     def destroy(self):
+        if getattr(self, "output", None) is not None:
+            self.output.close()
+            self.output = None
         if getattr(self, "_plan", None) is not None:
             self.torch.cuda.synchronize(self.dev)
             _lib_handle().gs_plan_destroy(self._plan)

@@ -256,6 +256,21 @@ int gs_apply_forces(gs_plan* plan, double* h, const double* rain, const double* 
                     double sealevel, double* bl);
 
 /*
+ * Output fields of one step for the HDF5 writer: WriteMesh._outputMesh
+ * (outmesh.py:252-478).  out is a device float32 array [9][n] whose rows are
+ * elev (h), erodep (cum_ed), EDrate (eb), waterFill, fillFA, FA, sedLoad
+ * (vsed), uplift (upsub) and rain, each rounded to nearest from float64; FA,
+ * fillFA and sedLoad are raised to DISCHARGE_FLOOR = 1e-8 (tools/constants.py:51)
+ * where at or below it, and FA and fillFA are 1 on sea vertices.  sea is the
+ * land/sea mask (1 = sea) or NULL for the mask of the elevation the last
+ * gs_hillslope call started from (hillslope.py:620; GS_EINVAL if there is none).
+ * upsub and rain may be NULL (their rows are left as they are).
+ */
+int gs_output_fields(gs_plan* plan, const double* h, const double* cum_ed, const double* eb,
+                     const double* water_filled, const double* fill_fa, const double* fa, const double* vsed,
+                     const double* upsub, const double* rain, const uint8_t* sea, float* out);
+
+/*
  * Adjoint.  No counterpart in the reference (goSPL has no derivatives).
  * gs_plan_record allocates nslots per-step records (0 frees them; single-
  * landscape plans only); after gs_plan_record_slot(plan, s) the forward calls

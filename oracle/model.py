@@ -953,3 +953,44 @@ class OracleModel:
             if self.tNow == self.tEnd:
                 break
             self.step()
+
+    # ----------------------------------------------------------------- output
+    def output_fields(self):
+        """The datasets WriteMesh._outputMesh writes for the current state
+        (see ``output_fields`` below), with the last seaID built."""
+        sea = np.zeros(self.lpoints, np.uint8)
+        sea[np.asarray(self.seaID, np.int64)] = 1
+        vsed = self.vSed if hasattr(self, "vSed") else np.zeros(self.lpoints)
+        return output_fields(self.h, self.cumED, self.EbLocal, self.waterFilled, self.fillFAL, self.FAL, vsed,
+                             self.upsub, self.rainVal, sea)
+
+
+DISCHARGE_FLOOR = 1.0e-8   # gospl/tools/constants.py:51
+
+
+def output_fields(h, cumED, Eb, waterFilled, fillFAL, FAL, vSed, upsub, rain, sea):
+    """WriteMesh._outputMesh (gospl/tools/outmesh.py:252-478) for one rank,
+    ``fast: False``, no ice, flexure, soil or dual lithology: name -> float32
+    [n, 1].  FA and fillFA are floored at DISCHARGE_FLOOR and set to 1 on sea
+    vertices (:334-356); sedLoad is floored (:426-435); every float64 field is
+    rounded to float32 by the file's datatype."""
+    sea = np.asarray(sea).astype(bool)
+
+    def col(a):
+        with np.errstate(over="ignore", invalid="ignore"):
+            return np.asarray(a, np.float64).astype(np.float32).reshape(-1, 1)
+
+    def floored(a, with_sea):
+        d = np.array(a, np.float64, copy=True)
+        d[d <= DISCHARGE_FLOOR] = DISCHARGE_FLOOR
+        if with_sea:
+            d[sea] = 1.0
+        return d
+
+    out = {"elev": col(h), "erodep": col(cumED), "EDrate": col(Eb), "waterFill": col(waterFilled),
+           "fillFA": col(floored(fillFAL, True)), "FA": col(floored(FAL, True)), "sedLoad": col(floored(vSed, False))}
+    if upsub is not None:
+        out["uplift"] = col(upsub)
+    if rain is not None:
+        out["rain"] = col(rain)
+    return out

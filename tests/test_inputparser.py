@@ -89,3 +89,19 @@ def test_defaults_and_errors(tmp_path):
     y, _ = _write(tmp_path, YML.replace("spl:\n    K: 4.0e-6\n    d: 0.\n    m: 0.5\n    G: 0.\n", ""))
     _, _, _, p = read_input(str(y))
     assert (p["K"], p["d"], p["m"]) == (1.0e-12, 0.0, 0.5)
+
+
+def test_output_and_restart_keys(tmp_path):
+    """time.tout clamped to [dt, end - start], time.rstep, the output section
+    (inputparser.py:404-429, 2096-2117)."""
+    y, _ = _write(tmp_path, YML)
+    p = read_input(str(y))[3]
+    assert (p["outputDir"], p["makedir"], p["compression"], p["rStep"]) == ("output", False, "gzip", 0)
+    assert p["finput"] == str(y)
+    y, _ = _write(tmp_path, YML.replace("    tout: 300\n", "    tout: 900\n    rstep: 2\n")
+                  + "output:\n    dir: run\n    makedir: True\n    compression: none\n")
+    p = read_input(str(y))[3]
+    assert (p["tout"], p["rStep"], p["outputDir"], p["compression"]) == (300.0, 2, "run", "none")
+    assert p["makedir"] is False          # a restart reuses the directory
+    y, _ = _write(tmp_path, YML.replace("    tout: 300\n", "    tout: 10\n"))
+    assert read_input(str(y))[3]["tout"] == 100.0

@@ -1,0 +1,69 @@
+"""Output files (gospl/tools/outmesh.py): the datasets and their edits against
+the reference's own _outputMesh, the XMF and XDMF text, the output directory
+rules."""
+import os
+
+import numpy as np
+import pytest
+
+from gospl_b200 import outmesh
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+GOLDEN = os.path.join(HERE, "golden", "output_planar2k.npz")
+
+
+def test_oracle_output_fields_match_reference():
+    """The oracle's restatement of _outputMesh (floors, sea edits, float32
+    rounding) gives the reference's datasets bit for bit at every output."""
+    from oracle.model import output_fields
+    g = np.load(GOLDEN)
+    for s in range(int(g["noutputs"])):
+        st = {k: g["s%d_%s" % (s, k)] for k in ("h", "cumED", "Eb", "waterFilled", "fillFAL", "FAL", "vSed", "sea")}
+        out = output_fields(st["h"], st["cumED"], st["Eb"], st["waterFilled"], st["fillFAL"], st["FAL"], st["vSed"],
+                            g["upsub"], np.maximum(g["rain"], 0.0), st["sea"])
+        assert sorted(out) == sorted(g["s%d_names" % s])
+        for k, v in out.items():
+            ref = g["s%d_ds_%s" % (s, k)]
+            assert v.dtype == ref.dtype and v.shape == ref.shape, (s, k)
+            assert np.array_equal(v, ref), (s, k)
+    # the fixture exercises both edits
+    assert g["s1_sea"].sum() > 0 and (g["s1_ds_FA"] == 1.0).sum() >= g["s1_sea"].sum()
+    assert (g["s1_ds_FA"] == np.float32(1e-8)).sum() > 0
+
+
+def test_xmf_and_xdmf_text_match_reference():
+    g = np.load(GOLDEN)
+    n = len(g["z"])
+    m = len(g["c"])
+    for s in range(int(g["noutputs"])):
+        txt = outmesh.xmf_text(s, float(g["save_times"][s]), m, n, float(g["p_sealevel"]))
+        assert txt == str(g["s%d_xmf" % s]), s
+    assert outmesh.xdmf_text(int(g["noutputs"]) - 1) == str(g["xdmf"])
+    # the topology: float32 coordinates, 1-based int32 cells
+    assert np.array_equal(g["topo_coords"], np.asarray(g["v"], np.float32))
+    assert np.array_equal(g["topo_cells"], (g["c"] + 1).astype(np.int32))
+
+
+def test_output_directory_rules(tmp_path, monkeypatch):
+    monkeypatch.chdir(tmp_path)
+    finput = tmp_path / "in.yml"
+    finput.write_text("x: 1\n")
+    d = outmesh.make_output_dir("run", False, 0, str(finput))
+    assert d == str(tmp_path / "run") and os.path.isdir(d + "/h5") and os.path.isdir(d + "/xmf")
+    assert os.path.exists(d + "/in.yml")
+    open(d + "/h5/old.h5", "w").close()
+    assert outmesh.make_output_dir("run", False, 0) == d and not os.path.exists(d + "/h5/old.h5")   # removed
+    assert outmesh.make_output_dir("run", True, 0) == d + "_0"
+    assert outmesh.make_output_dir("run", True, 0) == d + "_1"
+    open(d + "/h5/keep.h5", "w").close()
+    assert outmesh.make_output_dir("run", False, 2) == d and os.path.exists(d + "/h5/keep.h5")        # restart
+
+
+def test_compression_levels():
+    assert outmesh.compression_level("gzip") == 4
+    assert outmesh.compression_level(True) == 4
+    assert outmesh.compression_level(7) == 7
+    for off in (None, False, "none", "None", ""):
+        assert outmesh.compression_level(off) is None
+    with pytest.raises(ValueError):
+        outmesh.compression_level("lzf")
