@@ -168,7 +168,7 @@ def main():
     ap.add_argument("--cpu-level", type=int, default=7)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--workload", default="sphere", choices=["sphere", "planar", "ensemble", "precision",
-                                                                   "transport", "sediment"])
+                                                                   "transport", "sediment", "output"])
     ap.add_argument("--members", type=int, default=256)
     ap.add_argument("--loop", action="store_true", help="ensemble: also time the per-member loop")
     ap.add_argument("--adjoint-steps", type=int, default=4, help="sphere: steps of the adjoint timing (0: skip)")
@@ -197,6 +197,9 @@ def main():
         return
     if args.workload == "sediment":
         run_sediment(args, dev)
+        return
+    if args.workload == "output":
+        run_output(args, dev)
         return
     pg = None
     if world > 1:
@@ -626,6 +629,107 @@ def run_sediment(args, dev):
                                 "cascade_passes": o["passes"], "diffused_lakes": o["diffused_lakes"],
                                 "sed_pits": o["npits"], "vsed_max_m3_per_yr": o["vsed_max"]}
                          for name, o in out.items()}}
+    print(json.dumps(line), flush=True)
+
+
+def run_output(args, dev):
+    """Output files (goSPL's WriteMesh: HDF5 + XDMF every tout years) on the
+    2.6M-vertex sphere.  (1) The packing kernel alone (gs_output_fields: 73
+    bytes read and 36 written per vertex) against the measured HBM copy
+    bandwidth.  (2) The same steps from the same state without outputs and
+    with an output after every step (tout = dt), compressed (gzip, level 4)
+    and not: device time per step on the model's stream and wall time per
+    step including the wait for the files, so the cost a run pays for its
+    outputs is the difference."""
+    import shutil
+    import torch
+    from gospl_b200 import _lib
+    from gospl_b200.mesh import FVMesh
+    from gospl_b200.model import Model
+    c, f, z, rain, up, p = sphere_inputs(args.level)
+    work = tempfile.mkdtemp(prefix="gospl_out_")
+    try:
+        p = dict(p, rain=rain, upsub=up, tEnd=1.0e30, outputDir=os.path.join(work, "out"))
+        p["tout"] = p["dt"]
+        mesh = FVMesh(c, f, p["bc"], device=dev)
+        m = Model(coords=c, cells=f, elev=z, params=p, mesh=mesh, device=dev)
+        stream = torch.cuda.current_stream(dev)
+        n = m.lpoints
+        for _ in range(max(args.warmup, 1)):     # one step at least: the packing kernel's land/sea mask
+            m.step()
+        L = _lib.load()
+        stage = torch.empty((9, n), dtype=torch.float32, device=dev)
+
+        def pack():
+            _lib.check(L.gs_output_fields(m._plan, _lib.ptr(m.hGlobal), _lib.ptr(m.cumED), _lib.ptr(m.EbLocal),
+                                          _lib.ptr(m.waterFilled), _lib.ptr(m.fillFAL), _lib.ptr(m.FAL),
+                                          _lib.ptr(m.vSed), _lib.ptr(m.upsub), _lib.ptr(m.rainVal), None,
+                                          _lib.ptr(stage)))
+
+        for _ in range(3):
+            pack()
+        flush = torch.empty(64 << 20, dtype=torch.float32, device=dev)   # 256 MB > L2, between launches
+        reps = 20
+        t_pack = 0.0
+        for _ in range(reps):
+            flush.fill_(1.0)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            pack()
+            b.record(stream)
+            torch.cuda.synchronize(dev)
+            t_pack += a.elapsed_time(b) / reps
+        del flush
+        peak, src = peaks()
+        algo = 109.0 * n
+        state = {k: getattr(m, k).clone() for k in ("hGlobal", "cumED", "EbLocal", "FAL", "fillFAL", "waterFilled",
+                                                   "vSed", "bL")}
+        t0 = m.tNow
+
+        def restore():
+            for k, v in state.items():
+                getattr(m, k).copy_(v)
+            m.tNow = t0
+            m.output.saveTime = t0
+
+        runs = {}
+        nsteps = min(args.steps, 5)      # 5 outputs of 94 MB (uncompressed) at most on disk
+        for name, level in (("no_output", None), ("gzip", 4), ("uncompressed", None)):
+            restore()
+            m.output.level = level
+            torch.cuda.synchronize(dev)
+            w0 = time.perf_counter()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            for _ in range(nsteps):
+                if name != "no_output":
+                    m.visModel()
+                m.step()
+            b.record(stream)
+            torch.cuda.synchronize(dev)
+            m.output.flush()
+            wall = (time.perf_counter() - w0) * 1000.0 / nsteps
+            size = sum(os.path.getsize(os.path.join(dp, fn)) for dp, _, fns in os.walk(p["outputDir"]) for fn in fns)
+            runs[name] = {"device_ms_per_step": a.elapsed_time(b) / nsteps, "wall_ms_per_step": wall,
+                          "bytes_on_disk": size}
+            shutil.rmtree(os.path.join(p["outputDir"], "h5"), ignore_errors=True)
+            os.makedirs(os.path.join(p["outputDir"], "h5"))
+        m.destroy()
+    finally:
+        shutil.rmtree(work, ignore_errors=True)
+    base = runs["no_output"]["wall_ms_per_step"]
+    line = {"metric": "output overhead per step (an output after every step) @2.6M-vertex sphere",
+            "value": runs["gzip"]["wall_ms_per_step"] - base, "unit": "ms/step", "n_gpus": 1,
+            "steps": nsteps, "warmup": args.warmup, "ms_per_step": runs["gzip"]["wall_ms_per_step"],
+            "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64->f32",
+            "data": "synthetic (seeded sphere, SH relief)",
+            "config": {"workload": "sphere level %d (%d vertices), full physics step with goSPL's output files "
+                                   "(9 float32 fields, XMF, XDMF) written after every step" % (args.level, n),
+                       "vertices": n, "global_batch": 1, "seq_len": 0, "parallelism": "single",
+                       "l2": "256 MB buffer written between timed packing launches"},
+            "pack": {"ms": t_pack, "algorithmic_bytes": algo, "achieved_gbs": algo / t_pack / 1e6,
+                     "peak_gbs": peak, "frac": algo / t_pack / 1e6 / peak, "peak_source": src},
+            "runs": runs}
     print(json.dumps(line), flush=True)
 
 

@@ -266,12 +266,12 @@ class WriteMesh:
         (elevation, cumulative erosion/deposition, sediment load, rates and
         flow accumulations, float32 in the file) into the model."""
         self.flush()
-        m = self.m
-        t = m.torch
         path = os.path.join(self.outputDir, "h5", "%s.%d.p0.h5" % (self.file, self.step - 1))
         if not os.path.exists(path):
             raise ValueError("Restart file is missing...")
         d = hdf5.read(path, ["elev", "erodep", "sedLoad", "EDrate", "FA", "fillFA"])
+        m = self.m
+        t = m.torch
 
         def put(dst, name):
             dst.copy_(t.as_tensor(d[name][:, 0].astype(np.float64), device=m.dev))

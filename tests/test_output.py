@@ -67,3 +67,35 @@ def test_compression_levels():
         assert outmesh.compression_level(off) is None
     with pytest.raises(ValueError):
         outmesh.compression_level("lzf")
+
+
+class _FakeModel:
+    def __init__(self, t0=0.0, t1=5000.0, dt=1000.0):
+        self.tStart, self.tEnd, self.dt, self.tNow = t0, t1, dt, t0
+        self.lpoints = 4
+        self.mesh_cells = np.zeros((2, 3), np.int64)
+
+
+def test_output_schedule_and_restart_bookkeeping(tmp_path, monkeypatch):
+    """visModel writes at the start time and whenever tNow reaches the next
+    output time (outmesh.py:89-103) inside runProcesses' loop (model.py:347-
+    466); tout is clamped to [dt, tEnd - tStart]; a restart at output k
+    resumes at tStart + k tout with output counter k + 1 (outmesh.py:61-79)."""
+    written = []
+    monkeypatch.setattr(outmesh.WriteMesh, "_outputMesh",
+                        lambda self: (written.append((self.step, self.m.tNow)), setattr(self, "step", self.step + 1)))
+    m = _FakeModel()
+    w = outmesh.WriteMesh(m, str(tmp_path / "o"), tout=2000.0)
+    while m.tNow <= m.tEnd:
+        w.visModel()
+        if m.tNow == m.tEnd:
+            break
+        m.tNow += m.dt
+    assert written == [(0, 0.0), (1, 2000.0), (2, 4000.0)]
+    assert outmesh.WriteMesh(_FakeModel(), str(tmp_path / "o"), tout=1.0e9).tout == 5000.0
+    assert outmesh.WriteMesh(_FakeModel(), str(tmp_path / "o"), tout=10.0).tout == 1000.0
+    m = _FakeModel()
+    w = outmesh.WriteMesh(m, str(tmp_path / "o"), tout=2000.0, rstep=1)
+    assert (m.tNow, w.step, w.saveTime) == (2000.0, 2, 4000.0)
+    with pytest.raises(ValueError):
+        w.readData()                      # no gospl.1.p0.h5 in the directory
