@@ -99,3 +99,40 @@ def test_output_schedule_and_restart_bookkeeping(tmp_path, monkeypatch):
     assert (m.tNow, w.step, w.saveTime) == (2000.0, 2, 4000.0)
     with pytest.raises(ValueError):
         w.readData()                      # no gospl.1.p0.h5 in the directory
+
+
+def test_writer_files_carry_the_reference_datasets(tmp_path):
+    """The writer thread's half of an output (host rows -> HDF5 + XMF + XDMF)
+    given the reference's own float32 rows writes files whose datasets, XMF
+    and XDMF are the reference's, and that pass the HDF5 structure checks."""
+    import torch
+    from gospl_b200 import hdf5
+    from test_hdf5 import lint
+    g = np.load(GOLDEN)
+    n = len(g["z"])
+    m = _FakeModel()
+    m.lpoints = n
+    m.mesh_cells = g["c"]
+    m.mesh_coords = g["v"]
+    w = outmesh.WriteMesh(m, str(tmp_path / "out"), compression="gzip")
+
+    class _Done:
+        def synchronize(self):
+            pass
+
+    for s in range(int(g["noutputs"])):
+        host = torch.zeros((len(outmesh.FIELDS), n), dtype=torch.float32)
+        for k in g["s%d_names" % s]:
+            host[outmesh.FIELDS.index(str(k))] = torch.from_numpy(g["s%d_ds_%s" % (s, k)][:, 0])
+        w._write(dict(step=s, save_time=float(g["save_times"][s]), sealevel=float(g["p_sealevel"]), event=_Done(),
+                      host=host, upsub=True, rain=True, topology=w._topology() if s == 0 else None))
+        path = str(tmp_path / "out" / "h5" / ("gospl.%d.p0.h5" % s))
+        assert lint(path) == sorted(str(k) for k in g["s%d_names" % s])
+        d = hdf5.read(path)
+        for k in g["s%d_names" % s]:
+            assert np.array_equal(d[str(k)], g["s%d_ds_%s" % (s, k)]), (s, k)
+        assert (tmp_path / "out" / "xmf" / ("gospl%d.xmf" % s)).read_text() == str(g["s%d_xmf" % s])
+    topo = hdf5.read(str(tmp_path / "out" / "h5" / "topology.p0.h5"))
+    assert np.array_equal(topo["coords"], g["topo_coords"]) and np.array_equal(topo["cells"], g["topo_cells"])
+    assert (tmp_path / "out" / "gospl.xdmf").read_text() == str(g["xdmf"])
+    w.close()
