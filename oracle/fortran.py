@@ -63,6 +63,8 @@ def lib():
         L.orc_getpitvol.argtypes = [i, i, P, P, P, P, P]
         L.orc_flow_solve.argtypes = [i, i, P, P, P, P]
         L.orc_spl_solve.argtypes = [i, i, P, P, P, P]
+        L.orc_mfdrcvrs.argtypes = [i, i, d, P, d, P, P, P, P, P]
+        L.orc_epsfill.argtypes = [i, d, P, P]
         _lib = L
     return _lib
 
@@ -186,6 +188,31 @@ def mfdreceivers(nrcv, exp, elev, sl, gid, powfn=None):
     if st != 0:
         raise ValueError("mfdreceivers: nrcv must be in 1..12")
     return rcv, dist, wgt
+
+
+def mfdrcvrs(nrcv, exp, elev, sl, gid, powfn=None):
+    """f2py: rcv, dist, wgt = mfdrcvrs(nrcv, exp, elev, sl, gid); [nb, 12]
+    (functions.F90:1673-1785)."""
+    elev = _f64(elev)
+    gid = _i32(gid)
+    nb = elev.shape[0]
+    rcv = np.empty((nb, 12), np.int32)
+    dist = np.empty((nb, 12))
+    wgt = np.empty((nb, 12))
+    st = lib().orc_mfdrcvrs(nb, int(nrcv), float(exp), _p(elev), float(sl), _p(gid), _p(rcv), _p(dist),
+                            _p(wgt), powfn)
+    if st != 0:
+        raise ValueError("mfdrcvrs: nrcv must be in 1..12")
+    return rcv, dist, wgt
+
+
+def epsfill(sl, elev):
+    """f2py: fillz = epsfill(sl, elev) (functions.F90:2633-2697)."""
+    elev = _f64(elev)
+    fillz = np.empty_like(elev)
+    if lib().orc_epsfill(elev.shape[0], float(sl), _p(elev), _p(fillz)) != 0:
+        raise MemoryError("epsfill")
+    return fillz
 
 
 def quicksort12(values, indices):

@@ -996,3 +996,106 @@ int orc_spl_solve(int nb, int R, const int *rcv, const double *c, const double *
     free(nout); free(dptr); free(up); free(fill); free(queue);
     return left;
 }
+
+/* ---------------------------------------------------------------------------
+ * Marine routing (seaplex.py:_matOcean, seaplex.py:137-238)
+ * ------------------------------------------------------------------------- */
+/* mfdrcvrs (functions.F90:1673-1785): receivers of the marine routing,
+ * C-order [nb][12].  Every strictly lower neighbour is a receiver (up to
+ * nRcv above `sl`, 12 at or below it) with the equal weight `1. / kk`; the
+ * literal `1.` is a default (single precision) real in the reference's build
+ * (no -fdefault-real-8), so the weight is 1/kk rounded to float, widened. */
+int orc_mfdrcvrs(int nb, int nRcv, double exp_, const double *elev, double sl,
+                 const int *gid, int *rcv, double *dist, double *wgt, powfn_t powfn)
+{
+    if (nRcv < 1 || nRcv > 12) return -1;
+    if (!powfn) powfn = pow;
+    for (int i = 0; i < nb * 12; i++) { rcv[i] = -1; dist[i] = 0.0; wgt[i] = 0.0; }
+    for (int k = 0; k < nb; k++) {
+        int *r = &rcv[k * 12];
+        double *d = &dist[k * 12], *w = &wgt[k * 12];
+        int ngbs;
+        double fexp;
+        if (elev[k] > sl) { ngbs = nRcv; fexp = exp_; }
+        else { ngbs = 12; fexp = 0.01; }
+        double slp[12], dst[12];
+        int id[12];
+        for (int p = 0; p < 12; p++) { slp[p] = 0.0; id[p] = 0; dst[p] = 0.0; }
+        int kk = 0;
+        double val = 0.0;
+        for (int p = 0; p < FVnNb[k]; p++) {
+            int n = FVnID[k * MAXNB + p] + 1;
+            if (n > 0 && FVeLgt[k * MAXNB + p] > 0.0) {
+                val = powfn(elev[k] - elev[n - 1], fexp) / FVeLgt[k * MAXNB + p];
+                if (val > 0.0) {
+                    kk = kk + 1;
+                    slp[kk - 1] = val * (1.0 - 1.0e-15 * (double)gid[n - 1]);
+                    id[kk - 1] = n - 1;
+                    dst[kk - 1] = FVeLgt[k * MAXNB + p];
+                }
+            }
+        }
+        const double wk = kk > 0 ? (double)(1.0f / (float)kk) : 0.0;
+        if (kk == 0) {
+            for (int p = 0; p < 12; p++) r[p] = k;
+        } else if (kk <= ngbs) {
+            for (int p = 0; p < ngbs; p++) r[p] = k;
+            for (int p = 0; p < kk; p++) { r[p] = id[p]; d[p] = dst[p]; }
+            for (int p = 0; p < ngbs; p++) if (slp[p] > 0.0) w[p] = wk;
+        } else {
+            for (int p = 0; p < ngbs; p++) r[p] = k;
+            quicksort(slp, 1, kk, id);
+            int nn = 0;
+            for (int p = kk; p >= kk - ngbs + 1; p--) {
+                nn = nn + 1;
+                r[nn - 1] = id[p - 1];
+                d[nn - 1] = dst[p - 1];
+            }
+            for (int p = 0; p < ngbs; p++) if (slp[p] > 0.0) w[p] = wk;
+        }
+    }
+    return 0;
+}
+
+/* epsfill (functions.F90:2633-2697): priority-flood from the cells below `sl`
+ * that touch a cell at or above it; every cell reached is raised to at least
+ * the next double above the cell it was reached from (nearest(x, 1.0)), so
+ * the filled surface has no flats.  Cells below `sl` keep their value. */
+int orc_epsfill(int nb, double sl, const double *elev, double *fillz)
+{
+    char *flag = (char *)calloc(nb > 0 ? nb : 1, 1);
+    if (!flag) return -1;
+    for (int i = 0; i < nb; i++) fillz[i] = elev[i];
+    priorityqueue.n = 0;
+    for (int i = 0; i < nb; i++) {
+        if (fillz[i] < sl) {
+            flag[i] = 1;
+            for (int k = 0; k < FVnNb[i]; k++) {
+                int c = FVnID[i * MAXNB + k];
+                if (c >= 0 && fillz[c] >= sl) {
+                    pq_push(&priorityqueue, fillz[i], i);
+                    break;
+                }
+            }
+        }
+    }
+    while (priorityqueue.n > 0) {
+        qnode pt = pq_pop(&priorityqueue);
+        int i = pt.id;
+        for (int k = 0; k < FVnNb[i]; k++) {
+            int c = FVnID[i * MAXNB + k];
+            if (c >= 0 && !flag[c]) {
+                flag[c] = 1;
+                double h = nextafter(fillz[i], INFINITY);
+                if (fillz[c] > h) {
+                    pq_push(&priorityqueue, fillz[c], c);
+                } else {
+                    fillz[c] = h;
+                    pq_push(&priorityqueue, fillz[c], c);
+                }
+            }
+        }
+    }
+    free(flag);
+    return 0;
+}

@@ -21,6 +21,10 @@ from . import fortran as F
 from . import mesh as M
 
 MISSING_DATA_SENTINEL = -1.0e8   # gospl/tools/constants.py:34
+DEPOSIT_FLOOR = 1.0e-3           # gospl/tools/constants.py:58
+BOUNDARY_FLOW_SENTINEL = -1.0e6  # gospl/tools/constants.py:90
+MARINE_SMOOTH_N_LAND = 1.0       # gospl/tools/constants.py:126
+MARINE_SMOOTH_N_SEA = 5.0        # gospl/tools/constants.py:127
 GRAPH_OUTLIER_CAP = 1.0e7        # gospl/tools/constants.py:100
 
 
@@ -82,8 +86,10 @@ class OracleModel:
         self.sealevel = float(p.get("sealevel", 0.0))
         self.nodep = bool(p.get("nodep", True))
         self.seaDepo = bool(p.get("seadepo", False))
-        if not self.nodep and self.seaDepo:
-            raise NotImplementedError("marine deposition (seaChange) is not restated")
+        self.nlK = float(p.get("nonlinKm", 10.0))                                    # inputparser.py:554
+        self.clinSlp = max(1.0e-6, float(p.get("clinSlp", 1.0e-6)))                 # :555, 592
+        self.Gmar = float(p.get("Gmar", 0.0))                                        # :557
+        self.offshore = float(p.get("offshore", 100.0e5))                            # :558
         self.nl_pit_volume = float(p.get("nlPitVolume", 1.0e9))   # inputparser.py:562,584
         self.nl_pit_depth = float(p.get("nlPitDepth", 100.0))     # inputparser.py:563,585
         self.nl_pit_K = float(p.get("nlPitK", p.get("nonlinKm", 10.0)))             # inputparser.py:564
@@ -91,10 +97,18 @@ class OracleModel:
         self.marineSolver = str(p.get("marineSolver", "ts")).lower()                 # inputparser.py:576
         self.picardSub = int(p.get("picardSub", 10))
         self.picardIts = int(p.get("picardIts", 2))
+        if not self.nodep and self.seaDepo:
+            if self.Gmar > 0.0 and not self.flatModel:
+                raise NotImplementedError("marine transport-limited deposition (Gmar > 0, "
+                                          "seaplex.py:240-402) is not restated")
+            if self.marineSolver != "picard":
+                raise NotImplementedError("goSPL's adaptive TS solve of the marine diffusion is not "
+                                          "restated; use marineSolver picard")
         self.dexp = 0.05                                                             # hillslope.py:34
         self.minDiff = 1.0e-4                                                        # hillslope.py:35
         self._domainHasOutlet = len(self.outletIDs) > 0           # sedplex.py:45-47
         self.lcoords = np.asarray(coords, dtype=np.float64).reshape(-1, 3)
+        self.lcells = np.asarray(cells, dtype=np.int64)
         self.rainMesh = np.asarray(p["rain"], dtype=np.float64)
         up = p.get("upsub")
         self.upsub = None if up is None else np.asarray(up, dtype=np.float64)
@@ -933,6 +947,137 @@ class OracleModel:
         self._distributeSediment(hl)
         self._updateSinks(hl)
 
+
+    # ------------------------------------------------------ marine deposition
+    def _distanceCoasts(self, hl):
+        """seaplex.py:51-135 on one rank: the distance of every sea vertex
+        (seaID) to the nearest point of the coastline, the sea-level contour
+        of the elevation over the mesh triangles; 0 elsewhere and when there
+        is no coastline."""
+        self.coastDist = np.zeros(self.lpoints)
+        pts = coast_points(self.lcoords, self.lcells, hl, self.sealevel)
+        if len(pts) == 0:
+            return
+        from scipy import spatial
+        tree = spatial.cKDTree(pts, leafsize=10)
+        self.coastDist[self.seaID], _ = tree.query(self.lcoords[self.seaID, :], k=1)
+
+    def _smoothBathymetry(self):
+        """_hillSlope(smooth=2) (hillslope.py:124-139): one implicit step of
+        linear diffusion with K_d = N * area, N = 1 on land and 5 at sea
+        (tools/constants.py:126-127), solved exactly."""
+        Cd = np.full(self.lpoints, MARINE_SMOOTH_N_LAND)
+        Cd[self.seaID] = MARINE_SMOOTH_N_SEA
+        A = self.diffusion_matrix(Cd * self.larea)
+        return self._diffusion_solve(A, self.h.copy())
+
+    def _matOcean(self):
+        """seaplex.py:137-238: marine receivers on the epsilon-filled smoothed
+        bathymetry (every lower neighbour, equal weights), terminal sinks,
+        and the transposed routing matrix dMat1."""
+        hl = self.h.copy()
+        minh = self.h.min() + 0.1
+        if not self.flatModel:
+            minh = max(minh, self.oFill)
+            hsmth = self._smoothBathymetry()
+            hsmth[self.coastDist > self.offshore] = BOUNDARY_FLOW_SENTINEL
+        else:
+            minh = max(minh, self.oFill)
+            hsmth = hl.copy()
+            hsmth[self.outletIDs] = BOUNDARY_FLOW_SENTINEL
+        fillz = F.epsfill(minh, hsmth)
+        if not self.flatModel:
+            far = self.coastDist > self.offshore
+            fillz[far] = hl[far]
+        rcv, _, wght = F.mfdrcvrs(12, self.flowExp, fillz, BOUNDARY_FLOW_SENTINEL, self.gid)
+        if self.flatModel:
+            rcv[self.outletIDs, :] = np.tile(self.outletIDs, (12, 1)).T
+            wght[self.outletIDs, :] = 0.0
+        nodes = np.arange(self.lpoints)
+        self.is_sink_local = np.all(rcv.astype(int) == nodes[:, None], axis=1)
+        if self.flatModel:
+            self.is_sink_local[self.outletIDs] = False
+        data = wght.copy()
+        data[rcv == nodes[:, None]] = 0.0
+        # ADD_VALUES assembly: receivers shared by several directions sum
+        off = sp.csr_matrix((data.ravel(), rcv.ravel().astype(np.int64), np.arange(0, 12 * self.lpoints + 1, 12)),
+                            shape=(self.lpoints, self.lpoints))
+        off.sum_duplicates()
+        self.dMat1 = off.T.tocsr()
+        self.dMat1.sort_indices()
+
+    def _distOcean(self, sedflux):
+        """seaplex.py:404-619 (no provenance): the marine volumes pass down
+        dMat1 one hop per iteration; a cell keeps what fits in its remaining
+        capacity maxDepQs and passes the rest; terminal sinks keep all, open
+        outlets lose all; the iteration stops once the volume in transit is at
+        most max(1 m3, 1e-6 of the input) (or after 5000 passes) and what is
+        left in transit is deposited where it stands."""
+        marVol = self.maxDepQs.copy()
+        sinkVol = sedflux.copy()
+        vdep = np.zeros(self.lpoints)
+        sink = self.is_sink_local
+        if sink.any():
+            sink_mass = sinkVol[sink]
+            if (sink_mass != 0).any():
+                vdep[sink] += sink_mass
+                sinkVol[sink] = 0.0
+        tmp = sinkVol.copy()
+        sumExcess = float(np.sum(tmp))
+        threshold = max(1.0, 1.0e-6 * sumExcess)
+        step = 0
+        while sumExcess > threshold:
+            if step >= 5000:
+                break
+            sinkVol = self.dMat1 @ tmp
+            excess = sinkVol >= marVol
+            sinkVol[excess] -= marVol[excess]
+            vdep[excess] += marVol[excess]
+            marVol[excess] = 0.0
+            noexcess = np.invert(excess)
+            marVol[noexcess] -= sinkVol[noexcess]
+            vdep[noexcess] += sinkVol[noexcess]
+            vdep[self.outletIDs] = 0.0
+            sinkVol[noexcess] = 0.0
+            sinkVol[self.outletIDs] = 0.0
+            if sink.any():
+                vdep[sink] += sinkVol[sink]
+                sinkVol[sink] = 0.0
+            tmp = sinkVol.copy()
+            sumExcess = float(np.sum(tmp))
+            step += 1
+        self.marine_passes = step
+        if tmp.any():
+            vdep += tmp
+            vdep[self.outletIDs] = 0.0
+        return vdep
+
+    def seaChange(self):
+        """SEAMesh.seaChange (seaplex.py:738-861), one lithology, no
+        stratigraphy or provenance, Gmar = 0 on spheres, marineSolver picard:
+        clinoform capacity below sea level from the distance to the coast,
+        routing of the sediment flux reaching the sea (sinks of the sediment
+        fill) down the marine receivers, then non-linear diffusion of the
+        marine deposit over the sea cells (_diffuseOcean -> the Picard solve)."""
+        self.sinkIDs = self.lFill <= self.sealevel
+        hl = self.h.copy()
+        self._distanceCoasts(hl)                     # clinSlp >= 1e-6 always
+        clinoH = self.sealevel - 1.0e-3 - self.coastDist * self.clinSlp
+        clinoH[hl >= self.sealevel] = hl[hl >= self.sealevel]
+        clinoH[clinoH < hl] = hl[clinoH < hl]
+        self.maxDepQs = (clinoH - hl) * self.larea
+        sedFlux = self.vSed.copy() * self.dt
+        sedFlux[np.invert(self.sinkIDs)] = 0.0
+        sedFlux[sedFlux < 0] = 0.0
+        self._matOcean()
+        marDep = self._distOcean(sedFlux)
+        dh = np.divide(marDep, self.larea, out=np.zeros_like(self.larea), where=self.larea != 0)
+        dh[dh < DEPOSIT_FLOOR] = 0.0
+        ndepo = self._diffuseImplicitPicard(dh, self.seaID, self.nlK)     # _diffuseOcean, hillslope.py:739-787
+        self.cumED = self.cumED + ndepo
+        self.h = self.h + ndepo
+        self.EbLocal = self.EbLocal + ndepo / self.dt
+
     # ------------------------------------------------------------------- loop
     def step(self):
         """One iteration of runProcesses with fast=False (model.py:347-453):
@@ -943,6 +1088,8 @@ class OracleModel:
         if not self.nodep:
             self.flowAccumulation()
             self.sedChange()
+            if self.seaDepo:
+                self.seaChange()
         self.getHillslope()
         if self.tNow < self.tEnd:
             self.applyForces()
@@ -994,3 +1141,29 @@ def output_fields(h, cumED, Eb, waterFilled, fillFAL, FAL, vSed, upsub, rain, se
     if rain is not None:
         out["rain"] = col(rain)
     return out
+
+
+def coast_points(coords, cells, scalar, value):
+    """The points vtkContourFilter returns for the contour ``scalar ==
+    value`` over the triangles ``cells`` with triangle generation off, as
+    seaplex.py:105-120 uses it: marching triangles marks a vertex inside when
+    its scalar is >= value, and every edge with one end inside gives a point
+    interpolated from the end with the lower scalar,
+    t = (value - s_lo) / (s_hi - s_lo), x = x_lo + t (x_hi - x_lo); the point
+    locator merges the copies an edge's two triangles make (returned sorted,
+    unique)."""
+    cells = np.asarray(cells, dtype=np.int64)
+    if len(cells) == 0:
+        return np.zeros((0, 3))
+    e = np.concatenate([cells[:, [0, 1]], cells[:, [1, 2]], cells[:, [2, 0]]])
+    a, b = e[:, 0], e[:, 1]
+    cross = (scalar[a] >= value) != (scalar[b] >= value)
+    a, b = a[cross], b[cross]
+    up = (scalar[b] - scalar[a]) > 0
+    lo = np.where(up, a, b)
+    hi = np.where(up, b, a)
+    t = (value - scalar[lo]) / (scalar[hi] - scalar[lo])
+    x = coords[lo] + t[:, None] * (coords[hi] - coords[lo])
+    if len(x) == 0:
+        return np.zeros((0, 3))
+    return np.unique(x, axis=0)

@@ -97,6 +97,22 @@ def cases():
     p = dict(p, rain=rain, upsub=up, tEnd=10 * p["dt"], nodep=False, nlPitVolume=0.0, nlPitDepth=0.0,
              marineSolver="picard", picardSub=2, picardIts=2)
     out.append(("planar2k_lake", c, f, z, p, 3))
+    # marine deposition (seadepo on, Picard solver for the marine diffusion):
+    # a flat domain with its sea level at the 15th percentile of the relief,
+    # and the sphere with its ocean
+    c, f, z, rain, up, p = S.planar_config(n=2000, side=30.0e3, seed=7)
+    p = dict(p, rain=rain, upsub=up, tEnd=10 * p["dt"], nodep=False, seadepo=True, marineSolver="picard",
+             picardSub=2, picardIts=2, sealevel=float(np.percentile(z, 15)))
+    out.append(("planar2k_marine", c, f, z, p, 3))
+    c, f = S.icosphere(4)
+    z = S.rescale(S.sh_field(c, 48, 11), -4000.0, 3000.0)
+    g = S.sh_field(c, 16, 12)
+    rain = np.exp(0.5 * (g - g.mean()) / g.std())
+    up = S.belt_uplift(c, 13)
+    p = dict(dt=1.0e4, tEnd=1.0e5, flowDir=3, K=5.0e-7, d=0.0, m=0.5, Cda=0.05, Cdm=0.05,
+             sealevel=0.0, bc="oooo", rain=rain, upsub=up, nodep=False, seadepo=True, marineSolver="picard",
+             picardSub=2, picardIts=2)
+    out.append(("ico2562_marine", c, f, z, p, 3))
     return out
 
 
@@ -155,7 +171,7 @@ def main():
         for k in ("dt", "tEnd", "flowDir", "K", "d", "m", "Cda", "Cdm", "sealevel"):
             arrs["p_" + k] = np.array(params[k])
         arrs["p_bc"] = np.array(params["bc"])
-        for k in ("G", "nodep", "nlPitVolume", "nlPitDepth", "marineSolver", "picardSub", "picardIts"):
+        for k in ("G", "nodep", "nlPitVolume", "nlPitDepth", "marineSolver", "picardSub", "picardIts", "seadepo"):
             if k in params:
                 arrs["p_" + k] = np.array(params[k])
         for i, s in enumerate(snaps):

@@ -357,6 +357,9 @@ class _MPIComm:
         return x
 
     def Allgatherv(self, sendbuf, recv):
+        if isinstance(sendbuf, (list, tuple)):
+            sendbuf = sendbuf[0]
+        sendbuf = np.asarray(sendbuf).ravel()
         recvbuf = recv[0]
         recvbuf[: len(sendbuf)] = sendbuf
 
@@ -432,6 +435,125 @@ def _npi_module():
 
 
 # ---------------------------------------------------------------------------
+# vtk stand-in: the unstructured grid and contour filter seaplex.py:88-135
+# uses to extract the coastline
+# ---------------------------------------------------------------------------
+class _VtkArray:
+    def __init__(self, a):
+        self.a = np.array(a, copy=True)
+        self.name = None
+
+    def SetName(self, name):
+        self.name = name
+
+
+class _VtkPointData:
+    def __init__(self):
+        self.arrays = {}
+
+    def AddArray(self, arr):
+        self.arrays[arr.name] = arr
+
+
+class _VtkPoints:
+    def __init__(self, a=None):
+        self.a = a
+
+    def SetData(self, arr):
+        self.a = arr.a
+
+    def GetData(self):
+        return _VtkArray(self.a)
+
+
+class _VtkGrid:
+    """vtkUnstructuredGrid of triangles: points, cells, named point data."""
+
+    def __init__(self, points=None, cells=None):
+        self.points = None if points is None else np.asarray(points, dtype=np.float64)
+        self.cells = None if cells is None else np.asarray(cells, dtype=np.int64)
+        self.pd = _VtkPointData()
+
+    def GetPointData(self):
+        return self.pd
+
+    def SetFieldData(self, pd):
+        self.pd = pd
+
+    def SetPoints(self, pts):
+        self.points = pts.a
+
+
+class _VtkPolyOut:
+    def __init__(self, pts):
+        self.pts = pts
+
+    def GetPoints(self):
+        return None if self.pts is None else _VtkPoints(self.pts)
+
+
+class _VtkContourFilter:
+    """Marching triangles, one cell at a time as vtkTriangle::Contour does:
+    a vertex is inside when its scalar is >= the value; each edge with one
+    end inside gives the point interpolated from its lower-scalar end; a
+    point locator merges identical points (first-insertion order)."""
+
+    def SetInputData(self, grid):
+        self.grid = grid
+
+    def SetValue(self, i, v):
+        self.value = float(v)
+
+    def SetInputArrayToProcess(self, *a):
+        self.name = a[-1]
+
+    def GenerateTrianglesOff(self):
+        pass
+
+    def Update(self):
+        g = self.grid
+        s = g.pd.arrays[self.name].a
+        x = g.points
+        seen = {}
+        pts = []
+        for tri in g.cells:
+            for v0, v1 in ((tri[0], tri[1]), (tri[1], tri[2]), (tri[2], tri[0])):
+                if (s[v0] >= self.value) == (s[v1] >= self.value):
+                    continue
+                delta = s[v1] - s[v0]
+                if delta > 0:
+                    e1, e2 = v0, v1
+                else:
+                    e1, e2 = v1, v0
+                    delta = -delta
+                t = 0.0 if delta == 0.0 else (self.value - s[e1]) / delta
+                p = tuple(float(x[e1, j] + t * (x[e2, j] - x[e1, j])) for j in range(3))
+                if p not in seen:
+                    seen[p] = len(pts)
+                    pts.append(p)
+        self.out = _VtkPolyOut(np.array(pts, dtype=np.float64) if pts else None)
+
+    def GetOutput(self):
+        return self.out
+
+
+def _vtk_modules():
+    vtk = types.ModuleType("vtk")
+    vtk.vtkUnstructuredGrid = _VtkGrid
+    vtk.vtkPoints = _VtkPoints
+    vtk.vtkContourFilter = _VtkContourFilter
+    vtk.VTK_TRIANGLE = 5
+    vtk.vtkObject = types.SimpleNamespace(GlobalWarningDisplayOff=lambda: None)
+    util = types.ModuleType("vtk.util")
+    ns = types.ModuleType("vtk.util.numpy_support")
+    ns.numpy_to_vtk = lambda a, deep=1, **k: _VtkArray(a)
+    ns.vtk_to_numpy = lambda arr: np.asarray(arr.a)
+    util.numpy_support = ns
+    vtk.util = util
+    return {"vtk": vtk, "vtk.util": util, "vtk.util.numpy_support": ns}
+
+
+# ---------------------------------------------------------------------------
 # module loading
 # ---------------------------------------------------------------------------
 def load_reference(refroot):
@@ -441,10 +563,12 @@ def load_reference(refroot):
     sys.modules["petsc4py"] = _petsc_module()
     sys.modules["mpi4py"] = _mpi_module()
     sys.modules["numpy_indexed"] = _npi_module()
+    sys.modules.update(_vtk_modules())
     fort = types.ModuleType("gospl._fortran")
     for name in ("mfdreceivers", "sethillslopecoeff", "edge_tile", "fill_tile", "fill_edges",
                  "fill_dir", "nghb_dir", "getpitvol", "pits_cons", "fill_depressions",
-                 "graph_nodes", "combine_edges", "label_pits", "setmaxnb", "jacobiancoeff"):
+                 "graph_nodes", "combine_edges", "label_pits", "setmaxnb", "jacobiancoeff", "epsfill",
+                 "mfdrcvrs"):
         setattr(fort, name, getattr(F, name))
     for name in ("sort_ids", "hillslp_nl", "fctcoeff"):
         setattr(fort, name, lambda *a, **k: (_ for _ in ()).throw(NotImplementedError(name)))
@@ -463,7 +587,8 @@ def load_reference(refroot):
     SPLm = importlib.import_module("gospl.eroder.SPL")
     hill = importlib.import_module("gospl.sed.hillslope")
     sedplex = importlib.import_module("gospl.sed.sedplex")
-    return flowplex.FAMesh, pitfilling.PITFill, SPLm.SPL, hill.hillSLP, sedplex.SEDMesh
+    seaplex = importlib.import_module("gospl.sed.seaplex")
+    return flowplex.FAMesh, pitfilling.PITFill, SPLm.SPL, hill.hillSLP, sedplex.SEDMesh, seaplex.SEAMesh
 
 
 def load_meshfunc(refroot):
@@ -484,9 +609,9 @@ class _NullProfiler:
 
 
 def make_model_class(refroot):
-    FAMesh, PITFill, SPL, hillSLP, SEDMesh = load_reference(refroot)
+    FAMesh, PITFill, SPL, hillSLP, SEDMesh, SEAMesh = load_reference(refroot)
 
-    class RefModel(FAMesh, PITFill, SPL, hillSLP, SEDMesh):
+    class RefModel(FAMesh, PITFill, SPL, hillSLP, SEDMesh, SEAMesh):
         """One-rank goSPL model restricted to flowAccumulation / erodepSPL /
         getHillslope; forcing follows unstructuredmesh.py:743-972."""
 
@@ -560,16 +685,28 @@ def make_model_class(refroot):
             self.marineSolver = str(p.get("marineSolver", "ts"))
             self.picardSub = int(p.get("picardSub", 10))
             self.picardIts = int(p.get("picardIts", 2))
+            # marine deposition (inputparser.py:289, 554-592)
+            self.seaDepo = bool(p.get("seadepo", False))
+            self.nlK = float(p.get("nonlinKm", 10.0))
+            self.clinSlp = max(1.0e-6, float(p.get("clinSlp", 1.0e-6)))
+            self.Gmar = float(p.get("Gmar", 0.0))
+            self.offshore = float(p.get("offshore", 100.0e5))
+            self.lcells = np.asarray(mesh["cells"], dtype=np.int64)
+            self.vtkMesh = _VtkGrid(self.lcoords, self.lcells)
             FAMesh.__init__(self)
             PITFill.__init__(self)
             SPL.__init__(self)
             hillSLP.__init__(self)
             SEDMesh.__init__(self)
+            SEAMesh.__init__(self)
             self.applyForces()
             self.flowAccumulation()
 
         def _surfaceK(self):
             return np.ones(self.lpoints)
+
+        def _gatherGlobalOnRoot(self, local_full):
+            return np.array(local_full, copy=True)
 
         def _surfaceLithoK(self):
             return np.ones(self.lpoints)
@@ -598,6 +735,8 @@ def make_model_class(refroot):
             if not self.nodep:
                 self.flowAccumulation()
                 self.sedChange()
+                if self.seaDepo:
+                    self.seaChange()
             self.getHillslope()
             if self.tNow < self.tEnd:
                 self.applyForces()

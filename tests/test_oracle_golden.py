@@ -5,7 +5,8 @@ of the exact triangular solves)."""
 import numpy as np
 import pytest
 
-from conftest import GOLDEN_CASES, GOLDEN_G_CASES, GOLDEN_SED_CASES, golden_mesh, golden_params, load_golden
+from conftest import (GOLDEN_CASES, GOLDEN_G_CASES, GOLDEN_MARINE_CASES, GOLDEN_SED_CASES, golden_mesh,
+                      golden_params, load_golden)
 
 INT_KEYS = ("pitIDs", "flatDirs", "rcvIDi", "lsink", "lsinki", "pitInfo")
 FP_KEYS = ("h", "cumED", "EbLocal", "FAL", "fillFAL", "lFill", "waterFilled", "wghtVali",
@@ -24,7 +25,7 @@ def _compare(a, b, key, rtol):
         assert err <= rtol, (key, err)
 
 
-@pytest.mark.parametrize("case", GOLDEN_CASES + GOLDEN_G_CASES + GOLDEN_SED_CASES)
+@pytest.mark.parametrize("case", GOLDEN_CASES + GOLDEN_G_CASES + GOLDEN_SED_CASES + GOLDEN_MARINE_CASES)
 def test_mesh_geometry_matches_golden(case):
     from oracle import mesh as OM
     g = load_golden(case)
@@ -35,12 +36,15 @@ def test_mesh_geometry_matches_golden(case):
         assert np.array_equal(m[k], g[k]), k
 
 
-@pytest.mark.parametrize("case", GOLDEN_CASES + GOLDEN_SED_CASES)
+@pytest.mark.parametrize("case", GOLDEN_CASES + GOLDEN_SED_CASES + GOLDEN_MARINE_CASES)
 def test_oracle_steps_match_reference_orchestration(case):
     """Whole trajectories; the *_sed cases run with continental deposition
     (the reference's sedplex.py: sediment flux, depression filling with
     sediment, cascade over filled pits, bottom-up lake deposits with the
-    micro-tilt), and compare the routed sediment flux vSed as well."""
+    micro-tilt), and compare the routed sediment flux vSed as well; the
+    *_marine cases add marine deposition (seaplex.py: coastline distance,
+    clinoform capacity, epsilon-filled marine receivers, the capacity-limited
+    marine cascade and the Picard diffusion of the marine deposit)."""
     from oracle.model import OracleModel
     g = load_golden(case)
     params = golden_params(g)

@@ -62,3 +62,84 @@ def test_jacobiancoeff_derivative_term():
             c2 = 0.5 * (kd[k] + kd[j] + kp[j] * (h[j] - h[k])) / ar[k]
             assert d[k, s + 1] == -(c2 * vd[k, s] / el[k, s])
     assert d[k, 0] == diag
+
+
+def test_epsfill_matches_a_plain_priority_flood():
+    """epsfill (functions.F90:2633-2697) against a straightforward heapq
+    priority-flood with the same epsilon step: identical surfaces; the cells
+    below the level keep their elevation, and every cell the flood reached
+    has a strictly lower neighbour (no flats)."""
+    import heapq
+    from oracle import fortran as F
+    g, m = _mesh()
+    z = g["z"]
+    n = len(z)
+    ngb, nnb = np.asarray(m["ngb"]), np.asarray(m["nnb"])
+    sl = float(np.percentile(z, 20))
+    got = F.epsfill(sl, z)
+    fill = z.copy()
+    flag = fill < sl
+    heap = []
+    for i in range(n):
+        if flag[i] and any(fill[ngb[i, s]] >= sl for s in range(nnb[i]) if ngb[i, s] >= 0):
+            heapq.heappush(heap, (fill[i], i))
+    while heap:
+        zi, i = heapq.heappop(heap)
+        for s in range(nnb[i]):
+            c = ngb[i, s]
+            if c >= 0 and not flag[c]:
+                flag[c] = True
+                fill[c] = max(fill[c], np.nextafter(fill[i], np.inf))
+                heapq.heappush(heap, (fill[c], c))
+    assert np.array_equal(got, fill)
+    assert np.array_equal(got[z < sl], z[z < sl])
+    reached = (got >= sl)
+    for k in np.flatnonzero(reached)[::7]:
+        lower = [got[ngb[k, s]] < got[k] for s in range(nnb[k]) if ngb[k, s] >= 0]
+        assert any(lower), k
+
+
+def test_mfdrcvrs_equal_weights_over_lower_neighbours():
+    """mfdrcvrs (functions.F90:1673-1785): every strictly lower neighbour, in
+    neighbour order, is a receiver with the weight 1/kk rounded to single
+    precision (the literal `1.` is a default real); no lower neighbour:
+    every slot points at the vertex itself."""
+    from oracle import fortran as F
+    g, m = _mesh()
+    z = F.epsfill(float(g["z"].min()) + 0.1, g["z"])
+    n = len(z)
+    ngb, nnb, elgt = np.asarray(m["ngb"]), np.asarray(m["nnb"]), np.asarray(m["elgt"])
+    rcv, dist, wgt = F.mfdrcvrs(12, 1.1, z, -1.0e6, np.arange(n, dtype=np.int32))
+    for k in range(0, n, 11):
+        low = [(ngb[k, s], elgt[k, s]) for s in range(nnb[k]) if ngb[k, s] >= 0 and elgt[k, s] > 0 and z[ngb[k, s]] < z[k]]
+        kk = len(low)
+        if kk == 0:
+            assert (rcv[k] == k).all() and (wgt[k] == 0).all()
+            continue
+        assert list(rcv[k, :kk]) == [c for c, _ in low] and (rcv[k, kk:] == k).all()
+        assert list(dist[k, :kk]) == [e for _, e in low]
+        w = float(np.float32(1.0) / np.float32(kk))
+        assert (wgt[k, :kk] == w).all() and (wgt[k, kk:] == 0).all()
+
+
+def test_coast_points_marching_triangles():
+    """coast_points (vtkContourFilter as seaplex.py uses it) against a
+    triangle-by-triangle loop: the same set of points, each on a crossing
+    edge at the interpolated position."""
+    from oracle.model import coast_points
+    g, m = _mesh()
+    z = g["z"]
+    x = np.asarray(g["v"], np.float64).reshape(-1, 3)
+    cells = np.asarray(g["c"], np.int64)
+    level = float(np.percentile(z, 30))
+    got = coast_points(x, cells, z, level)
+    pts = set()
+    for tri in cells:
+        for a, b in ((tri[0], tri[1]), (tri[1], tri[2]), (tri[2], tri[0])):
+            if (z[a] >= level) == (z[b] >= level):
+                continue
+            lo, hi = (a, b) if z[b] - z[a] > 0 else (b, a)
+            t = (level - z[lo]) / (z[hi] - z[lo])
+            pts.add(tuple(x[lo] + t * (x[hi] - x[lo])))
+    assert len(got) == len(pts) > 0
+    assert set(map(tuple, got)) == pts
