@@ -4,6 +4,7 @@ jacobiancoeff (functions.F90:1423-1467) reduces to sethillslopecoeff
 diffusivity and Kp = 0, closes faces where either side has no diffusivity, and
 its Kp term follows the Fortran expression."""
 import numpy as np
+import pytest
 
 from conftest import golden_mesh, load_golden
 
@@ -143,3 +144,82 @@ def test_coast_points_marching_triangles():
             pts.add(tuple(x[lo] + t * (x[hi] - x[lo])))
     assert len(got) == len(pts) > 0
     assert set(map(tuple, got)) == pts
+
+
+def _marine_state(case, steps=1):
+    """An oracle model of a marine fixture advanced `steps` steps and then to
+    the point of seaChange where _distOcean runs: (model, sedFlux)."""
+    from conftest import golden_params
+    from oracle.model import OracleModel
+    g = load_golden(case)
+    om = OracleModel(g["v"], g["c"], g["z"], golden_params(g), mesh=golden_mesh(g))
+    for _ in range(steps):
+        om.step()
+    om.flowAccumulation()
+    om.erodepSPL()
+    om.flowAccumulation()
+    om.sedChange()
+    om.sinkIDs = om.lFill <= om.sealevel
+    hl = om.h.copy()
+    om._distanceCoasts(hl)
+    clinoH = om.sealevel - 1.0e-3 - om.coastDist * om.clinSlp
+    clinoH[hl >= om.sealevel] = hl[hl >= om.sealevel]
+    clinoH[clinoH < hl] = hl[clinoH < hl]
+    om.maxDepQs = (clinoH - hl) * om.larea
+    sed = om.vSed.copy() * om.dt
+    sed[~om.sinkIDs] = 0.0
+    sed[sed < 0] = 0.0
+    om._matOcean()
+    return om, sed
+
+
+@pytest.mark.parametrize("case", ["planar2k_marine", "ico2562_marine"])
+def test_marine_cascade_is_one_capacity_limited_sweep(case):
+    """_distOcean's iteration (seaplex.py:404-619) equals one sweep of the
+    marine DAG in topological order with a capacity clamp per vertex: a
+    vertex keeps min(arrivals, capacity) and passes its own input plus the
+    excess down its receivers; sinks keep all, outlets lose all.  The two
+    agree up to the volume the iteration leaves in transit when it stops
+    (deposited in place), at most max(1 m3, 1e-6 of the input)."""
+    import scipy.sparse as sp
+    om, sed = _marine_state(case)
+    it = om._distOcean(sed)
+    n = om.lpoints
+    W = om.dMat1.T.tocsr()                          # row j: j's receivers and weights
+    order = np.argsort(-_fillz(om), kind="stable")
+    arr = np.zeros(n)
+    dep = np.zeros(n)
+    cap = om.maxDepQs.copy()
+    out = set(np.asarray(om.outletIDs).tolist())
+    for j in order:
+        if om.is_sink_local[j]:
+            dep[j] = sed[j] + arr[j]
+            continue
+        if j in out:
+            continue
+        keep = min(arr[j], cap[j])
+        dep[j] = keep
+        send = sed[j] + arr[j] - keep
+        row = slice(W.indptr[j], W.indptr[j + 1])
+        arr[W.indices[row]] += send * W.data[row]
+    total = float(sed.sum())
+    assert np.abs(it - dep).sum() <= 2.0 * max(1.0, 1.0e-6 * total) + 1e-9 * total, (case, np.abs(it - dep).sum())
+    assert sp.issparse(om.dMat1)
+
+
+def _fillz(om):
+    """The epsilon-filled surface _matOcean routed on (recomputed as it does)."""
+    from oracle import fortran as F
+    from oracle.model import BOUNDARY_FLOW_SENTINEL
+    hl = om.h.copy()
+    minh = max(om.h.min() + 0.1, om.oFill)
+    if not om.flatModel:
+        hs = om._smoothBathymetry()
+        hs[om.coastDist > om.offshore] = BOUNDARY_FLOW_SENTINEL
+    else:
+        hs = hl.copy()
+        hs[om.outletIDs] = BOUNDARY_FLOW_SENTINEL
+    fz = F.epsfill(minh, hs)
+    if not om.flatModel:
+        fz[om.coastDist > om.offshore] = hl[om.coastDist > om.offshore]
+    return fz
