@@ -223,3 +223,58 @@ def _fillz(om):
     if not om.flatModel:
         fz[om.coastDist > om.offshore] = hl[om.coastDist > om.offshore]
     return fz
+
+
+@pytest.mark.parametrize("case", ["planar2k_marine", "ico2562_marine"])
+def test_epsfill_is_a_relaxation_fixpoint(case):
+    """epsfill's priority flood equals the fixpoint of the parallel
+    relaxation fill(c) = max(z(c), nextafter(min over flooded neighbours of
+    fill)) started from the seeds (cells below the level touching one at or
+    above it): a cell's value comes from its lowest flooded neighbour, and
+    the queue pops values in non-decreasing order.  Bit for bit, on the
+    smoothed bathymetry the marine routing fills."""
+    from oracle import fortran as F
+    om, _ = _marine_state(case, steps=0)
+    g = load_golden(case)
+    m = golden_mesh(g)
+    from oracle import mesh as OM
+    OM.load_mesh(m)
+    ngb = np.asarray(m["ngb"])
+    nnb = np.asarray(m["nnb"])
+    z = _fillz_input(om)
+    n = len(z)
+    W = ngb.shape[1]
+    valid = (np.arange(W)[None, :] < nnb[:, None]) & (ngb >= 0)
+    nb_ = np.where(valid, ngb, 0)
+    filled = 0
+    # the routing's own level (on the sphere nothing lies below it, so the
+    # flood never starts) and a level that floods the lowest tenth
+    for sl in (max(om.h.min() + 0.1, om.oFill), float(np.percentile(z, 10))):
+        ref = F.epsfill(sl, z)
+        below = z < sl
+        seeds = below & (valid & (z[nb_] >= sl)).any(axis=1)
+        val = np.full(n, np.inf)
+        val[seeds] = z[seeds]
+        for _ in range(n + 1):
+            nv = np.where(valid, val[nb_], np.inf).min(axis=1)
+            cand = np.where(np.isfinite(nv), np.maximum(z, np.nextafter(nv, np.inf)), np.inf)
+            new = np.where(below, val, cand)
+            if np.array_equal(new, val):
+                break
+            val = new
+        got = np.where(np.isfinite(val) & ~below, val, z)
+        assert np.array_equal(got, ref), sl
+        filled += int((ref > z).sum())
+    assert filled > 0
+
+
+def _fillz_input(om):
+    """The surface _matOcean hands to epsfill."""
+    from oracle.model import BOUNDARY_FLOW_SENTINEL
+    if not om.flatModel:
+        hs = om._smoothBathymetry()
+        hs[om.coastDist > om.offshore] = BOUNDARY_FLOW_SENTINEL
+    else:
+        hs = om.h.copy()
+        hs[om.outletIDs] = BOUNDARY_FLOW_SENTINEL
+    return hs
