@@ -278,3 +278,22 @@ def _fillz_input(om):
         hs = om.h.copy()
         hs[om.outletIDs] = BOUNDARY_FLOW_SENTINEL
     return hs
+
+
+@pytest.mark.parametrize("case", ["planar2k_marine", "ico2562_marine"])
+def test_coast_distance_is_a_plain_nearest_point_search(case):
+    """The k-d tree distances _distanceCoasts takes (scipy cKDTree, p = 2)
+    equal sqrt(min over coast points of (dx dx + dy dy) + dz dz) bit for
+    bit: a nearest-point search that sums the squares in that order, without
+    fused multiply-adds, reproduces them exactly."""
+    from scipy import spatial
+    from oracle.model import coast_points
+    om, _ = _marine_state(case, steps=0)
+    pts = coast_points(om.lcoords, om.lcells, om.h, om.sealevel)
+    q = om.lcoords[om.seaID]
+    d_tree, _ = spatial.cKDTree(pts, leafsize=10).query(q, k=1)
+    best = np.full(len(q), np.inf)
+    for p in pts:
+        dx, dy, dz = q[:, 0] - p[0], q[:, 1] - p[1], q[:, 2] - p[2]
+        best = np.minimum(best, (dx * dx + dy * dy) + dz * dz)
+    assert len(pts) > 0 and np.array_equal(np.sqrt(best), d_tree)
