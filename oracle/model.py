@@ -98,9 +98,6 @@ class OracleModel:
         self.picardSub = int(p.get("picardSub", 10))
         self.picardIts = int(p.get("picardIts", 2))
         if not self.nodep and self.seaDepo:
-            if self.Gmar > 0.0 and not self.flatModel:
-                raise NotImplementedError("marine transport-limited deposition (Gmar > 0, "
-                                          "seaplex.py:240-402) is not restated")
             if self.marineSolver != "picard":
                 raise NotImplementedError("goSPL's adaptive TS solve of the marine diffusion is not "
                                           "restated; use marineSolver picard")
@@ -1005,6 +1002,33 @@ class OracleModel:
         off.sum_duplicates()
         self.dMat1 = off.T.tocsr()
         self.dMat1.sort_indices()
+        if not self.flatModel and self.Gmar > 0.0:
+            d2 = (sp.identity(self.lpoints, format="csr") + off * -1.0).tocsr()
+            d2.sum_duplicates()
+            self.dMat2 = d2.T.tocsr()
+            self.dMat2.sort_indices()
+
+    def _depMarineSystem(self, sedflux):
+        """seaplex.py:240-402 (Gmar > 0, spheres): the coupled marine elevation
+        / flux system [[I - G, -G dt / A], [A / dt, dMat2]] [h; q] =
+        [(1 - G) h; sedflux / dt + h A (1 / dt)] with G = min(Gmar, 0.99) below
+        sea level and 0 above, solved exactly (goSPL: TFQMR with a Schur
+        fieldsplit to rtol); returns the deposited volumes (new h - h) * area,
+        negatives dropped."""
+        n = self.lpoints
+        hl = self.h.copy()
+        fDepm = np.full(n, self.Gmar)
+        fDepm[fDepm > 0.99] = 0.99
+        fDepm[hl > self.sealevel] = 0.0
+        A00 = sp.diags(-fDepm + 1.0, format="csr")
+        A01 = sp.diags(-fDepm * self.dt / self.larea, format="csr")
+        A10 = sp.diags(self.larea / self.dt, format="csr")
+        M = sp.bmat([[A00, A01], [A10, self.dMat2]], format="csc")
+        rhs = np.concatenate([(1.0 - fDepm) * self.h, sedflux / self.dt + (self.h * self.larea) * (1.0 / self.dt)])
+        x = spla.spsolve(M, rhs)
+        volDep = (x[:n] - self.h) * self.larea
+        volDep[volDep < 0] = 0.0
+        return volDep
 
     def _distOcean(self, sedflux):
         """seaplex.py:404-619 (no provenance): the marine volumes pass down
@@ -1054,7 +1078,7 @@ class OracleModel:
 
     def seaChange(self):
         """SEAMesh.seaChange (seaplex.py:738-861), one lithology, no
-        stratigraphy or provenance, Gmar = 0 on spheres, marineSolver picard:
+        stratigraphy or provenance, marineSolver picard:
         clinoform capacity below sea level from the distance to the coast,
         routing of the sediment flux reaching the sea (sinks of the sediment
         fill) down the marine receivers, then non-linear diffusion of the
@@ -1071,6 +1095,9 @@ class OracleModel:
         sedFlux[sedFlux < 0] = 0.0
         self._matOcean()
         marDep = self._distOcean(sedFlux)
+        if not self.flatModel and self.Gmar > 0.0:
+            vdep = self._depMarineSystem(marDep)
+            marDep = self._distOcean(vdep)
         dh = np.divide(marDep, self.larea, out=np.zeros_like(self.larea), where=self.larea != 0)
         dh[dh < DEPOSIT_FLOOR] = 0.0
         ndepo = self._diffuseImplicitPicard(dh, self.seaID, self.nlK)     # _diffuseOcean, hillslope.py:739-787

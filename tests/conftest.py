@@ -14,7 +14,7 @@ GOLDEN_G_CASES = ["ico2562_G05", "planar2k_G1"]
 # continental sediment routing and deposition (nodep off)
 GOLDEN_SED_CASES = ["incising_sed", "planar2k_sed", "ico2562_sed", "planar2k_lake"]
 # marine deposition (seadepo on): oracle only, the device path is not built
-GOLDEN_MARINE_CASES = ["planar2k_marine", "ico2562_marine"]
+GOLDEN_MARINE_CASES = ["planar2k_marine", "ico2562_marine", "ico2562_marine_G"]
 
 
 def pytest_configure(config):

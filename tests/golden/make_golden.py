@@ -113,6 +113,8 @@ def cases():
              sealevel=0.0, bc="oooo", rain=rain, upsub=up, nodep=False, seadepo=True, marineSolver="picard",
              picardSub=2, picardIts=2)
     out.append(("ico2562_marine", c, f, z, p, 3))
+    # marine deposition with the transport-limited marine system (Gmar > 0)
+    out.append(("ico2562_marine_G", c, f, z, dict(p, Gmar=0.5), 3))
     return out
 
 
@@ -171,7 +173,8 @@ def main():
         for k in ("dt", "tEnd", "flowDir", "K", "d", "m", "Cda", "Cdm", "sealevel"):
             arrs["p_" + k] = np.array(params[k])
         arrs["p_bc"] = np.array(params["bc"])
-        for k in ("G", "nodep", "nlPitVolume", "nlPitDepth", "marineSolver", "picardSub", "picardIts", "seadepo"):
+        for k in ("G", "nodep", "nlPitVolume", "nlPitDepth", "marineSolver", "picardSub", "picardIts", "seadepo",
+                  "Gmar"):
             if k in params:
                 arrs["p_" + k] = np.array(params[k])
         for i, s in enumerate(snaps):
