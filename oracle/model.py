@@ -28,6 +28,24 @@ MARINE_SMOOTH_N_SEA = 5.0        # gospl/tools/constants.py:127
 GRAPH_OUTLIER_CAP = 1.0e7        # gospl/tools/constants.py:100
 
 
+BUDGET_SLOTS = ("eroded", "pit_sinks", "kept", "dropped", "outlets", "sea", "retained", "excess", "zero_excess",
+                "inflow", "placed", "routed", "realised", "kept_deposit")
+
+
+def budget(b):
+    """Derived terms of a sediment budget: excess written at no spill node
+    (a spill node shared by several depressions keeps one depression's
+    excess, a depression without a spill node keeps none), placed excess left
+    unrouted, and the closure (eroded minus every destination), which
+    vanishes to rounding."""
+    b = dict(b)
+    b["unplaced"] = b["excess"] - b["placed"]
+    b["unrouted"] = b["placed"] - b["routed"]
+    b["closure"] = b["eroded"] - (b["retained"] + b["kept"] + b["dropped"] + b["outlets"] + b["sea"]
+                                  + b["zero_excess"] + b["unplaced"] + b["unrouted"])
+    return b
+
+
 def group_reduce(keys, values, op=np.add):
     """numpy_indexed.group_by(keys).reduce(values, op): (unique, reduced)."""
     keys = np.asarray(keys)
@@ -680,6 +698,7 @@ class OracleModel:
         Returns (excess, routed flux or None)."""
         excess = False
         changed = False
+        B = self.sed_budget
         csink = self.lsink & (self.pitIDs < 0)
         if csink.any():
             if not self._domainHasOutlet:
@@ -692,6 +711,11 @@ class OracleModel:
         inV[uID[ok]] = vol[ok]
         nvSed = np.zeros(self.lpoints)
         eV = inV - self.pitVol
+        # budget: the pass's inflow split (before pitVol changes)
+        B["retained"] += float(np.sum(np.where(eV > 0.0, self.pitVol, np.where(eV < 0.0, inV, 0.0))))
+        B["excess"] += float(np.sum(eV[eV > 0.0]))
+        B["zero_excess"] += float(np.sum(inV[eV == 0.0]))
+        B["inflow"] += float(np.sum(inV))
         if (eV > 0.0).any():
             eIDs = eV > 0.0
             spillIDs = self.pitInfo[eIDs, 0]
@@ -702,6 +726,7 @@ class OracleModel:
             ids = np.isin(self.pitIDs, np.where(eV > 0.0)[0])
             self.sedFilled[ids] = self.lFill[ids]
             changed = True
+            B["placed"] += float(nvSed.sum())
         eIDs = eV < 0
         self.pitVol[eIDs] -= inV[eIDs]
         self.pitVol[self.pitVol < 0] = 0.0
@@ -715,11 +740,29 @@ class OracleModel:
             if nvSed.sum() > 0.5 * self.maxarea[0]:
                 excess = True
                 routed = self._flow_solve(nvSed)
+                B["routed"] += float(nvSed.sum())
+                self._budget_cells(routed, self.wghtVal)
         return excess, routed
+
+    def _budget_cells(self, u, wgt):
+        """Sediment budget: the volumes u at the terminal cells of the graph
+        wgt (every weight 0), by kind (depression sinks, stray sinks kept on
+        a closed domain or dropped, open outlets, other terminal cells)."""
+        B = self.sed_budget
+        term = np.all(wgt == 0.0, axis=1)
+        out = np.zeros(self.lpoints, dtype=bool)
+        out[self.outletIDs] = True
+        lsink = self.lsink & ~out
+        B["outlets"] += float(np.sum(u[term & out]))
+        B["pit_sinks"] += float(np.sum(u[term & lsink & (self.pitIDs >= 0)]))
+        stray = float(np.sum(u[term & lsink & (self.pitIDs < 0)]))
+        B["dropped" if self._domainHasOutlet else "kept"] += stray
+        B["sea"] += float(np.sum(u[term & ~out & ~self.lsink]))
 
     def _distributeSediment(self, hl):
         """sedplex.py:376-522 (single lithology, no provenance)."""
         vSed = self.vSed.copy() * self.dt
+        self._budget_cells(vSed, self.wghtVali)
         self._closedDepo = np.zeros(self.lpoints)
         step = 0
         excess = True
@@ -735,6 +778,7 @@ class OracleModel:
                 vSed[self.outletIDs] = 0.0
             step += 1
         self.sed_passes = step
+        self.sed_budget["kept_deposit"] = float(np.sum(self._closedDepo))
         if self._closedDepo.any():
             delta = np.zeros(self.lpoints)
             nz = self._closedDepo > 0.0
@@ -934,7 +978,11 @@ class OracleModel:
         self.pitParams[:, 0] = self.pitVol.copy()
 
     def sedChange(self):
-        """sedplex.py:1061-1086."""
+        """sedplex.py:1061-1086.  Also keeps `sed_budget`, the step's sediment
+        budget (m3): where the eroded volume went (depressions, closed-domain
+        sinks, outlets, sea) and what the routing's rules drop (`budget`)."""
+        self.sed_budget = {k: 0.0 for k in BUDGET_SLOTS}
+        self.sed_budget["eroded"] = float(np.sum(-self.EbLocal * self.larea * self.dt))
         self._getSedFlux()
         self.fillElevation(sed=True)
         hl = self.h.copy()
@@ -943,6 +991,8 @@ class OracleModel:
         self.sedFilled = hl.copy()
         self._distributeSediment(hl)
         self._updateSinks(hl)
+        self.sed_budget["realised"] = float(np.sum(self.larea * (self.h - hl)))
+        self.sed_budget = budget(self.sed_budget)
 
 
     # ------------------------------------------------------ marine deposition
