@@ -1,9 +1,9 @@
 // Allocation-free variant of the flow-accumulation solve.
 //
 // Some callers cannot allocate device memory: code running inside another
-// application's CUDA context with a fixed memory budget, plugins driven from
-// a framework that owns every allocation, or a stream that is being captured
-// and must not call cudaMalloc.  gs_flow_solve_noalloc gives them the exact
+// application's CUDA context with a fixed memory budget, or plugins driven
+// from a framework that owns every allocation and forbids cudaMalloc outside
+// its own allocator.  gs_flow_solve_noalloc gives them the exact
 // solve of (I - W^T) q = b for a receiver graph without any allocation: every
 // scratch array lives in one file-scope __device__ array of fixed size, held
 // by each GPU that loads this library until the process exits.
@@ -13,8 +13,9 @@
 // one scratch array, so calls that overlap on the GPU (different streams, or
 // different host threads on the same device) race and must be serialised by
 // the caller.  The first call on a device resolves the array's device address
-// with cudaGetSymbolAddress (once per device, under a lock); make that first
-// call before any stream capture.
+// with cudaGetSymbolAddress (once per device, under a lock, with the device
+// of `stream` current); make that first call before any stream capture.  The
+// call synchronises `stream` to read the solve's status.
 #include <cub/cub.cuh>
 
 #include <mutex>
@@ -68,9 +69,21 @@ static NaLayout na_layout(unsigned char* base) {
 static std::mutex g_na_mutex;
 static unsigned char* g_na_ptr[64] = {nullptr};
 
-static int na_base(unsigned char** out) {
-    int dev = 0;
-    GS_CUDA(cudaGetDevice(&dev));
+// The device is the one that owns `s`; it must also be the current device,
+// since the symbol address and the launches are resolved there.
+static int na_device(cudaStream_t s, int* out) {
+    int cur = 0, dev = 0;
+    GS_CUDA(cudaGetDevice(&cur));
+    GS_CUDA(cudaStreamGetDevice(s, &dev));
+    if (dev != cur) {
+        set_error(GS_EINVAL, "gs_flow_solve_noalloc: the stream belongs to another device than the current one");
+        return GS_EINVAL;
+    }
+    *out = dev;
+    return GS_OK;
+}
+
+static int na_base(int dev, unsigned char** out) {
     if (dev < 0 || dev >= 64) {
         set_error(GS_EINVAL, "gs_flow_solve_noalloc: device index out of range");
         return GS_EINVAL;
@@ -253,10 +266,12 @@ extern "C" int gs_flow_solve_noalloc(int64_t nb, int32_t nrcv, const int32_t* rc
         set_error(GS_EINVAL, "gs_flow_solve_noalloc: null argument");
         return GS_EINVAL;
     }
-    unsigned char* base = nullptr;
-    GS_TRY(na_base(&base));
-    const int n = (int)nb, R = nrcv;
     cudaStream_t s = (cudaStream_t)stream;
+    int dev = 0;
+    GS_TRY(na_device(s, &dev));
+    unsigned char* base = nullptr;
+    GS_TRY(na_base(dev, &base));
+    const int n = (int)nb, R = nrcv;
     NaLayout L = na_layout(base);
     // the scratch keeps the previous call's contents: clear what must start at zero
     GS_CUDA(cudaMemsetAsync(L.cnt, 0, sizeof(int) * n, s));
@@ -274,9 +289,8 @@ extern "C" int gs_flow_solve_noalloc(int64_t nb, int32_t nrcv, const int32_t* rc
     NaSched sc{L.queue, L.ctr, L.left, (unsigned)n};
     NaFlowOp op{n, R, L.dptr, L.dlist, rcv, wgt, b, q, L.done};
     k_na_sources<<<G, B, 0, s>>>(op, sc, n);
-    int sms = 148, dev = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    int sms = 148;
+    GS_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     k_na_sweep<<<sms * 4, 128, 0, s>>>(op, sc, n, 4000000000ULL);
     GS_LAUNCH();
     unsigned h[8];

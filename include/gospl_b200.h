@@ -294,8 +294,8 @@ int gs_adjoint_step(gs_plan* plan, int32_t slot, double* lam, const double* rain
 /*
  * Allocation-free flow solve.  No counterpart in the reference: goSPL always
  * allocates its PETSc matrices and vectors.  For callers that cannot call
- * cudaMalloc (an embedding application that owns every allocation, a fixed
- * memory budget, a stream under capture), this solves (I - W^T) q = b for the
+ * cudaMalloc (an embedding application that owns every allocation, or one
+ * that runs under a fixed device-memory budget), this solves (I - W^T) q = b for the
  * receiver graph rcv/wgt ([nrcv][nb], as gs_mfdreceivers writes them) with
  * all scratch in a fixed file-scope device array, so it allocates nothing.
  * The caller passes inputs and the output q.  Limits: nb <= GS_NOALLOC_MAX_NB,
@@ -303,7 +303,9 @@ int gs_adjoint_step(gs_plan* plan, int32_t slot, double* lam, const double* rain
  * library holds the array (about 40 MB) until the process exits.  All calls
  * share it: calls that overlap on the GPU race and must be serialised by the
  * caller.  The first call on each device resolves the array's address (make
- * it before any stream capture).  Synchronises `stream` before returning.
+ * it before any stream capture).  `stream` must belong to the current device
+ * (else GS_EINVAL).  Synchronises `stream` before returning, to read the
+ * solve's status (GS_ECYCLE for a receiver graph with a cycle).
  */
 #define GS_NOALLOC_MAX_NB 1048576
 #define GS_NOALLOC_MAX_RCV 4
