@@ -331,6 +331,14 @@ int gs_sed_change(gs_plan* plan, double* h, double* cum_ed, const double* eb, co
                                    lfill, pit_ids, flat_dirs, rcv_i, wgt_i, lsink, sea, vsed, stats);)
 }
 
+int gs_sed_budget(gs_plan* plan, double* out16) {
+    NEED(plan);
+    NEED(out16);
+    for (int k = 0; k < 16; k++) out16[k] = 0.0;
+    if (!plan->led) return GS_OK;
+    GS_GUARD(return gs::sed_budget(plan, out16);)
+}
+
 int gs_hillslope(gs_plan* plan, double* h, double* cum_ed, double* eb, double sealevel, double cda, double cdm,
                  double dt, double rtol, int32_t max_iter, gs_stats* stats) {
     NEED(plan);

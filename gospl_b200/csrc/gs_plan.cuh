@@ -29,6 +29,8 @@ struct gs_plan {
     double* sed_buf = nullptr;           // [10][n] sediment-routing scratch
     uint8_t* sed_mask = nullptr;         // [5][n] sediment-routing masks
     double* sed_pit = nullptr;           // [2][n+1] per-depression scratch
+    double* led = nullptr;               // [16] sediment budget of the last sedChange (GS_LED_* slots)
+    double* led_part = nullptr;          // [5][LED_NB] block partial sums of the budget reductions
     double* sed_coef = nullptr;          // [W+1][n] lake diffusion operator (compacted to the lake cells)
     int* lake_i = nullptr;               // [W+1][n]: lake cell list, then the compact neighbour slots
     double* lake_d = nullptr;            // [3][n]: compact cell areas, right-hand side, solution
@@ -293,6 +295,7 @@ int sed_change(gs_plan* p, double* h, double* cum_ed, const double* eb, const do
                double ofill, double dt, double nl_pit_volume, double nl_pit_depth, double* lfill, int* pit_ids,
                int* flat_dirs, const int* rcv_i, const double* wgt_i, uint8_t* lsink, const uint8_t* sea,
                double* vsed, gs_stats* st);
+int sed_budget(gs_plan* p, double* out16);
 int diffusion_solve_on(gs_plan* p, int m, const int* nbr, const int8_t* nnb, const double* farea, const uint8_t* fix,
                        int flat, const uint8_t* outlet, const double* coef, const double* rhs, double* x, double rtol,
                        int max_iter, int* iters);

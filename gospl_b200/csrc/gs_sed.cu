@@ -494,12 +494,136 @@ __global__ void k_lake_scale(int n, const int* __restrict__ pit, const uint8_t* 
     ddiff[i] = d;
 }
 
+// --- sediment budget (gs_sed_budget) -------------------------------------
+// Each reduction runs on LED_NB blocks whatever n is: a block walks a fixed
+// strided set of indices, sums per thread in index order, then a fixed warp
+// butterfly and warp order; k_led_final adds the block sums in block order.
+// The result therefore depends on the data and n only.
+constexpr int LED_NB = 296;
+constexpr int LED_T = 256;
+
+template <int C>
+__device__ __forceinline__ void led_block(const double (&v)[C], double* part) {
+    __shared__ double sh[C][LED_T / 32];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+    for (int c = 0; c < C; c++) {
+        const double t = warp_sum(v[c]);
+        if (lane == 0) sh[c][w] = t;
+    }
+    __syncthreads();
+    if (threadIdx.x < C) {
+        double t = 0.0;
+        for (int k = 0; k < LED_T / 32; k++) t += sh[threadIdx.x][k];
+        part[threadIdx.x * LED_NB + blockIdx.x] = t;
+    }
+}
+
+// volumes u at the terminal cells of the graph wgt ([R][n], every weight 0),
+// by kind: depression sinks, stray sinks kept (member without outlet), stray
+// sinks dropped, open outlets, other terminal cells (sea)
+__global__ void __launch_bounds__(LED_T) k_led_cells(int n, int R, const double* __restrict__ u,
+                                                     const double* __restrict__ wgt, const uint8_t* __restrict__ lsink,
+                                                     const int* __restrict__ pit, const uint8_t* __restrict__ outlet,
+                                                     const uint8_t* __restrict__ mout, const int* __restrict__ vmember,
+                                                     double* part) {
+    double v[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    for (int i = blockIdx.x * LED_T + threadIdx.x; i < n; i += LED_NB * LED_T) {
+        bool term = true;
+        for (int k = 0; k < R; k++)
+            if (wgt[(size_t)k * n + i] != 0.0) term = false;
+        if (!term) continue;
+        const double x = u[i];
+        if (outlet[i]) v[3] += x;
+        else if (lsink[i]) {
+            if (pit[i] >= 0) v[0] += x;
+            else if (mout[vmember[i]]) v[2] += x;
+            else v[1] += x;
+        } else v[4] += x;
+    }
+    led_block<5>(v, part);
+}
+
+// one pass's split of the depressions' inflow, read before k_sed_pits
+// updates pitVol: retained, excess (eV > 0), inflow with eV == 0, inflow
+__global__ void __launch_bounds__(LED_T) k_led_pits(int np1, const double* __restrict__ inV,
+                                                    const double* __restrict__ vol, const int* __restrict__ pmember,
+                                                    const uint8_t* __restrict__ mact, double* part) {
+    double v[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int q = blockIdx.x * LED_T + threadIdx.x; q < np1; q += LED_NB * LED_T) {
+        if (!mact[pmember[q]]) continue;
+        const double in = inV[q];
+        const double e = in - vol[q];
+        if (e > 0.0) {
+            v[0] += vol[q];
+            v[1] += e;
+        } else if (e < 0.0) v[0] += in;
+        else v[2] += in;
+        v[3] += in;
+    }
+    led_block<4>(v, part);
+}
+
+// sum(x * scale), or sum((x - y) * scale) when y is given
+__global__ void __launch_bounds__(LED_T) k_led_sum(int n, const double* __restrict__ x, const double* __restrict__ y,
+                                                   const double* __restrict__ scale_v, double scale, double* part) {
+    double v[1] = {0.0};
+    for (int i = blockIdx.x * LED_T + threadIdx.x; i < n; i += LED_NB * LED_T) {
+        double a = y ? (x[i] - y[i]) : x[i];
+        a = scale_v ? a * scale_v[i] : a * scale;
+        v[0] += a;
+    }
+    led_block<1>(v, part);
+}
+
+// led[slot + c] += sum of the block sums of category c, c < C, block order
+__global__ void __launch_bounds__(LED_T) k_led_final(int C, const double* __restrict__ part, double* led, int slot) {
+    __shared__ double sh[LED_T / 32];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    for (int c = 0; c < C; c++) {
+        double t = 0.0;
+        for (int b = threadIdx.x; b < LED_NB; b += LED_T) t += part[c * LED_NB + b];
+        t = warp_sum(t);
+        if (lane == 0) sh[w] = t;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double a = 0.0;
+            for (int k = 0; k < LED_T / 32; k++) a += sh[k];
+            led[slot + c] += a;
+        }
+        __syncthreads();
+    }
+}
+
 __global__ void k_sed_pitfinal(int np1, const double* __restrict__ vol, double* params) {
     int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p < np1) params[3 * p] = vol[p];
 }
 
 }  // namespace
+
+static int led_cells(gs_plan* p, const double* u, const double* wgt, const uint8_t* lsink, const int* pit,
+                     const uint8_t* mout) {
+    launch(p, k_led_cells, LED_NB, LED_T, (int)p->n, p->R, u, wgt, lsink, pit, (const uint8_t*)p->outlet, mout,
+           (const int*)p->vmember, p->led_part);
+    launch(p, k_led_final, 1, LED_T, 5, (const double*)p->led_part, p->led, (int)GS_LED_PIT_SINKS);
+    GS_LAUNCH();
+    return GS_OK;
+}
+
+static int led_sum(gs_plan* p, int n, const double* x, const double* y, const double* scale_v, double scale,
+                   int slot) {
+    launch(p, k_led_sum, LED_NB, LED_T, n, x, y, scale_v, scale, p->led_part);
+    launch(p, k_led_final, 1, LED_T, 1, (const double*)p->led_part, p->led, slot);
+    GS_LAUNCH();
+    return GS_OK;
+}
+
+int sed_budget(gs_plan* p, double* out16) {
+    GS_CUDA(cudaMemcpyAsync(out16, p->led, sizeof(double) * 16, cudaMemcpyDeviceToHost, p->stream));
+    GS_CUDA(cudaStreamSynchronize(p->stream));
+    return GS_OK;
+}
 
 int sed_change(gs_plan* p, double* h, double* cum_ed, const double* eb, const double* xyz, double sealevel,
                double ofill, double dt, double nl_pit_volume, double nl_pit_depth, double* lfill, int* pit_ids,
@@ -522,6 +646,9 @@ int sed_change(gs_plan* p, double* h, double* cum_ed, const double* eb, const do
     uint8_t* sea_s = p->sed_mask;
     uint8_t* tmask = sea_s + n;
     uint8_t* mout = tmask + n;   // [nmem] (nmem <= n)
+    if (!p->led) GS_CUDA(cudaMalloc((void**)&p->led, sizeof(double) * 16));
+    if (!p->led_part) GS_CUDA(cudaMalloc((void**)&p->led_part, sizeof(double) * 5 * LED_NB));
+    GS_CUDA(cudaMemsetAsync(p->led, 0, sizeof(double) * 16, p->stream));
     GS_CUDA(cudaMemsetAsync(mout, 0, (size_t)p->nmem, p->stream));
     if (p->n_outlet > 0)
         launch(p, k_sed_moutlet, grid_for(p->n_outlet, B), B, p->n_outlet, (const int*)p->outlet_ids,
@@ -543,6 +670,9 @@ int sed_change(gs_plan* p, double* h, double* cum_ed, const double* eb, const do
     GS_TRY(sink_mask(p, wgt_i, sea, lsink));
     launch(p, k_sed_init, G, B, n, (const double*)vsed, (const double*)h, dt, vol, hl, sfill, closed);
     GS_LAUNCH();
+    // budget: the eroded volume, and where the snapshot solve delivers it
+    GS_TRY(led_sum(p, n, p->q2, nullptr, nullptr, dt, GS_LED_ERODED));
+    GS_TRY(led_cells(p, vol, wgt_i, lsink, pit_ids, mout));
 
     launch(p, k_sed_pitvol, grid_for(np1, B), B, np1, (const double*)p->pit_params, p->pit_vol);
     GS_LAUNCH();
@@ -575,6 +705,9 @@ int sed_change(gs_plan* p, double* h, double* cum_ed, const double* eb, const do
         GS_TRY(group_sum_by_pit(p, pit_ids, lsink, vol, p->pit_in, P));
         GS_CUDA(cudaMemsetAsync(p->mflags, 0, sizeof(int) * nm, p->stream));
         launch(p, k_fill_int_s, G, B, n, p->pit_win, -1);
+        launch(p, k_led_pits, LED_NB, LED_T, np1, (const double*)p->pit_in, (const double*)p->pit_vol,
+               (const int*)p->pmember, (const uint8_t*)p->mact, p->led_part);
+        launch(p, k_led_final, 1, LED_T, 4, (const double*)p->led_part, p->led, (int)GS_LED_RETAINED);
         launch(p, k_sed_pits, grid_for(np1, B), B, np1, (const double*)p->pit_in, p->pit_vol,
                (const int*)p->pit_info, (const int*)p->pmember, (const uint8_t*)p->mact, p->pit_ev, p->pit_state,
                p->pit_win, p->mflags);
@@ -596,6 +729,7 @@ int sed_change(gs_plan* p, double* h, double* cum_ed, const double* eb, const do
             launch(p, k_sed_cells, G, B, n, (const int*)pit_ids, (const uint8_t*)p->pit_state, (const double*)lfill,
                    sfill);
             GS_LAUNCH();
+            GS_TRY(led_sum(p, n, nv, nullptr, nullptr, 1.0, GS_LED_PLACED));
         }
         if (any(big)) {
             if (any(rebuild)) {
@@ -635,6 +769,8 @@ int sed_change(gs_plan* p, double* h, double* cum_ed, const double* eb, const do
                 const int ok = p->h_pinned[0] ? 0 : 1;
                 GS_TRY(flow_run(p, p->rcv, p->wgt, p->rslot, nv, routed, &cyc, p->order, ok));
                 total_cycles += cyc;
+                GS_TRY(led_sum(p, n, nv, nullptr, nullptr, 1.0, GS_LED_ROUTED));
+                GS_TRY(led_cells(p, routed, p->wgt, lsink, pit_ids, mout));
                 launch(p, k_sed_accum, G, B, n, (const double*)routed, (const double*)hl, (const double*)sfill,
                        (const uint8_t*)p->outlet, dt, (const int*)p->vmember, (const uint8_t*)p->msolve, vol, vsed);
                 GS_LAUNCH();
@@ -672,6 +808,7 @@ int sed_change(gs_plan* p, double* h, double* cum_ed, const double* eb, const do
         return GS_EINVAL;
     }
     // sediment kept at closed terminal sinks (sedplex.py:486-500)
+    GS_TRY(led_sum(p, n, closed, nullptr, nullptr, 1.0, GS_LED_KEPT_DEP));
     launch(p, k_sed_closed, G, B, n, (const double*)closed, (const double*)p->larea, h, cum_ed);
     launch(p, k_sed_ones, G, B, n, routed);
     GS_LAUNCH();
@@ -773,6 +910,7 @@ int sed_change(gs_plan* p, double* h, double* cum_ed, const double* eb, const do
            cum_ed);
     launch(p, k_sed_pitfinal, grid_for(np1, B), B, np1, (const double*)p->pit_vol, p->pit_params);
     GS_LAUNCH();
+    GS_TRY(led_sum(p, n, h, hl, (const double*)p->larea, 0.0, GS_LED_REALISED));
     return GS_OK;
 }
 

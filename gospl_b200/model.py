@@ -314,6 +314,22 @@ class Model:
         self.npits = st.npits
         self.stats["sed"] = st.as_dict()
 
+    def sed_budget(self):
+        """Sediment budget of the last sedChange (m3 over the step): where
+        the volume eroded by the step's SPL went in the continental routing
+        (gs_sed_budget: depressions, closed-domain sinks, outlets, sea, and
+        what goSPL's routing rules drop), plus `closure`, the eroded volume
+        minus every destination, which must vanish to rounding."""
+        L = _lib_handle()
+        out = np.zeros(16)
+        _lib.check(L.gs_sed_budget(self._plan, out.ctypes.data_as(ctypes.c_void_p)))
+        b = {k: float(out[i]) for i, k in enumerate(_lib.LED_SLOTS)}
+        b["unplaced"] = b["excess"] - b["placed"]
+        b["unrouted"] = b["placed"] - b["routed"]
+        b["closure"] = b["eroded"] - (b["retained"] + b["kept"] + b["dropped"] + b["outlets"] + b["sea"]
+                                      + b["zero_excess"] + b["unplaced"] + b["unrouted"])
+        return b
+
     def getHillslope(self):
         L = _lib_handle()
         st = _lib.GsStats()

@@ -243,6 +243,43 @@ int gs_sed_change(gs_plan* plan, double* h, double* cum_ed, const double* eb, co
                   const double* wgt_i, uint8_t* lsink, const uint8_t* sea, double* vsed,
                   gs_stats* stats);
 
+/*
+ * Sediment budget of the last gs_sed_change (m^3 over the step), summed on
+ * the device in a fixed order.  No single counterpart in the reference: it
+ * accounts, pass by pass, for where the volume eroded by the step's SPL goes
+ * in goSPL's continental routing (sedplex.py:103-522), including the volume
+ * that goSPL's own rules drop.  Every flow solve of the routing delivers its
+ * input to terminal cells (all weights 0), which are split into depression
+ * sinks, stray sinks kept on closed domains (sedplex.py:230-245), stray sinks
+ * dropped on domains with an outlet, open outlets and the sea; every pass
+ * splits the depressions' inflow into the retained volume, the excess (eV >
+ * 0) and inflow equal to the remaining volume (eV == 0, which goSPL drops);
+ * the excess is placed at spill nodes (one pit wins a shared spill node, a
+ * depression without a spill node places nothing) and routed when it exceeds
+ * half the largest cell area (sedplex.py:343-350).
+ *   eroded = retained + kept + dropped + outlets + sea + zero_excess
+ *            + (excess - placed) + (placed - routed)
+ * closes to rounding.  `realised` is the volume the step's deposits add to
+ * the surface, sum(larea * dh); it differs from retained + kept by goSPL's
+ * bottom-up lake level (np.interp over the depth-volume table) and tilt.
+ * out[16] receives the GS_LED_* slots.
+ */
+#define GS_LED_ERODED 0      /* sum(-Eb * larea) * dt                              */
+#define GS_LED_PIT_SINKS 1   /* volume reaching depression sinks (all passes)      */
+#define GS_LED_KEPT 2        /* stray sinks, domain without outlet: deposited      */
+#define GS_LED_DROPPED 3     /* stray sinks, domain with an outlet: leaves         */
+#define GS_LED_OUTLETS 4     /* reaching open outlets: leaves the domain           */
+#define GS_LED_SEA 5         /* reaching other terminal cells (sea): leaves        */
+#define GS_LED_RETAINED 6    /* kept by depressions                                */
+#define GS_LED_EXCESS 7      /* overflow of depressions (eV > 0)                   */
+#define GS_LED_ZERO 8        /* inflow of depressions with eV == 0                 */
+#define GS_LED_INFLOW 9      /* total inflow of depressions (all passes)           */
+#define GS_LED_PLACED 10     /* excess written at spill nodes                      */
+#define GS_LED_ROUTED 11     /* placed excess that was routed downstream           */
+#define GS_LED_REALISED 12   /* sum(larea * (h_after - h_before)) of sedChange     */
+#define GS_LED_KEPT_DEP 13   /* sum of the closed-domain deposit volumes           */
+int gs_sed_budget(gs_plan* plan, double* out16);
+
 int gs_hillslope(gs_plan* plan, double* h, double* cum_ed, double* eb, double sealevel,
                  double cda, double cdm, double dt, double rtol, int32_t max_iter,
                  gs_stats* stats);

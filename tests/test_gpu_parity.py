@@ -217,6 +217,32 @@ def _compare_sed(gm, om, tag):
     hs = float(np.abs(om.h).max())
     assert np.abs(_np(gm.hGlobal) - om.h).max() <= 1e-12 * hs, "%s h" % tag
     assert np.abs(_np(gm.cumED) - om.cumED).max() <= 1e-12 * hs, "%s cumED" % tag
+    _compare_budget(gm, om, tag, hs)
+
+
+BUDGET_TERMS = ("eroded", "pit_sinks", "kept", "dropped", "outlets", "sea", "retained", "excess", "zero_excess",
+                "inflow", "placed", "routed", "kept_deposit")
+
+
+def _compare_budget(gm, om, tag, hs):
+    """Sediment budget of the sedChange (gs_sed_budget): the eroded volume
+    minus every destination closes to 1e-12 of the eroded volume on the GPU,
+    and every term agrees with the oracle's budget to 1e-11 of it; the
+    deposited volume sum(larea * dh) to the elevation tolerance over the
+    area."""
+    bg = gm.sed_budget()
+    bo = om.sed_budget
+    E = bo["eroded"]
+    if E <= 0.0:
+        return
+    assert abs(bg["closure"]) <= 1e-12 * E, "%s GPU budget closure %g of the eroded volume" % (
+        tag, bg["closure"] / E)
+    assert abs(bo["closure"]) <= 1e-12 * E, "%s oracle budget closure %g" % (tag, bo["closure"] / E)
+    assert abs(bg["pit_sinks"] - bg["inflow"]) <= 1e-12 * E, "%s depression inflow" % tag
+    for k in BUDGET_TERMS:
+        assert abs(bg[k] - bo[k]) <= 1e-11 * E, "%s budget %s: %r vs %r" % (tag, k, bg[k], bo[k])
+    area = float(np.sum(om.larea))
+    assert abs(bg["realised"] - bo["realised"]) <= 1e-11 * E + 1e-12 * hs * area, "%s realised" % tag
 
 
 @pytest.mark.parametrize("case", GOLDEN_SED_CASES)
