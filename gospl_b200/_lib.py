@@ -20,7 +20,7 @@ ERRORS = {1: "GS_EINVAL", 2: "GS_ECUDA", 3: "GS_EMAXITER", 4: "GS_ENONFINITE", 5
 EXPORTS = ("gs_version", "gs_last_error", "gs_plan_create", "gs_plan_destroy", "gs_plan_set_members",
            "gs_plan_tune", "gs_plan_tuning", "gs_plan_set_precision", "gs_plan_set_deposition",
            "gs_plan_set_stream",
-           "gs_plan_launches", "gs_mfdreceivers", "gs_fill_elevation", "gs_pit_tables",
+           "gs_plan_launches", "gs_mfdreceivers", "gs_fill_elevation", "gs_build_flow_direction", "gs_pit_tables",
            "gs_flow_accumulation", "gs_erodep_spl", "gs_sed_change", "gs_sed_budget", "gs_plan_set_lake_diffusion", "gs_hillslope", "gs_apply_forces", "gs_output_fields", "gs_mesh_geometry", "gs_plan_profile",
            "gs_plan_profile_report", "gs_plan_profile_trace", "gs_plan_record", "gs_plan_record_slot",
            "gs_adjoint_step", "gs_flow_solve_noalloc")
@@ -71,7 +71,8 @@ def load(path=None):
     L.gs_plan_launches.argtypes = [P]
     L.gs_plan_launches.restype = i64
     L.gs_mfdreceivers.argtypes = [P, i32, d, P, d, P, P, P, P]
-    L.gs_fill_elevation.argtypes = [P, P, d, d, P, P, P, P]
+    L.gs_fill_elevation.argtypes = [P, P, d, d, i32, P, P, P, P]
+    L.gs_build_flow_direction.argtypes = [P, P, i32, d, P, P, P, P, P, P, P, P]
     L.gs_pit_tables.argtypes = [P, P, P, P, P]
     L.gs_flow_accumulation.argtypes = [P, P, P, d, d, d, P, P, P, P, P, P, P, P, P, P, P,
                                        ctypes.POINTER(GsStats)]

@@ -224,7 +224,7 @@ int gs_mfdreceivers(gs_plan* plan, int32_t nrcv, double exp, const double* elev,
     GS_GUARD(return gs::receivers(plan, nrcv, exp, elev, sl, gid, rcv, dist, wgt, nullptr);)
 }
 
-int gs_fill_elevation(gs_plan* plan, const double* h, double sealevel, double ofill, double* lfill,
+int gs_fill_elevation(gs_plan* plan, const double* h, double sealevel, double ofill, int32_t sed, double* lfill,
                       int32_t* pit_ids, int32_t* flat_dirs, int32_t* npits) {
     NEED(plan);
     if (plan->n > 0) {
@@ -235,10 +235,25 @@ int gs_fill_elevation(gs_plan* plan, const double* h, double sealevel, double of
     }
     GS_GUARD({
         gs_stats st{};
-        int s = gs::fill_elevation(plan, h, sealevel, ofill, lfill, pit_ids, flat_dirs, &st);
+        int s = gs::fill_elevation(plan, h, sealevel, ofill, lfill, pit_ids, flat_dirs, &st, false, nullptr,
+                                   sed != 0);
         if (npits) *npits = plan->npits;
         return s;
     })
+}
+
+int gs_build_flow_direction(gs_plan* plan, const double* h, int32_t down, double sealevel, const double* lfill,
+                            const int32_t* pit_ids, const int32_t* flat_dirs, int32_t* rcv, double* dist,
+                            double* wgt, uint8_t* lsink, uint8_t* sea) {
+    NEED(plan);
+    if (plan->n > 0) {
+        NEED(h); NEED(lfill); NEED(pit_ids); NEED(flat_dirs); NEED(rcv); NEED(dist); NEED(wgt); NEED(lsink);
+        NEED(sea);
+    }
+    // the plan's live-graph slot table is scratch here: every stage that
+    // reads it rebuilds it together with its own receivers first
+    GS_GUARD(return gs::flow_direction(plan, h, down != 0, lfill, pit_ids, flat_dirs, sealevel, rcv, dist, wgt,
+                                       plan->rslot, lsink, sea);)
 }
 
 int gs_pit_tables(gs_plan* plan, double* pit_params, int32_t* pit_info, double* filled_lvl,

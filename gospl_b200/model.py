@@ -148,6 +148,7 @@ class Model:
         self.lsink_mask = torch.zeros(n, **u8)
         self.sea_mask = torch.zeros(n, **u8)
         self.vSed = torch.zeros(n, **f64)
+        self.rcv_live = None                     # live receivers of _buildFlowDirection
         self.xyz = None
         if not self.nodep:
             if coords is None:
@@ -242,13 +243,14 @@ class Model:
         self.rainVal = self.rainMesh.clamp(min=0.0)   # unstructuredmesh.py:960
 
     def fillElevation(self, sed=False):
-        """pitfilling.py:849-903; per-pit tables read with pit_tables().  The
-        sediment fill (sed=True) runs inside sedChange."""
-        if sed:
-            raise NotImplementedError("fillElevation(sed=True) runs inside sedChange()")
+        """pitfilling.py:849-903: lFill, pitIDs and flatDirs of the current
+        elevation, per-pit tables read with pit_tables().  sed=True is the
+        sediment fill (marine depressions filled too, pits labelled above the
+        fill level, volumes on the unclipped surface), which sedChange also
+        runs itself."""
         L = _lib_handle()
         npits = ctypes.c_int32()
-        _lib.check(L.gs_fill_elevation(self._plan, _lib.ptr(self.hGlobal), self.sealevel, self.oFill,
+        _lib.check(L.gs_fill_elevation(self._plan, _lib.ptr(self.hGlobal), self.sealevel, self.oFill, int(bool(sed)),
                                        _lib.ptr(self.lFill), _lib.ptr(self.pitIDs), _lib.ptr(self.flatDirs),
                                        ctypes.byref(npits)))
         self.npits = int(npits.value)
@@ -266,15 +268,34 @@ class Model:
         return pp, pi, fl, fv
 
     def _buildFlowDirection(self, h, down=True):
-        """mfdreceivers only (flowplex.py:499-501) into [R, N] tensors."""
+        """FAMesh._buildFlowDirection (flowplex.py:480-544): the flow graph
+        of the surface h.  Sets the live receivers rcvID, distRcv, wghtVal
+        (views [N, R] of [R, N] storage), lsink and seaID on the model: MFD
+        receivers of h, with down=True the pit-flat routing over the last
+        fill (lFill, pitIDs, flatDirs), flat-model outlets as self-sinks."""
         t = self.torch
         R, n = self.flowDir, self.lpoints
-        rcv = t.empty((R, n), dtype=t.int32, device=self.dev)
-        dist = t.empty((R, n), dtype=t.float64, device=self.dev)
-        wgt = t.empty((R, n), dtype=t.float64, device=self.dev)
-        _lib.check(_lib_handle().gs_mfdreceivers(self._plan, R, self.flowExp, _lib.ptr(h), self.sealevel, None,
-                                                 _lib.ptr(rcv), _lib.ptr(dist), _lib.ptr(wgt)))
-        return rcv, dist, wgt
+        if self.rcv_live is None:
+            self.rcv_live = t.empty((R, n), dtype=t.int32, device=self.dev)
+            self.dist_live = t.empty((R, n), dtype=t.float64, device=self.dev)
+            self.wgt_live = t.empty((R, n), dtype=t.float64, device=self.dev)
+        h = t.as_tensor(h, dtype=t.float64, device=self.dev).contiguous()
+        _lib.check(_lib_handle().gs_build_flow_direction(
+            self._plan, _lib.ptr(h), int(bool(down)), self.sealevel, _lib.ptr(self.lFill), _lib.ptr(self.pitIDs),
+            _lib.ptr(self.flatDirs), _lib.ptr(self.rcv_live), _lib.ptr(self.dist_live), _lib.ptr(self.wgt_live),
+            _lib.ptr(self.lsink_mask), _lib.ptr(self.sea_mask)))
+
+    @property
+    def rcvID(self):
+        return self.rcv_live.t()
+
+    @property
+    def wghtVal(self):
+        return self.wgt_live.t()
+
+    @property
+    def distRcv(self):
+        return self.dist_live.t()
 
     def flowAccumulation(self):
         L = _lib_handle()

@@ -143,16 +143,34 @@ int gs_mfdreceivers(gs_plan* plan, int32_t nrcv, double exp, const double* elev,
                     const int32_t* gid, int32_t* rcv, double* dist, double* wgt);
 
 /*
- * Depression filling.  Replaces PITFill.fillElevation(sed=False)
+ * Depression filling.  Replaces PITFill.fillElevation(sed)
  * (gospl/flow/pitfilling.py:849-903) and the Fortran kernels it drives
  * (edge_tile, fill_tile, fill_edges, fill_depressions, label_pits, pits_cons,
- * fill_dir, nghb_dir, getpitvol: functions.F90:1845-2499).  Outputs per vertex:
- * lFill, pitIDs (-1 or 1..P), flatDirs (-1, self or a neighbour).  The per-pit
- * tables (pitParams, pitInfo, filled_lvl, filled_vol) stay in the plan; read
- * them with gs_pit_tables.  *npits receives P.
+ * fill_dir, nghb_dir, getpitvol: functions.F90:1845-2499).  sed != 0 is the
+ * sediment fill (pitfilling.py:690-692, 718-721, 828-834, 885-887): marine
+ * depressions filled too, pits labelled above the fill level, pit volumes on
+ * the unclipped surface.  Outputs per vertex: lFill, pitIDs (-1 or 1..P),
+ * flatDirs (-1, self or a neighbour).  The per-pit tables (pitParams,
+ * pitInfo, filled_lvl, filled_vol) stay in the plan; read them with
+ * gs_pit_tables.  *npits receives P.
  */
-int gs_fill_elevation(gs_plan* plan, const double* h, double sealevel, double ofill,
+int gs_fill_elevation(gs_plan* plan, const double* h, double sealevel, double ofill, int32_t sed,
                       double* lfill, int32_t* pit_ids, int32_t* flat_dirs, int32_t* npits);
+
+/*
+ * Flow direction of a surface.  Replaces FAMesh._buildFlowDirection(h, down)
+ * (gospl/flow/flowplex.py:480-544; the matrix of matrixFlow, 429-478, is the
+ * receiver table itself): mfdreceivers on h, then with down != 0 the
+ * pit-flat routing (cells with h == lFill in a depression, a flat receiver
+ * and no MFD receiver send all their flow to flatDirs), flat-model outlets
+ * made self-sinks, lsink = no receiver weight, not an outlet, not sea, and
+ * sea = lFill <= sealevel (seaID).  Reads lfill, pit_ids, flat_dirs of the
+ * last fill.  Outputs receiver-major rcv/dist/wgt [R][nb], lsink and sea
+ * (uint8 masks [nb]).  All pointers DEVICE.
+ */
+int gs_build_flow_direction(gs_plan* plan, const double* h, int32_t down, double sealevel,
+                            const double* lfill, const int32_t* pit_ids, const int32_t* flat_dirs,
+                            int32_t* rcv, double* dist, double* wgt, uint8_t* lsink, uint8_t* sea);
 /* Copy the pit tables of the last fill into caller DEVICE buffers sized
  * (P+1) rows: pit_params [P+1][3], pit_info [P+1][2], filled_lvl [P+1][5],
  * filled_vol [P+1][5] (rows as in pitfilling.py:521-555, 810-891). */
