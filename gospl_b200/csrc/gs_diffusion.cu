@@ -301,12 +301,26 @@ __device__ __forceinline__ double grid_total(const double* part, int stride, int
     return t;
 }
 
-__global__ void __launch_bounds__(256) k_cg_coop(int n, const int* __restrict__ nbr, const int8_t* __restrict__ nnb,
-                                                 const double* __restrict__ coef, const double* __restrict__ farea,
-                                                 const uint8_t* __restrict__ fix, const double* __restrict__ b,
-                                                 double* x, double* r, double* z, double* pp, double* ap,
-                                                 double* part, double rtol, int max_iter, int* it_out,
-                                                 double* res_out) {
+// Jacobi-PCG on the area-weighted symmetric form S = A (I + L) of the
+// hillslope system, in one cooperative launch:
+//   start x = x0; free rows b = A_k (x0_k - sum over fixed columns o x0_j),
+//   r = b - S x (free columns), z = r / (A_k c_k), p = z;
+//   per iteration  Sp and p.Sp  | grid barrier |  x += a p, r -= a Sp,
+//   z = r / diag, r.z and r.r  | grid barrier |,
+// and the direction update p' = z + b p of the next iteration is made inside
+// its product: each thread forms p'_j = z_j + b p_j of the neighbours it
+// gathers (the same operations as a separate update pass, so the same bits)
+// and writes its own p'_k to the other buffer.  Two barriers per iteration;
+// block partial sums are added in block order by every block.  Fixed rows
+// (flat outlets, no area) keep x = x0.  Slots are unrolled to MAXW so the
+// gathers of a row issue together; <= 64 registers for four 256-thread
+// blocks per SM.
+__global__ void __launch_bounds__(256, 4) k_cg_coop(int n, const int* __restrict__ nbr, const int8_t* __restrict__ nnb,
+                                                    const double* __restrict__ coef, const double* __restrict__ farea,
+                                                    const uint8_t* __restrict__ fix, const double* __restrict__ x0,
+                                                    double* x, double* b, double* r, double* z, double* p0, double* p1,
+                                                    double* ap, double* part, double rtol, int max_iter, int* it_out,
+                                                    double* res_out) {
     cg::grid_group grid = cg::this_grid();
     const int nb = gridDim.x, blk = blockIdx.x;
     const int gtid = blk * blockDim.x + threadIdx.x, gsz = nb * blockDim.x;
@@ -315,9 +329,42 @@ __global__ void __launch_bounds__(256) k_cg_coop(int n, const int* __restrict__ 
     double* pb = part + 5 * nb;    // r.z, r.r [2 nb]
     double a0 = 0.0, a1 = 0.0, a2 = 0.0;
     for (int k = gtid; k < n; k += gsz) {
-        a0 += r[k] * z[k];
-        a1 += r[k] * r[k];
-        a2 += b[k] * b[k];
+        const double xk = x0[k];
+        x[k] = xk;
+        if (fix[k]) {
+            b[k] = 0.0;
+            r[k] = 0.0;
+            z[k] = 0.0;
+            p0[k] = 0.0;
+            continue;
+        }
+        const int deg = nnb[k];
+        const double ck = coef[k];
+        double bk = xk;
+        double y = ck * xk;
+#pragma unroll
+        for (int s = 0; s < MAXW; s++) {
+            if (s < deg) {
+                const double o = coef[(size_t)(s + 1) * n + k];
+                const int j = nbr[(size_t)s * n + k];
+                if (o != 0.0 && j >= 0) {
+                    const double xj = x0[j];
+                    if (fix[j]) bk = bk - o * xj;
+                    else y = y + o * xj;
+                }
+            }
+        }
+        const double fa = farea[k];
+        bk = fa * bk;
+        b[k] = bk;
+        const double rk = bk - fa * y;
+        r[k] = rk;
+        const double zk = rk / (fa * ck);
+        z[k] = zk;
+        p0[k] = zk;
+        a0 += rk * zk;
+        a1 += rk * rk;
+        a2 += bk * bk;
     }
     block_sum2(a0, a1, &pc[3 * blk], &pc[3 * blk + 1]);
     block_sum2(a2, 0.0, &pc[3 * blk + 2], &pa[2 * blk + 1]);
@@ -327,23 +374,39 @@ __global__ void __launch_bounds__(256) k_cg_coop(int n, const int* __restrict__ 
     const double bnorm = sqrt(grid_total(pc, 3, 2, nb));
     double relres = bnorm > 0.0 ? sqrt(rr0) / bnorm : 0.0;
     int it = 0;
+    double beta = 0.0;
+    double* pcur = p0;     // direction of the previous iteration
+    double* pnew = p1;
     while (bnorm > 0.0 && relres > rtol && it < max_iter) {
+        // p' = z + beta p (it > 0), its product and p'.Sp'
         double acc = 0.0;
         for (int k = gtid; k < n; k += gsz) {
+            const double pk = it ? z[k] + beta * pcur[k] : pcur[k];
             double y = 0.0;
             if (!fix[k]) {
-                y = coef[k] * pp[k];
-                for (int s = 0; s < nnb[k]; s++) {
-                    double o = coef[(size_t)(s + 1) * n + k];
-                    if (o == 0.0) continue;
-                    int j = nbr[(size_t)s * n + k];
-                    if (fix[j]) continue;
-                    y = y + o * pp[j];
+                const int deg = nnb[k];
+                y = coef[k] * pk;
+#pragma unroll
+                for (int s = 0; s < MAXW; s++) {
+                    if (s < deg) {
+                        const double o = coef[(size_t)(s + 1) * n + k];
+                        const int j = nbr[(size_t)s * n + k];
+                        if (o != 0.0 && j >= 0 && !fix[j]) {
+                            const double pj = it ? z[j] + beta * pcur[j] : pcur[j];
+                            y = y + o * pj;
+                        }
+                    }
                 }
                 y = farea[k] * y;
             }
+            if (it) pnew[k] = pk;
             ap[k] = y;
-            acc += pp[k] * y;
+            acc += pk * y;
+        }
+        if (it) {
+            double* t = pcur;
+            pcur = pnew;
+            pnew = t;
         }
         block_sum2(acc, 0.0, &pa[2 * blk], &pa[2 * blk + 1]);
         grid.sync();
@@ -352,7 +415,7 @@ __global__ void __launch_bounds__(256) k_cg_coop(int n, const int* __restrict__ 
         double c0 = 0.0, c1 = 0.0;
         for (int k = gtid; k < n; k += gsz) {
             if (fix[k]) continue;
-            x[k] = x[k] + alpha * pp[k];
+            x[k] = x[k] + alpha * pcur[k];
             const double rk = r[k] - alpha * ap[k];
             r[k] = rk;
             const double zk = rk / (farea[k] * coef[k]);
@@ -364,13 +427,11 @@ __global__ void __launch_bounds__(256) k_cg_coop(int n, const int* __restrict__ 
         grid.sync();
         const double rzn = grid_total(pb, 2, 0, nb);
         const double rr = grid_total(pb, 2, 1, nb);
-        const double beta = (rz != 0.0) ? rzn / rz : 0.0;
+        beta = (rz != 0.0) ? rzn / rz : 0.0;
         rz = rzn;
         relres = sqrt(rr) / bnorm;
         it++;
         if (!(relres == relres) || relres <= rtol || it >= max_iter) break;
-        for (int k = gtid; k < n; k += gsz) pp[k] = z[k] + beta * pp[k];
-        grid.sync();
     }
     if (gtid == 0) {
         *it_out = it;
@@ -480,6 +541,12 @@ __global__ void k_cg_resid(int n, int W, int flat, const int* __restrict__ nbr, 
                                               : b[k] - diff_row(k, n, W, nbr, nnb, coef, farea, outlet, flat, x, true);
 }
 
+// the second direction buffer of k_cg_coop, allocated on first use
+static int cg_second_direction(gs_plan* p) {
+    if (!p->cg_p2) GS_CUDA(cudaMalloc((void**)&p->cg_p2, sizeof(double) * (size_t)std::max<int64_t>(p->n, 1)));
+    return GS_OK;
+}
+
 static int cg_launch(gs_plan* p, const void* fn, void** args) {
     cudaEvent_t stop = nullptr;
     if (p->profiling) prof_begin(p, fn, &stop);
@@ -574,11 +641,12 @@ int hillslope(gs_plan* p, double* h, double* cum_ed, double* eb, double sealevel
     p->dvalid_cdm = cdm;
     double* hold = p->hl;
     launch(p, k_copy_d2, G, B, n, (const double*)h, hold);
-    launch(p, k_cg_init, G, B, n, p->W, p->flat, (const int*)p->nbr, (const int8_t*)p->nnb,
-           (const double*)p->dcoef, (const double*)p->farea, (const uint8_t*)p->outlet, (const double*)hold,
-           p->cg_x, p->cg_b, p->cg_r, p->cg_z, p->cg_p);
     GS_LAUNCH();
     if (p->fp32) {
+        launch(p, k_cg_init, G, B, n, p->W, p->flat, (const int*)p->nbr, (const int8_t*)p->nnb,
+               (const double*)p->dcoef, (const double*)p->farea, (const uint8_t*)p->outlet, (const double*)hold,
+               p->cg_x, p->cg_b, p->cg_r, p->cg_z, p->cg_p);
+        GS_LAUNCH();
         int outer = 0;
         double relres = 0.0;
         const double tol = std::max(rtol, p->refine_tol);
@@ -601,13 +669,15 @@ int hillslope(gs_plan* p, double* h, double* cum_ed, double* eb, double sealevel
     }
     int* it_d = p->i_scalar + 12;
     double* res_d = p->red + 4100;
+    GS_TRY(cg_second_direction(p));
     {
         int nn = n, mi = max_iter;
         double rt = rtol;
+        const double* x0 = hold;
         void* args[] = {(void*)&nn, (void*)&p->nbr, (void*)&p->nnb, (void*)&p->dcoef, (void*)&p->farea,
-                        (void*)&p->dfix, (void*)&p->cg_b, (void*)&p->cg_x, (void*)&p->cg_r, (void*)&p->cg_z,
-                        (void*)&p->cg_p, (void*)&p->cg_ap, (void*)&p->red, (void*)&rt, (void*)&mi, (void*)&it_d,
-                        (void*)&res_d};
+                        (void*)&p->dfix, (void*)&x0, (void*)&p->cg_x, (void*)&p->cg_b, (void*)&p->cg_r,
+                        (void*)&p->cg_z, (void*)&p->cg_p, (void*)&p->cg_p2, (void*)&p->cg_ap, (void*)&p->red,
+                        (void*)&rt, (void*)&mi, (void*)&it_d, (void*)&res_d};
         cudaEvent_t stop = nullptr;
         if (p->profiling) prof_begin(p, (const void*)k_cg_coop, &stop);
         GS_CUDA(cudaLaunchCooperativeKernel((const void*)k_cg_coop, p->coop_blocks, 256, args, 0, p->stream));
@@ -648,19 +718,19 @@ int diffusion_solve_on(gs_plan* p, int m, const int* nbr, const int8_t* nnb, con
     const int n = m;
     if (n == 0) return GS_OK;
     const int B = 256, G = grid_for(n, B);
-    launch(p, k_cg_init, G, B, n, p->W, flat, nbr, nnb, coef, farea, outlet, rhs, p->cg_x, p->cg_b, p->cg_r, p->cg_z,
-           p->cg_p);
-    GS_LAUNCH();
+    (void)flat;
+    (void)outlet;
     int* it_d = p->i_scalar + 12;
     double* res_d = p->red + 4100;
+    GS_TRY(cg_second_direction(p));
     {
         int nn = n, mi = max_iter;
         double rt = rtol;
         const double* cf = coef;
         void* args[] = {(void*)&nn, (void*)&nbr, (void*)&nnb, (void*)&cf, (void*)&farea,
-                        (void*)&fix, (void*)&p->cg_b, (void*)&p->cg_x, (void*)&p->cg_r, (void*)&p->cg_z,
-                        (void*)&p->cg_p, (void*)&p->cg_ap, (void*)&p->red, (void*)&rt, (void*)&mi, (void*)&it_d,
-                        (void*)&res_d};
+                        (void*)&fix, (void*)&rhs, (void*)&p->cg_x, (void*)&p->cg_b, (void*)&p->cg_r,
+                        (void*)&p->cg_z, (void*)&p->cg_p, (void*)&p->cg_p2, (void*)&p->cg_ap, (void*)&p->red,
+                        (void*)&rt, (void*)&mi, (void*)&it_d, (void*)&res_d};
         cudaEvent_t stop = nullptr;
         if (p->profiling) prof_begin(p, (const void*)k_cg_coop, &stop);
         GS_CUDA(cudaLaunchCooperativeKernel((const void*)k_cg_coop, p->coop_blocks, 256, args, 0, p->stream));

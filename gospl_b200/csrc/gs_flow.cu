@@ -295,7 +295,7 @@ int flow_accumulation(gs_plan* p, const double* h, const double* bl, double seal
         GS_TRY(flow_prepare(p, rcv_i, wgt_i, p->rslot_i, fal, p->order_i, bad_a));
     }
     GS_CUDA(cudaEventRecord(p->ev_a, p->side_a));
-    GS_TRY(fill_elevation(p, h, sealevel, ofill, lfill, pit_ids, flat_dirs, st, true, sea));
+    GS_TRY(fill_elevation(p, h, sealevel, ofill, lfill, pit_ids, flat_dirs, st, true, sea, false, bl));
     const int P = p->npits, np1 = P + 1;
 
     // join: lsink of the snapshot graph, rain on land, the first flow sweep

@@ -49,7 +49,7 @@ __device__ __forceinline__ int agg_append(int* cnt) {
 }
 
 enum { D_MINH = 0, D_LEVEL = 1 };
-enum { I_CHANGED = 0, I_NEXT = 1, I_NPITS0 = 2, I_NPITS = 3 };
+enum { I_CHANGED = 0, I_NEXT = 1, I_NPITS0 = 2, I_NPITS = 3, I_NONFINITE = 13 };
 
 // --------------------------------------------------------------------------
 // reductions
@@ -655,6 +655,131 @@ __global__ void __launch_bounds__(1024) k_bfs_local(int M, int S, const int* __r
     if (tid == 0) *levels_out = levels;
 }
 
+// Flat distances by tiles, in one cooperative launch.  The reachable cells
+// are compacted in vertex order (local ids), and vertex ids follow a
+// space-filling curve, so tile t = local ids [tT, tT + T) is a compact patch
+// of the mesh.  A round: every block takes its tiles that were marked, loads
+// their adjacency rows and distances into shared memory and closes the BFS
+// inside the tile there (label-correcting: a cell whose distance dropped
+// relaxes its out-neighbours again, one block barrier per wave); a hop out of
+// the tile lowers the target's global distance with atomicMin and marks the
+// target's tile for the next round.  A grid barrier ends the round; the loop
+// ends after a round that marked nothing.  Distances only decrease and every
+// cell whose shortest path crosses r tile boundaries is exact after round r,
+// so the result is the breadth-first hop distance, and the round count is
+// bounded by the number of tiles a shortest path crosses (no timed wait).
+constexpr int BFT_THREADS = 512;
+
+__global__ void __launch_bounds__(BFT_THREADS, 2) k_bfs_tiles(int M, int S, int T, const int* __restrict__ rows,
+                                                              const int* __restrict__ seeds,
+                                                              const int* __restrict__ nseed_p, int* ld, int* ctl,
+                                                              int* depth_out) {
+    cg::grid_group grid = cg::this_grid();
+    extern __shared__ int sm_bft[];
+    const int INF = 0x7fffffff;
+    int* rs = sm_bft;              // [T * S] adjacency rows of the tile
+    int* ds = rs + T * S;          // [T] distances
+    int* fl0 = ds + T;             // [T] frontier lists
+    int* fl1 = fl0 + T;
+    __shared__ int s_cnt[3];
+    __shared__ int s_over[3];
+    __shared__ int s_mark;
+    const int ntiles = (M + T - 1) / T;
+    int* cnt = ctl;                // [3] tiles marked for rounds r % 3
+    int* mark = ctl + 3;           // [2][ntiles]
+    const int tid = threadIdx.x, nt = blockDim.x;
+    const unsigned gtid = grid.thread_rank(), gsz = (unsigned)grid.size();
+    for (unsigned i = gtid; i < (unsigned)M; i += gsz) ld[i] = INF;
+    for (unsigned t = gtid; t < 2u * (unsigned)ntiles; t += gsz) mark[t] = 0;
+    if (gtid < 3) cnt[gtid] = 0;
+    grid.sync();
+    const int ns = *nseed_p;
+    for (unsigned q = gtid; q < (unsigned)ns; q += gsz) {
+        const int li = seeds[q];
+        ld[li] = 1;
+        mark[li / T] = 1;
+    }
+    if (gtid == 0) cnt[0] = ns > 0 ? 1 : 0;
+    grid.sync();
+    for (int r = 0;; r++) {
+        if (((volatile int*)cnt)[r % 3] == 0) break;   // written before the last grid barrier: same in every block
+        int* mcur = mark + (r & 1) * ntiles;
+        int* mnext = mark + ((r + 1) & 1) * ntiles;
+        if (blockIdx.x == 0 && tid == 0) cnt[(r + 2) % 3] = 0;
+        if (tid == 0) s_mark = 0;
+        for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+            __syncthreads();
+            if (!((volatile int*)mcur)[t]) continue;
+            const int base = t * T, len = min(T, M - base);
+            {
+                const int4* src = reinterpret_cast<const int4*>(rows + (size_t)base * S);
+                int4* dst = reinterpret_cast<int4*>(rs);
+                const int nq = len * S / 4;
+                for (int q = tid; q < nq; q += nt) dst[q] = src[q];
+            }
+            for (int i = tid; i < len; i += nt) ds[i] = ((volatile int*)ld)[base + i];
+            // wave 0 relaxes every reached cell of the tile (a full wave,
+            // as any wave whose list overflowed)
+            if (tid < 3) {
+                s_cnt[tid] = 0;
+                s_over[tid] = tid == 0 ? 1 : 0;
+            }
+            __syncthreads();
+            for (int w = 0;; w++) {
+                const int rd = w % 3, wr = (w + 1) % 3;
+                int* lin = (w & 1) ? fl1 : fl0;
+                int* lout = (w & 1) ? fl0 : fl1;
+                const int full = s_over[rd];
+                const int size = full ? len : s_cnt[rd];
+                if (size == 0 && !full) break;
+                if (tid == 0) {
+                    s_cnt[(w + 2) % 3] = 0;
+                    s_over[(w + 2) % 3] = 0;
+                }
+                for (int e = tid; e < size; e += nt) {
+                    const int i = full ? e : lin[e];
+                    const int d = ds[i];
+                    if (d == INF) continue;
+                    const int* row = rs + i * S;
+                    const int k = row[0];
+                    const int nd = d + 1;
+                    for (int q = 1; q <= k; q++) {
+                        const int c = row[q];
+                        const int lc = c - base;
+                        if ((unsigned)lc < (unsigned)len) {
+                            if (atomicMin(&ds[lc], nd) > nd) {
+                                const int pos = atomicAdd(&s_cnt[wr], 1);
+                                if (pos < T) lout[pos] = lc;
+                                else s_over[wr] = 1;
+                            }
+                        } else if (atomicMin(&ld[c], nd) > nd) {
+                            mnext[c / T] = 1;
+                            s_mark = 1;
+                        }
+                    }
+                }
+                __syncthreads();
+            }
+            for (int i = tid; i < len; i += nt) {
+                const int d = ds[i];
+                if (d < ((volatile int*)ld)[base + i]) atomicMin(&ld[base + i], d);
+            }
+            if (tid == 0) mcur[t] = 0;
+        }
+        __syncthreads();
+        if (tid == 0 && s_mark) atomicAdd(&cnt[(r + 1) % 3], 1);
+        grid.sync();
+    }
+    int dmax = 0;
+    for (unsigned i = gtid; i < (unsigned)M; i += gsz) {
+        const int d = ld[i];
+        if (d == INF) ld[i] = -1;
+        else dmax = d > dmax ? d : dmax;
+    }
+    dmax = __reduce_max_sync(0xffffffffu, dmax);
+    if ((tid & 31) == 0 && dmax > 0) atomicMax(depth_out, dmax);
+}
+
 // Whole BFS in one cooperative launch: wide levels use the whole grid with a
 // grid-wide barrier per level; once a level is narrower than one block's
 // worth, block 0 finishes the remaining levels alone with block barriers
@@ -956,6 +1081,45 @@ static int launch_coop(gs_plan* p, const void* fn, void** args) {
     return GS_OK;
 }
 
+// Tiled flat-distance BFS (k_bfs_tiles) over the M compacted cells whose
+// rows, seeds (front0, count in i_scalar[6]) and local ids k_bfs_local_build
+// wrote; distances into ld (-1 unreached), depth into i_scalar[4].  Tiles of
+// T cells with T * (S + 3) ints of shared memory (<= 96 KB), as many blocks as
+// stay co-resident.
+static int bfs_tiles(gs_plan* p, int M, int S, const int* rows, int* ld) {
+    int T = 4096;
+    while (T > 256 && (size_t)T * (S + 3) * sizeof(int) > 96 * 1024) T >>= 1;
+    const size_t smem = (size_t)T * (S + 3) * sizeof(int);
+    GS_CUDA(cudaFuncSetAttribute(k_bfs_tiles, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int occ = 0;
+    GS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_bfs_tiles, BFT_THREADS, smem));
+    if (occ < 1) {
+        set_error(GS_ECUDA, "flat BFS: tile kernel cannot be resident");
+        return GS_ECUDA;
+    }
+    const int ntiles = (M + T - 1) / T;
+    const int grid = std::max(1, std::min(ntiles, p->sm_count * occ));
+    if (3 + 2 * ntiles > (int)p->n + 1) {
+        set_error(GS_EINVAL, "flat BFS: tile marks exceed their buffer");
+        return GS_EINVAL;
+    }
+    GS_CUDA(cudaMemsetAsync(p->i_scalar + 4, 0, sizeof(int), p->stream));
+    int m = M, s = S, t = T;
+    const int* seeds = p->front0;
+    const int* nseed = p->i_scalar + 6;
+    int* ctl = p->front1;
+    int* depth = p->i_scalar + 4;
+    void* args[] = {(void*)&m, (void*)&s, (void*)&t, (void*)&rows, (void*)&seeds, (void*)&nseed, (void*)&ld,
+                    (void*)&ctl, (void*)&depth};
+    cudaEvent_t stop = nullptr;
+    if (p->profiling) prof_begin(p, (const void*)k_bfs_tiles, &stop);
+    GS_CUDA(cudaLaunchCooperativeKernel((const void*)k_bfs_tiles, grid, BFT_THREADS, args, smem, p->stream));
+    if (stop) cudaEventRecord(stop, p->stream);
+    p->launches++;
+    GS_LAUNCH();
+    return GS_OK;
+}
+
 static int read_ints(gs_plan* p, int* dst, const int* src, int count) {
     GS_CUDA(cudaMemcpyAsync(dst, src, sizeof(int) * count, cudaMemcpyDeviceToHost, p->stream));
     GS_CUDA(cudaStreamSynchronize(p->stream));
@@ -988,13 +1152,29 @@ int fill_join(gs_plan* p, gs_stats* st) {
     return GS_OK;
 }
 
+// 1 in *flag when a or b (may be null) holds a NaN or an infinity
+__global__ void k_nonfinite(int n, const double* __restrict__ a, const double* __restrict__ b, int* flag) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    if (!isfinite(a[i]) || (b && !isfinite(b[i]))) *flag = 1;
+}
+
 int fill_elevation(gs_plan* p, const double* h, double sealevel, double ofill, double* lfill,
-                   int* pit_ids, int* flat_dirs, gs_stats* st, bool defer_flats, uint8_t* sea_out, bool sed) {
+                   int* pit_ids, int* flat_dirs, gs_stats* st, bool defer_flats, uint8_t* sea_out, bool sed,
+                   const double* check_b) {
     const int n = (int)p->n;
     GS_TRY(fill_join(p, nullptr));
     if (n == 0) { p->npits = 0; return GS_OK; }
     const int B = 256, G = grid_for(n, B);
     int hbuf[4];
+    // the inputs must be finite: checked on the device now, read at the
+    // first synchronisation below (the root search), before the relaxation,
+    // the flat pass and any sweep
+    GS_CUDA(cudaMemsetAsync(p->i_scalar + I_NONFINITE, 0, sizeof(int), p->stream));
+    launch(p, k_nonfinite, G, B, n, h, check_b, p->i_scalar + I_NONFINITE);
+    GS_LAUNCH();
+    GS_CUDA(cudaMemcpyAsync(p->h_pinned + 9, p->i_scalar + I_NONFINITE, sizeof(int), cudaMemcpyDeviceToHost,
+                            p->stream));
 
     // level
     GS_CUDA(cudaMemsetAsync(p->u_scalar, 0xff, sizeof(unsigned long long), p->stream));
@@ -1025,6 +1205,11 @@ int fill_elevation(gs_plan* p, const double* h, double sealevel, double ofill, d
         for (int r = 0; r < 2; r++) launch(p, k_jump, G, B, n, p->parent, p->i_scalar + I_CHANGED);
         GS_LAUNCH();
         GS_TRY(read_ints(p, hbuf, p->i_scalar + I_CHANGED, 1));
+        if (round == 0 && p->h_pinned[9]) {
+            set_error(GS_ENONFINITE, check_b ? "non-finite elevation or rain volume (NaN or Inf)"
+                                             : "non-finite elevation (NaN or Inf)");
+            return GS_ENONFINITE;
+        }
         if (!hbuf[0]) break;
         if (round == 63) { set_error(GS_EMAXITER, "pit fill: root search did not converge"); return GS_EMAXITER; }
     }
@@ -1131,8 +1316,7 @@ int fill_elevation(gs_plan* p, const double* h, double sealevel, double ofill, d
         GS_CUDA(cudaMemcpyAsync(&last[1], p->flagbuf + n - 1, sizeof(int), cudaMemcpyDeviceToHost, p->stream));
         GS_CUDA(cudaStreamSynchronize(p->stream));
         const int M = last[0] + last[1];
-        const size_t smem = sizeof(unsigned) * (size_t)((M + 31) / 32) + sizeof(int) * 2 * LBFS_CAP;
-        if (smem <= 200 * 1024) {
+        if (true) {
             GS_CUDA(cudaEventRecord(p->ev_fork_b, p->stream));
             GS_CUDA(cudaStreamWaitEvent(p->side_b, p->ev_fork_b, 0));
             {
@@ -1146,15 +1330,7 @@ int fill_elevation(gs_plan* p, const double* h, double sealevel, double ofill, d
                        (const int*)p->flagbuf, (const int*)p->scanbuf, (const int*)p->nbr, (const int8_t*)p->nnb,
                        (const int*)p->spill_flag, rows, p->comp, ldv, p->front0, p->i_scalar + 6);
                 GS_LAUNCH();
-                GS_CUDA(cudaFuncSetAttribute(k_bfs_local, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-                cudaEvent_t stop = nullptr;
-                if (p->profiling) prof_begin(p, (const void*)k_bfs_local, &stop);
-                k_bfs_local<<<1, 1024, smem, p->stream>>>(M, S, (const int*)rows, (const int*)p->front0,
-                                                           p->i_scalar + 6, p->front1, p->minseed, ldv,
-                                                           p->i_scalar + 4);
-                if (stop) cudaEventRecord(stop, p->stream);
-                p->launches++;
-                GS_LAUNCH();
+                GS_TRY(bfs_tiles(p, M, S, rows, ldv));
                 launch(p, k_bfs_local_scatter, grid_for(M, B), B, M, (const int*)p->comp, (const int*)ldv,
                        p->pdir);
                 launch(p, k_flat_dirs, G, B, n, (const double*)lfill, (const int*)pit_ids, (const int*)p->pdir,

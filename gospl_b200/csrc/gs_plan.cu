@@ -42,7 +42,7 @@ static void plan_free(gs_plan* p) {
                     p->u_scalar, p->pit_params, p->pit_info, p->filled_lvl, p->filled_vol, p->pit_vol,
                     p->pit_in, p->pit_ev, p->pit_win, p->pit_lvl, p->pit_state, p->seg_keys, p->seg_vals,
                     p->seg_keys2, p->seg_vals2, p->seg_start, p->seg_count, p->cub_tmp, p->nfa, p->wf,
-                    p->hl, p->dcoef, p->dsea, p->dsea2, p->dfix, p->cg_r, p->cg_z, p->cg_p, p->cg_ap, p->cg_x, p->cg_b,
+                    p->hl, p->dcoef, p->dsea, p->dsea2, p->dfix, p->cg_r, p->cg_z, p->cg_p, p->cg_p2, p->cg_ap, p->cg_x, p->cg_b,
                     p->red, p->cub_tmp2, p->pflag, p->pscan, p->f32a, p->f32b, p->f32c, p->f32d, p->f32e, p->r64, p->ed_buf,
                     p->sed_buf, p->sed_mask, p->ed_basis, p->sed_pit, p->led, p->led_part, p->sed_coef, p->lake_i, p->lake_d, p->lake_u8};
     for (void* q : ptrs)
@@ -412,6 +412,14 @@ int plan_tune(gs_plan* p, int knob, int value) {
         p->sweep_nap = (unsigned)value;
         return GS_OK;
     }
+    if (knob == GS_TUNE_SWEEP_BUDGET) {
+        if (value < 1 || value > 60000000) {
+            set_error(GS_EINVAL, "tune: sweep time budget must be in 1..60000000 us");
+            return GS_EINVAL;
+        }
+        p->sweep_budget_ns = (unsigned long long)value * 1000ULL;
+        return GS_OK;
+    }
     set_error(GS_EINVAL, "tune: unknown knob");
     return GS_EINVAL;
 }
@@ -421,6 +429,7 @@ int plan_tuning(const gs_plan* p, int knob) {
     if (knob == GS_TUNE_COOP_BLOCKS) return p->coop_blocks / std::max(p->sm_count, 1);
     if (knob == GS_TUNE_COOP_BLOCKS + 1) return p->coop_max_per_sm;
     if (knob == GS_TUNE_SWEEP_NAP) return (int)p->sweep_nap;
+    if (knob == GS_TUNE_SWEEP_BUDGET) return (int)(p->sweep_budget_ns / 1000ULL);
     if (knob == GS_TUNE_REFINE_PASSES) return (int)std::min<int64_t>(p->refine_iters, 0x7fffffff);
     return -1;
 }

@@ -19,6 +19,7 @@ struct gs_plan {
     int coop_max_per_sm = 1;             // occupancy limit of the cooperative kernels
     int sweep_per_sm = 8;                // 128-thread blocks per SM of the ordered sweeps
     unsigned sweep_nap = 128;            // longest back-off (ns) between polls of the ordered sweeps
+    unsigned long long sweep_budget_ns = 4000000000ULL;   // wall-clock budget of one dependency sweep
     // precision form: FP32 sweeps and CG inside FP64 refinement loops
     int fp32 = 0;
     double fdepa = 0.0;                  // SPL deposition coefficient G (0: detachment-limited)
@@ -203,6 +204,7 @@ struct gs_plan {
     double* cg_r = nullptr;
     double* cg_z = nullptr;
     double* cg_p = nullptr;
+    double* cg_p2 = nullptr;             // second direction buffer of the cooperative CG
     double* cg_ap = nullptr;
     double* cg_x = nullptr;
     double* cg_b = nullptr;
@@ -262,9 +264,12 @@ int sweep_spl_adjoint(gs_plan* p, const int* rcv, const double* wgt, const int8_
                       const int* order, const double* g, double* y);
 int spl_sweep(gs_plan* p, const int* rcv, const double* c, const int8_t* rslot, const double* hold,
               double* s, int* cycle_nodes, bool reuse_order);
+// check_b: a second input checked for NaN/Inf with h (the rain volume of a
+// flow accumulation); a non-finite value returns GS_ENONFINITE before the
+// relaxation and any sweep
 int fill_elevation(gs_plan* p, const double* h, double sealevel, double ofill, double* lfill,
                    int* pit_ids, int* flat_dirs, gs_stats* st, bool defer_flats = false,
-                   uint8_t* sea_out = nullptr, bool sed = false);
+                   uint8_t* sea_out = nullptr, bool sed = false, const double* check_b = nullptr);
 // joins the flat-distance BFS of the last fill (if it ran on side_b) into the
 // main stream and records its level count
 int fill_join(gs_plan* p, gs_stats* st);
@@ -316,9 +321,9 @@ __global__ void k_cg_coop32(int n, const int* __restrict__ nbr, const int8_t* __
                             double* res_out);
 __global__ void k_cg_coop(int n, const int* __restrict__ nbr, const int8_t* __restrict__ nnb,
                           const double* __restrict__ coef, const double* __restrict__ farea,
-                          const uint8_t* __restrict__ fix, const double* __restrict__ b, double* x, double* r,
-                          double* z, double* pp, double* ap, double* part, double rtol, int max_iter, int* it_out,
-                          double* res_out);
+                          const uint8_t* __restrict__ fix, const double* __restrict__ x0, double* x, double* b,
+                          double* r, double* z, double* p0, double* p1, double* ap, double* part, double rtol,
+                          int max_iter, int* it_out, double* res_out);
 int set_members(gs_plan* p, int nmem, const int64_t* start, const double* maxarea);
 int plan_tune(gs_plan* p, int knob, int value);
 int precision_buffers(gs_plan* p);

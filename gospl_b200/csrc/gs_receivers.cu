@@ -62,13 +62,15 @@ __device__ void dev_quicksort(double* a, int first, int last, int* ix) {
     }
 }
 
-__global__ void k_mfd_receivers(int n, int W, int R, double expo, const double* __restrict__ elev,
-                                double sl, const int* __restrict__ gid, const int* __restrict__ nbr,
-                                const double* __restrict__ elen, const int8_t* __restrict__ nnb,
-                                int* __restrict__ rcv, double* __restrict__ dist,
-                                double* __restrict__ wgt, int8_t* __restrict__ rslot) {
-    int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= n) return;
+// One vertex of mfdreceivers with its candidates in arrays: any R, and the
+// literal quicksort replay when candidate slopes tie exactly.  Not inlined:
+// it is the only code here that needs a stack frame, and the register form
+// below calls it for tied vertices only.
+__device__ __noinline__ void mfd_vertex_general(int k, int n, int R, double expo, const double* __restrict__ elev,
+                                                double sl, const int* __restrict__ gid, const int* __restrict__ nbr,
+                                                const double* __restrict__ elen, const int8_t* __restrict__ nnb,
+                                                int* __restrict__ rcv, double* __restrict__ dist,
+                                                double* __restrict__ wgt, int8_t* __restrict__ rslot) {
     const double hk = elev[k];
     for (int o = 0; o < R; o++) {
         rcv[(size_t)o * n + k] = k;
@@ -166,6 +168,184 @@ __global__ void k_mfd_receivers(int n, int W, int R, double expo, const double* 
     for (int o = 0; o < R; o++) wgt[(size_t)o * n + k] = slope[o] / val;
 }
 
+__global__ void k_mfd_receivers(int n, int W, int R, double expo, const double* __restrict__ elev,
+                                double sl, const int* __restrict__ gid, const int* __restrict__ nbr,
+                                const double* __restrict__ elen, const int8_t* __restrict__ nnb,
+                                int* __restrict__ rcv, double* __restrict__ dist,
+                                double* __restrict__ wgt, int8_t* __restrict__ rslot) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < n) mfd_vertex_general(k, n, R, expo, elev, sl, gid, nbr, elen, nnb, rcv, dist, wgt, rslot);
+}
+
+// Register form for R = RM <= 4 (the configurations' flowDir is 3): the
+// neighbour ids, edge lengths and candidate slopes of the <= 12 slots stay in
+// registers (every loop over slots is unrolled), the RM + 1 steepest
+// candidates are kept by insertion, and every output slot is written once.
+// Without exact ties among those RM + 1 the descending order is the one the
+// reference quicksort leaves, so the result is bit-identical to the general
+// form; a vertex with such a tie goes to mfd_vertex_general (literal replay).
+template <int RM>
+__global__ void __launch_bounds__(128) k_mfd_receivers_r(int n, double expo, const double* __restrict__ elev,
+                                                          double sl, const int* __restrict__ gid,
+                                                          const int* __restrict__ nbr, const double* __restrict__ elen,
+                                                          const int8_t* __restrict__ nnb, int* __restrict__ rcv,
+                                                          double* __restrict__ dist, double* __restrict__ wgt,
+                                                          int8_t* __restrict__ rslot) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const double hk = elev[k];
+    if (!(hk > sl)) {
+#pragma unroll
+        for (int o = 0; o < RM; o++) {
+            rcv[(size_t)o * n + k] = k;
+            dist[(size_t)o * n + k] = 0.0;
+            wgt[(size_t)o * n + k] = 0.0;
+            if (rslot) rslot[(size_t)o * n + k] = -1;
+        }
+        return;
+    }
+    const int deg = nnb[k];
+    int nb[MAXW];
+    double L[MAXW], v[MAXW];
+    double e = 0.0;
+#pragma unroll
+    for (int s = 0; s < MAXW; s++) {
+        nb[s] = -1;
+        L[s] = 0.0;
+        v[s] = 0.0;
+        if (s < deg) {
+            const int c = nbr[(size_t)s * n + k];
+            const double l = elen[(size_t)s * n + k];
+            if (c >= 0 && l > 0.0) {
+                nb[s] = c;
+                L[s] = l;
+                const double d = hk - elev[c];
+                v[s] = d;
+                const double g = d / l;
+                e = (g > e) ? g : e;
+            }
+        }
+    }
+    double fexp;
+    if (e > 0) {
+        const double me = (e < 1.0) ? e : 1.0;
+        fexp = 5.0 * me + expo;
+    } else {
+        fexp = 1.0;
+    }
+    const bool fexp_int = (fexp == floor(fexp));
+    // candidate slopes (0 = not a candidate), in slot order
+    int kk = 0;
+#pragma unroll
+    for (int s = 0; s < MAXW; s++) {
+        if (nb[s] >= 0) {
+            const double d = v[s];
+            double val;
+            if (d > 0.0) val = pow(d, fexp) / L[s];
+            else if (d == 0.0) val = 0.0;
+            else val = fexp_int ? pow(d, fexp) / L[s] : -1.0;
+            if (val > 0.0) {
+                v[s] = val * (1.0 - 1.0e-15 * (double)gid[nb[s]]);
+                kk++;
+            } else {
+                v[s] = 0.0;
+            }
+        } else {
+            v[s] = 0.0;
+        }
+    }
+    if (kk <= RM) {
+        // receivers in slot order, weights over the candidates' sum
+        double tot = 0.0;
+#pragma unroll
+        for (int s = 0; s < MAXW; s++)
+            if (v[s] > 0.0) tot = tot + v[s];
+        int o = 0;
+#pragma unroll
+        for (int s = 0; s < MAXW; s++) {
+            if (v[s] > 0.0) {
+                rcv[(size_t)o * n + k] = nb[s];
+                dist[(size_t)o * n + k] = L[s];
+                wgt[(size_t)o * n + k] = v[s] / tot;
+                if (rslot) rslot[(size_t)o * n + k] = (int8_t)s;
+                o++;
+            }
+        }
+        for (; o < RM; o++) {
+            rcv[(size_t)o * n + k] = k;
+            dist[(size_t)o * n + k] = 0.0;
+            wgt[(size_t)o * n + k] = 0.0;
+            if (rslot) rslot[(size_t)o * n + k] = -1;
+        }
+        return;
+    }
+    // the RM + 1 steepest candidates, descending (strict >: the earlier slot
+    // stays ahead of an equal one, and equal values are sent to the replay)
+    double tv[RM + 1];
+    int ts[RM + 1], tid[RM + 1];
+#pragma unroll
+    for (int j = 0; j <= RM; j++) {
+        tv[j] = -1.0;
+        ts[j] = -1;
+        tid[j] = -1;
+    }
+#pragma unroll
+    for (int s = 0; s < MAXW; s++) {
+        if (v[s] > 0.0) {
+            double x = v[s];
+            int xs = s, xi = nb[s];
+#pragma unroll
+            for (int j = 0; j <= RM; j++) {
+                if (x > tv[j]) {
+                    const double t = tv[j];
+                    const int a = ts[j], b = tid[j];
+                    tv[j] = x;
+                    ts[j] = xs;
+                    tid[j] = xi;
+                    x = t;
+                    xs = a;
+                    xi = b;
+                }
+            }
+        }
+    }
+    bool tie = false;
+#pragma unroll
+    for (int s = 0; s < MAXW; s++) {
+#pragma unroll
+        for (int j = 0; j <= RM; j++) tie |= (v[s] > 0.0) && (v[s] == tv[j]) && (s != ts[j]);
+    }
+    if (tie) {
+        mfd_vertex_general(k, n, RM, expo, elev, sl, gid, nbr, elen, nnb, rcv, dist, wgt, rslot);
+        return;
+    }
+    // reference quirk: receiver o takes the edge length of candidate kk-1-o
+    // in slot order (the sort permutes slopes and ids, not distances)
+    double dsel[RM];
+#pragma unroll
+    for (int o = 0; o < RM; o++) dsel[o] = 0.0;
+    int c = 0;
+#pragma unroll
+    for (int s = 0; s < MAXW; s++) {
+        if (v[s] > 0.0) {
+#pragma unroll
+            for (int o = 0; o < RM; o++)
+                if (c == kk - 1 - o) dsel[o] = L[s];
+            c++;
+        }
+    }
+    double tot = 0.0;
+#pragma unroll
+    for (int o = 0; o < RM; o++) tot = tot + tv[o];
+#pragma unroll
+    for (int o = 0; o < RM; o++) {
+        rcv[(size_t)o * n + k] = tid[o];
+        dist[(size_t)o * n + k] = dsel[o];
+        wgt[(size_t)o * n + k] = tv[o] / tot;
+        if (rslot) rslot[(size_t)o * n + k] = (int8_t)ts[o];
+    }
+}
+
 __global__ void k_flow_direction_post(int n, int W, int R, int flat, const double* __restrict__ h,
                                       int down, const double* __restrict__ lfill,
                                       const int* __restrict__ pit, const int* __restrict__ fdir,
@@ -244,8 +424,17 @@ int receivers(gs_plan* p, int nrcv, double exp, const double* elev, double sl, c
         return GS_EINVAL;
     }
     if (p->n == 0) return GS_OK;
-    launch(p, k_mfd_receivers, grid_for(p->n, 128), 128, (int)p->n, p->W, nrcv, exp, elev, sl,
-           gid ? gid : p->gid, p->nbr, p->elen, p->nnb, rcv, dist, wgt, rslot);
+    const int* g = gid ? gid : p->gid;
+    const int G = grid_for(p->n, 128), n = (int)p->n;
+    switch (nrcv) {
+        case 1: launch(p, k_mfd_receivers_r<1>, G, 128, n, exp, elev, sl, g, p->nbr, p->elen, p->nnb, rcv, dist, wgt, rslot); break;
+        case 2: launch(p, k_mfd_receivers_r<2>, G, 128, n, exp, elev, sl, g, p->nbr, p->elen, p->nnb, rcv, dist, wgt, rslot); break;
+        case 3: launch(p, k_mfd_receivers_r<3>, G, 128, n, exp, elev, sl, g, p->nbr, p->elen, p->nnb, rcv, dist, wgt, rslot); break;
+        case 4: launch(p, k_mfd_receivers_r<4>, G, 128, n, exp, elev, sl, g, p->nbr, p->elen, p->nnb, rcv, dist, wgt, rslot); break;
+        default:
+            launch(p, k_mfd_receivers, G, 128, n, p->W, nrcv, exp, elev, sl, g, p->nbr, p->elen, p->nnb, rcv, dist,
+                   wgt, rslot);
+    }
     GS_LAUNCH();
     return GS_OK;
 }

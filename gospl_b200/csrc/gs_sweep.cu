@@ -330,7 +330,6 @@ static int sweep_status(gs_plan* p, int* status_out) {
     return GS_OK;
 }
 
-static const unsigned long long SWEEP_BUDGET_NS = 4000000000ULL;   // 4 s
 
 int flow_solve_counted(gs_plan* p, const int* rcv, const double* wgt, const int8_t* rslot,
                        const double* b, double* x, int* cycle_nodes) {
@@ -350,7 +349,7 @@ int flow_solve_counted(gs_plan* p, const int* rcv, const double* wgt, const int8
     GS_LAUNCH();
     FlowOp op{n, p->R, p->nbr, p->don_mask, p->don_k, p->sorder, wgt, rcv, b, x, p->done_flag};
     launch(p, k_sources<FlowOp>, grid_for(n, 256), 256, op, sc, n, (const uint8_t*)p->done_flag);
-    launch(p, k_dataflow<FlowOp>, p->sm_count * 4, 128, op, sc, n, SWEEP_BUDGET_NS);
+    launch(p, k_dataflow<FlowOp>, p->sm_count * 4, 128, op, sc, n, p->sweep_budget_ns);
     GS_LAUNCH();
     int st = 0;
     GS_TRY(sweep_status(p, &st));
@@ -412,7 +411,7 @@ int spl_sweep_counted(gs_plan* p, const int* rcv, const double* c, const int8_t*
     GS_LAUNCH();
     SplOp op{n, p->R, p->nbr, p->don_mask, rcv, c, hold, s, p->done_flag};
     launch(p, k_sources<SplOp>, grid_for(n, 256), 256, op, sc, n, (const uint8_t*)p->done_flag);
-    launch(p, k_dataflow<SplOp>, p->sm_count * 4, 128, op, sc, n, SWEEP_BUDGET_NS);
+    launch(p, k_dataflow<SplOp>, p->sm_count * 4, 128, op, sc, n, p->sweep_budget_ns);
     GS_LAUNCH();
     int st = 0;
     GS_TRY(sweep_status(p, &st));
@@ -1036,7 +1035,7 @@ int flow_run(gs_plan* p, const int* rcv, const double* wgt, const int8_t* rslot,
     if (p->fp32) return flow_refine32(p, wgt, b, x, order);
     GS_CUDA(cudaMemsetAsync(p->ctr, 0, sizeof(unsigned) * 8, p->stream));
     FlowOrd op{n, p->nbr, p->don_mask, p->don_k, p->sorder, wgt, b, x};
-    launch(p, k_ordered<FlowOrd>, p->sm_count * p->sweep_per_sm, 128, op, n, (const int*)order, p->ctr, SWEEP_BUDGET_NS, p->sweep_nap);
+    launch(p, k_ordered<FlowOrd>, p->sm_count * p->sweep_per_sm, 128, op, n, (const int*)order, p->ctr, p->sweep_budget_ns, p->sweep_nap);
     GS_LAUNCH();
     int st = 0;
     GS_TRY(ordered_status(p, &st));
@@ -1098,7 +1097,7 @@ int spl_sweep(gs_plan* p, const int* rcv, const double* c, const int8_t* rslot, 
     GS_CUDA(cudaMemsetAsync(p->ctr, 0, sizeof(unsigned) * 8, p->stream));
     launch(p, k_fill_sent, grid_for(n, 256), 256, n, s);
     SplOrd op{n, p->R, rcv, c, hold, s};
-    launch(p, k_ordered<SplOrd>, p->sm_count * p->sweep_per_sm, 128, op, n, (const int*)p->order2, p->ctr, SWEEP_BUDGET_NS, p->sweep_nap);
+    launch(p, k_ordered<SplOrd>, p->sm_count * p->sweep_per_sm, 128, op, n, (const int*)p->order2, p->ctr, p->sweep_budget_ns, p->sweep_nap);
     GS_LAUNCH();
     int st = 0;
     GS_TRY(ordered_status(p, &st));
@@ -1117,7 +1116,7 @@ int sweep_flow_adjoint(gs_plan* p, const int* rcv, const double* wgt, const int*
     GS_CUDA(cudaMemsetAsync(p->ctr, 0, sizeof(unsigned) * 8, p->stream));
     launch(p, k_fill_sent, grid_for(n, 256), 256, n, y);
     FlowAdjOrd op{n, p->R, rcv, wgt, g, y};
-    launch(p, k_ordered<FlowAdjOrd>, p->sm_count * p->sweep_per_sm, 128, op, n, (const int*)p->order2, p->ctr, SWEEP_BUDGET_NS, p->sweep_nap);
+    launch(p, k_ordered<FlowAdjOrd>, p->sm_count * p->sweep_per_sm, 128, op, n, (const int*)p->order2, p->ctr, p->sweep_budget_ns, p->sweep_nap);
     GS_LAUNCH();
     int st = 0;
     GS_TRY(ordered_status(p, &st));
@@ -1141,7 +1140,7 @@ int sweep_spl_adjoint(gs_plan* p, const int* rcv, const double* wgt, const int8_
     GS_CUDA(cudaMemsetAsync(p->ctr, 0, sizeof(unsigned) * 8, p->stream));
     launch(p, k_fill_sent, grid_for(n, 256), 256, n, y);
     SplAdjOrd op{n, p->R, p->nbr, p->don_mask, p->don_k, p->sorder, c, g, y};
-    launch(p, k_ordered<SplAdjOrd>, p->sm_count * p->sweep_per_sm, 128, op, n, order, p->ctr, SWEEP_BUDGET_NS, p->sweep_nap);
+    launch(p, k_ordered<SplAdjOrd>, p->sm_count * p->sweep_per_sm, 128, op, n, order, p->ctr, p->sweep_budget_ns, p->sweep_nap);
     GS_LAUNCH();
     int st = 0;
     GS_TRY(ordered_status(p, &st));
@@ -1261,7 +1260,7 @@ int flow_refine32(gs_plan* p, const double* wgt, const double* b, double* x, con
         GS_CUDA(cudaMemsetAsync(p->ctr, 0, sizeof(unsigned) * 8, p->stream));
         launch(p, k_fill_sent32, G, B, n, p->f32a);
         FlowOrd32 op{n, p->nbr, p->don_mask, p->don_k, p->sorder, wgt, (const double*)p->r64, p->f32a};
-        launch(p, k_ordered<FlowOrd32>, p->sm_count * p->sweep_per_sm, 128, op, n, order, p->ctr, SWEEP_BUDGET_NS, p->sweep_nap);
+        launch(p, k_ordered<FlowOrd32>, p->sm_count * p->sweep_per_sm, 128, op, n, order, p->ctr, p->sweep_budget_ns, p->sweep_nap);
         GS_LAUNCH();
         int st = 0;
         GS_TRY(ordered_status(p, &st));
@@ -1298,7 +1297,7 @@ int spl_refine32(gs_plan* p, const int* rcv, const double* c, const double* hold
         GS_CUDA(cudaMemsetAsync(p->ctr, 0, sizeof(unsigned) * 8, p->stream));
         launch(p, k_fill_sent32, G, B, n, p->f32a);
         SplOrd32 op{n, p->R, rcv, c, (const double*)p->r64, p->f32a};
-        launch(p, k_ordered<SplOrd32>, p->sm_count * p->sweep_per_sm, 128, op, n, order2, p->ctr, SWEEP_BUDGET_NS, p->sweep_nap);
+        launch(p, k_ordered<SplOrd32>, p->sm_count * p->sweep_per_sm, 128, op, n, order2, p->ctr, p->sweep_budget_ns, p->sweep_nap);
         GS_LAUNCH();
         int st = 0;
         GS_TRY(ordered_status(p, &st));
@@ -1340,7 +1339,7 @@ int sweep_flow_rhs(gs_plan* p, const double* wgt, const int* order, const double
     GS_CUDA(cudaMemsetAsync(p->ctr, 0, sizeof(unsigned) * 8, p->stream));
     launch(p, k_fill_sent, grid_for(n, 256), 256, n, x);
     FlowOrd op{n, p->nbr, p->don_mask, p->don_k, p->sorder, wgt, b, x};
-    launch(p, k_ordered<FlowOrd>, p->sm_count * p->sweep_per_sm, 128, op, n, order, p->ctr, SWEEP_BUDGET_NS, p->sweep_nap);
+    launch(p, k_ordered<FlowOrd>, p->sm_count * p->sweep_per_sm, 128, op, n, order, p->ctr, p->sweep_budget_ns, p->sweep_nap);
     GS_LAUNCH();
     int st = 0;
     GS_TRY(ordered_status(p, &st));
@@ -1356,7 +1355,7 @@ int sweep_spl_rhs(gs_plan* p, const int* rcv, const double* c, const int* order2
     GS_CUDA(cudaMemsetAsync(p->ctr, 0, sizeof(unsigned) * 8, p->stream));
     launch(p, k_fill_sent, grid_for(n, 256), 256, n, x);
     SplOrd op{n, p->R, rcv, c, rhs, x};
-    launch(p, k_ordered<SplOrd>, p->sm_count * p->sweep_per_sm, 128, op, n, order2, p->ctr, SWEEP_BUDGET_NS, p->sweep_nap);
+    launch(p, k_ordered<SplOrd>, p->sm_count * p->sweep_per_sm, 128, op, n, order2, p->ctr, p->sweep_budget_ns, p->sweep_nap);
     GS_LAUNCH();
     int st = 0;
     GS_TRY(ordered_status(p, &st));
