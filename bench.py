@@ -131,7 +131,18 @@ def run_reference(args, rank, world):
     n = res[0][1]
     sample = ("oracle on icosphere level %d (%d vertices), %d concurrent processes x %d timed step(s) "
               "after %d untimed" % (level, n, cores, steps, warm))
+    full = None
+    if not args.no_ref_full and level != args.level:
+        # one measured step of the benchmark's own mesh, one process
+        v9, n9, st9, dt9 = cpu_sample(args.level, 1, 0)
+        full = {"vertices": n9, "processes": 1, "steps": st9, "ms_per_step": 1000.0 * dt9 / st9,
+                "value": v9, "unit": "vertex-steps/s",
+                "what": "one physics step of the oracle on the benchmark's sphere, measured (set-up and the "
+                        "init-time flow accumulation excluded)"}
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "vertex-steps/s", "n_gpus": world,
+            "same_config": level == args.level, "sampled_level": level,
+            "ms_per_step_derived": level != args.level,
+            "full_size_step": full,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * sphere_vertices(args.level) / value,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded sphere, SH relief)",
@@ -173,6 +184,8 @@ def main():
     ap.add_argument("--loop", action="store_true", help="ensemble: also time the per-member loop")
     ap.add_argument("--adjoint-steps", type=int, default=4, help="sphere: steps of the adjoint timing (0: skip)")
     ap.add_argument("--no-tune", action="store_true", help="keep the default launch shapes")
+    ap.add_argument("--no-ref-full", action="store_true",
+                    help="reference arm: skip the measured full-size oracle step")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -380,6 +393,9 @@ def main():
             "roofline": {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": hbm,
                          "unit": "GB/s", "frac": (achieved / hbm) if achieved else None,
                          "traffic": (traffic * n) if traffic else None,
+                         "traffic_source": ("DRAM bytes per vertex of the ncu capture of this kernel on the "
+                                            "655,362-vertex sphere (profiles/), scaled to %d vertices" % n)
+                         if traffic else None,
                          "algorithmic_bytes": algo, "peak_source": src + " (MEASURED_PEAKS.json hbm_gbs)"
                          if src == "measured" else src, "launch_ms": per_launch_ms, "launches": cnt},
             "step_roofline": {"algorithmic_bytes": step_bytes, "achieved": step_gbs, "peak": hbm, "unit": "GB/s",
@@ -389,7 +405,7 @@ def main():
             "gpu_launches": launches,
             "clocks": clocks,
             "cpu_baseline": cpu,
-            "stats": stats.get("flow"),
+            "stats": {k: stats.get(k) for k in ("flow", "spl", "hillslope")},
             "loop_baseline": loop,
             "tuned": tuned,
             "adjoint": adj,
@@ -762,6 +778,8 @@ def _short(name):
         return "k_ordered_flow" if "FlowOrd" in s else ("k_ordered_spl" if "SplOrd" in s else "k_ordered")
     if "k_dataflow" in s:
         return "k_dataflow_flow" if "FlowOp" in s else ("k_dataflow_spl" if "SplOp" in s else "k_dataflow")
+    if "k_mfd_receivers" in s:
+        return "k_mfd_receivers"
     for tok in s.replace("(", " ").replace("<", " ").split():
         if tok.startswith("_ZN2gs"):
             rest = tok[6:]
@@ -806,7 +824,7 @@ def algo_bytes_per_launch(kname, L):
     if kname == "k_ordered_spl":
         # order 4, rcv 4R, coefficient 8R, hOld 8, h write 8
         return n * (4 + 12 * R + 16)
-    if kname == "k_bfs_local":
+    if kname in ("k_bfs_local", "k_bfs_tiles"):
         # packed rows of the pit cells (count + up to W local ids, padded to
         # a multiple of 4 ints) and one distance write per cell
         S = ((W + 1 + 3) // 4) * 4

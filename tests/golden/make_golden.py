@@ -1,9 +1,9 @@
 """Generate the golden fixtures under tests/golden/ from the reference itself.
 
-Run in a container where a goSPL checkout is available (default
-/root/reference, override with GOSPL_REF):
+Run where a goSPL checkout is available, named by --ref or the GOSPL_REF
+environment variable (no default):
 
-    python tests/golden/make_golden.py [case ...]
+    python tests/golden/make_golden.py --ref /path/to/gospl [case ...]
 
 For each case it (1) checks the oracle's restatement of the numpy Voronoi
 helpers against the reference's own ``gospl/mesher/meshfunc.py``, (2) runs the
@@ -23,7 +23,19 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 sys.path.insert(0, HERE)
 
-REF = os.environ.get("GOSPL_REF", "/root/reference")
+REF = os.environ.get("GOSPL_REF")
+
+
+def _take_ref_argument():
+    """--ref PATH on the command line overrides GOSPL_REF; one of them must
+    name the goSPL checkout."""
+    global REF
+    if "--ref" in sys.argv:
+        k = sys.argv.index("--ref")
+        REF = sys.argv[k + 1]
+        del sys.argv[k:k + 2]
+    if not REF:
+        sys.exit("name the goSPL checkout with --ref PATH or the GOSPL_REF environment variable")
 
 SNAP = ("h", "cumED", "EbLocal", "FAL", "fillFAL", "lFill", "pitIDs", "flatDirs", "waterFilled",
         "rcvIDi", "wghtVali", "distRcvi", "lsink", "lsinki", "pitParams", "pitInfo", "filled_lvl",
@@ -185,4 +197,5 @@ def main():
 
 
 if __name__ == "__main__":
+    _take_ref_argument()
     main()

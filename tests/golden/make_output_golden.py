@@ -1,9 +1,9 @@
 """Generate tests/golden/output_planar2k.npz from the reference's own output code.
 
-Run where a goSPL checkout is available (default /root/reference, override
-with GOSPL_REF):
+Run where a goSPL checkout is available, named by --ref or the GOSPL_REF
+environment variable (no default):
 
-    python tests/golden/make_output_golden.py
+    python tests/golden/make_output_golden.py --ref /path/to/gospl
 
 It runs the reference's one-rank orchestration (refharness.py) with goSPL's
 ``WriteMesh`` (``gospl/tools/outmesh.py``) mixed in, over the runProcesses
@@ -27,7 +27,19 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 sys.path.insert(0, HERE)
 
-REF = os.environ.get("GOSPL_REF", "/root/reference")
+REF = os.environ.get("GOSPL_REF")
+
+
+def _take_ref_argument():
+    """--ref PATH on the command line overrides GOSPL_REF; one of them must
+    name the goSPL checkout."""
+    global REF
+    if "--ref" in sys.argv:
+        k = sys.argv.index("--ref")
+        REF = sys.argv[k + 1]
+        del sys.argv[k:k + 2]
+    if not REF:
+        sys.exit("name the goSPL checkout with --ref PATH or the GOSPL_REF environment variable")
 NSTEPS = 3
 
 
@@ -152,4 +164,5 @@ def main():
 
 
 if __name__ == "__main__":
+    _take_ref_argument()
     main()
