@@ -179,7 +179,8 @@ def main():
     ap.add_argument("--cpu-level", type=int, default=7)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--workload", default="sphere", choices=["sphere", "planar", "ensemble", "precision",
-                                                                   "transport", "sediment", "output"])
+                                                                   "transport", "sediment", "output", "adjoint"])
+    ap.add_argument("--fd-vertices", type=int, default=64, help="adjoint: finite-difference samples per field")
     ap.add_argument("--members", type=int, default=256)
     ap.add_argument("--loop", action="store_true", help="ensemble: also time the per-member loop")
     ap.add_argument("--adjoint-steps", type=int, default=4, help="sphere: steps of the adjoint timing (0: skip)")
@@ -213,6 +214,9 @@ def main():
         return
     if args.workload == "output":
         run_output(args, dev)
+        return
+    if args.workload == "adjoint":
+        run_adjoint(args, dev)
         return
     pg = None
     if world > 1:
@@ -466,6 +470,103 @@ def adjoint_ratio(model, k, stream, dev, pg):
                              "what": "every step recorded during the forward (no recomputation); ratio = "
                                      "reverse step / plain forward step"},
             "finite": finite}
+
+
+def run_adjoint(args, dev):
+    """Inversion for erodibility on the 160k-vertex planar landscape: the
+    target is the elevation after 100 steps with the hidden 'true' K field;
+    the loss is the L2 elevation misfit of a run from uniform K.  Gradients
+    with respect to K, uplift and rain come from the hand-written adjoint with
+    a checkpoint every 10 steps; forward and backward are timed with CUDA
+    events (adjoint:forward cost ratio, the replay of each segment included).
+    Central finite differences at seeded interior vertices check them: the
+    difference of the two misfits is summed as sum (h+ - h-)(h+ + h- - 2t),
+    so it does not cancel two large numbers.  A perturbation that changes a
+    discrete decision (the final receivers or depression ids differ between
+    the + and - runs) has no derivative on the piece the adjoint follows;
+    those samples are counted and left out of the error."""
+    import torch
+    from gospl_b200 import adjoint as A
+    from gospl_b200 import synthetic as S
+    from gospl_b200.mesh import FVMesh
+    from gospl_b200.model import Model
+    c, f, z, rain, up, p, onb, k0 = S.adjoint_config()
+    nsteps, every = 100, 10
+    p = dict(p, rain=rain, upsub=up, tEnd=1.0e30)
+    mesh = FVMesh(c, f, p["bc"], device=dev)
+    model = Model(coords=c, cells=f, elev=z, params=p, mesh=mesh, device=dev)
+    n = model.lpoints
+    f64 = dict(dtype=torch.float64, device=dev)
+    Ktrue = torch.tensor(p["K"], **f64)
+    U = torch.tensor(up, **f64)
+    R = torch.tensor(rain, **f64)
+    h0 = torch.tensor(z, **f64)
+    stream = torch.cuda.current_stream(dev)
+    target, _ = A.run(model, Ktrue, U, R, h0, nsteps, every)
+    K0 = torch.full((n,), k0, **f64)
+    # warm-up, then the timed forward (with checkpoints) and backward
+    hT, ck = A.run(model, K0, U, R, h0, nsteps, every)
+    A.backward(model, K0, U, R, ck, nsteps, every, 2.0 * (hT - target))
+    torch.cuda.synchronize(dev)
+    e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    e[0].record(stream)
+    hT, ck = A.run(model, K0, U, R, h0, nsteps, every)
+    e[1].record(stream)
+    gK, gU, gR, gh = A.backward(model, K0, U, R, ck, nsteps, every, 2.0 * (hT - target))
+    e[2].record(stream)
+    torch.cuda.synchronize(dev)
+    tf, tb = e[0].elapsed_time(e[1]), e[1].elapsed_time(e[2])
+    loss = float(((hT - target) ** 2).sum())
+
+    def final(args):
+        h, _ = A.run(model, *args, h0, nsteps, every)
+        return h, model.rcv_i.clone(), model.pitIDs.clone()
+
+    rng = np.random.default_rng(20261208)
+    interior = np.where(~onb)[0]
+    nfd = args.fd_vertices
+    fields = {"K": (K0, gK), "uplift": (U, gU), "rain": (R, gR)}
+    fd_out = {}
+    for name, (base, grad) in fields.items():
+        idx = rng.choice(interior, nfd, replace=False)
+        rel, flips, rows = [], 0, []
+        for i in idx:
+            eps = 1e-4 * abs(float(base[i]))
+            vals = []
+            for sgn in (1.0, -1.0):
+                b = base.clone()
+                b[i] += sgn * eps
+                args_ = [K0, U, R]
+                args_[list(fields).index(name)] = b
+                vals.append(final(args_))
+            (hp, rp, pp), (hm, rm, pm) = vals
+            fd = float(((hp - hm) * (hp + hm - 2.0 * target)).sum()) / (2.0 * eps)
+            ad = float(grad[i])
+            flip = not (torch.equal(rp, rm) and torch.equal(pp, pm))
+            if flip:
+                flips += 1
+            else:
+                rel.append(abs(ad - fd) / max(abs(fd), 1e-300))
+            rows.append([int(i), ad, fd, flip])
+        rel = np.array(rel) if rel else np.array([np.nan])
+        fd_out[name] = {"samples": nfd, "decision_flips": flips, "max_rel_err": float(np.max(rel)),
+                        "median_rel_err": float(np.median(rel)), "rows": rows[:8]}
+    line = {"metric": "adjoint:forward cost ratio", "value": tb / tf, "unit": "ratio", "n_gpus": 1,
+            "steps": nsteps, "warmup": 1, "ms_per_step": tf / nsteps, "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded jittered hex mesh, Gaussian-field ln K, fractal relief)",
+            "config": {"workload": "adjoint inversion for erodibility: %d-vertex planar mesh, 200 x 200 km, "
+                                   "100 steps of 1000 yr, checkpoint every 10, L2 elevation misfit from "
+                                   "uniform K = exp(-12.5)" % n, "vertices": n, "checkpoint_every": every},
+            "forward_ms": tf, "adjoint_ms": tb, "adjoint_ms_per_step": tb / nsteps, "loss": loss,
+            "grad_norms": {"K": float(gK.norm()), "uplift": float(gU.norm()), "rain": float(gR.norm())},
+            "finite_differences": fd_out,
+            "fd_what": "central differences, step 1e-4 of the value, at seeded interior vertices; misfit "
+                       "difference summed as sum (h+ - h-)(h+ + h- - 2 target); samples whose + and - runs "
+                       "end with different receivers or depression ids are counted as decision flips and "
+                       "left out of the error"}
+    print(json.dumps(line), flush=True)
+    model.destroy()
 
 
 def run_precision(args, dev):

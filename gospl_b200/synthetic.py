@@ -271,6 +271,52 @@ def sphere_config(level=9, seed=20261205, lmax=256, zlo=-4000.0, zhi=3000.0, ste
     return coords, cells, z, rain, up, params
 
 
+def gp_field(xy, extent, seed, ell, ngrid=512):
+    """Seeded stationary Gaussian field with squared-exponential covariance
+    exp(-r^2 / (2 ell^2)) at the points xy of [0, extent]^2: white noise on a
+    periodic ngrid^2 grid over twice the extent (so the period exceeds the
+    domain plus the correlation length), filtered by the square root of the
+    covariance's spectral density exp(-2 pi^2 ell^2 |f|^2), bilinear at xy;
+    unit variance."""
+    rng = np.random.default_rng(seed)
+    span = 2.0 * extent
+    f = np.fft.fftfreq(ngrid, d=span / ngrid)
+    fx = f[:, None]
+    fy = np.fft.rfftfreq(ngrid, d=span / ngrid)[None, :]
+    amp = np.exp(-np.pi ** 2 * ell ** 2 * (fx * fx + fy * fy))
+    noise = np.fft.rfft2(rng.standard_normal((ngrid, ngrid)))
+    grid = np.fft.irfft2(noise * amp, s=(ngrid, ngrid))
+    grid = (grid - grid.mean()) / grid.std()
+    u = np.clip(xy[:, 0] / span * ngrid, 0, ngrid - 1.000001)
+    w = np.clip(xy[:, 1] / span * ngrid, 0, ngrid - 1.000001)
+    i0 = np.floor(u).astype(int)
+    j0 = np.floor(w).astype(int)
+    fu = u - i0
+    fw = w - j0
+    g = grid
+    return ((1 - fu) * (1 - fw) * g[i0, j0] + fu * (1 - fw) * g[i0 + 1, j0] +
+            (1 - fu) * fw * g[i0, j0 + 1] + fu * fw * g[i0 + 1, j0 + 1])
+
+
+def adjoint_config(n=160000, side=200.0e3, seed=20261207):
+    """Inversion for erodibility: a jittered-hex planar mesh of ~n vertices over
+    side x side, fractal initial relief 0-100 m with fixed boundary vertices at
+    0, uplift 0.5 mm/yr (none on the boundary), rain 1 m/yr, dt 1000 yr, and
+    the hidden 'true' erodibility: ln K a Gaussian field (correlation length
+    20 km) scaled to -14..-11.  Returns coords, cells, z, rain, uplift,
+    params (K = the true field), the boundary mask and the uniform start
+    K0 = exp(-12.5)."""
+    coords, cells, onb = planar_hex_mesh(n, side, seed)
+    z = rescale(fractal_field(coords[:, :2], side, seed + 1), 0.0, 100.0)
+    z[onb] = 0.0
+    lnk = rescale(gp_field(coords[:, :2], side, seed + 2, 20.0e3), -14.0, -11.0)
+    up = np.full(len(z), 5.0e-4)
+    up[onb] = 0.0
+    params = dict(dt=1000.0, tStart=0.0, tEnd=100 * 1000.0, flowDir=3, K=np.exp(lnk), d=0.0, m=0.5,
+                  Cda=0.1, Cdm=0.1, sealevel=-100.0, oFill=-6000.0, bc="ffff")
+    return coords, cells, z, np.ones(len(z)), up, params, onb, float(np.exp(-12.5))
+
+
 def ensemble_member(n, seed, spacing=250.0):
     """One ensemble landscape: ~n vertices at `spacing`, own K, rain and relief."""
     rng = np.random.default_rng(seed)
