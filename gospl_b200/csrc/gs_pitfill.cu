@@ -655,25 +655,29 @@ __global__ void __launch_bounds__(1024) k_bfs_local(int M, int S, const int* __r
     if (tid == 0) *levels_out = levels;
 }
 
-// Flat distances by tiles, in one cooperative launch.  The reachable cells
-// are compacted in vertex order (local ids), and vertex ids follow a
-// space-filling curve, so tile t = local ids [tT, tT + T) is a compact patch
-// of the mesh.  A round: every block takes its tiles that were marked, loads
-// their adjacency rows and distances into shared memory and closes the BFS
-// inside the tile there (label-correcting: a cell whose distance dropped
-// relaxes its out-neighbours again, one block barrier per wave); a hop out of
-// the tile lowers the target's global distance with atomicMin and marks the
-// target's tile for the next round.  A grid barrier ends the round; the loop
-// ends after a round that marked nothing.  Distances only decrease and every
-// cell whose shortest path crosses r tile boundaries is exact after round r,
-// so the result is the breadth-first hop distance, and the round count is
-// bounded by the number of tiles a shortest path crosses (no timed wait).
+// Flat distances by tiles, in one cooperative launch (delta-stepping).  The
+// reachable cells are compacted in vertex order (local ids), and vertex ids
+// follow a space-filling curve, so tile t = local ids [tT, tT + T) is a
+// compact patch of the mesh; with no more tiles than blocks every block keeps
+// its tile's adjacency rows in shared memory for the whole launch.
+// Distances are settled by windows [lo, lo + window): in a round, every tile whose
+// smallest pending distance falls in the window loads its distances, relaxes
+// its cells of the window and then, one block barrier per wave, the cells they
+// lower within the window; a cell lowered beyond the window only records the
+// tile's pending minimum, and a hop out of the tile lowers the target's
+// global distance (atomicMin) and the target tile's pending minimum.  Every
+// pending minimum also lowers a global minimum for the round (three rotating
+// slots), which all blocks read after the grid barrier: the same window again
+// while it still holds pending cells, else the next window starts at the
+// smallest pending distance, and no pending cell ends the launch.  Distances
+// only decrease and a window is closed only when no cell of it is pending, so
+// every distance is the breadth-first hop count (exact, no timed wait).
 constexpr int BFT_THREADS = 512;
 
 __global__ void __launch_bounds__(BFT_THREADS, 2) k_bfs_tiles(int M, int S, int T, const int* __restrict__ rows,
                                                               const int* __restrict__ seeds,
                                                               const int* __restrict__ nseed_p, int* ld, int* ctl,
-                                                              int* depth_out) {
+                                                              int window, int* depth_out, int* rounds_out) {
     cg::grid_group grid = cg::this_grid();
     extern __shared__ int sm_bft[];
     const int INF = 0x7fffffff;
@@ -681,48 +685,66 @@ __global__ void __launch_bounds__(BFT_THREADS, 2) k_bfs_tiles(int M, int S, int 
     int* ds = rs + T * S;          // [T] distances
     int* fl0 = ds + T;             // [T] frontier lists
     int* fl1 = fl0 + T;
+    int* xc = fl1 + T;             // [T] hops out of the tile: target, distance
+    int* xd = xc + T;
     __shared__ int s_cnt[3];
     __shared__ int s_over[3];
-    __shared__ int s_mark;
+    __shared__ int s_pmin;
+    __shared__ int s_nx;
     const int ntiles = (M + T - 1) / T;
-    int* cnt = ctl;                // [3] tiles marked for rounds r % 3
-    int* mark = ctl + 3;           // [2][ntiles]
+    int* gmin = ctl;               // [3] smallest pending distance after rounds r % 3
+    int* pend = ctl + 3;           // [ntiles] smallest pending distance of each tile
     const int tid = threadIdx.x, nt = blockDim.x;
     const unsigned gtid = grid.thread_rank(), gsz = (unsigned)grid.size();
     for (unsigned i = gtid; i < (unsigned)M; i += gsz) ld[i] = INF;
-    for (unsigned t = gtid; t < 2u * (unsigned)ntiles; t += gsz) mark[t] = 0;
-    if (gtid < 3) cnt[gtid] = 0;
+    for (unsigned t = gtid; t < (unsigned)ntiles; t += gsz) pend[t] = INF;
+    if (gtid < 3) gmin[gtid] = INF;
     grid.sync();
     const int ns = *nseed_p;
     for (unsigned q = gtid; q < (unsigned)ns; q += gsz) {
         const int li = seeds[q];
         ld[li] = 1;
-        mark[li / T] = 1;
+        pend[li / T] = 1;
     }
-    if (gtid == 0) cnt[0] = ns > 0 ? 1 : 0;
     grid.sync();
-    for (int r = 0;; r++) {
-        if (((volatile int*)cnt)[r % 3] == 0) break;   // written before the last grid barrier: same in every block
-        int* mcur = mark + (r & 1) * ntiles;
-        int* mnext = mark + ((r + 1) & 1) * ntiles;
-        if (blockIdx.x == 0 && tid == 0) cnt[(r + 2) % 3] = 0;
-        if (tid == 0) s_mark = 0;
+    int lo = 1, hi = window;
+    int cached = -1;
+    int rounds = 0;
+    if (ns == 0) lo = INF;
+    for (int r = 0; lo != INF; r++) {
+        rounds++;
+        int* gnext = gmin + ((r + 1) % 3);
+        if (blockIdx.x == 0 && tid == 0) gmin[(r + 2) % 3] = INF;
         for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
             __syncthreads();
-            if (!((volatile int*)mcur)[t]) continue;
+            const int pt = ((volatile int*)pend)[t];
+            if (pt > hi) {
+                // nothing of this window here: its pending minimum stays for later
+                if (tid == 0 && pt != INF) atomicMin(gnext, pt);
+                continue;
+            }
             const int base = t * T, len = min(T, M - base);
-            {
+            if (cached != t) {
                 const int4* src = reinterpret_cast<const int4*>(rows + (size_t)base * S);
                 int4* dst = reinterpret_cast<int4*>(rs);
                 const int nq = len * S / 4;
                 for (int q = tid; q < nq; q += nt) dst[q] = src[q];
+                cached = t;
             }
+            if (tid == 0) {
+                atomicExch(&pend[t], INF);
+                __threadfence();
+            }
+            __syncthreads();
             for (int i = tid; i < len; i += nt) ds[i] = ((volatile int*)ld)[base + i];
-            // wave 0 relaxes every reached cell of the tile (a full wave,
-            // as any wave whose list overflowed)
+            // wave 0 relaxes every cell of the tile inside the window
             if (tid < 3) {
                 s_cnt[tid] = 0;
                 s_over[tid] = tid == 0 ? 1 : 0;
+            }
+            if (tid == 0) {
+                s_pmin = INF;
+                s_nx = 0;
             }
             __syncthreads();
             for (int w = 0;; w++) {
@@ -739,36 +761,78 @@ __global__ void __launch_bounds__(BFT_THREADS, 2) k_bfs_tiles(int M, int S, int 
                 for (int e = tid; e < size; e += nt) {
                     const int i = full ? e : lin[e];
                     const int d = ds[i];
-                    if (d == INF) continue;
+                    if (d < lo || d > hi) continue;
                     const int* row = rs + i * S;
                     const int k = row[0];
                     const int nd = d + 1;
+                    // lower the in-tile out-neighbours, then one append for
+                    // those that dropped inside the window; hops out of the
+                    // tile are buffered and applied once after the waves
+                    unsigned got = 0u;
                     for (int q = 1; q <= k; q++) {
                         const int c = row[q];
                         const int lc = c - base;
                         if ((unsigned)lc < (unsigned)len) {
-                            if (atomicMin(&ds[lc], nd) > nd) {
-                                const int pos = atomicAdd(&s_cnt[wr], 1);
-                                if (pos < T) lout[pos] = lc;
-                                else s_over[wr] = 1;
+                            if (atomicMin(&ds[lc], nd) > nd && nd <= hi) got |= 1u << q;
+                        } else {
+                            const int x = atomicAdd(&s_nx, 1);
+                            if (x < T) {
+                                xc[x] = c;
+                                xd[x] = nd;
+                            } else if (atomicMin(&ld[c], nd) > nd) {
+                                atomicMin(&pend[c / T], nd);
+                                atomicMin(gnext, nd);
                             }
-                        } else if (atomicMin(&ld[c], nd) > nd) {
-                            mnext[c / T] = 1;
-                            s_mark = 1;
+                        }
+                    }
+                    if (got) {
+                        int pos = atomicAdd(&s_cnt[wr], __popc(got));
+                        for (int q = 1; q <= k; q++) {
+                            if (!(got & (1u << q))) continue;
+                            if (pos < T) lout[pos] = row[q] - base;
+                            else s_over[wr] = 1;
+                            pos++;
                         }
                     }
                 }
                 __syncthreads();
             }
+            // the buffered hops out of the tile, their latencies overlapped
+            {
+                const int nx = min(s_nx, T);
+                for (int x = tid; x < nx; x += nt) {
+                    const int c = xc[x], nd = xd[x];
+                    if (atomicMin(&ld[c], nd) > nd) {
+                        atomicMin(&pend[c / T], nd);
+                        atomicMin(gnext, nd);
+                    }
+                }
+            }
+            // write back; no cell beyond the window has been relaxed yet, so
+            // the smallest such distance is the tile's pending minimum
+            int pmin = INF;
             for (int i = tid; i < len; i += nt) {
                 const int d = ds[i];
                 if (d < ((volatile int*)ld)[base + i]) atomicMin(&ld[base + i], d);
+                if (d > hi && d < pmin) pmin = d;
             }
-            if (tid == 0) mcur[t] = 0;
+            pmin = __reduce_min_sync(0xffffffffu, pmin);
+            if ((tid & 31) == 0 && pmin != INF) atomicMin(&s_pmin, pmin);
+            __syncthreads();
+            if (tid == 0 && s_pmin != INF) {
+                atomicMin(&pend[t], s_pmin);
+                atomicMin(gnext, s_pmin);
+            }
         }
-        __syncthreads();
-        if (tid == 0 && s_mark) atomicAdd(&cnt[(r + 1) % 3], 1);
         grid.sync();
+        // the same in every block: written before the barrier, cleared two rounds later
+        const int g = ((volatile int*)gmin)[(r + 1) % 3];
+        if (g == INF) break;
+        if (g > hi) {
+            lo = g;
+            hi = g + window - 1;
+        }
+        if (r > 4 * M + 8) break;   // cannot happen: every round settles a pending cell or moves the window
     }
     int dmax = 0;
     for (unsigned i = gtid; i < (unsigned)M; i += gsz) {
@@ -778,6 +842,7 @@ __global__ void __launch_bounds__(BFT_THREADS, 2) k_bfs_tiles(int M, int S, int 
     }
     dmax = __reduce_max_sync(0xffffffffu, dmax);
     if ((tid & 31) == 0 && dmax > 0) atomicMax(depth_out, dmax);
+    if (gtid == 0) *rounds_out = rounds;
 }
 
 // Whole BFS in one cooperative launch: wide levels use the whole grid with a
@@ -1084,12 +1149,12 @@ static int launch_coop(gs_plan* p, const void* fn, void** args) {
 // Tiled flat-distance BFS (k_bfs_tiles) over the M compacted cells whose
 // rows, seeds (front0, count in i_scalar[6]) and local ids k_bfs_local_build
 // wrote; distances into ld (-1 unreached), depth into i_scalar[4].  Tiles of
-// T cells with T * (S + 3) ints of shared memory (<= 96 KB), as many blocks as
-// stay co-resident.
+// T cells with T * (S + 5) ints of shared memory (<= 112 KB), as many blocks
+// as stay co-resident.
 static int bfs_tiles(gs_plan* p, int M, int S, const int* rows, int* ld) {
     int T = 4096;
-    while (T > 256 && (size_t)T * (S + 3) * sizeof(int) > 96 * 1024) T >>= 1;
-    const size_t smem = (size_t)T * (S + 3) * sizeof(int);
+    while (T > 256 && (size_t)T * (S + 5) * sizeof(int) > 112 * 1024) T >>= 1;
+    const size_t smem = (size_t)T * (S + 5) * sizeof(int);
     GS_CUDA(cudaFuncSetAttribute(k_bfs_tiles, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int occ = 0;
     GS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_bfs_tiles, BFT_THREADS, smem));
@@ -1099,7 +1164,7 @@ static int bfs_tiles(gs_plan* p, int M, int S, const int* rows, int* ld) {
     }
     const int ntiles = (M + T - 1) / T;
     const int grid = std::max(1, std::min(ntiles, p->sm_count * occ));
-    if (3 + 2 * ntiles > (int)p->n + 1) {
+    if (3 + ntiles > (int)p->n + 1) {
         set_error(GS_EINVAL, "flat BFS: tile marks exceed their buffer");
         return GS_EINVAL;
     }
@@ -1109,8 +1174,10 @@ static int bfs_tiles(gs_plan* p, int M, int S, const int* rows, int* ld) {
     const int* nseed = p->i_scalar + 6;
     int* ctl = p->front1;
     int* depth = p->i_scalar + 4;
+    int* rounds = p->i_scalar + 15;
+    int window = p->bfs_window;
     void* args[] = {(void*)&m, (void*)&s, (void*)&t, (void*)&rows, (void*)&seeds, (void*)&nseed, (void*)&ld,
-                    (void*)&ctl, (void*)&depth};
+                    (void*)&ctl, (void*)&window, (void*)&depth, (void*)&rounds};
     cudaEvent_t stop = nullptr;
     if (p->profiling) prof_begin(p, (const void*)k_bfs_tiles, &stop);
     GS_CUDA(cudaLaunchCooperativeKernel((const void*)k_bfs_tiles, grid, BFT_THREADS, args, smem, p->stream));
@@ -1330,7 +1397,22 @@ int fill_elevation(gs_plan* p, const double* h, double sealevel, double ofill, d
                        (const int*)p->flagbuf, (const int*)p->scanbuf, (const int*)p->nbr, (const int8_t*)p->nnb,
                        (const int*)p->spill_flag, rows, p->comp, ldv, p->front0, p->i_scalar + 6);
                 GS_LAUNCH();
-                GS_TRY(bfs_tiles(p, M, S, rows, ldv));
+                const size_t smem1 = sizeof(unsigned) * (size_t)((M + 31) / 32) + sizeof(int) * 2 * LBFS_CAP;
+                if (p->bfs_window > 0 || smem1 > 200 * 1024) {
+                    GS_TRY(bfs_tiles(p, M, S, rows, ldv));
+                } else {
+                    // one block: visited bitmap and frontiers in shared memory
+                    GS_CUDA(cudaFuncSetAttribute(k_bfs_local, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 (int)smem1));
+                    cudaEvent_t stop = nullptr;
+                    if (p->profiling) prof_begin(p, (const void*)k_bfs_local, &stop);
+                    k_bfs_local<<<1, 1024, smem1, p->stream>>>(M, S, (const int*)rows, (const int*)p->front0,
+                                                                p->i_scalar + 6, p->front1, p->minseed, ldv,
+                                                                p->i_scalar + 4);
+                    if (stop) cudaEventRecord(stop, p->stream);
+                    p->launches++;
+                    GS_LAUNCH();
+                }
                 launch(p, k_bfs_local_scatter, grid_for(M, B), B, M, (const int*)p->comp, (const int*)ldv,
                        p->pdir);
                 launch(p, k_flat_dirs, G, B, n, (const double*)lfill, (const int*)pit_ids, (const int*)p->pdir,

@@ -412,6 +412,14 @@ int plan_tune(gs_plan* p, int knob, int value) {
         p->sweep_nap = (unsigned)value;
         return GS_OK;
     }
+    if (knob == GS_TUNE_FLAT_BFS) {
+        if (value < 0 || value > 4096) {
+            set_error(GS_EINVAL, "tune: flat BFS must be 0 (one block) or a window of 1..4096 levels (tiles)");
+            return GS_EINVAL;
+        }
+        p->bfs_window = value;
+        return GS_OK;
+    }
     if (knob == GS_TUNE_SWEEP_BUDGET) {
         if (value < 1 || value > 60000000) {
             set_error(GS_EINVAL, "tune: sweep time budget must be in 1..60000000 us");
@@ -430,6 +438,7 @@ int plan_tuning(const gs_plan* p, int knob) {
     if (knob == GS_TUNE_COOP_BLOCKS + 1) return p->coop_max_per_sm;
     if (knob == GS_TUNE_SWEEP_NAP) return (int)p->sweep_nap;
     if (knob == GS_TUNE_SWEEP_BUDGET) return (int)(p->sweep_budget_ns / 1000ULL);
+    if (knob == GS_TUNE_FLAT_BFS) return p->bfs_window;
     if (knob == GS_TUNE_REFINE_PASSES) return (int)std::min<int64_t>(p->refine_iters, 0x7fffffff);
     return -1;
 }

@@ -192,3 +192,22 @@ def test_gpu_definitions_at_full_size(capsys):
         print("\nsphere 2621442: receiver slope pairs within 4 ulp among the %d steepest: %d"
               % (om.flowDir + 1, near))
     gm.destroy()
+
+
+@pytest.mark.parametrize("window", [0, 1, 8, 64, 4096])
+def test_flat_bfs_forms_are_the_definition(window):
+    """The flat distances (and so flatDirs) are the same breadth-first hop
+    counts whichever form computes them (GS_TUNE_FLAT_BFS): the one-block
+    BFS (0) and the tiled delta-stepping BFS with windows of 1 to 4096
+    levels, on a lake-rich planar case, the icosphere and a plateau."""
+    from gospl_b200 import _lib
+    L = _lib.load()
+    for case in ("planar2k", "ico2562", "flat_ffff"):
+        om = _oracle(case)
+        gm = _model_like(om)
+        _lib.check(L.gs_plan_tune(gm._plan, 7, window))
+        assert L.gs_plan_tuning(gm._plan, 7) == window
+        h0 = om.h.copy()
+        check_gpu_fill(gm, om, h0, False, "%s window %d" % (case, window))
+        check_gpu_fill(gm, om, h0, True, "%s sed window %d" % (case, window))
+        gm.destroy()
