@@ -1368,20 +1368,19 @@ int fill_elevation(gs_plan* p, const double* h, double sealevel, double ofill, d
     // hold no pit.
     GS_CUDA(cudaMemsetAsync(p->i_scalar + I_NEXT, 0, sizeof(int), p->stream));
     launch(p, k_bfs_init, G, B, n, (const int*)p->spill_flag, p->pdir, p->front0, p->i_scalar + I_NEXT);
+    // the reachable set is compacted before the seed count is read, so one
+    // synchronisation gives both (the compaction is wasted only without pits)
+    launch(p, k_bfs_flag, G, B, n, (const int*)pit_ids, (const int*)p->spill_flag, p->flagbuf);
     GS_LAUNCH();
-    GS_TRY(read_ints(p, hbuf, p->i_scalar + I_NEXT, 1));
-    int fsize = hbuf[0], levels = 0;
+    GS_TRY(exclusive_scan(p, p->flagbuf, p->scanbuf, n));
+    int last[3];
+    GS_CUDA(cudaMemcpyAsync(&last[0], p->scanbuf + n - 1, sizeof(int), cudaMemcpyDeviceToHost, p->stream));
+    GS_CUDA(cudaMemcpyAsync(&last[1], p->flagbuf + n - 1, sizeof(int), cudaMemcpyDeviceToHost, p->stream));
+    GS_CUDA(cudaMemcpyAsync(&last[2], p->i_scalar + I_NEXT, sizeof(int), cudaMemcpyDeviceToHost, p->stream));
+    GS_CUDA(cudaStreamSynchronize(p->stream));
+    int fsize = last[2], levels = 0;
     bool forked = false;
     if (fsize > 0) {
-        // compact the reachable set; use the shared-memory BFS when its
-        // visited bitmap fits, the cooperative grid BFS otherwise
-        launch(p, k_bfs_flag, G, B, n, (const int*)pit_ids, (const int*)p->spill_flag, p->flagbuf);
-        GS_LAUNCH();
-        GS_TRY(exclusive_scan(p, p->flagbuf, p->scanbuf, n));
-        int last[2];
-        GS_CUDA(cudaMemcpyAsync(&last[0], p->scanbuf + n - 1, sizeof(int), cudaMemcpyDeviceToHost, p->stream));
-        GS_CUDA(cudaMemcpyAsync(&last[1], p->flagbuf + n - 1, sizeof(int), cudaMemcpyDeviceToHost, p->stream));
-        GS_CUDA(cudaStreamSynchronize(p->stream));
         const int M = last[0] + last[1];
         if (true) {
             GS_CUDA(cudaEventRecord(p->ev_fork_b, p->stream));

@@ -20,7 +20,7 @@ struct gs_plan {
     int sweep_per_sm = 8;                // 128-thread blocks per SM of the ordered sweeps
     unsigned sweep_nap = 128;            // longest back-off (ns) between polls of the ordered sweeps
     unsigned long long sweep_budget_ns = 4000000000ULL;   // wall-clock budget of one dependency sweep
-    int bfs_window = 32;                 // flat-distance BFS: 0 one block, w > 0 tiles, windows of w levels
+    int bfs_window = 0;                  // flat-distance BFS: 0 one block, w > 0 tiles, windows of w levels
     // precision form: FP32 sweeps and CG inside FP64 refinement loops
     int fp32 = 0;
     double fdepa = 0.0;                  // SPL deposition coefficient G (0: detachment-limited)

@@ -94,9 +94,9 @@ int gs_plan_set_stream(gs_plan* plan, void* cuda_stream);
 #define GS_TUNE_SWEEP_NAP 5       /* longest back-off between polls of the ordered sweeps, ns (0..1024, default 128) */
 #define GS_TUNE_SWEEP_BUDGET 6    /* wall-clock budget of one dependency sweep, us (1..6e7, default 4e6): a sweep
                                      still waiting on a predecessor after it stops with GS_ETIMEOUT */
-#define GS_TUNE_FLAT_BFS 7        /* flat-distance BFS: w in 1..4096 tiles in one cooperative launch settling
-                                     distance windows of w levels (default 32), 0 one block with the visited
-                                     set in shared memory (when it fits) */
+#define GS_TUNE_FLAT_BFS 7        /* flat-distance BFS: 0 one block with the visited set in shared memory
+                                     (default; tiles when the set does not fit), w in 1..4096 tiles in one
+                                     cooperative launch settling distance windows of w levels */
 int gs_plan_tune(gs_plan* plan, int32_t knob, int32_t value);
 /*
  * Precision form (no counterpart in the reference, which is FP64 only).
