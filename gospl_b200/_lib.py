@@ -21,7 +21,7 @@ EXPORTS = ("gs_version", "gs_last_error", "gs_plan_create", "gs_plan_destroy", "
            "gs_plan_tune", "gs_plan_tuning", "gs_plan_set_precision", "gs_plan_set_deposition",
            "gs_plan_set_stream",
            "gs_plan_launches", "gs_mfdreceivers", "gs_fill_elevation", "gs_build_flow_direction", "gs_pit_tables",
-           "gs_flow_accumulation", "gs_erodep_spl", "gs_sed_change", "gs_sed_budget", "gs_plan_set_lake_diffusion", "gs_hillslope", "gs_apply_forces", "gs_output_fields", "gs_mesh_geometry", "gs_plan_profile",
+           "gs_flow_accumulation", "gs_erodep_spl", "gs_sed_change", "gs_sed_budget", "gs_sea_change", "gs_plan_set_lake_diffusion", "gs_hillslope", "gs_apply_forces", "gs_output_fields", "gs_mesh_geometry", "gs_plan_profile",
            "gs_plan_profile_report", "gs_plan_profile_trace", "gs_plan_record", "gs_plan_record_slot",
            "gs_adjoint_step", "gs_flow_solve_noalloc")
 
@@ -80,6 +80,7 @@ def load(path=None):
     L.gs_plan_set_lake_diffusion.argtypes = [P, d, d, i32, i32]
     L.gs_sed_change.argtypes = [P, P, P, P, P, d, d, d, d, d, P, P, P, P, P, P, P, P, ctypes.POINTER(GsStats)]
     L.gs_sed_budget.argtypes = [P, P]
+    L.gs_sea_change.argtypes = [P, P, P, P, P, P, P, i64, d, d, d, d, d, d, P, P, P, ctypes.POINTER(GsStats)]
     L.gs_hillslope.argtypes = [P, P, P, P, d, d, d, d, d, i32, ctypes.POINTER(GsStats)]
     L.gs_apply_forces.argtypes = [P, P, P, P, d, d, P]
     L.gs_output_fields.argtypes = [P, P, P, P, P, P, P, P, P, P, P, P]

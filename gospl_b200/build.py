@@ -15,7 +15,7 @@ CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libgospl_b200.so")
 SOURCES = ["gs_capi.cu", "gs_plan.cu", "gs_receivers.cu", "gs_sweep.cu", "gs_pitfill.cu", "gs_flow.cu",
            "gs_spl.cu", "gs_diffusion.cu", "gs_force.cu", "gs_mesh.cu", "gs_noalloc.cu", "gs_adjoint.cu",
-           "gs_sed.cu", "gs_output.cu"]
+           "gs_sed.cu", "gs_output.cu", "gs_marine.cu"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "--fmad=false", "-std=c++17",
          "-Xcompiler", "-fPIC", "-Xcompiler", "-O2", "-I" + os.path.join(ROOT, "include")]

@@ -332,7 +332,7 @@ int gs_plan_set_lake_diffusion(gs_plan* plan, double k, double inlet_bias, int32
 int gs_sed_change(gs_plan* plan, double* h, double* cum_ed, const double* eb, const double* xyz, double sealevel,
                   double ofill, double dt, double nl_pit_volume, double nl_pit_depth, double* lfill,
                   int32_t* pit_ids, int32_t* flat_dirs, const int32_t* rcv_i, const double* wgt_i, uint8_t* lsink,
-                  const uint8_t* sea, double* vsed, gs_stats* stats) {
+                  uint8_t* sea, double* vsed, gs_stats* stats) {
     NEED(plan);
     if (plan->n > 0) {
         NEED(h); NEED(cum_ed); NEED(eb); NEED(xyz); NEED(lfill); NEED(pit_ids); NEED(flat_dirs); NEED(rcv_i);
@@ -344,6 +344,24 @@ int gs_sed_change(gs_plan* plan, double* h, double* cum_ed, const double* eb, co
     }
     GS_GUARD(return gs::sed_change(plan, h, cum_ed, eb, xyz, sealevel, ofill, dt, nl_pit_volume, nl_pit_depth,
                                    lfill, pit_ids, flat_dirs, rcv_i, wgt_i, lsink, sea, vsed, stats);)
+}
+
+int gs_sea_change(gs_plan* plan, double* h, double* cum_ed, double* eb, const double* xyz, const double* box,
+                  const int32_t* edges, int64_t nedge, double sealevel, double ofill, double dt, double clinslp,
+                  double offshore, double nlk, const double* lfill, const double* vsed, const uint8_t* sea,
+                  gs_stats* stats) {
+    NEED(plan);
+    NEED(box);
+    if (plan->n > 0) {
+        NEED(h); NEED(cum_ed); NEED(eb); NEED(xyz); NEED(lfill); NEED(vsed); NEED(sea);
+        if (nedge > 0) NEED(edges);
+    }
+    if (!(dt > 0) || nedge < 0 || !(clinslp >= 0) || !(offshore > 0) || !(nlk >= 0)) {
+        gs::set_error(GS_EINVAL, "seaChange: need dt > 0, nedge >= 0, clinslp >= 0, offshore > 0, nlk >= 0");
+        return GS_EINVAL;
+    }
+    GS_GUARD(return gs::sea_change(plan, h, cum_ed, eb, xyz, box, edges, nedge, sealevel, ofill, dt, clinslp, offshore,
+                                   nlk, lfill, vsed, sea, stats);)
 }
 
 int gs_sed_budget(gs_plan* plan, double* out16) {

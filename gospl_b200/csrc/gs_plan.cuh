@@ -32,6 +32,11 @@ struct gs_plan {
     uint8_t* sed_mask = nullptr;         // [5][n] sediment-routing masks
     double* sed_pit = nullptr;           // [2][n+1] per-depression scratch
     double* led = nullptr;               // [16] sediment budget of the last sedChange (GS_LED_* slots)
+    double* sea_buf = nullptr;           // [12][n] marine deposition work vectors
+    uint8_t* sea_u8 = nullptr;           // [4][n] marine masks and receiver bit sets
+    double* sea_coef = nullptr;          // [W+1][n] bathymetry smoothing operator
+    double* sea_pts = nullptr;           // coastline points, sorted copies, keys and boxes
+    int64_t sea_pts_cap = 0;             // edges the coastline buffers hold
     double* led_part = nullptr;          // [5][LED_NB] block partial sums of the budget reductions
     double* sed_coef = nullptr;          // [W+1][n] lake diffusion operator (compacted to the lake cells)
     int* lake_i = nullptr;               // [W+1][n]: lake cell list, then the compact neighbour slots
@@ -299,9 +304,15 @@ int erodep_spl(gs_plan* p, double* h, double* cum_ed, double* eb, const double* 
                const uint8_t* lsink, const uint8_t* sea, gs_stats* st);
 int sed_change(gs_plan* p, double* h, double* cum_ed, const double* eb, const double* xyz, double sealevel,
                double ofill, double dt, double nl_pit_volume, double nl_pit_depth, double* lfill, int* pit_ids,
-               int* flat_dirs, const int* rcv_i, const double* wgt_i, uint8_t* lsink, const uint8_t* sea,
+               int* flat_dirs, const int* rcv_i, const double* wgt_i, uint8_t* lsink, uint8_t* sea,
                double* vsed, gs_stats* st);
 int sed_budget(gs_plan* p, double* out16);
+int sea_change(gs_plan* p, double* h, double* cum_ed, double* eb, const double* xyz, const double* box,
+               const int* edges, int64_t nedge, double sealevel, double ofill, double dt, double clinslp,
+               double offshore, double nlk, const double* lfill, const double* vsed, const uint8_t* sea,
+               gs_stats* st);
+int picard_diffuse(gs_plan* p, const uint8_t* lmask, const double* zb, double* hcur, double K, double dt,
+                   double* cd, double* hstart);
 int diffusion_solve_on(gs_plan* p, int m, const int* nbr, const int8_t* nnb, const double* farea, const uint8_t* fix,
                        int flat, const uint8_t* outlet, const double* coef, const double* rhs, double* x, double rtol,
                        int max_iter, int* iters);

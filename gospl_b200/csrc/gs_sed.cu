@@ -625,9 +625,72 @@ int sed_budget(gs_plan* p, double* out16) {
     return GS_OK;
 }
 
+// picardSub x picardIts lagged-diffusivity backward-Euler solves of
+// (I + dt_sub L(C_d(h))) h = h_start over the cells of lmask, faces to the
+// other cells closed (_diffuseImplicitPicard, hillslope.py:988-1076, with
+// C_d = 1e-4 + K (1 - exp(-0.05 (h - zb)))): hcur holds the start surface on
+// entry and the result on return; cd and hstart are [n] scratch.  The cells
+// of lmask form a sub-mesh of m rows, each solve is the cooperative CG on it.
+int picard_diffuse(gs_plan* p, const uint8_t* lmask, const double* zb, double* hcur, double K, double dt,
+                   double* cd, double* hstart) {
+    const int n = (int)p->n;
+    const int B = 256, G = grid_for(n, B);
+    // the lake cells as a sub-mesh of m rows
+    const int W = p->W;
+    if (!p->sed_coef) GS_CUDA(cudaMalloc((void**)&p->sed_coef, sizeof(double) * (size_t)n * (size_t)(W + 1)));
+    if (!p->lake_i) {
+        GS_CUDA(cudaMalloc((void**)&p->lake_i, sizeof(int) * (size_t)n * (size_t)(W + 1)));
+        GS_CUDA(cudaMalloc((void**)&p->lake_d, sizeof(double) * (size_t)n * 3));
+        GS_CUDA(cudaMalloc((void**)&p->lake_u8, (size_t)n * 2));
+    }
+    int* cell = p->lake_i;
+    int* nbr_c = cell + n;
+    double* farea_c = p->lake_d;
+    double* rhs_c = farea_c + n;
+    double* x_c = rhs_c + n;
+    int8_t* nnb_c = (int8_t*)p->lake_u8;
+    uint8_t* fix_c = p->lake_u8 + n;
+    launch(p, k_lake_flag, G, B, n, (const uint8_t*)lmask, p->flagbuf);
+    GS_LAUNCH();
+    {
+        size_t bytes = p->cub_bytes;
+        GS_CUDA(cub::DeviceScan::ExclusiveSum(p->cub_tmp, bytes, (const int*)p->flagbuf, p->scanbuf, n, p->stream));
+        p->launches++;
+    }
+    int last[2];
+    GS_CUDA(cudaMemcpyAsync(&last[0], p->scanbuf + n - 1, sizeof(int), cudaMemcpyDeviceToHost, p->stream));
+    GS_CUDA(cudaMemcpyAsync(&last[1], p->flagbuf + n - 1, sizeof(int), cudaMemcpyDeviceToHost, p->stream));
+    GS_CUDA(cudaStreamSynchronize(p->stream));
+    const int m = last[0] + last[1];
+    if (m == 0) return GS_OK;   // no cell to diffuse over: the surface stays
+    launch(p, k_lake_list, G, B, n, (const uint8_t*)lmask, (const int*)p->scanbuf, cell);
+    GS_LAUNCH();
+    launch(p, k_lake_submesh, grid_for(m, B), B, m, n, W, (const int*)cell, (const int*)p->scanbuf,
+           (const uint8_t*)lmask, (const int*)p->nbr, (const int8_t*)p->nnb, (const double*)p->farea, nbr_c, nnb_c,
+           farea_c, fix_c);
+    GS_LAUNCH();
+    const double dts = dt / p->lake_nsub;
+    for (int sub = 0; sub < p->lake_nsub; sub++) {
+        GS_CUDA(cudaMemcpyAsync(hstart, hcur, sizeof(double) * n, cudaMemcpyDeviceToDevice, p->stream));
+        for (int it = 0; it < p->lake_npic; it++) {
+            launch(p, k_lake_cd, G, B, n, (const uint8_t*)lmask, (const double*)hcur, zb, K, 0.05, 1.0e-4,
+                   cd);
+            launch(p, k_lake_rows_c, grid_for(m, B), B, m, n, W, (const int*)cell, (const int*)p->nbr,
+                   (const int8_t*)p->nnb, (const double*)p->elen, (const double*)p->vdist, (const double*)p->farea,
+                   (const double*)cd, dts, (const double*)hstart, p->sed_coef, rhs_c);
+            GS_LAUNCH();
+            GS_TRY(diffusion_solve_on(p, m, nbr_c, nnb_c, farea_c, fix_c, 0, nullptr, p->sed_coef, rhs_c, x_c,
+                                      1.0e-13, 5000, nullptr));
+            launch(p, k_lake_scatter, grid_for(m, B), B, m, (const int*)cell, (const double*)x_c, hcur);
+            GS_LAUNCH();
+        }
+    }
+    return GS_OK;
+}
+
 int sed_change(gs_plan* p, double* h, double* cum_ed, const double* eb, const double* xyz, double sealevel,
                double ofill, double dt, double nl_pit_volume, double nl_pit_depth, double* lfill, int* pit_ids,
-               int* flat_dirs, const int* rcv_i, const double* wgt_i, uint8_t* lsink, const uint8_t* sea,
+               int* flat_dirs, const int* rcv_i, const double* wgt_i, uint8_t* lsink, uint8_t* sea,
                double* vsed, gs_stats* st) {
     const int n = (int)p->n;
     if (n == 0) return GS_OK;
@@ -697,6 +760,7 @@ int sed_change(gs_plan* p, double* h, double* cum_ed, const double* eb, const do
         return true;
     };
     int step = 0, solves = 0;
+    bool rebuilt = false;
     while (any(act) && step < 5000) {
         GS_CUDA(cudaMemcpyAsync(p->mact, act.data(), nm, cudaMemcpyHostToDevice, p->stream));
         launch(p, k_sed_csink, G, B, n, (const uint8_t*)lsink, (const int*)pit_ids, (const uint8_t*)mout,
@@ -741,6 +805,7 @@ int sed_change(gs_plan* p, double* h, double* cum_ed, const double* eb, const do
                     GS_CUDA(cudaMemcpyAsync(p->mbig, rebuild.data(), nm, cudaMemcpyHostToDevice, p->stream));
                 }
                 const double* surf = (step == 100) ? lfill : sfill;
+                rebuilt = true;
                 GS_TRY(receivers(p, p->R, 1.1, surf, sealevel, p->gid, p->rcv, p->dist, p->wgt, p->rslot));
                 GS_TRY(flow_order_from(p, surf, hl, p->order_i, p->order));
                 GS_TRY(flow_order_ties_prepare(p));
@@ -781,6 +846,9 @@ int sed_change(gs_plan* p, double* h, double* cum_ed, const double* eb, const do
         step++;
     }
     GS_TRY(fill_join(p, st));
+    // a rebuild of the flow graph set goSPL's seaID (_buildFlowDirection,
+    // flowplex.py:494): the caller's live sea mask follows it
+    if (rebuilt) GS_CUDA(cudaMemcpyAsync(sea, sea_s, (size_t)n, cudaMemcpyDeviceToDevice, p->stream));
 
     // 4. deposits in the depressions
     if (!p->sed_pit) GS_CUDA(cudaMalloc((void**)&p->sed_pit, sizeof(double) * ((size_t)n + 1) * 2));
@@ -840,58 +908,7 @@ int sed_change(gs_plan* p, double* h, double* cum_ed, const double* eb, const do
                (const double*)wd, (const double*)p->pit_in, (const double*)pcnt, (const double*)pdepo,
                (const double*)p->larea, p->lake_bias, zb, hcur);
         GS_LAUNCH();
-        // the lake cells as a sub-mesh of m rows
-        const int W = p->W;
-        if (!p->lake_i) {
-            GS_CUDA(cudaMalloc((void**)&p->lake_i, sizeof(int) * (size_t)n * (size_t)(W + 1)));
-            GS_CUDA(cudaMalloc((void**)&p->lake_d, sizeof(double) * (size_t)n * 3));
-            GS_CUDA(cudaMalloc((void**)&p->lake_u8, (size_t)n * 2));
-        }
-        int* cell = p->lake_i;
-        int* nbr_c = cell + n;
-        double* farea_c = p->lake_d;
-        double* rhs_c = farea_c + n;
-        double* x_c = rhs_c + n;
-        int8_t* nnb_c = (int8_t*)p->lake_u8;
-        uint8_t* fix_c = p->lake_u8 + n;
-        launch(p, k_lake_flag, G, B, n, (const uint8_t*)lmask, p->flagbuf);
-        GS_LAUNCH();
-        {
-            size_t bytes = p->cub_bytes;
-            GS_CUDA(cub::DeviceScan::ExclusiveSum(p->cub_tmp, bytes, (const int*)p->flagbuf, p->scanbuf, n, p->stream));
-            p->launches++;
-        }
-        int last[2];
-        GS_CUDA(cudaMemcpyAsync(&last[0], p->scanbuf + n - 1, sizeof(int), cudaMemcpyDeviceToHost, p->stream));
-        GS_CUDA(cudaMemcpyAsync(&last[1], p->flagbuf + n - 1, sizeof(int), cudaMemcpyDeviceToHost, p->stream));
-        GS_CUDA(cudaStreamSynchronize(p->stream));
-        const int m = last[0] + last[1];
-        if (m == 0) {
-            set_error(GS_EINVAL, "sedChange: lake diffusion without lake cells");
-            return GS_EINVAL;
-        }
-        launch(p, k_lake_list, G, B, n, (const uint8_t*)lmask, (const int*)p->scanbuf, cell);
-        GS_LAUNCH();
-        launch(p, k_lake_submesh, grid_for(m, B), B, m, n, W, (const int*)cell, (const int*)p->scanbuf,
-               (const uint8_t*)lmask, (const int*)p->nbr, (const int8_t*)p->nnb, (const double*)p->farea, nbr_c, nnb_c,
-               farea_c, fix_c);
-        GS_LAUNCH();
-        const double dts = dt / p->lake_nsub;
-        for (int sub = 0; sub < p->lake_nsub; sub++) {
-            GS_CUDA(cudaMemcpyAsync(hstart, hcur, sizeof(double) * n, cudaMemcpyDeviceToDevice, p->stream));
-            for (int it = 0; it < p->lake_npic; it++) {
-                launch(p, k_lake_cd, G, B, n, (const uint8_t*)lmask, (const double*)hcur, zb, p->lake_K, 0.05, 1.0e-4,
-                       cd);
-                launch(p, k_lake_rows_c, grid_for(m, B), B, m, n, W, (const int*)cell, (const int*)p->nbr,
-                       (const int8_t*)p->nnb, (const double*)p->elen, (const double*)p->vdist, (const double*)p->farea,
-                       (const double*)cd, dts, (const double*)hstart, p->sed_coef, rhs_c);
-                GS_LAUNCH();
-                GS_TRY(diffusion_solve_on(p, m, nbr_c, nnb_c, farea_c, fix_c, 0, nullptr, p->sed_coef, rhs_c, x_c,
-                                          1.0e-13, 5000, nullptr));
-                launch(p, k_lake_scatter, grid_for(m, B), B, m, (const int*)cell, (const double*)x_c, hcur);
-                GS_LAUNCH();
-            }
-        }
+        GS_TRY(picard_diffuse(p, lmask, zb, hcur, p->lake_K, dt, cd, hstart));
         launch(p, k_lake_depo, G, B, n, (const uint8_t*)lmask, (const double*)hcur, zb, (const double*)p->larea, wd,
                wda);
         GS_LAUNCH();

@@ -7,7 +7,8 @@ uses, with goSPL's names, defaults and errors (gospl/tools/inputparser.py):
   ``.npz`` mesh, :263-266), ``flowdir`` (default 8, :189), ``bc`` (four of
   ``o f w c``, legacy ``0``/``1`` -> ``o``/``f``, :208-246), ``fast``, ``nodep``
   and ``seadepo`` (:289-300; continental deposition runs unless ``nodep``,
-  marine deposition is not implemented and must be switched off);
+  marine deposition when ``seadepo`` (default on), built for
+  ``marineSolver: picard`` and ``Gmar`` 0);
 * ``time``: ``start``, ``end``, ``dt`` required, ``tout`` (:343-404, clamped
   to [dt, end - start] as :413-429 does), ``rstep`` (restart, :411);
 * ``output``: ``dir`` (output), ``makedir`` (False), ``compression`` (gzip)
@@ -16,7 +17,8 @@ uses, with goSPL's names, defaults and errors (gospl/tools/inputparser.py):
 * ``diffusion``: ``hillslopeKa``, ``hillslopeKm``, ``oFill`` (-6000) (:498-545),
   ``nlPitVolume`` (1e9), ``nlPitDepth`` (100), ``nonlinKm``/``nlPitK`` (10),
   ``pitInletBias`` (0.10; 0.50 without the section), ``marineSolver`` (ts),
-  ``picardSub`` (10), ``picardIts`` (2) (:546-593);
+  ``picardSub`` (10), ``picardIts`` (2), ``clinSlp`` (1e-6, at least 1e-6),
+  ``Gmar`` (0), ``offshore`` (1e7 m) (:546-593);
 * ``sea``: ``position`` (default 0, :710-787);
 * ``climate``: events with ``start`` and ``uniform`` or ``map: [file, key]``
   (:1352-1520);
@@ -28,7 +30,8 @@ then relative to the YAML file.  Keys of other goSPL subsystems (sediment,
 stratigraphy, flexure, ice, orography) are ignored; options that would
 change this path's arithmetic and that the library does not implement
 (sea-level curves, time-varying climate or tectonic events, horizontal
-tectonics, marine deposition) raise ``ValueError``.
+tectonics, marine deposition with the TS solver or Gmar > 0) raise
+``ValueError``.
 """
 import os
 
@@ -89,9 +92,6 @@ def read_input(filename):
     p = {"flowDir": int(dom.get("flowdir", 8)), "bc": parse_bc(dom.get("bc", "oooo")),
          "fast": bool(dom.get("fast", False)), "nodep": bool(dom.get("nodep", False)),
          "seadepo": bool(dom.get("seadepo", True))}
-    if not p["nodep"] and p["seadepo"]:
-        raise ValueError("marine deposition (domain.seadepo, seaplex.py) is not implemented by gospl_b200; "
-                         "set domain.seadepo: False (continental deposition only) or domain.nodep: True")
 
     if "time" not in inp:
         raise KeyError("Key time is required in the input file!")
@@ -130,11 +130,20 @@ def read_input(filename):
         p["marineSolver"] = str(hill.get("marineSolver", "ts")).lower()
         p["picardSub"] = int(hill.get("picardSub", 10))
         p["picardIts"] = int(hill.get("picardIts", 2))
+        p["nonlinKm"] = float(hill.get("nonlinKm", 10.0))      # :554-558
+        p["clinSlp"] = max(1.0e-6, float(hill.get("clinSlp", 1.0e-6)))
+        p["Gmar"] = float(hill.get("Gmar", 0.0))
+        p["offshore"] = float(hill.get("offshore", 100.0e5))
     else:
         p["Cda"], p["Cdm"], p["oFill"] = 0.0, 0.0, -6000.0
         p["nlPitVolume"], p["nlPitDepth"] = 1.0e9, 100.0
         p["nlPitK"], p["pitInletBias"], p["marineSolver"] = 10.0, 0.50, "ts"
         p["picardSub"], p["picardIts"] = 10, 2
+        p["nonlinKm"], p["clinSlp"], p["Gmar"], p["offshore"] = 10.0, 1.0e-6, 0.0, 100.0e5
+
+    if not p["nodep"] and p["seadepo"] and (p["marineSolver"] != "picard" or p["Gmar"] > 0.0):
+        raise ValueError("marine deposition (domain.seadepo) is built for diffusion.marineSolver: picard and "
+                         "Gmar = 0; set them, or domain.seadepo: False (continental deposition only)")
 
     sea = inp.get("sea") or {}
     if "curve" in sea:

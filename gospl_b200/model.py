@@ -13,9 +13,11 @@
 * ``applyForces()``       — UnstMesh.applyForces (unstructuredmesh.py:743-794)
 * ``visModel()`` / ``readData()`` — WriteMesh (tools/outmesh.py): HDF5 and
   XDMF outputs every ``tout`` years and the restart from output ``rStep``
+* ``seaChange()``         — SEAMesh.seaChange (seaplex.py:738-861): marine
+  deposition (``seadepo``; Gmar = 0, marineSolver picard)
 * ``runProcesses()``      — the time loop of model.py:331-466 with
-  ``fast: false`` and continental deposition unless ``nodep`` (marine
-  deposition, ``seadepo``, is not built).
+  ``fast: false``, continental deposition unless ``nodep`` and marine
+  deposition when ``seadepo``.
 
 All state lives in torch CUDA tensors (float64 / int32 / uint8); every stage is
 one call through the C ABI of ``libgospl_b200.so``.  Per-receiver arrays are
@@ -100,13 +102,22 @@ class Model:
         self.sealevel = float(p.get("sealevel", 0.0))
         self.flatModel = bool(mesh.flat)
         self.nodep = bool(p.get("nodep", True))
-        if not self.nodep and bool(p.get("seadepo", False)):
-            raise NotImplementedError("marine deposition (seaChange, seadepo) is not built")
+        # marine deposition (seaChange) after the continental one; goSPL's
+        # default is on (inputparser.py:289), built for Gmar = 0 and the
+        # Picard marine solver
+        self.seadepo = (not self.nodep) and bool(p.get("seadepo", False))
+        self.nlK = float(p.get("nonlinKm", 10.0))                   # inputparser.py:554
+        self.clinSlp = max(1.0e-6, float(p.get("clinSlp", 1.0e-6)))   # :555, 592
+        self.Gmar = float(p.get("Gmar", 0.0))                      # :557
+        self.offshore = float(p.get("offshore", 100.0e5))          # :558
         self.nl_pit_volume = float(p.get("nlPitVolume", 1.0e9))    # inputparser.py:562,584
         self.nl_pit_depth = float(p.get("nlPitDepth", 100.0))      # inputparser.py:563,585
         # lake deposits of large deep depressions: marineSolver picard
         # (inputparser.py:564-580); goSPL's default adaptive TS is not built
         self.marineSolver = str(p.get("marineSolver", "ts")).lower()
+        if self.seadepo and (self.marineSolver != "picard" or self.Gmar > 0.0):
+            raise NotImplementedError("marine deposition is built for marineSolver picard and Gmar = 0 (goSPL's "
+                                      "adaptive TS solve and the coupled Gmar > 0 system are not)")
         self.nl_pit_K = float(p.get("nlPitK", p.get("nonlinKm", 10.0)))
         self.nl_pit_inlet_bias = min(1.0, max(0.0, float(p.get("pitInletBias", 0.5))))
         self.picardSub = int(p.get("picardSub", 10))
@@ -157,6 +168,17 @@ class Model:
             c = np.asarray(coords, np.float64)
             xyz[:, :c.shape[1]] = c
             self.xyz = torch.as_tensor(xyz, **f64)
+        self.edges = None
+        if self.seadepo:
+            # the mesh's unique edges for the coastline contour, and the
+            # vertices' bounding box (lo, span)
+            cl = np.asarray(cells, np.int64)
+            e = np.sort(np.concatenate([cl[:, [0, 1]], cl[:, [1, 2]], cl[:, [2, 0]]]), axis=1)
+            e = np.unique(e, axis=0)
+            self.edges = torch.as_tensor(np.ascontiguousarray(e, np.int32), device=self.dev)
+            lo = xyz.min(axis=0)
+            span = np.maximum(xyz.max(axis=0) - lo, 1.0)
+            self.xyz_box = np.ascontiguousarray(np.concatenate([lo, span]), np.float64)
 
         handle = ctypes.c_void_p()
         outlet = np.ascontiguousarray(mesh.outlet, np.int32)
@@ -335,6 +357,23 @@ class Model:
         self.npits = st.npits
         self.stats["sed"] = st.as_dict()
 
+    def seaChange(self):
+        """SEAMesh.seaChange (seaplex.py:738-861): the sediment flux that
+        reached the sea after sedChange is spread down the marine receivers
+        within the clinoform capacity and smoothed by the Picard diffusion
+        over the sea cells (gs_sea_change)."""
+        if self.edges is None:
+            raise RuntimeError("seaChange needs a Model built with nodep=False and seadepo=True")
+        L = _lib_handle()
+        st = _lib.GsStats()
+        _lib.check(L.gs_sea_change(
+            self._plan, _lib.ptr(self.hGlobal), _lib.ptr(self.cumED), _lib.ptr(self.EbLocal), _lib.ptr(self.xyz),
+            self.xyz_box.ctypes.data_as(ctypes.c_void_p), _lib.ptr(self.edges), int(self.edges.shape[0]),
+            self.sealevel, self.oFill, self.dt, self.clinSlp, self.offshore, self.nlK, _lib.ptr(self.lFill),
+            _lib.ptr(self.vSed), _lib.ptr(self.sea_mask), ctypes.byref(st)))
+        self.stats["sea"] = {"coast_points": st.npits, "marine_passes": st.cascade_passes,
+                             "epsfill_passes": st.fill_rounds}
+
     def sed_budget(self):
         """Sediment budget of the last sedChange (m3 over the step): where
         the volume eroded by the step's SPL went in the continental routing
@@ -369,6 +408,8 @@ class Model:
         if not self.nodep:
             self.flowAccumulation()
             self.sedChange()
+            if self.seadepo:
+                self.seaChange()
         self.getHillslope()
         if self.tNow < self.tEnd:
             self.applyForces()

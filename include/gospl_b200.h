@@ -246,7 +246,10 @@ int gs_erodep_spl(gs_plan* plan, double* h, double* cum_ed, double* eb, const do
  * GS_EINVAL when it is off (stats.status = their count).
  * Ensemble members (gs_plan_set_members) each run their own cascade, with
  * closed-domain deposits for members without an outlet.  stats: npits,
- * cascade passes and solves.
+ * cascade passes and solves.  `sea` is goSPL's live seaID: read for the
+ * sinks of the snapshot graph, and overwritten (lFill <= sealevel of the
+ * sediment fill) when the cascade rebuilds the flow graph, as
+ * _buildFlowDirection does (flowplex.py:494).
  */
 /*
  * Lake deposits of large deep depressions (gs_sed_change path 3): goSPL's
@@ -263,7 +266,7 @@ int gs_plan_set_lake_diffusion(gs_plan* plan, double k, double inlet_bias, int32
 int gs_sed_change(gs_plan* plan, double* h, double* cum_ed, const double* eb, const double* xyz,
                   double sealevel, double ofill, double dt, double nl_pit_volume, double nl_pit_depth,
                   double* lfill, int32_t* pit_ids, int32_t* flat_dirs, const int32_t* rcv_i,
-                  const double* wgt_i, uint8_t* lsink, const uint8_t* sea, double* vsed,
+                  const double* wgt_i, uint8_t* lsink, uint8_t* sea, double* vsed,
                   gs_stats* stats);
 
 /*
@@ -302,6 +305,31 @@ int gs_sed_change(gs_plan* plan, double* h, double* cum_ed, const double* eb, co
 #define GS_LED_REALISED 12   /* sum(larea * (h_after - h_before)) of sedChange     */
 #define GS_LED_KEPT_DEP 13   /* sum of the closed-domain deposit volumes           */
 int gs_sed_budget(gs_plan* plan, double* out16);
+
+/*
+ * Marine deposition.  Replaces SEAMesh.seaChange (gospl/sed/seaplex.py:738-861)
+ * for one lithology, no stratigraphy or provenance, Gmar = 0 and marineSolver
+ * picard (the plan's lake-diffusion settings, gs_plan_set_lake_diffusion,
+ * give picardSub and picardIts; nlk is nonlinKm): distance of the sea
+ * vertices to the sea-level contour of h (_distanceCoasts, 51-135),
+ * clinoform capacity from clinslp, the sediment reaching the sea (vsed * dt
+ * where the sediment fill lfill <= sealevel), marine receivers on the
+ * epsilon-filled routing surface (_matOcean, 137-238: bathymetry smoothed by
+ * one implicit diffusion step on spheres, cells farther than `offshore` or
+ * planar outlets at the boundary sentinel; epsfill and mfdrcvrs,
+ * functions.F90:2633-2697 and 1673-1785), the capacity-limited cascade
+ * (_distOcean, 404-619) and the Picard diffusion of the deposit over the sea
+ * cells (_diffuseOcean, hillslope.py:739-787); h, cum_ed and eb are updated.
+ * `sea` is goSPL's seaID at this point (lFill <= sealevel of the last flow
+ * direction built), `edges` the mesh's unique edges [nedge][2] (DEVICE),
+ * `box` (HOST, 6 doubles) the vertices' bounding box as (lo, span).  stats:
+ * npits = coastline points, cascade_passes = marine passes, fill_rounds =
+ * epsfill relaxation passes.
+ */
+int gs_sea_change(gs_plan* plan, double* h, double* cum_ed, double* eb, const double* xyz, const double* box,
+                  const int32_t* edges, int64_t nedge, double sealevel, double ofill, double dt, double clinslp,
+                  double offshore, double nlk, const double* lfill, const double* vsed, const uint8_t* sea,
+                  gs_stats* stats);
 
 int gs_hillslope(gs_plan* plan, double* h, double* cum_ed, double* eb, double sealevel,
                  double cda, double cdm, double dt, double rtol, int32_t max_iter,
