@@ -513,13 +513,23 @@ int sea_change(gs_plan* p, double* h, double* cum_ed, double* eb, const double* 
     if (!p->sea_buf) GS_CUDA(cudaMalloc((void**)&p->sea_buf, sizeof(double) * N * 12));
     if (!p->sea_u8) GS_CUDA(cudaMalloc((void**)&p->sea_u8, N * 4));
     if (!p->sea_coef) GS_CUDA(cudaMalloc((void**)&p->sea_coef, sizeof(double) * N * (size_t)(p->W + 1)));
+    // coastline buffers, in doubles: raw and sorted points [3 cap] each, keys
+    // [2 cap], ids [2 cap] int32 (= cap), leaf boxes [6 (cap/LEAF + 1)],
+    // super boxes [6 (cap/(LEAF SUPER) + 1)], then the sort's scratch
+    auto pts_doubles = [](size_t cap) {
+        return 3 * cap + 3 * cap + 2 * cap + cap + 6 * (cap / LEAF + 1) + 6 * (cap / (LEAF * SUPER) + 1) + 8;
+    };
     if (p->sea_pts_cap < nedge) {
         if (p->sea_pts) cudaFree(p->sea_pts);
         p->sea_pts = nullptr;
+        p->sea_pts_cap = 0;
         const size_t cap = (size_t)std::max<int64_t>(nedge, 1);
-        // raw points [3 cap], sorted [3 cap], keys and ids [2 cap] each,
-        // leaf and super boxes [6 cap]
-        GS_CUDA(cudaMalloc((void**)&p->sea_pts, sizeof(double) * cap * 16));
+        size_t sb = 0;
+        GS_CUDA(cub::DeviceRadixSort::SortPairs((void*)nullptr, sb, (const unsigned long long*)nullptr,
+                                                (unsigned long long*)nullptr, (const int*)nullptr, (int*)nullptr,
+                                                (int)cap, 0, 63, p->stream));
+        p->sea_sort_bytes = (sb + 255) & ~(size_t)255;
+        GS_CUDA(cudaMalloc((void**)&p->sea_pts, sizeof(double) * pts_doubles(cap) + p->sea_sort_bytes));
         p->sea_pts_cap = nedge;
     }
     double* cdist = p->sea_buf;
@@ -546,6 +556,7 @@ int sea_change(gs_plan* p, double* h, double* cum_ed, double* eb, const double* 
     int* idx2 = idx + cap;
     double* lbox = (double*)(idx2 + cap);
     double* sbox = lbox + 6 * (cap / LEAF + 1);
+    void* sort_tmp = (void*)(p->sea_pts + pts_doubles(cap));
     double* dbox = p->d_scalar + 8;   // [6] mesh box (lo, span)
     int* icnt = p->i_scalar + 10;
     GS_CUDA(cudaMemcpyAsync(hl, h, sizeof(double) * N, cudaMemcpyDeviceToDevice, p->stream));
@@ -566,12 +577,12 @@ int sea_change(gs_plan* p, double* h, double* cum_ed, double* eb, const double* 
         GS_LAUNCH();
         size_t bytes = 0;
         GS_CUDA(cub::DeviceRadixSort::SortPairs((void*)nullptr, bytes, key, key2, idx, idx2, m, 0, 63, p->stream));
-        if (bytes > p->cub_bytes) {
-            set_error(GS_ENOMEM, "seaChange: more coastline points than the sort scratch holds");
+        if (bytes > p->sea_sort_bytes || (size_t)m > cap) {
+            set_error(GS_ENOMEM, "seaChange: more coastline points than the coastline buffers hold");
             return GS_ENOMEM;
         }
-        bytes = p->cub_bytes;
-        GS_CUDA(cub::DeviceRadixSort::SortPairs(p->cub_tmp, bytes, key, key2, idx, idx2, m, 0, 63, p->stream));
+        bytes = p->sea_sort_bytes;
+        GS_CUDA(cub::DeviceRadixSort::SortPairs(sort_tmp, bytes, key, key2, idx, idx2, m, 0, 63, p->stream));
         p->launches++;
         launch(p, k_coast_gather, grid_for(m, B), B, m, (const int*)idx2, (const double*)raw, spts);
         nleaf = (m + LEAF - 1) / LEAF;
