@@ -19,8 +19,6 @@ struct gs_plan {
     int coop_max_per_sm = 1;             // occupancy limit of the cooperative kernels
     int sweep_per_sm = 8;                // 128-thread blocks per SM of the ordered sweeps
     unsigned sweep_nap = 128;            // longest back-off (ns) between polls of the ordered sweeps
-    int sweep_tiles = 1;                 // ordered sweeps by tiles in shared memory when they fit
-    int* tord = nullptr;                 // [3][n] tile-major order of the tiled sweeps and its sort keys
     unsigned long long sweep_budget_ns = 4000000000ULL;   // wall-clock budget of one dependency sweep
     int bfs_window = 0;                  // flat-distance BFS: 0 one block, w > 0 tiles, windows of w levels
     // precision form: FP32 sweeps and CG inside FP64 refinement loops

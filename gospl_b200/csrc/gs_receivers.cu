@@ -111,7 +111,7 @@ __device__ __noinline__ void mfd_vertex_general(int k, int n, int R, double expo
             else val = fexp_int ? pow(d, fexp) / L : -1.0;   // non-integer power of a
                                                              // negative base is NaN: no receiver
             if (val > 0.0) {
-                slp[kk] = val * (1.0 - 1.0e-15 * (double)gid[nb]);
+                slp[kk] = val * (1.0 - 1.0e-15 * (double)(gid ? gid[nb] : nb));
                 cid[kk] = nb;
                 cs[kk] = s;
                 dst[kk] = L;
@@ -177,13 +177,18 @@ __global__ void k_mfd_receivers(int n, int W, int R, double expo, const double* 
     if (k < n) mfd_vertex_general(k, n, R, expo, elev, sl, gid, nbr, elen, nnb, rcv, dist, wgt, rslot);
 }
 
-// Register form for R = RM <= 4 (the configurations' flowDir is 3): the
-// neighbour ids, edge lengths and candidate slopes of the <= 12 slots stay in
-// registers (every loop over slots is unrolled), the RM + 1 steepest
-// candidates are kept by insertion, and every output slot is written once.
-// Without exact ties among those RM + 1 the descending order is the one the
-// reference quicksort leaves, so the result is bit-identical to the general
-// form; a vertex with such a tie goes to mfd_vertex_general (literal replay).
+// Register form for R = RM <= 4 (the configurations' flowDir is 3), in two
+// passes over the neighbour slots so that no per-slot array is held: the
+// first finds the steepest gradient (the exponent), the second forms every
+// candidate slope, sums them in slot order and keeps the RM + 1 steepest by
+// insertion.  The second pass re-reads the slot's id, edge length and the
+// neighbour's elevation (L1/L2 hits) instead of keeping 12 of each in
+// registers, which keeps the kernel near 64 registers and the SMs full of
+// warps for the gathers.  Without exact ties among the kept candidates the
+// descending order is the one the reference quicksort leaves, so the result
+// is bit-identical to the general form; a vertex whose new candidate equals a
+// kept one goes to mfd_vertex_general (literal replay).  gid == nullptr means
+// the identity numbering (one partition).
 template <int RM>
 __global__ void __launch_bounds__(128) k_mfd_receivers_r(int n, double expo, const double* __restrict__ elev,
                                                           double sl, const int* __restrict__ gid,
@@ -205,25 +210,13 @@ __global__ void __launch_bounds__(128) k_mfd_receivers_r(int n, double expo, con
         return;
     }
     const int deg = nnb[k];
-    int nb[MAXW];
-    double L[MAXW], v[MAXW];
     double e = 0.0;
-#pragma unroll
-    for (int s = 0; s < MAXW; s++) {
-        nb[s] = -1;
-        L[s] = 0.0;
-        v[s] = 0.0;
-        if (s < deg) {
-            const int c = nbr[(size_t)s * n + k];
-            const double l = elen[(size_t)s * n + k];
-            if (c >= 0 && l > 0.0) {
-                nb[s] = c;
-                L[s] = l;
-                const double d = hk - elev[c];
-                v[s] = d;
-                const double g = d / l;
-                e = (g > e) ? g : e;
-            }
+    for (int s = 0; s < deg; s++) {
+        const int c = nbr[(size_t)s * n + k];
+        const double l = elen[(size_t)s * n + k];
+        if (c >= 0 && l > 0.0) {
+            const double g = (hk - elev[c]) / l;
+            e = (g > e) ? g : e;
         }
     }
     double fexp;
@@ -234,53 +227,8 @@ __global__ void __launch_bounds__(128) k_mfd_receivers_r(int n, double expo, con
         fexp = 1.0;
     }
     const bool fexp_int = (fexp == floor(fexp));
-    // candidate slopes (0 = not a candidate), in slot order
-    int kk = 0;
-#pragma unroll
-    for (int s = 0; s < MAXW; s++) {
-        if (nb[s] >= 0) {
-            const double d = v[s];
-            double val;
-            if (d > 0.0) val = pow(d, fexp) / L[s];
-            else if (d == 0.0) val = 0.0;
-            else val = fexp_int ? pow(d, fexp) / L[s] : -1.0;
-            if (val > 0.0) {
-                v[s] = val * (1.0 - 1.0e-15 * (double)gid[nb[s]]);
-                kk++;
-            } else {
-                v[s] = 0.0;
-            }
-        } else {
-            v[s] = 0.0;
-        }
-    }
-    if (kk <= RM) {
-        // receivers in slot order, weights over the candidates' sum
-        double tot = 0.0;
-#pragma unroll
-        for (int s = 0; s < MAXW; s++)
-            if (v[s] > 0.0) tot = tot + v[s];
-        int o = 0;
-#pragma unroll
-        for (int s = 0; s < MAXW; s++) {
-            if (v[s] > 0.0) {
-                rcv[(size_t)o * n + k] = nb[s];
-                dist[(size_t)o * n + k] = L[s];
-                wgt[(size_t)o * n + k] = v[s] / tot;
-                if (rslot) rslot[(size_t)o * n + k] = (int8_t)s;
-                o++;
-            }
-        }
-        for (; o < RM; o++) {
-            rcv[(size_t)o * n + k] = k;
-            dist[(size_t)o * n + k] = 0.0;
-            wgt[(size_t)o * n + k] = 0.0;
-            if (rslot) rslot[(size_t)o * n + k] = -1;
-        }
-        return;
-    }
-    // the RM + 1 steepest candidates, descending (strict >: the earlier slot
-    // stays ahead of an equal one, and equal values are sent to the replay)
+    // candidates: slope (scaled by the global-id tie-break), kept descending;
+    // strict > keeps the earlier slot ahead of an equal value
     double tv[RM + 1];
     int ts[RM + 1], tid[RM + 1];
 #pragma unroll
@@ -289,58 +237,80 @@ __global__ void __launch_bounds__(128) k_mfd_receivers_r(int n, double expo, con
         ts[j] = -1;
         tid[j] = -1;
     }
+    unsigned mask = 0u;
+    int kk = 0;
+    double tot_all = 0.0;
+    bool tie = false;
+    for (int s = 0; s < deg; s++) {
+        const int c = nbr[(size_t)s * n + k];
+        const double l = elen[(size_t)s * n + k];
+        if (c < 0 || !(l > 0.0)) continue;
+        const double d = hk - elev[c];
+        double val;
+        if (d > 0.0) val = pow(d, fexp) / l;
+        else if (d == 0.0) val = 0.0;
+        else val = fexp_int ? pow(d, fexp) / l : -1.0;   // non-integer power of a negative base is NaN
+        if (!(val > 0.0)) continue;
+        double x = val * (1.0 - 1.0e-15 * (double)(gid ? gid[c] : c));
+        mask |= 1u << s;
+        kk++;
+        tot_all = tot_all + x;
+        int xs = s, xi = c;
 #pragma unroll
-    for (int s = 0; s < MAXW; s++) {
-        if (v[s] > 0.0) {
-            double x = v[s];
-            int xs = s, xi = nb[s];
+        for (int j = 0; j <= RM; j++) tie |= (x == tv[j]);
 #pragma unroll
-            for (int j = 0; j <= RM; j++) {
-                if (x > tv[j]) {
-                    const double t = tv[j];
-                    const int a = ts[j], b = tid[j];
-                    tv[j] = x;
-                    ts[j] = xs;
-                    tid[j] = xi;
-                    x = t;
-                    xs = a;
-                    xi = b;
-                }
+        for (int j = 0; j <= RM; j++) {
+            if (x > tv[j]) {
+                const double t = tv[j];
+                const int a = ts[j], b = tid[j];
+                tv[j] = x;
+                ts[j] = xs;
+                tid[j] = xi;
+                x = t;
+                xs = a;
+                xi = b;
             }
         }
     }
-    bool tie = false;
+    if (kk <= RM) {
+        // every candidate is kept: receivers in slot order, weights over the
+        // sum of all candidates taken in slot order
 #pragma unroll
-    for (int s = 0; s < MAXW; s++) {
+        for (int j = 0; j < RM; j++) {
+            if (j < kk) {
+                int o = 0;
 #pragma unroll
-        for (int j = 0; j <= RM; j++) tie |= (v[s] > 0.0) && (v[s] == tv[j]) && (s != ts[j]);
+                for (int i = 0; i < RM; i++) o += (i < kk && ts[i] < ts[j]) ? 1 : 0;
+                rcv[(size_t)o * n + k] = tid[j];
+                dist[(size_t)o * n + k] = elen[(size_t)ts[j] * n + k];
+                wgt[(size_t)o * n + k] = tv[j] / tot_all;
+                if (rslot) rslot[(size_t)o * n + k] = (int8_t)ts[j];
+            } else {
+                rcv[(size_t)j * n + k] = k;
+                dist[(size_t)j * n + k] = 0.0;
+                wgt[(size_t)j * n + k] = 0.0;
+                if (rslot) rslot[(size_t)j * n + k] = -1;
+            }
+        }
+        return;
     }
     if (tie) {
         mfd_vertex_general(k, n, RM, expo, elev, sl, gid, nbr, elen, nnb, rcv, dist, wgt, rslot);
         return;
     }
     // reference quirk: receiver o takes the edge length of candidate kk-1-o
-    // in slot order (the sort permutes slopes and ids, not distances)
-    double dsel[RM];
-#pragma unroll
-    for (int o = 0; o < RM; o++) dsel[o] = 0.0;
-    int c = 0;
-#pragma unroll
-    for (int s = 0; s < MAXW; s++) {
-        if (v[s] > 0.0) {
-#pragma unroll
-            for (int o = 0; o < RM; o++)
-                if (c == kk - 1 - o) dsel[o] = L[s];
-            c++;
-        }
-    }
+    // in slot order (the sort permutes slopes and ids, not distances), i.e.
+    // of the (o+1)-th highest candidate slot
     double tot = 0.0;
 #pragma unroll
     for (int o = 0; o < RM; o++) tot = tot + tv[o];
+    unsigned m = mask;
 #pragma unroll
     for (int o = 0; o < RM; o++) {
+        const int hs = 31 - __clz(m);
+        m &= ~(1u << hs);
         rcv[(size_t)o * n + k] = tid[o];
-        dist[(size_t)o * n + k] = dsel[o];
+        dist[(size_t)o * n + k] = elen[(size_t)hs * n + k];
         wgt[(size_t)o * n + k] = tv[o] / tot;
         if (rslot) rslot[(size_t)o * n + k] = (int8_t)ts[o];
     }
@@ -424,7 +394,7 @@ int receivers(gs_plan* p, int nrcv, double exp, const double* elev, double sl, c
         return GS_EINVAL;
     }
     if (p->n == 0) return GS_OK;
-    const int* g = gid ? gid : p->gid;
+    const int* g = gid == p->gid ? nullptr : gid;   // the plan's own numbering is the identity
     const int G = grid_for(p->n, 128), n = (int)p->n;
     switch (nrcv) {
         case 1: launch(p, k_mfd_receivers_r<1>, G, 128, n, exp, elev, sl, g, p->nbr, p->elen, p->nnb, rcv, dist, wgt, rslot); break;
