@@ -388,9 +388,14 @@ __global__ void k_ocean_step(int n, int flat, const int* __restrict__ nbr, const
                              const int8_t* __restrict__ rev, const unsigned long long* __restrict__ sorder,
                              const unsigned short* __restrict__ cand, const double* __restrict__ w,
                              const uint8_t* __restrict__ sink, const uint8_t* __restrict__ outlet,
-                             const double* __restrict__ tmp, double* out, double* marvol, double* vdep) {
+                             const double* __restrict__ tmp, double* out, double* marvol, double* vdep,
+                             const int* __restrict__ stop) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
+    if (*stop) {             // the loop has ended: keep the volumes in transit
+        out[i] = tmp[i];
+        return;
+    }
     const unsigned long long so = sorder[i];
     double s = 0.0;
     for (int q = 0; q < nnb[i]; q++) {
@@ -458,8 +463,10 @@ __global__ void k_marine_apply(int n, const double* __restrict__ hcur, const dou
 // fixed-order sum over LED-like blocks: part[b] for 296 blocks, then one block
 constexpr int SUM_NB = 296;
 
-__global__ void __launch_bounds__(256) k_ocean_sum(int n, const double* __restrict__ x, double* part) {
+__global__ void __launch_bounds__(256) k_ocean_sum(int n, const double* __restrict__ x, double* part,
+                                                   const int* __restrict__ stop) {
     __shared__ double sh[8];
+    if (stop && *stop) return;
     double v = 0.0;
     for (int i = blockIdx.x * 256 + threadIdx.x; i < n; i += SUM_NB * 256) v += x[i];
     v = warp_sum(v);
@@ -472,8 +479,13 @@ __global__ void __launch_bounds__(256) k_ocean_sum(int n, const double* __restri
     }
 }
 
-__global__ void __launch_bounds__(256) k_ocean_sum_final(const double* __restrict__ part, double* out) {
+// the volume in transit after a pass; with `stop`, also the loop control of
+// _distOcean (seaplex.py:542-610): one more pass counted, and the loop ends
+// once the volume is at most the threshold or 5000 passes have run
+__global__ void __launch_bounds__(256) k_ocean_sum_final(const double* __restrict__ part, double* out, int* stop,
+                                                         int* passes, const double* __restrict__ threshold) {
     __shared__ double sh[8];
+    if (stop && *stop) return;
     double v = 0.0;
     for (int b = threadIdx.x; b < SUM_NB; b += 256) v += part[b];
     v = warp_sum(v);
@@ -483,14 +495,20 @@ __global__ void __launch_bounds__(256) k_ocean_sum_final(const double* __restric
         double t = 0.0;
         for (int k = 0; k < 8; k++) t += sh[k];
         *out = t;
+        if (stop) {
+            const int ps = *passes + 1;
+            *passes = ps;
+            if (!(t > *threshold) || ps >= 5000) *stop = 1;
+        }
     }
 }
 
 }  // namespace
 
 static int ocean_sum(gs_plan* p, const double* x, double* dev_out, double* host_out) {
-    launch(p, k_ocean_sum, SUM_NB, 256, (int)p->n, x, p->red);
-    launch(p, k_ocean_sum_final, 1, 256, (const double*)p->red, dev_out);
+    launch(p, k_ocean_sum, SUM_NB, 256, (int)p->n, x, p->red, (const int*)nullptr);
+    launch(p, k_ocean_sum_final, 1, 256, (const double*)p->red, dev_out, (int*)nullptr, (int*)nullptr,
+           (const double*)nullptr);
     GS_LAUNCH();
     GS_CUDA(cudaMemcpyAsync(host_out, dev_out, sizeof(double), cudaMemcpyDeviceToHost, p->stream));
     GS_CUDA(cudaStreamSynchronize(p->stream));
@@ -652,19 +670,36 @@ int sea_change(gs_plan* p, double* h, double* cum_ed, double* eb, const double* 
     double sum = 0.0;
     GS_TRY(ocean_sum(p, tmpa, sres, &sum));
     const double threshold = std::max(1.0, 1.0e-6 * sum);
+    // the loop control lives on the device (stop flag, pass count): passes
+    // are queued eight at a time and those after the stop only carry the
+    // volumes over, so the host synchronises once per eight passes
+    int* stop = p->i_scalar + 10;
+    int* dpass = p->i_scalar + 11;
+    double* dthr = p->d_scalar + 7;
+    {
+        const int h[2] = {(sum > threshold) ? 0 : 1, 0};
+        GS_CUDA(cudaMemcpyAsync(stop, h, sizeof(int) * 2, cudaMemcpyHostToDevice, p->stream));
+        GS_CUDA(cudaMemcpyAsync(dthr, &threshold, sizeof(double), cudaMemcpyHostToDevice, p->stream));
+    }
     int step = 0;
     double* cur = tmpa;
     double* nxt = tmpb;
-    while (sum > threshold && step < 5000) {
-        launch(p, k_ocean_step, G, B, n, p->flat, (const int*)p->nbr, (const int8_t*)p->nnb,
-               (const int8_t*)p->rev, (const unsigned long long*)p->sorder, (const unsigned short*)cand,
-               (const double*)wgt, (const uint8_t*)sink, (const uint8_t*)p->outlet, (const double*)cur, nxt, marvol,
-               vdep);
+    int hs[2] = {(sum > threshold) ? 0 : 1, 0};
+    while (!hs[0]) {
+        for (int q = 0; q < 8; q++) {
+            launch(p, k_ocean_step, G, B, n, p->flat, (const int*)p->nbr, (const int8_t*)p->nnb,
+                   (const int8_t*)p->rev, (const unsigned long long*)p->sorder, (const unsigned short*)cand,
+                   (const double*)wgt, (const uint8_t*)sink, (const uint8_t*)p->outlet, (const double*)cur, nxt,
+                   marvol, vdep, (const int*)stop);
+            launch(p, k_ocean_sum, SUM_NB, 256, n, (const double*)nxt, p->red, (const int*)stop);
+            launch(p, k_ocean_sum_final, 1, 256, (const double*)p->red, sres, stop, dpass, (const double*)dthr);
+            std::swap(cur, nxt);
+        }
         GS_LAUNCH();
-        std::swap(cur, nxt);
-        GS_TRY(ocean_sum(p, cur, sres, &sum));
-        step++;
+        GS_CUDA(cudaMemcpyAsync(hs, stop, sizeof(int) * 2, cudaMemcpyDeviceToHost, p->stream));
+        GS_CUDA(cudaStreamSynchronize(p->stream));
     }
+    step = hs[1];
     // what is still in transit stays where it is
     launch(p, k_ocean_rest, G, B, n, p->flat, (const uint8_t*)p->outlet, (const double*)cur, vdep);
     GS_LAUNCH();
