@@ -308,7 +308,9 @@ int flow_accumulation(gs_plan* p, const double* h, const double* bl, double seal
     const int ok_i = *bad_a ? 0 : 1;
     p->order_i_valid = ok_i;
     int cyc = 0;
-    GS_TRY(flow_run(p, rcv_i, wgt_i, p->rslot_i, p->nfa, fal, &cyc, p->order_i, ok_i));
+    // the sweep's status is read at the next synchronisation (the lakes flag)
+    int* sweep_st = p->h_pinned + 10;
+    GS_TRY(flow_run(p, rcv_i, wgt_i, p->rslot_i, p->nfa, fal, &cyc, p->order_i, ok_i, sweep_st));
     GS_TRY(rec_initial(p, h, rcv_i, wgt_i, dist_i, p->rslot_i, p->order_i, ok_i, fal, sea));
     int total_cycles = cyc;
     launch(p, k_copy, G, B, (int64_t)n, h, p->wf);
@@ -324,6 +326,10 @@ int flow_accumulation(gs_plan* p, const double* h, const double* bl, double seal
     std::vector<uint8_t> lakes(nm, 0);
     GS_CUDA(cudaMemcpyAsync(lakes.data(), p->mlakes, nm, cudaMemcpyDeviceToHost, p->stream));
     GS_CUDA(cudaStreamSynchronize(p->stream));
+    if (*sweep_st != 0) {
+        set_error(*sweep_st, "ordered flow sweep did not complete");
+        return *sweep_st;
+    }
     bool anyvol = false;
     for (int m = 0; m < nm; m++) anyvol = anyvol || lakes[m];
     int passes = 0, solves = 0;
@@ -425,7 +431,7 @@ int flow_accumulation(gs_plan* p, const double* h, const double* bl, double seal
                     GS_TRY(flow_prepare(p, p->rcv, p->wgt, p->rslot, p->q, p->order, p->h_pinned));
                     GS_CUDA(cudaStreamSynchronize(p->stream));
                     const int ok_c = p->h_pinned[0] ? 0 : 1;
-                    GS_TRY(flow_run(p, p->rcv, p->wgt, p->rslot, p->q2, p->q, &cyc, p->order, ok_c));
+                    GS_TRY(flow_run(p, p->rcv, p->wgt, p->rslot, p->q2, p->q, &cyc, p->order, ok_c, nullptr));
                     GS_TRY(rec_pass_solve(p, step, p->order, ok_c, p->q));
                     total_cycles += cyc;
                     launch(p, k_cascade_accum, G, B, n, (const double*)p->q, dt, h, (const double*)p->wf,

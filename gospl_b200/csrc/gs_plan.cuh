@@ -18,7 +18,7 @@ struct gs_plan {
     int coop_blocks = 148;               // co-resident 256-thread blocks for cooperative launches
     int coop_max_per_sm = 1;             // occupancy limit of the cooperative kernels
     int sweep_per_sm = 8;                // 128-thread blocks per SM of the ordered sweeps
-    unsigned sweep_nap = 128;            // longest back-off (ns) between polls of the ordered sweeps
+    unsigned sweep_nap = 32;             // longest back-off (ns) between polls of the ordered sweeps
     unsigned long long sweep_budget_ns = 4000000000ULL;   // wall-clock budget of one dependency sweep
     int bfs_window = 0;                  // flat-distance BFS: 0 one block, w > 0 tiles, windows of w levels
     // precision form: FP32 sweeps and CG inside FP64 refinement loops
@@ -291,8 +291,11 @@ int flow_order_ties_prepare(gs_plan* p);   // after flow_order: tie groups of th
 int flow_order_ties(gs_plan* p, const int* pdir, int* order);   // after prepare: ties by pdir
 int flow_prepare(gs_plan* p, const int* rcv, const double* wgt, const int8_t* rslot, double* x, const int* order,
                  int* bad_host);
+// status_host (pinned): when given, the ordered sweep's status is copied
+// there asynchronously and the caller checks it after its next
+// synchronisation of the plan's stream; otherwise flow_run synchronises
 int flow_run(gs_plan* p, const int* rcv, const double* wgt, const int8_t* rslot, const double* b,
-             double* x, int* cycle_nodes, int* order, int ok);
+             double* x, int* cycle_nodes, int* order, int ok, int* status_host);
 int group_sum_by_pit(gs_plan* p, const int* pit_ids, const uint8_t* mask, const double* vals,
                      double* out, int npits);
 int flow_accumulation(gs_plan* p, const double* h, const double* bl, double sealevel, double ofill,

@@ -727,7 +727,7 @@ int sed_change(gs_plan* p, double* h, double* cum_ed, const double* eb, const do
     launch(p, k_sed_rhs, G, B, n, eb, (const double*)p->larea, p->q2);
     GS_LAUNCH();
     GS_TRY(flow_prepare(p, rcv_i, wgt_i, p->rslot_i, vsed, p->order_i, p->h_pinned + 3));
-    GS_TRY(flow_run(p, rcv_i, wgt_i, p->rslot_i, p->q2, vsed, &cyc, p->order_i, p->order_i_valid));
+    GS_TRY(flow_run(p, rcv_i, wgt_i, p->rslot_i, p->q2, vsed, &cyc, p->order_i, p->order_i_valid, nullptr));
     total_cycles += cyc;
     // lsinki: sinks of the snapshot graph (flowplex.py:785-791)
     GS_TRY(sink_mask(p, wgt_i, sea, lsink));
@@ -832,7 +832,7 @@ int sed_change(gs_plan* p, double* h, double* cum_ed, const double* eb, const do
                 GS_TRY(flow_prepare(p, p->rcv, p->wgt, p->rslot, routed, p->order, p->h_pinned));
                 GS_CUDA(cudaStreamSynchronize(p->stream));
                 const int ok = p->h_pinned[0] ? 0 : 1;
-                GS_TRY(flow_run(p, p->rcv, p->wgt, p->rslot, nv, routed, &cyc, p->order, ok));
+                GS_TRY(flow_run(p, p->rcv, p->wgt, p->rslot, nv, routed, &cyc, p->order, ok, nullptr));
                 total_cycles += cyc;
                 GS_TRY(led_sum(p, n, nv, nullptr, nullptr, 1.0, GS_LED_ROUTED));
                 GS_TRY(led_cells(p, routed, p->wgt, lsink, pit_ids, mout));

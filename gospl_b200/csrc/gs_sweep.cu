@@ -542,6 +542,7 @@ struct FlowOrd {
     }
     __device__ __forceinline__ double init(int i) const { return b[i]; }
     __device__ __forceinline__ double combine(double s, double w, double xj) const { return s + w * xj; }
+    __device__ __forceinline__ double aux(int) const { return 0.0; }
     __device__ __forceinline__ double finish(int, double s, double) const { return s; }
 };
 
@@ -564,11 +565,13 @@ struct SplOrd {
     }
     __device__ __forceinline__ double init(int i) const { return hold[i]; }
     __device__ __forceinline__ double combine(double s, double w, double xj) const { return s + w * xj; }
-    __device__ __forceinline__ double finish(int i, double num, double) const {
+    // the denominator, formed when the vertex is ticketed (off the hop)
+    __device__ __forceinline__ double aux(int i) const {
         double den = 1.0;
         for (int k = 0; k < R; k++) den = den + c[(size_t)k * n + i];
-        return num / den;
+        return den;
     }
+    __device__ __forceinline__ double finish(int, double num, double den) const { return num / den; }
 };
 
 // Transposed flow system (I - W) y = g: y_i = g_i + sum_k w_ik y_{rcv_ik},
@@ -592,6 +595,7 @@ struct FlowAdjOrd {
     }
     __device__ __forceinline__ double init(int i) const { return g[i]; }
     __device__ __forceinline__ double combine(double s, double w, double xj) const { return s + w * xj; }
+    __device__ __forceinline__ double aux(int) const { return 0.0; }
     __device__ __forceinline__ double finish(int, double s, double) const { return s; }
 };
 
@@ -629,11 +633,12 @@ struct SplAdjOrd {
     }
     __device__ __forceinline__ double init(int i) const { return g[i]; }
     __device__ __forceinline__ double combine(double s, double w, double xj) const { return s + w * xj; }
-    __device__ __forceinline__ double finish(int i, double s, double) const {
+    __device__ __forceinline__ double aux(int i) const {
         double den = 1.0;
         for (int k = 0; k < R; k++) den = den + c[(size_t)k * n + i];
-        return s / den;
+        return den;
     }
+    __device__ __forceinline__ double finish(int, double s, double den) const { return s / den; }
 };
 
 // ---- FP32 operators of the precision form: values and arithmetic in FP32,
@@ -669,6 +674,7 @@ struct FlowOrd32 {
     }
     __device__ __forceinline__ float init(int i) const { return (float)b[i]; }
     __device__ __forceinline__ float combine(float s, float w, float xj) const { return s + w * xj; }
+    __device__ __forceinline__ double aux(int) const { return 0.0; }
     __device__ __forceinline__ float finish(int, float s, double) const { return s; }
 };
 
@@ -691,16 +697,26 @@ struct SplOrd32 {
     }
     __device__ __forceinline__ float init(int i) const { return (float)hold[i]; }
     __device__ __forceinline__ float combine(float s, float w, float xj) const { return s + w * xj; }
-    __device__ __forceinline__ float finish(int i, float num, double) const {
+    __device__ __forceinline__ double aux(int i) const {
         float den = 1.0f;
         for (int k = 0; k < R; k++) den = den + (float)c[(size_t)k * n + i];
-        return num / den;
+        return (double)den;    // exact: a float widened
     }
+    __device__ __forceinline__ float finish(int, float num, double den) const { return num / (float)den; }
 };
+
+// status of an ordered sweep whose order failed its check (skip flag set):
+// no vertex computed, the caller runs the counter-based sweep instead
+constexpr unsigned ORDER_REJECTED = 0x100u;
 
 template <class Op>
 __global__ void __launch_bounds__(128) k_ordered(Op op, int n, const int* __restrict__ order, unsigned* ctr,
-                                                 unsigned long long budget_ns, unsigned nap_max) {
+                                                 unsigned long long budget_ns, unsigned nap_max,
+                                                 const int* __restrict__ skip) {
+    if (skip && *skip) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) atomicCAS(&ctr[C_STATUS], 0u, ORDER_REJECTED);
+        return;
+    }
     const unsigned long long t0 = globaltimer_ns();
     const int lane = threadIdx.x & 31;
     const unsigned full = 0xffffffffu;
@@ -714,35 +730,41 @@ __global__ void __launch_bounds__(128) k_ordered(Op op, int n, const int* __rest
         if (base >= (unsigned)n) return;
         const unsigned t = base + lane;
         int node = -1, np = 0;
+        T init = T(0);
+        double aux = 0.0;
         if (t < (unsigned)n) {
             node = order[t];
             np = op.prep(node, pj, pw);
+            init = op.init(node);
+            aux = op.aux(node);
         }
         unsigned pending = __ballot_sync(full, node >= 0);
         unsigned rounds = 0, nap = 0;
         while (pending) {
             bool rdy = false;
             if (pending & (1u << lane)) {
-                // predecessor loads go out four at a time before any is looked
-                // at, so a polling round costs one memory latency per four
-                // predecessors; the sum keeps the predecessors' order
+                // the predecessor loads go out eight at a time before any is
+                // looked at, so a polling round costs one memory latency for up
+                // to eight predecessors (every vertex of a mesh of degree <= 8);
+                // the sum keeps the predecessors' order
+                constexpr int PB = Op::MAXP < 8 ? Op::MAXP : 8;
                 rdy = true;
-                T acc = op.init(node);
-                for (int q0 = 0; q0 < np && rdy; q0 += 4) {
-                    T v[4];
+                T acc = init;
+                for (int q0 = 0; q0 < np && rdy; q0 += PB) {
+                    T v[PB];
 #pragma unroll
-                    for (int u = 0; u < 4; u++)
+                    for (int u = 0; u < PB; u++)
                         if (q0 + u < np) v[u] = ld_val(&op.x[pj[q0 + u]]);
 #pragma unroll
-                    for (int u = 0; u < 4; u++)
+                    for (int u = 0; u < PB; u++)
                         if (q0 + u < np && is_sent(v[u])) rdy = false;
                     if (rdy) {
 #pragma unroll
-                        for (int u = 0; u < 4; u++)
+                        for (int u = 0; u < PB; u++)
                             if (q0 + u < np) acc = op.combine(acc, pw[q0 + u], v[u]);
                     }
                 }
-                if (rdy) st_val(&op.x[node], op.finish(node, acc, 0.0));
+                if (rdy) st_val(&op.x[node], op.finish(node, acc, aux));
             }
             unsigned done = __ballot_sync(full, rdy);
             pending &= ~done;
@@ -1027,16 +1049,22 @@ int flow_prepare(gs_plan* p, const int* rcv, const double* wgt, const int8_t* rs
 // The sweep proper, after flow_prepare: the ordered kernel when the order is
 // valid (ok), else the counter-based dataflow solve.
 int flow_run(gs_plan* p, const int* rcv, const double* wgt, const int8_t* rslot, const double* b, double* x,
-             int* cycle_nodes, int* order, int ok) {
+             int* cycle_nodes, int* order, int ok, int* status_host) {
     const int n = (int)p->n;
     *cycle_nodes = 0;
+    if (status_host) *status_host = 0;
     if (n == 0) return GS_OK;
     if (!ok) return flow_solve_counted(p, rcv, wgt, rslot, b, x, cycle_nodes);
     if (p->fp32) return flow_refine32(p, wgt, b, x, order);
     GS_CUDA(cudaMemsetAsync(p->ctr, 0, sizeof(unsigned) * 8, p->stream));
     FlowOrd op{n, p->nbr, p->don_mask, p->don_k, p->sorder, wgt, b, x};
-    launch(p, k_ordered<FlowOrd>, p->sm_count * p->sweep_per_sm, 128, op, n, (const int*)order, p->ctr, p->sweep_budget_ns, p->sweep_nap);
+    launch(p, k_ordered<FlowOrd>, p->sm_count * p->sweep_per_sm, 128, op, n, (const int*)order, p->ctr, p->sweep_budget_ns, p->sweep_nap, (const int*)nullptr);
     GS_LAUNCH();
+    if (status_host) {
+        // the caller reads the status at its next synchronisation
+        GS_CUDA(cudaMemcpyAsync(status_host, p->ctr + C_STATUS, sizeof(int), cudaMemcpyDeviceToHost, p->stream));
+        return GS_OK;
+    }
     int st = 0;
     GS_TRY(ordered_status(p, &st));
     if (st != 0) {
@@ -1060,7 +1088,7 @@ int flow_solve(gs_plan* p, const int* rcv, const double* wgt, const int8_t* rslo
         ok = p->h_pinned[0] ? 0 : 1;
     }
     if (order == p->order_i) p->order_i_valid = ok;
-    return flow_run(p, rcv, wgt, rslot, b, x, cycle_nodes, order, ok);
+    return flow_run(p, rcv, wgt, rslot, b, x, cycle_nodes, order, ok, nullptr);
 }
 
 // SPL edges i -> rcv (c != 0) run against the flow order: need pos[rcv] > pos[i]
@@ -1079,28 +1107,34 @@ int spl_sweep(gs_plan* p, const int* rcv, const double* c, const int8_t* rslot, 
     const int n = (int)p->n;
     *cycle_nodes = 0;
     if (n == 0) return GS_OK;
-    int ok = reuse_order && p->order_i_valid;
-    if (ok) {
-        launch(p, k_positions, grid_for(n, 256), 256, n, (const int*)p->order_i, p->pos);
-        GS_CUDA(cudaMemsetAsync(p->i_scalar + 14, 0, sizeof(int), p->stream));
-        launch(p, k_check_spl_order, grid_for(n, 256), 256, n, p->R, rcv, c, (const int*)p->pos, p->i_scalar + 14);
-        GS_LAUNCH();
+    const int ok = reuse_order && p->order_i_valid;
+    if (!ok) return spl_sweep_counted(p, rcv, c, rslot, hold, s, cycle_nodes);
+    // the check of the order against the SPL edges is read by the sweep
+    // itself (no host round trip): a rejected order stops it at once and the
+    // counter-based sweep runs instead
+    launch(p, k_positions, grid_for(n, 256), 256, n, (const int*)p->order_i, p->pos);
+    GS_CUDA(cudaMemsetAsync(p->i_scalar + 14, 0, sizeof(int), p->stream));
+    launch(p, k_check_spl_order, grid_for(n, 256), 256, n, p->R, rcv, c, (const int*)p->pos, p->i_scalar + 14);
+    GS_LAUNCH();
+    // the SPL system is solved receivers first: the flow order reversed
+    launch(p, k_reverse, grid_for(n, 256), 256, n, (const int*)p->order_i, p->order2);
+    if (p->fp32) {
+        // the refinement runs several sweeps: read the check first
         int bad = 0;
         GS_CUDA(cudaMemcpyAsync(&bad, p->i_scalar + 14, sizeof(int), cudaMemcpyDeviceToHost, p->stream));
         GS_CUDA(cudaStreamSynchronize(p->stream));
-        ok = !bad;
+        if (bad) return spl_sweep_counted(p, rcv, c, rslot, hold, s, cycle_nodes);
+        return spl_refine32(p, rcv, c, hold, s, p->order2);
     }
-    if (!ok) return spl_sweep_counted(p, rcv, c, rslot, hold, s, cycle_nodes);
-    // the SPL system is solved receivers first: the flow order reversed
-    launch(p, k_reverse, grid_for(n, 256), 256, n, (const int*)p->order_i, p->order2);
-    if (p->fp32) return spl_refine32(p, rcv, c, hold, s, p->order2);
     GS_CUDA(cudaMemsetAsync(p->ctr, 0, sizeof(unsigned) * 8, p->stream));
     launch(p, k_fill_sent, grid_for(n, 256), 256, n, s);
     SplOrd op{n, p->R, rcv, c, hold, s};
-    launch(p, k_ordered<SplOrd>, p->sm_count * p->sweep_per_sm, 128, op, n, (const int*)p->order2, p->ctr, p->sweep_budget_ns, p->sweep_nap);
+    launch(p, k_ordered<SplOrd>, p->sm_count * p->sweep_per_sm, 128, op, n, (const int*)p->order2, p->ctr,
+           p->sweep_budget_ns, p->sweep_nap, (const int*)(p->i_scalar + 14));
     GS_LAUNCH();
     int st = 0;
     GS_TRY(ordered_status(p, &st));
+    if ((unsigned)st == ORDER_REJECTED) return spl_sweep_counted(p, rcv, c, rslot, hold, s, cycle_nodes);
     if (st != 0) {
         set_error(st, "ordered SPL sweep did not complete");
         return st;
@@ -1116,7 +1150,7 @@ int sweep_flow_adjoint(gs_plan* p, const int* rcv, const double* wgt, const int*
     GS_CUDA(cudaMemsetAsync(p->ctr, 0, sizeof(unsigned) * 8, p->stream));
     launch(p, k_fill_sent, grid_for(n, 256), 256, n, y);
     FlowAdjOrd op{n, p->R, rcv, wgt, g, y};
-    launch(p, k_ordered<FlowAdjOrd>, p->sm_count * p->sweep_per_sm, 128, op, n, (const int*)p->order2, p->ctr, p->sweep_budget_ns, p->sweep_nap);
+    launch(p, k_ordered<FlowAdjOrd>, p->sm_count * p->sweep_per_sm, 128, op, n, (const int*)p->order2, p->ctr, p->sweep_budget_ns, p->sweep_nap, (const int*)nullptr);
     GS_LAUNCH();
     int st = 0;
     GS_TRY(ordered_status(p, &st));
@@ -1140,7 +1174,7 @@ int sweep_spl_adjoint(gs_plan* p, const int* rcv, const double* wgt, const int8_
     GS_CUDA(cudaMemsetAsync(p->ctr, 0, sizeof(unsigned) * 8, p->stream));
     launch(p, k_fill_sent, grid_for(n, 256), 256, n, y);
     SplAdjOrd op{n, p->R, p->nbr, p->don_mask, p->don_k, p->sorder, c, g, y};
-    launch(p, k_ordered<SplAdjOrd>, p->sm_count * p->sweep_per_sm, 128, op, n, order, p->ctr, p->sweep_budget_ns, p->sweep_nap);
+    launch(p, k_ordered<SplAdjOrd>, p->sm_count * p->sweep_per_sm, 128, op, n, order, p->ctr, p->sweep_budget_ns, p->sweep_nap, (const int*)nullptr);
     GS_LAUNCH();
     int st = 0;
     GS_TRY(ordered_status(p, &st));
@@ -1260,7 +1294,7 @@ int flow_refine32(gs_plan* p, const double* wgt, const double* b, double* x, con
         GS_CUDA(cudaMemsetAsync(p->ctr, 0, sizeof(unsigned) * 8, p->stream));
         launch(p, k_fill_sent32, G, B, n, p->f32a);
         FlowOrd32 op{n, p->nbr, p->don_mask, p->don_k, p->sorder, wgt, (const double*)p->r64, p->f32a};
-        launch(p, k_ordered<FlowOrd32>, p->sm_count * p->sweep_per_sm, 128, op, n, order, p->ctr, p->sweep_budget_ns, p->sweep_nap);
+        launch(p, k_ordered<FlowOrd32>, p->sm_count * p->sweep_per_sm, 128, op, n, order, p->ctr, p->sweep_budget_ns, p->sweep_nap, (const int*)nullptr);
         GS_LAUNCH();
         int st = 0;
         GS_TRY(ordered_status(p, &st));
@@ -1297,7 +1331,7 @@ int spl_refine32(gs_plan* p, const int* rcv, const double* c, const double* hold
         GS_CUDA(cudaMemsetAsync(p->ctr, 0, sizeof(unsigned) * 8, p->stream));
         launch(p, k_fill_sent32, G, B, n, p->f32a);
         SplOrd32 op{n, p->R, rcv, c, (const double*)p->r64, p->f32a};
-        launch(p, k_ordered<SplOrd32>, p->sm_count * p->sweep_per_sm, 128, op, n, order2, p->ctr, p->sweep_budget_ns, p->sweep_nap);
+        launch(p, k_ordered<SplOrd32>, p->sm_count * p->sweep_per_sm, 128, op, n, order2, p->ctr, p->sweep_budget_ns, p->sweep_nap, (const int*)nullptr);
         GS_LAUNCH();
         int st = 0;
         GS_TRY(ordered_status(p, &st));
@@ -1339,7 +1373,7 @@ int sweep_flow_rhs(gs_plan* p, const double* wgt, const int* order, const double
     GS_CUDA(cudaMemsetAsync(p->ctr, 0, sizeof(unsigned) * 8, p->stream));
     launch(p, k_fill_sent, grid_for(n, 256), 256, n, x);
     FlowOrd op{n, p->nbr, p->don_mask, p->don_k, p->sorder, wgt, b, x};
-    launch(p, k_ordered<FlowOrd>, p->sm_count * p->sweep_per_sm, 128, op, n, order, p->ctr, p->sweep_budget_ns, p->sweep_nap);
+    launch(p, k_ordered<FlowOrd>, p->sm_count * p->sweep_per_sm, 128, op, n, order, p->ctr, p->sweep_budget_ns, p->sweep_nap, (const int*)nullptr);
     GS_LAUNCH();
     int st = 0;
     GS_TRY(ordered_status(p, &st));
@@ -1355,7 +1389,7 @@ int sweep_spl_rhs(gs_plan* p, const int* rcv, const double* c, const int* order2
     GS_CUDA(cudaMemsetAsync(p->ctr, 0, sizeof(unsigned) * 8, p->stream));
     launch(p, k_fill_sent, grid_for(n, 256), 256, n, x);
     SplOrd op{n, p->R, rcv, c, rhs, x};
-    launch(p, k_ordered<SplOrd>, p->sm_count * p->sweep_per_sm, 128, op, n, order2, p->ctr, p->sweep_budget_ns, p->sweep_nap);
+    launch(p, k_ordered<SplOrd>, p->sm_count * p->sweep_per_sm, 128, op, n, order2, p->ctr, p->sweep_budget_ns, p->sweep_nap, (const int*)nullptr);
     GS_LAUNCH();
     int st = 0;
     GS_TRY(ordered_status(p, &st));

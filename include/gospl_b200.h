@@ -91,7 +91,7 @@ int gs_plan_set_stream(gs_plan* plan, void* cuda_stream);
 #define GS_TUNE_SWEEP_BLOCKS 1
 #define GS_TUNE_COOP_BLOCKS 2
 #define GS_TUNE_REFINE_PASSES 4   /* gs_plan_tuning only: refinement passes so far */
-#define GS_TUNE_SWEEP_NAP 5       /* longest back-off between polls of the ordered sweeps, ns (0..1024, default 128) */
+#define GS_TUNE_SWEEP_NAP 5       /* longest back-off between polls of the ordered sweeps, ns (0..1024, default 32) */
 #define GS_TUNE_SWEEP_BUDGET 6    /* wall-clock budget of one dependency sweep, us (1..6e7, default 4e6): a sweep
                                      still waiting on a predecessor after it stops with GS_ETIMEOUT */
 #define GS_TUNE_FLAT_BFS 7        /* flat-distance BFS: 0 one block with the visited set in shared memory
