@@ -705,12 +705,29 @@ struct SplOrd32 {
     __device__ __forceinline__ float finish(int, float num, double den) const { return num / (float)den; }
 };
 
+// predecessors q0..np-1 of a vertex of high degree, read together; false
+// while any is unpublished (kept out of line: rare, and its registers would
+// crowd the polling loop)
+template <class Op>
+__device__ __noinline__ bool ordered_tail(const Op& op, const int* pj, const typename Op::T* pw, int q0, int np,
+                                          typename Op::T* acc) {
+    using T = typename Op::T;
+    T v[Op::MAXP];
+    for (int q = q0; q < np; q++) v[q - q0] = ld_val(&op.x[pj[q]]);
+    for (int q = q0; q < np; q++)
+        if (is_sent(v[q - q0])) return false;
+    T a = *acc;
+    for (int q = q0; q < np; q++) a = op.combine(a, pw[q], v[q - q0]);
+    *acc = a;
+    return true;
+}
+
 // status of an ordered sweep whose order failed its check (skip flag set):
 // no vertex computed, the caller runs the counter-based sweep instead
 constexpr unsigned ORDER_REJECTED = 0x100u;
 
 template <class Op>
-__global__ void __launch_bounds__(128) k_ordered(Op op, int n, const int* __restrict__ order, unsigned* ctr,
+__global__ void __launch_bounds__(128, 8) k_ordered(Op op, int n, const int* __restrict__ order, unsigned* ctr,
                                                  unsigned long long budget_ns, unsigned nap_max,
                                                  const int* __restrict__ skip) {
     if (skip && *skip) {
@@ -740,31 +757,36 @@ __global__ void __launch_bounds__(128) k_ordered(Op op, int n, const int* __rest
         }
         unsigned pending = __ballot_sync(full, node >= 0);
         unsigned rounds = 0, nap = 0;
+        // The first PB predecessors of a lane are read until each is seen
+        // published and then kept in registers: a polling round loads only
+        // the predecessors still missing (mostly one), not all of them again.
+        // Re-reading every predecessor each round floods the SM's load path
+        // with requests that answer nothing new and stretches every round
+        // well past one L2 latency.  Predecessors beyond the first PB (rare:
+        // degree > 8) are read together each round.  The sum keeps the
+        // predecessors' order.
+        constexpr int PB = Op::MAXP < 6 ? Op::MAXP : 6;
+        unsigned seen = 0u;
+        T vals[PB];
+        const unsigned need = np >= PB ? ((1u << PB) - 1u) : ((1u << np) - 1u);
         while (pending) {
             bool rdy = false;
             if (pending & (1u << lane)) {
-                // the predecessor loads go out eight at a time before any is
-                // looked at, so a polling round costs one memory latency for up
-                // to eight predecessors (every vertex of a mesh of degree <= 8);
-                // the sum keeps the predecessors' order
-                constexpr int PB = Op::MAXP < 8 ? Op::MAXP : 8;
-                rdy = true;
-                T acc = init;
-                for (int q0 = 0; q0 < np && rdy; q0 += PB) {
-                    T v[PB];
+#pragma unroll
+                for (int u = 0; u < PB; u++)
+                    if (u < np && !((seen >> u) & 1u)) vals[u] = ld_val(&op.x[pj[u]]);
+#pragma unroll
+                for (int u = 0; u < PB; u++)
+                    if (u < np && !((seen >> u) & 1u) && !is_sent(vals[u])) seen |= 1u << u;
+                rdy = (seen & need) == need;
+                if (rdy) {
+                    T acc = init;
 #pragma unroll
                     for (int u = 0; u < PB; u++)
-                        if (q0 + u < np) v[u] = ld_val(&op.x[pj[q0 + u]]);
-#pragma unroll
-                    for (int u = 0; u < PB; u++)
-                        if (q0 + u < np && is_sent(v[u])) rdy = false;
-                    if (rdy) {
-#pragma unroll
-                        for (int u = 0; u < PB; u++)
-                            if (q0 + u < np) acc = op.combine(acc, pw[q0 + u], v[u]);
-                    }
+                        if (u < np) acc = op.combine(acc, pw[u], vals[u]);
+                    if (np > PB) rdy = ordered_tail(op, pj, pw, PB, np, &acc);
+                    if (rdy) st_val(&op.x[node], op.finish(node, acc, aux));
                 }
-                if (rdy) st_val(&op.x[node], op.finish(node, acc, aux));
             }
             unsigned done = __ballot_sync(full, rdy);
             pending &= ~done;
