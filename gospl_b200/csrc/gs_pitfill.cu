@@ -918,6 +918,8 @@ __global__ void k_basin_stamp(int n, const unsigned long long* __restrict__ L, i
     if (v < n) stamp[v] = (L[v] != ~0ULL) ? 0 : -1;
 }
 
+constexpr int RELAX_EDGES = 16;
+
 __global__ void __launch_bounds__(256) k_relax_active(const int* __restrict__ m_count, int cap,
                                                       const int* __restrict__ xu, const int* __restrict__ xv,
                                                       const double* __restrict__ xw, unsigned long long* L,
@@ -929,19 +931,21 @@ __global__ void __launch_bounds__(256) k_relax_active(const int* __restrict__ m_
     int r = 1;
     for (; r <= max_rounds; r++) {
         int changed = 0;
-        // four edges per thread and pass: their source ids and stamps are
-        // loaded before any is used, so the gathers overlap
-        for (int e0 = gtid; e0 < m; e0 += 4 * gsz) {
-            int v[4], sv[4];
+        // RELAX_EDGES edges per thread and pass: their source ids and stamps
+        // are loaded before any is used, so the gathers overlap and a round
+        // over the whole edge list costs about two memory round trips
+        constexpr int RE = RELAX_EDGES;
+        for (int e0 = gtid; e0 < m; e0 += RE * gsz) {
+            int v[RE], sv[RE];
 #pragma unroll
-            for (int q = 0; q < 4; q++) {
+            for (int q = 0; q < RE; q++) {
                 const int e = e0 + q * gsz;
                 v[q] = e < m ? xv[e] : -1;
             }
 #pragma unroll
-            for (int q = 0; q < 4; q++) sv[q] = v[q] >= 0 ? ((volatile int*)stamp)[v[q]] : -2;
+            for (int q = 0; q < RE; q++) sv[q] = v[q] >= 0 ? ((volatile int*)stamp)[v[q]] : -2;
 #pragma unroll
-            for (int q = 0; q < 4; q++) {
+            for (int q = 0; q < RE; q++) {
                 if (sv[q] < r - 1) continue;
                 const int e = e0 + q * gsz;
                 const unsigned long long lv = ((volatile unsigned long long*)L)[v[q]];
@@ -1373,11 +1377,22 @@ int fill_elevation(gs_plan* p, const double* h, double sealevel, double ofill, d
     launch(p, k_bfs_flag, G, B, n, (const int*)pit_ids, (const int*)p->spill_flag, p->flagbuf);
     GS_LAUNCH();
     GS_TRY(exclusive_scan(p, p->flagbuf, p->scanbuf, n));
-    int last[3];
+    // pit cells, compacted in id order for the per-pit reductions below (they
+    // read only the labels): their count comes back with the BFS counts
+    GS_CUDA(cudaMemsetAsync(p->seg_count, 0, sizeof(int) * (np1 + 1), p->stream));
+    launch(p, k_pit_flag, G, B, n, (const int*)pit_ids, p->pflag, p->seg_count);
+    GS_LAUNCH();
+    GS_TRY(exclusive_scan(p, p->pflag, p->pscan, n));
+    launch(p, k_pit_compact, G, B, n, (const int*)pit_ids, (const int*)p->pscan, p->seg_keys, p->seg_vals);
+    GS_LAUNCH();
+    int last[5];
     GS_CUDA(cudaMemcpyAsync(&last[0], p->scanbuf + n - 1, sizeof(int), cudaMemcpyDeviceToHost, p->stream));
     GS_CUDA(cudaMemcpyAsync(&last[1], p->flagbuf + n - 1, sizeof(int), cudaMemcpyDeviceToHost, p->stream));
     GS_CUDA(cudaMemcpyAsync(&last[2], p->i_scalar + I_NEXT, sizeof(int), cudaMemcpyDeviceToHost, p->stream));
+    GS_CUDA(cudaMemcpyAsync(&last[3], p->pscan + n - 1, sizeof(int), cudaMemcpyDeviceToHost, p->stream));
+    GS_CUDA(cudaMemcpyAsync(&last[4], p->pflag + n - 1, sizeof(int), cudaMemcpyDeviceToHost, p->stream));
     GS_CUDA(cudaStreamSynchronize(p->stream));
+    const int ncell = last[3] + last[4];
     int fsize = last[2], levels = 0;
     bool forked = false;
     if (fsize > 0) {
@@ -1454,23 +1469,8 @@ int fill_elevation(gs_plan* p, const double* h, double sealevel, double ofill, d
     if (sed) GS_TRY(fill_join(p, st));
 
     // pit cells sorted by (pit, id): segments for the per-pit reductions.
-    // Ordered compaction (scan) keeps id order; the stable radix sort by pit
-    // then lists every pit's cells in increasing id.
-    GS_CUDA(cudaMemsetAsync(p->seg_count, 0, sizeof(int) * (np1 + 1), p->stream));
-    launch(p, k_pit_flag, G, B, n, (const int*)pit_ids, p->pflag, p->seg_count);
-    GS_LAUNCH();
-    GS_TRY(exclusive_scan(p, p->pflag, p->pscan, n));
-    launch(p, k_pit_compact, G, B, n, (const int*)pit_ids, (const int*)p->pscan, p->seg_keys,
-           p->seg_vals);
-    GS_LAUNCH();
-    int ncell = 0;
-    {
-        int last[2];
-        GS_CUDA(cudaMemcpyAsync(&last[0], p->pscan + n - 1, sizeof(int), cudaMemcpyDeviceToHost, p->stream));
-        GS_CUDA(cudaMemcpyAsync(&last[1], p->pflag + n - 1, sizeof(int), cudaMemcpyDeviceToHost, p->stream));
-        GS_CUDA(cudaStreamSynchronize(p->stream));
-        ncell = last[0] + last[1];
-    }
+    // The ordered compaction (before the BFS) keeps id order; the stable
+    // radix sort by pit then lists every pit's cells in increasing id.
     if (ncell > 0) {
         int bits = 1;
         while ((1 << bits) <= P && bits < 31) bits++;
