@@ -80,7 +80,7 @@ def load(path=None):
     L.gs_plan_set_lake_diffusion.argtypes = [P, d, d, i32, i32]
     L.gs_sed_change.argtypes = [P, P, P, P, P, d, d, d, d, d, P, P, P, P, P, P, P, P, ctypes.POINTER(GsStats)]
     L.gs_sed_budget.argtypes = [P, P]
-    L.gs_sea_change.argtypes = [P, P, P, P, P, P, P, i64, d, d, d, d, d, d, P, P, P, ctypes.POINTER(GsStats)]
+    L.gs_sea_change.argtypes = [P, P, P, P, P, P, P, i64, d, d, d, d, d, d, d, P, P, P, ctypes.POINTER(GsStats)]
     L.gs_hillslope.argtypes = [P, P, P, P, d, d, d, d, d, i32, ctypes.POINTER(GsStats)]
     L.gs_apply_forces.argtypes = [P, P, P, P, d, d, P]
     L.gs_output_fields.argtypes = [P, P, P, P, P, P, P, P, P, P, P, P]

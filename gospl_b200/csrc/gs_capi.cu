@@ -348,20 +348,21 @@ int gs_sed_change(gs_plan* plan, double* h, double* cum_ed, const double* eb, co
 
 int gs_sea_change(gs_plan* plan, double* h, double* cum_ed, double* eb, const double* xyz, const double* box,
                   const int32_t* edges, int64_t nedge, double sealevel, double ofill, double dt, double clinslp,
-                  double offshore, double nlk, const double* lfill, const double* vsed, const uint8_t* sea,
-                  gs_stats* stats) {
+                  double offshore, double nlk, double gmar, const double* lfill, const double* vsed,
+                  const uint8_t* sea, gs_stats* stats) {
     NEED(plan);
     NEED(box);
     if (plan->n > 0) {
         NEED(h); NEED(cum_ed); NEED(eb); NEED(xyz); NEED(lfill); NEED(vsed); NEED(sea);
         if (nedge > 0) NEED(edges);
     }
-    if (!(dt > 0) || nedge < 0 || !(clinslp >= 0) || !(offshore > 0) || !(nlk >= 0)) {
-        gs::set_error(GS_EINVAL, "seaChange: need dt > 0, nedge >= 0, clinslp >= 0, offshore > 0, nlk >= 0");
+    if (!(dt > 0) || nedge < 0 || !(clinslp >= 0) || !(offshore > 0) || !(nlk >= 0) || !(gmar >= 0)) {
+        gs::set_error(GS_EINVAL,
+                      "seaChange: need dt > 0, nedge >= 0, clinslp >= 0, offshore > 0, nlk >= 0, gmar >= 0");
         return GS_EINVAL;
     }
     GS_GUARD(return gs::sea_change(plan, h, cum_ed, eb, xyz, box, edges, nedge, sealevel, ofill, dt, clinslp, offshore,
-                                   nlk, lfill, vsed, sea, stats);)
+                                   nlk, gmar, lfill, vsed, sea, stats);)
 }
 
 int gs_sed_budget(gs_plan* plan, double* out16) {

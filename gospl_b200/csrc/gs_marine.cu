@@ -503,6 +503,41 @@ __global__ void __launch_bounds__(256) k_ocean_sum_final(const double* __restric
     }
 }
 
+// ---- 4b. the coupled marine system ---------------------------------------
+__global__ void k_marine_g(int n, const double* __restrict__ hl, double sealevel, double gmar, double* g) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double v = gmar > 0.99 ? 0.99 : gmar;
+    if (hl[i] > sealevel) v = 0.0;
+    g[i] = v;
+}
+
+// y = s x, times the area when `area` is given
+__global__ void k_marine_scale(int n, double s, const double* __restrict__ x, const double* __restrict__ area,
+                               double* y) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    y[i] = area ? area[i] * s * x[i] : s * x[i];
+}
+
+// y = G dt/A q, plus (1 - G) x when x is given
+__global__ void k_marine_gsq(int n, const double* __restrict__ g, double dt, const double* __restrict__ area,
+                             const double* __restrict__ q, const double* __restrict__ x, double* y) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double gi = g[i];
+    double v = gi * dt / area[i] * q[i];
+    if (x) v = (1.0 - gi) * x[i] + v;
+    y[i] = v;
+}
+
+__global__ void k_marine_voldep(int n, const double* __restrict__ d, const double* __restrict__ area, double* v) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double x = d[i] * area[i];
+    v[i] = x < 0.0 ? 0.0 : x;
+}
+
 }  // namespace
 
 static int ocean_sum(gs_plan* p, const double* x, double* dev_out, double* host_out) {
@@ -515,10 +550,37 @@ static int ocean_sum(gs_plan* p, const double* x, double* dev_out, double* host_
     return GS_OK;
 }
 
+// The coupled system reduced to the elevation change d = h_new - h:
+// q = S [dep/dt + A/dt (h - h_new)] with S = (I - W^T)^-1 (row 2), so row 1
+// reads (1 - G) d + G dt/A S[A/dt d] = G dt/A S[dep/dt]; one application is
+// one ordered marine flow sweep.
+struct MarineSystem : LinOp {
+    gs_plan* p;
+    int n;
+    const double* g;
+    double dt;
+    const unsigned short* cand;
+    const double* w;
+    double* t1;
+    double* t2;
+    MarineSystem(gs_plan* p_, int n_, const double* g_, double dt_, const unsigned short* cand_, const double* w_,
+                 double* t1_, double* t2_)
+        : p(p_), n(n_), g(g_), dt(dt_), cand(cand_), w(w_), t1(t1_), t2(t2_) {}
+    int apply(const double* x, double* y) override {
+        const int B = 256, G = grid_for(n, B);
+        launch(p, k_marine_scale, G, B, n, 1.0 / dt, x, (const double*)p->larea, t1);
+        GS_LAUNCH();
+        GS_TRY(sweep_marine(p, cand, w, p->order, t1, t2));
+        launch(p, k_marine_gsq, G, B, n, g, dt, (const double*)p->larea, (const double*)t2, x, y);
+        GS_LAUNCH();
+        return GS_OK;
+    }
+};
+
 int sea_change(gs_plan* p, double* h, double* cum_ed, double* eb, const double* xyz, const double* box,
                const int* edges, int64_t nedge, double sealevel, double ofill, double dt, double clinslp,
-               double offshore, double nlk, const double* lfill, const double* vsed, const uint8_t* sea,
-               gs_stats* st) {
+               double offshore, double nlk, double gmar, const double* lfill, const double* vsed,
+               const uint8_t* sea, gs_stats* st) {
     const int n = (int)p->n;
     if (n == 0) return GS_OK;
     if (!p->lake_on) {
@@ -662,50 +724,89 @@ int sea_change(gs_plan* p, double* h, double* cum_ed, double* eb, const double* 
     GS_LAUNCH();
 
     // 4. the cascade: until the volume in transit is at most max(1, 1e-6 of
-    // the input) or 5000 passes (seaplex.py:542-610)
-    launch(p, k_ocean_init, G, B, n, (const double*)maxdep, (const double*)sedflux, (const uint8_t*)sink, marvol,
-           tmpa, vdep);
-    GS_LAUNCH();
+    // the input) or 5000 passes (seaplex.py:542-610); every call starts from
+    // the full capacity (marvol = maxDepQs) with the given input volumes, and
+    // deposits into vdep
     double* sres = p->d_scalar + 15;
-    double sum = 0.0;
-    GS_TRY(ocean_sum(p, tmpa, sres, &sum));
-    const double threshold = std::max(1.0, 1.0e-6 * sum);
-    // the loop control lives on the device (stop flag, pass count): passes
-    // are queued eight at a time and those after the stop only carry the
-    // volumes over, so the host synchronises once per eight passes
     int* stop = p->i_scalar + 10;
     int* dpass = p->i_scalar + 11;
     double* dthr = p->d_scalar + 7;
-    {
-        const int h[2] = {(sum > threshold) ? 0 : 1, 0};
-        GS_CUDA(cudaMemcpyAsync(stop, h, sizeof(int) * 2, cudaMemcpyHostToDevice, p->stream));
-        GS_CUDA(cudaMemcpyAsync(dthr, &threshold, sizeof(double), cudaMemcpyHostToDevice, p->stream));
-    }
     int step = 0;
-    double* cur = tmpa;
-    double* nxt = tmpb;
-    int hs[2] = {(sum > threshold) ? 0 : 1, 0};
-    while (!hs[0]) {
-        for (int q = 0; q < 8; q++) {
-            launch(p, k_ocean_step, G, B, n, p->flat, (const int*)p->nbr, (const int8_t*)p->nnb,
-                   (const int8_t*)p->rev, (const unsigned long long*)p->sorder, (const unsigned short*)cand,
-                   (const double*)wgt, (const uint8_t*)sink, (const uint8_t*)p->outlet, (const double*)cur, nxt,
-                   marvol, vdep, (const int*)stop);
-            launch(p, k_ocean_sum, SUM_NB, 256, n, (const double*)nxt, p->red, (const int*)stop);
-            launch(p, k_ocean_sum_final, 1, 256, (const double*)p->red, sres, stop, dpass, (const double*)dthr);
-            std::swap(cur, nxt);
-        }
+    auto cascade = [&](const double* input) -> int {
+        launch(p, k_ocean_init, G, B, n, (const double*)maxdep, input, (const uint8_t*)sink, marvol, tmpa, vdep);
         GS_LAUNCH();
-        GS_CUDA(cudaMemcpyAsync(hs, stop, sizeof(int) * 2, cudaMemcpyDeviceToHost, p->stream));
-        GS_CUDA(cudaStreamSynchronize(p->stream));
+        double sum = 0.0;
+        GS_TRY(ocean_sum(p, tmpa, sres, &sum));
+        const double threshold = std::max(1.0, 1.0e-6 * sum);
+        // the loop control lives on the device (stop flag, pass count):
+        // passes are queued eight at a time and those after the stop only
+        // carry the volumes over, so the host synchronises once per eight
+        {
+            const int h0[2] = {(sum > threshold) ? 0 : 1, 0};
+            GS_CUDA(cudaMemcpyAsync(stop, h0, sizeof(int) * 2, cudaMemcpyHostToDevice, p->stream));
+            GS_CUDA(cudaMemcpyAsync(dthr, &threshold, sizeof(double), cudaMemcpyHostToDevice, p->stream));
+        }
+        double* cur = tmpa;
+        double* nxt = tmpb;
+        int hs[2] = {(sum > threshold) ? 0 : 1, 0};
+        while (!hs[0]) {
+            for (int q = 0; q < 8; q++) {
+                launch(p, k_ocean_step, G, B, n, p->flat, (const int*)p->nbr, (const int8_t*)p->nnb,
+                       (const int8_t*)p->rev, (const unsigned long long*)p->sorder, (const unsigned short*)cand,
+                       (const double*)wgt, (const uint8_t*)sink, (const uint8_t*)p->outlet, (const double*)cur, nxt,
+                       marvol, vdep, (const int*)stop);
+                launch(p, k_ocean_sum, SUM_NB, 256, n, (const double*)nxt, p->red, (const int*)stop);
+                launch(p, k_ocean_sum_final, 1, 256, (const double*)p->red, sres, stop, dpass, (const double*)dthr);
+                std::swap(cur, nxt);
+            }
+            GS_LAUNCH();
+            GS_CUDA(cudaMemcpyAsync(hs, stop, sizeof(int) * 2, cudaMemcpyDeviceToHost, p->stream));
+            GS_CUDA(cudaStreamSynchronize(p->stream));
+        }
+        step = hs[1];
+        // what is still in transit stays where it is
+        launch(p, k_ocean_rest, G, B, n, p->flat, (const uint8_t*)p->outlet, (const double*)cur, vdep);
+        GS_LAUNCH();
+        return GS_OK;
+    };
+    GS_TRY(cascade(sedflux));
+
+    // 4b. the coupled marine system (Gmar > 0 on spheres, seaplex.py:240-402):
+    // its deposit, negatives dropped, goes down the cascade again
+    int gm_applies = 0;
+    if (!p->flat && gmar > 0.0) {
+        double* G_ = marvol;     // G = min(gmar, 0.99) below sea level (marvol is reset by the next cascade)
+        double* dd = hsm;        // the elevation change d = h_new - h
+        double* r0 = zsurf;
+        double* t1 = tmpa;
+        double* t2 = tmpb;
+        launch(p, k_marine_g, G, B, n, (const double*)hl, sealevel, gmar, G_);
+        GS_LAUNCH();
+        GS_TRY(flow_order(p, fz, p->order));
+        // r0 = G dt/A S[dep / dt]
+        launch(p, k_marine_scale, G, B, n, 1.0 / dt, (const double*)vdep, (const double*)nullptr, t1);
+        GS_LAUNCH();
+        GS_TRY(sweep_marine(p, cand, wgt, p->order, t1, t2));
+        launch(p, k_marine_gsq, G, B, n, (const double*)G_, dt, (const double*)p->larea, (const double*)t2,
+               (const double*)nullptr, r0);
+        GS_CUDA(cudaMemsetAsync(dd, 0, sizeof(double) * N, p->stream));
+        GS_LAUNCH();
+        MarineSystem op(p, n, G_, dt, cand, wgt, t1, t2);
+        double relres = 0.0;
+        const int gst = gmres_solve(p, op, r0, dd, 1.0e-13, 400, &gm_applies, &relres);
+        if (gst == GS_EMAXITER) {
+            set_error(GS_EMAXITER, "seaChange: the coupled marine system did not converge");
+            return GS_EMAXITER;
+        }
+        GS_TRY(gst);
+        // volDep = max(d A, 0), the input of the second cascade
+        launch(p, k_marine_voldep, G, B, n, (const double*)dd, (const double*)p->larea, sedflux);
+        GS_LAUNCH();
+        GS_TRY(cascade(sedflux));
     }
-    step = hs[1];
-    // what is still in transit stays where it is
-    launch(p, k_ocean_rest, G, B, n, p->flat, (const uint8_t*)p->outlet, (const double*)cur, vdep);
-    GS_LAUNCH();
 
     // 5. thickness, Picard diffusion over the sea cells, updates
-    double* zb = tmpb == cur ? tmpa : tmpb;   // free buffer
+    double* zb = tmpb;     // free once the cascade has deposited what was in transit
     double* hcur = hsm;
     double* cd = zsurf;
     double* hstart = marvol;
@@ -718,6 +819,7 @@ int sea_change(gs_plan* p, double* h, double* cum_ed, double* eb, const double* 
         st->cascade_passes = step;
         st->fill_rounds = passes;
         st->npits = m;
+        st->cg_iters = gm_applies;
     }
     return GS_OK;
 }

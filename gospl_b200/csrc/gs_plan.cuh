@@ -294,6 +294,21 @@ int flow_prepare(gs_plan* p, const int* rcv, const double* wgt, const int8_t* rs
 // status_host (pinned): when given, the ordered sweep's status is copied
 // there asynchronously and the caller checks it after its next
 // synchronisation of the plan's stream; otherwise flow_run synchronises
+// A linear operator on device vectors of the plan's length, for GMRES.
+struct LinOp {
+    virtual int apply(const double* x, double* y) = 0;
+    virtual ~LinOp() {}
+};
+// Restarted GMRES(30) on op x = a from the given x to |a - op x| <= tol |a|
+// (at most max_applies applications); GS_EMAXITER when it stops short.
+int gmres_solve(gs_plan* p, LinOp& op, const double* a, double* x, double tol, int max_applies, int* applies,
+                double* relres);
+int gm_axpby(gs_plan* p, int n, double a, const double* x, double b, const double* y, double* z);
+// Marine flow accumulation q = (I - W^T)^-1 b over the marine receivers
+// (bit sets cand over the neighbour slots, weights w), donors summed in
+// ascending id, in the order of the marine surface (descending).
+int sweep_marine(gs_plan* p, const unsigned short* cand, const double* w, const int* order, const double* b,
+                 double* q);
 int flow_run(gs_plan* p, const int* rcv, const double* wgt, const int8_t* rslot, const double* b,
              double* x, int* cycle_nodes, int* order, int ok, int* status_host);
 int group_sum_by_pit(gs_plan* p, const int* pit_ids, const uint8_t* mask, const double* vals,
@@ -313,8 +328,8 @@ int sed_change(gs_plan* p, double* h, double* cum_ed, const double* eb, const do
 int sed_budget(gs_plan* p, double* out16);
 int sea_change(gs_plan* p, double* h, double* cum_ed, double* eb, const double* xyz, const double* box,
                const int* edges, int64_t nedge, double sealevel, double ofill, double dt, double clinslp,
-               double offshore, double nlk, const double* lfill, const double* vsed, const uint8_t* sea,
-               gs_stats* st);
+               double offshore, double nlk, double gmar, const double* lfill, const double* vsed,
+               const uint8_t* sea, gs_stats* st);
 int picard_diffuse(gs_plan* p, const uint8_t* lmask, const double* zb, double* hcur, double K, double dt,
                    double* cd, double* hstart);
 int diffusion_solve_on(gs_plan* p, int m, const int* nbr, const int8_t* nnb, const double* farea, const uint8_t* fix,

@@ -140,7 +140,18 @@ __global__ void k_ed_dot_final(int parts, const double* __restrict__ part, doubl
 
 constexpr int GMRES_M1 = 31;   // GMRES restart length + 1
 
-struct EdSolve {
+// fixed-order dot product (block partials, then one block), read on the host
+static int gm_dot(gs_plan* p, int n, const double* a, const double* b, double* out) {
+    const int PARTS = 512;
+    launch(p, k_ed_dot_part, PARTS, 256, n, a, b, p->red);
+    launch(p, k_ed_dot_final, 1, 1024, PARTS, (const double*)p->red, p->red + 4200);
+    GS_LAUNCH();
+    GS_CUDA(cudaMemcpyAsync(out, p->red + 4200, sizeof(double), cudaMemcpyDeviceToHost, p->stream));
+    GS_CUDA(cudaStreamSynchronize(p->stream));
+    return GS_OK;
+}
+
+struct EdSolve : LinOp {
     gs_plan* p;
     int n;
     const int* rcv;
@@ -152,8 +163,11 @@ struct EdSolve {
     double* u;
     double* w;
     double* y2;
+    EdSolve(gs_plan* p_, int n_, const int* rcv_, const double* wgt_, const double* c_, const double* f_,
+            double dt_, double* t1_, double* u_, double* w_, double* y2_)
+        : p(p_), n(n_), rcv(rcv_), wgt(wgt_), c(c_), f(f_), dt(dt_), t1(t1_), u(u_), w(w_), y2(y2_) {}
     // y = (I + B) x
-    int apply(const double* x, double* y) {
+    int apply(const double* x, double* y) override {
         const int B = 256, G = grid_for(n, B);
         launch(p, k_ed_scale, G, B, n, (const double*)p->larea, dt, x, t1);
         GS_LAUNCH();
@@ -163,15 +177,6 @@ struct EdSolve {
         GS_TRY(sweep_spl_rhs(p, rcv, c, p->order2, w, y2));
         launch(p, k_ed_axpby, G, B, n, 1.0, x, 1.0, (const double*)y2, y);
         GS_LAUNCH();
-        return GS_OK;
-    }
-    int dot(const double* a, const double* b, double* out) {
-        const int PARTS = 512;
-        launch(p, k_ed_dot_part, PARTS, 256, n, a, b, p->red);
-        launch(p, k_ed_dot_final, 1, 1024, PARTS, (const double*)p->red, p->red + 4200);
-        GS_LAUNCH();
-        GS_CUDA(cudaMemcpyAsync(out, p->red + 4200, sizeof(double), cudaMemcpyDeviceToHost, p->stream));
-        GS_CUDA(cudaStreamSynchronize(p->stream));
         return GS_OK;
     }
 };
@@ -230,61 +235,40 @@ __global__ void k_mupdate(int n, int k, const double* __restrict__ V, const doub
     w[i] = s;
 }
 
-static int coupled_ed(gs_plan* p, const double* hold, const double* fal, const uint8_t* sea, double dt,
-                      const int* rcv_i, const double* wgt_i, double* x) {
+// Restarted GMRES(30) in FP64 on op x = a from the given x: Arnoldi with
+// classical Gram-Schmidt applied twice (fixed-order block dot products of the
+// new vector with the basis, k_mdot_part / k_mdot_final / k_mupdate), Givens
+// rotations of the Hessenberg matrix on the host, one synchronisation per
+// step; stops at |a - op x| <= tol |a| or after max_applies applications.
+int gmres_solve(gs_plan* p, LinOp& op, const double* a, double* x, double tol, int max_applies, int* applies_out,
+                double* relres_out) {
     const int n = (int)p->n;
     const int B = 256, G = grid_for(n, B);
-    if (!p->order_i_valid) {
-        set_error(GS_EINVAL, "transport-limited SPL needs a topological order of the receiver graph");
-        return GS_EINVAL;
-    }
     constexpr int M = GMRES_M1 - 1;   // restart length
     const int PARTS = p->sm_count * 8;
-    if (!p->ed_buf) GS_CUDA(cudaMalloc((void**)&p->ed_buf, sizeof(double) * (size_t)std::max(n, 1) * 6));
     if (!p->ed_basis)
         GS_CUDA(cudaMalloc((void**)&p->ed_basis,
                            sizeof(double) * ((size_t)std::max(n, 1) * GMRES_M1 + (size_t)PARTS * GMRES_M1 + 4 * GMRES_M1)));
     // (PARTS depends only on the SM count, fixed for the plan's device)
-    double* f = p->ed_buf;
-    double* t1 = f + n;
-    double* u = t1 + n;
-    double* w = u + n;
-    double* y2 = w + n;
-    double* a = y2 + n;
     double* V = p->ed_basis;
     double* part = V + (size_t)n * GMRES_M1;
     double* hd = part + (size_t)PARTS * GMRES_M1;    // [0, M1): pass 1, [M1, 2 M1): pass 2, 2 M1: norm^2
     double* r = p->cg_r;
-    launch(p, k_fdep, G, B, n, p->fdepa, (const double*)p->larea, fal, sea, (const uint8_t*)p->outlet, p->flat, f);
-    GS_LAUNCH();
-    GS_TRY(build_donors(p, rcv_i, wgt_i, p->rslot_i));
-    GS_TRY(spl_order(p));
-    EdSolve op{p, n, rcv_i, wgt_i, (const double*)p->c, (const double*)f, dt, t1, u, w, y2};
-    // x0 = M^-1 hOld (detachment-limited), a = x0 + B hOld
-    GS_TRY(sweep_spl_rhs(p, rcv_i, p->c, p->order2, hold, x));
-    GS_TRY(op.apply(hold, a));                                        // a = hOld + B hOld
-    launch(p, k_ed_axpby, G, B, n, 1.0, (const double*)a, -1.0, hold, a);
-    launch(p, k_ed_axpby, G, B, n, 1.0, (const double*)a, 1.0, (const double*)x, a);
-    GS_LAUNCH();
     double an = 0.0;
-    GS_TRY(op.dot(a, a, &an));
+    GS_TRY(gm_dot(p, n, a, a, &an));
     const double anorm = sqrt(an);
-    const double tol = 1.0e-13;
-    // GMRES(M) on (I + B) x = a: Arnoldi with classical Gram-Schmidt applied
-    // twice, Givens rotations of the Hessenberg matrix on the host, one
-    // synchronisation per step
     std::vector<double> H((size_t)(M + 1) * M), cs(M), sn(M), g(M + 1), y(M), hh(2 * GMRES_M1 + 1);
     int applies = 0;
     double res = 0.0;
     bool conv = anorm == 0.0;
-    while (!conv && applies < 200) {
-        // r = a - (I + B) x, V_0 = r / |r|
+    while (!conv && applies < max_applies) {
+        // r = a - op x, V_0 = r / |r|
         GS_TRY(op.apply(x, r));
         applies++;
-        launch(p, k_ed_axpby, G, B, n, 1.0, (const double*)a, -1.0, (const double*)r, r);
+        launch(p, k_ed_axpby, G, B, n, 1.0, a, -1.0, (const double*)r, r);
         GS_LAUNCH();
         double rn2 = 0.0;
-        GS_TRY(op.dot(r, r, &rn2));
+        GS_TRY(gm_dot(p, n, r, r, &rn2));
         const double beta = sqrt(rn2);
         res = beta;
         if (!(beta == beta)) break;
@@ -294,7 +278,7 @@ static int coupled_ed(gs_plan* p, const double* hold, const double* fal, const u
         std::fill(g.begin(), g.end(), 0.0);
         g[0] = beta;
         int k = 0;
-        for (; k < M && applies < 200; k++) {
+        for (; k < M && applies < max_applies; k++) {
             double* vk1 = V + (size_t)(k + 1) * n;
             GS_TRY(op.apply(V + (size_t)k * n, vk1));
             applies++;
@@ -345,13 +329,55 @@ static int coupled_ed(gs_plan* p, const double* hold, const double* fal, const u
         GS_CUDA(cudaStreamSynchronize(p->stream));
         if (!(res == res)) break;
     }
+    if (applies_out) *applies_out = applies;
+    if (relres_out) *relres_out = anorm > 0.0 ? res / anorm : 0.0;
+    return conv ? GS_OK : GS_EMAXITER;
+}
+
+// x = y (device copy through the GMRES axpby kernel)
+int gm_axpby(gs_plan* p, int n, double a, const double* x, double b, const double* y, double* z) {
+    launch(p, k_ed_axpby, grid_for(n, 256), 256, n, a, x, b, y, z);
+    GS_LAUNCH();
+    return GS_OK;
+}
+
+static int coupled_ed(gs_plan* p, const double* hold, const double* fal, const uint8_t* sea, double dt,
+                      const int* rcv_i, const double* wgt_i, double* x) {
+    const int n = (int)p->n;
+    const int B = 256, G = grid_for(n, B);
+    if (!p->order_i_valid) {
+        set_error(GS_EINVAL, "transport-limited SPL needs a topological order of the receiver graph");
+        return GS_EINVAL;
+    }
+    if (!p->ed_buf) GS_CUDA(cudaMalloc((void**)&p->ed_buf, sizeof(double) * (size_t)std::max(n, 1) * 6));
+    double* f = p->ed_buf;
+    double* t1 = f + n;
+    double* u = t1 + n;
+    double* w = u + n;
+    double* y2 = w + n;
+    double* a = y2 + n;
+    launch(p, k_fdep, G, B, n, p->fdepa, (const double*)p->larea, fal, sea, (const uint8_t*)p->outlet, p->flat, f);
+    GS_LAUNCH();
+    GS_TRY(build_donors(p, rcv_i, wgt_i, p->rslot_i));
+    GS_TRY(spl_order(p));
+    EdSolve op(p, n, rcv_i, wgt_i, (const double*)p->c, (const double*)f, dt, t1, u, w, y2);
+    // x0 = M^-1 hOld (detachment-limited), a = x0 + B hOld
+    GS_TRY(sweep_spl_rhs(p, rcv_i, p->c, p->order2, hold, x));
+    GS_TRY(op.apply(hold, a));                                        // a = hOld + B hOld
+    launch(p, k_ed_axpby, G, B, n, 1.0, (const double*)a, -1.0, hold, a);
+    launch(p, k_ed_axpby, G, B, n, 1.0, (const double*)a, 1.0, (const double*)x, a);
+    GS_LAUNCH();
+    // GMRES(30) on (I + B) x = a to 1e-13 of |a|, at most 200 applications
+    int applies = 0;
+    double relres = 0.0;
+    const int st = gmres_solve(p, op, a, x, 1.0e-13, 200, &applies, &relres);
     p->ed_iters = applies;
-    p->ed_relres = anorm > 0.0 ? res / anorm : 0.0;
-    if (!conv) {
+    p->ed_relres = relres;
+    if (st == GS_EMAXITER) {
         set_error(GS_EMAXITER, "transport-limited SPL: GMRES did not converge");
         return GS_EMAXITER;
     }
-    return GS_OK;
+    return st;
 }
 
 int erodep_spl(gs_plan* p, double* h, double* cum_ed, double* eb, const double* fal,

@@ -808,6 +808,58 @@ __global__ void __launch_bounds__(128, 8) k_ordered(Op op, int n, const int* __r
     }
 }
 
+// ---- marine flow accumulation (the coupled marine system, Gmar > 0) ----
+// q_i = b_i + sum over donors j of w_j q_j, a donor being a neighbour whose
+// receiver bit set (cand, over its neighbour slots) holds the slot of i; the
+// weight is the donor's 1/kk.  Donors in ascending id.
+struct MarineOrd {
+    using T = double;
+    int n;
+    const int* nbr;
+    const int8_t* nnb;
+    const int8_t* rev;
+    const unsigned long long* sorder;
+    const unsigned short* cand;
+    const double* w;
+    const double* b;
+    double* x;
+    static constexpr int MAXP = MAXW;
+    __device__ __forceinline__ int prep(int i, int* pj, double* pw) const {
+        const unsigned long long so = sorder[i];
+        int np = 0;
+        for (int q = 0; q < nnb[i]; q++) {
+            const int sl = (int)((so >> (4 * q)) & 15ULL);
+            const int j = nbr[(size_t)sl * n + i];
+            if (j < 0) continue;
+            const int r = rev[(size_t)sl * n + i];
+            if (r >= 0 && ((cand[j] >> r) & 1u)) {
+                pj[np] = j;
+                pw[np] = w[j];
+                np++;
+            }
+        }
+        return np;
+    }
+    __device__ __forceinline__ double init(int i) const { return b[i]; }
+    __device__ __forceinline__ double combine(double s, double wj, double xj) const { return s + wj * xj; }
+    __device__ __forceinline__ double aux(int) const { return 0.0; }
+    __device__ __forceinline__ double finish(int, double s, double) const { return s; }
+};
+
+// every marine receiver edge j -> i must go forward in the order
+__global__ void k_check_marine_order(int n, const int* __restrict__ nbr, const int8_t* __restrict__ nnb,
+                                     const unsigned short* __restrict__ cand, const int* __restrict__ pos,
+                                     int* bad) {
+    int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    const unsigned m = cand[j];
+    for (int s = 0; s < nnb[j]; s++) {
+        if (!((m >> s) & 1u)) continue;
+        const int i = nbr[(size_t)s * n + j];
+        if (i >= 0 && pos[j] >= pos[i]) { *bad = 1; return; }
+    }
+}
+
 // sort vertices by (surface desc, flat distance desc); returns 1 when the
 // order is topological for the given flow edges
 // Tie groups of the surface-sorted order: run start of every position (max-
@@ -1159,6 +1211,35 @@ int spl_sweep(gs_plan* p, const int* rcv, const double* c, const int8_t* rslot, 
     if ((unsigned)st == ORDER_REJECTED) return spl_sweep_counted(p, rcv, c, rslot, hold, s, cycle_nodes);
     if (st != 0) {
         set_error(st, "ordered SPL sweep did not complete");
+        return st;
+    }
+    return GS_OK;
+}
+
+int sweep_marine(gs_plan* p, const unsigned short* cand, const double* w, const int* order, const double* b,
+                 double* q) {
+    const int n = (int)p->n;
+    if (n == 0) return GS_OK;
+    launch(p, k_positions, grid_for(n, 256), 256, n, order, p->pos);
+    GS_CUDA(cudaMemsetAsync(p->i_scalar + 14, 0, sizeof(int), p->stream));
+    launch(p, k_check_marine_order, grid_for(n, 256), 256, n, (const int*)p->nbr, (const int8_t*)p->nnb, cand,
+           (const int*)p->pos, p->i_scalar + 14);
+    GS_CUDA(cudaMemsetAsync(p->ctr, 0, sizeof(unsigned) * 8, p->stream));
+    launch(p, k_fill_sent, grid_for(n, 256), 256, n, q);
+    MarineOrd op{n, p->nbr, p->nnb, p->rev, p->sorder, cand, w, b, q};
+    // a rejected order (a marine receiver not below its donor) stops the
+    // sweep at once: the receivers are strictly lower, so it cannot happen
+    launch(p, k_ordered<MarineOrd>, p->sm_count * p->sweep_per_sm, 128, op, n, order, p->ctr, p->sweep_budget_ns,
+           p->sweep_nap, (const int*)(p->i_scalar + 14));
+    GS_LAUNCH();
+    int st = 0;
+    GS_TRY(ordered_status(p, &st));
+    if ((unsigned)st == ORDER_REJECTED) {
+        set_error(GS_EINVAL, "marine sweep: the marine receivers are not below their donors in the surface order");
+        return GS_EINVAL;
+    }
+    if (st != 0) {
+        set_error(st, "marine sweep did not complete");
         return st;
     }
     return GS_OK;

@@ -8,7 +8,7 @@ uses, with goSPL's names, defaults and errors (gospl/tools/inputparser.py):
   ``o f w c``, legacy ``0``/``1`` -> ``o``/``f``, :208-246), ``fast``, ``nodep``
   and ``seadepo`` (:289-300; continental deposition runs unless ``nodep``,
   marine deposition when ``seadepo`` (default on), built for
-  ``marineSolver: picard`` and ``Gmar`` 0);
+  ``marineSolver: picard``);
 * ``time``: ``start``, ``end``, ``dt`` required, ``tout`` (:343-404, clamped
   to [dt, end - start] as :413-429 does), ``rstep`` (restart, :411);
 * ``output``: ``dir`` (output), ``makedir`` (False), ``compression`` (gzip)
@@ -30,7 +30,7 @@ then relative to the YAML file.  Keys of other goSPL subsystems (sediment,
 stratigraphy, flexure, ice, orography) are ignored; options that would
 change this path's arithmetic and that the library does not implement
 (sea-level curves, time-varying climate or tectonic events, horizontal
-tectonics, marine deposition with the TS solver or Gmar > 0) raise
+tectonics, marine deposition with the TS solver) raise
 ``ValueError``.
 """
 import os
@@ -141,9 +141,9 @@ def read_input(filename):
         p["picardSub"], p["picardIts"] = 10, 2
         p["nonlinKm"], p["clinSlp"], p["Gmar"], p["offshore"] = 10.0, 1.0e-6, 0.0, 100.0e5
 
-    if not p["nodep"] and p["seadepo"] and (p["marineSolver"] != "picard" or p["Gmar"] > 0.0):
-        raise ValueError("marine deposition (domain.seadepo) is built for diffusion.marineSolver: picard and "
-                         "Gmar = 0; set them, or domain.seadepo: False (continental deposition only)")
+    if not p["nodep"] and p["seadepo"] and p["marineSolver"] != "picard":
+        raise ValueError("marine deposition (domain.seadepo) is built for diffusion.marineSolver: picard; set it, "
+                         "or domain.seadepo: False (continental deposition only)")
 
     sea = inp.get("sea") or {}
     if "curve" in sea:

@@ -14,7 +14,7 @@
 * ``visModel()`` / ``readData()`` — WriteMesh (tools/outmesh.py): HDF5 and
   XDMF outputs every ``tout`` years and the restart from output ``rStep``
 * ``seaChange()``         — SEAMesh.seaChange (seaplex.py:738-861): marine
-  deposition (``seadepo``; Gmar = 0, marineSolver picard)
+  deposition (``seadepo``; marineSolver picard; the coupled system when Gmar > 0)
 * ``runProcesses()``      — the time loop of model.py:331-466 with
   ``fast: false``, continental deposition unless ``nodep`` and marine
   deposition when ``seadepo``.
@@ -115,9 +115,9 @@ class Model:
         # lake deposits of large deep depressions: marineSolver picard
         # (inputparser.py:564-580); goSPL's default adaptive TS is not built
         self.marineSolver = str(p.get("marineSolver", "ts")).lower()
-        if self.seadepo and (self.marineSolver != "picard" or self.Gmar > 0.0):
-            raise NotImplementedError("marine deposition is built for marineSolver picard and Gmar = 0 (goSPL's "
-                                      "adaptive TS solve and the coupled Gmar > 0 system are not)")
+        if self.seadepo and self.marineSolver != "picard":
+            raise NotImplementedError("marine deposition is built for marineSolver picard (goSPL's adaptive TS "
+                                      "solve is not)")
         self.nl_pit_K = float(p.get("nlPitK", p.get("nonlinKm", 10.0)))
         self.nl_pit_inlet_bias = min(1.0, max(0.0, float(p.get("pitInletBias", 0.5))))
         self.picardSub = int(p.get("picardSub", 10))
@@ -369,10 +369,10 @@ class Model:
         _lib.check(L.gs_sea_change(
             self._plan, _lib.ptr(self.hGlobal), _lib.ptr(self.cumED), _lib.ptr(self.EbLocal), _lib.ptr(self.xyz),
             self.xyz_box.ctypes.data_as(ctypes.c_void_p), _lib.ptr(self.edges), int(self.edges.shape[0]),
-            self.sealevel, self.oFill, self.dt, self.clinSlp, self.offshore, self.nlK, _lib.ptr(self.lFill),
-            _lib.ptr(self.vSed), _lib.ptr(self.sea_mask), ctypes.byref(st)))
+            self.sealevel, self.oFill, self.dt, self.clinSlp, self.offshore, self.nlK, self.Gmar,
+            _lib.ptr(self.lFill), _lib.ptr(self.vSed), _lib.ptr(self.sea_mask), ctypes.byref(st)))
         self.stats["sea"] = {"coast_points": st.npits, "marine_passes": st.cascade_passes,
-                             "epsfill_passes": st.fill_rounds}
+                             "epsfill_passes": st.fill_rounds, "coupled_applies": st.cg_iters}
 
     def sed_budget(self):
         """Sediment budget of the last sedChange (m3 over the step): where

@@ -308,7 +308,7 @@ int gs_sed_budget(gs_plan* plan, double* out16);
 
 /*
  * Marine deposition.  Replaces SEAMesh.seaChange (gospl/sed/seaplex.py:738-861)
- * for one lithology, no stratigraphy or provenance, Gmar = 0 and marineSolver
+ * for one lithology, no stratigraphy or provenance, and marineSolver
  * picard (the plan's lake-diffusion settings, gs_plan_set_lake_diffusion,
  * give picardSub and picardIts; nlk is nonlinKm): distance of the sea
  * vertices to the sea-level contour of h (_distanceCoasts, 51-135),
@@ -323,13 +323,21 @@ int gs_sed_budget(gs_plan* plan, double* out16);
  * `sea` is goSPL's seaID at this point (lFill <= sealevel of the last flow
  * direction built), `edges` the mesh's unique edges [nedge][2] (DEVICE),
  * `box` (HOST, 6 doubles) the vertices' bounding box as (lo, span).  stats:
- * npits = coastline points, cascade_passes = marine passes, fill_rounds =
- * epsfill relaxation passes.
+ * npits = coastline points, cascade_passes = marine passes (of the last
+ * cascade), fill_rounds = epsfill relaxation passes, cg_iters = GMRES
+ * operator applications of the coupled system.  gmar > 0 on a spherical mesh
+ * (_depMarineSystem, seaplex.py:240-402): the deposit of the first cascade
+ * feeds the coupled marine elevation / flux system [[I - G, -G dt/A],
+ * [A/dt, (I - W)^T]] [h; q] = [(1 - G) h; dep/dt + h A/dt] with
+ * G = min(gmar, 0.99) below sea level, W the marine receivers; its deposit
+ * (negatives dropped) goes down the cascade again.  The system is reduced to
+ * the elevation and solved by GMRES(30) to 1e-13, each application one
+ * ordered marine flow sweep.
  */
 int gs_sea_change(gs_plan* plan, double* h, double* cum_ed, double* eb, const double* xyz, const double* box,
                   const int32_t* edges, int64_t nedge, double sealevel, double ofill, double dt, double clinslp,
-                  double offshore, double nlk, const double* lfill, const double* vsed, const uint8_t* sea,
-                  gs_stats* stats);
+                  double offshore, double nlk, double gmar, const double* lfill, const double* vsed,
+                  const uint8_t* sea, gs_stats* stats);
 
 int gs_hillslope(gs_plan* plan, double* h, double* cum_ed, double* eb, double sealevel,
                  double cda, double cdm, double dt, double rtol, int32_t max_iter,

@@ -9,9 +9,10 @@ as in the continental tests, the live sea mask after sedChange must equal the
 oracle's seaID, and after seaChange the marine cascade must take the oracle's
 number of passes and elevation, cumED and EbLocal must agree to 1e-11 of the
 elevation scale (the oracle solves the smoothing and the Picard systems
-exactly, the GPU by CG to 1e-14 and 1e-13).  One free-running step is checked
-against the reference-generated fixtures.  The coupled Gmar > 0 system is not
-built: the model refuses it.
+exactly, the GPU by CG to 1e-14 and 1e-13).  ico2562_marine_G (Gmar = 0.5)
+adds the coupled marine elevation / flux system between two cascades (the
+oracle by sparse LU, the GPU by GMRES over ordered marine sweeps to 1e-13).
+One free-running step is checked against the reference-generated fixtures.
 """
 import numpy as np
 import pytest
@@ -21,7 +22,7 @@ from test_gpu_parity import _compare_dz, _compare_flow, _compare_sed, _gpu_model
 
 pytestmark = pytest.mark.gpu
 
-CASES = ["planar2k_marine", "ico2562_marine"]
+CASES = ["planar2k_marine", "ico2562_marine", "ico2562_marine_G"]
 
 
 @pytest.mark.parametrize("case", CASES)
@@ -62,6 +63,8 @@ def test_marine_stage_parity_from_identical_state(case):
         torch.cuda.synchronize()
         hs = float(np.abs(om.h).max())
         assert gm.stats["sea"]["marine_passes"] == om.marine_passes, (tag, gm.stats["sea"], om.marine_passes)
+        if om.Gmar > 0.0 and not om.flatModel:
+            assert gm.stats["sea"]["coupled_applies"] > 0, tag
         assert np.abs(_np(gm.hGlobal) - om.h).max() <= 1e-11 * hs, "%s sea h %g" % (
             tag, np.abs(_np(gm.hGlobal) - om.h).max() / hs)
         assert np.abs(_np(gm.cumED) - om.cumED).max() <= 1e-11 * hs, tag + " sea cumED"
@@ -93,9 +96,3 @@ def test_marine_matches_reference_golden_first_step(case):
     assert _rel(gm.hGlobal, g["s1_h"]) <= 1e-10
     gm.destroy()
 
-
-def test_coupled_marine_system_is_refused():
-    g = load_golden("ico2562_marine_G")
-    params = golden_params(g)
-    with pytest.raises(NotImplementedError):
-        _gpu_model(g, params)

@@ -65,12 +65,18 @@ def test_reads_the_path_keys(tmp_path):
     assert (q["nlPitK"], q["marineSolver"], q["picardSub"]) == (4.0, "picard", 3)
 
 
-def test_marine_deposition_is_refused(tmp_path):
-    """goSPL's default (nodep False, seadepo True) also runs marine deposition,
-    which this library does not implement: the input must switch it off."""
+def test_marine_deposition_needs_the_picard_solver(tmp_path):
+    """goSPL's default (nodep False, seadepo True) also runs marine deposition
+    with its adaptive TS solve of the marine diffusion, which this library
+    does not build: the input must choose marineSolver picard (any Gmar) or
+    switch marine deposition off."""
     y, _ = _write(tmp_path, YML.replace("    seadepo: False\n", ""))
     with pytest.raises(ValueError, match="seadepo"):
         read_input(str(y))
+    y, _ = _write(tmp_path, YML.replace("    seadepo: False\n", "").replace(
+        "    hillslopeKa: 0.01\n", "    hillslopeKa: 0.01\n    marineSolver: picard\n    Gmar: 0.5\n"))
+    _, _, _, p = read_input(str(y))
+    assert (p["seadepo"], p["marineSolver"], p["Gmar"]) == (True, "picard", 0.5)
     y, _ = _write(tmp_path, YML.replace("    nodep: False\n    seadepo: False\n", "    nodep: True\n"))
     assert read_input(str(y))[3]["nodep"] is True
 
