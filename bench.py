@@ -788,6 +788,7 @@ def run_sediment(args, dev):
     stream = torch.cuda.current_stream(dev)
     runs = {"picard": dict(nodep=False, marineSolver="picard"),
             "marine": dict(nodep=False, marineSolver="picard", seadepo=True),
+            "marine-Gmar0.5": dict(nodep=False, marineSolver="picard", seadepo=True, Gmar=0.5),
             "bottom-up": dict(nodep=False, nlPitVolume=float("inf")),
             "nodep": dict(nodep=True)}
     out = {}
