@@ -1061,9 +1061,9 @@ def step_algo_bytes(L):
 # under profiles/; scaled by the vertex count of the run.
 NCU_TRAFFIC_PER_VERTEX = {
     "k_mfd_receivers": (24.905728e6 + 2.152192e6) / 655362,
-    "k_ordered_flow": (34.788608e6 + 1.394944e6) / 655362,
+    "k_ordered_flow": (38.153216e6 + 1.851392e6) / 655362,
     "k_bfs_local": 1.788672e6 / 655362,
-    "k_relax_active": (9.614592e6 + 0.072192e6) / 655362,
+    "k_relax_active": (5.856768e6 + 0.024320e6) / 655362,
 }
 
 

@@ -680,13 +680,14 @@ int sea_change(gs_plan* p, double* h, double* cum_ed, double* eb, const double* 
 
     // 3. routing surface: smoothed bathymetry (spheres), sentinel cells
     const double* base = hl;
+    int smooth_iters = 0;
     if (!p->flat) {
         launch(p, k_smooth_rows, G, B, n, p->W, p->flat, sea, (const double*)p->larea, (const int*)p->nbr,
                (const int8_t*)p->nnb, (const double*)p->elen, (const double*)p->vdist, (const double*)p->farea,
                (const uint8_t*)p->outlet, p->sea_coef);
         GS_LAUNCH();
         GS_TRY(diffusion_solve_on(p, n, p->nbr, p->nnb, p->farea, p->dfix, p->flat, p->outlet, p->sea_coef, hl, hsm,
-                                  1.0e-14, 5000, nullptr));
+                                  1.0e-14, 5000, &smooth_iters));
         base = hsm;
     }
     unsigned long long* mk = p->u_scalar + 6;
@@ -820,6 +821,7 @@ int sea_change(gs_plan* p, double* h, double* cum_ed, double* eb, const double* 
         st->fill_rounds = passes;
         st->npits = m;
         st->cg_iters = gm_applies;
+        st->flat_rounds = smooth_iters;
     }
     return GS_OK;
 }

@@ -372,7 +372,8 @@ class Model:
             self.sealevel, self.oFill, self.dt, self.clinSlp, self.offshore, self.nlK, self.Gmar,
             _lib.ptr(self.lFill), _lib.ptr(self.vSed), _lib.ptr(self.sea_mask), ctypes.byref(st)))
         self.stats["sea"] = {"coast_points": st.npits, "marine_passes": st.cascade_passes,
-                             "epsfill_passes": st.fill_rounds, "coupled_applies": st.cg_iters}
+                             "epsfill_passes": st.fill_rounds, "smoothing_cg_iters": st.flat_rounds,
+                             "coupled_applies": st.cg_iters}
 
     def sed_budget(self):
         """Sediment budget of the last sedChange (m3 over the step): where

@@ -324,8 +324,9 @@ int gs_sed_budget(gs_plan* plan, double* out16);
  * direction built), `edges` the mesh's unique edges [nedge][2] (DEVICE),
  * `box` (HOST, 6 doubles) the vertices' bounding box as (lo, span).  stats:
  * npits = coastline points, cascade_passes = marine passes (of the last
- * cascade), fill_rounds = epsfill relaxation passes, cg_iters = GMRES
- * operator applications of the coupled system.  gmar > 0 on a spherical mesh
+ * cascade), fill_rounds = epsfill relaxation passes, flat_rounds = CG
+ * iterations of the bathymetry smoothing, cg_iters = GMRES operator
+ * applications of the coupled system.  gmar > 0 on a spherical mesh
  * (_depMarineSystem, seaplex.py:240-402): the deposit of the first cascade
  * feeds the coupled marine elevation / flux system [[I - G, -G dt/A],
  * [A/dt, (I - W)^T]] [h; q] = [(1 - G) h; dep/dt + h A/dt] with
