@@ -320,7 +320,7 @@ __global__ void __launch_bounds__(256, 4) k_cg_coop(int n, const int* __restrict
                                                     const uint8_t* __restrict__ fix, const double* __restrict__ x0,
                                                     double* x, double* b, double* r, double* z, double* p0, double* p1,
                                                     double* ap, double* part, double rtol, int max_iter, int* it_out,
-                                                    double* res_out) {
+                                                    double* res_out, const double* __restrict__ guess) {
     cg::grid_group grid = cg::this_grid();
     const int nb = gridDim.x, blk = blockIdx.x;
     const int gtid = blk * blockDim.x + threadIdx.x, gsz = nb * blockDim.x;
@@ -329,18 +329,21 @@ __global__ void __launch_bounds__(256, 4) k_cg_coop(int n, const int* __restrict
     double* pb = part + 5 * nb;    // r.z, r.r [2 nb]
     double a0 = 0.0, a1 = 0.0, a2 = 0.0;
     for (int k = gtid; k < n; k += gsz) {
-        const double xk = x0[k];
-        x[k] = xk;
+        const double x0k = x0[k];
         if (fix[k]) {
+            x[k] = x0k;
             b[k] = 0.0;
             r[k] = 0.0;
             z[k] = 0.0;
             p0[k] = 0.0;
             continue;
         }
+        // the start: x0 (the right-hand side), or the guess on free rows
+        const double xk = guess ? guess[k] : x0k;
+        x[k] = xk;
         const int deg = nnb[k];
         const double ck = coef[k];
-        double bk = xk;
+        double bk = x0k;
         double y = ck * xk;
 #pragma unroll
         for (int s = 0; s < MAXW; s++) {
@@ -349,8 +352,9 @@ __global__ void __launch_bounds__(256, 4) k_cg_coop(int n, const int* __restrict
                 const int j = nbr[(size_t)s * n + k];
                 if (o != 0.0 && j >= 0) {
                     const double xj = x0[j];
+                    const double gj = guess ? guess[j] : xj;
                     if (fix[j]) bk = bk - o * xj;
-                    else y = y + o * xj;
+                    else y = y + o * gj;
                 }
             }
         }
@@ -391,9 +395,16 @@ __global__ void __launch_bounds__(256, 4) k_cg_coop(int n, const int* __restrict
                     if (s < deg) {
                         const double o = coef[(size_t)(s + 1) * n + k];
                         const int j = nbr[(size_t)s * n + k];
-                        if (o != 0.0 && j >= 0 && !fix[j]) {
-                            const double pj = it ? z[j] + beta * pcur[j] : pcur[j];
-                            y = y + o * pj;
+                        if (o != 0.0 && j >= 0) {
+                            // the fixed flag and the values are loaded together
+                            // (not the values after the flag): one round trip
+                            const bool fj = fix[j] != 0;
+                            const double zj = it ? z[j] : 0.0;
+                            const double qj = pcur[j];
+                            if (!fj) {
+                                const double pj = it ? zj + beta * qj : qj;
+                                y = y + o * pj;
+                            }
                         }
                     }
                 }
@@ -674,10 +685,11 @@ int hillslope(gs_plan* p, double* h, double* cum_ed, double* eb, double sealevel
         int nn = n, mi = max_iter;
         double rt = rtol;
         const double* x0 = hold;
+        const double* guess = nullptr;
         void* args[] = {(void*)&nn, (void*)&p->nbr, (void*)&p->nnb, (void*)&p->dcoef, (void*)&p->farea,
                         (void*)&p->dfix, (void*)&x0, (void*)&p->cg_x, (void*)&p->cg_b, (void*)&p->cg_r,
                         (void*)&p->cg_z, (void*)&p->cg_p, (void*)&p->cg_p2, (void*)&p->cg_ap, (void*)&p->red,
-                        (void*)&rt, (void*)&mi, (void*)&it_d, (void*)&res_d};
+                        (void*)&rt, (void*)&mi, (void*)&it_d, (void*)&res_d, (void*)&guess};
         cudaEvent_t stop = nullptr;
         if (p->profiling) prof_begin(p, (const void*)k_cg_coop, &stop);
         GS_CUDA(cudaLaunchCooperativeKernel((const void*)k_cg_coop, p->coop_blocks, 256, args, 0, p->stream));
@@ -714,7 +726,7 @@ int hillslope(gs_plan* p, double* h, double* cum_ed, double* eb, double sealevel
 // the sediment step.
 int diffusion_solve_on(gs_plan* p, int m, const int* nbr, const int8_t* nnb, const double* farea, const uint8_t* fix,
                        int flat, const uint8_t* outlet, const double* coef, const double* rhs, double* x, double rtol,
-                       int max_iter, int* iters) {
+                       int max_iter, int* iters, const double* guess) {
     const int n = m;
     if (n == 0) return GS_OK;
     const int B = 256, G = grid_for(n, B);
@@ -730,7 +742,7 @@ int diffusion_solve_on(gs_plan* p, int m, const int* nbr, const int8_t* nnb, con
         void* args[] = {(void*)&nn, (void*)&nbr, (void*)&nnb, (void*)&cf, (void*)&farea,
                         (void*)&fix, (void*)&rhs, (void*)&p->cg_x, (void*)&p->cg_b, (void*)&p->cg_r,
                         (void*)&p->cg_z, (void*)&p->cg_p, (void*)&p->cg_p2, (void*)&p->cg_ap, (void*)&p->red,
-                        (void*)&rt, (void*)&mi, (void*)&it_d, (void*)&res_d};
+                        (void*)&rt, (void*)&mi, (void*)&it_d, (void*)&res_d, (void*)&guess};
         cudaEvent_t stop = nullptr;
         if (p->profiling) prof_begin(p, (const void*)k_cg_coop, &stop);
         GS_CUDA(cudaLaunchCooperativeKernel((const void*)k_cg_coop, p->coop_blocks, 256, args, 0, p->stream));

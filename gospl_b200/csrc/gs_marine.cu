@@ -686,8 +686,16 @@ int sea_change(gs_plan* p, double* h, double* cum_ed, double* eb, const double* 
                (const int8_t*)p->nnb, (const double*)p->elen, (const double*)p->vdist, (const double*)p->farea,
                (const uint8_t*)p->outlet, p->sea_coef);
         GS_LAUNCH();
+        // warm start from the last smoothing of this mesh: the residual
+        // starts at the elevation change of a step, not at L h
+        if (!p->sea_prev) {
+            GS_CUDA(cudaMalloc((void**)&p->sea_prev, sizeof(double) * N));
+            p->sea_prev_ok = 0;
+        }
         GS_TRY(diffusion_solve_on(p, n, p->nbr, p->nnb, p->farea, p->dfix, p->flat, p->outlet, p->sea_coef, hl, hsm,
-                                  1.0e-14, 5000, &smooth_iters));
+                                  1.0e-14, 5000, &smooth_iters, p->sea_prev_ok ? (const double*)p->sea_prev : nullptr));
+        GS_CUDA(cudaMemcpyAsync(p->sea_prev, hsm, sizeof(double) * N, cudaMemcpyDeviceToDevice, p->stream));
+        p->sea_prev_ok = 1;
         base = hsm;
     }
     unsigned long long* mk = p->u_scalar + 6;

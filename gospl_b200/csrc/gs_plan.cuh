@@ -37,6 +37,8 @@ struct gs_plan {
     double* sea_coef = nullptr;          // [W+1][n] bathymetry smoothing operator
     double* sea_pts = nullptr;           // coastline points, sorted copies, keys and boxes
     int64_t sea_pts_cap = 0;             // edges the coastline buffers hold
+    double* sea_prev = nullptr;          // [n] the last smoothed bathymetry (start of the next smoothing)
+    int sea_prev_ok = 0;                 // sea_prev holds a smoothing of this plan's mesh
     size_t sea_sort_bytes = 0;           // sort scratch at the end of sea_pts
     double* led_part = nullptr;          // [5][LED_NB] block partial sums of the budget reductions
     double* sed_coef = nullptr;          // [W+1][n] lake diffusion operator (compacted to the lake cells)
@@ -332,9 +334,10 @@ int sea_change(gs_plan* p, double* h, double* cum_ed, double* eb, const double* 
                const uint8_t* sea, gs_stats* st);
 int picard_diffuse(gs_plan* p, const uint8_t* lmask, const double* zb, double* hcur, double K, double dt,
                    double* cd, double* hstart);
+// guess: start of the free rows (nullptr: the right-hand side)
 int diffusion_solve_on(gs_plan* p, int m, const int* nbr, const int8_t* nnb, const double* farea, const uint8_t* fix,
                        int flat, const uint8_t* outlet, const double* coef, const double* rhs, double* x, double rtol,
-                       int max_iter, int* iters);
+                       int max_iter, int* iters, const double* guess = nullptr);
 int hillslope(gs_plan* p, double* h, double* cum_ed, double* eb, double sealevel, double cda,
               double cdm, double dt, double rtol, int max_iter, gs_stats* st);
 int apply_forces(gs_plan* p, double* h, const double* rain, const double* upsub, double dt,
@@ -354,7 +357,7 @@ __global__ void k_cg_coop(int n, const int* __restrict__ nbr, const int8_t* __re
                           const double* __restrict__ coef, const double* __restrict__ farea,
                           const uint8_t* __restrict__ fix, const double* __restrict__ x0, double* x, double* b,
                           double* r, double* z, double* p0, double* p1, double* ap, double* part, double rtol,
-                          int max_iter, int* it_out, double* res_out);
+                          int max_iter, int* it_out, double* res_out, const double* guess);
 int set_members(gs_plan* p, int nmem, const int64_t* start, const double* maxarea);
 int plan_tune(gs_plan* p, int knob, int value);
 int precision_buffers(gs_plan* p);
