@@ -1220,6 +1220,7 @@ int fill_join(gs_plan* p, gs_stats* st) {
     GS_CUDA(cudaStreamWaitEvent(p->stream, p->ev_b, 0));
     GS_CUDA(cudaEventSynchronize(p->ev_b));
     if (st) st->flat_rounds = p->h_pinned[2];
+    p->pdir_bound = p->h_pinned[2] + 2;   // the deepest distance is the BFS depth
     return GS_OK;
 }
 
@@ -1371,6 +1372,7 @@ int fill_elevation(gs_plan* p, const double* h, double sealevel, double ofill, d
     // the sea reset of lFill in k_flat_dirs touches open-sea cells, which
     // hold no pit.
     GS_CUDA(cudaMemsetAsync(p->i_scalar + I_NEXT, 0, sizeof(int), p->stream));
+    p->pdir_bound = 0;
     launch(p, k_bfs_init, G, B, n, (const int*)p->spill_flag, p->pdir, p->front0, p->i_scalar + I_NEXT);
     // the reachable set is compacted before the seed count is read, so one
     // synchronisation gives both (the compaction is wasted only without pits)
@@ -1393,12 +1395,42 @@ int fill_elevation(gs_plan* p, const double* h, double sealevel, double ofill, d
     GS_CUDA(cudaMemcpyAsync(&last[4], p->pflag + n - 1, sizeof(int), cudaMemcpyDeviceToHost, p->stream));
     GS_CUDA(cudaStreamSynchronize(p->stream));
     const int ncell = last[3] + last[4];
+    // pit cells sorted by (pit, id): segments for the per-pit reductions.
+    // The ordered compaction (before the BFS) keeps id order; the stable
+    // radix sort by pit then lists every pit's cells in increasing id.
+    auto pit_tables = [&]() -> int {
+        if (ncell > 0) {
+            int bits = 1;
+            while ((1 << bits) <= P && bits < 31) bits++;
+            size_t bytes = p->cub_bytes;
+            GS_CUDA(cub::DeviceRadixSort::SortPairs(p->cub_tmp, bytes, p->seg_keys, p->seg_keys2, p->seg_vals,
+                                                    p->seg_vals2, ncell, 0, bits, p->stream));
+            p->launches++;
+        }
+        GS_TRY(exclusive_scan(p, p->seg_count, p->seg_start, np1));
+        launch(p, k_pit_params, np1, 256, np1, (const int*)p->seg_start,
+               (const int*)p->seg_count, (const int*)p->seg_vals2, (const double*)lfill, h, clip_sl,
+               (const double*)p->larea, p->pit_params);
+        launch(p, k_filled_lvl, grid_for(np1, B), B, np1, (const double*)p->pit_params, p->filled_lvl);
+        launch(p, k_filled_vol, np1, 256, np1, (const int*)p->seg_start,
+               (const int*)p->seg_count, (const int*)p->seg_vals2, h, clip_sl, (const double*)p->farea,
+               (const double*)p->filled_lvl, (const double*)p->pit_params, p->filled_vol);
+        GS_LAUNCH();
+        return GS_OK;
+    };
+    // Without sediment the pit tables go first on the main stream, so that its
+    // sort is queued before the host spends time queueing the flat pass on
+    // side_b: the pit cells are above sea level and the flat pass rewrites
+    // lFill only at open-sea cells, so the two read and write disjoint data.
+    // The flat pass forks from here: it needs the compaction above, not the
+    // pit tables.
+    GS_CUDA(cudaEventRecord(p->ev_fork_b, p->stream));
+    if (!sed) GS_TRY(pit_tables());
     int fsize = last[2], levels = 0;
     bool forked = false;
     if (fsize > 0) {
         const int M = last[0] + last[1];
         if (true) {
-            GS_CUDA(cudaEventRecord(p->ev_fork_b, p->stream));
             GS_CUDA(cudaStreamWaitEvent(p->side_b, p->ev_fork_b, 0));
             {
                 StreamSwap sw(p, p->side_b, nullptr);
@@ -1457,6 +1489,7 @@ int fill_elevation(gs_plan* p, const double* h, double sealevel, double ofill, d
     }
     if (!forked) {
         if (st) st->flat_rounds = levels;
+        p->pdir_bound = levels + 2;
         launch(p, k_flat_dirs, G, B, n, (const double*)lfill, (const int*)pit_ids, (const int*)p->pdir,
                (const int*)p->nbr, (const int8_t*)p->nnb, (const int*)p->spill_flag, sealevel, h,
                flat_dirs, lfill);
@@ -1466,29 +1499,10 @@ int fill_elevation(gs_plan* p, const double* h, double sealevel, double ofill, d
     // With sediment the open-sea reset of lFill in k_flat_dirs touches pit
     // cells (marine depressions are labelled), and the pit tables read the
     // reset lFill (pitfilling.py:820-846): join the BFS first.
-    if (sed) GS_TRY(fill_join(p, st));
-
-    // pit cells sorted by (pit, id): segments for the per-pit reductions.
-    // The ordered compaction (before the BFS) keeps id order; the stable
-    // radix sort by pit then lists every pit's cells in increasing id.
-    if (ncell > 0) {
-        int bits = 1;
-        while ((1 << bits) <= P && bits < 31) bits++;
-        size_t bytes = p->cub_bytes;
-        GS_CUDA(cub::DeviceRadixSort::SortPairs(p->cub_tmp, bytes, p->seg_keys, p->seg_keys2, p->seg_vals,
-                                                p->seg_vals2, ncell, 0, bits, p->stream));
-        p->launches++;
+    if (sed) {
+        GS_TRY(fill_join(p, st));
+        GS_TRY(pit_tables());
     }
-    GS_TRY(exclusive_scan(p, p->seg_count, p->seg_start, np1));
-    // pit tables
-    launch(p, k_pit_params, np1, 256, np1, (const int*)p->seg_start,
-           (const int*)p->seg_count, (const int*)p->seg_vals2, (const double*)lfill, h, clip_sl,
-           (const double*)p->larea, p->pit_params);
-    launch(p, k_filled_lvl, grid_for(np1, B), B, np1, (const double*)p->pit_params, p->filled_lvl);
-    launch(p, k_filled_vol, np1, 256, np1, (const int*)p->seg_start,
-           (const int*)p->seg_count, (const int*)p->seg_vals2, h, clip_sl, (const double*)p->farea,
-           (const double*)p->filled_lvl, (const double*)p->pit_params, p->filled_vol);
-    GS_LAUNCH();
     if (!defer_flats) GS_TRY(fill_join(p, st));
     return GS_OK;
 }

@@ -97,6 +97,7 @@ struct gs_plan {
     int* order_i = nullptr;              // order of the snapshot (unfilled) flow graph
     int order_i_valid = 0;
     int tie_m = 0;                       // vertices in surface tie groups of the last flow_order
+    int pdir_bound = 0;                  // pdir + 1 <= pdir_bound after the last fill (0: unknown)
     unsigned long long* okey = nullptr;
     unsigned long long* okey2 = nullptr;
     unsigned* ok32 = nullptr;

@@ -874,15 +874,18 @@ __global__ void k_tie_runs(int n, const unsigned long long* __restrict__ skey, i
     flag[t] = (first && last) ? 0 : 1;
 }
 
-// tie members as (run start, descending flat distance) keys, in position order
+// tie members as (run start, descending flat distance) keys, in position
+// order: the low pb bits hold (2^pb - 1) - (pdir + 1), pdir + 1 < 2^pb
+template <class K>
 __global__ void k_tie_compact(int n, const int* __restrict__ run, const int* __restrict__ flag,
                               const int* __restrict__ scan, const int* __restrict__ order,
-                              const int* __restrict__ pdir, unsigned long long* ckey, int* cval, int* cpos) {
+                              const int* __restrict__ pdir, int pb, K* ckey, int* cval, int* cpos) {
     int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= n || !flag[t]) return;
     const int j = scan[t];
     const int v = order[t];
-    ckey[j] = ((unsigned long long)(unsigned)run[t] << 32) | (unsigned long long)(~(unsigned)(pdir[v] + 1));
+    const unsigned long long lo = ((1ULL << pb) - 1ULL) - (unsigned long long)(unsigned)(pdir[v] + 1);
+    ckey[j] = (K)((((unsigned long long)(unsigned)run[t]) << pb) | lo);
     cval[j] = v;
     cpos[j] = t;
 }
@@ -944,13 +947,37 @@ static int order_ties_finish(gs_plan* p, const int* pdir, int* order) {
     int* cval = p->oval;
     int* cval2 = (int*)p->ok32b;   // run is consumed by the compaction before the sort writes here
     int* cpos = p->pos;            // rewritten by the positions pass that follows
-    launch(p, k_tie_compact, G, B, n, run, flag, scan, (const int*)order, pdir, p->okey, cval, cpos);
-    GS_LAUNCH();
     int hb = 1;
     while ((1LL << hb) <= (long long)n && hb < 31) hb++;
-    size_t bytes = p->cub_bytes;
-    GS_CUDA(cub::DeviceRadixSort::SortPairs(p->cub_tmp, bytes, p->okey, p->okey2, cval, cval2, m, 0, 32 + hb,
-                                            p->stream));
+    // the flat distances of the plan's last fill are bounded by its BFS depth:
+    // then the keys need only hb + pb bits, mostly 32 or fewer (half the key
+    // bytes and about half the radix passes of the general 64-bit layout)
+    int pb = 32;
+    if (pdir == p->pdir && p->pdir_bound > 0) {
+        pb = 1;
+        while ((1LL << pb) <= (long long)p->pdir_bound + 1 && pb < 32) pb++;
+    }
+    size_t need32 = 0;
+    if (hb + pb <= 32)
+        GS_CUDA(cub::DeviceRadixSort::SortPairs((void*)nullptr, need32, (const unsigned*)nullptr, (unsigned*)nullptr,
+                                                (const int*)nullptr, (int*)nullptr, m, 0, hb + pb, p->stream));
+    if (hb + pb <= 32 && need32 <= p->cub_bytes) {
+        unsigned* k32 = reinterpret_cast<unsigned*>(p->okey);
+        unsigned* k32b = reinterpret_cast<unsigned*>(p->okey2);
+        launch(p, k_tie_compact<unsigned>, G, B, n, run, flag, scan, (const int*)order, pdir, pb, k32, cval, cpos);
+        GS_LAUNCH();
+        size_t bytes = p->cub_bytes;
+        GS_CUDA(cub::DeviceRadixSort::SortPairs(p->cub_tmp, bytes, (const unsigned*)k32, k32b, (const int*)cval,
+                                                cval2, m, 0, hb + pb, p->stream));
+    } else {
+        pb = 32;
+        launch(p, k_tie_compact<unsigned long long>, G, B, n, run, flag, scan, (const int*)order, pdir, pb, p->okey,
+               cval, cpos);
+        GS_LAUNCH();
+        size_t bytes = p->cub_bytes;
+        GS_CUDA(cub::DeviceRadixSort::SortPairs(p->cub_tmp, bytes, p->okey, p->okey2, cval, cval2, m, 0, 32 + hb,
+                                                p->stream));
+    }
     p->launches++;
     launch(p, k_tie_scatter, grid_for(m, B), B, m, (const int*)cpos, (const int*)cval2, order);
     GS_LAUNCH();
