@@ -49,7 +49,7 @@ __device__ __forceinline__ int agg_append(int* cnt) {
 }
 
 enum { D_MINH = 0, D_LEVEL = 1 };
-enum { I_CHANGED = 0, I_NEXT = 1, I_NPITS0 = 2, I_NPITS = 3, I_NONFINITE = 13 };
+enum { I_CHANGED = 0, I_NEXT = 1, I_XRAW = 2, I_XDEDUP = 3, I_NONFINITE = 13 };
 
 // --------------------------------------------------------------------------
 // reductions
@@ -905,62 +905,135 @@ __global__ void __launch_bounds__(256) k_bfs_coop(int* fa, int* fb, int* sizes, 
     if (threadIdx.x == 0) *levels_out = levels;
 }
 
-// Minimax relaxation over the basin graph in one cooperative launch, edge-
-// parallel: round r relaxes the edges whose source basin was lowered in round
-// r-1 or later (stamp[v] >= r - 1; seed basins carry stamp 0), so every round
-// reads every edge's source once but does the level work only for the active
-// ones.  Lowered basins get stamp r.  Rounds end when none changed (three
-// rotating change flags: round r sets flags[r % 3], reads it after the
-// barrier and clears flags[(r + 1) % 3]); the fixed point is that of the all-edges
-// relaxation, whatever the order of the updates.
-__global__ void k_basin_stamp(int n, const unsigned long long* __restrict__ L, int* stamp) {
-    int v = blockIdx.x * blockDim.x + threadIdx.x;
-    if (v < n) stamp[v] = (L[v] != ~0ULL) ? 0 : -1;
+// Basin-graph edges deduplicated: k_cross_edges emits one edge per boundary
+// cell and neighbouring basin, so a pair of basins is joined by as many
+// parallel edges as it has boundary cells (about twelve per pair on the
+// sphere's relief).  Only the lowest of them can lower a level, so the edges
+// go through an open-addressing table keyed by (u, v) that keeps the smallest
+// weight key, and the relaxation runs over one edge per pair.  The table has
+// a power-of-two size of at least twice the edge count (linear probing ends
+// at an empty slot within the table size); when the edges outnumber half the
+// table, the relaxation uses them undeduplicated (*raw = 1).
+__device__ __forceinline__ unsigned long long xh_mix(unsigned long long k) {
+    // the 64-bit finaliser of MurmurHash3 (Appleby)
+    k ^= k >> 33;
+    k *= 0xff51afd7ed558ccdULL;
+    k ^= k >> 33;
+    k *= 0xc4ceb9fe1a85ec53ULL;
+    k ^= k >> 33;
+    return k;
 }
 
-constexpr int RELAX_EDGES = 16;
+__global__ void k_xedge_insert(const int* __restrict__ m_count, int cap, const int* __restrict__ xu,
+                               const int* __restrict__ xv, const double* __restrict__ xw,
+                               unsigned long long* hkey, unsigned long long* hval, long long hcap, int* raw) {
+    const int m = *m_count < cap ? *m_count : cap;
+    if (2LL * m > hcap) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) *raw = 1;
+        return;
+    }
+    const int gtid = blockIdx.x * blockDim.x + threadIdx.x, gsz = gridDim.x * blockDim.x;
+    const unsigned long long mask = (unsigned long long)hcap - 1ULL;
+    for (int e = gtid; e < m; e += gsz) {
+        const unsigned long long key = ((unsigned long long)(unsigned)xu[e] << 32) | (unsigned)xv[e];
+        const unsigned long long w = dkey(xw[e]);
+        unsigned long long s = xh_mix(key) & mask;
+        for (long long probe = 0; probe < hcap; probe++) {
+            const unsigned long long k = atomicCAS(&hkey[s], ~0ULL, key);
+            if (k == ~0ULL || k == key) {
+                atomicMin(&hval[s], w);
+                break;
+            }
+            s = (s + 1ULL) & mask;
+        }
+    }
+}
+
+// table -> edge list (any order: the relaxation's fixed point does not depend
+// on it); every used slot is emptied again for the next fill
+__global__ void k_xedge_compact(long long hcap, unsigned long long* hkey, unsigned long long* hval, int* du, int* dv,
+                                unsigned long long* dw, int* count) {
+    const long long gtid = (long long)blockIdx.x * blockDim.x + threadIdx.x, gsz = (long long)gridDim.x * blockDim.x;
+    for (long long s = gtid; s < hcap; s += gsz) {
+        const unsigned long long k = hkey[s];
+        if (k == ~0ULL) continue;
+        const int pos = agg_append(count);
+        du[pos] = (int)(k >> 32);
+        dv[pos] = (int)(unsigned)(k & 0xffffffffULL);
+        dw[pos] = hval[s];
+        hkey[s] = ~0ULL;
+        hval[s] = ~0ULL;
+    }
+}
+
+// Minimax relaxation over the basin graph in one cooperative launch:
+// L[u] = min(L[u], max(w, L[v])) over the edges v -> u until nothing
+// changes.  A thread keeps its first RELAX_REG edges (u, v, weight and the
+// level of v it last used) in registers for the whole launch, and between two
+// grid barriers relaxes them RELAX_SUB times, each time only when the level
+// of v changed since it last relaxed that edge: a lowered level travels along
+// a chain of basins within one round instead of one basin per round.  Edges
+// beyond the registers are relaxed once per round.  A round ends with a grid
+// barrier and continues while any level changed in it (three rotating change
+// flags: round r sets flags[r % 3], reads it after the barrier and clears
+// flags[(r + 1) % 3]).  Levels only decrease and a round without any change
+// used only final levels, so the result is the fixed point of the all-edges
+// relaxation whatever the order of the updates.
+constexpr int RELAX_REG = 2;
+constexpr int RELAX_SUB = 8;
 
 __global__ void __launch_bounds__(256) k_relax_active(const int* __restrict__ m_count, int cap,
-                                                      const int* __restrict__ xu, const int* __restrict__ xv,
-                                                      const double* __restrict__ xw, unsigned long long* L,
-                                                      int* stamp, int* flags, int max_rounds, int* rounds_out) {
+                                                      const int* __restrict__ raw_p, const int* __restrict__ xu,
+                                                      const int* __restrict__ xv, const double* __restrict__ xw,
+                                                      const int* __restrict__ md_count, const int* __restrict__ du,
+                                                      const int* __restrict__ dv,
+                                                      const unsigned long long* __restrict__ dw,
+                                                      unsigned long long* L, int* flags, int max_rounds,
+                                                      int* rounds_out) {
     cg::grid_group grid = cg::this_grid();
-    // edge count as k_cross_edges left it (its appends stop at the capacity)
-    const int m = *m_count < cap ? *m_count : cap;
+    const bool raw = *raw_p != 0;
+    // raw: the edge count as k_cross_edges left it (its appends stop at the capacity)
+    const int m = raw ? (*m_count < cap ? *m_count : cap) : *md_count;
     const int gtid = blockIdx.x * blockDim.x + threadIdx.x, gsz = gridDim.x * blockDim.x;
+    int cu[RELAX_REG], cv[RELAX_REG];
+    unsigned long long cw[RELAX_REG], last[RELAX_REG];
+#pragma unroll
+    for (int q = 0; q < RELAX_REG; q++) {
+        const int e = gtid + q * gsz;
+        cv[q] = -1;
+        cu[q] = 0;
+        cw[q] = 0ULL;
+        last[q] = ~0ULL;
+        if (e < m) {
+            cu[q] = raw ? xu[e] : du[e];
+            cv[q] = raw ? xv[e] : dv[e];
+            cw[q] = raw ? dkey(xw[e]) : dw[e];
+        }
+    }
+    volatile unsigned long long* VL = L;
     int r = 1;
     for (; r <= max_rounds; r++) {
         int changed = 0;
-        // RELAX_EDGES edges per thread and pass: their source ids and stamps
-        // are loaded before any is used, so the gathers overlap and a round
-        // over the whole edge list costs about two memory round trips
-        constexpr int RE = RELAX_EDGES;
-        for (int e0 = gtid; e0 < m; e0 += RE * gsz) {
-            int v[RE], sv[RE];
+        for (int sub = 0; sub < RELAX_SUB; sub++) {
+            unsigned long long lv[RELAX_REG];
 #pragma unroll
-            for (int q = 0; q < RE; q++) {
-                const int e = e0 + q * gsz;
-                v[q] = e < m ? xv[e] : -1;
+            for (int q = 0; q < RELAX_REG; q++) lv[q] = cv[q] >= 0 ? VL[cv[q]] : ~0ULL;
+#pragma unroll
+            for (int q = 0; q < RELAX_REG; q++) {
+                if (lv[q] == ~0ULL || lv[q] == last[q]) continue;
+                last[q] = lv[q];
+                const unsigned long long cand = cw[q] > lv[q] ? cw[q] : lv[q];
+                if (cand < atomicMin(&L[cu[q]], cand)) changed = 1;
             }
-#pragma unroll
-            for (int q = 0; q < RE; q++) sv[q] = v[q] >= 0 ? ((volatile int*)stamp)[v[q]] : -2;
-#pragma unroll
-            for (int q = 0; q < RE; q++) {
-                if (sv[q] < r - 1) continue;
-                const int e = e0 + q * gsz;
-                const unsigned long long lv = ((volatile unsigned long long*)L)[v[q]];
-                if (lv == ~0ULL) continue;
-                const unsigned long long w = dkey(xw[e]);
-                const unsigned long long cand = w > lv ? w : lv;
-                const int u = xu[e];
-                if (cand < ((volatile unsigned long long*)L)[u]) {
-                    const unsigned long long old = atomicMin(&L[u], cand);
-                    if (cand < old) {
-                        ((volatile int*)stamp)[u] = r;
-                        changed = 1;
-                    }
-                }
-            }
+        }
+        for (int e = gtid + RELAX_REG * gsz; e < m; e += gsz) {
+            const int v = raw ? xv[e] : dv[e];
+            const unsigned long long lv = VL[v];
+            if (lv == ~0ULL) continue;
+            const unsigned long long w = raw ? dkey(xw[e]) : dw[e];
+            const unsigned long long cand = w > lv ? w : lv;
+            const int u = raw ? xu[e] : du[e];
+            if (cand < VL[u] && cand < atomicMin(&L[u], cand)) changed = 1;
         }
         if (__any_sync(0xffffffffu, changed) && (threadIdx.x & 31) == 0) flags[r % 3] = 1;
         // clear the flag of the next round: its last readers (end of round
@@ -1293,17 +1366,31 @@ int fill_elevation(gs_plan* p, const double* h, double sealevel, double ofill, d
            p->xe_w, p->i_scalar + I_NEXT, p->xe_cap);
     GS_LAUNCH();
     {
-        // the edge count stays on the device: the relaxation reads it, and the
-        // host checks it against the capacity at the next synchronisation
-        launch(p, k_basin_stamp, G, B, n, (const unsigned long long*)p->basinL, p->comp);
-        GS_CUDA(cudaMemsetAsync(p->i_scalar + 5, 0, sizeof(int) * 3, p->stream));
-        GS_LAUNCH();
+        // the edge count stays on the device: the deduplication and the
+        // relaxation read it, and the host checks it against the capacity at
+        // the next synchronisation
         const int* mc = p->i_scalar + I_NEXT;
         int cap = (int)std::min<int64_t>(p->xe_cap, INT_MAX), maxr = 1000000;
+        int* raw = p->i_scalar + I_XRAW;
+        int* mdc = p->i_scalar + I_XDEDUP;
+        GS_CUDA(cudaMemsetAsync(p->i_scalar + I_XRAW, 0, sizeof(int) * 2, p->stream));
+        GS_CUDA(cudaMemsetAsync(p->i_scalar + 5, 0, sizeof(int) * 3, p->stream));
+        if (p->xh_cap > 0) {
+            launch(p, k_xedge_insert, p->sm_count * 8, 256, mc, cap, (const int*)p->xe_u, (const int*)p->xe_v,
+                   (const double*)p->xe_w, p->xh_key, p->xh_val, (long long)p->xh_cap, raw);
+            launch(p, k_xedge_compact, p->sm_count * 8, 256, (long long)p->xh_cap, p->xh_key, p->xh_val, p->xd_u,
+                   p->xd_v, p->xd_w, mdc);
+            GS_LAUNCH();
+        } else {
+            // no table yet (first fill of the plan): the undeduplicated edges
+            launch(p, k_fill_int, 1, 32, 1, raw, 1);
+            GS_LAUNCH();
+        }
         int* flags = p->i_scalar + 5;
         int* rout = p->i_scalar + I_CHANGED;
-        void* args[] = {(void*)&mc, (void*)&cap, (void*)&p->xe_u, (void*)&p->xe_v, (void*)&p->xe_w,
-                        (void*)&p->basinL, (void*)&p->comp, (void*)&flags, (void*)&maxr, (void*)&rout};
+        void* args[] = {(void*)&mc,       (void*)&cap,      (void*)&raw,       (void*)&p->xe_u, (void*)&p->xe_v,
+                        (void*)&p->xe_w,  (void*)&mdc,      (void*)&p->xd_u,   (void*)&p->xd_v, (void*)&p->xd_w,
+                        (void*)&p->basinL, (void*)&flags,   (void*)&maxr,      (void*)&rout};
         GS_TRY(launch_coop(p, (const void*)k_relax_active, args));
         GS_CUDA(cudaMemcpyAsync(p->h_pinned + 6, p->i_scalar + I_CHANGED, sizeof(int), cudaMemcpyDeviceToHost,
                                 p->stream));
@@ -1347,6 +1434,32 @@ int fill_elevation(gs_plan* p, const double* h, double sealevel, double ofill, d
     if ((int64_t)p->h_pinned[7] > p->xe_cap) {
         set_error(GS_ENOMEM, "pit fill: cross-edge capacity exceeded");
         return GS_ENOMEM;
+    }
+    // size the deduplication table for the next fill: at least four times
+    // this fill's edge count, so that the edges of a landscape that changes
+    // from step to step still fit in half of it
+    {
+        const int64_t want = 4 * (int64_t)p->h_pinned[7];
+        if (want > p->xh_cap) {
+            int64_t cap = 1 << 16;
+            while (cap < want) cap <<= 1;
+            unsigned long long* ptrs[] = {p->xh_key, p->xh_val, p->xd_w};
+            for (unsigned long long* q : ptrs)
+                if (q) cudaFree(q);
+            if (p->xd_u) cudaFree(p->xd_u);
+            if (p->xd_v) cudaFree(p->xd_v);
+            p->xh_key = p->xh_val = p->xd_w = nullptr;
+            p->xd_u = p->xd_v = nullptr;
+            p->xh_cap = 0;
+            GS_CUDA(cudaMalloc((void**)&p->xh_key, sizeof(unsigned long long) * cap));
+            GS_CUDA(cudaMalloc((void**)&p->xh_val, sizeof(unsigned long long) * cap));
+            GS_CUDA(cudaMalloc((void**)&p->xd_u, sizeof(int) * (cap / 2)));
+            GS_CUDA(cudaMalloc((void**)&p->xd_v, sizeof(int) * (cap / 2)));
+            GS_CUDA(cudaMalloc((void**)&p->xd_w, sizeof(unsigned long long) * (cap / 2)));
+            GS_CUDA(cudaMemsetAsync(p->xh_key, 0xff, sizeof(unsigned long long) * cap, p->stream));
+            GS_CUDA(cudaMemsetAsync(p->xh_val, 0xff, sizeof(unsigned long long) * cap, p->stream));
+            p->xh_cap = cap;
+        }
     }
     if (st) st->fill_rounds = p->h_pinned[6];
     const int P = p->npits, np1 = P + 1;
