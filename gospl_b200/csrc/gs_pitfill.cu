@@ -911,9 +911,9 @@ __global__ void __launch_bounds__(256) k_bfs_coop(int* fa, int* fb, int* sizes, 
 // sphere's relief).  Only the lowest of them can lower a level, so the edges
 // go through an open-addressing table keyed by (u, v) that keeps the smallest
 // weight key, and the relaxation runs over one edge per pair.  The table has
-// a power-of-two size of at least twice the edge count (linear probing ends
-// at an empty slot within the table size); when the edges outnumber half the
-// table, the relaxation uses them undeduplicated (*raw = 1).
+// a power-of-two size of about four times the pairs of the previous fill;
+// linear probing gives up after XH_PROBES slots, and then the relaxation uses
+// the edges as emitted (*raw = 1) and the next fill gets a larger table.
 __device__ __forceinline__ unsigned long long xh_mix(unsigned long long k) {
     // the 64-bit finaliser of MurmurHash3 (Appleby)
     k ^= k >> 33;
@@ -924,28 +924,29 @@ __device__ __forceinline__ unsigned long long xh_mix(unsigned long long k) {
     return k;
 }
 
+constexpr int XH_PROBES = 64;
+
 __global__ void k_xedge_insert(const int* __restrict__ m_count, int cap, const int* __restrict__ xu,
                                const int* __restrict__ xv, const double* __restrict__ xw,
                                unsigned long long* hkey, unsigned long long* hval, long long hcap, int* raw) {
     const int m = *m_count < cap ? *m_count : cap;
-    if (2LL * m > hcap) {
-        if (blockIdx.x == 0 && threadIdx.x == 0) *raw = 1;
-        return;
-    }
     const int gtid = blockIdx.x * blockDim.x + threadIdx.x, gsz = gridDim.x * blockDim.x;
     const unsigned long long mask = (unsigned long long)hcap - 1ULL;
     for (int e = gtid; e < m; e += gsz) {
         const unsigned long long key = ((unsigned long long)(unsigned)xu[e] << 32) | (unsigned)xv[e];
         const unsigned long long w = dkey(xw[e]);
         unsigned long long s = xh_mix(key) & mask;
-        for (long long probe = 0; probe < hcap; probe++) {
+        bool placed = false;
+        for (int probe = 0; probe < XH_PROBES; probe++) {
             const unsigned long long k = atomicCAS(&hkey[s], ~0ULL, key);
             if (k == ~0ULL || k == key) {
                 atomicMin(&hval[s], w);
+                placed = true;
                 break;
             }
             s = (s + 1ULL) & mask;
         }
+        if (!placed) *raw = 1;
     }
 }
 
@@ -1097,7 +1098,12 @@ __global__ void k_pit_compact(int n, const int* __restrict__ pit, const int* __r
 }
 
 // Block-per-pit reductions in a fixed order (deterministic): strided partial
-// sums per thread, then a fixed shared-memory tree.
+// sums per thread, then a fixed shared-memory tree.  A thread visits its
+// cells t = lane, lane + 256, ... in order; the cells of PIT_UNROLL visits and
+// their values are loaded before any is added, so that the gathers of a large
+// pit overlap, and the additions keep the visiting order.
+constexpr int PIT_UNROLL = 8;
+
 template <int NV>
 __device__ __forceinline__ void block_reduce(double (&v)[NV], bool is_max[NV]) {
     __shared__ double sh[NV][256];
@@ -1123,13 +1129,27 @@ __global__ void __launch_bounds__(256) k_pit_params(int np1, const int* __restri
     if (p >= np1) return;
     int s0 = start[p], c = counts[p];
     double v[3] = {0.0, -INFINITY, -INFINITY};
-    for (int t = lane; t < c; t += 256) {
-        int i = cells[s0 + t];
-        double hc = h[i] < sl ? sl : h[i];
-        double d = f[i] - hc;
-        v[0] += d * larea[i];
-        v[1] = fmax(v[1], f[i]);
-        v[2] = fmax(v[2], d);
+    for (int t0 = lane; t0 < c; t0 += 256 * PIT_UNROLL) {
+        int ii[PIT_UNROLL];
+        double fi[PIT_UNROLL], hi[PIT_UNROLL], ai[PIT_UNROLL];
+#pragma unroll
+        for (int u = 0; u < PIT_UNROLL; u++) ii[u] = t0 + u * 256 < c ? cells[s0 + t0 + u * 256] : -1;
+#pragma unroll
+        for (int u = 0; u < PIT_UNROLL; u++) {
+            if (ii[u] < 0) continue;
+            fi[u] = f[ii[u]];
+            hi[u] = h[ii[u]];
+            ai[u] = larea[ii[u]];
+        }
+#pragma unroll
+        for (int u = 0; u < PIT_UNROLL; u++) {
+            if (ii[u] < 0) continue;
+            double hc = hi[u] < sl ? sl : hi[u];
+            double d = fi[u] - hc;
+            v[0] += d * ai[u];
+            v[1] = fmax(v[1], fi[u]);
+            v[2] = fmax(v[2], d);
+        }
     }
     bool mx[3] = {false, true, true};
     block_reduce<3>(v, mx);
@@ -1173,14 +1193,27 @@ __global__ void __launch_bounds__(256) k_filled_vol(int np1, const int* __restri
     int s0 = start[p], c = counts[p];
     double l0 = lvl[5 * p], l1 = lvl[5 * p + 1], l2 = lvl[5 * p + 2], l3 = lvl[5 * p + 3];
     double v[4] = {0, 0, 0, 0};
-    for (int t = lane; t < c; t += 256) {
-        int i = cells[s0 + t];
-        double e = h[i] < sl ? sl : h[i];
-        double a = farea[i];
-        if (l0 > e) v[0] += (l0 - e) * a;
-        if (l1 > e) v[1] += (l1 - e) * a;
-        if (l2 > e) v[2] += (l2 - e) * a;
-        if (l3 > e) v[3] += (l3 - e) * a;
+    for (int t0 = lane; t0 < c; t0 += 256 * PIT_UNROLL) {
+        int ii[PIT_UNROLL];
+        double hi[PIT_UNROLL], ai[PIT_UNROLL];
+#pragma unroll
+        for (int u = 0; u < PIT_UNROLL; u++) ii[u] = t0 + u * 256 < c ? cells[s0 + t0 + u * 256] : -1;
+#pragma unroll
+        for (int u = 0; u < PIT_UNROLL; u++) {
+            if (ii[u] < 0) continue;
+            hi[u] = h[ii[u]];
+            ai[u] = farea[ii[u]];
+        }
+#pragma unroll
+        for (int u = 0; u < PIT_UNROLL; u++) {
+            if (ii[u] < 0) continue;
+            double e = hi[u] < sl ? sl : hi[u];
+            double a = ai[u];
+            if (l0 > e) v[0] += (l0 - e) * a;
+            if (l1 > e) v[1] += (l1 - e) * a;
+            if (l2 > e) v[2] += (l2 - e) * a;
+            if (l3 > e) v[3] += (l3 - e) * a;
+        }
     }
     bool mx[4] = {false, false, false, false};
     block_reduce<4>(v, mx);
@@ -1202,9 +1235,22 @@ __global__ void __launch_bounds__(256) k_pit_masked_sum(int np1, const int* __re
     if (p >= np1) return;
     int s0 = start[p], c = counts[p];
     double v[1] = {0.0};
-    for (int t = lane; t < c; t += 256) {
-        int i = cells[s0 + t];
-        if (mask[i]) v[0] += vals[i];
+    for (int t0 = lane; t0 < c; t0 += 256 * PIT_UNROLL) {
+        int ii[PIT_UNROLL];
+        uint8_t mi[PIT_UNROLL];
+        double xi[PIT_UNROLL];
+#pragma unroll
+        for (int u = 0; u < PIT_UNROLL; u++) ii[u] = t0 + u * 256 < c ? cells[s0 + t0 + u * 256] : -1;
+#pragma unroll
+        for (int u = 0; u < PIT_UNROLL; u++) {
+            mi[u] = 0;
+            if (ii[u] < 0) continue;
+            mi[u] = mask[ii[u]];
+            xi[u] = vals[ii[u]];
+        }
+#pragma unroll
+        for (int u = 0; u < PIT_UNROLL; u++)
+            if (mi[u]) v[0] += xi[u];
     }
     bool mx[1] = {false};
     block_reduce<1>(v, mx);
@@ -1392,6 +1438,9 @@ int fill_elevation(gs_plan* p, const double* h, double sealevel, double ofill, d
                         (void*)&p->xe_w,  (void*)&mdc,      (void*)&p->xd_u,   (void*)&p->xd_v, (void*)&p->xd_w,
                         (void*)&p->basinL, (void*)&flags,   (void*)&maxr,      (void*)&rout};
         GS_TRY(launch_coop(p, (const void*)k_relax_active, args));
+        // the table's outcome, for its size at the next fill
+        GS_CUDA(cudaMemcpyAsync(p->h_pinned + 11, p->i_scalar + I_XRAW, sizeof(int) * 2, cudaMemcpyDeviceToHost,
+                                p->stream));
         GS_CUDA(cudaMemcpyAsync(p->h_pinned + 6, p->i_scalar + I_CHANGED, sizeof(int), cudaMemcpyDeviceToHost,
                                 p->stream));
         GS_CUDA(cudaMemcpyAsync(p->h_pinned + 7, p->i_scalar + I_NEXT, sizeof(int), cudaMemcpyDeviceToHost,
@@ -1435,13 +1484,15 @@ int fill_elevation(gs_plan* p, const double* h, double sealevel, double ofill, d
         set_error(GS_ENOMEM, "pit fill: cross-edge capacity exceeded");
         return GS_ENOMEM;
     }
-    // size the deduplication table for the next fill: at least four times
-    // this fill's edge count, so that the edges of a landscape that changes
-    // from step to step still fit in half of it
+    // size the deduplication table for the next fill: four times this fill's
+    // basin pairs (its edge count when the pairs are not known: no table yet,
+    // or probing gave up), grown at once, shrunk only when 16 times too large
     {
-        const int64_t want = 4 * (int64_t)p->h_pinned[7];
-        if (want > p->xh_cap) {
-            int64_t cap = 1 << 16;
+        const bool known = p->xh_cap > 0 && !p->h_pinned[11];
+        const int64_t pairs = known ? (int64_t)p->h_pinned[12] : (int64_t)p->h_pinned[7];
+        const int64_t want = std::max<int64_t>(4 * pairs, 1 << 12);
+        if (want > p->xh_cap || (known && p->xh_cap > 4 * want)) {
+            int64_t cap = 1 << 12;
             while (cap < want) cap <<= 1;
             unsigned long long* ptrs[] = {p->xh_key, p->xh_val, p->xd_w};
             for (unsigned long long* q : ptrs)
@@ -1453,9 +1504,9 @@ int fill_elevation(gs_plan* p, const double* h, double sealevel, double ofill, d
             p->xh_cap = 0;
             GS_CUDA(cudaMalloc((void**)&p->xh_key, sizeof(unsigned long long) * cap));
             GS_CUDA(cudaMalloc((void**)&p->xh_val, sizeof(unsigned long long) * cap));
-            GS_CUDA(cudaMalloc((void**)&p->xd_u, sizeof(int) * (cap / 2)));
-            GS_CUDA(cudaMalloc((void**)&p->xd_v, sizeof(int) * (cap / 2)));
-            GS_CUDA(cudaMalloc((void**)&p->xd_w, sizeof(unsigned long long) * (cap / 2)));
+            GS_CUDA(cudaMalloc((void**)&p->xd_u, sizeof(int) * cap));
+            GS_CUDA(cudaMalloc((void**)&p->xd_v, sizeof(int) * cap));
+            GS_CUDA(cudaMalloc((void**)&p->xd_w, sizeof(unsigned long long) * cap));
             GS_CUDA(cudaMemsetAsync(p->xh_key, 0xff, sizeof(unsigned long long) * cap, p->stream));
             GS_CUDA(cudaMemsetAsync(p->xh_val, 0xff, sizeof(unsigned long long) * cap, p->stream));
             p->xh_cap = cap;

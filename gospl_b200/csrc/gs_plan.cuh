@@ -119,7 +119,7 @@ struct gs_plan {
     unsigned long long* xh_key = nullptr; // [xh_cap] basin-pair table of the edge deduplication (~0: empty)
     unsigned long long* xh_val = nullptr; // [xh_cap] smallest weight key of the pair
     int64_t xh_cap = 0;                   // power of two (0: no table, edges used as emitted)
-    int* xd_u = nullptr;                  // [xh_cap / 2] deduplicated edges
+    int* xd_u = nullptr;                  // [xh_cap] deduplicated edges
     int* xd_v = nullptr;
     unsigned long long* xd_w = nullptr;
     int* bfs_rows = nullptr;             // packed BFS adjacency rows, stride ((W+4)/4)*4
