@@ -546,6 +546,11 @@ __global__ void k_bfs_local_scatter(int M, const int* __restrict__ l2g, const in
 
 constexpr int LBFS_CAP = 6144;
 
+// S4: int4 words of a packed adjacency row (S = 4 * S4 ints, row[0] the
+// count).  A level's cost is the instruction chain of its busiest warp, so
+// the row width is a compile-time constant and the claimed cells are
+// appended by walking the set bits of the claim mask.
+template <int S4>
 __global__ void __launch_bounds__(1024) k_bfs_local(int M, int S, const int* __restrict__ rows,
                                                     const int* __restrict__ seeds, const int* __restrict__ nseed_p,
                                                     int* gA, int* gB, int* ld, int* levels_out) {
@@ -575,7 +580,6 @@ __global__ void __launch_bounds__(1024) k_bfs_local(int M, int S, const int* __r
     int* nxtS = fB;
     int* curG = gA;
     int* nxtG = gB;
-    const int S4 = S >> 2;
     int d = 1, levels = 0, r = 0;
     while (size > 0 && levels <= M) {
         int* cnt = &s_cnt[(r + 1) % 3];
@@ -585,40 +589,32 @@ __global__ void __launch_bounds__(1024) k_bfs_local(int M, int S, const int* __r
             const int t = base + tid;
             // warps past the end of the frontier go straight to the barrier
             if (!__any_sync(0xffffffffu, t < size)) break;
-            int row[16];
+            constexpr int RW = 4 * S4;
+            int row[RW];
             int k = 0;
             if (t < size) {
                 const int li = t < LBFS_CAP ? curS[t] : curG[t];
                 const int4* r4 = reinterpret_cast<const int4*>(rows + (size_t)li * S);
 #pragma unroll
-                for (int q = 0; q < 4; q++) {
-                    if (q < S4) {
-                        int4 v = r4[q];
-                        row[4 * q] = v.x; row[4 * q + 1] = v.y; row[4 * q + 2] = v.z; row[4 * q + 3] = v.w;
-                    }
+                for (int q = 0; q < S4; q++) {
+                    int4 v = r4[q];
+                    row[4 * q] = v.x; row[4 * q + 1] = v.y; row[4 * q + 2] = v.z; row[4 * q + 3] = v.w;
                 }
                 k = row[0];
             }
             // claim the unvisited out-neighbours: plain checks, then the
             // atomics, all independent so their latencies overlap
-            const int kmax = __reduce_max_sync(0xffffffffu, k);
             unsigned cand = 0u;
 #pragma unroll
-            for (int q = 1; q < 16; q++) {
-                if (q > kmax) break;
+            for (int q = 1; q < RW; q++)
                 if (q <= k && !(vis[row[q] >> 5] & (1u << (row[q] & 31)))) cand |= 1u << q;
-            }
-            unsigned olds[16];
+            unsigned olds[RW];
 #pragma unroll
-            for (int q = 1; q < 16; q++) {
-                if (q > kmax) break;
-                olds[q] = (cand & (1u << q)) ? atomicOr(&vis[row[q] >> 5], 1u << (row[q] & 31)) : 0xffffffffu;
-            }
+            for (int q = 1; q < RW; q++)
+                olds[q] = (cand & (1u << q)) ? atomicOr(&vis[row[q] >> 5], 1u << (row[q] & 31)) : 0u;
 #pragma unroll
-            for (int q = 1; q < 16; q++) {
-                if (q > kmax) break;
-                if ((cand & (1u << q)) && (olds[q] & (1u << (row[q] & 31)))) cand &= ~(1u << q);
-            }
+            for (int q = 1; q < RW; q++)
+                if (olds[q] & (1u << (row[q] & 31))) cand &= ~(1u << q);
             // warp-aggregated append of the claimed cells
             const int mine = __popc(cand);
             int incl = mine;
@@ -633,8 +629,7 @@ __global__ void __launch_bounds__(1024) k_bfs_local(int M, int S, const int* __r
             pos0 = __shfl_sync(0xffffffffu, pos0, 31);
             int pos = pos0 + incl - mine;
 #pragma unroll
-            for (int q = 1; q < 16; q++) {
-                if (q > kmax) break;
+            for (int q = 1; q < RW; q++) {
                 if (cand & (1u << q)) {
                     const int c = row[q];
                     ld[c] = d + 1;
@@ -1612,14 +1607,21 @@ int fill_elevation(gs_plan* p, const double* h, double sealevel, double ofill, d
                     GS_TRY(bfs_tiles(p, M, S, rows, ldv));
                 } else {
                     // one block: visited bitmap and frontiers in shared memory
-                    GS_CUDA(cudaFuncSetAttribute(k_bfs_local, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                 (int)smem1));
-                    cudaEvent_t stop = nullptr;
-                    if (p->profiling) prof_begin(p, (const void*)k_bfs_local, &stop);
-                    k_bfs_local<<<1, 1024, smem1, p->stream>>>(M, S, (const int*)rows, (const int*)p->front0,
-                                                                p->i_scalar + 6, p->front1, p->minseed, ldv,
-                                                                p->i_scalar + 4);
-                    if (stop) cudaEventRecord(stop, p->stream);
+                    auto run = [&](auto kern) -> int {
+                        GS_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem1));
+                        cudaEvent_t stop = nullptr;
+                        if (p->profiling) prof_begin(p, (const void*)kern, &stop);
+                        kern<<<1, 1024, smem1, p->stream>>>(M, S, (const int*)rows, (const int*)p->front0,
+                                                            p->i_scalar + 6, p->front1, p->minseed, ldv,
+                                                            p->i_scalar + 4);
+                        if (stop) cudaEventRecord(stop, p->stream);
+                        return GS_OK;
+                    };
+                    const int S4 = S / 4;
+                    if (S4 <= 1) GS_TRY(run(k_bfs_local<1>));
+                    else if (S4 == 2) GS_TRY(run(k_bfs_local<2>));
+                    else if (S4 == 3) GS_TRY(run(k_bfs_local<3>));
+                    else GS_TRY(run(k_bfs_local<4>));
                     p->launches++;
                     GS_LAUNCH();
                 }
