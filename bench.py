@@ -1062,8 +1062,8 @@ def step_algo_bytes(L):
 NCU_TRAFFIC_PER_VERTEX = {
     "k_mfd_receivers": (24.905728e6 + 2.152192e6) / 655362,
     "k_ordered_flow": (38.153216e6 + 1.851392e6) / 655362,
-    "k_bfs_local": 1.788672e6 / 655362,
-    "k_relax_active": (5.856768e6 + 0.024320e6) / 655362,
+    "k_bfs_local": 1.780992e6 / 655362,
+    "k_relax_active": (1.359360e6 + 0.125440e6) / 655362,
 }
 
 
