@@ -17,7 +17,28 @@ states, land/sea and lake masks) are held fixed, so the gradient is that of
 the piecewise-smooth map on the piece the forward ran on; the level of a
 partially filled lake is held constant.
 """
+import contextlib
+
 import numpy as np
+
+from . import _lib
+
+GS_TUNE_WARM_START = 8
+
+
+@contextlib.contextmanager
+def _cold(model):
+    """Solver warm starts off (GS_TUNE_WARM_START = 0) while the adjoint runs:
+    a warm-started CG depends on the previous step's solution, so a replayed
+    segment and the two runs of a finite difference would differ from the
+    forward in the solver's last digits."""
+    L = _lib.load()
+    prev = int(L.gs_plan_tuning(model._plan, GS_TUNE_WARM_START))
+    _lib.check(L.gs_plan_tune(model._plan, GS_TUNE_WARM_START, 0))
+    try:
+        yield
+    finally:
+        _lib.check(L.gs_plan_tune(model._plan, GS_TUNE_WARM_START, prev))
 
 
 def _set_params(model, K, U, rain):
@@ -43,6 +64,11 @@ def run(model, K, U, rain, h0, nsteps, every=10):
     """Forward with checkpoints: (h_T, [h at steps 0, every, 2 every, ...]);
     with every=None every step is recorded for the backward instead
     (h_T, None)."""
+    with _cold(model):
+        return _run(model, K, U, rain, h0, nsteps, every)
+
+
+def _run(model, K, U, rain, h0, nsteps, every):
     _set_params(model, K, U, rain)
     _restart(model, h0)
     if every is None:
@@ -65,6 +91,11 @@ def run(model, K, U, rain, h0, nsteps, every=10):
 def backward(model, K, U, rain, ckpt, nsteps, every, lam_T):
     """dJ/d(K, U, rain, h0) from lam_T = dJ/dh_T by checkpointed replay, or
     from the records of a forward run with every=None."""
+    with _cold(model):
+        return _backward(model, K, U, rain, ckpt, nsteps, every, lam_T)
+
+
+def _backward(model, K, U, rain, ckpt, nsteps, every, lam_T):
     t = model.torch
     n = model.lpoints
     f64 = dict(dtype=t.float64, device=model.dev)

@@ -240,13 +240,23 @@ __global__ void k_cg_rotate(const double* __restrict__ sc_new, double* sc) {
 }
 
 __global__ void k_hill_apply(int n, const double* __restrict__ hold, const double* __restrict__ x, double dt,
-                             double* h, double* cum_ed, double* eb) {
+                             double* h, double* cum_ed, double* eb, double* dz_out) {
     int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
     double dz = x[k] - hold[k];
     cum_ed[k] = cum_ed[k] + dz;
     h[k] = x[k];
     eb[k] = eb[k] + dz / dt;
+    if (dz_out) dz_out[k] = dz;
+}
+
+// start of the hillslope CG: this step's elevation plus the previous step's
+// diffusion change (fixed rows keep their elevation)
+__global__ void k_hill_guess(int n, const double* __restrict__ hold, const double* __restrict__ dprev,
+                             const uint8_t* __restrict__ fix, double* g) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    g[k] = fix[k] ? hold[k] : hold[k] + dprev[k];
 }
 
 __global__ void k_copy_d2(int n, const double* __restrict__ a, double* b) {
@@ -662,7 +672,8 @@ int hillslope(gs_plan* p, double* h, double* cum_ed, double* eb, double sealevel
         double relres = 0.0;
         const double tol = std::max(rtol, p->refine_tol);
         GS_TRY(hillslope_refine32(p, tol, max_iter, &outer, &relres));
-        launch(p, k_hill_apply, G, B, n, (const double*)hold, (const double*)p->cg_x, dt, h, cum_ed, eb);
+        launch(p, k_hill_apply, G, B, n, (const double*)hold, (const double*)p->cg_x, dt, h, cum_ed, eb,
+               (double*)nullptr);
         GS_LAUNCH();
         if (st) {
             st->cg_iters = outer;
@@ -681,11 +692,25 @@ int hillslope(gs_plan* p, double* h, double* cum_ed, double* eb, double sealevel
     int* it_d = p->i_scalar + 12;
     double* res_d = p->red + 4100;
     GS_TRY(cg_second_direction(p));
+    // The CG starts from h plus the last step's diffusion change: the change
+    // varies slowly from step to step, so the start residual is a fraction of
+    // the change's own and one iteration fewer reaches the tolerance.  The
+    // solution is the same to the solver tolerance.
+    if (!p->hill_dprev) {
+        GS_CUDA(cudaMalloc((void**)&p->hill_dprev, sizeof(double) * (size_t)n));
+        p->hill_dprev_ok = 0;
+    }
+    const double* guess = nullptr;
+    if (p->hill_dprev_ok && p->warm_start) {
+        launch(p, k_hill_guess, G, B, n, (const double*)hold, (const double*)p->hill_dprev,
+               (const uint8_t*)p->dfix, p->cg_x);
+        GS_LAUNCH();
+        guess = p->cg_x;   // read before written, row by row, with equal values
+    }
     {
         int nn = n, mi = max_iter;
         double rt = rtol;
         const double* x0 = hold;
-        const double* guess = nullptr;
         void* args[] = {(void*)&nn, (void*)&p->nbr, (void*)&p->nnb, (void*)&p->dcoef, (void*)&p->farea,
                         (void*)&p->dfix, (void*)&x0, (void*)&p->cg_x, (void*)&p->cg_b, (void*)&p->cg_r,
                         (void*)&p->cg_z, (void*)&p->cg_p, (void*)&p->cg_p2, (void*)&p->cg_ap, (void*)&p->red,
@@ -696,8 +721,10 @@ int hillslope(gs_plan* p, double* h, double* cum_ed, double* eb, double sealevel
         if (stop) cudaEventRecord(stop, p->stream);
         p->launches++;
     }
-    launch(p, k_hill_apply, G, B, n, (const double*)hold, (const double*)p->cg_x, dt, h, cum_ed, eb);
+    launch(p, k_hill_apply, G, B, n, (const double*)hold, (const double*)p->cg_x, dt, h, cum_ed, eb,
+           p->hill_dprev);
     GS_LAUNCH();
+    p->hill_dprev_ok = p->warm_start;
     int it = 0;
     double relres = 0.0;
     GS_CUDA(cudaMemcpyAsync(&it, it_d, sizeof(int), cudaMemcpyDeviceToHost, p->stream));

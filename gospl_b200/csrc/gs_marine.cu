@@ -693,9 +693,9 @@ int sea_change(gs_plan* p, double* h, double* cum_ed, double* eb, const double* 
             p->sea_prev_ok = 0;
         }
         GS_TRY(diffusion_solve_on(p, n, p->nbr, p->nnb, p->farea, p->dfix, p->flat, p->outlet, p->sea_coef, hl, hsm,
-                                  1.0e-14, 5000, &smooth_iters, p->sea_prev_ok ? (const double*)p->sea_prev : nullptr));
+                                  1.0e-14, 5000, &smooth_iters, (p->sea_prev_ok && p->warm_start) ? (const double*)p->sea_prev : nullptr));
         GS_CUDA(cudaMemcpyAsync(p->sea_prev, hsm, sizeof(double) * N, cudaMemcpyDeviceToDevice, p->stream));
-        p->sea_prev_ok = 1;
+        p->sea_prev_ok = p->warm_start;
         base = hsm;
     }
     unsigned long long* mk = p->u_scalar + 6;

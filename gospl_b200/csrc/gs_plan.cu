@@ -44,7 +44,7 @@ static void plan_free(gs_plan* p) {
                     p->seg_keys2, p->seg_vals2, p->seg_start, p->seg_count, p->cub_tmp, p->nfa, p->wf,
                     p->hl, p->dcoef, p->dsea, p->dsea2, p->dfix, p->cg_r, p->cg_z, p->cg_p, p->cg_p2, p->cg_ap, p->cg_x, p->cg_b,
                     p->red, p->cub_tmp2, p->pflag, p->pscan, p->f32a, p->f32b, p->f32c, p->f32d, p->f32e, p->r64, p->ed_buf,
-                    p->sed_buf, p->sed_mask, p->ed_basis, p->sed_pit, p->led, p->led_part, p->sea_buf, p->sea_u8, p->sea_coef, p->sea_pts, p->sea_prev, p->xh_key, p->xh_val, p->xd_u, p->xd_v, p->xd_w, p->sed_coef, p->lake_i, p->lake_d, p->lake_u8};
+                    p->sed_buf, p->sed_mask, p->ed_basis, p->sed_pit, p->led, p->led_part, p->sea_buf, p->sea_u8, p->sea_coef, p->sea_pts, p->sea_prev, p->hill_dprev, p->xh_key, p->xh_val, p->xd_u, p->xd_v, p->xd_w, p->sed_coef, p->lake_i, p->lake_d, p->lake_u8};
     for (void* q : ptrs)
         if (q) cudaFree(q);
     cudaEvent_t evs[] = {p->ev_fork_a, p->ev_a, p->ev_fork_b, p->ev_b};
@@ -412,6 +412,16 @@ int plan_tune(gs_plan* p, int knob, int value) {
         p->sweep_nap = (unsigned)value;
         return GS_OK;
     }
+    if (knob == GS_TUNE_WARM_START) {
+        if (value != 0 && value != 1) {
+            set_error(GS_EINVAL, "tune: warm start must be 0 or 1");
+            return GS_EINVAL;
+        }
+        p->warm_start = value;
+        p->hill_dprev_ok = 0;
+        p->sea_prev_ok = 0;
+        return GS_OK;
+    }
     if (knob == GS_TUNE_FLAT_BFS) {
         if (value < 0 || value > 4096) {
             set_error(GS_EINVAL, "tune: flat BFS must be 0 (one block) or a window of 1..4096 levels (tiles)");
@@ -439,6 +449,7 @@ int plan_tuning(const gs_plan* p, int knob) {
     if (knob == GS_TUNE_SWEEP_NAP) return (int)p->sweep_nap;
     if (knob == GS_TUNE_SWEEP_BUDGET) return (int)(p->sweep_budget_ns / 1000ULL);
     if (knob == GS_TUNE_FLAT_BFS) return p->bfs_window;
+    if (knob == GS_TUNE_WARM_START) return p->warm_start;
     if (knob == GS_TUNE_REFINE_PASSES) return (int)std::min<int64_t>(p->refine_iters, 0x7fffffff);
     return -1;
 }

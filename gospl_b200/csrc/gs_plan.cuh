@@ -37,6 +37,9 @@ struct gs_plan {
     double* sea_coef = nullptr;          // [W+1][n] bathymetry smoothing operator
     double* sea_pts = nullptr;           // coastline points, sorted copies, keys and boxes
     int64_t sea_pts_cap = 0;             // edges the coastline buffers hold
+    double* hill_dprev = nullptr;        // [n] the last hillslope change (start of the next CG)
+    int hill_dprev_ok = 0;
+    int warm_start = 1;                  // GS_TUNE_WARM_START
     double* sea_prev = nullptr;          // [n] the last smoothed bathymetry (start of the next smoothing)
     int sea_prev_ok = 0;                 // sea_prev holds a smoothing of this plan's mesh
     size_t sea_sort_bytes = 0;           // sort scratch at the end of sea_pts

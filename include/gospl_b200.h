@@ -97,6 +97,11 @@ int gs_plan_set_stream(gs_plan* plan, void* cuda_stream);
 #define GS_TUNE_FLAT_BFS 7        /* flat-distance BFS: 0 one block with the visited set in shared memory
                                      (default; tiles when the set does not fit), w in 1..4096 tiles in one
                                      cooperative launch settling distance windows of w levels */
+#define GS_TUNE_WARM_START 8      /* 1 (default): the hillslope CG starts from h plus the previous step's
+                                     diffusion change and the bathymetry smoothing from the previous
+                                     smoothing; 0: both start from their right-hand side, so that a step
+                                     depends only on its inputs (the adjoint's runs and their finite-
+                                     difference checks).  Setting it forgets the stored starts. */
 int gs_plan_tune(gs_plan* plan, int32_t knob, int32_t value);
 /*
  * Precision form (no counterpart in the reference, which is FP64 only).

@@ -203,16 +203,19 @@ def test_adjoint_matches_dense_autograd():
     f64 = dict(dtype=torch.float64, device=dev)
     Kt, Ut, Rt, h0 = (torch.tensor(a, **f64) for a in (K, U, rain, z))
     nsteps = 3
-    # GPU forward, keeping each step's receivers and masks
+    # GPU forward, keeping each step's receivers and masks; solver warm starts
+    # off, as in the adjoint's own runs (A.run), so that A.run repeats it bit
+    # for bit
     A._set_params(model, Kt, Ut, Rt)
     A._restart(model, h0)
     structure, hs = [], []
-    for _ in range(nsteps):
-        model.step()
-        assert model.stats["flow"]["cascade_passes"] == 0
-        structure.append((model.rcv_i.clone(), model.dist_i.clone(), model.lsink_mask.bool().clone(),
-                          model.sea_mask.bool().clone()))
-        hs.append(model.hGlobal.clone())
+    with A._cold(model):
+        for _ in range(nsteps):
+            model.step()
+            assert model.stats["flow"]["cascade_passes"] == 0
+            structure.append((model.rcv_i.clone(), model.dist_i.clone(), model.lsink_mask.bool().clone(),
+                              model.sea_mask.bool().clone()))
+            hs.append(model.hGlobal.clone())
     hT = hs[-1]
     rng = np.random.default_rng(4)
     target = hT + 1e-3 * torch.tensor(rng.standard_normal(n), **f64)
