@@ -1387,8 +1387,13 @@ int fill_elevation(gs_plan* p, const double* h, double sealevel, double ofill, d
            (const int8_t*)p->nnb, (const int8_t*)p->ledge, p->parent);
     GS_LAUNCH();
     for (int round = 0; round < 64; round++) {
+        // two launches a round; the flag is cleared between them, so it tells
+        // whether the second one still met a chain longer than JUMP_HOPS (a
+        // launch in which every vertex reached its root leaves the roots)
         GS_CUDA(cudaMemsetAsync(p->i_scalar + I_CHANGED, 0, sizeof(int), p->stream));
-        for (int r = 0; r < 2; r++) launch(p, k_jump, G, B, n, p->parent, p->i_scalar + I_CHANGED);
+        launch(p, k_jump, G, B, n, p->parent, p->i_scalar + I_CHANGED);
+        GS_CUDA(cudaMemsetAsync(p->i_scalar + I_CHANGED, 0, sizeof(int), p->stream));
+        launch(p, k_jump, G, B, n, p->parent, p->i_scalar + I_CHANGED);
         GS_LAUNCH();
         GS_TRY(read_ints(p, hbuf, p->i_scalar + I_CHANGED, 1));
         if (round == 0 && p->h_pinned[9]) {
