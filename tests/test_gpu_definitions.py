@@ -211,3 +211,26 @@ def test_flat_bfs_forms_are_the_definition(window):
         check_gpu_fill(gm, om, h0, False, "%s window %d" % (case, window))
         check_gpu_fill(gm, om, h0, True, "%s sed window %d" % (case, window))
         gm.destroy()
+
+
+def test_fill_is_the_definition_when_the_basin_pair_table_overflows():
+    """The basin-pair table of the fill's relaxation is sized from the plan's
+    previous fill.  A tilted plane first (no interior basin: the smallest
+    table), then white-noise relief on the same plan (hundreds of basins and
+    thousands of basin pairs: probing gives up and the relaxation takes the
+    edges as emitted), then the same relief again (the table has grown): the
+    filled surface, the labels and the flat directions are their definitions
+    every time."""
+    from test_definitions import _planar_oracle
+    om = _planar_oracle("ffff", n=6000, seed=9)
+    gm = _model_like(om)
+    xy = np.asarray(om.mesh["coords"])[:, :2]
+    onb = np.zeros(om.lpoints, bool)
+    onb[om.outletIDs] = True
+    plane = 1.0 + 1.0e-3 * (xy[:, 0] - xy[:, 0].min())
+    plane[onb] = 0.0
+    noise = np.random.default_rng(12).uniform(1.0, 50.0, om.lpoints)
+    noise[onb] = 0.0
+    for h, tag in ((plane, "plane"), (noise, "noise, small table"), (noise, "noise, grown table")):
+        check_gpu_fill(gm, om, h, False, tag)
+    gm.destroy()
