@@ -1114,52 +1114,103 @@ __device__ __forceinline__ void block_reduce(double (&v)[NV], bool is_max[NV]) {
     for (int q = 0; q < NV; q++) v[q] = sh[q][0];
 }
 
-// one block per pit: vol, max fill, max depth over its cells (sorted by id)
-__global__ void __launch_bounds__(256) k_pit_params(int np1, const int* __restrict__ start, const int* __restrict__ counts,
-                             const int* __restrict__ cells, const double* __restrict__ f,
-                             const double* __restrict__ h, double sl,
-                             const double* __restrict__ larea, double* params) {
-    int p = blockIdx.x;
-    int lane = threadIdx.x;
+// Per-pit reductions over chunks: a pit's cells (sorted by id, segments of
+// seg_vals2) are cut into chunks of PIT_CHUNK = 256 * PIT_UNROLL cells, one
+// block per chunk, so that a lake of tens of thousands of cells spreads over
+// many blocks instead of holding one block while the others have finished.
+// Within a chunk thread `lane` adds its cells lane, lane + 256, ... in order
+// and the block tree combines the threads; a finishing pass adds a pit's chunk
+// partials in chunk order.  A pit of one chunk therefore sums exactly as a
+// block over the whole pit did.
+constexpr int PIT_CHUNK = 256 * PIT_UNROLL;
+
+__global__ void k_pit_nchunk(int np1, const int* __restrict__ counts, int* nch) {
+    int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p < np1) nch[p] = (counts[p] + PIT_CHUNK - 1) / PIT_CHUNK;
+}
+
+// item -> pit (items of pit p: chs[p] .. chs[p] + nch[p] - 1)
+__global__ void k_pit_items(int np1, const int* __restrict__ nch, const int* __restrict__ chs, int* item_pit) {
+    int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= np1) return;
-    int s0 = start[p], c = counts[p];
+    const int c0 = chs[p], k = nch[p];
+    for (int c = 0; c < k; c++) item_pit[c0 + c] = p;
+}
+
+// the item of this block: its pit, first cell and cell count; false past the last item
+__device__ __forceinline__ bool pit_item(int np1, const int* __restrict__ nch, const int* __restrict__ chs,
+                                         const int* __restrict__ item_pit, const int* __restrict__ start,
+                                         const int* __restrict__ counts, int* p, int* s0, int* c) {
+    const int i = blockIdx.x;
+    if (i >= chs[np1 - 1] + nch[np1 - 1]) return false;
+    const int q = item_pit[i];
+    const int k = i - chs[q];
+    *p = q;
+    *s0 = start[q] + k * PIT_CHUNK;
+    const int rest = counts[q] - k * PIT_CHUNK;
+    *c = rest < PIT_CHUNK ? rest : PIT_CHUNK;
+    return true;
+}
+
+// chunk partials of vol, max fill, max depth (cells sorted by id)
+__global__ void __launch_bounds__(256) k_pit_params(int np1, const int* __restrict__ nch, const int* __restrict__ chs,
+                                                    const int* __restrict__ item_pit,
+                                                    const int* __restrict__ start, const int* __restrict__ counts,
+                                                    const int* __restrict__ cells, const double* __restrict__ f,
+                                                    const double* __restrict__ h, double sl,
+                                                    const double* __restrict__ larea, double* part) {
+    int p, s0, c;
+    if (!pit_item(np1, nch, chs, item_pit, start, counts, &p, &s0, &c)) return;
+    const int lane = threadIdx.x;
     double v[3] = {0.0, -INFINITY, -INFINITY};
-    for (int t0 = lane; t0 < c; t0 += 256 * PIT_UNROLL) {
-        int ii[PIT_UNROLL];
-        double fi[PIT_UNROLL], hi[PIT_UNROLL], ai[PIT_UNROLL];
+    int ii[PIT_UNROLL];
+    double fi[PIT_UNROLL], hi[PIT_UNROLL], ai[PIT_UNROLL];
 #pragma unroll
-        for (int u = 0; u < PIT_UNROLL; u++) ii[u] = t0 + u * 256 < c ? cells[s0 + t0 + u * 256] : -1;
+    for (int u = 0; u < PIT_UNROLL; u++) ii[u] = lane + u * 256 < c ? cells[s0 + lane + u * 256] : -1;
 #pragma unroll
-        for (int u = 0; u < PIT_UNROLL; u++) {
-            if (ii[u] < 0) continue;
-            fi[u] = f[ii[u]];
-            hi[u] = h[ii[u]];
-            ai[u] = larea[ii[u]];
-        }
+    for (int u = 0; u < PIT_UNROLL; u++) {
+        if (ii[u] < 0) continue;
+        fi[u] = f[ii[u]];
+        hi[u] = h[ii[u]];
+        ai[u] = larea[ii[u]];
+    }
 #pragma unroll
-        for (int u = 0; u < PIT_UNROLL; u++) {
-            if (ii[u] < 0) continue;
-            double hc = hi[u] < sl ? sl : hi[u];
-            double d = fi[u] - hc;
-            v[0] += d * ai[u];
-            v[1] = fmax(v[1], fi[u]);
-            v[2] = fmax(v[2], d);
-        }
+    for (int u = 0; u < PIT_UNROLL; u++) {
+        if (ii[u] < 0) continue;
+        double hc = hi[u] < sl ? sl : hi[u];
+        double d = fi[u] - hc;
+        v[0] += d * ai[u];
+        v[1] = fmax(v[1], fi[u]);
+        v[2] = fmax(v[2], d);
     }
     bool mx[3] = {false, true, true};
     block_reduce<3>(v, mx);
-    double vol = v[0], hmax = v[1], dmax = v[2];
-    if (lane == 0) {
-        if (c > 0) {
-            params[3 * p] = vol;
-            params[3 * p + 1] = hmax;
-            params[3 * p + 2] = dmax;
-        } else {
-            params[3 * p] = 0.0;
-            params[3 * p + 1] = -1.0e8;   // MISSING_DATA_SENTINEL (constants.py:34)
-            params[3 * p + 2] = 0.0;
-        }
+    if (lane == 0)
+        for (int q = 0; q < 3; q++) part[3 * (size_t)blockIdx.x + q] = v[q];
+}
+
+// pit params from the chunk partials, in chunk order
+__global__ void k_pit_params_fin(int np1, const int* __restrict__ nch, const int* __restrict__ chs,
+                                 const double* __restrict__ part, double* params) {
+    int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= np1) return;
+    const int k = nch[p];
+    if (k == 0) {
+        params[3 * p] = 0.0;
+        params[3 * p + 1] = -1.0e8;   // MISSING_DATA_SENTINEL (constants.py:34)
+        params[3 * p + 2] = 0.0;
+        return;
     }
+    const size_t i0 = chs[p];
+    double vol = part[3 * i0], hmax = part[3 * i0 + 1], dmax = part[3 * i0 + 2];
+    for (int j = 1; j < k; j++) {
+        vol = vol + part[3 * (i0 + j)];
+        hmax = fmax(hmax, part[3 * (i0 + j) + 1]);
+        dmax = fmax(dmax, part[3 * (i0 + j) + 2]);
+    }
+    params[3 * p] = vol;
+    params[3 * p + 1] = hmax;
+    params[3 * p + 2] = dmax;
 }
 
 __global__ void k_filled_lvl(int np1, const double* __restrict__ params, double* lvl) {
@@ -1178,78 +1229,105 @@ __global__ void k_filled_lvl(int np1, const double* __restrict__ params, double*
     }
 }
 
-__global__ void __launch_bounds__(256) k_filled_vol(int np1, const int* __restrict__ start, const int* __restrict__ counts,
-                             const int* __restrict__ cells, const double* __restrict__ h, double sl,
-                             const double* __restrict__ farea, const double* __restrict__ lvl,
-                             const double* __restrict__ params, double* vol) {
-    int p = blockIdx.x;
-    int lane = threadIdx.x;
-    if (p >= np1) return;
-    int s0 = start[p], c = counts[p];
-    double l0 = lvl[5 * p], l1 = lvl[5 * p + 1], l2 = lvl[5 * p + 2], l3 = lvl[5 * p + 3];
+// chunk partials of the filled volumes at the four intermediate levels
+__global__ void __launch_bounds__(256) k_filled_vol(int np1, const int* __restrict__ nch, const int* __restrict__ chs,
+                                                    const int* __restrict__ item_pit,
+                                                    const int* __restrict__ start, const int* __restrict__ counts,
+                                                    const int* __restrict__ cells, const double* __restrict__ h,
+                                                    double sl, const double* __restrict__ farea,
+                                                    const double* __restrict__ lvl, double* part) {
+    int p, s0, c;
+    if (!pit_item(np1, nch, chs, item_pit, start, counts, &p, &s0, &c)) return;
+    const int lane = threadIdx.x;
+    const double l0 = lvl[5 * p], l1 = lvl[5 * p + 1], l2 = lvl[5 * p + 2], l3 = lvl[5 * p + 3];
     double v[4] = {0, 0, 0, 0};
-    for (int t0 = lane; t0 < c; t0 += 256 * PIT_UNROLL) {
-        int ii[PIT_UNROLL];
-        double hi[PIT_UNROLL], ai[PIT_UNROLL];
+    int ii[PIT_UNROLL];
+    double hi[PIT_UNROLL], ai[PIT_UNROLL];
 #pragma unroll
-        for (int u = 0; u < PIT_UNROLL; u++) ii[u] = t0 + u * 256 < c ? cells[s0 + t0 + u * 256] : -1;
+    for (int u = 0; u < PIT_UNROLL; u++) ii[u] = lane + u * 256 < c ? cells[s0 + lane + u * 256] : -1;
 #pragma unroll
-        for (int u = 0; u < PIT_UNROLL; u++) {
-            if (ii[u] < 0) continue;
-            hi[u] = h[ii[u]];
-            ai[u] = farea[ii[u]];
-        }
+    for (int u = 0; u < PIT_UNROLL; u++) {
+        if (ii[u] < 0) continue;
+        hi[u] = h[ii[u]];
+        ai[u] = farea[ii[u]];
+    }
 #pragma unroll
-        for (int u = 0; u < PIT_UNROLL; u++) {
-            if (ii[u] < 0) continue;
-            double e = hi[u] < sl ? sl : hi[u];
-            double a = ai[u];
-            if (l0 > e) v[0] += (l0 - e) * a;
-            if (l1 > e) v[1] += (l1 - e) * a;
-            if (l2 > e) v[2] += (l2 - e) * a;
-            if (l3 > e) v[3] += (l3 - e) * a;
-        }
+    for (int u = 0; u < PIT_UNROLL; u++) {
+        if (ii[u] < 0) continue;
+        double e = hi[u] < sl ? sl : hi[u];
+        double a = ai[u];
+        if (l0 > e) v[0] += (l0 - e) * a;
+        if (l1 > e) v[1] += (l1 - e) * a;
+        if (l2 > e) v[2] += (l2 - e) * a;
+        if (l3 > e) v[3] += (l3 - e) * a;
     }
     bool mx[4] = {false, false, false, false};
     block_reduce<4>(v, mx);
-    if (lane == 0) {
-        vol[5 * p] = v[0];
-        vol[5 * p + 1] = v[1];
-        vol[5 * p + 2] = v[2];
-        vol[5 * p + 3] = v[3];
-        vol[5 * p + 4] = params[3 * p];
-    }
+    if (lane == 0)
+        for (int q = 0; q < 4; q++) part[4 * (size_t)blockIdx.x + q] = v[q];
 }
 
-// per-pit masked sum (one block per pit), deterministic
-__global__ void __launch_bounds__(256) k_pit_masked_sum(int np1, const int* __restrict__ start, const int* __restrict__ counts,
-                                 const int* __restrict__ cells, const uint8_t* __restrict__ mask,
-                                 const double* __restrict__ vals, double* out) {
-    int p = blockIdx.x;
-    int lane = threadIdx.x;
+__global__ void k_filled_vol_fin(int np1, const int* __restrict__ nch, const int* __restrict__ chs,
+                                 const double* __restrict__ part, const double* __restrict__ params, double* vol) {
+    int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= np1) return;
-    int s0 = start[p], c = counts[p];
-    double v[1] = {0.0};
-    for (int t0 = lane; t0 < c; t0 += 256 * PIT_UNROLL) {
-        int ii[PIT_UNROLL];
-        uint8_t mi[PIT_UNROLL];
-        double xi[PIT_UNROLL];
-#pragma unroll
-        for (int u = 0; u < PIT_UNROLL; u++) ii[u] = t0 + u * 256 < c ? cells[s0 + t0 + u * 256] : -1;
-#pragma unroll
-        for (int u = 0; u < PIT_UNROLL; u++) {
-            mi[u] = 0;
-            if (ii[u] < 0) continue;
-            mi[u] = mask[ii[u]];
-            xi[u] = vals[ii[u]];
-        }
-#pragma unroll
-        for (int u = 0; u < PIT_UNROLL; u++)
-            if (mi[u]) v[0] += xi[u];
+    const int k = nch[p];
+    double v[4] = {0, 0, 0, 0};
+    if (k > 0) {
+        const size_t i0 = chs[p];
+        for (int q = 0; q < 4; q++) v[q] = part[4 * i0 + q];
+        for (int j = 1; j < k; j++)
+            for (int q = 0; q < 4; q++) v[q] = v[q] + part[4 * (i0 + j) + q];
     }
+    for (int q = 0; q < 4; q++) vol[5 * p + q] = v[q];
+    vol[5 * p + 4] = params[3 * p];
+}
+
+// per-pit masked sum: chunk partials, then a pit's partials in chunk order
+__global__ void __launch_bounds__(256) k_pit_masked_sum(int np1, const int* __restrict__ nch,
+                                                        const int* __restrict__ chs,
+                                                        const int* __restrict__ item_pit,
+                                                        const int* __restrict__ start,
+                                                        const int* __restrict__ counts,
+                                                        const int* __restrict__ cells,
+                                                        const uint8_t* __restrict__ mask,
+                                                        const double* __restrict__ vals, double* part) {
+    int p, s0, c;
+    if (!pit_item(np1, nch, chs, item_pit, start, counts, &p, &s0, &c)) return;
+    const int lane = threadIdx.x;
+    double v[1] = {0.0};
+    int ii[PIT_UNROLL];
+    uint8_t mi[PIT_UNROLL];
+    double xi[PIT_UNROLL];
+#pragma unroll
+    for (int u = 0; u < PIT_UNROLL; u++) ii[u] = lane + u * 256 < c ? cells[s0 + lane + u * 256] : -1;
+#pragma unroll
+    for (int u = 0; u < PIT_UNROLL; u++) {
+        mi[u] = 0;
+        if (ii[u] < 0) continue;
+        mi[u] = mask[ii[u]];
+        xi[u] = vals[ii[u]];
+    }
+#pragma unroll
+    for (int u = 0; u < PIT_UNROLL; u++)
+        if (mi[u]) v[0] += xi[u];
     bool mx[1] = {false};
     block_reduce<1>(v, mx);
-    if (lane == 0) out[p] = v[0];
+    if (lane == 0) part[blockIdx.x] = v[0];
+}
+
+__global__ void k_pit_masked_fin(int np1, const int* __restrict__ nch, const int* __restrict__ chs,
+                                 const double* __restrict__ part, double* out) {
+    int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= np1) return;
+    const int k = nch[p];
+    double v = 0.0;
+    if (k > 0) {
+        const int i0 = chs[p];
+        v = part[i0];
+        for (int j = 1; j < k; j++) v = v + part[i0 + j];
+    }
+    out[p] = v;
 }
 
 // --------------------------------------------------------------------------
@@ -1318,12 +1396,47 @@ static int exclusive_scan(gs_plan* p, const int* in, int* out, int count) {
     return GS_OK;
 }
 
+// chunk items of the pit segments (after seg_count and seg_start): at most
+// np1 + ncell / PIT_CHUNK of them, the grid of the chunk kernels
+static int pit_chunks(gs_plan* p, int np1, int ncell) {
+    const int B = 256;
+    const int64_t imax = (int64_t)np1 + ncell / PIT_CHUNK + 1;
+    if (imax > INT_MAX) {
+        set_error(GS_ENOMEM, "pit tables: too many chunk items");
+        return GS_ENOMEM;
+    }
+    if (!p->pit_nch) {
+        GS_CUDA(cudaMalloc((void**)&p->pit_nch, sizeof(int) * ((size_t)p->n + 2)));
+        GS_CUDA(cudaMalloc((void**)&p->pit_chs, sizeof(int) * ((size_t)p->n + 2)));
+    }
+    if (imax > p->pit_item_cap) {
+        const int64_t cap = std::max<int64_t>(imax, 2 * p->pit_item_cap);
+        if (p->pit_item) cudaFree(p->pit_item);
+        if (p->pit_part) cudaFree(p->pit_part);
+        p->pit_item = nullptr;
+        p->pit_part = nullptr;
+        p->pit_item_cap = 0;
+        GS_CUDA(cudaMalloc((void**)&p->pit_item, sizeof(int) * (size_t)cap));
+        GS_CUDA(cudaMalloc((void**)&p->pit_part, sizeof(double) * 4 * (size_t)cap));
+        p->pit_item_cap = cap;
+    }
+    launch(p, k_pit_nchunk, grid_for(np1, B), B, np1, (const int*)p->seg_count, p->pit_nch);
+    GS_LAUNCH();
+    GS_TRY(exclusive_scan(p, p->pit_nch, p->pit_chs, np1));
+    launch(p, k_pit_items, grid_for(np1, B), B, np1, (const int*)p->pit_nch, (const int*)p->pit_chs, p->pit_item);
+    GS_LAUNCH();
+    p->pit_items_max = (int)imax;
+    return GS_OK;
+}
+
 int group_sum_by_pit(gs_plan* p, const int* /*pit_ids*/, const uint8_t* mask, const double* vals,
                      double* out, int npits) {
     const int np1 = npits + 1;
-    launch(p, k_pit_masked_sum, np1, 256, np1,
-           (const int*)p->seg_start, (const int*)p->seg_count, (const int*)p->seg_vals2, mask, vals,
-           out);
+    launch(p, k_pit_masked_sum, p->pit_items_max, 256, np1, (const int*)p->pit_nch, (const int*)p->pit_chs,
+           (const int*)p->pit_item, (const int*)p->seg_start, (const int*)p->seg_count, (const int*)p->seg_vals2,
+           mask, vals, p->pit_part);
+    launch(p, k_pit_masked_fin, grid_for(np1, 256), 256, np1, (const int*)p->pit_nch, (const int*)p->pit_chs,
+           (const double*)p->pit_part, out);
     GS_LAUNCH();
     return GS_OK;
 }
@@ -1572,13 +1685,21 @@ int fill_elevation(gs_plan* p, const double* h, double sealevel, double ofill, d
             p->launches++;
         }
         GS_TRY(exclusive_scan(p, p->seg_count, p->seg_start, np1));
-        launch(p, k_pit_params, np1, 256, np1, (const int*)p->seg_start,
-               (const int*)p->seg_count, (const int*)p->seg_vals2, (const double*)lfill, h, clip_sl,
-               (const double*)p->larea, p->pit_params);
+        GS_TRY(pit_chunks(p, np1, ncell));
+        const int NI = p->pit_items_max;
+        const int* nch = p->pit_nch;
+        const int* chs = p->pit_chs;
+        const int* itp = p->pit_item;
+        launch(p, k_pit_params, NI, 256, np1, nch, chs, itp, (const int*)p->seg_start, (const int*)p->seg_count,
+               (const int*)p->seg_vals2, (const double*)lfill, h, clip_sl, (const double*)p->larea, p->pit_part);
+        launch(p, k_pit_params_fin, grid_for(np1, B), B, np1, nch, chs, (const double*)p->pit_part,
+               p->pit_params);
         launch(p, k_filled_lvl, grid_for(np1, B), B, np1, (const double*)p->pit_params, p->filled_lvl);
-        launch(p, k_filled_vol, np1, 256, np1, (const int*)p->seg_start,
-               (const int*)p->seg_count, (const int*)p->seg_vals2, h, clip_sl, (const double*)p->farea,
-               (const double*)p->filled_lvl, (const double*)p->pit_params, p->filled_vol);
+        launch(p, k_filled_vol, NI, 256, np1, nch, chs, itp, (const int*)p->seg_start, (const int*)p->seg_count,
+               (const int*)p->seg_vals2, h, clip_sl, (const double*)p->farea, (const double*)p->filled_lvl,
+               p->pit_part);
+        launch(p, k_filled_vol_fin, grid_for(np1, B), B, np1, nch, chs, (const double*)p->pit_part,
+               (const double*)p->pit_params, p->filled_vol);
         GS_LAUNCH();
         return GS_OK;
     };

@@ -41,7 +41,7 @@ static void plan_free(gs_plan* p) {
                     p->front0, p->front1, p->spill_flag, p->bestlid, p->d_scalar, p->i_scalar,
                     p->u_scalar, p->pit_params, p->pit_info, p->filled_lvl, p->filled_vol, p->pit_vol,
                     p->pit_in, p->pit_ev, p->pit_win, p->pit_lvl, p->pit_state, p->seg_keys, p->seg_vals,
-                    p->seg_keys2, p->seg_vals2, p->seg_start, p->seg_count, p->cub_tmp, p->nfa, p->wf,
+                    p->seg_keys2, p->seg_vals2, p->seg_start, p->seg_count, p->pit_nch, p->pit_chs, p->pit_item, p->pit_part, p->cub_tmp, p->nfa, p->wf,
                     p->hl, p->dcoef, p->dsea, p->dsea2, p->dfix, p->cg_r, p->cg_z, p->cg_p, p->cg_p2, p->cg_ap, p->cg_x, p->cg_b,
                     p->red, p->cub_tmp2, p->pflag, p->pscan, p->f32a, p->f32b, p->f32c, p->f32d, p->f32e, p->r64, p->ed_buf,
                     p->sed_buf, p->sed_mask, p->ed_basis, p->sed_pit, p->led, p->led_part, p->sea_buf, p->sea_u8, p->sea_coef, p->sea_pts, p->sea_prev, p->hill_dprev, p->xh_key, p->xh_val, p->xd_u, p->xd_v, p->xd_w, p->sed_coef, p->lake_i, p->lake_d, p->lake_u8};

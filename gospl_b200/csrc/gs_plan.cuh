@@ -158,6 +158,12 @@ struct gs_plan {
     int* seg_vals2 = nullptr;
     int* seg_start = nullptr;
     int* seg_count = nullptr;
+    int* pit_nch = nullptr;              // [n + 2] chunks of each pit (per-pit reductions)
+    int* pit_chs = nullptr;              // [n + 2] first chunk item of each pit
+    int* pit_item = nullptr;             // [pit_item_cap] pit of each chunk item
+    double* pit_part = nullptr;          // [4 * pit_item_cap] chunk partials
+    int64_t pit_item_cap = 0;
+    int pit_items_max = 0;               // chunk items of the last fill, at most (the chunk kernels' grid)
     void* cub_tmp = nullptr;
     size_t cub_bytes = 0;
     void* cub_tmp2 = nullptr;            // cub scratch of work issued on side stream A
