@@ -239,6 +239,11 @@ __global__ void k_cg_rotate(const double* __restrict__ sc_new, double* sc) {
     sc[0] = sc_new[0];
 }
 
+// slot of the CG's final residual in the reduction scratch (8192 doubles),
+// beyond the block partials of the cooperative CG (7 per block, at most 4 blocks
+// per SM) and the scalars at 4096..4103
+constexpr int RES_SLOT = 8190;
+
 __global__ void k_hill_apply(int n, const double* __restrict__ hold, const double* __restrict__ x, double dt,
                              double* h, double* cum_ed, double* eb, double* dz_out) {
     int k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -599,7 +604,7 @@ static int hillslope_refine32(gs_plan* p, double tol, int max_iter, int* outer, 
     double relres = bnorm > 0.0 ? sqrt(hs[1]) / bnorm : 0.0;
     int it = 0;
     int* it_d = p->i_scalar + 12;
-    double* res_d = p->red + 4100;
+    double* res_d = p->red + RES_SLOT;
     for (; it < 10 && relres > tol; it++) {
         int nn = n, mi = max_iter;
         double rt = 1.0e-5;
@@ -690,7 +695,7 @@ int hillslope(gs_plan* p, double* h, double* cum_ed, double* eb, double sealevel
         return GS_OK;
     }
     int* it_d = p->i_scalar + 12;
-    double* res_d = p->red + 4100;
+    double* res_d = p->red + RES_SLOT;
     GS_TRY(cg_second_direction(p));
     // The CG starts from h plus the last step's diffusion change: the change
     // varies slowly from step to step, so the start residual is a fraction of
@@ -751,16 +756,22 @@ int hillslope(gs_plan* p, double* h, double* cum_ed, double* eb, double sealevel
 // rows without area held fixed as in the hillslope solve; the cooperative CG on
 // the area-weighted symmetric form.  Used by the non-linear lake diffusion of
 // the sediment step.
+// the worst relative residual of a run of solves (NaN wins), for one check at its end
+__global__ void k_cg_fold(const double* __restrict__ res, double* worst) {
+    const double r = *res, w = *worst;
+    if (!(r == r) || r > w) *worst = r;
+}
+
 int diffusion_solve_on(gs_plan* p, int m, const int* nbr, const int8_t* nnb, const double* farea, const uint8_t* fix,
                        int flat, const uint8_t* outlet, const double* coef, const double* rhs, double* x, double rtol,
-                       int max_iter, int* iters, const double* guess) {
+                       int max_iter, int* iters, const double* guess, double* worst) {
     const int n = m;
     if (n == 0) return GS_OK;
     const int B = 256, G = grid_for(n, B);
     (void)flat;
     (void)outlet;
     int* it_d = p->i_scalar + 12;
-    double* res_d = p->red + 4100;
+    double* res_d = p->red + RES_SLOT;
     GS_TRY(cg_second_direction(p));
     {
         int nn = n, mi = max_iter;
@@ -770,14 +781,24 @@ int diffusion_solve_on(gs_plan* p, int m, const int* nbr, const int8_t* nnb, con
                         (void*)&fix, (void*)&rhs, (void*)&p->cg_x, (void*)&p->cg_b, (void*)&p->cg_r,
                         (void*)&p->cg_z, (void*)&p->cg_p, (void*)&p->cg_p2, (void*)&p->cg_ap, (void*)&p->red,
                         (void*)&rt, (void*)&mi, (void*)&it_d, (void*)&res_d, (void*)&guess};
+        // a small sub-mesh (a few lakes) takes about four rows per thread and
+        // no fewer blocks than SMs: fewer blocks meet at each grid barrier
+        const int nb = std::min(p->coop_blocks, std::max(p->sm_count, (n + 4 * B - 1) / (4 * B)));
         cudaEvent_t stop = nullptr;
         if (p->profiling) prof_begin(p, (const void*)k_cg_coop, &stop);
-        GS_CUDA(cudaLaunchCooperativeKernel((const void*)k_cg_coop, p->coop_blocks, 256, args, 0, p->stream));
+        GS_CUDA(cudaLaunchCooperativeKernel((const void*)k_cg_coop, nb, 256, args, 0, p->stream));
         if (stop) cudaEventRecord(stop, p->stream);
         p->launches++;
     }
     launch(p, k_copy_d2, G, B, n, (const double*)p->cg_x, x);
     GS_LAUNCH();
+    if (worst) {
+        // the caller checks the worst residual of its solves once, at its end
+        launch(p, k_cg_fold, 1, 1, (const double*)res_d, worst);
+        GS_LAUNCH();
+        if (iters) *iters = 0;
+        return GS_OK;
+    }
     int it = 0;
     double relres = 0.0;
     GS_CUDA(cudaMemcpyAsync(&it, it_d, sizeof(int), cudaMemcpyDeviceToHost, p->stream));

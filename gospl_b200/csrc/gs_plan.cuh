@@ -353,7 +353,7 @@ int picard_diffuse(gs_plan* p, const uint8_t* lmask, const double* zb, double* h
 // guess: start of the free rows (nullptr: the right-hand side)
 int diffusion_solve_on(gs_plan* p, int m, const int* nbr, const int8_t* nnb, const double* farea, const uint8_t* fix,
                        int flat, const uint8_t* outlet, const double* coef, const double* rhs, double* x, double rtol,
-                       int max_iter, int* iters, const double* guess = nullptr);
+                       int max_iter, int* iters, const double* guess = nullptr, double* worst = nullptr);
 int hillslope(gs_plan* p, double* h, double* cum_ed, double* eb, double sealevel, double cda,
               double cdm, double dt, double rtol, int max_iter, gs_stats* st);
 int apply_forces(gs_plan* p, double* h, const double* rain, const double* upsub, double dt,

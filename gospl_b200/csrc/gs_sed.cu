@@ -670,6 +670,10 @@ int picard_diffuse(gs_plan* p, const uint8_t* lmask, const double* zb, double* h
            farea_c, fix_c);
     GS_LAUNCH();
     const double dts = dt / p->lake_nsub;
+    // the solves' residuals are checked once, after the last one (they feed
+    // only the device): no host round trip between two Picard iterations
+    double* worst = p->d_scalar + 2;
+    GS_CUDA(cudaMemsetAsync(worst, 0, sizeof(double), p->stream));
     for (int sub = 0; sub < p->lake_nsub; sub++) {
         GS_CUDA(cudaMemcpyAsync(hstart, hcur, sizeof(double) * n, cudaMemcpyDeviceToDevice, p->stream));
         for (int it = 0; it < p->lake_npic; it++) {
@@ -680,10 +684,21 @@ int picard_diffuse(gs_plan* p, const uint8_t* lmask, const double* zb, double* h
                    (const double*)cd, dts, (const double*)hstart, p->sed_coef, rhs_c);
             GS_LAUNCH();
             GS_TRY(diffusion_solve_on(p, m, nbr_c, nnb_c, farea_c, fix_c, 0, nullptr, p->sed_coef, rhs_c, x_c,
-                                      1.0e-13, 5000, nullptr));
+                                      1.0e-13, 5000, nullptr, nullptr, worst));
             launch(p, k_lake_scatter, grid_for(m, B), B, m, (const int*)cell, (const double*)x_c, hcur);
             GS_LAUNCH();
         }
+    }
+    double w = 0.0;
+    GS_CUDA(cudaMemcpyAsync(&w, worst, sizeof(double), cudaMemcpyDeviceToHost, p->stream));
+    GS_CUDA(cudaStreamSynchronize(p->stream));
+    if (!(w == w)) {
+        set_error(GS_ENONFINITE, "diffusion CG produced a non-finite residual");
+        return GS_ENONFINITE;
+    }
+    if (w > 1.0e-13) {
+        set_error(GS_EMAXITER, "diffusion CG reached max_iter");
+        return GS_EMAXITER;
     }
     return GS_OK;
 }
