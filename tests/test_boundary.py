@@ -73,3 +73,17 @@ def test_bad_plan_arguments_are_rejected():
                             ctypes.byref(h)) == 1
     assert L.gs_plan_create(10, None, None, None, None, None, None, None, 0, None, 0, 0, 13,
                             ctypes.byref(h)) == 1
+
+
+def test_knob_numbers_used_from_python_match_the_header():
+    """The GS_TUNE_* numbers that the Python side and the tests pass to
+    gs_plan_tune are the header's."""
+    src = open(os.path.join(ROOT, "include", "gospl_b200.h")).read()
+    header = {k: int(v) for k, v in re.findall(r"#define (GS_TUNE_[A-Z_]+) (\d+)", src)}
+    assert header["GS_TUNE_WARM_START"] == 8
+    from gospl_b200 import adjoint
+    assert adjoint.GS_TUNE_WARM_START == header["GS_TUNE_WARM_START"]
+    import test_gpu_failures
+    import test_gpu_warm_start
+    assert test_gpu_failures.GS_TUNE_SWEEP_BUDGET == header["GS_TUNE_SWEEP_BUDGET"]
+    assert test_gpu_warm_start.GS_TUNE_WARM_START == header["GS_TUNE_WARM_START"]
